@@ -1,0 +1,409 @@
+"""elemental_b200 -- Python binding of libelemgpu.so (the sm_100a factor-and-solve kernels).
+
+The product is the C ABI in include/elemgpu.h (and the C++ drop-in headers in
+include/elemgpu/).  This module binds that ABI with ctypes for tests and
+benchmarks: device-memory calls take column-major torch CUDA tensors, host
+calls take column-major numpy arrays.  There is no CPU fallback: importing
+raises if the CUDA library is missing, and every call raises if the library
+reports an error.
+
+Names follow Elemental (lapack-like/Cholesky.hpp, LU.hpp, HPDSolve.hpp,
+GaussianElimination.hpp, blas-like/level3/{Trsm,Gemm,Herk}.hpp).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libelemgpu.so")
+
+LOWER, UPPER = 0, 1
+NORMAL, TRANSPOSE, ADJOINT = 0, 1, 2
+LEFT, RIGHT = 0, 1
+NON_UNIT, UNIT = 0, 1
+
+OK, NOT_HPD, SINGULAR, TIMEOUT = 0, 1, 2, 3
+
+
+class ElemGPUError(RuntimeError):
+    """A negative return code from libelemgpu (argument, CUDA or allocation error)."""
+
+
+class NonHPDError(ValueError):
+    """Cholesky met a non-positive pivot (the reference throws
+    std::logic_error("A was not numerically HPD"), Cholesky/LVar3.hpp:37-38)."""
+
+    def __init__(self, column):
+        super().__init__(f"A was not numerically HPD (column {column})")
+        self.column = column
+
+
+class SingularMatrixError(ValueError):
+    """LU met an exact zero pivot (SingularMatrixException, LU/Panel.hpp:76-77)."""
+
+    def __init__(self, column):
+        super().__init__(f"Matrix was singular (column {column})")
+        self.column = column
+
+
+class DeviceTimeoutError(RuntimeError):
+    """A bounded device-side wait ran out; the kernel returned instead of hanging."""
+
+
+_lib = None
+
+
+def lib():
+    """Load libelemgpu.so (build it first if a compiler is present)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        from . import build as _b
+        _b.build()
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"libelemgpu.so not found at {LIB_PATH}; run elemental_b200/build.py")
+    L = ctypes.CDLL(LIB_PATH)
+    _declare(L)
+    _lib = L
+    return L
+
+
+def exported_symbols() -> list[str]:
+    """Names declared in include/elemgpu.h (used by the load/export test)."""
+    import re
+    hdr = open(os.path.join(_HERE, "..", "include", "elemgpu.h")).read()
+    return re.findall(r"^EGPU_API [^()]*?\b(egpu_\w+)\(", hdr, flags=re.M)
+
+
+def _declare(L):
+    I, D, P, LL = ctypes.c_int, ctypes.c_double, ctypes.c_void_p, ctypes.c_longlong
+    H = ctypes.c_void_p
+    sig = {
+        "egpu_create": ([P, I], I),
+        "egpu_destroy": ([H], I),
+        "egpu_set_stream": ([H, P], I),
+        "egpu_get_stream": ([H], P),
+        "egpu_synchronize": ([H], I),
+        "egpu_set_blocksize": ([H, I], I),
+        "egpu_get_blocksize": ([H], I),
+        "egpu_error_string": ([I], ctypes.c_char_p),
+        "egpu_last_error_detail": ([], ctypes.c_char_p),
+        "egpu_launch_count": ([H], LL),
+        "egpu_trace_enable": ([H, I], I),
+        "egpu_trace_summary": ([H, I, P, P, P, P], I),
+        "egpu_dpotrf": ([H, I, I, P, I, P], I),
+        "egpu_dpotrs": ([H, I, I, I, I, P, I, P, I], I),
+        "egpu_dposv": ([H, I, I, I, I, P, I, P, I, P], I),
+        "egpu_dgetrf": ([H, I, I, P, I, P, P], I),
+        "egpu_dgetrf_nopiv": ([H, I, I, P, I, P], I),
+        "egpu_dgetrs": ([H, I, I, I, P, I, P, P, I], I),
+        "egpu_dgesv": ([H, I, I, P, I, P, I, P], I),
+        "egpu_dtrsm": ([H, I, I, I, I, I, I, D, P, I, P, I], I),
+        "egpu_dtrsv": ([H, I, I, I, I, P, I, P], I),
+        "egpu_dgemm": ([H, I, I, I, I, I, D, P, I, P, I, D, P, I], I),
+        "egpu_dherk": ([H, I, I, I, I, D, P, I, D, P, I], I),
+        "egpu_dlaswp": ([H, I, I, I, P, I, P, I], I),
+        "egpu_host_dpotrf": ([H, I, I, P, I, P], I),
+        "egpu_host_dpotrs": ([H, I, I, I, I, P, I, P, I], I),
+        "egpu_host_dposv": ([H, I, I, I, I, P, I, P, I, P], I),
+        "egpu_host_dgetrf": ([H, I, I, P, I, P, P], I),
+        "egpu_host_dgetrf_nopiv": ([H, I, I, P, I, P], I),
+        "egpu_host_dgetrs": ([H, I, I, I, P, I, P, P, I], I),
+        "egpu_host_dgesv": ([H, I, I, P, I, P, I, P], I),
+        "egpu_host_dtrsm": ([H, I, I, I, I, I, I, D, P, I, P, I], I),
+        "egpu_host_dgemm": ([H, I, I, I, I, I, D, P, I, P, I, D, P, I], I),
+        "egpu_host_dherk": ([H, I, I, I, I, D, P, I, D, P, I], I),
+        "egpu_host_dlaswp": ([H, I, I, I, P, I, P, I], I),
+    }
+    for name, (args, res) in sig.items():
+        if hasattr(L, name):
+            f = getattr(L, name)
+            f.argtypes = args
+            f.restype = res
+
+
+def _check(rc: int, info: int = 0):
+    if rc == OK:
+        return
+    if rc == NOT_HPD:
+        raise NonHPDError(info)
+    if rc == SINGULAR:
+        raise SingularMatrixError(info)
+    if rc == TIMEOUT:
+        raise DeviceTimeoutError(f"device wait timed out (site {info})")
+    detail = lib().egpu_last_error_detail().decode()
+    raise ElemGPUError(f"{lib().egpu_error_string(rc).decode()} ({rc}) {detail}")
+
+
+# ------------------------------------------------------------ helpers --
+
+def colmajor_cuda(a, device="cuda", dtype=None):
+    """Copy a 2-D numpy/torch array into a column-major CUDA tensor (stride (1, rows))."""
+    import torch
+    t = torch.as_tensor(np.asarray(a) if not isinstance(a, torch.Tensor) else a)
+    if dtype is not None:
+        t = t.to(dtype)
+    if t.dim() == 1:
+        t = t.reshape(-1, 1)
+    m, n = t.shape
+    out = torch.empty_strided((m, n), (1, max(m, 1)), dtype=t.dtype, device=device)
+    out.copy_(t)
+    return out
+
+
+def empty_colmajor(m, n, dtype=None, device="cuda", ld=None):
+    import torch
+    dtype = dtype or torch.float64
+    ld = ld or max(m, 1)
+    store = torch.empty(ld * max(n, 1), dtype=dtype, device=device)
+    return torch.as_strided(store, (m, n), (1, ld))
+
+
+def _ld(t) -> int:
+    if t.dim() == 1:
+        return max(t.shape[0], 1)
+    if t.shape[1] <= 1:
+        return max(t.shape[0], 1) if t.stride(0) == 1 else t.stride(1)
+    if t.stride(0) != 1:
+        raise ValueError("device matrices must be column-major (stride(0) == 1)")
+    return t.stride(1)
+
+
+def _ptr(t):
+    return ctypes.c_void_p(t.data_ptr())
+
+
+def _np_f(a: np.ndarray):
+    a = np.asarray(a)
+    if a.dtype != np.float64:
+        raise TypeError("host API expects float64 arrays")
+    if a.ndim == 1:
+        a = a.reshape(-1, 1, order="F")
+    if not a.flags.f_contiguous:
+        raise ValueError("host arrays must be Fortran-ordered (column-major)")
+    return a
+
+
+def _np_ptr(a):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+class Handle:
+    """One egpu_context: stream + workspace on one device."""
+
+    def __init__(self, device: int = 0):
+        h = ctypes.c_void_p()
+        _check(lib().egpu_create(ctypes.byref(h), device))
+        self._h = h
+        self.device = device
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            lib().egpu_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    @property
+    def h(self):
+        return self._h
+
+    def _bind_stream(self):
+        # Device-API calls run on torch's current stream so that they are
+        # ordered after the torch ops that produced their inputs.
+        import torch
+        s = torch.cuda.current_stream(self.device).cuda_stream
+        if s != getattr(self, "_bound", None):
+            _check(lib().egpu_set_stream(self._h, ctypes.c_void_p(s)))
+            self._bound = s
+
+    def set_blocksize(self, nb: int):
+        _check(lib().egpu_set_blocksize(self._h, nb))
+
+    def blocksize(self) -> int:
+        return lib().egpu_get_blocksize(self._h)
+
+    def set_stream(self, stream_ptr: int | None):
+        _check(lib().egpu_set_stream(self._h, ctypes.c_void_p(stream_ptr or 0)))
+        self._bound = stream_ptr
+
+    def synchronize(self):
+        _check(lib().egpu_synchronize(self._h))
+
+    def launch_count(self) -> int:
+        return int(lib().egpu_launch_count(self._h))
+
+    TRACE_KINDS = {"update": 0, "trsm": 1, "diag": 2, "panel": 3, "swap": 4, "other": 5}
+
+    def trace_enable(self, on: bool = True):
+        """Bracket every launch with CUDA events on its stream (clears old records)."""
+        _check(lib().egpu_trace_enable(self._h, int(on)))
+
+    def trace_summary(self) -> dict:
+        """{kind: {"ms", "flops", "bytes", "launches"}} over the traced launches."""
+        out = {}
+        for name, k in self.TRACE_KINDS.items():
+            ms, fl, by, n = ctypes.c_double(), ctypes.c_double(), ctypes.c_double(), ctypes.c_longlong()
+            _check(lib().egpu_trace_summary(self._h, k, ctypes.byref(ms), ctypes.byref(fl), ctypes.byref(by),
+                                            ctypes.byref(n)))
+            out[name] = {"ms": ms.value, "flops": fl.value, "bytes": by.value, "launches": n.value}
+        return out
+
+    # ---------------- device API (torch CUDA tensors, column-major) ----
+    def cholesky(self, A, uplo=LOWER):
+        self._bind_stream()
+        info = ctypes.c_int(0)
+        rc = lib().egpu_dpotrf(self._h, uplo, A.shape[0], _ptr(A), _ld(A), ctypes.byref(info))
+        _check(rc, info.value)
+
+    def cholesky_solve_after(self, A, B, uplo=LOWER, orient=NORMAL):
+        self._bind_stream()
+        _check(lib().egpu_dpotrs(self._h, uplo, orient, A.shape[0], B.shape[1] if B.dim() > 1 else 1,
+                                 _ptr(A), _ld(A), _ptr(B), _ld(B)))
+
+    def hpd_solve(self, A, B, uplo=LOWER, orient=NORMAL):
+        self._bind_stream()
+        info = ctypes.c_int(0)
+        rc = lib().egpu_dposv(self._h, uplo, orient, A.shape[0], B.shape[1] if B.dim() > 1 else 1,
+                              _ptr(A), _ld(A), _ptr(B), _ld(B), ctypes.byref(info))
+        _check(rc, info.value)
+
+    def lu(self, A, p):
+        self._bind_stream()
+        info = ctypes.c_int(0)
+        rc = lib().egpu_dgetrf(self._h, A.shape[0], A.shape[1], _ptr(A), _ld(A), _ptr(p), ctypes.byref(info))
+        _check(rc, info.value)
+
+    def lu_nopiv(self, A):
+        self._bind_stream()
+        info = ctypes.c_int(0)
+        rc = lib().egpu_dgetrf_nopiv(self._h, A.shape[0], A.shape[1], _ptr(A), _ld(A), ctypes.byref(info))
+        _check(rc, info.value)
+
+    def lu_solve_after(self, A, p, B, orient=NORMAL):
+        self._bind_stream()
+        _check(lib().egpu_dgetrs(self._h, orient, A.shape[0], B.shape[1] if B.dim() > 1 else 1, _ptr(A), _ld(A),
+                                 None if p is None else _ptr(p), _ptr(B), _ld(B)))
+
+    def gaussian_elimination(self, A, B):
+        self._bind_stream()
+        info = ctypes.c_int(0)
+        rc = lib().egpu_dgesv(self._h, A.shape[0], B.shape[1] if B.dim() > 1 else 1, _ptr(A), _ld(A), _ptr(B),
+                              _ld(B), ctypes.byref(info))
+        _check(rc, info.value)
+
+    def trsm(self, side, uplo, orient, diag, alpha, A, B):
+        self._bind_stream()
+        m, n = B.shape[0], (B.shape[1] if B.dim() > 1 else 1)
+        _check(lib().egpu_dtrsm(self._h, side, uplo, orient, diag, m, n, float(alpha), _ptr(A), _ld(A), _ptr(B),
+                                _ld(B)))
+
+    def trsv(self, uplo, orient, diag, A, x):
+        self._bind_stream()
+        _check(lib().egpu_dtrsv(self._h, uplo, orient, diag, A.shape[0], _ptr(A), _ld(A), _ptr(x)))
+
+    def gemm(self, oA, oB, alpha, A, B, beta, C):
+        self._bind_stream()
+        m, n = C.shape
+        k = A.shape[1] if oA == NORMAL else A.shape[0]
+        _check(lib().egpu_dgemm(self._h, oA, oB, m, n, k, float(alpha), _ptr(A), _ld(A), _ptr(B), _ld(B),
+                                float(beta), _ptr(C), _ld(C)))
+
+    def herk(self, uplo, orient, alpha, A, beta, C):
+        self._bind_stream()
+        n = C.shape[0]
+        k = A.shape[1] if orient == NORMAL else A.shape[0]
+        _check(lib().egpu_dherk(self._h, uplo, orient, n, k, float(alpha), _ptr(A), _ld(A), float(beta), _ptr(C),
+                                _ld(C)))
+
+    def apply_row_pivots(self, B, p, inverse=False):
+        self._bind_stream()
+        m, n = B.shape[0], (B.shape[1] if B.dim() > 1 else 1)
+        _check(lib().egpu_dlaswp(self._h, int(inverse), m, n, _ptr(B), _ld(B), _ptr(p), p.shape[0]))
+
+    # ---------------- host API (numpy, Fortran order, in place) --------
+    def host_cholesky(self, A: np.ndarray, uplo=LOWER):
+        A = _np_f(A)
+        info = ctypes.c_int(0)
+        rc = lib().egpu_host_dpotrf(self._h, uplo, A.shape[0], _np_ptr(A), max(A.shape[0], 1), ctypes.byref(info))
+        _check(rc, info.value)
+
+    def host_hpd_solve(self, A: np.ndarray, B: np.ndarray, uplo=LOWER, orient=NORMAL):
+        A, B = _np_f(A), _np_f(B)
+        info = ctypes.c_int(0)
+        rc = lib().egpu_host_dposv(self._h, uplo, orient, A.shape[0], B.shape[1], _np_ptr(A), max(A.shape[0], 1),
+                                   _np_ptr(B), max(B.shape[0], 1), ctypes.byref(info))
+        _check(rc, info.value)
+
+    def host_cholesky_solve_after(self, A, B, uplo=LOWER, orient=NORMAL):
+        A, B = _np_f(A), _np_f(B)
+        _check(lib().egpu_host_dpotrs(self._h, uplo, orient, A.shape[0], B.shape[1], _np_ptr(A),
+                                      max(A.shape[0], 1), _np_ptr(B), max(B.shape[0], 1)))
+
+    def host_lu(self, A: np.ndarray) -> np.ndarray:
+        A = _np_f(A)
+        m, n = A.shape
+        p = np.zeros(min(m, n), dtype=np.int32)
+        info = ctypes.c_int(0)
+        rc = lib().egpu_host_dgetrf(self._h, m, n, _np_ptr(A), max(m, 1), _np_ptr(p), ctypes.byref(info))
+        _check(rc, info.value)
+        return p
+
+    def host_lu_nopiv(self, A: np.ndarray):
+        A = _np_f(A)
+        info = ctypes.c_int(0)
+        rc = lib().egpu_host_dgetrf_nopiv(self._h, A.shape[0], A.shape[1], _np_ptr(A), max(A.shape[0], 1),
+                                          ctypes.byref(info))
+        _check(rc, info.value)
+
+    def host_lu_solve_after(self, A, p, B, orient=NORMAL):
+        A, B = _np_f(A), _np_f(B)
+        pp = None if p is None else np.ascontiguousarray(p, dtype=np.int32)
+        _check(lib().egpu_host_dgetrs(self._h, orient, A.shape[0], B.shape[1], _np_ptr(A), max(A.shape[0], 1),
+                                      None if pp is None else _np_ptr(pp), _np_ptr(B), max(B.shape[0], 1)))
+
+    def host_gaussian_elimination(self, A, B):
+        A, B = _np_f(A), _np_f(B)
+        info = ctypes.c_int(0)
+        rc = lib().egpu_host_dgesv(self._h, A.shape[0], B.shape[1], _np_ptr(A), max(A.shape[0], 1), _np_ptr(B),
+                                   max(B.shape[0], 1), ctypes.byref(info))
+        _check(rc, info.value)
+
+    def host_trsm(self, side, uplo, orient, diag, alpha, A, B):
+        A, B = _np_f(A), _np_f(B)
+        _check(lib().egpu_host_dtrsm(self._h, side, uplo, orient, diag, B.shape[0], B.shape[1], float(alpha),
+                                     _np_ptr(A), max(A.shape[0], 1), _np_ptr(B), max(B.shape[0], 1)))
+
+    def host_gemm(self, oA, oB, alpha, A, B, beta, C):
+        A, B, C = _np_f(A), _np_f(B), _np_f(C)
+        m, n = C.shape
+        k = A.shape[1] if oA == NORMAL else A.shape[0]
+        _check(lib().egpu_host_dgemm(self._h, oA, oB, m, n, k, float(alpha), _np_ptr(A), max(A.shape[0], 1),
+                                     _np_ptr(B), max(B.shape[0], 1), float(beta), _np_ptr(C), max(m, 1)))
+
+    def host_herk(self, uplo, orient, alpha, A, beta, C):
+        A, C = _np_f(A), _np_f(C)
+        n = C.shape[0]
+        k = A.shape[1] if orient == NORMAL else A.shape[0]
+        _check(lib().egpu_host_dherk(self._h, uplo, orient, n, k, float(alpha), _np_ptr(A), max(A.shape[0], 1),
+                                     float(beta), _np_ptr(C), max(n, 1)))
+
+    def host_apply_row_pivots(self, B, p, inverse=False):
+        B = _np_f(B)
+        pp = np.ascontiguousarray(p, dtype=np.int32)
+        _check(lib().egpu_host_dlaswp(self._h, int(inverse), B.shape[0], B.shape[1], _np_ptr(B),
+                                      max(B.shape[0], 1), _np_ptr(pp), len(pp)))

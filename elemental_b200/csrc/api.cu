@@ -1,0 +1,1004 @@
+// C-ABI entry points: handle, workspace, and the blocked right-looking
+// drivers that sequence the sm_100a kernels for Cholesky, LU and the solves.
+#include <atomic>
+#include <cstring>
+#include <vector>
+#include <new>
+#include <string>
+
+#include "internal.h"
+
+namespace egpu {
+
+static thread_local std::string t_last_error;
+static std::atomic<long long> g_launches{0};
+
+void set_last_error(cudaError_t e, const char* what, const char* file, int line) {
+  t_last_error = std::string(what) + ": " + cudaGetErrorString(e) + " (" + file + ":" + std::to_string(line) + ")";
+}
+
+void count_launch(int n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+
+struct Trace {
+  struct Rec {
+    int kind;
+    double flops, bytes;
+    cudaEvent_t e0, e1;
+  };
+  bool on = false;
+  std::vector<Rec> recs;
+  std::vector<cudaEvent_t> pool;
+  cudaEvent_t get() {
+    if (pool.empty()) {
+      cudaEvent_t e;
+      if (cudaEventCreate(&e) != cudaSuccess) return nullptr;
+      return e;
+    }
+    cudaEvent_t e = pool.back();
+    pool.pop_back();
+    return e;
+  }
+  void clear() {
+    for (auto& r : recs) {
+      if (r.e0) pool.push_back(r.e0);
+      if (r.e1) pool.push_back(r.e1);
+    }
+    recs.clear();
+  }
+  ~Trace() {
+    clear();
+    for (auto e : pool) cudaEventDestroy(e);
+  }
+};
+
+static thread_local Trace* t_trace = nullptr;
+
+TraceMark::TraceMark(cudaStream_t s, int kind, double flops, double bytes) {
+  if (t_trace == nullptr || !t_trace->on) return;
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(s, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) return;
+  Trace::Rec r{kind, flops, bytes, t_trace->get(), t_trace->get()};
+  if (!r.e0 || !r.e1) return;
+  t = t_trace;
+  st = s;
+  idx = (int)t->recs.size();
+  cudaEventRecord(r.e0, s);
+  t->recs.push_back(r);
+}
+
+TraceMark::~TraceMark() {
+  if (t) cudaEventRecord(t->recs[idx].e1, st);
+}
+
+}  // namespace egpu
+
+using namespace egpu;
+
+struct egpu_context {
+  int device = 0;
+  int sm_count = 148;
+  cudaStream_t own_stream = nullptr;
+  cudaStream_t stream = nullptr;
+  int nb = 128;
+  void* ws = nullptr;
+  size_t ws_bytes = 0;
+  DevStatus* dstatus = nullptr;
+  DevStatus* hstatus = nullptr;  // pinned
+  // host-API staging buffers
+  void* stage[3] = {nullptr, nullptr, nullptr};
+  size_t stage_bytes[3] = {0, 0, 0};
+  Trace trace;
+};
+
+namespace {
+
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev) {
+    cudaGetDevice(&prev);
+    if (prev != dev) cudaSetDevice(dev);
+  }
+  ~DeviceGuard() {
+    int cur;
+    cudaGetDevice(&cur);
+    if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+  }
+};
+
+int ensure_ws(egpu_context* h, size_t bytes) {
+  if (bytes <= h->ws_bytes) return EGPU_OK;
+  if (h->ws) {
+    cudaStreamSynchronize(h->stream);
+    cudaFree(h->ws);
+    h->ws = nullptr;
+    h->ws_bytes = 0;
+  }
+  bytes = (bytes + (1 << 20) - 1) & ~size_t((1 << 20) - 1);
+  cudaError_t e = cudaMalloc(&h->ws, bytes);
+  if (e != cudaSuccess) {
+    set_last_error(e, "workspace cudaMalloc", __FILE__, __LINE__);
+    cudaGetLastError();
+    return EGPU_ERR_ALLOC;
+  }
+  h->ws_bytes = bytes;
+  return EGPU_OK;
+}
+
+int ensure_stage(egpu_context* h, int slot, size_t bytes) {
+  if (bytes <= h->stage_bytes[slot]) return EGPU_OK;
+  if (h->stage[slot]) {
+    cudaStreamSynchronize(h->stream);
+    cudaFree(h->stage[slot]);
+    h->stage[slot] = nullptr;
+    h->stage_bytes[slot] = 0;
+  }
+  bytes = (bytes + (1 << 20) - 1) & ~size_t((1 << 20) - 1);
+  cudaError_t e = cudaMalloc(&h->stage[slot], bytes);
+  if (e != cudaSuccess) {
+    set_last_error(e, "staging cudaMalloc", __FILE__, __LINE__);
+    cudaGetLastError();
+    return EGPU_ERR_ALLOC;
+  }
+  h->stage_bytes[slot] = bytes;
+  return EGPU_OK;
+}
+
+// Entered by every C-ABI call: selects the handle's device and makes its
+// trace the calling thread's active trace.
+struct Enter {
+  DeviceGuard g;
+  Trace* prev;
+  explicit Enter(egpu_context* h) : g(h->device), prev(t_trace) { t_trace = &h->trace; }
+  ~Enter() { t_trace = prev; }
+};
+
+inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+inline long long ld_aligned(int rows) { return std::max<long long>(32, align_up((size_t)std::max(rows, 1), 32)); }
+
+// Simple bump allocator over the handle workspace.
+struct Carve {
+  unsigned char* base;
+  size_t off = 0;
+  explicit Carve(void* b) : base(static_cast<unsigned char*>(b)) {}
+  template <class T>
+  T* take(size_t count) {
+    off = align_up(off, 256);
+    T* p = reinterpret_cast<T*>(base + off);
+    off += sizeof(T) * count;
+    return p;
+  }
+};
+
+int reset_status(egpu_context* h) {
+  EGPU_CUDA_TRY(cudaMemsetAsync(h->dstatus, 0, sizeof(DevStatus), h->stream));
+  return EGPU_OK;
+}
+
+int read_status(egpu_context* h, int* info) {
+  EGPU_CUDA_TRY(cudaMemcpyAsync(h->hstatus, h->dstatus, sizeof(DevStatus), cudaMemcpyDeviceToHost, h->stream));
+  EGPU_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  if (info) *info = h->hstatus->code ? h->hstatus->info : 0;
+  switch (h->hstatus->code) {
+    case kOk: return EGPU_OK;
+    case kNotHPD: return EGPU_NOT_HPD;
+    case kSingular: return EGPU_SINGULAR;
+    default: return EGPU_TIMEOUT;
+  }
+}
+
+#define TRY(x)               \
+  do {                       \
+    int _r = (x);            \
+    if (_r != EGPU_OK) return _r; \
+  } while (0)
+
+// A device matrix argument that may need repacking into an aligned copy for TMA.
+struct Operand {
+  double* ptr;
+  long long ld;
+  double* user;
+  long long user_ld;
+  int rows, cols;
+  bool packed = false;
+};
+
+// Blocked triangular solve with the diagonal blocks pre-inverted (Winv, one
+// nb x nb block per diagonal block, ld nb).  Covers Trsm's eight
+// side/uplo/orientation cases (blas-like/level3/Trsm.hpp:49-86); the
+// unit/non-unit choice is carried by Winv.  B is m x n; alpha already applied.
+int trsm_blocked(cudaStream_t st, int side, int uplo, int trans, int m, int n, const double* A, long long lda,
+                 const double* Winv, int nb, double* B, long long ldb, DevStatus* status) {
+  const int nt = (side == EGPU_LEFT) ? m : n;  // order of the triangle
+  const int nblk = (nt + nb - 1) / nb;
+  const bool fwd = (side == EGPU_LEFT) ? ((uplo == EGPU_LOWER) == !trans) : ((uplo == EGPU_UPPER) == !trans);
+  for (int s = 0; s < nblk; ++s) {
+    const int i = fwd ? s : nblk - 1 - s;
+    const int i0 = i * nb;
+    const int bi = std::min(nb, nt - i0);
+    const double* Wi = Winv + (size_t)i * nb * nb;
+    if (side == EGPU_LEFT) {
+      double* Bi = B + i0;
+      // B_i := op(inv(A_ii)) * B_i   (in place; one CTA holds all bi rows)
+      TRY(launch_dgemm(st, trans != 0, true, bi, n, bi, 1.0, Wi, nb, Bi, ldb, 0.0, Bi, ldb, 0, false, status));
+      if (fwd) {
+        const int r0 = i0 + bi, mr = nt - r0;
+        if (mr > 0) {
+          // B_below -= op(A)_{below,i} * B_i
+          if (!trans)  // A_{below,i} stored rows r0.., cols i0.. : MN-major
+            TRY(launch_dgemm(st, false, true, mr, n, bi, -1.0, A + r0 + (size_t)i0 * lda, lda, Bi, ldb, 1.0,
+                             B + r0, ldb, 0, false, status));
+          else  // (A_{i,below})^T, A_{i,below} = rows i0.., cols r0.. : K-major
+            TRY(launch_dgemm(st, true, true, mr, n, bi, -1.0, A + i0 + (size_t)r0 * lda, lda, Bi, ldb, 1.0,
+                             B + r0, ldb, 0, false, status));
+        }
+      } else {
+        const int mr = i0;
+        if (mr > 0) {
+          if (!trans)  // A_{above,i}: rows 0..i0, cols i0.. : MN-major
+            TRY(launch_dgemm(st, false, true, mr, n, bi, -1.0, A + (size_t)i0 * lda, lda, Bi, ldb, 1.0, B, ldb, 0,
+                             false, status));
+          else  // (A_{i,above})^T, A_{i,above}: rows i0.., cols 0..i0 : K-major
+            TRY(launch_dgemm(st, true, true, mr, n, bi, -1.0, A + i0, lda, Bi, ldb, 1.0, B, ldb, 0, false,
+                             status));
+        }
+      }
+    } else {
+      double* Bi = B + (size_t)i0 * ldb;
+      // B_i := B_i * op(inv(A_ii))   (in place; one CTA holds all bi columns)
+      TRY(launch_dgemm(st, false, trans == 0, m, bi, bi, 1.0, Bi, ldb, Wi, nb, 0.0, Bi, ldb, 0, true, status));
+      if (fwd) {
+        const int c0 = i0 + bi, nc = nt - c0;
+        if (nc > 0) {
+          if (!trans)  // op(A) = A_{i,right}: rows i0.., cols c0.. (K x N) : K-major
+            TRY(launch_dgemm(st, false, true, m, nc, bi, -1.0, Bi, ldb, A + i0 + (size_t)c0 * lda, lda, 1.0,
+                             B + (size_t)c0 * ldb, ldb, 0, false, status));
+          else  // op(A) = (A_{right,i})^T: A rows c0.., cols i0.. (N x K) : MN-major
+            TRY(launch_dgemm(st, false, false, m, nc, bi, -1.0, Bi, ldb, A + c0 + (size_t)i0 * lda, lda, 1.0,
+                             B + (size_t)c0 * ldb, ldb, 0, false, status));
+        }
+      } else {
+        const int nc = i0;
+        if (nc > 0) {
+          if (!trans)  // A_{i,left}: rows i0.., cols 0.. : K-major
+            TRY(launch_dgemm(st, false, true, m, nc, bi, -1.0, Bi, ldb, A + i0, lda, 1.0, B, ldb, 0, false,
+                             status));
+          else  // (A_{left,i})^T: A rows 0.., cols i0.. : MN-major
+            TRY(launch_dgemm(st, false, false, m, nc, bi, -1.0, Bi, ldb, A + (size_t)i0 * lda, lda, 1.0, B, ldb,
+                             0, false, status));
+        }
+      }
+    }
+  }
+  return EGPU_OK;
+}
+
+int check_handle(egpu_context* h) { return h ? EGPU_OK : EGPU_ERR_ARG; }
+
+// Workspace carve for diag-block inverses of an order-nt triangle.
+size_t winv_bytes(int nt, int nb) { return sizeof(double) * (size_t)((nt + nb - 1) / nb) * nb * nb; }
+
+// ----- core device drivers on TMA-compatible operands -----
+
+int potrf_core(egpu_context* h, int uplo, int n, double* A, long long lda) {
+  const int nb = h->nb;
+  cudaStream_t st = h->stream;
+  TRY(ensure_ws(h, sizeof(double) * (size_t)nb * nb + 4096));
+  Carve cv(h->ws);
+  double* W = cv.take<double>((size_t)nb * nb);
+  for (int k = 0; k < n; k += nb) {
+    const int b = std::min(nb, n - k);
+    const int m2 = n - k - b;
+    double* A11 = A + k + (size_t)k * lda;
+    TRY(launch_potrf_diag(st, uplo, A11, lda, b, W, nb, h->dstatus, k));
+    if (m2 == 0) continue;
+    if (uplo == EGPU_LOWER) {
+      double* A21 = A + (k + b) + (size_t)k * lda;
+      double* A22 = A + (k + b) + (size_t)(k + b) * lda;
+      // Trsm(RIGHT, LOWER, ADJOINT, NON_UNIT, 1, A11, A21): A21 := A21 * inv(L11)^T
+      TRY(launch_dgemm(st, false, false, m2, b, b, 1.0, A21, lda, W, nb, 0.0, A21, lda, 0, true, h->dstatus));
+      // Herk(LOWER, NORMAL, -1, A21, 1, A22)
+      TRY(launch_dgemm(st, false, false, m2, m2, b, -1.0, A21, lda, A21, lda, 1.0, A22, lda, 1, false, h->dstatus));
+    } else {
+      double* A12 = A + k + (size_t)(k + b) * lda;
+      double* A22 = A + (k + b) + (size_t)(k + b) * lda;
+      // Trsm(LEFT, UPPER, ADJOINT, NON_UNIT, 1, A11, A12): A12 := inv(U11)^T * A12
+      TRY(launch_dgemm(st, true, true, b, m2, b, 1.0, W, nb, A12, lda, 0.0, A12, lda, 0, false, h->dstatus));
+      // Herk(UPPER, ADJOINT, -1, A12, 1, A22)
+      TRY(launch_dgemm(st, true, true, m2, m2, b, -1.0, A12, lda, A12, lda, 1.0, A22, lda, 2, false, h->dstatus));
+    }
+  }
+  return EGPU_OK;
+}
+
+int getrf_core(egpu_context* h, int m, int n, double* A, long long lda, int* dp) {
+  const int nb = h->nb;
+  const int mn = std::min(m, n);
+  cudaStream_t st = h->stream;
+  const size_t panel_bytes = lu_panel_scratch_bytes(m, nb, h->sm_count);
+  TRY(ensure_ws(h, sizeof(double) * (size_t)nb * nb + 2 * sizeof(int) * nb + panel_bytes + 4096));
+  Carve cv(h->ws);
+  double* W = cv.take<double>((size_t)nb * nb);
+  int* image = cv.take<int>(nb);
+  int* preimage = cv.take<int>(nb);
+  void* pscr = cv.take<unsigned char>(panel_bytes);
+  for (int k = 0; k < mn; k += nb) {
+    const int b = std::min(nb, mn - k);
+    const int mr = m - k, nr = n - k - b;
+    double* ABRL = A + k + (size_t)k * lda;
+    TRY(launch_lu_panel(st, mr, b, ABRL, lda, dp + k, k, image, preimage, W, nb, pscr, h->dstatus, h->sm_count));
+    // ApplyRowPivots(ABL, image, preimage); ApplyRowPivots(ABRR, image, preimage)   (LU.hpp:198-199)
+    TRY(launch_apply_composed(st, mr, k, A + k, lda, b, image, preimage, h->dstatus));
+    TRY(launch_apply_composed(st, mr, nr, A + k + (size_t)(k + b) * lda, lda, b, image, preimage, h->dstatus));
+    if (nr > 0) {
+      double* A12 = A + k + (size_t)(k + b) * lda;
+      // Trsm(LEFT, LOWER, NORMAL, UNIT, 1, A11, A12): A12 := inv(L11) * A12
+      TRY(launch_dgemm(st, false, true, b, nr, b, 1.0, W, nb, A12, lda, 0.0, A12, lda, 0, false, h->dstatus));
+      if (mr - b > 0) {
+        double* A21 = A + (k + b) + (size_t)k * lda;
+        double* A22 = A + (k + b) + (size_t)(k + b) * lda;
+        // Gemm(NORMAL, NORMAL, -1, A21, A12, 1, A22)
+        TRY(launch_dgemm(st, false, true, mr - b, nr, b, -1.0, A21, lda, A12, lda, 1.0, A22, lda, 0, false,
+                         h->dstatus));
+      }
+    }
+  }
+  return EGPU_OK;
+}
+
+int getrf_nopiv_core(egpu_context* h, int m, int n, double* A, long long lda) {
+  const int nb = h->nb;
+  const int mn = std::min(m, n);
+  cudaStream_t st = h->stream;
+  TRY(ensure_ws(h, 2 * sizeof(double) * (size_t)nb * nb + 4096));
+  Carve cv(h->ws);
+  double* W = cv.take<double>((size_t)nb * nb);
+  double* W2 = cv.take<double>((size_t)nb * nb);
+  for (int k = 0; k < mn; k += nb) {
+    const int b = std::min(nb, mn - k);
+    const int m2 = m - k - b, n2 = n - k - b;
+    double* A11 = A + k + (size_t)k * lda;
+    TRY(launch_getrf_diag_nopiv(st, A11, lda, b, W, nb, W2, h->dstatus, k));
+    double* A21 = A + (k + b) + (size_t)k * lda;
+    double* A12 = A + k + (size_t)(k + b) * lda;
+    double* A22 = A + (k + b) + (size_t)(k + b) * lda;
+    // Trsm(RIGHT, UPPER, NORMAL, NON_UNIT, 1, A11, A21): A21 := A21 * inv(U11)
+    if (m2 > 0) TRY(launch_dgemm(st, false, true, m2, b, b, 1.0, A21, lda, W2, nb, 0.0, A21, lda, 0, true, h->dstatus));
+    // Trsm(LEFT, LOWER, NORMAL, UNIT, 1, A11, A12): A12 := inv(L11) * A12
+    if (n2 > 0) TRY(launch_dgemm(st, false, true, b, n2, b, 1.0, W, nb, A12, lda, 0.0, A12, lda, 0, false, h->dstatus));
+    // Gemm(NORMAL, NORMAL, -1, A21, A12, 1, A22)
+    if (m2 > 0 && n2 > 0)
+      TRY(launch_dgemm(st, false, true, m2, n2, b, -1.0, A21, lda, A12, lda, 1.0, A22, lda, 0, false, h->dstatus));
+  }
+  return EGPU_OK;
+}
+
+// Triangular solve of order nt with diag-block inverses computed here.
+int trsm_core(egpu_context* h, int side, int uplo, int trans, int unit, int m, int n, double alpha,
+              const double* A, long long lda, double* B, long long ldb, size_t ws_offset = 0) {
+  const int nb = h->nb;
+  const int nt = side == EGPU_LEFT ? m : n;
+  if (m == 0 || n == 0) return EGPU_OK;
+  cudaStream_t st = h->stream;
+  TRY(ensure_ws(h, ws_offset + winv_bytes(nt, nb) + 4096));
+  Carve cv(h->ws);
+  cv.off = ws_offset;
+  double* Winv = cv.take<double>((size_t)((nt + nb - 1) / nb) * nb * nb);
+  if (alpha != 1.0) TRY(launch_scale(st, m, n, alpha, B, ldb, 0));
+  TRY(launch_trtri_blocks(st, uplo, unit, A, lda, nt, nb, Winv, nb));
+  return trsm_blocked(st, side, uplo, trans, m, n, A, lda, Winv, nb, B, ldb, h->dstatus);
+}
+
+int getrs_core(egpu_context* h, int orient, int n, int nrhs, const double* A, long long lda, const int* dp,
+               double* B, long long ldb) {
+  // laswp scratch: perm (n ints) + n*nrhs doubles; placed after the Winv area
+  const size_t winv = winv_bytes(n, h->nb);
+  const size_t lsw = align_up(sizeof(int) * (size_t)((n + 1) & ~1), 256) + sizeof(double) * (size_t)n * nrhs;
+  TRY(ensure_ws(h, align_up(winv + 4096, 256) + lsw + 4096));
+  int* perm = reinterpret_cast<int*>(static_cast<unsigned char*>(h->ws) + align_up(winv + 4096, 256));
+  const size_t trsm_off = 0;
+  if (orient == EGPU_NORMAL) {
+    if (dp) TRY(launch_laswp_seq(h->stream, 0, n, nrhs, B, ldb, dp, n, perm));
+    TRY(trsm_core(h, EGPU_LEFT, EGPU_LOWER, 0, 1, n, nrhs, 1.0, A, lda, B, ldb, trsm_off));
+    TRY(trsm_core(h, EGPU_LEFT, EGPU_UPPER, 0, 0, n, nrhs, 1.0, A, lda, B, ldb, trsm_off));
+  } else {
+    TRY(trsm_core(h, EGPU_LEFT, EGPU_UPPER, 1, 0, n, nrhs, 1.0, A, lda, B, ldb, trsm_off));
+    TRY(trsm_core(h, EGPU_LEFT, EGPU_LOWER, 1, 1, n, nrhs, 1.0, A, lda, B, ldb, trsm_off));
+    if (dp) TRY(launch_laswp_seq(h->stream, 1, n, nrhs, B, ldb, dp, n, perm));
+  }
+  return EGPU_OK;
+}
+
+int potrs_core(egpu_context* h, int uplo, int n, int nrhs, const double* A, long long lda, double* B,
+               long long ldb) {
+  // cholesky::SolveAfter (Cholesky/SolveAfter.hpp:20-75); TRANSPOSE only
+  // conjugates B, a no-op for real data.
+  if (uplo == EGPU_LOWER) {
+    TRY(trsm_core(h, EGPU_LEFT, EGPU_LOWER, 0, 0, n, nrhs, 1.0, A, lda, B, ldb));
+    TRY(trsm_core(h, EGPU_LEFT, EGPU_LOWER, 1, 0, n, nrhs, 1.0, A, lda, B, ldb));
+  } else {
+    TRY(trsm_core(h, EGPU_LEFT, EGPU_UPPER, 1, 0, n, nrhs, 1.0, A, lda, B, ldb));
+    TRY(trsm_core(h, EGPU_LEFT, EGPU_UPPER, 0, 0, n, nrhs, 1.0, A, lda, B, ldb));
+  }
+  return EGPU_OK;
+}
+
+// RowEchelon + upper solve (GaussianElimination.hpp:94-209, 216-232): LU
+// with partial pivoting whose pivots are also applied to B and whose L is
+// applied to B on the fly; then B := inv(U) B.
+int gesv_core(egpu_context* h, int n, int nrhs, double* A, long long lda, double* B, long long ldb) {
+  const int nb = h->nb;
+  cudaStream_t st = h->stream;
+  const size_t panel_bytes = lu_panel_scratch_bytes(n, nb, h->sm_count);
+  const size_t need = sizeof(double) * (size_t)nb * nb + 2 * sizeof(int) * nb + sizeof(int) * nb + panel_bytes;
+  TRY(ensure_ws(h, std::max(need, winv_bytes(n, nb)) + 8192));
+  {
+    Carve cv(h->ws);
+    double* W = cv.take<double>((size_t)nb * nb);
+    int* image = cv.take<int>(nb);
+    int* preimage = cv.take<int>(nb);
+    int* p1 = cv.take<int>(nb);
+    void* pscr = cv.take<unsigned char>(panel_bytes);
+    for (int k = 0; k < n; k += nb) {
+      const int b = std::min(nb, n - k);
+      const int mr = n - k, nr = n - k - b;
+      double* A11 = A + k + (size_t)k * lda;
+      TRY(launch_lu_panel(st, mr, b, A11, lda, p1, k, image, preimage, W, nb, pscr, h->dstatus, h->sm_count));
+      double* A12 = A + k + (size_t)(k + b) * lda;
+      TRY(launch_apply_composed(st, mr, nr, A12, lda, b, image, preimage, h->dstatus));
+      TRY(launch_apply_composed(st, mr, nrhs, B + k, ldb, b, image, preimage, h->dstatus));
+      double* B1 = B + k;
+      if (nr > 0) TRY(launch_dgemm(st, false, true, b, nr, b, 1.0, W, nb, A12, lda, 0.0, A12, lda, 0, false, h->dstatus));
+      TRY(launch_dgemm(st, false, true, b, nrhs, b, 1.0, W, nb, B1, ldb, 0.0, B1, ldb, 0, false, h->dstatus));
+      if (nr > 0) {
+        double* A21 = A + (k + b) + (size_t)k * lda;
+        double* A22 = A + (k + b) + (size_t)(k + b) * lda;
+        TRY(launch_dgemm(st, false, true, nr, nr, b, -1.0, A21, lda, A12, lda, 1.0, A22, lda, 0, false, h->dstatus));
+        TRY(launch_dgemm(st, false, true, nr, nrhs, b, -1.0, A21, lda, B1, ldb, 1.0, B + k + b, ldb, 0, false,
+                         h->dstatus));
+      }
+    }
+  }
+  int info = 0;
+  int rc = read_status(h, &info);
+  if (rc != EGPU_OK) return rc;
+  return trsm_core(h, EGPU_LEFT, EGPU_UPPER, 0, 0, n, nrhs, 1.0, A, lda, B, ldb);
+}
+
+// ----- operand repacking for TMA alignment -----
+
+int pack(egpu_context* h, int slot, Operand& op, bool copy_in) {
+  op.packed = false;
+  if (tma_compatible(op.ptr, op.ld)) return EGPU_OK;
+  const long long ld = ld_aligned(op.rows);
+  TRY(ensure_stage(h, slot, sizeof(double) * (size_t)ld * std::max(op.cols, 1)));
+  op.user = op.ptr;
+  op.user_ld = op.ld;
+  op.ptr = static_cast<double*>(h->stage[slot]);
+  op.ld = ld;
+  op.packed = true;
+  if (copy_in) TRY(launch_copy(h->stream, op.rows, op.cols, op.user, op.user_ld, op.ptr, op.ld));
+  return EGPU_OK;
+}
+
+int unpack(egpu_context* h, const Operand& op) {
+  if (!op.packed) return EGPU_OK;
+  return launch_copy(h->stream, op.rows, op.cols, op.ptr, op.ld, op.user, op.user_ld);
+}
+
+Operand make_op(double* p, long long ld, int rows, int cols) {
+  Operand o;
+  o.ptr = p; o.ld = ld; o.user = p; o.user_ld = ld; o.rows = rows; o.cols = cols;
+  return o;
+}
+
+bool bad_ld(long long ld, int rows) { return ld < std::max(1, rows); }
+
+}  // namespace
+
+// ======================================================================
+extern "C" {
+
+int egpu_create(egpu_handle* out, int device) {
+  if (!out) return EGPU_ERR_ARG;
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return EGPU_ERR_NO_DEVICE;
+  }
+  if (device < 0 || device >= ndev) return EGPU_ERR_ARG;
+  egpu_context* h = new (std::nothrow) egpu_context();
+  if (!h) return EGPU_ERR_ALLOC;
+  h->device = device;
+  DeviceGuard g(device);
+  cudaDeviceGetAttribute(&h->sm_count, cudaDevAttrMultiProcessorCount, device);
+  if (cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaMalloc(&h->dstatus, sizeof(DevStatus)) != cudaSuccess ||
+      cudaMallocHost(&h->hstatus, sizeof(DevStatus)) != cudaSuccess) {
+    set_last_error(cudaGetLastError(), "egpu_create", __FILE__, __LINE__);
+    egpu_destroy(h);
+    return EGPU_ERR_CUDA;
+  }
+  h->stream = h->own_stream;
+  cudaMemset(h->dstatus, 0, sizeof(DevStatus));
+  *out = h;
+  return EGPU_OK;
+}
+
+int egpu_destroy(egpu_handle h) {
+  if (!h) return EGPU_OK;
+  Enter g(h);
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  if (h->ws) cudaFree(h->ws);
+  for (int i = 0; i < 3; ++i)
+    if (h->stage[i]) cudaFree(h->stage[i]);
+  if (h->dstatus) cudaFree(h->dstatus);
+  if (h->hstatus) cudaFreeHost(h->hstatus);
+  if (h->own_stream) cudaStreamDestroy(h->own_stream);
+  delete h;
+  return EGPU_OK;
+}
+
+int egpu_set_stream(egpu_handle h, void* s) {
+  TRY(check_handle(h));
+  h->stream = s ? static_cast<cudaStream_t>(s) : h->own_stream;
+  return EGPU_OK;
+}
+
+void* egpu_get_stream(egpu_handle h) { return h ? static_cast<void*>(h->stream) : nullptr; }
+
+int egpu_synchronize(egpu_handle h) {
+  TRY(check_handle(h));
+  Enter g(h);
+  EGPU_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  return EGPU_OK;
+}
+
+int egpu_set_blocksize(egpu_handle h, int nb) {
+  TRY(check_handle(h));
+  if (nb < 1) return EGPU_ERR_ARG;
+  nb = std::min(128, std::max(2, nb));
+  h->nb = nb & ~1;
+  return EGPU_OK;
+}
+
+int egpu_get_blocksize(egpu_handle h) { return h ? h->nb : -1; }
+
+long long egpu_launch_count(egpu_handle) { return g_launches.load(); }
+
+int egpu_trace_enable(egpu_handle h, int on) {
+  TRY(check_handle(h));
+  Enter g(h);
+  cudaStreamSynchronize(h->stream);
+  h->trace.clear();
+  h->trace.on = on != 0;
+  return EGPU_OK;
+}
+
+int egpu_trace_summary(egpu_handle h, int kind, double* total_ms, double* total_flops, double* total_bytes,
+                       long long* launches) {
+  TRY(check_handle(h));
+  Enter g(h);
+  double ms = 0, fl = 0, by = 0;
+  long long n = 0;
+  for (auto& r : h->trace.recs) {
+    if (r.kind != kind) continue;
+    EGPU_CUDA_TRY(cudaEventSynchronize(r.e1));
+    float t = 0;
+    EGPU_CUDA_TRY(cudaEventElapsedTime(&t, r.e0, r.e1));
+    ms += t; fl += r.flops; by += r.bytes; ++n;
+  }
+  if (total_ms) *total_ms = ms;
+  if (total_flops) *total_flops = fl;
+  if (total_bytes) *total_bytes = by;
+  if (launches) *launches = n;
+  return EGPU_OK;
+}
+
+const char* egpu_error_string(int code) {
+  switch (code) {
+    case EGPU_OK: return "ok";
+    case EGPU_NOT_HPD: return "A was not numerically HPD";
+    case EGPU_SINGULAR: return "Matrix was singular";
+    case EGPU_TIMEOUT: return "device-side wait timed out";
+    case EGPU_ERR_ARG: return "invalid argument";
+    case EGPU_ERR_CUDA: return "CUDA error";
+    case EGPU_ERR_ALLOC: return "device allocation failed";
+    case EGPU_ERR_ALIGN: return "operand not 16-byte aligned";
+    case EGPU_ERR_TMA: return "tensor-map encoding failed";
+    case EGPU_ERR_UNSUPPORTED: return "unsupported size";
+    case EGPU_ERR_NO_DEVICE: return "no CUDA device";
+    default: return "unknown";
+  }
+}
+
+const char* egpu_last_error_detail(void) { return t_last_error.c_str(); }
+
+// ---------------------------------------------------------- device API --
+
+int egpu_dpotrf(egpu_handle h, int uplo, int n, double* dA, int lda, int* info) {
+  TRY(check_handle(h));
+  if (info) *info = 0;
+  if (n < 0 || (uplo != EGPU_LOWER && uplo != EGPU_UPPER) || bad_ld(lda, n)) return EGPU_ERR_ARG;
+  if (n == 0) return EGPU_OK;
+  Enter g(h);
+  Operand A = make_op(dA, lda, n, n);
+  TRY(pack(h, 0, A, true));
+  TRY(reset_status(h));
+  TRY(potrf_core(h, uplo, n, A.ptr, A.ld));
+  TRY(unpack(h, A));
+  return read_status(h, info);
+}
+
+int egpu_dpotrs(egpu_handle h, int uplo, int orient, int n, int nrhs, const double* dA, int lda, double* dB,
+                int ldb) {
+  TRY(check_handle(h));
+  if (n < 0 || nrhs < 0 || bad_ld(lda, n) || bad_ld(ldb, n)) return EGPU_ERR_ARG;
+  if (n == 0 || nrhs == 0) return EGPU_OK;
+  (void)orient;
+  Enter g(h);
+  Operand A = make_op(const_cast<double*>(dA), lda, n, n), B = make_op(dB, ldb, n, nrhs);
+  TRY(pack(h, 0, A, true));
+  TRY(pack(h, 1, B, true));
+  TRY(reset_status(h));
+  TRY(potrs_core(h, uplo, n, nrhs, A.ptr, A.ld, B.ptr, B.ld));
+  TRY(unpack(h, B));
+  return read_status(h, nullptr);
+}
+
+int egpu_dposv(egpu_handle h, int uplo, int orient, int n, int nrhs, double* dA, int lda, double* dB, int ldb,
+               int* info) {
+  int rc = egpu_dpotrf(h, uplo, n, dA, lda, info);
+  if (rc != EGPU_OK) return rc;
+  return egpu_dpotrs(h, uplo, orient, n, nrhs, dA, lda, dB, ldb);
+}
+
+int egpu_dgetrf(egpu_handle h, int m, int n, double* dA, int lda, int* dp, int* info) {
+  TRY(check_handle(h));
+  if (info) *info = 0;
+  if (m < 0 || n < 0 || bad_ld(lda, m) || (!dp && std::min(m, n) > 0)) return EGPU_ERR_ARG;
+  if (m == 0 || n == 0) return EGPU_OK;
+  Enter g(h);
+  Operand A = make_op(dA, lda, m, n);
+  TRY(pack(h, 0, A, true));
+  TRY(reset_status(h));
+  TRY(getrf_core(h, m, n, A.ptr, A.ld, dp));
+  TRY(unpack(h, A));
+  return read_status(h, info);
+}
+
+int egpu_dgetrf_nopiv(egpu_handle h, int m, int n, double* dA, int lda, int* info) {
+  TRY(check_handle(h));
+  if (info) *info = 0;
+  if (m < 0 || n < 0 || bad_ld(lda, m)) return EGPU_ERR_ARG;
+  if (m == 0 || n == 0) return EGPU_OK;
+  Enter g(h);
+  Operand A = make_op(dA, lda, m, n);
+  TRY(pack(h, 0, A, true));
+  TRY(reset_status(h));
+  TRY(getrf_nopiv_core(h, m, n, A.ptr, A.ld));
+  TRY(unpack(h, A));
+  return read_status(h, info);
+}
+
+int egpu_dgetrs(egpu_handle h, int orient, int n, int nrhs, const double* dA, int lda, const int* dp, double* dB,
+                int ldb) {
+  TRY(check_handle(h));
+  if (n < 0 || nrhs < 0 || bad_ld(lda, n) || bad_ld(ldb, n)) return EGPU_ERR_ARG;
+  if (n == 0 || nrhs == 0) return EGPU_OK;
+  Enter g(h);
+  Operand A = make_op(const_cast<double*>(dA), lda, n, n), B = make_op(dB, ldb, n, nrhs);
+  TRY(pack(h, 0, A, true));
+  TRY(pack(h, 1, B, true));
+  TRY(reset_status(h));
+  TRY(getrs_core(h, orient == EGPU_NORMAL ? EGPU_NORMAL : EGPU_TRANSPOSE, n, nrhs, A.ptr, A.ld, dp, B.ptr, B.ld));
+  TRY(unpack(h, B));
+  return read_status(h, nullptr);
+}
+
+int egpu_dgesv(egpu_handle h, int n, int nrhs, double* dA, int lda, double* dB, int ldb, int* info) {
+  TRY(check_handle(h));
+  if (info) *info = 0;
+  if (n < 0 || nrhs < 0 || bad_ld(lda, n) || bad_ld(ldb, n)) return EGPU_ERR_ARG;
+  if (n == 0) return EGPU_OK;
+  Enter g(h);
+  Operand A = make_op(dA, lda, n, n), B = make_op(dB, ldb, n, std::max(nrhs, 1));
+  B.cols = nrhs;
+  TRY(pack(h, 0, A, true));
+  if (nrhs > 0) TRY(pack(h, 1, B, true));
+  TRY(reset_status(h));
+  int rc = gesv_core(h, n, nrhs, A.ptr, A.ld, B.ptr, B.ld);
+  if (rc < 0) return rc;
+  TRY(unpack(h, A));
+  if (nrhs > 0) TRY(unpack(h, B));
+  int rc2 = read_status(h, info);
+  return rc != EGPU_OK ? rc : rc2;
+}
+
+int egpu_dtrsm(egpu_handle h, int side, int uplo, int orient, int diag, int m, int n, double alpha,
+               const double* dA, int lda, double* dB, int ldb) {
+  TRY(check_handle(h));
+  const int nt = side == EGPU_LEFT ? m : n;
+  if (m < 0 || n < 0 || bad_ld(lda, nt) || bad_ld(ldb, m)) return EGPU_ERR_ARG;
+  if (m == 0 || n == 0) return EGPU_OK;
+  Enter g(h);
+  Operand A = make_op(const_cast<double*>(dA), lda, nt, nt), B = make_op(dB, ldb, m, n);
+  TRY(pack(h, 0, A, true));
+  TRY(pack(h, 1, B, true));
+  TRY(reset_status(h));
+  TRY(trsm_core(h, side, uplo, orient != EGPU_NORMAL, diag == EGPU_UNIT, m, n, alpha, A.ptr, A.ld, B.ptr, B.ld));
+  TRY(unpack(h, B));
+  return read_status(h, nullptr);
+}
+
+int egpu_dtrsv(egpu_handle h, int uplo, int orient, int diag, int n, const double* dA, int lda, double* dx) {
+  return egpu_dtrsm(h, EGPU_LEFT, uplo, orient, diag, n, 1, 1.0, dA, lda, dx, std::max(n, 1));
+}
+
+int egpu_dgemm(egpu_handle h, int oA, int oB, int m, int n, int k, double alpha, const double* dA, int lda,
+               const double* dB, int ldb, double beta, double* dC, int ldc) {
+  TRY(check_handle(h));
+  const bool ta = oA != EGPU_NORMAL, tb = oB != EGPU_NORMAL;
+  if (m < 0 || n < 0 || k < 0 || bad_ld(lda, ta ? k : m) || bad_ld(ldb, tb ? n : k) || bad_ld(ldc, m))
+    return EGPU_ERR_ARG;
+  if (m == 0 || n == 0) return EGPU_OK;
+  Enter g(h);
+  Operand A = make_op(const_cast<double*>(dA), lda, ta ? k : m, ta ? m : k);
+  Operand B = make_op(const_cast<double*>(dB), ldb, tb ? n : k, tb ? k : n);
+  TRY(pack(h, 0, A, true));
+  TRY(pack(h, 1, B, true));
+  TRY(reset_status(h));
+  TRY(launch_dgemm(h->stream, ta, !tb, m, n, k, alpha, A.ptr, A.ld, B.ptr, B.ld, beta, dC, ldc, 0, false,
+                   h->dstatus));
+  return read_status(h, nullptr);
+}
+
+int egpu_dherk(egpu_handle h, int uplo, int orient, int n, int k, double alpha, const double* dA, int lda,
+               double beta, double* dC, int ldc) {
+  TRY(check_handle(h));
+  const bool tr = orient != EGPU_NORMAL;
+  if (n < 0 || k < 0 || bad_ld(lda, tr ? k : n) || bad_ld(ldc, n)) return EGPU_ERR_ARG;
+  if (n == 0) return EGPU_OK;
+  Enter g(h);
+  Operand A = make_op(const_cast<double*>(dA), lda, tr ? k : n, tr ? n : k);
+  TRY(pack(h, 0, A, true));
+  TRY(reset_status(h));
+  // NORMAL: C = a A A^T  (op(A) = A MN-major, op(B) = A^T MN-major)
+  // ADJOINT: C = a A^T A (op(A) = A^T K-major, op(B) = A K-major)
+  TRY(launch_dgemm(h->stream, tr, tr, n, n, k, alpha, A.ptr, A.ld, A.ptr, A.ld, beta, dC, ldc,
+                   uplo == EGPU_LOWER ? 1 : 2, false, h->dstatus));
+  return read_status(h, nullptr);
+}
+
+int egpu_dlaswp(egpu_handle h, int inverse, int m, int n, double* dA, int lda, const int* dp, int npiv) {
+  TRY(check_handle(h));
+  if (m < 0 || n < 0 || npiv < 0 || npiv > m || bad_ld(lda, m)) return EGPU_ERR_ARG;
+  if (m == 0 || n == 0 || npiv == 0) return EGPU_OK;
+  Enter g(h);
+  TRY(ensure_ws(h, align_up(sizeof(int) * (size_t)((m + 1) & ~1), 256) + sizeof(double) * (size_t)m * n + 4096));
+  TRY(launch_laswp_seq(h->stream, inverse, m, n, dA, lda, dp, npiv, static_cast<int*>(h->ws)));
+  EGPU_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  return EGPU_OK;
+}
+
+// ------------------------------------------------------------ host API --
+// Copy host column-major buffers into handle staging memory (ld multiple of
+// 32), run the device path, copy results back.
+
+static int h2d(egpu_context* h, int slot, const double* src, int lda, int rows, int cols, double** dst,
+               long long* ldd) {
+  *ldd = ld_aligned(rows);
+  TRY(ensure_stage(h, slot, sizeof(double) * (size_t)(*ldd) * std::max(cols, 1)));
+  *dst = static_cast<double*>(h->stage[slot]);
+  if (rows > 0 && cols > 0)
+    EGPU_CUDA_TRY(cudaMemcpy2DAsync(*dst, sizeof(double) * (*ldd), src, sizeof(double) * lda,
+                                    sizeof(double) * rows, cols, cudaMemcpyHostToDevice, h->stream));
+  return EGPU_OK;
+}
+
+static int d2h(egpu_context* h, const double* src, long long ldd, double* dst, int lda, int rows, int cols) {
+  if (rows > 0 && cols > 0)
+    EGPU_CUDA_TRY(cudaMemcpy2DAsync(dst, sizeof(double) * lda, src, sizeof(double) * ldd, sizeof(double) * rows,
+                                    cols, cudaMemcpyDeviceToHost, h->stream));
+  return EGPU_OK;
+}
+
+static int* stage_ints(egpu_context* h, int slot, size_t count) {
+  if (ensure_stage(h, slot, sizeof(int) * std::max<size_t>(count, 1)) != EGPU_OK) return nullptr;
+  return static_cast<int*>(h->stage[slot]);
+}
+
+int egpu_host_dpotrf(egpu_handle h, int uplo, int n, double* A, int lda, int* info) {
+  TRY(check_handle(h));
+  if (info) *info = 0;
+  if (n < 0 || bad_ld(lda, n) || (uplo != EGPU_LOWER && uplo != EGPU_UPPER)) return EGPU_ERR_ARG;
+  if (n == 0) return EGPU_OK;
+  Enter g(h);
+  double* d; long long ld;
+  TRY(h2d(h, 0, A, lda, n, n, &d, &ld));
+  TRY(reset_status(h));
+  int rc = potrf_core(h, uplo, n, d, ld);
+  if (rc < 0) return rc;
+  TRY(d2h(h, d, ld, A, lda, n, n));
+  return read_status(h, info);
+}
+
+int egpu_host_dpotrs(egpu_handle h, int uplo, int orient, int n, int nrhs, const double* A, int lda, double* B,
+                     int ldb) {
+  TRY(check_handle(h));
+  (void)orient;
+  if (n < 0 || nrhs < 0 || bad_ld(lda, n) || bad_ld(ldb, n)) return EGPU_ERR_ARG;
+  if (n == 0 || nrhs == 0) return EGPU_OK;
+  Enter g(h);
+  double *dA, *dB; long long la, lb;
+  TRY(h2d(h, 0, A, lda, n, n, &dA, &la));
+  TRY(h2d(h, 1, B, ldb, n, nrhs, &dB, &lb));
+  TRY(reset_status(h));
+  TRY(potrs_core(h, uplo, n, nrhs, dA, la, dB, lb));
+  TRY(d2h(h, dB, lb, B, ldb, n, nrhs));
+  return read_status(h, nullptr);
+}
+
+int egpu_host_dposv(egpu_handle h, int uplo, int orient, int n, int nrhs, double* A, int lda, double* B, int ldb,
+                    int* info) {
+  TRY(check_handle(h));
+  (void)orient;
+  if (info) *info = 0;
+  if (n < 0 || nrhs < 0 || bad_ld(lda, n) || bad_ld(ldb, n)) return EGPU_ERR_ARG;
+  if (n == 0) return EGPU_OK;
+  Enter g(h);
+  double *dA, *dB; long long la, lb;
+  TRY(h2d(h, 0, A, lda, n, n, &dA, &la));
+  TRY(h2d(h, 1, B, ldb, n, nrhs, &dB, &lb));
+  TRY(reset_status(h));
+  TRY(potrf_core(h, uplo, n, dA, la));
+  int rc = read_status(h, info);
+  if (rc == EGPU_OK && nrhs > 0) TRY(potrs_core(h, uplo, n, nrhs, dA, la, dB, lb));
+  TRY(d2h(h, dA, la, A, lda, n, n));
+  if (rc == EGPU_OK && nrhs > 0) TRY(d2h(h, dB, lb, B, ldb, n, nrhs));
+  int rc2 = read_status(h, nullptr);
+  return rc != EGPU_OK ? rc : rc2;
+}
+
+int egpu_host_dgetrf(egpu_handle h, int m, int n, double* A, int lda, int* p, int* info) {
+  TRY(check_handle(h));
+  if (info) *info = 0;
+  if (m < 0 || n < 0 || bad_ld(lda, m)) return EGPU_ERR_ARG;
+  if (m == 0 || n == 0) return EGPU_OK;
+  Enter g(h);
+  double* d; long long ld;
+  TRY(h2d(h, 0, A, lda, m, n, &d, &ld));
+  const int mn = std::min(m, n);
+  int* dp = stage_ints(h, 2, mn);
+  if (!dp) return EGPU_ERR_ALLOC;
+  TRY(reset_status(h));
+  int rc = getrf_core(h, m, n, d, ld, dp);
+  if (rc < 0) return rc;
+  TRY(d2h(h, d, ld, A, lda, m, n));
+  EGPU_CUDA_TRY(cudaMemcpyAsync(p, dp, sizeof(int) * mn, cudaMemcpyDeviceToHost, h->stream));
+  return read_status(h, info);
+}
+
+int egpu_host_dgetrf_nopiv(egpu_handle h, int m, int n, double* A, int lda, int* info) {
+  TRY(check_handle(h));
+  if (info) *info = 0;
+  if (m < 0 || n < 0 || bad_ld(lda, m)) return EGPU_ERR_ARG;
+  if (m == 0 || n == 0) return EGPU_OK;
+  Enter g(h);
+  double* d; long long ld;
+  TRY(h2d(h, 0, A, lda, m, n, &d, &ld));
+  TRY(reset_status(h));
+  int rc = getrf_nopiv_core(h, m, n, d, ld);
+  if (rc < 0) return rc;
+  TRY(d2h(h, d, ld, A, lda, m, n));
+  return read_status(h, info);
+}
+
+int egpu_host_dgetrs(egpu_handle h, int orient, int n, int nrhs, const double* A, int lda, const int* p,
+                     double* B, int ldb) {
+  TRY(check_handle(h));
+  if (n < 0 || nrhs < 0 || bad_ld(lda, n) || bad_ld(ldb, n)) return EGPU_ERR_ARG;
+  if (n == 0 || nrhs == 0) return EGPU_OK;
+  Enter g(h);
+  double *dA, *dB; long long la, lb;
+  TRY(h2d(h, 0, A, lda, n, n, &dA, &la));
+  TRY(h2d(h, 1, B, ldb, n, nrhs, &dB, &lb));
+  int* dp = nullptr;
+  if (p) {
+    dp = stage_ints(h, 2, n);
+    if (!dp) return EGPU_ERR_ALLOC;
+    EGPU_CUDA_TRY(cudaMemcpyAsync(dp, p, sizeof(int) * n, cudaMemcpyHostToDevice, h->stream));
+  }
+  TRY(reset_status(h));
+  TRY(getrs_core(h, orient == EGPU_NORMAL ? EGPU_NORMAL : EGPU_TRANSPOSE, n, nrhs, dA, la, dp, dB, lb));
+  TRY(d2h(h, dB, lb, B, ldb, n, nrhs));
+  return read_status(h, nullptr);
+}
+
+int egpu_host_dgesv(egpu_handle h, int n, int nrhs, double* A, int lda, double* B, int ldb, int* info) {
+  TRY(check_handle(h));
+  if (info) *info = 0;
+  if (n < 0 || nrhs < 0 || bad_ld(lda, n) || bad_ld(ldb, n)) return EGPU_ERR_ARG;
+  if (n == 0) return EGPU_OK;
+  Enter g(h);
+  double *dA, *dB; long long la, lb;
+  TRY(h2d(h, 0, A, lda, n, n, &dA, &la));
+  TRY(h2d(h, 1, B, ldb, n, std::max(nrhs, 1), &dB, &lb));
+  TRY(reset_status(h));
+  int rc = gesv_core(h, n, nrhs, dA, la, dB, lb);
+  if (rc < 0) return rc;
+  TRY(d2h(h, dA, la, A, lda, n, n));
+  if (nrhs > 0) TRY(d2h(h, dB, lb, B, ldb, n, nrhs));
+  int rc2 = read_status(h, info);
+  return rc != EGPU_OK ? rc : rc2;
+}
+
+int egpu_host_dtrsm(egpu_handle h, int side, int uplo, int orient, int diag, int m, int n, double alpha,
+                    const double* A, int lda, double* B, int ldb) {
+  TRY(check_handle(h));
+  const int nt = side == EGPU_LEFT ? m : n;
+  if (m < 0 || n < 0 || bad_ld(lda, nt) || bad_ld(ldb, m)) return EGPU_ERR_ARG;
+  if (m == 0 || n == 0) return EGPU_OK;
+  Enter g(h);
+  double *dA, *dB; long long la, lb;
+  TRY(h2d(h, 0, A, lda, nt, nt, &dA, &la));
+  TRY(h2d(h, 1, B, ldb, m, n, &dB, &lb));
+  TRY(reset_status(h));
+  TRY(trsm_core(h, side, uplo, orient != EGPU_NORMAL, diag == EGPU_UNIT, m, n, alpha, dA, la, dB, lb));
+  TRY(d2h(h, dB, lb, B, ldb, m, n));
+  return read_status(h, nullptr);
+}
+
+int egpu_host_dgemm(egpu_handle h, int oA, int oB, int m, int n, int k, double alpha, const double* A, int lda,
+                    const double* B, int ldb, double beta, double* C, int ldc) {
+  TRY(check_handle(h));
+  const bool ta = oA != EGPU_NORMAL, tb = oB != EGPU_NORMAL;
+  if (m < 0 || n < 0 || k < 0 || bad_ld(lda, ta ? k : m) || bad_ld(ldb, tb ? n : k) || bad_ld(ldc, m))
+    return EGPU_ERR_ARG;
+  if (m == 0 || n == 0) return EGPU_OK;
+  Enter g(h);
+  double *dA, *dB, *dC; long long la, lb, lc;
+  TRY(h2d(h, 0, A, lda, ta ? k : m, ta ? m : k, &dA, &la));
+  TRY(h2d(h, 1, B, ldb, tb ? n : k, tb ? k : n, &dB, &lb));
+  TRY(h2d(h, 2, C, ldc, m, n, &dC, &lc));
+  TRY(reset_status(h));
+  TRY(launch_dgemm(h->stream, ta, !tb, m, n, k, alpha, dA, la, dB, lb, beta, dC, lc, 0, false, h->dstatus));
+  TRY(d2h(h, dC, lc, C, ldc, m, n));
+  return read_status(h, nullptr);
+}
+
+int egpu_host_dherk(egpu_handle h, int uplo, int orient, int n, int k, double alpha, const double* A, int lda,
+                    double beta, double* C, int ldc) {
+  TRY(check_handle(h));
+  const bool tr = orient != EGPU_NORMAL;
+  if (n < 0 || k < 0 || bad_ld(lda, tr ? k : n) || bad_ld(ldc, n)) return EGPU_ERR_ARG;
+  if (n == 0) return EGPU_OK;
+  Enter g(h);
+  double *dA, *dC; long long la, lc;
+  TRY(h2d(h, 0, A, lda, tr ? k : n, tr ? n : k, &dA, &la));
+  TRY(h2d(h, 2, C, ldc, n, n, &dC, &lc));
+  TRY(reset_status(h));
+  TRY(launch_dgemm(h->stream, tr, tr, n, n, k, alpha, dA, la, dA, la, beta, dC, lc, uplo == EGPU_LOWER ? 1 : 2,
+                   false, h->dstatus));
+  TRY(d2h(h, dC, lc, C, ldc, n, n));
+  return read_status(h, nullptr);
+}
+
+int egpu_host_dlaswp(egpu_handle h, int inverse, int m, int n, double* A, int lda, const int* p, int npiv) {
+  TRY(check_handle(h));
+  if (m < 0 || n < 0 || npiv < 0 || npiv > m || bad_ld(lda, m)) return EGPU_ERR_ARG;
+  if (m == 0 || n == 0 || npiv == 0) return EGPU_OK;
+  Enter g(h);
+  double* dA; long long la;
+  TRY(h2d(h, 0, A, lda, m, n, &dA, &la));
+  int* dp = stage_ints(h, 2, npiv);
+  if (!dp) return EGPU_ERR_ALLOC;
+  EGPU_CUDA_TRY(cudaMemcpyAsync(dp, p, sizeof(int) * npiv, cudaMemcpyHostToDevice, h->stream));
+  TRY(ensure_ws(h, align_up(sizeof(int) * (size_t)((m + 1) & ~1), 256) + sizeof(double) * (size_t)m * n + 4096));
+  TRY(launch_laswp_seq(h->stream, inverse, m, n, dA, la, dp, npiv, static_cast<int*>(h->ws)));
+  TRY(d2h(h, dA, la, A, lda, m, n));
+  EGPU_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  return EGPU_OK;
+}
+
+}  // extern "C"

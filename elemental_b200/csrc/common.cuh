@@ -1,0 +1,132 @@
+// Shared device/host helpers for the sm_100a factor-and-solve kernels:
+// status words, bounded waits, mbarrier + TMA wrappers, DMMA wrapper.
+#pragma once
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstdio>
+
+namespace egpu {
+
+// ---------------------------------------------------------------- status --
+// Per-factorization status word written by the kernels (device memory).
+// code 0 = ok; the host maps the others to Elemental's exceptions.
+enum StatusCode : int {
+  kOk = 0,
+  kNotHPD = 1,     // Cholesky: non-positive pivot (std::logic_error in the reference)
+  kSingular = 2,   // LU: exact zero pivot (SingularMatrixException)
+  kTimeout = 3,    // a bounded device-side wait ran out
+};
+
+struct DevStatus {
+  int code;   // StatusCode (first failure wins)
+  int info;   // 1-based global column of the failure, or wait-site id
+};
+
+__device__ __forceinline__ void set_status(DevStatus* st, int code, int info) {
+  if (st == nullptr) return;
+  if (atomicCAS(&st->code, 0, code) == 0) st->info = info;
+}
+
+// Upper bound on spin iterations of any device-side wait.  Each iteration is
+// a try_wait / acquire load plus a short nanosleep, so the bound is ~1 s.
+constexpr long long kSpinLimit = 1ll << 22;
+
+// -------------------------------------------------------------- mbarrier --
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void fence_mbar_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// Bounded wait on an mbarrier phase.  Returns false when the limit ran out.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
+  for (long long it = 0; it < kSpinLimit; ++it) {
+    if (mbar_try_wait(bar, parity)) return true;
+    if (it > 64) __nanosleep(64);
+  }
+  return false;
+}
+
+// ------------------------------------------------------------------- TMA --
+__device__ __forceinline__ void tma_load_2d(void* smem_dst, const CUtensorMap* map, uint64_t* bar, int c0,
+                                            int c1) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], "
+      "[%4];" ::"r"(smem_u32(smem_dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(smem_u32(bar))
+      : "memory");
+}
+
+__device__ __forceinline__ void tma_prefetch_desc(const CUtensorMap* map) {
+  asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(map)) : "memory");
+}
+
+// ------------------------------------------------------------------ DMMA --
+// D = A(16x8) * B(8x8) + D, FP64 tensor-core MMA (legacy warp-level form;
+// tcgen05 has no f64 kind).
+__device__ __forceinline__ void dmma_16x8x8(double (&d)[4], const double (&a)[4], const double (&b)[2]) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k8.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%0,%1,%2,%3};\n"
+      : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
+      : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(b[0]), "d"(b[1]));
+}
+
+// ------------------------------------------------------------ grid sync --
+// Bounded grid-wide barrier over `nblocks` co-resident CTAs (cooperative
+// launch).  `counter` is a monotonically increasing arrival counter in
+// global memory; `target` = nblocks * (barrier ordinal + 1).
+__device__ __forceinline__ bool grid_barrier(unsigned int* counter, unsigned int target) {
+  __syncthreads();
+  bool ok = true;
+  if (threadIdx.x == 0) {
+    __threadfence();
+    atomicAdd(counter, 1u);
+    long long it = 0;
+    while (true) {
+      unsigned int v;
+      asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(counter) : "memory");
+      if ((int)(v - target) >= 0) break;
+      if (++it > kSpinLimit) { ok = false; break; }
+      if (it > 32) __nanosleep(32);
+    }
+  }
+  __shared__ int s_ok;
+  if (threadIdx.x == 0) s_ok = ok;
+  __syncthreads();
+  return s_ok != 0;
+}
+
+}  // namespace egpu
+
+// ----------------------------------------------------------- host errors --
+#define EGPU_CUDA_TRY(expr)                                                                   \
+  do {                                                                                        \
+    cudaError_t _e = (expr);                                                                  \
+    if (_e != cudaSuccess) {                                                                  \
+      egpu::set_last_error(_e, #expr, __FILE__, __LINE__);                                    \
+      return EGPU_ERR_CUDA;                                                                   \
+    }                                                                                         \
+  } while (0)

@@ -1,0 +1,72 @@
+// Internal declarations shared by the .cu translation units.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <algorithm>
+
+#include "../../include/elemgpu.h"
+#include "common.cuh"
+
+namespace egpu {
+
+void set_last_error(cudaError_t e, const char* what, const char* file, int line);
+
+// Process-wide count of kernel launches issued by this library.
+void count_launch(int n = 1);
+
+bool tma_compatible(const void* p, long long ld);
+
+// ---- launch tracing (per-kernel-class CUDA-event timing on the launch stream)
+enum TraceKind { kTraceUpdate = 0, kTraceTrsm = 1, kTraceDiag = 2, kTracePanel = 3, kTraceSwap = 4,
+                 kTraceOther = 5, kTraceKinds = 6 };
+struct Trace;
+// Records an event pair around one launch when the calling thread has an
+// active trace; no-op otherwise.
+struct TraceMark {
+  Trace* t = nullptr;
+  int idx = -1;
+  cudaStream_t st = nullptr;
+  TraceMark(cudaStream_t s, int kind, double flops, double bytes);
+  ~TraceMark();
+};
+
+int launch_dgemm(cudaStream_t st, bool a_kmajor, bool b_kmajor, int M, int N, int K, double alpha,
+                 const double* A, long long lda, const double* B, long long ldb, double beta, double* C,
+                 long long ldc, int tri, bool wide, DevStatus* status);
+int launch_scale(cudaStream_t st, int M, int N, double beta, double* C, long long ldc, int tri);
+
+// Diagonal-block Cholesky (factor in place + triangular inverse into W).
+int launch_potrf_diag(cudaStream_t st, int uplo, double* A, long long lda, int b, double* W, int ldw,
+                      DevStatus* status, int col_base);
+
+// Batched triangular inverse of `count` diagonal blocks of size b (the last
+// one may be smaller: n total), block i at A + i*b*(lda+1), into W + i*b*ldw.
+int launch_trtri_blocks(cudaStream_t st, int uplo, int unit, const double* A, long long lda, int n, int b,
+                        double* W, int ldw);
+
+// LU panel: factor the m x b panel at A in place with partial pivoting;
+// p (device, b entries) receives absolute rows (offset added); image/preimage
+// (device, b entries each) receive the composed permutation; W receives
+// inv(unit-lower L11).  scratch: see lu_panel_scratch_bytes.
+size_t lu_panel_scratch_bytes(int m, int b, int sm_count);
+int launch_lu_panel(cudaStream_t st, int m, int b, double* A, long long lda, int* p, int offset, int* image,
+                    int* preimage, double* W, int ldw, void* scratch, DevStatus* status, int sm_count);
+
+// Apply composed panel pivots (image/preimage of b rows) to columns of the
+// m-row block A (ld lda), columns [0, ncols).
+int launch_apply_composed(cudaStream_t st, int m, int ncols, double* A, long long lda, int b, const int* image,
+                          const int* preimage, const DevStatus* status);
+
+// Apply sequential swaps p[0..np) (absolute rows) to rows of A (m x n).
+int launch_laswp_seq(cudaStream_t st, int inverse, int m, int n, double* A, long long lda, const int* p, int np,
+                     int* perm_scratch);
+
+// Unpivoted LU of a b x b diagonal block in place; W receives inv(unit L11),
+// W2 receives inv(U11).
+int launch_getrf_diag_nopiv(cudaStream_t st, double* A, long long lda, int b, double* W, int ldw, double* W2,
+                            DevStatus* status, int col_base);
+
+// Copy between strided device matrices.
+int launch_copy(cudaStream_t st, int m, int n, const double* src, long long lds, double* dst, long long ldd);
+
+}  // namespace egpu

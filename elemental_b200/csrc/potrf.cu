@@ -1,0 +1,262 @@
+// Diagonal-block kernels: unblocked Cholesky / LU of one nb x nb block held in
+// shared memory, and triangular inverses of diagonal blocks (the trsm sweeps
+// multiply by these inverses on the tensor cores).
+#include "internal.h"
+
+namespace egpu {
+
+constexpr int kDiagThreads = 256;
+constexpr int kMaxNB = 128;
+
+// In-place inverse of the uplo triangle of the b x b column-major block S
+// (ld b) in shared memory.  unit: the diagonal is taken as 1 and left as 1.
+// Row-parallel forward/backward substitution, two barriers per column.  The
+// diagonal of a unit triangle is never read, so a unit-lower inverse can share
+// S with an upper triangle (the two touch disjoint entries).
+__device__ void tri_inverse_smem(double* S, int b, int uplo, int unit) {
+  const int i = threadIdx.x;
+  if (uplo == EGPU_LOWER) {
+    for (int j = b - 1; j >= 0; --j) {
+      const double dinv = unit ? 1.0 : 1.0 / S[j + j * b];
+      double tmp = 0.0;
+      if (i > j && i < b) {
+        // X[i, j] = -(sum_{k=j+1..i} X[i,k] L[k,j]) / L[j,j]   (X[i,i] already inverted)
+        for (int k = j + 1; k < i; ++k) tmp = fma(S[i + k * b], S[k + j * b], tmp);
+        tmp = fma(unit ? 1.0 : S[i + i * b], S[i + j * b], tmp);
+      }
+      __syncthreads();
+      if (i > j && i < b) S[i + j * b] = -tmp * dinv;
+      if (i == 0 && !unit) S[j + j * b] = dinv;
+      __syncthreads();
+    }
+  } else {
+    for (int j = 0; j < b; ++j) {
+      const double dinv = unit ? 1.0 : 1.0 / S[j + j * b];
+      double tmp = 0.0;
+      if (i < j) {
+        // X[i, j] = -(sum_{k=i..j-1} X[i,k] U[k,j]) / U[j,j]
+        tmp = (unit ? 1.0 : S[i + i * b]) * S[i + j * b];
+        for (int k = i + 1; k < j; ++k) tmp = fma(S[i + k * b], S[k + j * b], tmp);
+      }
+      __syncthreads();
+      if (i < j) S[i + j * b] = -tmp * dinv;
+      if (i == 0 && !unit) S[j + j * b] = dinv;
+      __syncthreads();
+    }
+  }
+}
+
+// Cholesky of the b x b diagonal block (cholesky::LVar3Unb,
+// lapack-like/Cholesky/LVar3.hpp:19-49, or UVar3Unb, Cholesky/UVar3.hpp:21-50),
+// followed by the inverse of the factor into W (other triangle zeroed).
+template <int UPLO>
+__global__ void __launch_bounds__(kDiagThreads) potrf_diag_kernel(double* A, long long lda, int b, double* W,
+                                                                   int ldw, DevStatus* st, int col_base) {
+  extern __shared__ double S[];
+  if (st != nullptr && st->code != 0) return;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  constexpr int NW = kDiagThreads / 32;
+  for (int idx = tid; idx < b * b; idx += kDiagThreads) {
+    const int r = idx % b, c = idx / b;
+    S[idx] = (UPLO == EGPU_LOWER ? r >= c : r <= c) ? A[r + c * lda] : 0.0;
+  }
+  __syncthreads();
+  for (int j = 0; j < b; ++j) {
+    const double ajj = S[j + j * b];
+    if (ajj <= 0.0) {  // "A was not numerically HPD"
+      if (tid == 0) set_status(st, kNotHPD, col_base + j + 1);
+      return;
+    }
+    const double alpha = sqrt(ajj);
+    __syncthreads();
+    if (UPLO == EGPU_LOWER) {
+      for (int i = j + 1 + tid; i < b; i += kDiagThreads) S[i + j * b] /= alpha;
+    } else {
+      for (int k = j + 1 + tid; k < b; k += kDiagThreads) S[j + k * b] /= alpha;
+    }
+    if (tid == 0) S[j + j * b] = alpha;
+    __syncthreads();
+    if (UPLO == EGPU_LOWER) {
+      for (int k = j + 1 + warp; k < b; k += NW) {
+        const double lk = S[k + j * b];
+        for (int i = k + lane; i < b; i += 32) S[i + k * b] -= S[i + j * b] * lk;
+      }
+    } else {
+      for (int k = j + 1 + warp; k < b; k += NW) {
+        const double uk = S[j + k * b];
+        for (int i = j + 1 + lane; i <= k; i += 32) S[i + k * b] -= S[j + i * b] * uk;
+      }
+    }
+    __syncthreads();
+  }
+  for (int idx = tid; idx < b * b; idx += kDiagThreads) {
+    const int r = idx % b, c = idx / b;
+    if (UPLO == EGPU_LOWER ? r >= c : r <= c) A[r + c * lda] = S[idx];
+  }
+  __syncthreads();
+  tri_inverse_smem(S, b, UPLO, 0);
+  for (int idx = tid; idx < b * b; idx += kDiagThreads) {
+    const int r = idx % b, c = idx / b;
+    W[r + (long long)c * ldw] = (UPLO == EGPU_LOWER ? r >= c : r <= c) ? S[idx] : 0.0;
+  }
+}
+
+int launch_potrf_diag(cudaStream_t st, int uplo, double* A, long long lda, int b, double* W, int ldw,
+                      DevStatus* status, int col_base) {
+  if (b <= 0) return EGPU_OK;
+  if (b > kMaxNB) return EGPU_ERR_ARG;
+  const size_t smem = sizeof(double) * b * b;
+  TraceMark tm(st, kTraceDiag, (double)b * b * b / 3.0 * 2.0, 16.0 * b * b);
+  cudaError_t e;
+  if (uplo == EGPU_LOWER) {
+    e = cudaFuncSetAttribute(potrf_diag_kernel<EGPU_LOWER>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)(sizeof(double) * kMaxNB * kMaxNB));
+    if (e == cudaSuccess)
+      potrf_diag_kernel<EGPU_LOWER><<<1, kDiagThreads, smem, st>>>(A, lda, b, W, ldw, status, col_base);
+      count_launch();
+  } else {
+    e = cudaFuncSetAttribute(potrf_diag_kernel<EGPU_UPPER>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)(sizeof(double) * kMaxNB * kMaxNB));
+    if (e == cudaSuccess)
+      potrf_diag_kernel<EGPU_UPPER><<<1, kDiagThreads, smem, st>>>(A, lda, b, W, ldw, status, col_base);
+      count_launch();
+  }
+  if (e == cudaSuccess) e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    set_last_error(e, "potrf_diag launch", __FILE__, __LINE__);
+    return EGPU_ERR_CUDA;
+  }
+  return EGPU_OK;
+}
+
+// Inverse of each diagonal block (block i covers rows/cols [i b, min(n, i b + b))).
+__global__ void __launch_bounds__(kDiagThreads) trtri_blocks_kernel(int uplo, int unit, const double* A,
+                                                                     long long lda, int n, int b, double* W,
+                                                                     int ldw) {
+  extern __shared__ double S[];
+  const int blk = blockIdx.x;
+  const int off = blk * b;
+  const int bb = min(b, n - off);
+  const double* Ab = A + off + (long long)off * lda;
+  double* Wb = W + (long long)blk * b * ldw;
+  const int tid = threadIdx.x;
+  for (int idx = tid; idx < bb * bb; idx += kDiagThreads) {
+    const int r = idx % bb, c = idx / bb;
+    const bool in = (uplo == EGPU_LOWER) ? (unit ? r > c : r >= c) : (unit ? r < c : r <= c);
+    S[idx] = in ? Ab[r + c * lda] : ((r == c) ? 1.0 : 0.0);
+  }
+  __syncthreads();
+  tri_inverse_smem(S, bb, uplo, unit);
+  for (int idx = tid; idx < b * b; idx += kDiagThreads) {
+    const int r = idx % b, c = idx / b;
+    double v = 0.0;
+    if (r < bb && c < bb) {
+      const bool in = (uplo == EGPU_LOWER) ? r >= c : r <= c;
+      v = in ? S[r + c * bb] : 0.0;
+      if (unit && r == c) v = 1.0;
+    }
+    Wb[r + (long long)c * ldw] = v;
+  }
+}
+
+int launch_trtri_blocks(cudaStream_t st, int uplo, int unit, const double* A, long long lda, int n, int b,
+                        double* W, int ldw) {
+  if (n <= 0) return EGPU_OK;
+  if (b > kMaxNB || b <= 0) return EGPU_ERR_ARG;
+  const int count = (n + b - 1) / b;
+  TraceMark tm(st, kTraceDiag, (double)count * b * b * b / 3.0, 16.0 * count * b * b);
+  cudaError_t e = cudaFuncSetAttribute(trtri_blocks_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)(sizeof(double) * kMaxNB * kMaxNB));
+  if (e == cudaSuccess) {
+    trtri_blocks_kernel<<<count, kDiagThreads, sizeof(double) * b * b, st>>>(uplo, unit, A, lda, n, b, W, ldw);
+    count_launch();
+    e = cudaGetLastError();
+  }
+  if (e != cudaSuccess) {
+    set_last_error(e, "trtri launch", __FILE__, __LINE__);
+    return EGPU_ERR_CUDA;
+  }
+  return EGPU_OK;
+}
+
+// Unpivoted LU of the b x b diagonal block (lu::Unb, lapack-like/LU/Local.hpp:61-82);
+// W := inv(unit lower L11), W2 := inv(U11).
+__global__ void __launch_bounds__(kDiagThreads) getrf_diag_nopiv_kernel(double* A, long long lda, int b, double* W,
+                                                                         int ldw, double* W2, DevStatus* st,
+                                                                         int col_base) {
+  extern __shared__ double S[];
+  if (st != nullptr && st->code != 0) return;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  constexpr int NW = kDiagThreads / 32;
+  for (int idx = tid; idx < b * b; idx += kDiagThreads) S[idx] = A[idx % b + (idx / b) * lda];
+  __syncthreads();
+  for (int j = 0; j < b; ++j) {
+    const double alpha = S[j + j * b];
+    if (alpha == 0.0) {
+      if (tid == 0) set_status(st, kSingular, col_base + j + 1);
+      return;
+    }
+    const double inv = 1.0 / alpha;
+    for (int i = j + 1 + tid; i < b; i += kDiagThreads) S[i + j * b] *= inv;
+    __syncthreads();
+    for (int c = j + 1 + warp; c < b; c += NW) {
+      const double u = S[j + c * b];
+      for (int i = j + 1 + lane; i < b; i += 32) S[i + c * b] -= S[i + j * b] * u;
+    }
+    __syncthreads();
+  }
+  for (int idx = tid; idx < b * b; idx += kDiagThreads) A[idx % b + (idx / b) * lda] = S[idx];
+  __syncthreads();
+  // Strict lower (unit L) and upper-with-diagonal (U) are disjoint: invert both in place.
+  tri_inverse_smem(S, b, EGPU_LOWER, 1);
+  tri_inverse_smem(S, b, EGPU_UPPER, 0);
+  for (int idx = tid; idx < b * b; idx += kDiagThreads) {
+    const int r = idx % b, c = idx / b;
+    W[r + (long long)c * ldw] = r > c ? S[idx] : (r == c ? 1.0 : 0.0);
+    W2[r + (long long)c * ldw] = r <= c ? S[idx] : 0.0;
+  }
+}
+
+int launch_getrf_diag_nopiv(cudaStream_t st, double* A, long long lda, int b, double* W, int ldw, double* W2,
+                            DevStatus* status, int col_base) {
+  if (b <= 0) return EGPU_OK;
+  if (b > kMaxNB) return EGPU_ERR_ARG;
+  cudaError_t e = cudaFuncSetAttribute(getrf_diag_nopiv_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)(sizeof(double) * kMaxNB * kMaxNB));
+  if (e == cudaSuccess) {
+    getrf_diag_nopiv_kernel<<<1, kDiagThreads, sizeof(double) * b * b, st>>>(A, lda, b, W, ldw, W2, status,
+                                                                             col_base);
+    count_launch();
+    e = cudaGetLastError();
+  }
+  if (e != cudaSuccess) {
+    set_last_error(e, "getrf_diag launch", __FILE__, __LINE__);
+    return EGPU_ERR_CUDA;
+  }
+  return EGPU_OK;
+}
+
+__global__ void copy_kernel(int m, int n, const double* src, long long lds, double* dst, long long ldd) {
+  const long long total = (long long)m * n;
+  for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
+       idx += (long long)gridDim.x * blockDim.x) {
+    const int r = (int)(idx % m), c = (int)(idx / m);
+    dst[r + c * ldd] = src[r + c * lds];
+  }
+}
+
+int launch_copy(cudaStream_t st, int m, int n, const double* src, long long lds, double* dst, long long ldd) {
+  if (m <= 0 || n <= 0) return EGPU_OK;
+  const long long total = (long long)m * n;
+  const int blocks = (int)std::min<long long>((total + 255) / 256, 148 * 16);
+  copy_kernel<<<blocks, 256, 0, st>>>(m, n, src, lds, dst, ldd);
+  count_launch();
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    set_last_error(e, "copy launch", __FILE__, __LINE__);
+    return EGPU_ERR_CUDA;
+  }
+  return EGPU_OK;
+}
+
+}  // namespace egpu

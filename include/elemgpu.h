@@ -1,0 +1,173 @@
+/*
+ * elemgpu.h -- C ABI of the B200 (sm_100a) factor-and-solve library.
+ *
+ * Plain pointers and sizes only.  Matrices are column-major with a leading
+ * dimension, indices 0-based, exactly as Elemental's Matrix<F> stores them
+ * (core/matrix.hpp:16-183; ldim = max(height,1), src/core/matrix.cpp:76).
+ * Pivot vectors follow Elemental's convention: p[i] is the absolute 0-based
+ * row swapped with row i at step i (lapack-like/LU/Panel.hpp:64).
+ *
+ * Two families of entry points:
+ *   egpu_d*      operate on DEVICE memory (the matrix stays resident in HBM);
+ *                they run on the handle's stream.
+ *   egpu_host_d* operate on HOST buffers (the Matrix<F> drop-in path): copy
+ *                in, run, copy out, synchronize.
+ *
+ * Return value: EGPU_OK, a factorization status (EGPU_NOT_HPD,
+ * EGPU_SINGULAR, EGPU_TIMEOUT; *info = 1-based global column), or a negative
+ * error.  The C++ layer (elemgpu/elemental.hpp) maps the statuses to
+ * Elemental's exceptions: std::logic_error("A was not numerically HPD")
+ * (Cholesky/LVar3.hpp:37-38) and SingularMatrixException (LU/Panel.hpp:76-77).
+ *
+ * Enum values equal Elemental's (core/types_decl.hpp:104-155).
+ */
+#ifndef ELEMGPU_H
+#define ELEMGPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- return codes ---- */
+#define EGPU_OK 0
+#define EGPU_NOT_HPD 1    /* non-positive pivot in Cholesky */
+#define EGPU_SINGULAR 2   /* exact zero pivot in LU */
+#define EGPU_TIMEOUT 3    /* a bounded device-side wait ran out */
+#define EGPU_ERR_ARG (-1)
+#define EGPU_ERR_CUDA (-2)
+#define EGPU_ERR_ALLOC (-3)
+#define EGPU_ERR_ALIGN (-4)
+#define EGPU_ERR_TMA (-5)
+#define EGPU_ERR_UNSUPPORTED (-6)
+#define EGPU_ERR_NO_DEVICE (-7)
+
+/* ---- enums (Elemental core/types_decl.hpp) ---- */
+#define EGPU_LOWER 0       /* UpperOrLower */
+#define EGPU_UPPER 1
+#define EGPU_NORMAL 0      /* Orientation */
+#define EGPU_TRANSPOSE 1
+#define EGPU_ADJOINT 2
+#define EGPU_LEFT 0        /* LeftOrRight */
+#define EGPU_RIGHT 1
+#define EGPU_NON_UNIT 0    /* UnitOrNonUnit */
+#define EGPU_UNIT 1
+
+#if defined(__GNUC__)
+#define EGPU_API __attribute__((visibility("default")))
+#else
+#define EGPU_API
+#endif
+
+typedef struct egpu_context* egpu_handle;
+
+/* ---- handle ---- */
+/* One handle per host thread; it owns a stream, side streams for look-ahead
+ * and a device workspace.  Replaces the reference's global environment
+ * (elem::Initialize, core/environment_decl.hpp:16-38). */
+EGPU_API int egpu_create(egpu_handle* h, int device);
+EGPU_API int egpu_destroy(egpu_handle h);
+/* Use an external cudaStream_t (NULL restores the handle's own stream). */
+EGPU_API int egpu_set_stream(egpu_handle h, void* cuda_stream);
+EGPU_API void* egpu_get_stream(egpu_handle h);
+EGPU_API int egpu_synchronize(egpu_handle h);
+/* Algorithmic block size, default 128: elem::SetBlocksize / Blocksize
+ * (src/core/global.cpp:277-283; default at :194).  The GPU kernels use it as
+ * the panel width; values are rounded to an even number in [2, 128]. */
+EGPU_API int egpu_set_blocksize(egpu_handle h, int nb);
+EGPU_API int egpu_get_blocksize(egpu_handle h);
+EGPU_API const char* egpu_error_string(int code);
+/* Text of the last CUDA error seen by this thread (or ""). */
+EGPU_API const char* egpu_last_error_detail(void);
+/* Number of kernel launches issued by this library so far (process-wide). */
+EGPU_API long long egpu_launch_count(egpu_handle h);
+
+/* Launch tracing (the role of the reference's CallStackEntry/Timer,
+ * core/environment_decl.hpp:260-272, core/timer_decl.hpp:15-34): when on,
+ * every kernel launch issued through this handle is bracketed by CUDA events
+ * on its own stream.  Kinds: 0 trailing update (Gemm/Herk), 1 triangular
+ * multiply by an inverted diagonal block (Trsm), 2 diagonal-block kernels,
+ * 3 LU panel, 4 row interchanges, 5 other.  enable() clears the records;
+ * summary() waits for the recorded launches and sums their device time,
+ * algorithmic flops and algorithmic bytes. */
+EGPU_API int egpu_trace_enable(egpu_handle h, int on);
+EGPU_API int egpu_trace_summary(egpu_handle h, int kind, double* total_ms, double* total_flops,
+                                double* total_bytes, long long* launches);
+
+/* ---- device-memory API ---- */
+
+/* Cholesky(uplo, Matrix<F>& A), lapack-like/Cholesky.hpp:49-62 (blocked
+ * right-looking LVar3 / UVar3, Cholesky/LVar3.hpp:83-123,
+ * Cholesky/UVar3.hpp:85-125).  Only the uplo triangle is read and written. */
+EGPU_API int egpu_dpotrf(egpu_handle h, int uplo, int n, double* dA, int lda, int* info);
+
+/* cholesky::SolveAfter(uplo, orientation, A, B),
+ * lapack-like/Cholesky/SolveAfter.hpp:20-75. */
+EGPU_API int egpu_dpotrs(egpu_handle h, int uplo, int orient, int n, int nrhs, const double* dA, int lda, double* dB,
+                int ldb);
+
+/* HPDSolve(uplo, orientation, A, B), lapack-like/HPDSolve.hpp:18-28. */
+EGPU_API int egpu_dposv(egpu_handle h, int uplo, int orient, int n, int nrhs, double* dA, int lda, double* dB, int ldb,
+               int* info);
+
+/* LU(Matrix<F>& A, Matrix<int>& p), lapack-like/LU.hpp:144-218.
+ * dp: device int32[min(m,n)]. */
+EGPU_API int egpu_dgetrf(egpu_handle h, int m, int n, double* dA, int lda, int* dp, int* info);
+
+/* LU(Matrix<F>& A) without pivoting, lapack-like/LU.hpp:36-74. */
+EGPU_API int egpu_dgetrf_nopiv(egpu_handle h, int m, int n, double* dA, int lda, int* info);
+
+/* lu::SolveAfter(orientation, A, p, B), lapack-like/LU/SolveAfter.hpp:101-146;
+ * dp == NULL selects the unpivoted overload (:20-57). */
+EGPU_API int egpu_dgetrs(egpu_handle h, int orient, int n, int nrhs, const double* dA, int lda, const int* dp,
+                double* dB, int ldb);
+
+/* GaussianElimination(A, B), lapack-like/GaussianElimination.hpp:216-232. */
+EGPU_API int egpu_dgesv(egpu_handle h, int n, int nrhs, double* dA, int lda, double* dB, int ldb, int* info);
+
+/* Trsm(side, uplo, orientation, diag, alpha, A, B),
+ * blas-like/level3/Trsm.hpp:49-86 (dtrsm_ at src/core/imports/blas.cpp:1203). */
+EGPU_API int egpu_dtrsm(egpu_handle h, int side, int uplo, int orient, int diag, int m, int n, double alpha,
+               const double* dA, int lda, double* dB, int ldb);
+
+/* Trsv(uplo, orientation, diag, A, x), blas-like/level2/Trsv.hpp:20-44. */
+EGPU_API int egpu_dtrsv(egpu_handle h, int uplo, int orient, int diag, int n, const double* dA, int lda, double* dx);
+
+/* Gemm(orientA, orientB, alpha, A, B, beta, C), blas-like/level3/Gemm.hpp:158-211
+ * (dgemm_ at blas.cpp:930-941). */
+EGPU_API int egpu_dgemm(egpu_handle h, int orientA, int orientB, int m, int n, int k, double alpha, const double* dA,
+               int lda, const double* dB, int ldb, double beta, double* dC, int ldc);
+
+/* Herk(uplo, orientation, alpha, A, beta, C) for real F (= Syrk),
+ * blas-like/level3/Herk.hpp:17-27, Syrk.hpp:20-57 (dsyrk_ at blas.cpp:1043).
+ * orient NORMAL: C := alpha A A^T + beta C (A n x k); otherwise A^T A. */
+EGPU_API int egpu_dherk(egpu_handle h, int uplo, int orient, int n, int k, double alpha, const double* dA, int lda,
+               double beta, double* dC, int ldc);
+
+/* ApplyRowPivots(A, p) / ApplyInverseRowPivots(A, p),
+ * lapack-like/ApplyRowPivots.hpp:17-79 (sequential swaps i <-> p[i]). */
+EGPU_API int egpu_dlaswp(egpu_handle h, int inverse, int m, int n, double* dA, int lda, const int* dp, int npiv);
+
+/* ---- host-memory API (Matrix<F> buffers; synchronous) ---- */
+EGPU_API int egpu_host_dpotrf(egpu_handle h, int uplo, int n, double* A, int lda, int* info);
+EGPU_API int egpu_host_dpotrs(egpu_handle h, int uplo, int orient, int n, int nrhs, const double* A, int lda, double* B,
+                     int ldb);
+EGPU_API int egpu_host_dposv(egpu_handle h, int uplo, int orient, int n, int nrhs, double* A, int lda, double* B, int ldb,
+                    int* info);
+EGPU_API int egpu_host_dgetrf(egpu_handle h, int m, int n, double* A, int lda, int* p, int* info);
+EGPU_API int egpu_host_dgetrf_nopiv(egpu_handle h, int m, int n, double* A, int lda, int* info);
+EGPU_API int egpu_host_dgetrs(egpu_handle h, int orient, int n, int nrhs, const double* A, int lda, const int* p,
+                     double* B, int ldb);
+EGPU_API int egpu_host_dgesv(egpu_handle h, int n, int nrhs, double* A, int lda, double* B, int ldb, int* info);
+EGPU_API int egpu_host_dtrsm(egpu_handle h, int side, int uplo, int orient, int diag, int m, int n, double alpha,
+                    const double* A, int lda, double* B, int ldb);
+EGPU_API int egpu_host_dgemm(egpu_handle h, int orientA, int orientB, int m, int n, int k, double alpha, const double* A,
+                    int lda, const double* B, int ldb, double beta, double* C, int ldc);
+EGPU_API int egpu_host_dherk(egpu_handle h, int uplo, int orient, int n, int k, double alpha, const double* A, int lda,
+                    double beta, double* C, int ldc);
+EGPU_API int egpu_host_dlaswp(egpu_handle h, int inverse, int m, int n, double* A, int lda, const int* p, int npiv);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ELEMGPU_H */

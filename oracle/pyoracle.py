@@ -1,0 +1,209 @@
+"""ctypes front end of the CPU oracle (liboracle.so) -- TEST INFRASTRUCTURE ONLY.
+
+Only tests/, ``__graft_entry__.smoke()`` and bench.py's CPU-baseline leg import
+this module, and only as the checker.  Every routine mirrors an Elemental
+entry point (citations in oracle/oref_impl.h); matrices are numpy arrays in
+column-major (Fortran) order, indices are 0-based as in Elemental.
+
+Parity status: unpinned (the reference ships no golden vectors and cannot be
+built here); the oracle is cross-checked against LAPACK and exact
+constructions in tests/test_oracle.py.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = os.path.join(_HERE, "liboracle.so")
+_lib = None
+
+LOWER, UPPER = 0, 1
+NORMAL, TRANSPOSE, ADJOINT = 0, 1, 2
+
+
+def build() -> str:
+    """Compile liboracle.so with oracle/Makefile (idempotent)."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    return _LIB
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB) or (
+            os.path.getmtime(_LIB) < os.path.getmtime(os.path.join(_HERE, "oref_impl.h"))
+        ):
+            build()
+        _lib = ctypes.CDLL(_LIB)
+        _declare(_lib)
+    return _lib
+
+
+def _declare(L):
+    I, D, F, C = ctypes.c_int, ctypes.c_double, ctypes.c_float, ctypes.c_char
+    P = ctypes.c_void_p
+    for pfx, R in (("d", D), ("s", F)):
+        g = lambda n: getattr(L, f"oref_{pfx}{n}")  # noqa: E731
+        g("gemm").argtypes = [C, C, I, I, I, R, P, I, P, I, R, P, I]
+        g("syrk").argtypes = [C, C, I, I, R, P, I, R, P, I]
+        g("trsm").argtypes = [C, C, C, C, I, I, R, P, I, P, I]
+        g("trsv").argtypes = [C, C, C, I, P, I, P]
+        g("cholesky").argtypes = [I, I, P, I, I]
+        g("cholesky").restype = I
+        g("cholesky_solve_after").argtypes = [I, I, I, I, P, I, P, I]
+        g("hpd_solve").argtypes = [I, I, I, I, P, I, P, I, I]
+        g("hpd_solve").restype = I
+        g("compose_pivots").argtypes = [P, I, I, P, P]
+        g("apply_composed_pivots").argtypes = [I, I, P, I, I, P, P]
+        g("apply_row_pivots").argtypes = [I, I, P, I, P, I]
+        g("apply_inverse_row_pivots").argtypes = [I, I, P, I, P, I]
+        g("lu").argtypes = [I, I, P, I, P, I]
+        g("lu").restype = I
+        g("lu_nopiv").argtypes = [I, I, P, I, I]
+        g("lu_nopiv").restype = I
+        g("lu_solve_after").argtypes = [I, I, I, P, I, P, P, I]
+        g("gaussian_elimination").argtypes = [I, I, P, I, P, I, I]
+        g("gaussian_elimination").restype = I
+    L.oref_set_threads.argtypes = [I]
+    L.oref_get_threads.restype = I
+
+
+def set_threads(n: int) -> None:
+    lib().oref_set_threads(int(n))
+
+
+def get_threads() -> int:
+    return int(lib().oref_get_threads())
+
+
+def _pfx(a: np.ndarray) -> str:
+    if a.dtype == np.float64:
+        return "d"
+    if a.dtype == np.float32:
+        return "s"
+    raise TypeError(f"oracle supports float64/float32, got {a.dtype}")
+
+
+def _f(a, dtype=None):
+    a = np.asarray(a, dtype=dtype)
+    return np.require(a, requirements=["F", "A", "W"]) if a.ndim == 2 else np.require(a, requirements=["A", "W"])
+
+
+def _p(a):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def _ld(a):
+    return max(1, a.shape[0])
+
+
+def cholesky(A, uplo=LOWER, nb=128):
+    """Cholesky(uplo, A): returns (factored copy, status); status = 0 or the
+    1-based column where A stopped being numerically HPD."""
+    A = _f(A).copy(order="F")
+    n = A.shape[0]
+    st = getattr(lib(), f"oref_{_pfx(A)}cholesky")(uplo, n, _p(A), _ld(A), nb)
+    return A, int(st)
+
+
+def cholesky_solve_after(A, B, uplo=LOWER, orient=NORMAL):
+    B = _f(B).copy(order="F")
+    B2 = B.reshape(B.shape[0], -1, order="F")
+    getattr(lib(), f"oref_{_pfx(A)}cholesky_solve_after")(
+        uplo, orient, A.shape[0], B2.shape[1], _p(_f(A)), _ld(A), _p(B2), _ld(B2))
+    return B2.reshape(B.shape, order="F")
+
+
+def hpd_solve(A, B, uplo=LOWER, orient=NORMAL, nb=128):
+    A = _f(A).copy(order="F")
+    B = _f(B).copy(order="F")
+    B2 = B.reshape(B.shape[0], -1, order="F")
+    st = getattr(lib(), f"oref_{_pfx(A)}hpd_solve")(
+        uplo, orient, A.shape[0], B2.shape[1], _p(A), _ld(A), _p(B2), _ld(B2), nb)
+    return A, B2.reshape(B.shape, order="F"), int(st)
+
+
+def lu(A, nb=128):
+    """LU(A, p): returns (L\\U copy, p int32, status)."""
+    A = _f(A).copy(order="F")
+    m, n = A.shape
+    p = np.zeros(min(m, n), dtype=np.int32)
+    st = getattr(lib(), f"oref_{_pfx(A)}lu")(m, n, _p(A), _ld(A), _p(p), nb)
+    return A, p, int(st)
+
+
+def lu_nopiv(A, nb=128):
+    A = _f(A).copy(order="F")
+    m, n = A.shape
+    st = getattr(lib(), f"oref_{_pfx(A)}lu_nopiv")(m, n, _p(A), _ld(A), nb)
+    return A, int(st)
+
+
+def lu_solve_after(A, p, B, orient=NORMAL):
+    B = _f(B).copy(order="F")
+    B2 = B.reshape(B.shape[0], -1, order="F")
+    pp = None if p is None else np.ascontiguousarray(p, dtype=np.int32)
+    getattr(lib(), f"oref_{_pfx(A)}lu_solve_after")(
+        orient, A.shape[0], B2.shape[1], _p(_f(A)), _ld(A),
+        None if pp is None else _p(pp), _p(B2), _ld(B2))
+    return B2.reshape(B.shape, order="F")
+
+
+def gaussian_elimination(A, B, nb=128):
+    A = _f(A).copy(order="F")
+    B = _f(B).copy(order="F")
+    B2 = B.reshape(B.shape[0], -1, order="F")
+    st = getattr(lib(), f"oref_{_pfx(A)}gaussian_elimination")(
+        A.shape[0], B2.shape[1], _p(A), _ld(A), _p(B2), _ld(B2), nb)
+    return A, B2.reshape(B.shape, order="F"), int(st)
+
+
+def apply_row_pivots(B, p, inverse=False):
+    B = _f(B).copy(order="F")
+    B2 = B.reshape(B.shape[0], -1, order="F")
+    pp = np.ascontiguousarray(p, dtype=np.int32)
+    name = "apply_inverse_row_pivots" if inverse else "apply_row_pivots"
+    getattr(lib(), f"oref_{_pfx(B)}{name}")(B2.shape[0], B2.shape[1], _p(B2), _ld(B2), _p(pp), len(pp))
+    return B2.reshape(B.shape, order="F")
+
+
+def compose_pivots(p, offset):
+    pp = np.ascontiguousarray(p, dtype=np.int32)
+    b = len(pp)
+    image = np.zeros(b, np.int32)
+    pre = np.zeros(b, np.int32)
+    lib().oref_dcompose_pivots(_p(pp), b, offset, _p(image), _p(pre))
+    return image, pre
+
+
+def trsm(side, uplo, orient, diag, alpha, A, B):
+    """Trsm(side, uplo, orientation, diag, alpha, A, B) with Elemental's
+    character mapping (blas-like/level3/Trsm.hpp:49-86)."""
+    B = _f(B).copy(order="F")
+    m, n = B.shape
+    getattr(lib(), f"oref_{_pfx(B)}trsm")(
+        side.encode(), uplo.encode(), orient.encode(), diag.encode(), m, n,
+        alpha, _p(_f(A)), _ld(A), _p(B), _ld(B))
+    return B
+
+
+def gemm(ta, tb, alpha, A, B, beta, C):
+    C = _f(C).copy(order="F")
+    m, n = C.shape
+    k = A.shape[1] if ta == "N" else A.shape[0]
+    getattr(lib(), f"oref_{_pfx(C)}gemm")(
+        ta.encode(), tb.encode(), m, n, k, alpha, _p(_f(A)), _ld(A), _p(_f(B)), _ld(B), beta, _p(C), _ld(C))
+    return C
+
+
+def syrk(uplo, trans, alpha, A, beta, C):
+    C = _f(C).copy(order="F")
+    n = C.shape[0]
+    k = A.shape[1] if trans == "N" else A.shape[0]
+    getattr(lib(), f"oref_{_pfx(C)}syrk")(
+        uplo.encode(), trans.encode(), n, k, alpha, _p(_f(A)), _ld(A), beta, _p(C), _ld(C))
+    return C

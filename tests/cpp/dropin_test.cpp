@@ -1,0 +1,169 @@
+// Drop-in check written the way the reference's own drivers are
+// (tests/lapack-like/Cholesky.cpp, tests/lapack-like/SequentialLU.cpp):
+// factor with elem::Cholesky / elem::LU, then apply the factors to a block of
+// random vectors and compare against A X.  Exercises Matrix<F> views with
+// LDim > Height, the Blocksize stack, DistMatrix on a 1 x 1 Grid, float and
+// double, and the exception mapping.  Prints one line per check and exits
+// non-zero on the first failure.
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <random>
+
+#include "elemgpu/elemental.hpp"
+
+using namespace elem;
+
+static std::mt19937_64 gen(12345);
+
+template <typename F>
+void Uniform(Matrix<F>& A, int m, int n) {  // U[-1,1], like matrices/Uniform.hpp
+  A.ResizeTo(m, n);
+  std::uniform_real_distribution<double> u(-1.0, 1.0);
+  for (int j = 0; j < n; ++j)
+    for (int i = 0; i < m; ++i) A.Set(i, j, (F)u(gen));
+}
+
+template <typename F>
+double MaxAbs(const Matrix<F>& A) {
+  double r = 0;
+  for (int j = 0; j < A.Width(); ++j)
+    for (int i = 0; i < A.Height(); ++i) r = std::max(r, std::fabs((double)A.Get(i, j)));
+  return r;
+}
+
+static int failures = 0;
+static void Check(bool ok, const char* what, double value) {
+  std::printf("%-48s %s  (%.3e)\n", what, ok ? "ok" : "FAIL", value);
+  if (!ok) ++failures;
+}
+
+template <typename F>
+void TestCholesky(UpperOrLower uplo, int m, double tol) {
+  // HPD A = G G^T + m I
+  Matrix<F> G, A(m, m), X, Y(m, 100), Z(m, 100);
+  Uniform(G, m, m);
+  Gemm(NORMAL, TRANSPOSE, F(1), G, G, F(0), A);
+  for (int i = 0; i < m; ++i) A.Update(i, i, F(m));
+  Uniform(X, m, 100);
+  Gemm(NORMAL, NORMAL, F(1), A, X, F(0), Y);  // Y = A X
+  Matrix<F> L(A);
+  Cholesky(uplo, L);
+  // Z = L L^H X (or U^H U X) applied with triangular products built from L
+  Matrix<F> T(m, m);
+  for (int j = 0; j < m; ++j)
+    for (int i = 0; i < m; ++i) {
+      const bool in = uplo == LOWER ? i >= j : i <= j;
+      T.Set(i, j, in ? L.Get(i, j) : F(0));
+    }
+  Matrix<F> W(m, 100);
+  if (uplo == LOWER) {
+    Gemm(TRANSPOSE, NORMAL, F(1), T, X, F(0), W);
+    Gemm(NORMAL, NORMAL, F(1), T, W, F(0), Z);
+  } else {
+    Gemm(NORMAL, NORMAL, F(1), T, X, F(0), W);
+    Gemm(TRANSPOSE, NORMAL, F(1), T, W, F(0), Z);
+  }
+  double err = 0;
+  for (int j = 0; j < 100; ++j)
+    for (int i = 0; i < m; ++i) err = std::max(err, std::fabs((double)(Y.Get(i, j) - Z.Get(i, j))));
+  Check(err / MaxAbs(Y) < tol, uplo == LOWER ? "Cholesky(LOWER) ||AX - LL^H X|| / ||AX||" : "Cholesky(UPPER)", err / MaxAbs(Y));
+  // HPDSolve on the same A recovers X
+  Matrix<F> A2(A), B(Y);
+  HPDSolve(uplo, NORMAL, A2, B);
+  double e2 = 0;
+  for (int j = 0; j < 100; ++j)
+    for (int i = 0; i < m; ++i) e2 = std::max(e2, std::fabs((double)(B.Get(i, j) - X.Get(i, j))));
+  Check(e2 < tol * 10, "HPDSolve recovers X", e2);
+}
+
+template <typename F>
+void TestLU(int m, double tol) {
+  Matrix<F> A, X, Y(m, 100);
+  Uniform(A, m, m);
+  Uniform(X, m, 100);
+  Gemm(NORMAL, NORMAL, F(1), A, X, F(0), Y);
+  Matrix<F> LU_(A);
+  Matrix<int> p;
+  LU(LU_, p);
+  Check(p.Height() == m && p.Width() == 1, "LU resizes p to min(m,n) x 1", p.Height());
+  Matrix<F> B(Y);
+  lu::SolveAfter(NORMAL, LU_, p, B);
+  double e = 0;
+  for (int j = 0; j < 100; ++j)
+    for (int i = 0; i < m; ++i) e = std::max(e, std::fabs((double)(B.Get(i, j) - X.Get(i, j))));
+  Check(e < tol * m, "LU + lu::SolveAfter recovers X", e);
+  Matrix<F> A3(A), B3(Y);
+  GaussianElimination(A3, B3);
+  double e3 = 0;
+  for (int j = 0; j < 100; ++j)
+    for (int i = 0; i < m; ++i) e3 = std::max(e3, std::fabs((double)(B3.Get(i, j) - X.Get(i, j))));
+  Check(e3 < tol * m, "GaussianElimination recovers X", e3);
+}
+
+int main(int argc, char** argv) {
+  Initialize(argc, argv);
+  PushBlocksizeStack(96);
+  TestCholesky<double>(LOWER, 500, 1e-12);
+  TestCholesky<double>(UPPER, 333, 1e-12);
+  PopBlocksizeStack();
+  TestCholesky<float>(LOWER, 200, 1e-5);
+  TestLU<double>(700, 1e-12);
+  TestLU<float>(150, 1e-5);
+
+  // A view with LDim > Height: factor the leading 300 x 300 block in place.
+  {
+    Matrix<double> big(400, 400);
+    Matrix<double> G;
+    Uniform(G, 300, 300);
+    Matrix<double> view;
+    View(view, big, 50, 60, 300, 300);
+    Gemm(NORMAL, TRANSPOSE, 1.0, G, G, 0.0, view);
+    for (int i = 0; i < 300; ++i) view.Update(i, i, 300.0);
+    Matrix<double> copy(view);
+    Cholesky(LOWER, view);
+    Cholesky(LOWER, copy);
+    double d = 0;
+    for (int j = 0; j < 300; ++j)
+      for (int i = j; i < 300; ++i) d = std::max(d, std::fabs(view.Get(i, j) - copy.Get(i, j)));
+    Check(d == 0.0 && big.Get(0, 0) == 0.0 && big.Get(49, 60) == 0.0, "Cholesky on a view (LDim 400)", d);
+  }
+
+  // DistMatrix over a 1 x 1 Grid delegates to the sequential path.
+  {
+    Grid g;
+    DistMatrix<double> A(g), B(g);
+    Uniform(A.Matrix(), 256, 256);
+    for (int i = 0; i < 256; ++i) A.Matrix().Update(i, i, 256.0);
+    Uniform(B.Matrix(), 256, 4);
+    DistMatrix<double> A0(A), B0(B);
+    DistMatrix<int, VC, STAR> p(g);
+    LU(A, p);
+    lu::SolveAfter(NORMAL, A, p, B);
+    Matrix<double> R(256, 4);
+    Gemm(NORMAL, NORMAL, 1.0, A0.LockedMatrix(), B.LockedMatrix(), 0.0, R);
+    double e = 0;
+    for (int j = 0; j < 4; ++j)
+      for (int i = 0; i < 256; ++i) e = std::max(e, std::fabs(R.Get(i, j) - B0.Get(i, j)));
+    Check(e < 1e-11, "DistMatrix 1x1 LU + SolveAfter", e);
+  }
+
+  // Exceptions: non-HPD -> std::logic_error, exact zero pivot -> SingularMatrixException
+  {
+    Matrix<double> A(50, 50);
+    for (int i = 0; i < 50; ++i) A.Set(i, i, i == 30 ? -1.0 : 2.0);
+    bool caught = false;
+    try { Cholesky(LOWER, A); } catch (std::logic_error& e) { caught = std::string(e.what()) == "A was not numerically HPD"; }
+    Check(caught, "Cholesky throws logic_error on non-HPD input", 0);
+    Matrix<double> S;
+    Uniform(S, 40, 40);
+    for (int i = 0; i < 40; ++i) S.Set(i, 7, 0.0);
+    Matrix<int> p;
+    caught = false;
+    try { LU(S, p); } catch (SingularMatrixException&) { caught = true; }
+    Check(caught, "LU throws SingularMatrixException", 0);
+  }
+  Finalize();
+  std::printf("%s\n", failures ? "FAILED" : "PASSED");
+  return failures ? 1 : 0;
+}
