@@ -90,6 +90,10 @@ def _declare(L):
         "egpu_synchronize": ([H], I),
         "egpu_set_blocksize": ([H, I], I),
         "egpu_get_blocksize": ([H], I),
+        "egpu_set_lookahead": ([H, I], I),
+        "egpu_set_async": ([H, I], I),
+        "egpu_get_status": ([H, P], I),
+        "egpu_reserve": ([H, ctypes.c_size_t], I),
         "egpu_error_string": ([I], ctypes.c_char_p),
         "egpu_last_error_detail": ([], ctypes.c_char_p),
         "egpu_launch_count": ([H], LL),
@@ -227,6 +231,8 @@ class Handle:
         # ordered after the torch ops that produced their inputs.
         import torch
         s = torch.cuda.current_stream(self.device).cuda_stream
+        if s == 0:
+            s = 1  # torch's default is the legacy stream (cudaStreamLegacy == 0x1)
         if s != getattr(self, "_bound", None):
             _check(lib().egpu_set_stream(self._h, ctypes.c_void_p(s)))
             self._bound = s
@@ -236,6 +242,22 @@ class Handle:
 
     def blocksize(self) -> int:
         return lib().egpu_get_blocksize(self._h)
+
+    def set_async(self, on: bool):
+        """Device API only enqueues; failures are kept for get_status()."""
+        _check(lib().egpu_set_async(self._h, int(on)))
+
+    def get_status(self):
+        """Wait for the handle's work; raise the first failure (and clear it)."""
+        info = ctypes.c_int(0)
+        _check(lib().egpu_get_status(self._h, ctypes.byref(info)), info.value)
+
+    def reserve(self, nbytes: int):
+        _check(lib().egpu_reserve(self._h, int(nbytes)))
+
+    def set_lookahead(self, depth: int):
+        """0: one stream, steps in order; 1 (default): panel k+1 overlaps update k."""
+        _check(lib().egpu_set_lookahead(self._h, depth))
 
     def set_stream(self, stream_ptr: int | None):
         _check(lib().egpu_set_stream(self._h, ctypes.c_void_p(stream_ptr or 0)))

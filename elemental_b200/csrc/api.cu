@@ -88,6 +88,13 @@ struct egpu_context {
   void* stage[3] = {nullptr, nullptr, nullptr};
   size_t stage_bytes[3] = {0, 0, 0};
   Trace trace;
+  // look-ahead: a high-priority side stream for the panel chain and events
+  // joining it with the update chain on `stream`
+  cudaStream_t side = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  cudaEvent_t ev_panel[2] = {nullptr, nullptr}, ev_rest[2] = {nullptr, nullptr};
+  int lookahead = 1;
+  int async = 0;  // device API: enqueue only; status read by egpu_get_status
 };
 
 namespace {
@@ -152,6 +159,14 @@ struct Enter {
   ~Enter() { t_trace = prev; }
 };
 
+// Host-memory entry points are synchronous whatever the handle's mode.
+struct SyncScope {
+  egpu_context* h;
+  int saved;
+  explicit SyncScope(egpu_context* hh) : h(hh), saved(hh->async) { hh->async = 0; }
+  ~SyncScope() { h->async = saved; }
+};
+
 inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 inline long long ld_aligned(int rows) { return std::max<long long>(32, align_up((size_t)std::max(rows, 1), 32)); }
 
@@ -170,11 +185,12 @@ struct Carve {
 };
 
 int reset_status(egpu_context* h) {
+  if (h->async) return EGPU_OK;  // async: the first failure stays until egpu_get_status
   EGPU_CUDA_TRY(cudaMemsetAsync(h->dstatus, 0, sizeof(DevStatus), h->stream));
   return EGPU_OK;
 }
 
-int read_status(egpu_context* h, int* info) {
+int read_status_now(egpu_context* h, int* info) {
   EGPU_CUDA_TRY(cudaMemcpyAsync(h->hstatus, h->dstatus, sizeof(DevStatus), cudaMemcpyDeviceToHost, h->stream));
   EGPU_CUDA_TRY(cudaStreamSynchronize(h->stream));
   if (info) *info = h->hstatus->code ? h->hstatus->info : 0;
@@ -184,6 +200,15 @@ int read_status(egpu_context* h, int* info) {
     case kSingular: return EGPU_SINGULAR;
     default: return EGPU_TIMEOUT;
   }
+}
+
+// Synchronous mode: wait and map the status.  Async mode: return at once.
+int read_status(egpu_context* h, int* info) {
+  if (h->async) {
+    if (info) *info = 0;
+    return EGPU_OK;
+  }
+  return read_status_now(h, info);
 }
 
 #define TRY(x)               \
@@ -279,12 +304,12 @@ size_t winv_bytes(int nt, int nb) { return sizeof(double) * (size_t)((nt + nb - 
 
 // ----- core device drivers on TMA-compatible operands -----
 
-int potrf_core(egpu_context* h, int uplo, int n, double* A, long long lda) {
+// Sequential blocked right-looking Cholesky: per block column, potrf of the
+// diagonal block (+ its inverse), the panel Trsm as a multiply by that
+// inverse, and the Herk trailing update (LVar3.hpp:83-123 / UVar3.hpp:85-125).
+int potrf_seq(egpu_context* h, int uplo, int n, double* A, long long lda, double* W) {
   const int nb = h->nb;
   cudaStream_t st = h->stream;
-  TRY(ensure_ws(h, sizeof(double) * (size_t)nb * nb + 4096));
-  Carve cv(h->ws);
-  double* W = cv.take<double>((size_t)nb * nb);
   for (int k = 0; k < n; k += nb) {
     const int b = std::min(nb, n - k);
     const int m2 = n - k - b;
@@ -310,37 +335,169 @@ int potrf_core(egpu_context* h, int uplo, int n, double* A, long long lda) {
   return EGPU_OK;
 }
 
-int getrf_core(egpu_context* h, int m, int n, double* A, long long lda, int* dp) {
+// The Herk update of step k restricted to the trailing block columns
+// [c0, c1) (lower) or block rows [c0, c1) (upper).  Rows/cols are global.
+int potrf_update_cols(egpu_context* h, cudaStream_t st, int uplo, int n, double* A, long long lda, int k, int b,
+                      int c0, int c1) {
+  if (c1 <= c0) return EGPU_OK;
+  if (uplo == EGPU_LOWER) {
+    // A[c0:n, c0:c1] -= A[c0:n, k:k+b] * A[c0:c1, k:k+b]^T   (lower part)
+    return launch_dgemm(st, false, false, n - c0, c1 - c0, b, -1.0, A + c0 + (size_t)k * lda, lda,
+                        A + c0 + (size_t)k * lda, lda, 1.0, A + c0 + (size_t)c0 * lda, lda, 1, false, h->dstatus);
+  }
+  // A[c0:c1, c0:n] -= A[k:k+b, c0:c1]^T * A[k:k+b, c0:n]   (upper part)
+  return launch_dgemm(st, true, true, c1 - c0, n - c0, b, -1.0, A + k + (size_t)c0 * lda, lda,
+                      A + k + (size_t)c0 * lda, lda, 1.0, A + c0 + (size_t)c0 * lda, lda, 2, false, h->dstatus);
+}
+
+// The diagonal-block factorization and panel Trsm of step k.
+int potrf_panel(egpu_context* h, cudaStream_t st, int uplo, int n, double* A, long long lda, int k, int b,
+                double* W) {
   const int nb = h->nb;
-  const int mn = std::min(m, n);
-  cudaStream_t st = h->stream;
-  const size_t panel_bytes = lu_panel_scratch_bytes(m, nb, h->sm_count);
-  TRY(ensure_ws(h, sizeof(double) * (size_t)nb * nb + 2 * sizeof(int) * nb + panel_bytes + 4096));
+  const int m2 = n - k - b;
+  TRY(launch_potrf_diag(st, uplo, A + k + (size_t)k * lda, lda, b, W, nb, h->dstatus, k));
+  if (m2 == 0) return EGPU_OK;
+  if (uplo == EGPU_LOWER) {
+    double* A21 = A + (k + b) + (size_t)k * lda;
+    return launch_dgemm(st, false, false, m2, b, b, 1.0, A21, lda, W, nb, 0.0, A21, lda, 0, true, h->dstatus);
+  }
+  double* A12 = A + k + (size_t)(k + b) * lda;
+  return launch_dgemm(st, true, true, b, m2, b, 1.0, W, nb, A12, lda, 0.0, A12, lda, 0, false, h->dstatus);
+}
+
+// Look-ahead depth 1: the panel of step k+1 (update of block column k+1 by
+// step k, diagonal factorization, panel Trsm) runs on a high-priority side
+// stream while the rest of step k's trailing update runs on the main stream.
+//   side:  [upd(k -> col k+1)] [potrf k+1] [trsm k+1] -> ev_panel
+//   main:  wait ev_panel(k) -> [upd(k -> cols >= k+2)] -> ev_rest
+// The side stream waits for ev_rest(k-1) before touching column k+1, which
+// step k-1's main-stream update also wrote.
+int potrf_lookahead(egpu_context* h, int uplo, int n, double* A, long long lda, double* W) {
+  const int nb = h->nb;
+  const int nblk = (n + nb - 1) / nb;
+  cudaStream_t M = h->stream, P = h->side;
+  EGPU_CUDA_TRY(cudaEventRecord(h->ev_fork, M));
+  EGPU_CUDA_TRY(cudaStreamWaitEvent(P, h->ev_fork, 0));
+  TRY(potrf_panel(h, P, uplo, n, A, lda, 0, std::min(nb, n), W));
+  EGPU_CUDA_TRY(cudaEventRecord(h->ev_panel[0], P));
+  for (int kb = 0; kb < nblk; ++kb) {
+    const int k = kb * nb, b = std::min(nb, n - k);
+    const int c1 = k + b, c2 = std::min(n, c1 + nb);
+    if (kb + 1 < nblk) {
+      if (kb >= 1) EGPU_CUDA_TRY(cudaStreamWaitEvent(P, h->ev_rest[(kb - 1) & 1], 0));
+      TRY(potrf_update_cols(h, P, uplo, n, A, lda, k, b, c1, c2));
+      TRY(potrf_panel(h, P, uplo, n, A, lda, c1, c2 - c1, W));
+      EGPU_CUDA_TRY(cudaEventRecord(h->ev_panel[(kb + 1) & 1], P));
+    }
+    EGPU_CUDA_TRY(cudaStreamWaitEvent(M, h->ev_panel[kb & 1], 0));
+    TRY(potrf_update_cols(h, M, uplo, n, A, lda, k, b, c2, n));
+    EGPU_CUDA_TRY(cudaEventRecord(h->ev_rest[kb & 1], M));
+  }
+  EGPU_CUDA_TRY(cudaEventRecord(h->ev_join, P));
+  EGPU_CUDA_TRY(cudaStreamWaitEvent(M, h->ev_join, 0));
+  return EGPU_OK;
+}
+
+int potrf_core(egpu_context* h, int uplo, int n, double* A, long long lda) {
+  const int nb = h->nb;
+  TRY(ensure_ws(h, sizeof(double) * (size_t)nb * nb + 4096));
   Carve cv(h->ws);
   double* W = cv.take<double>((size_t)nb * nb);
-  int* image = cv.take<int>(nb);
-  int* preimage = cv.take<int>(nb);
+  if (h->lookahead && n > nb) return potrf_lookahead(h, uplo, n, A, lda, W);
+  return potrf_seq(h, uplo, n, A, lda, W);
+}
+
+// Step k of LU after its panel: pivots applied to the block columns [c0, c1)
+// (global columns, rows k..m), then the row-panel Trsm (multiply by
+// inv(L11)) and the Gemm trailing update of those columns (LU.hpp:198-203).
+int getrf_update_cols(egpu_context* h, cudaStream_t st, int m, double* A, long long lda, int k, int b,
+                      const double* W, const int* image, const int* preimage, int c0, int c1) {
+  if (c1 <= c0) return EGPU_OK;
+  const int mr = m - k, nc = c1 - c0;
+  TRY(launch_apply_composed(st, mr, nc, A + k + (size_t)c0 * lda, lda, b, image, preimage, h->dstatus));
+  double* A12 = A + k + (size_t)c0 * lda;
+  TRY(launch_dgemm(st, false, true, b, nc, b, 1.0, W, h->nb, A12, lda, 0.0, A12, lda, 0, false, h->dstatus));
+  if (mr - b > 0)
+    TRY(launch_dgemm(st, false, true, mr - b, nc, b, -1.0, A + (k + b) + (size_t)k * lda, lda, A12, lda, 1.0,
+                     A + (k + b) + (size_t)c0 * lda, lda, 0, false, h->dstatus));
+  return EGPU_OK;
+}
+
+// Blocked right-looking LU with partial pivoting (LU.hpp:144-218).
+// With B != nullptr the n x nrhs block B is carried along as extra trailing
+// columns (pivots, row-panel solve and Gemm update applied to it each step),
+// which is RowEchelon (GaussianElimination.hpp:94-209); pivot_left = false
+// then leaves the already-factored L columns unpermuted, as RowEchelon does.
+int getrf_core(egpu_context* h, int m, int n, double* A, long long lda, int* dp, double* B = nullptr,
+               long long ldb = 0, int nrhs = 0, bool pivot_left = true) {
+  const int nb = h->nb;
+  const int mn = std::min(m, n);
+  const int nblk = (mn + nb - 1) / nb;
+  const size_t panel_bytes = lu_panel_scratch_bytes(m, nb, h->sm_count);
+  TRY(ensure_ws(h, 2 * (sizeof(double) * (size_t)nb * nb + 2 * sizeof(int) * nb + 512) + panel_bytes + 4096));
+  Carve cv(h->ws);
+  double* W[2];
+  int *image[2], *preimage[2];
+  for (int i = 0; i < 2; ++i) {
+    W[i] = cv.take<double>((size_t)nb * nb);
+    image[i] = cv.take<int>(nb);
+    preimage[i] = cv.take<int>(nb);
+  }
   void* pscr = cv.take<unsigned char>(panel_bytes);
-  for (int k = 0; k < mn; k += nb) {
-    const int b = std::min(nb, mn - k);
-    const int mr = m - k, nr = n - k - b;
-    double* ABRL = A + k + (size_t)k * lda;
-    TRY(launch_lu_panel(st, mr, b, ABRL, lda, dp + k, k, image, preimage, W, nb, pscr, h->dstatus, h->sm_count));
-    // ApplyRowPivots(ABL, image, preimage); ApplyRowPivots(ABRR, image, preimage)   (LU.hpp:198-199)
-    TRY(launch_apply_composed(st, mr, k, A + k, lda, b, image, preimage, h->dstatus));
-    TRY(launch_apply_composed(st, mr, nr, A + k + (size_t)(k + b) * lda, lda, b, image, preimage, h->dstatus));
-    if (nr > 0) {
-      double* A12 = A + k + (size_t)(k + b) * lda;
-      // Trsm(LEFT, LOWER, NORMAL, UNIT, 1, A11, A12): A12 := inv(L11) * A12
-      TRY(launch_dgemm(st, false, true, b, nr, b, 1.0, W, nb, A12, lda, 0.0, A12, lda, 0, false, h->dstatus));
-      if (mr - b > 0) {
-        double* A21 = A + (k + b) + (size_t)k * lda;
-        double* A22 = A + (k + b) + (size_t)(k + b) * lda;
-        // Gemm(NORMAL, NORMAL, -1, A21, A12, 1, A22)
-        TRY(launch_dgemm(st, false, true, mr - b, nr, b, -1.0, A21, lda, A12, lda, 1.0, A22, lda, 0, false,
-                         h->dstatus));
-      }
+  const bool la = h->lookahead && nblk > 1;
+  cudaStream_t M = h->stream, P = la ? h->side : h->stream;
+  auto rest = [&](cudaStream_t st, int k, int b, int s, int c0) -> int {
+    if (pivot_left) TRY(launch_apply_composed(st, m - k, k, A + k, lda, b, image[s], preimage[s], h->dstatus));
+    TRY(getrf_update_cols(h, st, m, A, lda, k, b, W[s], image[s], preimage[s], c0, n));
+    if (B != nullptr && nrhs > 0) {  // B rides along as columns n .. n + nrhs
+      const int mr = m - k;
+      double* B1 = B + k;
+      TRY(launch_apply_composed(st, mr, nrhs, B1, ldb, b, image[s], preimage[s], h->dstatus));
+      TRY(launch_dgemm(st, false, true, b, nrhs, b, 1.0, W[s], nb, B1, ldb, 0.0, B1, ldb, 0, false, h->dstatus));
+      if (mr - b > 0)
+        TRY(launch_dgemm(st, false, true, mr - b, nrhs, b, -1.0, A + (k + b) + (size_t)k * lda, lda, B1, ldb, 1.0,
+                         B + k + b, ldb, 0, false, h->dstatus));
     }
+    return EGPU_OK;
+  };
+  if (la) {
+    EGPU_CUDA_TRY(cudaEventRecord(h->ev_fork, M));
+    EGPU_CUDA_TRY(cudaStreamWaitEvent(P, h->ev_fork, 0));
+  }
+  TRY(launch_lu_panel(P, m, std::min(nb, mn), A, lda, dp, 0, image[0], preimage[0], W[0], nb, pscr, h->dstatus,
+                      h->sm_count));
+  if (la) EGPU_CUDA_TRY(cudaEventRecord(h->ev_panel[0], P));
+  for (int kb = 0; kb < nblk; ++kb) {
+    const int k = kb * nb, b = std::min(nb, mn - k), s = kb & 1;
+    const int c1 = k + b;                 // first column right of the panel
+    const int c2 = std::min(n, c1 + nb);  // end of the next block column
+    if (!la) {
+      TRY(rest(M, k, b, s, c1));
+      if (kb + 1 < nblk) {
+        const int k1 = c1, b1 = std::min(nb, mn - k1);
+        TRY(launch_lu_panel(M, m - k1, b1, A + k1 + (size_t)k1 * lda, lda, dp + k1, k1, image[s ^ 1],
+                            preimage[s ^ 1], W[s ^ 1], nb, pscr, h->dstatus, h->sm_count));
+      }
+      continue;
+    }
+    if (kb + 1 < nblk) {
+      // side stream: bring block column kb+1 up to date, then factor it
+      if (kb >= 1) EGPU_CUDA_TRY(cudaStreamWaitEvent(P, h->ev_rest[(kb - 1) & 1], 0));
+      TRY(getrf_update_cols(h, P, m, A, lda, k, b, W[s], image[s], preimage[s], c1, c2));
+      const int k1 = c1, b1 = std::min(nb, mn - k1);
+      TRY(launch_lu_panel(P, m - k1, b1, A + k1 + (size_t)k1 * lda, lda, dp + k1, k1, image[s ^ 1],
+                          preimage[s ^ 1], W[s ^ 1], nb, pscr, h->dstatus, h->sm_count));
+      EGPU_CUDA_TRY(cudaEventRecord(h->ev_panel[(kb + 1) & 1], P));
+    }
+    // main stream: pivots on the left columns and the rest of the update
+    // (after the last panel nothing ran on the side stream: start at c1)
+    EGPU_CUDA_TRY(cudaStreamWaitEvent(M, h->ev_panel[s], 0));
+    TRY(rest(M, k, b, s, kb + 1 < nblk ? c2 : c1));
+    EGPU_CUDA_TRY(cudaEventRecord(h->ev_rest[s], M));
+  }
+  if (la) {
+    EGPU_CUDA_TRY(cudaEventRecord(h->ev_join, P));
+    EGPU_CUDA_TRY(cudaStreamWaitEvent(M, h->ev_join, 0));
   }
   return EGPU_OK;
 }
@@ -422,45 +579,19 @@ int potrs_core(egpu_context* h, int uplo, int n, int nrhs, const double* A, long
   return EGPU_OK;
 }
 
-// RowEchelon + upper solve (GaussianElimination.hpp:94-209, 216-232): LU
-// with partial pivoting whose pivots are also applied to B and whose L is
-// applied to B on the fly; then B := inv(U) B.
+// GaussianElimination (GaussianElimination.hpp:216-232): RowEchelon -- LU
+// with partial pivoting with B carried along as trailing columns and the
+// L columns left unpermuted (the distributed RowEchelon, :94-209, which a
+// 1 x 1 grid runs) -- then B := inv(U) B.
 int gesv_core(egpu_context* h, int n, int nrhs, double* A, long long lda, double* B, long long ldb) {
-  const int nb = h->nb;
-  cudaStream_t st = h->stream;
-  const size_t panel_bytes = lu_panel_scratch_bytes(n, nb, h->sm_count);
-  const size_t need = sizeof(double) * (size_t)nb * nb + 2 * sizeof(int) * nb + sizeof(int) * nb + panel_bytes;
-  TRY(ensure_ws(h, std::max(need, winv_bytes(n, nb)) + 8192));
-  {
-    Carve cv(h->ws);
-    double* W = cv.take<double>((size_t)nb * nb);
-    int* image = cv.take<int>(nb);
-    int* preimage = cv.take<int>(nb);
-    int* p1 = cv.take<int>(nb);
-    void* pscr = cv.take<unsigned char>(panel_bytes);
-    for (int k = 0; k < n; k += nb) {
-      const int b = std::min(nb, n - k);
-      const int mr = n - k, nr = n - k - b;
-      double* A11 = A + k + (size_t)k * lda;
-      TRY(launch_lu_panel(st, mr, b, A11, lda, p1, k, image, preimage, W, nb, pscr, h->dstatus, h->sm_count));
-      double* A12 = A + k + (size_t)(k + b) * lda;
-      TRY(launch_apply_composed(st, mr, nr, A12, lda, b, image, preimage, h->dstatus));
-      TRY(launch_apply_composed(st, mr, nrhs, B + k, ldb, b, image, preimage, h->dstatus));
-      double* B1 = B + k;
-      if (nr > 0) TRY(launch_dgemm(st, false, true, b, nr, b, 1.0, W, nb, A12, lda, 0.0, A12, lda, 0, false, h->dstatus));
-      TRY(launch_dgemm(st, false, true, b, nrhs, b, 1.0, W, nb, B1, ldb, 0.0, B1, ldb, 0, false, h->dstatus));
-      if (nr > 0) {
-        double* A21 = A + (k + b) + (size_t)k * lda;
-        double* A22 = A + (k + b) + (size_t)(k + b) * lda;
-        TRY(launch_dgemm(st, false, true, nr, nr, b, -1.0, A21, lda, A12, lda, 1.0, A22, lda, 0, false, h->dstatus));
-        TRY(launch_dgemm(st, false, true, nr, nrhs, b, -1.0, A21, lda, B1, ldb, 1.0, B + k + b, ldb, 0, false,
-                         h->dstatus));
-      }
-    }
-  }
+  // pivots of RowEchelon are not returned; keep them in a staging slot
+  if (ensure_stage(h, 2, sizeof(int) * (size_t)std::max(n, 1)) != EGPU_OK) return EGPU_ERR_ALLOC;
+  int* p = static_cast<int*>(h->stage[2]);
+  TRY(getrf_core(h, n, n, A, lda, p, B, ldb, nrhs, false));
   int info = 0;
   int rc = read_status(h, &info);
   if (rc != EGPU_OK) return rc;
+  if (nrhs == 0) return EGPU_OK;
   return trsm_core(h, EGPU_LEFT, EGPU_UPPER, 0, 0, n, nrhs, 1.0, A, lda, B, ldb);
 }
 
@@ -520,6 +651,22 @@ int egpu_create(egpu_handle* out, int device) {
     return EGPU_ERR_CUDA;
   }
   h->stream = h->own_stream;
+  {
+    int lo = 0, hi = 0;
+    cudaDeviceGetStreamPriorityRange(&lo, &hi);  // hi = greatest priority
+    bool ok = cudaStreamCreateWithPriority(&h->side, cudaStreamNonBlocking, hi) == cudaSuccess;
+    ok = ok && cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming) == cudaSuccess;
+    ok = ok && cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming) == cudaSuccess;
+    for (int i = 0; i < 2; ++i) {
+      ok = ok && cudaEventCreateWithFlags(&h->ev_panel[i], cudaEventDisableTiming) == cudaSuccess;
+      ok = ok && cudaEventCreateWithFlags(&h->ev_rest[i], cudaEventDisableTiming) == cudaSuccess;
+    }
+    if (!ok) {
+      set_last_error(cudaGetLastError(), "egpu_create streams", __FILE__, __LINE__);
+      egpu_destroy(h);
+      return EGPU_ERR_CUDA;
+    }
+  }
   cudaMemset(h->dstatus, 0, sizeof(DevStatus));
   *out = h;
   return EGPU_OK;
@@ -534,6 +681,10 @@ int egpu_destroy(egpu_handle h) {
     if (h->stage[i]) cudaFree(h->stage[i]);
   if (h->dstatus) cudaFree(h->dstatus);
   if (h->hstatus) cudaFreeHost(h->hstatus);
+  if (h->side) cudaStreamSynchronize(h->side);
+  for (cudaEvent_t e : {h->ev_fork, h->ev_join, h->ev_panel[0], h->ev_panel[1], h->ev_rest[0], h->ev_rest[1]})
+    if (e) cudaEventDestroy(e);
+  if (h->side) cudaStreamDestroy(h->side);
   if (h->own_stream) cudaStreamDestroy(h->own_stream);
   delete h;
   return EGPU_OK;
@@ -563,6 +714,37 @@ int egpu_set_blocksize(egpu_handle h, int nb) {
 }
 
 int egpu_get_blocksize(egpu_handle h) { return h ? h->nb : -1; }
+
+int egpu_set_async(egpu_handle h, int on) {
+  TRY(check_handle(h));
+  Enter g(h);
+  if (h->async && !on) {  // leaving async mode: settle outstanding work
+    EGPU_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  }
+  h->async = on ? 1 : 0;
+  return EGPU_OK;
+}
+
+int egpu_get_status(egpu_handle h, int* info) {
+  TRY(check_handle(h));
+  Enter g(h);
+  int rc = read_status_now(h, info);
+  EGPU_CUDA_TRY(cudaMemsetAsync(h->dstatus, 0, sizeof(DevStatus), h->stream));
+  return rc;
+}
+
+int egpu_reserve(egpu_handle h, size_t bytes) {
+  TRY(check_handle(h));
+  Enter g(h);
+  return ensure_ws(h, bytes);
+}
+
+int egpu_set_lookahead(egpu_handle h, int depth) {
+  TRY(check_handle(h));
+  if (depth < 0) return EGPU_ERR_ARG;
+  h->lookahead = depth > 0 ? 1 : 0;
+  return EGPU_OK;
+}
 
 long long egpu_launch_count(egpu_handle) { return g_launches.load(); }
 
@@ -814,6 +996,7 @@ int egpu_host_dpotrf(egpu_handle h, int uplo, int n, double* A, int lda, int* in
   if (n < 0 || bad_ld(lda, n) || (uplo != EGPU_LOWER && uplo != EGPU_UPPER)) return EGPU_ERR_ARG;
   if (n == 0) return EGPU_OK;
   Enter g(h);
+  SyncScope ss(h);
   double* d; long long ld;
   TRY(h2d(h, 0, A, lda, n, n, &d, &ld));
   TRY(reset_status(h));
@@ -830,6 +1013,7 @@ int egpu_host_dpotrs(egpu_handle h, int uplo, int orient, int n, int nrhs, const
   if (n < 0 || nrhs < 0 || bad_ld(lda, n) || bad_ld(ldb, n)) return EGPU_ERR_ARG;
   if (n == 0 || nrhs == 0) return EGPU_OK;
   Enter g(h);
+  SyncScope ss(h);
   double *dA, *dB; long long la, lb;
   TRY(h2d(h, 0, A, lda, n, n, &dA, &la));
   TRY(h2d(h, 1, B, ldb, n, nrhs, &dB, &lb));
@@ -847,6 +1031,7 @@ int egpu_host_dposv(egpu_handle h, int uplo, int orient, int n, int nrhs, double
   if (n < 0 || nrhs < 0 || bad_ld(lda, n) || bad_ld(ldb, n)) return EGPU_ERR_ARG;
   if (n == 0) return EGPU_OK;
   Enter g(h);
+  SyncScope ss(h);
   double *dA, *dB; long long la, lb;
   TRY(h2d(h, 0, A, lda, n, n, &dA, &la));
   TRY(h2d(h, 1, B, ldb, n, nrhs, &dB, &lb));
@@ -866,6 +1051,7 @@ int egpu_host_dgetrf(egpu_handle h, int m, int n, double* A, int lda, int* p, in
   if (m < 0 || n < 0 || bad_ld(lda, m)) return EGPU_ERR_ARG;
   if (m == 0 || n == 0) return EGPU_OK;
   Enter g(h);
+  SyncScope ss(h);
   double* d; long long ld;
   TRY(h2d(h, 0, A, lda, m, n, &d, &ld));
   const int mn = std::min(m, n);
@@ -885,6 +1071,7 @@ int egpu_host_dgetrf_nopiv(egpu_handle h, int m, int n, double* A, int lda, int*
   if (m < 0 || n < 0 || bad_ld(lda, m)) return EGPU_ERR_ARG;
   if (m == 0 || n == 0) return EGPU_OK;
   Enter g(h);
+  SyncScope ss(h);
   double* d; long long ld;
   TRY(h2d(h, 0, A, lda, m, n, &d, &ld));
   TRY(reset_status(h));
@@ -900,6 +1087,7 @@ int egpu_host_dgetrs(egpu_handle h, int orient, int n, int nrhs, const double* A
   if (n < 0 || nrhs < 0 || bad_ld(lda, n) || bad_ld(ldb, n)) return EGPU_ERR_ARG;
   if (n == 0 || nrhs == 0) return EGPU_OK;
   Enter g(h);
+  SyncScope ss(h);
   double *dA, *dB; long long la, lb;
   TRY(h2d(h, 0, A, lda, n, n, &dA, &la));
   TRY(h2d(h, 1, B, ldb, n, nrhs, &dB, &lb));
@@ -921,6 +1109,7 @@ int egpu_host_dgesv(egpu_handle h, int n, int nrhs, double* A, int lda, double* 
   if (n < 0 || nrhs < 0 || bad_ld(lda, n) || bad_ld(ldb, n)) return EGPU_ERR_ARG;
   if (n == 0) return EGPU_OK;
   Enter g(h);
+  SyncScope ss(h);
   double *dA, *dB; long long la, lb;
   TRY(h2d(h, 0, A, lda, n, n, &dA, &la));
   TRY(h2d(h, 1, B, ldb, n, std::max(nrhs, 1), &dB, &lb));
@@ -940,6 +1129,7 @@ int egpu_host_dtrsm(egpu_handle h, int side, int uplo, int orient, int diag, int
   if (m < 0 || n < 0 || bad_ld(lda, nt) || bad_ld(ldb, m)) return EGPU_ERR_ARG;
   if (m == 0 || n == 0) return EGPU_OK;
   Enter g(h);
+  SyncScope ss(h);
   double *dA, *dB; long long la, lb;
   TRY(h2d(h, 0, A, lda, nt, nt, &dA, &la));
   TRY(h2d(h, 1, B, ldb, m, n, &dB, &lb));
@@ -957,6 +1147,7 @@ int egpu_host_dgemm(egpu_handle h, int oA, int oB, int m, int n, int k, double a
     return EGPU_ERR_ARG;
   if (m == 0 || n == 0) return EGPU_OK;
   Enter g(h);
+  SyncScope ss(h);
   double *dA, *dB, *dC; long long la, lb, lc;
   TRY(h2d(h, 0, A, lda, ta ? k : m, ta ? m : k, &dA, &la));
   TRY(h2d(h, 1, B, ldb, tb ? n : k, tb ? k : n, &dB, &lb));
@@ -974,6 +1165,7 @@ int egpu_host_dherk(egpu_handle h, int uplo, int orient, int n, int k, double al
   if (n < 0 || k < 0 || bad_ld(lda, tr ? k : n) || bad_ld(ldc, n)) return EGPU_ERR_ARG;
   if (n == 0) return EGPU_OK;
   Enter g(h);
+  SyncScope ss(h);
   double *dA, *dC; long long la, lc;
   TRY(h2d(h, 0, A, lda, tr ? k : n, tr ? n : k, &dA, &la));
   TRY(h2d(h, 2, C, ldc, n, n, &dC, &lc));
@@ -989,6 +1181,7 @@ int egpu_host_dlaswp(egpu_handle h, int inverse, int m, int n, double* A, int ld
   if (m < 0 || n < 0 || npiv < 0 || npiv > m || bad_ld(lda, m)) return EGPU_ERR_ARG;
   if (m == 0 || n == 0 || npiv == 0) return EGPU_OK;
   Enter g(h);
+  SyncScope ss(h);
   double* dA; long long la;
   TRY(h2d(h, 0, A, lda, m, n, &dA, &la));
   int* dp = stage_ints(h, 2, npiv);

@@ -85,6 +85,7 @@ int launch_dgemm(cudaStream_t st, bool a_kmajor, bool b_kmajor, int M, int N, in
   p.tiles_m = (M + BM - 1) / BM;
   p.tiles_n = (N + BN - 1) / BN;
   p.status = status;
+  p.cvec = (reinterpret_cast<uintptr_t>(C) % 16 == 0) && (ldc % 2 == 0);
   long long nblocks;
   if (tri == 0) {
     nblocks = (long long)p.tiles_m * p.tiles_n;

@@ -34,6 +34,7 @@ struct GemmParams {
   double alpha, beta;
   int tri;  // 0 full, 1 lower (row >= col), 2 upper (row <= col)
   int tiles_m, tiles_n;
+  int cvec;  // C base 16-byte aligned and ldc even: paired 16-byte epilogue
   DevStatus* status;
 };
 
@@ -51,16 +52,21 @@ struct GemmShape {
 
 // Map a linear CTA index onto (tile_m, tile_n) for the triangular modes with
 // BM = 2*BN (tile-row i covers rows [BM i, BM i + BM), tile-col j covers
-// [BN j, BN j + BN)).  Lower: column j needs rows i >= j/2; upper: i <= j/2.
-__device__ __forceinline__ long long tri_cum_lower(int j, int MT) {
-  long long a = j / 2;
-  long long S = (j & 1) ? a * a : a * (a - 1);
-  return (long long)j * MT - S;
+// [BN j, BN j + BN)).  Lower: column j needs rows i >= j/2 (count
+// max(0, MT - j/2)); upper: rows i <= j/2 (count min(j/2 + 1, MT)).
+// cum(j) = number of tiles in columns < j.
+__device__ __forceinline__ long long tri_S(long long j) {  // sum_{j'<j} floor(j'/2)
+  const long long a = j / 2;
+  return (j & 1) ? a * a : a * (a - 1);
 }
-__device__ __forceinline__ long long tri_cum_upper(int j) {
-  long long a = j / 2;
-  long long S = (j & 1) ? a * a : a * (a - 1);
-  return S + j;
+__device__ __forceinline__ long long tri_cum_lower(int j, int MT) {
+  const long long jj = min((long long)j, 2ll * MT);
+  return jj * MT - tri_S(jj);
+}
+__device__ __forceinline__ long long tri_cum_upper(int j, int MT) {
+  const long long J0 = 2ll * MT;
+  if (j <= J0) return tri_S(j) + j;
+  return tri_S(J0) + J0 + (j - J0) * MT;
 }
 
 __device__ __forceinline__ bool map_tile(const GemmParams& p, int& ti, int& tj) {
@@ -73,14 +79,14 @@ __device__ __forceinline__ bool map_tile(const GemmParams& p, int& ti, int& tj) 
   int lo = 0, hi = p.tiles_n;  // find largest j with cum(j) <= L
   while (hi - lo > 1) {
     int mid = (lo + hi) >> 1;
-    long long c = p.tri == 1 ? tri_cum_lower(mid, p.tiles_m) : tri_cum_upper(mid);
+    long long c = p.tri == 1 ? tri_cum_lower(mid, p.tiles_m) : tri_cum_upper(mid, p.tiles_m);
     if (c <= L) lo = mid; else hi = mid;
   }
   tj = lo;
   if (p.tri == 1) {
     ti = tj / 2 + (int)(L - tri_cum_lower(tj, p.tiles_m));
   } else {
-    ti = (int)(L - tri_cum_upper(tj));
+    ti = (int)(L - tri_cum_upper(tj, p.tiles_m));
   }
   return ti < p.tiles_m && tj < p.tiles_n;
 }
@@ -226,6 +232,49 @@ __global__ void __launch_bounds__(32 * WARPS_M * WARPS_N, (WARPS_M * WARPS_N <= 
     if (p.tri == 2 && row > col) return false;
     return true;
   };
+  // MN-major A: tiles 2pr and 2pr+1 hold rows (2g, 2g+1) -> one 16-byte access
+  const bool vec = !AK && p.cvec;
+  if (vec) {
+#pragma unroll
+    for (int pr = 0; pr < 2; ++pr)
+#pragma unroll
+      for (int j = 0; j < 4; ++j)
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+          const int row = row_of(2 * pr, r), col = col_of(j, r);
+          const bool v0 = valid(row, col), v1 = valid(row + 1, col);
+          double* cp = p.C + (long long)col * p.ldc + row;
+          double c0 = 0.0, c1 = 0.0;
+          if (beta != 0.0) {
+            if (v0 && v1) {
+              const double2 cc = *reinterpret_cast<const double2*>(cp);
+              c0 = cc.x; c1 = cc.y;
+            } else {
+              if (v0) c0 = cp[0];
+              if (v1) c1 = cp[1];
+            }
+          }
+          acc[2 * pr][j][r] = fma(beta, c0, alpha * acc[2 * pr][j][r]);
+          acc[2 * pr + 1][j][r] = fma(beta, c1, alpha * acc[2 * pr + 1][j][r]);
+        }
+#pragma unroll
+    for (int pr = 0; pr < 2; ++pr)
+#pragma unroll
+      for (int j = 0; j < 4; ++j)
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+          const int row = row_of(2 * pr, r), col = col_of(j, r);
+          const bool v0 = valid(row, col), v1 = valid(row + 1, col);
+          double* cp = p.C + (long long)col * p.ldc + row;
+          if (v0 && v1) {
+            *reinterpret_cast<double2*>(cp) = make_double2(acc[2 * pr][j][r], acc[2 * pr + 1][j][r]);
+          } else {
+            if (v0) cp[0] = acc[2 * pr][j][r];
+            if (v1) cp[1] = acc[2 * pr + 1][j][r];
+          }
+        }
+    return;
+  }
   if (beta != 0.0) {
 #pragma unroll
     for (int i = 0; i < 4; ++i)

@@ -65,6 +65,7 @@ __global__ void __launch_bounds__(kPanelThreads) lu_panel_kernel(int m, int b, d
   __shared__ double red_abs[kPanelThreads / 32];
   __shared__ int red_row[kPanelThreads / 32];
   __shared__ double red_val[kPanelThreads / 32];
+  __shared__ int red_cta[kPanelThreads / 32];
   __shared__ int s_win, s_prow, s_stop;
   __shared__ double s_pval;
 
@@ -122,28 +123,44 @@ __global__ void __launch_bounds__(kPanelThreads) lu_panel_kernel(int m, int b, d
       if (j >= r0 && j < r0 + rows)
         for (int c = tid; c < b; c += kPanelThreads) jrow[par * b + c] = S[c * R + (j - r0)];
     }
-    __threadfence();
-    // 2. one grid-wide barrier per column
+    // 2. one grid-wide barrier per column (its leading __syncthreads orders
+    //    this CTA's stores before thread 0's release fence)
     if (!grid_barrier(counter, (unsigned)P * (unsigned)(j + 1))) {
       if (tid == 0) set_status(st, kTimeout, 200 + j);
       return;
     }
-    // 3. global winner: strict '>' over CTAs in row order, ties -> lowest row
-    if (tid == 0) {
+    // 3. global winner: largest |a|, ties -> lowest row (the strict '>' scan
+    //    of LU/Panel.hpp:52-63).  Thread c reads CTA c's candidate with an
+    //    L2-coherent load (.cg), then a block argmax reduction.
+    {
       double wb = -1.0, wv = 0.0;
       int wr = 0x7fffffff, wc = 0;
-      for (int c = 0; c < P; ++c) {
-        // L2-coherent loads (.cg): another CTA wrote these after our last visit
-        const PanelCand* cp = &cand[par * P + c];
-        const double ca = __ldcg(&cp->absv);
-        const int cr = __ldcg(&cp->row);
-        if (cand_better(ca, cr, wb, wr)) { wb = ca; wr = cr; wv = __ldcg(&cp->val); wc = c; }
+      if (tid < P) {
+        const PanelCand* cp = &cand[par * P + tid];
+        wb = __ldcg(&cp->absv);
+        wr = __ldcg(&cp->row);
+        wv = __ldcg(&cp->val);
+        wc = tid;
       }
-      s_win = wc; s_prow = wr; s_pval = wv;
-      s_stop = (wv == 0.0);
-      if (cta == 0) p[j] = wr + offset;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        const double ob = __shfl_down_sync(0xffffffffu, wb, o);
+        const int orow = __shfl_down_sync(0xffffffffu, wr, o);
+        const double ov = __shfl_down_sync(0xffffffffu, wv, o);
+        const int oc = __shfl_down_sync(0xffffffffu, wc, o);
+        if (cand_better(ob, orow, wb, wr)) { wb = ob; wr = orow; wv = ov; wc = oc; }
+      }
+      if (lane == 0) { red_abs[warp] = wb; red_row[warp] = wr; red_val[warp] = wv; red_cta[warp] = wc; }
+      __syncthreads();
+      if (tid == 0) {
+        for (int w = 1; w < kPanelThreads / 32; ++w)
+          if (cand_better(red_abs[w], red_row[w], wb, wr)) { wb = red_abs[w]; wr = red_row[w]; wv = red_val[w]; wc = red_cta[w]; }
+        s_win = wc; s_prow = wr; s_pval = wv;
+        s_stop = (wv == 0.0);
+        if (cta == 0) p[j] = wr + offset;
+      }
+      __syncthreads();
     }
-    __syncthreads();
     const int prow = s_prow;
     const double pval = s_pval;
     const double* wrow = rowbuf + ((size_t)par * P + s_win) * b;
@@ -223,10 +240,293 @@ __global__ void __launch_bounds__(kPanelThreads) lu_panel_kernel(int m, int b, d
   }
 }
 
+// ---------------------------------------------------------------------------
+// Cluster form of the panel for m <= 16 * 192 rows: the P <= 16 CTAs form one
+// thread-block cluster.  Candidates are written straight into every CTA's
+// shared memory (DSMEM), the per-column barrier is the hardware cluster
+// barrier, and the winning row is read from the winner's shared memory.  Each
+// CTA keeps private copies of its candidate row and of row j, double-buffered
+// by column parity, so one cluster barrier per column suffices: a buffer is
+// rewritten two columns later, after every reader has passed the next barrier.
+struct ClusterCand {
+  double absv, val, row, pad;
+};
+
+__device__ __forceinline__ void cluster_arrive_release() {
+  asm volatile("barrier.cluster.arrive.release.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void cluster_wait_acquire() {
+  asm volatile("barrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+__device__ __forceinline__ unsigned cluster_ctarank() {
+  unsigned r;
+  asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+  return r;
+}
+// Generic address of the same shared-memory object in CTA `rank` of the cluster.
+template <class T>
+__device__ __forceinline__ T* cluster_map(T* p, unsigned rank) {
+  uint64_t out;
+  asm volatile("mapa.u64 %0, %1, %2;" : "=l"(out) : "l"(reinterpret_cast<uint64_t>(p)), "r"(rank));
+  return reinterpret_cast<T*>(out);
+}
+
+__global__ void __launch_bounds__(kPanelThreads) lu_panel_cluster_kernel(int m, int b, double* A, long long lda,
+                                                                          int* p, int offset, int* image,
+                                                                          int* preimage, double* W, int ldw, int R,
+                                                                          DevStatus* st) {
+  extern __shared__ double S[];  // b x R rows (ld R) | u[b] | crow[2][b] | jbuf[2][b] | cand[2][16]
+  double* u = S + (size_t)b * R;
+  double* crow = u + b;
+  double* jbuf = crow + 2 * b;
+  ClusterCand* cand = reinterpret_cast<ClusterCand*>(jbuf + 2 * b);
+  __shared__ double red_abs[kPanelThreads / 32];
+  __shared__ int red_row[kPanelThreads / 32];
+  __shared__ double red_val[kPanelThreads / 32];
+  __shared__ int s_win, s_prow, s_stop;
+  __shared__ double s_pval;
+
+  const int P = gridDim.x;  // == cluster size
+  const unsigned cta = cluster_ctarank();
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int r0 = (int)cta * R;
+  const int rows = max(0, min(R, m - r0));
+  // An earlier failure (status word) skips the panel.  CTA 0's reading is
+  // the cluster's decision, so every CTA leaves at the same point.
+  __shared__ int s_skip;
+  if (tid == 0) s_skip = (st != nullptr && ((volatile DevStatus*)st)->code != 0);
+  for (int c = 0; c < b; ++c)
+    for (int lr = tid; lr < rows; lr += kPanelThreads) S[c * R + lr] = A[(long long)c * lda + r0 + lr];
+  __syncthreads();
+  cluster_arrive_release();  // all CTAs resident and initialised before any DSMEM traffic
+  cluster_wait_acquire();
+  const int skip = *cluster_map(&s_skip, 0u);
+  cluster_arrive_release();  // CTA 0's flag has been read by all before anyone leaves
+  cluster_wait_acquire();
+  if (skip) return;
+
+  const int ncols = min(b, m);
+  for (int j = 0; j < ncols; ++j) {
+    const int par = j & 1;
+    double best = -1.0, bval = 0.0;
+    int brow = 0x7fffffff;
+    for (int lr = max(0, j - r0) + tid; lr < rows; lr += kPanelThreads) {
+      const double v = S[j * R + lr];
+      const double av = fabs(v);
+      if (cand_better(av, r0 + lr, best, brow)) { best = av; brow = r0 + lr; bval = v; }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const double ob = __shfl_down_sync(0xffffffffu, best, o);
+      const int orow = __shfl_down_sync(0xffffffffu, brow, o);
+      const double ov = __shfl_down_sync(0xffffffffu, bval, o);
+      if (cand_better(ob, orow, best, brow)) { best = ob; brow = orow; bval = ov; }
+    }
+    if (lane == 0) { red_abs[warp] = best; red_row[warp] = brow; red_val[warp] = bval; }
+    __syncthreads();
+    if (warp == 0) {
+      best = lane < kPanelThreads / 32 ? red_abs[lane] : -1.0;
+      brow = lane < kPanelThreads / 32 ? red_row[lane] : 0x7fffffff;
+      bval = lane < kPanelThreads / 32 ? red_val[lane] : 0.0;
+#pragma unroll
+      for (int o = 4; o > 0; o >>= 1) {
+        const double ob = __shfl_down_sync(0xffffffffu, best, o);
+        const int orow = __shfl_down_sync(0xffffffffu, brow, o);
+        const double ov = __shfl_down_sync(0xffffffffu, bval, o);
+        if (cand_better(ob, orow, best, brow)) { best = ob; brow = orow; bval = ov; }
+      }
+      best = __shfl_sync(0xffffffffu, best, 0);
+      brow = __shfl_sync(0xffffffffu, brow, 0);
+      bval = __shfl_sync(0xffffffffu, bval, 0);
+      if (lane < P) {  // candidate into every CTA's slot [par][cta]
+        ClusterCand* dst = cluster_map(&cand[par * 16 + cta], (unsigned)lane);
+        dst->absv = best; dst->val = bval; dst->row = (double)brow;
+      }
+      if (lane == 0) red_row[0] = brow;
+    }
+    __syncthreads();
+    {
+      const int myrow = red_row[0];
+      if (myrow != 0x7fffffff)
+        for (int c = tid; c < b; c += kPanelThreads) crow[par * b + c] = S[c * R + (myrow - r0)];
+      if (j >= r0 && j < r0 + rows)
+        for (int c = tid; c < b; c += kPanelThreads) jbuf[par * b + c] = S[c * R + (j - r0)];
+    }
+    __syncthreads();
+    cluster_arrive_release();
+    cluster_wait_acquire();
+    if (warp == 0) {
+      double wb = -1.0, wv = 0.0;
+      int wr = 0x7fffffff, wc = 0;
+      if (lane < P) {
+        const ClusterCand cc = cand[par * 16 + lane];
+        wb = cc.absv; wv = cc.val; wr = (int)cc.row; wc = lane;
+      }
+#pragma unroll
+      for (int o = 8; o > 0; o >>= 1) {
+        const double ob = __shfl_down_sync(0xffffffffu, wb, o);
+        const int orow = __shfl_down_sync(0xffffffffu, wr, o);
+        const double ov = __shfl_down_sync(0xffffffffu, wv, o);
+        const int oc = __shfl_down_sync(0xffffffffu, wc, o);
+        if (cand_better(ob, orow, wb, wr)) { wb = ob; wr = orow; wv = ov; wc = oc; }
+      }
+      if (lane == 0) {
+        s_win = wc; s_prow = wr; s_pval = wv;
+        s_stop = (wv == 0.0);
+        if (cta == 0) p[j] = wr + offset;
+      }
+    }
+    __syncthreads();
+    const int prow = s_prow;
+    const double pval = s_pval;
+    if (s_stop) {  // exact zero pivot: SingularMatrixException (LU/Panel.hpp:76-77)
+      if (cta == 0 && tid == 0) set_status(st, kSingular, offset + j + 1);
+      break;
+    }
+    const double* wrow = cluster_map(crow + par * b, (unsigned)s_win);
+    if (prow != j) {
+      if (prow >= r0 && prow < r0 + rows) {
+        const double* jr = cluster_map(jbuf + par * b, (unsigned)(j / R));
+        for (int c = tid; c < b; c += kPanelThreads) S[c * R + (prow - r0)] = jr[c];
+      }
+      if (j >= r0 && j < r0 + rows)
+        for (int c = tid; c < b; c += kPanelThreads) S[c * R + (j - r0)] = wrow[c];
+    }
+    for (int c = j + 1 + tid; c < b; c += kPanelThreads) u[c] = wrow[c];
+    const double inv = 1.0 / pval;
+    const int lr1 = max(0, j + 1 - r0);
+    __syncthreads();
+    for (int lr = lr1 + tid; lr < rows; lr += kPanelThreads) S[j * R + lr] *= inv;
+    __syncthreads();
+    const int nr = rows - lr1;
+    if (nr > 0) {
+      const int tpr = (nr >= kPanelThreads) ? 1 : (nr >= kPanelThreads / 2 ? 2 : 4);
+      const int ph = tid % tpr;
+      for (int lr = lr1 + tid / tpr; lr < rows; lr += kPanelThreads / tpr) {
+        const double l = S[j * R + lr];
+        for (int c = j + 1 + ph; c < b; c += tpr) S[c * R + lr] -= l * u[c];
+      }
+    }
+    __syncthreads();
+  }
+  for (int c = 0; c < b; ++c)
+    for (int lr = tid; lr < rows; lr += kPanelThreads) A[(long long)c * lda + r0 + lr] = S[c * R + lr];
+  // no CTA may exit while others can still read its shared memory
+  __syncthreads();
+  cluster_arrive_release();
+  cluster_wait_acquire();
+  if (cta != 0) return;
+  if (st != nullptr && ((volatile DevStatus*)st)->code != 0) return;
+  if (tid < b) {  // ComposePivots(p, offset, image, preimage), ComposePivots.hpp:81-125
+    const int i = tid;
+    int k = p[i] - offset;
+    for (int jj = i - 1; jj >= 0; --jj) {
+      const int pj = p[jj] - offset;
+      if (pj == k) k = jj;
+      else if (jj == k) k = pj;
+    }
+    preimage[i] = k;
+    k = i;
+    for (int jj = 0; jj < min(k + 1, b); ++jj) {
+      const int pj = p[jj] - offset;
+      if (pj == k) k = jj;
+      else if (jj == k) k = pj;
+    }
+    image[i] = k;
+  }
+  __syncthreads();
+  if (W != nullptr) {  // inv(unit lower L11)
+    const int i = tid;
+    for (int j = b - 1; j >= 0; --j) {
+      double tmp = 0.0;
+      if (i > j && i < b) {
+        for (int k = j + 1; k < i; ++k) tmp = fma(S[k * R + i], S[j * R + k], tmp);
+        tmp += S[j * R + i];
+      }
+      __syncthreads();
+      if (i > j && i < b) S[j * R + i] = -tmp;
+      __syncthreads();
+    }
+    for (int idx = tid; idx < b * b; idx += kPanelThreads) {
+      const int r = idx % b, c = idx / b;
+      W[r + (long long)c * ldw] = r > c ? S[c * R + r] : (r == c ? 1.0 : 0.0);
+    }
+  }
+}
+
+static size_t cluster_panel_smem(int b, int R) {
+  return sizeof(double) * ((size_t)b * R + 5 * (size_t)b) + sizeof(ClusterCand) * 32;
+}
+
+// Largest usable cluster for the panel (16 needs the non-portable opt-in and
+// 16 co-schedulable SMs); 0 when clusters cannot be used.
+static int panel_cluster_max() {
+  static int cached = -1;
+  if (cached >= 0) return cached;
+  cached = 0;
+  const int R = kPanelMaxRowsPerCta, b = 128;
+  const size_t smem = cluster_panel_smem(b, R);
+  if (cudaFuncSetAttribute(lu_panel_cluster_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+      cudaSuccess) {
+    cudaGetLastError();
+    return cached;
+  }
+  cudaFuncSetAttribute(lu_panel_cluster_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+  cudaGetLastError();
+  for (int c : {16, 8}) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(c);
+    cfg.blockDim = dim3(kPanelThreads);
+    cfg.dynamicSmemBytes = smem;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = c;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    int nclusters = 0;
+    if (cudaOccupancyMaxActiveClusters(&nclusters, lu_panel_cluster_kernel, &cfg) == cudaSuccess && nclusters > 0) {
+      cached = c;
+      break;
+    }
+    cudaGetLastError();
+  }
+  return cached;
+}
+
 int launch_lu_panel(cudaStream_t st, int m, int b, double* A, long long lda, int* p, int offset, int* image,
                     int* preimage, double* W, int ldw, void* scratch, DevStatus* status, int sm_count) {
   if (m <= 0 || b <= 0) return EGPU_OK;
   if (b > 128) return EGPU_ERR_ARG;
+  // cluster form when the panel fits in one cluster's shared memory
+  const int cmax = panel_cluster_max();
+  if (cmax > 0 && m <= cmax * kPanelMaxRowsPerCta) {
+    int R = std::max(b, 32);
+    while ((m + R - 1) / R > cmax) R += 32;
+    const int P = (m + R - 1) / R;
+    TraceMark tm(st, kTracePanel, (double)m * b * b, 16.0 * m * b);
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(P);
+    cfg.blockDim = dim3(kPanelThreads);
+    cfg.dynamicSmemBytes = cluster_panel_smem(b, R);
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = P;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaError_t e = cudaLaunchKernelEx(&cfg, lu_panel_cluster_kernel, m, b, A, lda, p, offset, image, preimage, W,
+                                       ldw, R, status);
+    count_launch();
+    if (e != cudaSuccess) {
+      set_last_error(e, "lu_panel_cluster launch", __FILE__, __LINE__);
+      return EGPU_ERR_CUDA;
+    }
+    return EGPU_OK;
+  }
   const int R = panel_rows_per_cta(m, sm_count);
   const int P = (m + R - 1) / R;
   if (P > sm_count || R < b) return EGPU_ERR_UNSUPPORTED;

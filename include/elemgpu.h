@@ -24,6 +24,8 @@
 #ifndef ELEMGPU_H
 #define ELEMGPU_H
 
+#include <stddef.h>
+
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -66,7 +68,8 @@ typedef struct egpu_context* egpu_handle;
  * (elem::Initialize, core/environment_decl.hpp:16-38). */
 EGPU_API int egpu_create(egpu_handle* h, int device);
 EGPU_API int egpu_destroy(egpu_handle h);
-/* Use an external cudaStream_t (NULL restores the handle's own stream). */
+/* Use an external cudaStream_t (NULL restores the handle's own stream;
+ * cudaStreamLegacy, 0x1, selects the legacy default stream). */
 EGPU_API int egpu_set_stream(egpu_handle h, void* cuda_stream);
 EGPU_API void* egpu_get_stream(egpu_handle h);
 EGPU_API int egpu_synchronize(egpu_handle h);
@@ -75,6 +78,20 @@ EGPU_API int egpu_synchronize(egpu_handle h);
  * the panel width; values are rounded to an even number in [2, 128]. */
 EGPU_API int egpu_set_blocksize(egpu_handle h, int nb);
 EGPU_API int egpu_get_blocksize(egpu_handle h);
+/* Panel look-ahead depth (0 = sequential steps on one stream, 1 = default:
+ * the next panel is factored on a high-priority side stream while the current
+ * trailing update runs).  Results are identical either way. */
+EGPU_API int egpu_set_lookahead(egpu_handle h, int depth);
+/* Asynchronous mode for the device-memory API: calls only enqueue work on the
+ * handle's stream and return EGPU_OK; a failure status (not HPD, singular,
+ * timeout) is kept on the device, later kernels of the handle skip their work,
+ * and egpu_get_status() waits, returns the first failure and clears it.  Needed
+ * for CUDA-graph capture of whole factorizations.  Host-memory calls always
+ * synchronize. */
+EGPU_API int egpu_set_async(egpu_handle h, int on);
+EGPU_API int egpu_get_status(egpu_handle h, int* info);
+/* Pre-size the device workspace (bytes) so that later calls allocate nothing. */
+EGPU_API int egpu_reserve(egpu_handle h, size_t bytes);
 EGPU_API const char* egpu_error_string(int code);
 /* Text of the last CUDA error seen by this thread (or ""). */
 EGPU_API const char* egpu_last_error_detail(void);

@@ -301,3 +301,70 @@ def test_host_api_matches_device_api(handle):
     ref, pref, _ = orc.lu(G, 128)
     assert np.array_equal(p, pref)
     assert np.max(np.abs(Gh - ref)) <= 1e-10 * np.max(np.abs(ref))
+
+
+@pytest.mark.parametrize("uplo", [eg.LOWER, eg.UPPER])
+def test_cholesky_lookahead_matches_sequential(handle, uplo):
+    n = 1500
+    A = inputs.spd_ggt(n, 61)
+    out = []
+    for depth in (0, 1):
+        handle.set_lookahead(depth)
+        dA = cuda(A)
+        handle.cholesky(dA, uplo)
+        out.append(host(dA))
+    handle.set_lookahead(1)
+    tri = np.tril if uplo == eg.LOWER else np.triu
+    assert np.max(np.abs(tri(out[0]) - tri(out[1]))) <= 1e-13 * np.max(np.abs(out[0]))
+
+
+def test_lu_lookahead_matches_sequential(handle):
+    import torch
+    n = 1500
+    A = inputs.uniform(n, n, 62)
+    res = []
+    for depth in (0, 1):
+        handle.set_lookahead(depth)
+        dA = cuda(A)
+        dp = torch.zeros(n, dtype=torch.int32, device="cuda")
+        handle.lu(dA, dp)
+        res.append((host(dA), dp.cpu().numpy()))
+    handle.set_lookahead(1)
+    assert np.array_equal(res[0][1], res[1][1])
+    assert np.max(np.abs(res[0][0] - res[1][0])) <= 1e-12 * np.max(np.abs(res[0][0]))
+
+
+def test_async_mode_keeps_first_failure(handle):
+    # async: calls only enqueue; the first failure is reported by get_status
+    good = inputs.spd_ggt(300, 71)
+    bad = good.copy(order="F")
+    bad[100, 100] = -1.0
+    handle.set_async(True)
+    try:
+        d1, d2, d3 = cuda(good), cuda(bad), cuda(good)
+        handle.cholesky(d1, eg.LOWER)
+        handle.cholesky(d2, eg.LOWER)
+        handle.cholesky(d3, eg.LOWER)  # skipped: a failure is pending
+        with pytest.raises(eg.NonHPDError) as ei:
+            handle.get_status()
+        assert ei.value.column == 101
+        handle.get_status()  # cleared
+    finally:
+        handle.set_async(False)
+    ref, _ = orc.cholesky(good, eg.LOWER, 128)
+    assert np.max(np.abs(np.tril(host(d1)) - np.tril(ref))) <= 1e-11 * np.max(np.abs(ref))
+    assert np.array_equal(host(d3), good)  # untouched
+
+
+def test_trace_records_kernel_classes(handle):
+    import torch
+    A = inputs.uniform(640, 640, 72)
+    dA = cuda(A)
+    dp = torch.zeros(640, dtype=torch.int32, device="cuda")
+    handle.trace_enable(True)
+    handle.lu(dA, dp)
+    s = handle.trace_summary()
+    handle.trace_enable(False)
+    assert s["panel"]["launches"] == 5
+    assert s["update"]["launches"] >= 4 and s["update"]["flops"] > 0
+    assert all(v["ms"] >= 0 for v in s.values())
