@@ -267,6 +267,10 @@ def our_arm(args, ws, rank, local):
     if rank != 0:
         return
     # ---- roofline of the dominant kernel (trailing-update DMMA GEMM)
+    try:
+        live_peak = h.measure_fp64_peak()
+    except Exception:
+        live_peak = None
     upd = trace["update"]
     achieved = upd["flops"] / (upd["ms"] / 1e3) / 1e12 if upd["ms"] > 0 else None
     traffic = None
@@ -301,6 +305,7 @@ def our_arm(args, ws, rank, local):
                      "achieved": achieved, "peak": FP64_PEAK_TFLOPS, "unit": "TFLOP/s",
                      "frac": (achieved / FP64_PEAK_TFLOPS) if achieved else None,
                      "peak_source": "measured FP64 DMMA peak (profiles/fp64_peak.md); MEASURED_PEAKS.json has no FP64 entry",
+                     "peak_live_tflops": live_peak,
                      "traffic": traffic, "launches": upd["launches"],
                      "share_of_traced_time": upd["ms"] / total_ms if total_ms else None},
         "kernels": {k: {"ms": v["ms"], "launches": v["launches"]} for k, v in trace.items() if v["launches"]},
@@ -311,6 +316,74 @@ def our_arm(args, ws, rank, local):
     print(json.dumps(line), flush=True)
 
 
+def kernel_case(args):
+    """One launch of a single kernel class at a chosen size, for profiler
+    captures (ncu -k ...): 'update' = one lower Herk trailing update
+    (n x n, K = 128), 'gemm' = one Gemm trailing update, 'panel' = one LU panel
+    (n x 128), 'diag' = one diagonal-block Cholesky (128 x 128)."""
+    import torch
+    import elemental_b200 as eg
+    from elemental_b200 import inputs
+    h = eg.Handle(0)
+    n = args.n
+    if args.case in ("update", "gemm"):
+        A = eg.empty_colmajor(n, NB).normal_()
+        C = eg.empty_colmajor(n, n).normal_()
+        if args.case == "update":
+            h.herk(eg.LOWER, eg.NORMAL, -1.0, A, 1.0, C)
+        else:
+            Bm = eg.empty_colmajor(NB, n).normal_()
+            h.gemm(eg.NORMAL, eg.NORMAL, -1.0, A, Bm, 1.0, C)
+    elif args.case == "panel":
+        A = eg.colmajor_cuda(inputs.uniform(n, NB, 1))
+        p = torch.zeros(NB, dtype=torch.int32, device="cuda")
+        h.lu(A, p)
+    elif args.case == "peaks":
+        # roofline denominators and vendor reference points on this GPU
+        out = {"dmma_peak_tflops": h.measure_fp64_peak()}
+        torch.backends.cuda.matmul.allow_tf32 = False
+        for m in (4096, 8192):
+            a = torch.randn(m, m, dtype=torch.float64, device="cuda")
+            b_ = torch.randn(m, m, dtype=torch.float64, device="cuda")
+            for _ in range(2):
+                c = a @ b_
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record()
+            for _ in range(3):
+                c = a @ b_
+            e1.record()
+            torch.cuda.synchronize()
+            out[f"cublas_dgemm_{m}_tflops"] = 2 * m ** 3 * 3 / (e0.elapsed_time(e1) / 1e3) / 1e12
+            del a, b_, c
+        for m in (2048, 8192, 16384):
+            g = torch.randn(m, m, dtype=torch.float64, device="cuda")
+            spd = g @ g.T + m * torch.eye(m, dtype=torch.float64, device="cuda")
+            torch.linalg.cholesky(spd)
+            torch.linalg.lu_factor(g)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record()
+            torch.linalg.cholesky(spd)
+            e1.record()
+            torch.cuda.synchronize()
+            out[f"cusolver_potrf_{m}_ms"] = e0.elapsed_time(e1)
+            if m <= 8192:
+                e0.record()
+                torch.linalg.lu_factor(g)
+                e1.record()
+                torch.cuda.synchronize()
+                out[f"cusolver_getrf_{m}_ms"] = e0.elapsed_time(e1)
+            del g, spd
+        print(json.dumps(out))
+        return
+    elif args.case == "diag":
+        A = eg.colmajor_cuda(inputs.spd_ggt(NB, 1))
+        h.cholesky(A, eg.LOWER)
+    torch.cuda.synchronize()
+    print(json.dumps({"case": args.case, "n": n, "ok": True}))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -318,7 +391,13 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline leg")
+    ap.add_argument("--case", choices=["update", "gemm", "panel", "diag", "peaks"], default=None,
+                    help="run one launch of one kernel class (profiling)")
+    ap.add_argument("--n", type=int, default=6144, help="size for --case")
     args = ap.parse_args()
+    if args.case:
+        kernel_case(args)
+        return
     ws, rank, local = dist_setup()
     try:
         if args.impl == "reference":

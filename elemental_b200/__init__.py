@@ -94,6 +94,7 @@ def _declare(L):
         "egpu_set_async": ([H, I], I),
         "egpu_get_status": ([H, P], I),
         "egpu_reserve": ([H, ctypes.c_size_t], I),
+        "egpu_measure_fp64_peak": ([H, P], I),
         "egpu_error_string": ([I], ctypes.c_char_p),
         "egpu_last_error_detail": ([], ctypes.c_char_p),
         "egpu_launch_count": ([H], LL),
@@ -251,6 +252,12 @@ class Handle:
         """Wait for the handle's work; raise the first failure (and clear it)."""
         info = ctypes.c_int(0)
         _check(lib().egpu_get_status(self._h, ctypes.byref(info)), info.value)
+
+    def measure_fp64_peak(self) -> float:
+        """FP64 DMMA throughput of this GPU (TFLOP/s), the FP64 roofline peak."""
+        v = ctypes.c_double()
+        _check(lib().egpu_measure_fp64_peak(self._h, ctypes.byref(v)))
+        return v.value
 
     def reserve(self, nbytes: int):
         _check(lib().egpu_reserve(self._h, int(nbytes)))

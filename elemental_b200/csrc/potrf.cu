@@ -47,223 +47,237 @@ __device__ void tri_inverse_smem(double* S, int b, int uplo, int unit) {
 }
 
 // ---------------------------------------------------------------------------
-// Blocked diagonal-block kernels.  The nb x nb block (nb <= 128) lives in
-// shared memory with leading dimension kLDS = 129 (odd, so both row and
-// column sweeps are bank-conflict free).  It is processed in 32-column
-// sub-blocks: one warp factors / inverts each 32 x 32 diagonal sub-block in
-// registers (lane = row, warp shuffles carry the pivots), and all eight warps
-// apply the resulting panel solve and trailing update as shared-memory
-// mini-GEMMs.  An upper triangle is handled as the lower triangle of its
-// transpose (UVar3Unb and LVar3Unb perform the same operations on A and A^T).
+// Diagonal-block kernels.  The nb x nb block (nb <= 128) lives in shared
+// memory with leading dimension kLDS = 129 (odd: row and column sweeps are
+// both bank-conflict free), always as a LOWER triangle (an upper triangle is
+// handled as the lower triangle of its transpose: UVar3Unb and LVar3Unb
+// perform the same operations on A and A^T).
+//
+// Factorization: 16-column sub-panels.  Inside a sub-panel every column costs
+// one barrier: all threads read a_jj, each updates its share of the
+// sub-panel columns with  a_ik -= a_ij a_kj / a_jj  (the rank-1 update of
+// LVar3Unb, Cholesky/LVar3.hpp:40-46, applied before the column is scaled),
+// and the previous column is scaled by 1/sqrt(a_jj) in the same phase (no
+// thread reads it any more).  After the sub-panel, the trailing triangle is
+// updated by a register-blocked shared-memory mini-GEMM (4x4 per thread).
+// The inverse of the factor is built the same way: 16 x 16 diagonal blocks
+// inverted in parallel (one per warp), then block columns from the right,
+// X21 = -inv(L22) (L21 X11), with 4x4-blocked mini-GEMMs.
+// All loops are rolled: straight-line unrolled code run by one warp stalls
+// on instruction fetch.
 constexpr int kLDS = 129;
-constexpr int kXLD = 33;
-constexpr int kDiagSmem = (128 * kLDS + 4 * 32 * kXLD) * (int)sizeof(double);
+constexpr int kSP = 16;  // sub-panel width
+constexpr int kDiagSmem = (128 * kLDS + 128) * (int)sizeof(double);
 
-// Warp-level Cholesky of the w x w lower sub-block at S[c0.., c0..]
-// (cholesky::LVar3Unb arithmetic, Cholesky/LVar3.hpp:19-49) followed by the
-// inverse of the factor into X (column-major, ld kXLD).  Returns 0 or the
-// 1-based column (within the sub-block) of a non-positive pivot.
-__device__ int warp_chol32(double* S, int c0, int w, double* X) {
-  const int lane = threadIdx.x & 31;
-  double d[32];
+__device__ __forceinline__ double& SE(double* S, int r, int c) { return S[r + c * kLDS]; }
+
+// C[r0.., c0..] (nr x nc, lower part r >= c when tri) -= A[r0.., k0..k0+K) * B[c0.., k0..k0+K)^T
+// reading A and B from S; 4x4 register tiles per thread.  sign = +1 or -1 for
+// "-=" or "+=" (the inverse uses the opposite sign).
+__device__ void smem_syrk_tiles(double* S, int r0, int nr, int c0, int nc, int k0, int K, bool tri) {
+  const int tr = (nr + 3) / 4, tc = (nc + 3) / 4;
+  for (int t = threadIdx.x; t < tr * tc; t += blockDim.x) {
+    const int ti = t % tr, tj = t / tr;
+    const int rb = r0 + 4 * ti, cb = c0 + 4 * tj;
+    if (tri && rb + 3 < cb) continue;  // tile strictly above the diagonal
+    double acc[4][4];
 #pragma unroll
-  for (int k = 0; k < 32; ++k) d[k] = (lane < w && k < w && k <= lane) ? S[c0 + lane + (c0 + k) * kLDS] : 0.0;
-  int fail = 0;
+    for (int a = 0; a < 4; ++a)
 #pragma unroll
-  for (int j = 0; j < 32; ++j) {
-    if (j < w && !fail) {
-      const double djj = __shfl_sync(0xffffffffu, d[j], j);
-      if (djj <= 0.0) {
-        fail = j + 1;
-      } else {
-        const double alpha = sqrt(djj);
-        if (lane > j) d[j] /= alpha;
-        else if (lane == j) d[j] = alpha;
-        const double lj = d[j];
+      for (int b = 0; b < 4; ++b) acc[a][b] = 0.0;
+    for (int k = k0; k < k0 + K; ++k) {
+      double x[4], y[4];
 #pragma unroll
-        for (int k = j + 1; k < 32; ++k) {
-          const double lkj = __shfl_sync(0xffffffffu, lj, k);
-          if (lane >= k) d[k] -= lj * lkj;
-        }
+      for (int a = 0; a < 4; ++a) {
+        x[a] = (rb + a < r0 + nr) ? SE(S, rb + a, k) : 0.0;
+        y[a] = (cb + a < c0 + nc) ? SE(S, cb + a, k) : 0.0;
       }
+#pragma unroll
+      for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) acc[a][b] = fma(x[a], y[b], acc[a][b]);
+    }
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int b = 0; b < 4; ++b) {
+        const int r = rb + a, c = cb + b;
+        if (r < r0 + nr && c < c0 + nc && (!tri || r >= c)) SE(S, r, c) -= acc[a][b];
+      }
+  }
+}
+
+// Lower Cholesky of the b x b block in S.  Returns 0 or the 1-based column
+// of a non-positive pivot ("A was not numerically HPD", LVar3.hpp:37-38); the
+// decision is uniform across the block (every thread reads the same a_jj).
+__device__ int smem_chol(double* S, int b) {
+  __shared__ double s_alpha[128];
+  const int tid = threadIdx.x;
+  const int row = tid & 127, half = tid >> 7;  // two threads per row
+  for (int c0 = 0; c0 < b; c0 += kSP) {
+    const int c1 = min(b, c0 + kSP);
+    for (int j = c0; j < c1; ++j) {
+      const double ajj = SE(S, j, j);
+      if (ajj <= 0.0) return j + 1;
+      if (tid == 0) s_alpha[j] = sqrt(ajj);
+      // column j-1 is read by nobody in this phase: scale it now
+      if (j > c0 && half == 1 && row >= j && row < b) SE(S, row, j - 1) /= s_alpha[j - 1];
+      if (row > j && row < b) {
+        const double lij = SE(S, row, j) / ajj;
+        for (int k = j + 1 + half; k < c1 && k <= row; k += 2) SE(S, row, k) -= lij * SE(S, k, j);
+      }
+      __syncthreads();
+    }
+    if (half == 0 && row >= c1 && row < b) SE(S, row, c1 - 1) /= s_alpha[c1 - 1];
+    if (half == 1 && row >= c0 && row < c1) SE(S, row, row) = s_alpha[row];
+    __syncthreads();
+    if (c1 < b) {
+      smem_syrk_tiles(S, c1, b - c1, c1, b - c1, c0, c1 - c0, true);
+      __syncthreads();
     }
   }
-  if (fail) return fail;
-#pragma unroll
-  for (int k = 0; k < 32; ++k)
-    if (lane < w && k <= lane) S[c0 + lane + (c0 + k) * kLDS] = d[k];
-  // inverse: lane c computes column c of X = L^{-1} by forward substitution
-  double x[32];
-#pragma unroll
-  for (int k = 0; k < 32; ++k) {
-    double acc = (k == lane) ? 1.0 : 0.0;
-#pragma unroll
-    for (int m = 0; m < k; ++m) {
-      const double lkm = __shfl_sync(0xffffffffu, d[m], k);
-      acc = fma(-lkm, x[m], acc);
-    }
-    const double lkk = __shfl_sync(0xffffffffu, d[k], k);
-    x[k] = (k >= lane && k < w) ? acc / lkk : 0.0;
-  }
-#pragma unroll
-  for (int k = 0; k < 32; ++k)
-    if (lane < w && k < w) X[k + lane * kXLD] = x[k];
   return 0;
 }
 
-// Warp-level inverse of the w x w lower sub-block at S[c0.., c0..] into X
-// (unit: the diagonal is taken as 1).
-__device__ void warp_trinv32(const double* S, int c0, int w, int unit, double* X) {
-  const int lane = threadIdx.x & 31;
-  double d[32];
+// In-place inverse of the lower b x b triangle in S (unit: diagonal taken as 1
+// and written as 1).  Uses Xs (16 x 16 scratch per warp would not fit; the
+// diagonal blocks are inverted in place column by column by their warp).
+__device__ void smem_trinv(double* S, int b, int unit) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int nblk = (b + kSP - 1) / kSP;
+  // 1. 16 x 16 diagonal blocks, one warp each: lane c (< 16) computes column c
+  //    of the block inverse by forward substitution, in place is impossible,
+  //    so results go to registers first, then back to S.
+  for (int blk = warp; blk < nblk; blk += blockDim.x / 32) {
+    const int o = blk * kSP, w = min(kSP, b - o);
+    double x[kSP];
+    const int c = lane;
 #pragma unroll
-  for (int k = 0; k < 32; ++k) {
-    double v = (lane < w && k < w && k <= lane) ? S[c0 + lane + (c0 + k) * kLDS] : 0.0;
-    if (unit && k == lane) v = 1.0;
-    d[k] = v;
+    for (int i = 0; i < kSP; ++i) x[i] = 0.0;
+    if (c < w) {
+#pragma unroll
+      for (int i = 0; i < kSP; ++i) {
+        if (i < w && i >= c) {
+          double acc = (i == c) ? 1.0 : 0.0;
+#pragma unroll
+          for (int m = 0; m < kSP; ++m)
+            if (m >= c && m < i) acc = fma(-SE(S, o + i, o + m), x[m], acc);
+          x[i] = unit ? acc : acc / SE(S, o + i, o + i);
+        }
+      }
+    }
+    __syncwarp();
+    if (c < w) {
+#pragma unroll
+      for (int i = 0; i < kSP; ++i)
+        if (i < w && i >= c) SE(S, o + i, o + c) = (unit && i == c) ? 1.0 : x[i];
+    }
   }
-  double x[32];
+  __syncthreads();
+  // 2. block columns from the right: X21 = -inv(L22) * (L21 * X11)
+  for (int blk = nblk - 2; blk >= 0; --blk) {
+    const int o = blk * kSP, w = min(kSP, b - o), r0 = o + w, R = b - r0;
+    // T = L21 * X11 (R x w), computed into registers, written over L21
+    {
+      const int tr = (R + 3) / 4;
+      double acc[4][4];
+      const int t = tid;
+      const bool act = t < tr * 4;  // tiles: 4 rows x 4 cols, w <= 16 -> 4 col tiles
+      const int ti = t % max(tr, 1), tj = t / max(tr, 1);
 #pragma unroll
-  for (int k = 0; k < 32; ++k) {
-    double acc = (k == lane) ? 1.0 : 0.0;
+      for (int a = 0; a < 4; ++a)
 #pragma unroll
-    for (int m = 0; m < k; ++m) {
-      const double lkm = __shfl_sync(0xffffffffu, d[m], k);
-      acc = fma(-lkm, x[m], acc);
-    }
-    const double lkk = __shfl_sync(0xffffffffu, d[k], k);
-    x[k] = (k >= lane && k < w) ? (unit ? acc : acc / lkk) : 0.0;
-  }
+        for (int q = 0; q < 4; ++q) acc[a][q] = 0.0;
+      if (act) {
+        for (int k = 0; k < w; ++k) {
 #pragma unroll
-  for (int k = 0; k < 32; ++k)
-    if (lane < w && k < w) X[k + lane * kXLD] = x[k];
-}
-
-// Blocked in-place inverse of the lower b x b triangle in S, given the
-// inverses of its 32 x 32 diagonal sub-blocks in Xd (block jb at
-// Xd + jb*32*kXLD).  Block columns are processed last to first:
-//   X21 = -inv(L22) * (L21 * X11),  inv(L22) already in place.
-__device__ void block_trinv_inplace(double* S, int b, const double* Xd) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int nsub = (b + 31) / 32;
-  for (int jb = nsub - 1; jb >= 0; --jb) {
-    const int c0 = 32 * jb, w = min(32, b - c0), r0 = c0 + w, R = b - r0;
-    const double* X11 = Xd + jb * 32 * kXLD;
-    if (R > 0) {
-      double res[12];
+          for (int a = 0; a < 4; ++a) {
+            const int r = r0 + 4 * ti + a;
+            const double l = (r < b) ? SE(S, r, o + k) : 0.0;
 #pragma unroll
-      for (int i = 0; i < 12; ++i) {  // T = L21 * X11
-        const int r = warp + 8 * i;
-        double acc = 0.0;
-        if (r < R && lane < w)
-          for (int k = lane; k < w; ++k) acc = fma(S[r0 + r + (c0 + k) * kLDS], X11[k + lane * kXLD], acc);
-        res[i] = acc;
+            for (int q = 0; q < 4; ++q) {
+              const int cc = 4 * tj + q;
+              const double xv = (cc < w && k >= cc) ? SE(S, o + k, o + cc) : 0.0;
+              acc[a][q] = fma(l, xv, acc[a][q]);
+            }
+          }
+        }
       }
       __syncthreads();
+      if (act)
 #pragma unroll
-      for (int i = 0; i < 12; ++i) {
-        const int r = warp + 8 * i;
-        if (r < R && lane < w) S[r0 + r + (c0 + lane) * kLDS] = res[i];
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            const int r = r0 + 4 * ti + a, cc = 4 * tj + q;
+            if (r < b && cc < w) SE(S, r, o + cc) = acc[a][q];
+          }
+      __syncthreads();
+      // X21 = -inv(L22) * T : row r of X21 = -sum_{m <= r} X22[r, m] T[m, :]
+      if (act) {
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+          for (int q = 0; q < 4; ++q) acc[a][q] = 0.0;
+        const int rmax = min(b - 1, r0 + 4 * ti + 3);
+        for (int m = r0; m <= rmax; ++m) {
+          double tv[4];
+#pragma unroll
+          for (int q = 0; q < 4; ++q) tv[q] = (4 * tj + q < w) ? SE(S, m, o + 4 * tj + q) : 0.0;
+#pragma unroll
+          for (int a = 0; a < 4; ++a) {
+            const int r = r0 + 4 * ti + a;
+            const double xv = (r < b && m <= r) ? (unit && m == r ? 1.0 : SE(S, r, m)) : 0.0;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) acc[a][q] = fma(xv, tv[q], acc[a][q]);
+          }
+        }
       }
       __syncthreads();
+      if (act)
 #pragma unroll
-      for (int i = 0; i < 12; ++i) {  // X21 = -inv(L22) * T
-        const int r = warp + 8 * i;
-        double acc = 0.0;
-        if (r < R && lane < w)
-          for (int m = 0; m <= r; ++m) acc = fma(S[r0 + r + (r0 + m) * kLDS], S[r0 + m + (c0 + lane) * kLDS], acc);
-        res[i] = -acc;
-      }
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            const int r = r0 + 4 * ti + a, cc = 4 * tj + q;
+            if (r < b && cc < w) SE(S, r, o + cc) = -acc[a][q];
+          }
       __syncthreads();
-#pragma unroll
-      for (int i = 0; i < 12; ++i) {
-        const int r = warp + 8 * i;
-        if (r < R && lane < w) S[r0 + r + (c0 + lane) * kLDS] = res[i];
-      }
     }
-    for (int idx = threadIdx.x; idx < w * w; idx += blockDim.x) {
-      const int i = idx % w, k = idx / w;
-      if (i >= k) S[c0 + i + (c0 + k) * kLDS] = X11[i + k * kXLD];
-    }
-    __syncthreads();
   }
 }
 
 // Cholesky of the b x b diagonal block (cholesky::LVar3Unb,
 // lapack-like/Cholesky/LVar3.hpp:19-49, or UVar3Unb, Cholesky/UVar3.hpp:21-50),
-// followed by the inverse of the factor into W (other triangle zeroed).
+// then the inverse of the factor into W (other triangle zeroed).
 template <int UPLO>
 __global__ void __launch_bounds__(kDiagThreads) potrf_diag_kernel(double* A, long long lda, int b, double* W,
                                                                    int ldw, DevStatus* st, int col_base) {
-  extern __shared__ double sm[];
-  double* S = sm;
-  double* Xd = sm + 128 * kLDS;
-  __shared__ int s_fail;
+  extern __shared__ double S[];
   if (st != nullptr && st->code != 0) return;
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  for (int idx = tid; idx < b * b; idx += kDiagThreads) {
-    const int r = idx % b, c = idx / b;
-    if (r >= c) S[r + c * kLDS] = (UPLO == EGPU_LOWER) ? A[r + (long long)c * lda] : A[c + (long long)r * lda];
-  }
-  if (tid == 0) s_fail = 0;
+  const int tid = threadIdx.x;
+  for (int c = 0; c < b; ++c)
+    for (int r = c + tid; r < b; r += kDiagThreads)
+      SE(S, r, c) = (UPLO == EGPU_LOWER) ? A[r + (long long)c * lda] : A[c + (long long)r * lda];
   __syncthreads();
-  const int nsub = (b + 31) / 32;
-  for (int jb = 0; jb < nsub; ++jb) {
-    const int c0 = 32 * jb, w = min(32, b - c0), r0 = c0 + w, R = b - r0;
-    double* X11 = Xd + jb * 32 * kXLD;
-    if (warp == 0) {
-      const int f = warp_chol32(S, c0, w, X11);
-      if (f && lane == 0) {
-        s_fail = 1;
-        set_status(st, kNotHPD, col_base + c0 + f);
-      }
-    }
-    __syncthreads();
-    if (s_fail) return;  // "A was not numerically HPD" (LVar3.hpp:37-38)
-    if (R > 0) {
-      // L21 := A21 * inv(L11)^T   (lane = column c: sum_{k<=c} A21[r,k] X11[c,k])
-      double res[12];
-#pragma unroll
-      for (int i = 0; i < 12; ++i) {
-        const int r = warp + 8 * i;
-        double acc = 0.0;
-        if (r < R && lane < w)
-          for (int k = 0; k <= lane; ++k) acc = fma(S[r0 + r + (c0 + k) * kLDS], X11[lane + k * kXLD], acc);
-        res[i] = acc;
-      }
-      __syncthreads();
-#pragma unroll
-      for (int i = 0; i < 12; ++i) {
-        const int r = warp + 8 * i;
-        if (r < R && lane < w) S[r0 + r + (c0 + lane) * kLDS] = res[i];
-      }
-      __syncthreads();
-      // A22 -= L21 L21^T (lower)
-      for (int c = r0 + warp; c < b; c += 8)
-        for (int r = c + lane; r < b; r += 32) {
-          double acc = 0.0;
-#pragma unroll 8
-          for (int k = 0; k < w; ++k) acc = fma(S[r + (c0 + k) * kLDS], S[c + (c0 + k) * kLDS], acc);
-          S[r + c * kLDS] -= acc;
-        }
-      __syncthreads();
-    }
+  const int f = smem_chol(S, b);
+  if (f) {
+    if (tid == 0) set_status(st, kNotHPD, col_base + f);
+    return;
   }
-  for (int idx = tid; idx < b * b; idx += kDiagThreads) {
-    const int r = idx % b, c = idx / b;
-    if (r >= c) {
-      if (UPLO == EGPU_LOWER) A[r + (long long)c * lda] = S[r + c * kLDS];
-      else A[c + (long long)r * lda] = S[r + c * kLDS];
+  for (int c = 0; c < b; ++c)
+    for (int r = c + tid; r < b; r += kDiagThreads) {
+      if (UPLO == EGPU_LOWER) A[r + (long long)c * lda] = SE(S, r, c);
+      else A[c + (long long)r * lda] = SE(S, r, c);
     }
-  }
   __syncthreads();
-  block_trinv_inplace(S, b, Xd);
-  for (int idx = tid; idx < b * b; idx += kDiagThreads) {
-    const int r = idx % b, c = idx / b;
-    const double v = (r >= c) ? S[r + c * kLDS] : 0.0;
-    if (UPLO == EGPU_LOWER) W[r + (long long)c * ldw] = v;
-    else W[c + (long long)r * ldw] = v;  // inv(U) = inv(L)^T
-  }
+  smem_trinv(S, b, 0);
+  for (int c = 0; c < b; ++c)
+    for (int r = tid; r < b; r += kDiagThreads) {
+      const double v = (r >= c) ? SE(S, r, c) : 0.0;
+      if (UPLO == EGPU_LOWER) W[r + (long long)c * ldw] = v;
+      else W[c + (long long)r * ldw] = v;  // inv(U) = inv(L)^T
+    }
 }
 
 int launch_potrf_diag(cudaStream_t st, int uplo, double* A, long long lda, int b, double* W, int ldw,
@@ -295,40 +309,29 @@ int launch_potrf_diag(cudaStream_t st, int uplo, double* A, long long lda, int b
 }
 
 // Inverse of each diagonal block (block i covers rows/cols [i b, min(n, i b + b))),
-// lower or upper (as the transpose of a lower), unit or not.  The 32 x 32
-// diagonal sub-blocks are inverted by four warps in parallel, then the
-// blocked in-place substitution fills the rest.
+// lower or upper (as the transpose of a lower), unit or not.
 __global__ void __launch_bounds__(kDiagThreads) trtri_blocks_kernel(int uplo, int unit, const double* A,
                                                                      long long lda, int n, int b, double* W,
                                                                      int ldw) {
-  extern __shared__ double sm[];
-  double* S = sm;
-  double* Xd = sm + 128 * kLDS;
+  extern __shared__ double S[];
   const int blk = blockIdx.x;
   const int off = blk * b;
   const int bb = min(b, n - off);
   const double* Ab = A + off + (long long)off * lda;
   double* Wb = W + (long long)blk * b * ldw;
-  const int tid = threadIdx.x, warp = tid >> 5;
-  for (int idx = tid; idx < bb * bb; idx += kDiagThreads) {
-    const int r = idx % bb, c = idx / bb;
-    if (r >= c) S[r + c * kLDS] = (uplo == EGPU_LOWER) ? Ab[r + (long long)c * lda] : Ab[c + (long long)r * lda];
-  }
+  const int tid = threadIdx.x;
+  for (int c = 0; c < bb; ++c)
+    for (int r = c + tid; r < bb; r += kDiagThreads)
+      SE(S, r, c) = (uplo == EGPU_LOWER) ? Ab[r + (long long)c * lda] : Ab[c + (long long)r * lda];
   __syncthreads();
-  const int nsub = (bb + 31) / 32;
-  if (warp < nsub) warp_trinv32(S, 32 * warp, min(32, bb - 32 * warp), unit, Xd + warp * 32 * kXLD);
-  __syncthreads();
-  if (unit)  // the substitution reads unit diagonals from S
-    for (int i = tid; i < bb; i += kDiagThreads) S[i + i * kLDS] = 1.0;
-  __syncthreads();
-  block_trinv_inplace(S, bb, Xd);
-  for (int idx = tid; idx < b * b; idx += kDiagThreads) {
-    const int r = idx % b, c = idx / b;
-    double v = 0.0;
-    if (r < bb && c < bb && r >= c) v = S[r + c * kLDS];
-    if (uplo == EGPU_LOWER) Wb[r + (long long)c * ldw] = v;
-    else Wb[c + (long long)r * ldw] = v;
-  }
+  smem_trinv(S, bb, unit);
+  for (int c = 0; c < b; ++c)
+    for (int r = tid; r < b; r += kDiagThreads) {
+      double v = 0.0;
+      if (r < bb && c < bb && r >= c) v = SE(S, r, c);
+      if (uplo == EGPU_LOWER) Wb[r + (long long)c * ldw] = v;
+      else Wb[c + (long long)r * ldw] = v;
+    }
 }
 
 int launch_trtri_blocks(cudaStream_t st, int uplo, int unit, const double* A, long long lda, int n, int b,

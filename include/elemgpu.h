@@ -110,6 +110,10 @@ EGPU_API int egpu_trace_enable(egpu_handle h, int on);
 EGPU_API int egpu_trace_summary(egpu_handle h, int kind, double* total_ms, double* total_flops,
                                 double* total_bytes, long long* launches);
 
+/* Roofline denominator: measured FP64 tensor-core (DMMA) throughput of the
+ * handle's GPU in TFLOP/s (in-register mma.sync loop, ~30 ms). */
+EGPU_API int egpu_measure_fp64_peak(egpu_handle h, double* tflops);
+
 /* ---- device-memory API ---- */
 
 /* Cholesky(uplo, Matrix<F>& A), lapack-like/Cholesky.hpp:49-62 (blocked
