@@ -168,6 +168,19 @@ EGPU_API int egpu_dherk(egpu_handle h, int uplo, int orient, int n, int k, doubl
  * lapack-like/ApplyRowPivots.hpp:17-79 (sequential swaps i <-> p[i]). */
 EGPU_API int egpu_dlaswp(egpu_handle h, int inverse, int m, int n, double* dA, int lda, const int* dp, int npiv);
 
+/* Cholesky factorization that allocates no device memory (no counterpart in
+ * the reference).  For callers that cannot let a library allocate: a process
+ * that gives all device memory to its own pool at start-up and must not see an
+ * allocation fail or synchronise the device mid-run.  Same result as
+ * egpu_dpotrf with lookahead 0, on the caller's stream (NULL = the legacy
+ * default stream), no handle.  dA must be 16-byte aligned with an even lda
+ * (EGPU_ERR_ALIGN otherwise); nb in [2, 128] (EGPU_ERR_UNSUPPORTED otherwise).
+ * Scratch: a file-scope 128 KiB + 256 B __device__ array on every GPU that
+ * loads the library, held until exit; its device address is looked up on the
+ * first call on each device (make that first call before any stream capture).
+ * All calls share the array: calls that overlap on the GPU race. */
+EGPU_API int egpu_dpotrf_noalloc(void* stream, int uplo, int n, double* dA, int lda, int nb, int* info);
+
 /* ---- host-memory API (Matrix<F> buffers; synchronous) ---- */
 EGPU_API int egpu_host_dpotrf(egpu_handle h, int uplo, int n, double* A, int lda, int* info);
 EGPU_API int egpu_host_dpotrs(egpu_handle h, int uplo, int orient, int n, int nrhs, const double* A, int lda, double* B,
