@@ -112,6 +112,8 @@ def _declare(L):
         "egpu_dgemm": ([H, I, I, I, I, I, D, P, I, P, I, D, P, I], I),
         "egpu_dherk": ([H, I, I, I, I, D, P, I, D, P, I], I),
         "egpu_dlaswp": ([H, I, I, I, P, I, P, I], I),
+        "egpu_dposv_batched": ([H, I, P, P, P, P, P, P, P], I),
+        "egpu_dgesv_batched": ([H, I, P, P, P, P, P, P, P], I),
         "egpu_host_dpotrf": ([H, I, I, P, I, P], I),
         "egpu_host_dpotrs": ([H, I, I, I, I, P, I, P, I], I),
         "egpu_host_dposv": ([H, I, I, I, I, P, I, P, I, P], I),
@@ -363,6 +365,55 @@ class Handle:
         self._bind_stream()
         m, n = B.shape[0], (B.shape[1] if B.dim() > 1 else 1)
         _check(lib().egpu_dlaswp(self._h, int(inverse), m, n, _ptr(B), _ld(B), _ptr(p), p.shape[0]))
+
+    def _batched(self, fn, As, Bs):
+        self._bind_stream()
+        cnt = len(As)
+        IA = ctypes.c_int * cnt
+        PA = ctypes.c_void_p * cnt
+        n = IA(*[a.shape[0] for a in As])
+        lda = IA(*[_ld(a) for a in As])
+        ptrA = PA(*[a.data_ptr() for a in As])
+        if Bs is not None:
+            nr = IA(*[(b.shape[1] if b.dim() > 1 else 1) for b in Bs])
+            ldb = IA(*[_ld(b) for b in Bs])
+            ptrB = PA(*[b.data_ptr() for b in Bs])
+        else:
+            nr = IA(*([0] * cnt))
+            ldb = IA(*([1] * cnt))
+            ptrB = None
+        info = IA()
+        _check(fn(self._h, cnt, n, nr, ptrA, lda, ptrB, ldb, info))
+        return list(info)
+
+    def gaussian_elimination_batched(self, As, Bs):
+        """Batched GaussianElimination (LU with partial pivoting + solve), n <= 512,
+        nrhs <= 16, one persistent launch.  Returns per-system info (0 or the
+        1-based column of an exact zero pivot)."""
+        return self._batched(lib().egpu_dgesv_batched, As, Bs)
+
+    def hpd_solve_batched(self, As, Bs=None):
+        """Batched HPDSolve(LOWER) over lists of column-major CUDA tensors (n <= 512,
+        nrhs <= 16) in one persistent launch.  Returns the per-system info list
+        (0, or the 1-based column where that system stopped being HPD)."""
+        self._bind_stream()
+        cnt = len(As)
+        IA = ctypes.c_int * cnt
+        PA = ctypes.c_void_p * cnt
+        n = IA(*[a.shape[0] for a in As])
+        lda = IA(*[_ld(a) for a in As])
+        ptrA = PA(*[a.data_ptr() for a in As])
+        if Bs is not None:
+            nr = IA(*[(b.shape[1] if b.dim() > 1 else 1) for b in Bs])
+            ldb = IA(*[_ld(b) for b in Bs])
+            ptrB = PA(*[b.data_ptr() for b in Bs])
+        else:
+            nr = IA(*([0] * cnt))
+            ldb = IA(*([1] * cnt))
+            ptrB = None
+        info = IA()
+        _check(lib().egpu_dposv_batched(self._h, cnt, n, nr, ptrA, lda, ptrB, ldb, info))
+        return list(info)
 
     # ---------------- host API (numpy, Fortran order, in place) --------
     def host_cholesky(self, A: np.ndarray, uplo=LOWER):

@@ -897,6 +897,28 @@ int egpu_dgesv(egpu_handle h, int n, int nrhs, double* dA, int lda, double* dB, 
   return rc != EGPU_OK ? rc : rc2;
 }
 
+int egpu_dposv_batched(egpu_handle h, int count, const int* n, const int* nrhs, double* const* dA, const int* lda,
+                       double* const* dB, const int* ldb, int* info) {
+  TRY(check_handle(h));
+  if (count < 0 || (count > 0 && (!n || !nrhs || !dA || !lda || !info))) return EGPU_ERR_ARG;
+  if (count == 0) return EGPU_OK;
+  Enter g(h);
+  TRY(ensure_ws(h, egpu_batched_ws_bytes(count, h->sm_count) + 4096));
+  return egpu_batched_launch(0, h->stream, h->sm_count, count, n, nrhs, dA, lda, dB, ldb, h->ws, h->ws_bytes,
+                             info);
+}
+
+int egpu_dgesv_batched(egpu_handle h, int count, const int* n, const int* nrhs, double* const* dA, const int* lda,
+                       double* const* dB, const int* ldb, int* info) {
+  TRY(check_handle(h));
+  if (count < 0 || (count > 0 && (!n || !nrhs || !dA || !lda || !info))) return EGPU_ERR_ARG;
+  if (count == 0) return EGPU_OK;
+  Enter g(h);
+  TRY(ensure_ws(h, egpu_batched_ws_bytes(count, h->sm_count) + 4096));
+  return egpu_batched_launch(1, h->stream, h->sm_count, count, n, nrhs, dA, lda, dB, ldb, h->ws, h->ws_bytes,
+                             info);
+}
+
 int egpu_dtrsm(egpu_handle h, int side, int uplo, int orient, int diag, int m, int n, double alpha,
                const double* dA, int lda, double* dB, int ldb) {
   TRY(check_handle(h));

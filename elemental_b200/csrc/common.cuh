@@ -94,6 +94,40 @@ __device__ __forceinline__ void dmma_16x8x8(double (&d)[4], const double (&a)[4]
       : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(b[0]), "d"(b[1]));
 }
 
+// ------------------------------------------------------------- cp.async --
+// 8-byte asynchronous global->shared copy (no register staging, so a thread can
+// have many loads in flight); cp_async_wait_all() waits for this thread's.
+__device__ __forceinline__ void cp_async8(void* smem_dst, const void* gmem_src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_u32(smem_dst)), "l"(gmem_src) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+// 16-byte form that bypasses L1 (.cg): for data other CTAs may have written
+// since this SM last cached it (L1 is not coherent).  Both addresses 16-byte aligned.
+__device__ __forceinline__ void cp_async16_cg(void* smem_dst, const void* gmem_src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(smem_dst)), "l"(gmem_src) : "memory");
+}
+
+// -------------------------------------------------------------- cluster --
+__device__ __forceinline__ void cluster_arrive_release() {
+  asm volatile("barrier.cluster.arrive.release.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void cluster_wait_acquire() {
+  asm volatile("barrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+__device__ __forceinline__ unsigned cluster_ctarank() {
+  unsigned r;
+  asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+  return r;
+}
+// Generic address of the same shared-memory object in CTA `rank` of the cluster.
+template <class T>
+__device__ __forceinline__ T* cluster_map(T* p, unsigned rank) {
+  uint64_t out;
+  asm volatile("mapa.u64 %0, %1, %2;" : "=l"(out) : "l"(reinterpret_cast<uint64_t>(p)), "r"(rank));
+  return reinterpret_cast<T*>(out);
+}
+
+
 // ------------------------------------------------------------ grid sync --
 // Bounded grid-wide barrier over `nblocks` co-resident CTAs (cooperative
 // launch).  `counter` is a monotonically increasing arrival counter in

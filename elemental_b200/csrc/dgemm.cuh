@@ -133,6 +133,17 @@ __global__ void __launch_bounds__(32 * WARPS_M * WARPS_N, (WARPS_M * WARPS_N <= 
 
   if (tid == 0)
     for (int kt = 0; kt < kStages && kt < KT; ++kt) issue(kt);
+  // Pull this tile of C into L2 while the main loop runs, so the epilogue's
+  // read-modify-write does not wait on HBM (one bulk prefetch per column).
+  if (p.beta != 0.0 && p.cvec) {
+    const int nrow = min(BM, p.M - row0);
+    const int ncol = min(BN, p.N - col0);
+    const unsigned bytes = (unsigned)((nrow * 8) & ~15);  // never past the column's end
+    for (int c = tid; c < ncol && bytes > 0; c += S::kThreads) {
+      const double* src = p.C + (long long)(col0 + c) * p.ldc + row0;
+      asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src), "r"(bytes) : "memory");
+    }
+  }
 
   double acc[4][4][4];
 #pragma unroll

@@ -1,0 +1,411 @@
+// Shared-memory building blocks for nb x nb diagonal blocks (nb <= 128):
+// blocked Cholesky, triangular inverse and register-blocked mini-GEMMs.
+#pragma once
+#include "internal.h"
+
+namespace egpu {
+
+// ---------------------------------------------------------------------------
+// Diagonal-block kernels.  The nb x nb block (nb <= 128) lives in shared
+// memory with leading dimension kLDS = 129 (odd: row and column sweeps are
+// both bank-conflict free), always as a LOWER triangle (an upper triangle is
+// handled as the lower triangle of its transpose: UVar3Unb and LVar3Unb
+// perform the same operations on A and A^T).
+//
+// Factorization: 16-column sub-panels.  Inside a sub-panel every column costs
+// one barrier: all threads read a_jj, each updates its share of the
+// sub-panel columns with  a_ik -= a_ij a_kj / a_jj  (the rank-1 update of
+// LVar3Unb, Cholesky/LVar3.hpp:40-46, applied before the column is scaled),
+// and the previous column is scaled by 1/sqrt(a_jj) in the same phase (no
+// thread reads it any more).  After the sub-panel, the trailing triangle is
+// updated by a register-blocked shared-memory mini-GEMM (4x4 per thread).
+// The inverse of the factor is built the same way: 16 x 16 diagonal blocks
+// inverted in parallel (one per warp), then block columns from the right,
+// X21 = -inv(L22) (L21 X11), with 4x4-blocked mini-GEMMs.
+// All loops are rolled: straight-line unrolled code run by one warp stalls
+// on instruction fetch.
+constexpr int kLDS = 129;
+constexpr int kSP = 16;  // sub-panel width
+constexpr int kDiagSmemBase = (128 * kLDS + 128) * (int)sizeof(double);
+
+__device__ __forceinline__ double& SE(double* S, int r, int c) { return S[r + c * kLDS]; }
+
+// C[r0.., c0..] (nr x nc, lower part r >= c when tri) -= A[r0.., k0..k0+K) * B[c0.., k0..k0+K)^T
+// reading A and B from S; 4x4 register tiles per thread.  sign = +1 or -1 for
+// "-=" or "+=" (the inverse uses the opposite sign).
+__device__ inline void smem_syrk_tiles(double* S, int r0, int nr, int c0, int nc, int k0, int K, bool tri) {
+  const int tr = (nr + 3) / 4, tc = (nc + 3) / 4;
+  for (int t = threadIdx.x; t < tr * tc; t += blockDim.x) {
+    const int ti = t % tr, tj = t / tr;
+    const int rb = r0 + 4 * ti, cb = c0 + 4 * tj;
+    if (tri && rb + 3 < cb) continue;  // tile strictly above the diagonal
+    double acc[4][4];
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int b = 0; b < 4; ++b) acc[a][b] = 0.0;
+    for (int k = k0; k < k0 + K; ++k) {
+      double x[4], y[4];
+#pragma unroll
+      for (int a = 0; a < 4; ++a) {
+        x[a] = (rb + a < r0 + nr) ? SE(S, rb + a, k) : 0.0;
+        y[a] = (cb + a < c0 + nc) ? SE(S, cb + a, k) : 0.0;
+      }
+#pragma unroll
+      for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) acc[a][b] = fma(x[a], y[b], acc[a][b]);
+    }
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int b = 0; b < 4; ++b) {
+        const int r = rb + a, c = cb + b;
+        if (r < r0 + nr && c < c0 + nc && (!tri || r >= c)) SE(S, r, c) -= acc[a][b];
+      }
+  }
+}
+
+// Lower Cholesky of the b x b block in S.  Returns 0 or the 1-based column
+// of a non-positive pivot ("A was not numerically HPD", LVar3.hpp:37-38); the
+// decision is uniform across the block (every thread reads the same a_jj).
+__device__ inline int smem_chol(double* S, int b) {
+  __shared__ double s_alpha[128];
+  const int tid = threadIdx.x;
+  const int row = tid & 127, half = tid >> 7;  // two threads per row
+  for (int c0 = 0; c0 < b; c0 += kSP) {
+    const int c1 = min(b, c0 + kSP);
+    for (int j = c0; j < c1; ++j) {
+      const double ajj = SE(S, j, j);
+      if (ajj <= 0.0) return j + 1;
+      if (tid == 0) s_alpha[j] = sqrt(ajj);
+      // column j-1 is read by nobody in this phase: scale it now
+      if (j > c0 && half == 1 && row >= j && row < b) SE(S, row, j - 1) /= s_alpha[j - 1];
+      if (row > j && row < b) {
+        const double lij = SE(S, row, j) / ajj;
+        for (int k = j + 1 + half; k < c1 && k <= row; k += 2) SE(S, row, k) -= lij * SE(S, k, j);
+      }
+      __syncthreads();
+    }
+    if (half == 0 && row >= c1 && row < b) SE(S, row, c1 - 1) /= s_alpha[c1 - 1];
+    if (half == 1 && row >= c0 && row < c1) SE(S, row, row) = s_alpha[row];
+    __syncthreads();
+    if (c1 < b) {
+      smem_syrk_tiles(S, c1, b - c1, c1, b - c1, c0, c1 - c0, true);
+      __syncthreads();
+    }
+  }
+  return 0;
+}
+
+// In-place inverse of the lower b x b triangle in S (unit: diagonal taken as 1
+// and written as 1).  Uses Xs (16 x 16 scratch per warp would not fit; the
+// diagonal blocks are inverted in place column by column by their warp).
+__device__ inline void smem_trinv(double* S, int b, int unit) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int nblk = (b + kSP - 1) / kSP;
+  // 1. 16 x 16 diagonal blocks, one warp each: lane c (< 16) computes column c
+  //    of the block inverse by forward substitution, in place is impossible,
+  //    so results go to registers first, then back to S.
+  for (int blk = warp; blk < nblk; blk += blockDim.x / 32) {
+    const int o = blk * kSP, w = min(kSP, b - o);
+    double x[kSP];
+    const int c = lane;
+#pragma unroll
+    for (int i = 0; i < kSP; ++i) x[i] = 0.0;
+    if (c < w) {
+#pragma unroll
+      for (int i = 0; i < kSP; ++i) {
+        if (i < w && i >= c) {
+          double acc = (i == c) ? 1.0 : 0.0;
+#pragma unroll
+          for (int m = 0; m < kSP; ++m)
+            if (m >= c && m < i) acc = fma(-SE(S, o + i, o + m), x[m], acc);
+          x[i] = unit ? acc : acc / SE(S, o + i, o + i);
+        }
+      }
+    }
+    __syncwarp();
+    if (c < w) {
+#pragma unroll
+      for (int i = 0; i < kSP; ++i)
+        if (i < w && i >= c) SE(S, o + i, o + c) = (unit && i == c) ? 1.0 : x[i];
+    }
+  }
+  __syncthreads();
+  // 2. block columns from the right: X21 = -inv(L22) * (L21 * X11)
+  for (int blk = nblk - 2; blk >= 0; --blk) {
+    const int o = blk * kSP, w = min(kSP, b - o), r0 = o + w, R = b - r0;
+    // T = L21 * X11 (R x w), computed into registers, written over L21
+    {
+      const int tr = (R + 3) / 4;
+      double acc[4][4];
+      const int t = tid;
+      const bool act = t < tr * 4;  // tiles: 4 rows x 4 cols, w <= 16 -> 4 col tiles
+      const int ti = t % max(tr, 1), tj = t / max(tr, 1);
+#pragma unroll
+      for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) acc[a][q] = 0.0;
+      if (act) {
+        for (int k = 0; k < w; ++k) {
+#pragma unroll
+          for (int a = 0; a < 4; ++a) {
+            const int r = r0 + 4 * ti + a;
+            const double l = (r < b) ? SE(S, r, o + k) : 0.0;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+              const int cc = 4 * tj + q;
+              const double xv = (cc < w && k >= cc) ? SE(S, o + k, o + cc) : 0.0;
+              acc[a][q] = fma(l, xv, acc[a][q]);
+            }
+          }
+        }
+      }
+      __syncthreads();
+      if (act)
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            const int r = r0 + 4 * ti + a, cc = 4 * tj + q;
+            if (r < b && cc < w) SE(S, r, o + cc) = acc[a][q];
+          }
+      __syncthreads();
+      // X21 = -inv(L22) * T : row r of X21 = -sum_{m <= r} X22[r, m] T[m, :]
+      if (act) {
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+          for (int q = 0; q < 4; ++q) acc[a][q] = 0.0;
+        const int rmax = min(b - 1, r0 + 4 * ti + 3);
+        for (int m = r0; m <= rmax; ++m) {
+          double tv[4];
+#pragma unroll
+          for (int q = 0; q < 4; ++q) tv[q] = (4 * tj + q < w) ? SE(S, m, o + 4 * tj + q) : 0.0;
+#pragma unroll
+          for (int a = 0; a < 4; ++a) {
+            const int r = r0 + 4 * ti + a;
+            const double xv = (r < b && m <= r) ? (unit && m == r ? 1.0 : SE(S, r, m)) : 0.0;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) acc[a][q] = fma(xv, tv[q], acc[a][q]);
+          }
+        }
+      }
+      __syncthreads();
+      if (act)
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            const int r = r0 + 4 * ti + a, cc = 4 * tj + q;
+            if (r < b && cc < w) SE(S, r, o + cc) = -acc[a][q];
+          }
+      __syncthreads();
+    }
+  }
+}
+
+
+// ---------------------------------------------------------------------------
+// DMMA building blocks on shared-memory operands (all column-major).
+//
+// C = alpha * A * op(B) + beta * C for M % 16 == 0, N % 8 == 0, K % 8 == 0.
+// A_LOWER: A[r][k] = 0 for k > r.  B_TRANS: op(B)[k][c] = B[c][k] (B stored
+// N x K).  B_LOWER: op(B)[k][c] = 0 for c > k.  C_LOWER: only r >= c is
+// written.  C must not alias A or B.  All warps of the CTA share the 16x8
+// output tiles; the caller synchronises afterwards.
+template <bool A_LOWER, bool B_TRANS, bool B_LOWER, bool C_LOWER>
+__device__ inline void smem_dmma_gemm(const double* A, int lda, const double* B, int ldb, double* C, int ldc,
+                                      int M, int N, int K, double alpha, double beta) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int g = lane >> 2, t = lane & 3;
+  const int tm = M / 16, tn = N / 8;
+  for (int tile = warp; tile < tm * tn; tile += nw) {
+    const int r0 = (tile % tm) * 16, c0 = (tile / tm) * 8;
+    if (C_LOWER && r0 + 15 < c0) continue;
+    double acc[4] = {0.0, 0.0, 0.0, 0.0};
+    const int kend = A_LOWER ? min(K, r0 + 16) : K;  // A is zero right of its diagonal
+    const int kbeg = B_LOWER ? (c0 / 8) * 8 : 0;      // op(B) is zero above its diagonal
+    for (int k0 = kbeg; k0 < kend; k0 += 8) {
+      double a[4], b[2];
+      const int ka = k0 + t, kb = k0 + t + 4;
+      const int ra = r0 + g, rb = r0 + g + 8;
+      a[0] = (!A_LOWER || ka <= ra) ? A[ra + ka * lda] : 0.0;
+      a[1] = (!A_LOWER || ka <= rb) ? A[rb + ka * lda] : 0.0;
+      a[2] = (!A_LOWER || kb <= ra) ? A[ra + kb * lda] : 0.0;
+      a[3] = (!A_LOWER || kb <= rb) ? A[rb + kb * lda] : 0.0;
+      const int cc = c0 + g;
+      b[0] = (!B_LOWER || cc <= ka) ? (B_TRANS ? B[cc + ka * ldb] : B[ka + cc * ldb]) : 0.0;
+      b[1] = (!B_LOWER || cc <= kb) ? (B_TRANS ? B[cc + kb * ldb] : B[kb + cc * ldb]) : 0.0;
+      dmma_16x8x8(acc, a, b);
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int r = r0 + g + ((q >= 2) ? 8 : 0), c = c0 + 2 * t + (q & 1);
+      if (C_LOWER && r < c) continue;
+      double* cp = C + r + c * ldc;
+      *cp = (beta == 0.0) ? alpha * acc[q] : fma(alpha, acc[q], beta * *cp);
+    }
+  }
+}
+
+// Cholesky of one 16 x 16 lower block at S[o.., o..] by one warp, rows in
+// registers (lane i < 16 holds row i), pivots broadcast by shuffles; then the
+// inverse of the factor into X (16 x 16, ld ldx) and the factor back into S.
+// The diagonal uses 1/sqrt(a_jj): a_jj * r = sqrt(a_jj), a_ij * r = l_ij.
+// Returns 0 or the 1-based column of a non-positive pivot (warp-uniform).
+__device__ inline int warp_chol16(double* S, int lds, int o, double* X, int ldx) {
+  const int lane = threadIdx.x & 31;
+  const bool act = lane < 16;
+  double d[16];
+#pragma unroll
+  for (int k = 0; k < 16; ++k) d[k] = (act && k <= lane) ? S[(o + lane) + (o + k) * lds] : 0.0;
+  int fail = 0;
+#pragma unroll
+  for (int j = 0; j < 16; ++j) {
+    const double djj = __shfl_sync(0xffffffffu, d[j], j);
+    if (!fail) {
+      if (djj <= 0.0) {
+        fail = j + 1;
+      } else {
+        const double r = rsqrt(djj);
+        d[j] *= r;  // lane j: sqrt(a_jj); lanes > j: l_ij
+        const double lj = d[j];
+#pragma unroll
+        for (int k = j + 1; k < 16; ++k) {
+          const double lkj = __shfl_sync(0xffffffffu, lj, k);
+          if (lane >= k) d[k] = fma(-lj, lkj, d[k]);
+        }
+      }
+    }
+  }
+  if (fail) return fail;
+#pragma unroll
+  for (int k = 0; k < 16; ++k)
+    if (act && k <= lane) S[(o + lane) + (o + k) * lds] = d[k];
+  // X = inv(L): lane c computes column c
+  double x[16];
+#pragma unroll
+  for (int k = 0; k < 16; ++k) {
+    double acc = (k == lane) ? 1.0 : 0.0;
+#pragma unroll
+    for (int m = 0; m < k; ++m) acc = fma(-__shfl_sync(0xffffffffu, d[m], k), x[m], acc);
+    const double lkk = __shfl_sync(0xffffffffu, d[k], k);
+    x[k] = (k >= lane) ? acc / lkk : 0.0;
+  }
+#pragma unroll
+  for (int k = 0; k < 16; ++k)
+    if (act) X[k + lane * ldx] = x[k];
+  return 0;
+}
+
+// Inverse of one 16 x 16 lower block at S[o.., o..] (unit: diagonal taken as
+// 1) by one warp, into X (ld ldx).
+__device__ inline void warp_trinv16(const double* S, int lds, int o, int unit, double* X, int ldx) {
+  const int lane = threadIdx.x & 31;
+  const bool act = lane < 16;
+  double d[16];
+#pragma unroll
+  for (int k = 0; k < 16; ++k) {
+    double v = (act && k <= lane) ? S[(o + lane) + (o + k) * lds] : 0.0;
+    if (unit && k == lane) v = 1.0;
+    d[k] = v;
+  }
+  double x[16];
+#pragma unroll
+  for (int k = 0; k < 16; ++k) {
+    double acc = (k == lane) ? 1.0 : 0.0;
+#pragma unroll
+    for (int m = 0; m < k; ++m) acc = fma(-__shfl_sync(0xffffffffu, d[m], k), x[m], acc);
+    const double lkk = __shfl_sync(0xffffffffu, d[k], k);
+    x[k] = (k >= lane) ? (unit ? acc : acc / lkk) : 0.0;
+  }
+#pragma unroll
+  for (int k = 0; k < 16; ++k)
+    if (act) X[k + lane * ldx] = x[k];
+}
+
+// Temporary area of the DMMA diagonal kernels: 16 leaf inverses (ld 17) and
+// one 64 x 64 product buffer (ld 68).
+constexpr int kLeafLD = 17;
+constexpr int kTmpLD = 68;
+constexpr int kDiagTmpDoubles = 8 * 16 * kLeafLD + 64 * kTmpLD;
+constexpr int kDiagSmem = kDiagSmemBase + kDiagTmpDoubles * (int)sizeof(double);
+
+// Pad the lower b x b triangle in S to bp = round_up(b, 16) with identity.
+__device__ inline int pad16_identity(double* S, int b) {
+  const int bp = (b + 15) & ~15;
+  for (int e = threadIdx.x; e < (bp - b) * bp; e += blockDim.x) {
+    const int r = b + e / bp, c = e % bp;  // rows b..bp-1, all columns
+    if (r >= c) S[r + c * kLDS] = (r == c) ? 1.0 : 0.0;
+  }
+  return bp;
+}
+
+// In-place inverse of the lower bp x bp triangle in S (bp a multiple of 16,
+// padded with identity), given the inverses of its 16 x 16 diagonal blocks in
+// Xl (block q at Xl + q*16*kLeafLD).  Levels of doubling block size:
+//   inv([[A, 0], [B, C]]) = [[Ai, 0], [-Ci B Ai, Ci]],  T = B Ai, X21 = -Ci T.
+__device__ inline void smem_trinv_dmma(double* S, int bp, const double* Xl, double* T) {
+  // leaves into place
+  const int nleaf = bp / 16;
+  for (int e = threadIdx.x; e < nleaf * 256; e += blockDim.x) {
+    const int q = e >> 8, i = (e >> 4) & 15, k = e & 15;
+    if (i >= k) S[(16 * q + i) + (16 * q + k) * kLDS] = Xl[q * 16 * kLeafLD + i + k * kLeafLD];
+  }
+  __syncthreads();
+  for (int s = 16; s < bp; s *= 2) {
+    for (int o = 0; o + s < bp; o += 2 * s) {
+      const int s2 = min(s, bp - o - s);
+      // T = B * Ai   (s2 x s), B = S[o+s.., o..], Ai = S[o.., o..] lower
+      smem_dmma_gemm<false, false, true, false>(S + (o + s) + o * kLDS, kLDS, S + o + o * kLDS, kLDS, T, kTmpLD,
+                                                s2, s, s, 1.0, 0.0);
+      __syncthreads();
+      // X21 = -Ci * T  (s2 x s), Ci = S[o+s.., o+s..] lower
+      smem_dmma_gemm<true, false, false, false>(S + (o + s) + (o + s) * kLDS, kLDS, T, kTmpLD,
+                                                S + (o + s) + o * kLDS, kLDS, s2, s, s2, -1.0, 0.0);
+      __syncthreads();
+    }
+  }
+}
+
+// Lower Cholesky of the bp x bp block in S (bp a multiple of 16; the caller
+// pads with identity) in 16-column steps: warp 0 factors the 16 x 16 diagonal
+// block and inverts it (Xl), all warps form L21 = A21 X11^T and the trailing
+// update A22 -= L21 L21^T on the tensor cores.  Returns 0 or the 1-based column
+// of a non-positive pivot (uniform).
+__device__ inline int smem_chol_dmma(double* S, int bp, double* Xl, double* T) {
+  __shared__ int s_fail;
+  for (int o = 0; o < bp; o += 16) {
+    double* X11 = Xl + (o / 16) * 16 * kLeafLD;
+    if (threadIdx.x < 32) {
+      const int f = warp_chol16(S, kLDS, o, X11, kLeafLD);
+      if (threadIdx.x == 0) s_fail = f ? o + f : 0;
+    }
+    __syncthreads();
+    if (s_fail) return s_fail;
+    const int m2 = bp - o - 16;
+    if (m2 > 0) {
+      // L21 = A21 * X11^T into T (m2 x 16), then back into S
+      for (int r0 = 0; r0 < m2; r0 += 64) {
+        const int mr = min(64, m2 - r0);
+        smem_dmma_gemm<false, true, false, false>(S + (o + 16 + r0) + o * kLDS, kLDS, X11, kLeafLD, T, kTmpLD,
+                                                  mr, 16, 16, 1.0, 0.0);
+        __syncthreads();
+        for (int e = threadIdx.x; e < mr * 16; e += blockDim.x) {
+          const int r = e % mr, c = e / mr;
+          S[(o + 16 + r0 + r) + (o + c) * kLDS] = T[r + c * kTmpLD];
+        }
+        __syncthreads();
+      }
+      // A22 -= L21 L21^T (lower part)
+      smem_dmma_gemm<false, true, false, true>(S + (o + 16) + o * kLDS, kLDS, S + (o + 16) + o * kLDS, kLDS,
+                                               S + (o + 16) + (o + 16) * kLDS, kLDS, m2, m2, 16, -1.0, 1.0);
+      __syncthreads();
+    }
+  }
+  return 0;
+}
+
+}  // namespace egpu

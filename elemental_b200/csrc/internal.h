@@ -66,6 +66,13 @@ int launch_laswp_seq(cudaStream_t st, int inverse, int m, int n, double* A, long
 int launch_getrf_diag_nopiv(cudaStream_t st, double* A, long long lda, int b, double* W, int ldw, double* W2,
                             DevStatus* status, int col_base);
 
+// Batched (one persistent launch) HPDSolve, lower, n <= 512, nrhs <= 16.
+size_t egpu_batched_ws_bytes(int count, int sm_count);
+// kind 0: HPDSolve (lower Cholesky + solve); kind 1: GaussianElimination (LU + solve)
+int egpu_batched_launch(int kind, cudaStream_t st, int sm_count, int count, const int* n, const int* nrhs,
+                        double* const* A, const int* lda, double* const* B, const int* ldb, void* ws,
+                        size_t ws_bytes, int* info_host);
+
 // Copy between strided device matrices.
 int launch_copy(cudaStream_t st, int m, int n, const double* src, long long lds, double* dst, long long ldd);
 

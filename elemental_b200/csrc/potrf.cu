@@ -1,6 +1,7 @@
 // Diagonal-block kernels: unblocked Cholesky / LU of one nb x nb block held in
 // shared memory, and triangular inverses of diagonal blocks (the trsm sweeps
 // multiply by these inverses on the tensor cores).
+#include "diag_common.cuh"
 #include "internal.h"
 
 namespace egpu {
@@ -46,207 +47,6 @@ __device__ void tri_inverse_smem(double* S, int b, int uplo, int unit) {
   }
 }
 
-// ---------------------------------------------------------------------------
-// Diagonal-block kernels.  The nb x nb block (nb <= 128) lives in shared
-// memory with leading dimension kLDS = 129 (odd: row and column sweeps are
-// both bank-conflict free), always as a LOWER triangle (an upper triangle is
-// handled as the lower triangle of its transpose: UVar3Unb and LVar3Unb
-// perform the same operations on A and A^T).
-//
-// Factorization: 16-column sub-panels.  Inside a sub-panel every column costs
-// one barrier: all threads read a_jj, each updates its share of the
-// sub-panel columns with  a_ik -= a_ij a_kj / a_jj  (the rank-1 update of
-// LVar3Unb, Cholesky/LVar3.hpp:40-46, applied before the column is scaled),
-// and the previous column is scaled by 1/sqrt(a_jj) in the same phase (no
-// thread reads it any more).  After the sub-panel, the trailing triangle is
-// updated by a register-blocked shared-memory mini-GEMM (4x4 per thread).
-// The inverse of the factor is built the same way: 16 x 16 diagonal blocks
-// inverted in parallel (one per warp), then block columns from the right,
-// X21 = -inv(L22) (L21 X11), with 4x4-blocked mini-GEMMs.
-// All loops are rolled: straight-line unrolled code run by one warp stalls
-// on instruction fetch.
-constexpr int kLDS = 129;
-constexpr int kSP = 16;  // sub-panel width
-constexpr int kDiagSmem = (128 * kLDS + 128) * (int)sizeof(double);
-
-__device__ __forceinline__ double& SE(double* S, int r, int c) { return S[r + c * kLDS]; }
-
-// C[r0.., c0..] (nr x nc, lower part r >= c when tri) -= A[r0.., k0..k0+K) * B[c0.., k0..k0+K)^T
-// reading A and B from S; 4x4 register tiles per thread.  sign = +1 or -1 for
-// "-=" or "+=" (the inverse uses the opposite sign).
-__device__ void smem_syrk_tiles(double* S, int r0, int nr, int c0, int nc, int k0, int K, bool tri) {
-  const int tr = (nr + 3) / 4, tc = (nc + 3) / 4;
-  for (int t = threadIdx.x; t < tr * tc; t += blockDim.x) {
-    const int ti = t % tr, tj = t / tr;
-    const int rb = r0 + 4 * ti, cb = c0 + 4 * tj;
-    if (tri && rb + 3 < cb) continue;  // tile strictly above the diagonal
-    double acc[4][4];
-#pragma unroll
-    for (int a = 0; a < 4; ++a)
-#pragma unroll
-      for (int b = 0; b < 4; ++b) acc[a][b] = 0.0;
-    for (int k = k0; k < k0 + K; ++k) {
-      double x[4], y[4];
-#pragma unroll
-      for (int a = 0; a < 4; ++a) {
-        x[a] = (rb + a < r0 + nr) ? SE(S, rb + a, k) : 0.0;
-        y[a] = (cb + a < c0 + nc) ? SE(S, cb + a, k) : 0.0;
-      }
-#pragma unroll
-      for (int a = 0; a < 4; ++a)
-#pragma unroll
-        for (int b = 0; b < 4; ++b) acc[a][b] = fma(x[a], y[b], acc[a][b]);
-    }
-#pragma unroll
-    for (int a = 0; a < 4; ++a)
-#pragma unroll
-      for (int b = 0; b < 4; ++b) {
-        const int r = rb + a, c = cb + b;
-        if (r < r0 + nr && c < c0 + nc && (!tri || r >= c)) SE(S, r, c) -= acc[a][b];
-      }
-  }
-}
-
-// Lower Cholesky of the b x b block in S.  Returns 0 or the 1-based column
-// of a non-positive pivot ("A was not numerically HPD", LVar3.hpp:37-38); the
-// decision is uniform across the block (every thread reads the same a_jj).
-__device__ int smem_chol(double* S, int b) {
-  __shared__ double s_alpha[128];
-  const int tid = threadIdx.x;
-  const int row = tid & 127, half = tid >> 7;  // two threads per row
-  for (int c0 = 0; c0 < b; c0 += kSP) {
-    const int c1 = min(b, c0 + kSP);
-    for (int j = c0; j < c1; ++j) {
-      const double ajj = SE(S, j, j);
-      if (ajj <= 0.0) return j + 1;
-      if (tid == 0) s_alpha[j] = sqrt(ajj);
-      // column j-1 is read by nobody in this phase: scale it now
-      if (j > c0 && half == 1 && row >= j && row < b) SE(S, row, j - 1) /= s_alpha[j - 1];
-      if (row > j && row < b) {
-        const double lij = SE(S, row, j) / ajj;
-        for (int k = j + 1 + half; k < c1 && k <= row; k += 2) SE(S, row, k) -= lij * SE(S, k, j);
-      }
-      __syncthreads();
-    }
-    if (half == 0 && row >= c1 && row < b) SE(S, row, c1 - 1) /= s_alpha[c1 - 1];
-    if (half == 1 && row >= c0 && row < c1) SE(S, row, row) = s_alpha[row];
-    __syncthreads();
-    if (c1 < b) {
-      smem_syrk_tiles(S, c1, b - c1, c1, b - c1, c0, c1 - c0, true);
-      __syncthreads();
-    }
-  }
-  return 0;
-}
-
-// In-place inverse of the lower b x b triangle in S (unit: diagonal taken as 1
-// and written as 1).  Uses Xs (16 x 16 scratch per warp would not fit; the
-// diagonal blocks are inverted in place column by column by their warp).
-__device__ void smem_trinv(double* S, int b, int unit) {
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int nblk = (b + kSP - 1) / kSP;
-  // 1. 16 x 16 diagonal blocks, one warp each: lane c (< 16) computes column c
-  //    of the block inverse by forward substitution, in place is impossible,
-  //    so results go to registers first, then back to S.
-  for (int blk = warp; blk < nblk; blk += blockDim.x / 32) {
-    const int o = blk * kSP, w = min(kSP, b - o);
-    double x[kSP];
-    const int c = lane;
-#pragma unroll
-    for (int i = 0; i < kSP; ++i) x[i] = 0.0;
-    if (c < w) {
-#pragma unroll
-      for (int i = 0; i < kSP; ++i) {
-        if (i < w && i >= c) {
-          double acc = (i == c) ? 1.0 : 0.0;
-#pragma unroll
-          for (int m = 0; m < kSP; ++m)
-            if (m >= c && m < i) acc = fma(-SE(S, o + i, o + m), x[m], acc);
-          x[i] = unit ? acc : acc / SE(S, o + i, o + i);
-        }
-      }
-    }
-    __syncwarp();
-    if (c < w) {
-#pragma unroll
-      for (int i = 0; i < kSP; ++i)
-        if (i < w && i >= c) SE(S, o + i, o + c) = (unit && i == c) ? 1.0 : x[i];
-    }
-  }
-  __syncthreads();
-  // 2. block columns from the right: X21 = -inv(L22) * (L21 * X11)
-  for (int blk = nblk - 2; blk >= 0; --blk) {
-    const int o = blk * kSP, w = min(kSP, b - o), r0 = o + w, R = b - r0;
-    // T = L21 * X11 (R x w), computed into registers, written over L21
-    {
-      const int tr = (R + 3) / 4;
-      double acc[4][4];
-      const int t = tid;
-      const bool act = t < tr * 4;  // tiles: 4 rows x 4 cols, w <= 16 -> 4 col tiles
-      const int ti = t % max(tr, 1), tj = t / max(tr, 1);
-#pragma unroll
-      for (int a = 0; a < 4; ++a)
-#pragma unroll
-        for (int q = 0; q < 4; ++q) acc[a][q] = 0.0;
-      if (act) {
-        for (int k = 0; k < w; ++k) {
-#pragma unroll
-          for (int a = 0; a < 4; ++a) {
-            const int r = r0 + 4 * ti + a;
-            const double l = (r < b) ? SE(S, r, o + k) : 0.0;
-#pragma unroll
-            for (int q = 0; q < 4; ++q) {
-              const int cc = 4 * tj + q;
-              const double xv = (cc < w && k >= cc) ? SE(S, o + k, o + cc) : 0.0;
-              acc[a][q] = fma(l, xv, acc[a][q]);
-            }
-          }
-        }
-      }
-      __syncthreads();
-      if (act)
-#pragma unroll
-        for (int a = 0; a < 4; ++a)
-#pragma unroll
-          for (int q = 0; q < 4; ++q) {
-            const int r = r0 + 4 * ti + a, cc = 4 * tj + q;
-            if (r < b && cc < w) SE(S, r, o + cc) = acc[a][q];
-          }
-      __syncthreads();
-      // X21 = -inv(L22) * T : row r of X21 = -sum_{m <= r} X22[r, m] T[m, :]
-      if (act) {
-#pragma unroll
-        for (int a = 0; a < 4; ++a)
-#pragma unroll
-          for (int q = 0; q < 4; ++q) acc[a][q] = 0.0;
-        const int rmax = min(b - 1, r0 + 4 * ti + 3);
-        for (int m = r0; m <= rmax; ++m) {
-          double tv[4];
-#pragma unroll
-          for (int q = 0; q < 4; ++q) tv[q] = (4 * tj + q < w) ? SE(S, m, o + 4 * tj + q) : 0.0;
-#pragma unroll
-          for (int a = 0; a < 4; ++a) {
-            const int r = r0 + 4 * ti + a;
-            const double xv = (r < b && m <= r) ? (unit && m == r ? 1.0 : SE(S, r, m)) : 0.0;
-#pragma unroll
-            for (int q = 0; q < 4; ++q) acc[a][q] = fma(xv, tv[q], acc[a][q]);
-          }
-        }
-      }
-      __syncthreads();
-      if (act)
-#pragma unroll
-        for (int a = 0; a < 4; ++a)
-#pragma unroll
-          for (int q = 0; q < 4; ++q) {
-            const int r = r0 + 4 * ti + a, cc = 4 * tj + q;
-            if (r < b && cc < w) SE(S, r, o + cc) = -acc[a][q];
-          }
-      __syncthreads();
-    }
-  }
-}
-
 // Cholesky of the b x b diagonal block (cholesky::LVar3Unb,
 // lapack-like/Cholesky/LVar3.hpp:19-49, or UVar3Unb, Cholesky/UVar3.hpp:21-50),
 // then the inverse of the factor into W (other triangle zeroed).
@@ -256,11 +56,17 @@ __global__ void __launch_bounds__(kDiagThreads) potrf_diag_kernel(double* A, lon
   extern __shared__ double S[];
   if (st != nullptr && st->code != 0) return;
   const int tid = threadIdx.x;
+  // all loads in flight at once (a plain load loop waits ~one memory latency per column)
   for (int c = 0; c < b; ++c)
     for (int r = c + tid; r < b; r += kDiagThreads)
-      SE(S, r, c) = (UPLO == EGPU_LOWER) ? A[r + (long long)c * lda] : A[c + (long long)r * lda];
+      cp_async8(&SE(S, r, c), (UPLO == EGPU_LOWER) ? &A[r + (long long)c * lda] : &A[c + (long long)r * lda]);
+  cp_async_wait_all();
   __syncthreads();
-  const int f = smem_chol(S, b);
+  double* Xl = S + 128 * kLDS + 128;
+  double* T = Xl + 8 * 16 * kLeafLD;
+  const int bp = pad16_identity(S, b);
+  __syncthreads();
+  const int f = smem_chol_dmma(S, bp, Xl, T);
   if (f) {
     if (tid == 0) set_status(st, kNotHPD, col_base + f);
     return;
@@ -271,7 +77,7 @@ __global__ void __launch_bounds__(kDiagThreads) potrf_diag_kernel(double* A, lon
       else A[c + (long long)r * lda] = SE(S, r, c);
     }
   __syncthreads();
-  smem_trinv(S, b, 0);
+  smem_trinv_dmma(S, bp, Xl, T);
   for (int c = 0; c < b; ++c)
     for (int r = tid; r < b; r += kDiagThreads) {
       const double v = (r >= c) ? SE(S, r, c) : 0.0;
@@ -322,9 +128,18 @@ __global__ void __launch_bounds__(kDiagThreads) trtri_blocks_kernel(int uplo, in
   const int tid = threadIdx.x;
   for (int c = 0; c < bb; ++c)
     for (int r = c + tid; r < bb; r += kDiagThreads)
-      SE(S, r, c) = (uplo == EGPU_LOWER) ? Ab[r + (long long)c * lda] : Ab[c + (long long)r * lda];
+      cp_async8(&SE(S, r, c), (uplo == EGPU_LOWER) ? &Ab[r + (long long)c * lda] : &Ab[c + (long long)r * lda]);
+  cp_async_wait_all();
   __syncthreads();
-  smem_trinv(S, bb, unit);
+  double* Xl = S + 128 * kLDS + 128;
+  double* T = Xl + 8 * 16 * kLeafLD;
+  const int bp = pad16_identity(S, bb);
+  __syncthreads();
+  const int warp = tid >> 5;
+  for (int q = warp; q < bp / 16; q += kDiagThreads / 32)
+    warp_trinv16(S, kLDS, 16 * q, unit, Xl + q * 16 * kLeafLD, kLeafLD);
+  __syncthreads();
+  smem_trinv_dmma(S, bp, Xl, T);
   for (int c = 0; c < b; ++c)
     for (int r = tid; r < b; r += kDiagThreads) {
       double v = 0.0;

@@ -145,6 +145,22 @@ EGPU_API int egpu_dgetrs(egpu_handle h, int orient, int n, int nrhs, const doubl
 /* GaussianElimination(A, B), lapack-like/GaussianElimination.hpp:216-232. */
 EGPU_API int egpu_dgesv(egpu_handle h, int n, int nrhs, double* dA, int lda, double* dB, int ldb, int* info);
 
+/* Batched HPDSolve(LOWER, NORMAL, A_i, B_i) (HPDSolve.hpp:18-28) for `count`
+ * independent systems of uneven orders n[i] <= 512 with nrhs[i] <= 16, in one
+ * persistent launch (one CTA per system at a time, largest first).  n, nrhs,
+ * lda, ldb, info: host arrays; dA[i], dB[i]: device pointers (dB may be NULL:
+ * factor only).  info[i] = 0, or the 1-based column where A_i stopped being
+ * numerically HPD (that system's B_i is left unsolved).  Synchronous. */
+EGPU_API int egpu_dposv_batched(egpu_handle h, int count, const int* n, const int* nrhs, double* const* dA,
+                                const int* lda, double* const* dB, const int* ldb, int* info);
+
+/* Batched GaussianElimination(A_i, B_i) (GaussianElimination.hpp:216-232) for
+ * `count` independent systems, n[i] <= 512, nrhs[i] <= 16, one persistent
+ * launch; same argument conventions as egpu_dposv_batched.  info[i] = 0 or the
+ * 1-based column of an exact zero pivot (SingularMatrixException). */
+EGPU_API int egpu_dgesv_batched(egpu_handle h, int count, const int* n, const int* nrhs, double* const* dA,
+                                const int* lda, double* const* dB, const int* ldb, int* info);
+
 /* Trsm(side, uplo, orientation, diag, alpha, A, B),
  * blas-like/level3/Trsm.hpp:49-86 (dtrsm_ at src/core/imports/blas.cpp:1203). */
 EGPU_API int egpu_dtrsm(egpu_handle h, int side, int uplo, int orient, int diag, int m, int n, double alpha,

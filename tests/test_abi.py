@@ -40,3 +40,9 @@ def test_enums_match_reference_values():
     assert (eg.NORMAL, eg.TRANSPOSE, eg.ADJOINT) == (0, 1, 2)
     assert (eg.LEFT, eg.RIGHT) == (0, 1)
     assert (eg.NON_UNIT, eg.UNIT) == (0, 1)
+
+
+def test_library_has_no_unresolved_own_symbols():
+    out = subprocess.run(["nm", "-D", eg.LIB_PATH], capture_output=True, text=True).stdout
+    undefined = [l.split()[-1] for l in out.splitlines() if " U " in l and "egpu" in l]
+    assert not undefined, undefined

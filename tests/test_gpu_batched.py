@@ -1,0 +1,76 @@
+"""Batched uneven factor-and-solve (one persistent launch) against the CPU
+oracle, system by system.  Same tolerances as the single-system parity tests:
+factors within 1e-11 * max|L| of the oracle's, solutions within 1e-9."""
+import numpy as np
+import pytest
+
+import elemental_b200 as eg
+from elemental_b200 import inputs
+from oracle import pyoracle as orc
+
+pytestmark = pytest.mark.gpu
+
+
+def test_hpd_solve_batched_uneven(handle):
+    r = inputs.rng(2024)
+    sizes = [1, 2, 31, 32, 33, 64, 127, 128, 129, 300, 511, 512] + list(r.integers(1, 513, 36))
+    nrhs = [int(x) for x in r.integers(1, 9, len(sizes))]
+    As, Bs, dA, dB = [], [], [], []
+    for i, (n, k) in enumerate(zip(sizes, nrhs)):
+        A = inputs.spd_ggt(int(n), seed=3000 + i)
+        B = inputs.normal(int(n), k, seed=4000 + i)
+        As.append(A); Bs.append(B)
+        dA.append(eg.colmajor_cuda(A)); dB.append(eg.colmajor_cuda(B))
+    info = handle.hpd_solve_batched(dA, dB)
+    assert info == [0] * len(sizes)
+    for i, (A, B) in enumerate(zip(As, Bs)):
+        F, X, st = orc.hpd_solve(A, B, orc.LOWER, nb=32)
+        assert st == 0
+        L = np.tril(dA[i].cpu().numpy())
+        assert np.max(np.abs(L - np.tril(F))) <= 1e-11 * np.max(np.abs(F)), i
+        Xg = dB[i].cpu().numpy()
+        assert np.max(np.abs(Xg - X)) <= 1e-9 * max(1.0, np.max(np.abs(X))), i
+        # upper triangle untouched
+        n = A.shape[0]
+        up = np.triu(np.ones((n, n), bool), 1)
+        assert np.array_equal(dA[i].cpu().numpy()[up], A[up])
+
+
+def test_hpd_batched_reports_failures_per_system(handle):
+    good = inputs.spd_ggt(100, 1)
+    bad = good.copy(order="F")
+    bad[70, 70] = -3.0
+    dA = [eg.colmajor_cuda(good), eg.colmajor_cuda(bad), eg.colmajor_cuda(good)]
+    dB = [eg.colmajor_cuda(inputs.normal(100, 2, s)) for s in range(3)]
+    info = handle.hpd_solve_batched(dA, dB)
+    assert info == [0, 71, 0]
+
+
+def test_gaussian_elimination_batched_uneven(handle):
+    r = inputs.rng(77)
+    sizes = [1, 2, 31, 32, 33, 64, 100, 255, 256, 257, 511, 512] + list(r.integers(1, 513, 24))
+    nrhs = [int(x) for x in r.integers(1, 9, len(sizes))]
+    As, Bs, dA, dB = [], [], [], []
+    for i, (n, k) in enumerate(zip(sizes, nrhs)):
+        A = inputs.uniform(int(n), int(n), seed=5000 + i)
+        B = inputs.normal(int(n), k, seed=6000 + i)
+        As.append(A); Bs.append(B)
+        dA.append(eg.colmajor_cuda(A)); dB.append(eg.colmajor_cuda(B))
+    info = handle.gaussian_elimination_batched(dA, dB)
+    assert info == [0] * len(sizes)
+    for i, (A, B) in enumerate(zip(As, Bs)):
+        F, X, st = orc.gaussian_elimination(A, B, nb=32)
+        assert st == 0
+        U = np.triu(dA[i].cpu().numpy())
+        assert np.max(np.abs(U - np.triu(F))) <= 1e-10 * max(1.0, np.max(np.abs(F))), i
+        Xg = dB[i].cpu().numpy()
+        assert np.max(np.abs(Xg - X)) <= 1e-8 * max(1.0, np.max(np.abs(X))), i
+
+
+def test_gaussian_elimination_batched_singular(handle):
+    good = inputs.uniform(80, 80, 1)
+    bad = good.copy(order="F")
+    bad[:, 45] = 0.0
+    dA = [eg.colmajor_cuda(good), eg.colmajor_cuda(bad)]
+    dB = [eg.colmajor_cuda(inputs.normal(80, 1, s)) for s in range(2)]
+    assert handle.gaussian_elimination_batched(dA, dB) == [0, 46]
