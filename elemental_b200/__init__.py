@@ -25,7 +25,7 @@ NORMAL, TRANSPOSE, ADJOINT = 0, 1, 2
 LEFT, RIGHT = 0, 1
 NON_UNIT, UNIT = 0, 1
 
-OK, NOT_HPD, SINGULAR, TIMEOUT = 0, 1, 2, 3
+OK, NOT_HPD, SINGULAR, TIMEOUT, NO_CONVERGENCE = 0, 1, 2, 3, 4
 
 
 class ElemGPUError(RuntimeError):
@@ -113,6 +113,8 @@ def _declare(L):
         "egpu_dherk": ([H, I, I, I, I, D, P, I, D, P, I], I),
         "egpu_dlaswp": ([H, I, I, I, P, I, P, I], I),
         "egpu_dposv_batched": ([H, I, P, P, P, P, P, P, P], I),
+        "egpu_dposv_mixed": ([H, I, I, I, P, I, P, I, P, I, I, D, P, P], I),
+        "egpu_tc_gemm_split": ([H, I, I, I, D, P, I, P, I, D, P, I, I, I], I),
         "egpu_dgesv_batched": ([H, I, P, P, P, P, P, P, P], I),
         "egpu_host_dpotrf": ([H, I, I, P, I, P], I),
         "egpu_host_dpotrs": ([H, I, I, I, I, P, I, P, I], I),
@@ -278,7 +280,7 @@ class Handle:
     def launch_count(self) -> int:
         return int(lib().egpu_launch_count(self._h))
 
-    TRACE_KINDS = {"update": 0, "trsm": 1, "diag": 2, "panel": 3, "swap": 4, "other": 5}
+    TRACE_KINDS = {"update": 0, "trsm": 1, "diag": 2, "panel": 3, "swap": 4, "other": 5, "tc": 6}
 
     def trace_enable(self, on: bool = True):
         """Bracket every launch with CUDA events on its stream (clears old records)."""
@@ -391,6 +393,29 @@ class Handle:
         nrhs <= 16, one persistent launch.  Returns per-system info (0 or the
         1-based column of an exact zero pivot)."""
         return self._batched(lib().egpu_dgesv_batched, As, Bs)
+
+    def hpd_solve_mixed(self, A, B, uplo=LOWER, max_iter=30, tol=1e-14):
+        """Mixed-precision HPDSolve: returns (X, corrections, backward error).
+        A and B (column-major float64 CUDA tensors) are left unchanged."""
+        import torch
+        self._bind_stream()
+        nrhs = B.shape[1] if B.dim() > 1 else 1
+        X = empty_colmajor(A.shape[0], nrhs, torch.float64, A.device)
+        it = ctypes.c_int(0)
+        be = ctypes.c_double(0.0)
+        rc = lib().egpu_dposv_mixed(self._h, uplo, A.shape[0], nrhs, _ptr(A), _ld(A), _ptr(B), _ld(B), _ptr(X),
+                                    _ld(X), max_iter, tol, ctypes.byref(it), ctypes.byref(be))
+        if rc == NO_CONVERGENCE:
+            raise ElemGPUError(f"refinement did not reach {tol:g} in {it.value} corrections (berr {be.value:.3e})")
+        _check(rc)
+        return X, it.value, be.value
+
+    def tc_gemm_split(self, A, B, C, alpha=1.0, beta=0.0, lower=False, terms=3):
+        """C (float32, column-major) = alpha A B^T + beta C on the tcgen05 tensor cores
+        (A, B float64 column-major, split into TF32 hi/lo parts)."""
+        self._bind_stream()
+        _check(lib().egpu_tc_gemm_split(self._h, A.shape[0], B.shape[0], A.shape[1], alpha, _ptr(A), _ld(A), _ptr(B),
+                                        _ld(B), beta, _ptr(C), _ld(C), 1 if lower else 0, terms))
 
     def hpd_solve_batched(self, As, Bs=None):
         """Batched HPDSolve(LOWER) over lists of column-major CUDA tensors (n <= 512,

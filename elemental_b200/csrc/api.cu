@@ -6,7 +6,7 @@
 #include <new>
 #include <string>
 
-#include "internal.h"
+#include "context.h"
 
 namespace egpu {
 
@@ -19,39 +19,8 @@ void set_last_error(cudaError_t e, const char* what, const char* file, int line)
 
 void count_launch(int n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 
-struct Trace {
-  struct Rec {
-    int kind;
-    double flops, bytes;
-    cudaEvent_t e0, e1;
-  };
-  bool on = false;
-  std::vector<Rec> recs;
-  std::vector<cudaEvent_t> pool;
-  cudaEvent_t get() {
-    if (pool.empty()) {
-      cudaEvent_t e;
-      if (cudaEventCreate(&e) != cudaSuccess) return nullptr;
-      return e;
-    }
-    cudaEvent_t e = pool.back();
-    pool.pop_back();
-    return e;
-  }
-  void clear() {
-    for (auto& r : recs) {
-      if (r.e0) pool.push_back(r.e0);
-      if (r.e1) pool.push_back(r.e1);
-    }
-    recs.clear();
-  }
-  ~Trace() {
-    clear();
-    for (auto e : pool) cudaEventDestroy(e);
-  }
-};
+thread_local Trace* t_trace = nullptr;
 
-static thread_local Trace* t_trace = nullptr;
 
 TraceMark::TraceMark(cudaStream_t s, int kind, double flops, double bytes) {
   if (t_trace == nullptr || !t_trace->on) return;
@@ -74,148 +43,8 @@ TraceMark::~TraceMark() {
 
 using namespace egpu;
 
-struct egpu_context {
-  int device = 0;
-  int sm_count = 148;
-  cudaStream_t own_stream = nullptr;
-  cudaStream_t stream = nullptr;
-  int nb = 128;
-  void* ws = nullptr;
-  size_t ws_bytes = 0;
-  DevStatus* dstatus = nullptr;
-  DevStatus* hstatus = nullptr;  // pinned
-  // host-API staging buffers
-  void* stage[3] = {nullptr, nullptr, nullptr};
-  size_t stage_bytes[3] = {0, 0, 0};
-  Trace trace;
-  // look-ahead: a high-priority side stream for the panel chain and events
-  // joining it with the update chain on `stream`
-  cudaStream_t side = nullptr;
-  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
-  cudaEvent_t ev_panel[2] = {nullptr, nullptr}, ev_rest[2] = {nullptr, nullptr};
-  int lookahead = 1;
-  int async = 0;  // device API: enqueue only; status read by egpu_get_status
-};
 
-namespace {
 
-struct DeviceGuard {
-  int prev = -1;
-  explicit DeviceGuard(int dev) {
-    cudaGetDevice(&prev);
-    if (prev != dev) cudaSetDevice(dev);
-  }
-  ~DeviceGuard() {
-    int cur;
-    cudaGetDevice(&cur);
-    if (prev >= 0 && cur != prev) cudaSetDevice(prev);
-  }
-};
-
-int ensure_ws(egpu_context* h, size_t bytes) {
-  if (bytes <= h->ws_bytes) return EGPU_OK;
-  if (h->ws) {
-    cudaStreamSynchronize(h->stream);
-    cudaFree(h->ws);
-    h->ws = nullptr;
-    h->ws_bytes = 0;
-  }
-  bytes = (bytes + (1 << 20) - 1) & ~size_t((1 << 20) - 1);
-  cudaError_t e = cudaMalloc(&h->ws, bytes);
-  if (e != cudaSuccess) {
-    set_last_error(e, "workspace cudaMalloc", __FILE__, __LINE__);
-    cudaGetLastError();
-    return EGPU_ERR_ALLOC;
-  }
-  h->ws_bytes = bytes;
-  return EGPU_OK;
-}
-
-int ensure_stage(egpu_context* h, int slot, size_t bytes) {
-  if (bytes <= h->stage_bytes[slot]) return EGPU_OK;
-  if (h->stage[slot]) {
-    cudaStreamSynchronize(h->stream);
-    cudaFree(h->stage[slot]);
-    h->stage[slot] = nullptr;
-    h->stage_bytes[slot] = 0;
-  }
-  bytes = (bytes + (1 << 20) - 1) & ~size_t((1 << 20) - 1);
-  cudaError_t e = cudaMalloc(&h->stage[slot], bytes);
-  if (e != cudaSuccess) {
-    set_last_error(e, "staging cudaMalloc", __FILE__, __LINE__);
-    cudaGetLastError();
-    return EGPU_ERR_ALLOC;
-  }
-  h->stage_bytes[slot] = bytes;
-  return EGPU_OK;
-}
-
-// Entered by every C-ABI call: selects the handle's device and makes its
-// trace the calling thread's active trace.
-struct Enter {
-  DeviceGuard g;
-  Trace* prev;
-  explicit Enter(egpu_context* h) : g(h->device), prev(t_trace) { t_trace = &h->trace; }
-  ~Enter() { t_trace = prev; }
-};
-
-// Host-memory entry points are synchronous whatever the handle's mode.
-struct SyncScope {
-  egpu_context* h;
-  int saved;
-  explicit SyncScope(egpu_context* hh) : h(hh), saved(hh->async) { hh->async = 0; }
-  ~SyncScope() { h->async = saved; }
-};
-
-inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
-inline long long ld_aligned(int rows) { return std::max<long long>(32, align_up((size_t)std::max(rows, 1), 32)); }
-
-// Simple bump allocator over the handle workspace.
-struct Carve {
-  unsigned char* base;
-  size_t off = 0;
-  explicit Carve(void* b) : base(static_cast<unsigned char*>(b)) {}
-  template <class T>
-  T* take(size_t count) {
-    off = align_up(off, 256);
-    T* p = reinterpret_cast<T*>(base + off);
-    off += sizeof(T) * count;
-    return p;
-  }
-};
-
-int reset_status(egpu_context* h) {
-  if (h->async) return EGPU_OK;  // async: the first failure stays until egpu_get_status
-  EGPU_CUDA_TRY(cudaMemsetAsync(h->dstatus, 0, sizeof(DevStatus), h->stream));
-  return EGPU_OK;
-}
-
-int read_status_now(egpu_context* h, int* info) {
-  EGPU_CUDA_TRY(cudaMemcpyAsync(h->hstatus, h->dstatus, sizeof(DevStatus), cudaMemcpyDeviceToHost, h->stream));
-  EGPU_CUDA_TRY(cudaStreamSynchronize(h->stream));
-  if (info) *info = h->hstatus->code ? h->hstatus->info : 0;
-  switch (h->hstatus->code) {
-    case kOk: return EGPU_OK;
-    case kNotHPD: return EGPU_NOT_HPD;
-    case kSingular: return EGPU_SINGULAR;
-    default: return EGPU_TIMEOUT;
-  }
-}
-
-// Synchronous mode: wait and map the status.  Async mode: return at once.
-int read_status(egpu_context* h, int* info) {
-  if (h->async) {
-    if (info) *info = 0;
-    return EGPU_OK;
-  }
-  return read_status_now(h, info);
-}
-
-#define TRY(x)               \
-  do {                       \
-    int _r = (x);            \
-    if (_r != EGPU_OK) return _r; \
-  } while (0)
 
 // A device matrix argument that may need repacking into an aligned copy for TMA.
 struct Operand {
@@ -624,7 +453,6 @@ Operand make_op(double* p, long long ld, int rows, int cols) {
 
 bool bad_ld(long long ld, int rows) { return ld < std::max(1, rows); }
 
-}  // namespace
 
 // ======================================================================
 extern "C" {

@@ -250,10 +250,34 @@ __device__ inline void smem_dmma_gemm(const double* A, int lda, const double* B,
   }
 }
 
+// Columns of X = inv(L) for the 16 x 16 lower block L at S[o.., o..] (read
+// with all lanes on the same address: shared-memory broadcasts), given
+// rinv = 1 / L[lane][lane] in lane `lane` (< 16).  Lane c < 16 computes column
+// c by forward substitution, x[k] = (delta_kc - sum_{m<k} L[k][m] x[m]) rinv_k.
+__device__ inline void warp_trinv16_cols(const double* S, int lds, int o, double rinv, double* X, int ldx) {
+  const int lane = threadIdx.x & 31;
+  double x[16];
+#pragma unroll
+  for (int k = 0; k < 16; ++k) {
+    const double rk = __shfl_sync(0xffffffffu, rinv, k);
+    double a0 = (k == lane) ? 1.0 : 0.0, a1 = 0.0;
+#pragma unroll
+    for (int m = 0; m < k; m += 2) {
+      a0 = fma(-S[(o + k) + (o + m) * lds], x[m], a0);
+      if (m + 1 < k) a1 = fma(-S[(o + k) + (o + m + 1) * lds], x[m + 1], a1);
+    }
+    x[k] = (k >= lane) ? (a0 + a1) * rk : 0.0;
+  }
+  if (lane < 16)
+#pragma unroll
+    for (int k = 0; k < 16; ++k) X[k + lane * ldx] = x[k];
+}
+
 // Cholesky of one 16 x 16 lower block at S[o.., o..] by one warp, rows in
-// registers (lane i < 16 holds row i), pivots broadcast by shuffles; then the
-// inverse of the factor into X (16 x 16, ld ldx) and the factor back into S.
-// The diagonal uses 1/sqrt(a_jj): a_jj * r = sqrt(a_jj), a_ij * r = l_ij.
+// registers (lane i < 16 holds row i), pivots broadcast by shuffles; the
+// factor goes back into S and its inverse into X (16 x 16, ld ldx).
+// The diagonal uses r = 1/sqrt(a_jj): a_jj r = sqrt(a_jj), a_ij r = l_ij, and
+// r is also the reciprocal the inverse needs.
 // Returns 0 or the 1-based column of a non-positive pivot (warp-uniform).
 __device__ inline int warp_chol16(double* S, int lds, int o, double* X, int ldx) {
   const int lane = threadIdx.x & 31;
@@ -262,6 +286,7 @@ __device__ inline int warp_chol16(double* S, int lds, int o, double* X, int ldx)
 #pragma unroll
   for (int k = 0; k < 16; ++k) d[k] = (act && k <= lane) ? S[(o + lane) + (o + k) * lds] : 0.0;
   int fail = 0;
+  double myr = 1.0;
 #pragma unroll
   for (int j = 0; j < 16; ++j) {
     const double djj = __shfl_sync(0xffffffffu, d[j], j);
@@ -270,6 +295,7 @@ __device__ inline int warp_chol16(double* S, int lds, int o, double* X, int ldx)
         fail = j + 1;
       } else {
         const double r = rsqrt(djj);
+        if (lane == j) myr = r;
         d[j] *= r;  // lane j: sqrt(a_jj); lanes > j: l_ij
         const double lj = d[j];
 #pragma unroll
@@ -284,46 +310,18 @@ __device__ inline int warp_chol16(double* S, int lds, int o, double* X, int ldx)
 #pragma unroll
   for (int k = 0; k < 16; ++k)
     if (act && k <= lane) S[(o + lane) + (o + k) * lds] = d[k];
-  // X = inv(L): lane c computes column c
-  double x[16];
-#pragma unroll
-  for (int k = 0; k < 16; ++k) {
-    double acc = (k == lane) ? 1.0 : 0.0;
-#pragma unroll
-    for (int m = 0; m < k; ++m) acc = fma(-__shfl_sync(0xffffffffu, d[m], k), x[m], acc);
-    const double lkk = __shfl_sync(0xffffffffu, d[k], k);
-    x[k] = (k >= lane) ? acc / lkk : 0.0;
-  }
-#pragma unroll
-  for (int k = 0; k < 16; ++k)
-    if (act) X[k + lane * ldx] = x[k];
+  __syncwarp();
+  warp_trinv16_cols(S, lds, o, myr, X, ldx);
   return 0;
 }
 
 // Inverse of one 16 x 16 lower block at S[o.., o..] (unit: diagonal taken as
-// 1) by one warp, into X (ld ldx).
+// 1) by one warp, into X (ld ldx).  The 16 reciprocals of the diagonal are
+// formed in parallel, one per lane.
 __device__ inline void warp_trinv16(const double* S, int lds, int o, int unit, double* X, int ldx) {
   const int lane = threadIdx.x & 31;
-  const bool act = lane < 16;
-  double d[16];
-#pragma unroll
-  for (int k = 0; k < 16; ++k) {
-    double v = (act && k <= lane) ? S[(o + lane) + (o + k) * lds] : 0.0;
-    if (unit && k == lane) v = 1.0;
-    d[k] = v;
-  }
-  double x[16];
-#pragma unroll
-  for (int k = 0; k < 16; ++k) {
-    double acc = (k == lane) ? 1.0 : 0.0;
-#pragma unroll
-    for (int m = 0; m < k; ++m) acc = fma(-__shfl_sync(0xffffffffu, d[m], k), x[m], acc);
-    const double lkk = __shfl_sync(0xffffffffu, d[k], k);
-    x[k] = (k >= lane) ? (unit ? acc : acc / lkk) : 0.0;
-  }
-#pragma unroll
-  for (int k = 0; k < 16; ++k)
-    if (act) X[k + lane * ldx] = x[k];
+  const double rinv = (unit || lane >= 16) ? 1.0 : 1.0 / S[(o + lane) + (o + lane) * lds];
+  warp_trinv16_cols(S, lds, o, rinv, X, ldx);
 }
 
 // Temporary area of the DMMA diagonal kernels: 16 leaf inverses (ld 17) and
@@ -332,6 +330,29 @@ constexpr int kLeafLD = 17;
 constexpr int kTmpLD = 68;
 constexpr int kDiagTmpDoubles = 8 * 16 * kLeafLD + 64 * kTmpLD;
 constexpr int kDiagSmem = kDiagSmemBase + kDiagTmpDoubles * (int)sizeof(double);
+
+// Flat (one pass, all copies in flight) transfers of a b x b triangle between
+// global memory and S; a column-by-column loop costs one memory round trip
+// per column.  `upper`: the global block holds the triangle transposed
+// (S(r, c) = G[c + r ld]); consecutive threads always take consecutive
+// global addresses.
+__device__ inline void tri_load_async(double* S, const double* G, long long ld, int b, bool upper) {
+  for (int e = threadIdx.x; e < b * b; e += blockDim.x) {
+    const int i = e % b, j = e / b;  // G row i, column j
+    if (!upper && i >= j) cp_async8(&S[i + j * kLDS], &G[i + (long long)j * ld]);
+    if (upper && j >= i) cp_async8(&S[j + i * kLDS], &G[i + (long long)j * ld]);
+  }
+}
+// Lower triangle of S (r >= c) into G; the other triangle of the b x b block
+// is written as zero when `zero_other`, else left alone.
+__device__ inline void tri_store(const double* S, double* G, long long ld, int b, bool upper, bool zero_other) {
+  for (int e = threadIdx.x; e < b * b; e += blockDim.x) {
+    const int i = e % b, j = e / b;
+    const int r = upper ? j : i, c = upper ? i : j;  // S coordinates
+    if (r >= c) G[i + (long long)j * ld] = S[r + c * kLDS];
+    else if (zero_other) G[i + (long long)j * ld] = 0.0;
+  }
+}
 
 // Pad the lower b x b triangle in S to bp = round_up(b, 16) with identity.
 __device__ inline int pad16_identity(double* S, int b) {

@@ -18,7 +18,7 @@ bool tma_compatible(const void* p, long long ld);
 
 // ---- launch tracing (per-kernel-class CUDA-event timing on the launch stream)
 enum TraceKind { kTraceUpdate = 0, kTraceTrsm = 1, kTraceDiag = 2, kTracePanel = 3, kTraceSwap = 4,
-                 kTraceOther = 5, kTraceKinds = 6 };
+                 kTraceOther = 5, kTraceTc = 6, kTraceKinds = 7 };
 struct Trace;
 // Records an event pair around one launch when the calling thread has an
 // active trace; no-op otherwise.
@@ -34,6 +34,24 @@ int launch_dgemm(cudaStream_t st, bool a_kmajor, bool b_kmajor, int M, int N, in
                  const double* A, long long lda, const double* B, long long ldb, double beta, double* C,
                  long long ldc, int tri, bool wide, DevStatus* status);
 int launch_scale(cudaStream_t st, int M, int N, double beta, double* C, long long ldc, int tri);
+
+// 2-D TMA tensor map (dtype: a CUtensorMapDataType value) over `outer` rows of
+// `inner` contiguous elements, rows ld_bytes apart.
+bool make_tma_2d(CUtensorMap* m, int dtype, const void* base, uint64_t inner, uint64_t outer, uint64_t ld_bytes,
+                 uint32_t box_inner, uint32_t box_outer, bool swz128);
+
+// tcgen05 TF32 GEMM: C (FP32, col-major) = alpha * sum_t A_t B_t^T + beta * C,
+// A_t (M x K) and B_t (N x K) K-major FP32 buffers (row stride ldk elements,
+// ldk % 4 == 0, 16-byte aligned) holding TF32 values; terms 1 uses (Ahi, Bhi),
+// terms 3 adds (Ahi, Blo) and (Alo, Bhi).  tri 1: lower triangle of a square C.
+int launch_tc_gemm(cudaStream_t st, int M, int N, int K, float alpha, const float* Ahi, const float* Alo,
+                   const float* Bhi, const float* Blo, long long ldk, float beta, float* C, long long ldc, int tri,
+                   int terms, DevStatus* status);
+
+// X (rows x cols, column-major FP64) -> TF32 hi/lo parts in K-major rows
+// (hi[r*ldk + c]), columns cols..ldk-1 zero.
+int launch_split_tf32(cudaStream_t st, int rows, int cols, const double* X, long long ldx, float* hi, float* lo,
+                      long long ldk);
 
 // Diagonal-block Cholesky (factor in place + triangular inverse into W).
 int launch_potrf_diag(cudaStream_t st, int uplo, double* A, long long lda, int b, double* W, int ldw,
@@ -51,6 +69,11 @@ int launch_trtri_blocks(cudaStream_t st, int uplo, int unit, const double* A, lo
 size_t lu_panel_scratch_bytes(int m, int b, int sm_count);
 int launch_lu_panel(cudaStream_t st, int m, int b, double* A, long long lda, int* p, int offset, int* image,
                     int* preimage, double* W, int ldw, void* scratch, DevStatus* status, int sm_count);
+
+// Register-resident cluster form of the LU panel (m <= 16384); returns
+// EGPU_ERR_UNSUPPORTED when it does not apply.
+int launch_lu_panel_rp(cudaStream_t st, int m, int b, double* A, long long lda, int* p, int offset, int* image,
+                       int* preimage, double* W, int ldw, DevStatus* status, int cluster_max);
 
 // Apply composed panel pivots (image/preimage of b rows) to columns of the
 // m-row block A (ld lda), columns [0, ncols).

@@ -804,6 +804,11 @@ int launch_lu_panel(cudaStream_t st, int m, int b, double* A, long long lda, int
                     int* preimage, double* W, int ldw, void* scratch, DevStatus* status, int sm_count) {
   if (m <= 0 || b <= 0) return EGPU_OK;
   if (b > 128) return EGPU_ERR_ARG;
+  {
+    const int rc = launch_lu_panel_rp(st, m, b, A, lda, p, offset, image, preimage, W, ldw, status,
+                                      panel_cluster_max());
+    if (rc != EGPU_ERR_UNSUPPORTED) return rc;
+  }
   // sub-panel cluster form: panel in global memory, 16 columns in shared memory
   {
     static int sp_ok = -1;

@@ -1,0 +1,316 @@
+// Mixed-precision HPD solve: Cholesky with the trailing updates on the
+// tcgen05 tensor cores (TF32 x 3 split products, FP32 accumulation, FP32
+// trailing matrix), the diagonal blocks and panel solves in FP64, and
+// iterative refinement with FP64 residuals to an FP64-level backward error.
+//
+// Per block column k (nb = the handle's block size):
+//   1. the panel columns [k, k+b) of the FP32 working matrix are widened into
+//      the FP64 factor buffer Lf;
+//   2. potrf of the b x b diagonal block and its inverse (FP64, the same
+//      kernel as the plain path: cholesky::LVar3Unb, Cholesky/LVar3.hpp:19-49);
+//   3. L21 := A21 inv(L11)^T (FP64 DMMA GEMM);
+//   4. L21 is split into TF32 hi/lo parts in K-major layout;
+//   5. A22 -= L21 L21^T on the lower triangle of the FP32 matrix with
+//      tcgen05.mma kind::tf32 (hi*hi + hi*lo + lo*hi).
+// The factor Lf (FP64 storage, FP32-level accuracy) then drives the
+// refinement: x = Lf^-T Lf^-1 b, and while the normwise backward error
+//   max_j ||b_j - A x_j||_inf / (||A||_inf ||x_j||_inf + ||b_j||_inf)
+// is above the tolerance: r = b - A x (FP64 GEMM on a full symmetric copy of
+// A), d = Lf^-T Lf^-1 r, x += d.
+#include <cmath>
+#include <vector>
+
+#include "context.h"
+
+namespace egpu {
+
+namespace {
+
+// A (uplo triangle valid) -> As (full symmetric FP64, ld lds) and Af (lower FP32, ld ldf)
+__global__ void mixed_prepare_kernel(int uplo, int n, const double* A, long long lda, double* As, long long lds,
+                                     float* Af, long long ldf) {
+  __shared__ double tile[32][33];
+  const int bi = blockIdx.x * 32, bj = blockIdx.y * 32;  // tile rows bi.., cols bj..
+  if (bi < bj) return;                                  // lower tiles (and their mirrors) only
+  const int tx = threadIdx.x, ty = threadIdx.y;         // 32 x 8
+  for (int q = ty; q < 32; q += 8) {
+    const int r = bi + tx, c = bj + q;
+    double v = 0.0;
+    if (r < n && c < n && r >= c) v = (uplo == EGPU_LOWER) ? A[r + (long long)c * lda] : A[c + (long long)r * lda];
+    tile[tx][q] = v;
+    if (r < n && c < n && r >= c) {
+      As[r + (long long)c * lds] = v;
+      Af[r + (long long)c * ldf] = (float)v;
+    }
+  }
+  __syncthreads();
+  for (int q = ty; q < 32; q += 8) {  // mirror: As[c, r] = A(r, c) for r > c
+    const int c = bj + tx, r = bi + q;
+    if (r < n && c < n && r > c) As[c + (long long)r * lds] = tile[q][tx];
+  }
+}
+
+// Lf[k+i, k+c] = Af[k+i, k+c] for the panel (rows i in [0, m), cols c in [0, b), lower part)
+__global__ void widen_panel_kernel(int m, int b, const float* Af, long long ldf, double* Lf, long long ldl) {
+  const int c = blockIdx.y;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x)
+    if (i >= c) Lf[i + (long long)c * ldl] = (double)Af[i + (long long)c * ldf];
+}
+
+__device__ __forceinline__ float tf32_rna(float x) {
+  uint32_t r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+  return __uint_as_float(r);
+}
+
+// X (rows x cols, column-major FP64) -> hi/lo TF32 in K-major rows: hi[r*ldk + c]
+__global__ void split_tf32_kernel(int rows, int cols, const double* X, long long ldx, float* hi, float* lo,
+                                  long long ldk) {
+  __shared__ double tile[32][33];
+  const int r0 = blockIdx.x * 32, c0 = blockIdx.y * 32;
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  for (int q = ty; q < 32; q += 8) {
+    const int r = r0 + tx, c = c0 + q;
+    tile[q][tx] = (r < rows && c < cols) ? X[r + (long long)c * ldx] : 0.0;
+  }
+  __syncthreads();
+  for (int q = ty; q < 32; q += 8) {
+    const int r = r0 + q, c = c0 + tx;
+    if (r < rows && c < ldk) {
+      const double x = (c < cols) ? tile[tx][q] : 0.0;
+      const float h = tf32_rna((float)x);
+      hi[(long long)r * ldk + c] = h;
+      lo[(long long)r * ldk + c] = tf32_rna((float)(x - (double)h));
+    }
+  }
+}
+
+// per-column max |X[:, j]| into out[j] (one block per column)
+__global__ void colmax_kernel(int n, int ncols, const double* X, long long ldx, double* out) {
+  const int j = blockIdx.x;
+  double m = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) m = fmax(m, fabs(X[i + (long long)j * ldx]));
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  __shared__ double red[32];
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    m = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if (threadIdx.x == 0) out[j] = m;
+  }
+}
+
+// ||As||_inf = max_i sum_j |As[i, j]| : per-row sums, one thread per row
+__global__ void rowsum_abs_kernel(int n, const double* As, long long lds, double* rows) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double s = 0.0;
+  for (int j = 0; j < n; ++j) s += fabs(As[i + (long long)j * lds]);
+  rows[i] = s;
+}
+
+// Y = X (n x ncols) ; Y += X
+__global__ void copy_cols_kernel(int n, int ncols, const double* X, long long ldx, double* Y, long long ldy,
+                                 int add) {
+  const int j = blockIdx.y;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double x = X[i + (long long)j * ldx];
+    double* y = &Y[i + (long long)j * ldy];
+    *y = add ? *y + x : x;
+  }
+}
+
+}  // namespace
+
+int launch_split_tf32(cudaStream_t st, int rows, int cols, const double* X, long long ldx, float* hi, float* lo,
+                      long long ldk) {
+  if (rows <= 0 || cols <= 0) return EGPU_OK;
+  dim3 grid((rows + 31) / 32, (int)((ldk + 31) / 32)), block(32, 8);
+  split_tf32_kernel<<<grid, block, 0, st>>>(rows, cols, X, ldx, hi, lo, ldk);
+  count_launch();
+  EGPU_CUDA_TRY(cudaGetLastError());
+  return EGPU_OK;
+}
+
+// Workspace layout of the mixed solve.
+struct MixedLayout {
+  size_t as, af, lf, w, pkh, pkl, xw, r, winv, norms, total;
+  long long lds, ldf, ldk;
+};
+
+static MixedLayout mixed_layout(int n, int nrhs, int nb) {
+  MixedLayout L;
+  L.lds = std::max<long long>(32, ((long long)n + 31) / 32 * 32);
+  L.ldf = L.lds;
+  L.ldk = ((long long)nb + 31) / 32 * 32;
+  size_t off = 0;
+  auto take = [&](size_t bytes) { off = (off + 1023) & ~size_t(1023); size_t o = off; off += bytes; return o; };
+  L.as = take(sizeof(double) * L.lds * n);
+  L.af = take(sizeof(float) * L.ldf * n);
+  L.lf = take(sizeof(double) * L.lds * n);
+  L.w = take(sizeof(double) * (size_t)nb * nb);
+  L.pkh = take(sizeof(float) * (size_t)n * L.ldk);
+  L.pkl = take(sizeof(float) * (size_t)n * L.ldk);
+  L.xw = take(sizeof(double) * L.lds * std::max(nrhs, 1));
+  L.r = take(sizeof(double) * L.lds * std::max(nrhs, 1));
+  L.winv = take(winv_bytes(n, nb));
+  L.norms = take(sizeof(double) * ((size_t)n + 4 * (size_t)std::max(nrhs, 1)));
+  L.total = (off + 4095) & ~size_t(4095);
+  return L;
+}
+
+// X := Lf^-T Lf^-1 X with the pre-inverted diagonal blocks Winv
+static int mixed_solve(egpu_context* h, int n, int nrhs, const double* Lf, long long lds, const double* Winv,
+                       double* X) {
+  TRY(trsm_blocked(h->stream, EGPU_LEFT, EGPU_LOWER, 0, n, nrhs, Lf, lds, Winv, h->nb, X, lds, h->dstatus));
+  return trsm_blocked(h->stream, EGPU_LEFT, EGPU_LOWER, 1, n, nrhs, Lf, lds, Winv, h->nb, X, lds, h->dstatus);
+}
+
+// Backward error of the current iterate: max_j ||r_j|| / (||A|| ||x_j|| + ||b_j||), inf-norms.
+static int mixed_berr(egpu_context* h, int n, int nrhs, const double* R, const double* Xw, const double* B,
+                      long long ldb, long long lds, double anorm, double* norms, double* berr) {
+  cudaStream_t st = h->stream;
+  colmax_kernel<<<nrhs, 256, 0, st>>>(n, nrhs, R, lds, norms);
+  colmax_kernel<<<nrhs, 256, 0, st>>>(n, nrhs, Xw, lds, norms + nrhs);
+  colmax_kernel<<<nrhs, 256, 0, st>>>(n, nrhs, B, ldb, norms + 2 * nrhs);
+  count_launch(3);
+  EGPU_CUDA_TRY(cudaGetLastError());
+  std::vector<double> hn(3 * (size_t)nrhs);
+  EGPU_CUDA_TRY(cudaMemcpyAsync(hn.data(), norms, sizeof(double) * 3 * nrhs, cudaMemcpyDeviceToHost, st));
+  EGPU_CUDA_TRY(cudaStreamSynchronize(st));
+  double e = 0.0;
+  for (int j = 0; j < nrhs; ++j) {
+    const double den = anorm * hn[nrhs + j] + hn[2 * nrhs + j];
+    e = std::max(e, den > 0.0 ? hn[j] / den : (hn[j] > 0.0 ? INFINITY : 0.0));
+  }
+  *berr = e;
+  return EGPU_OK;
+}
+
+int dposv_mixed_core(egpu_context* h, int uplo, int n, int nrhs, const double* A, long long lda, const double* B,
+                     long long ldb, double* X, long long ldx, int max_iter, double tol, int* iters, double* berr) {
+  const int nb = h->nb;
+  cudaStream_t st = h->stream;
+  const MixedLayout L = mixed_layout(n, nrhs, nb);
+  TRY(ensure_ws(h, L.total + 4096));
+  unsigned char* ws = static_cast<unsigned char*>(h->ws);
+  double* As = reinterpret_cast<double*>(ws + L.as);
+  float* Af = reinterpret_cast<float*>(ws + L.af);
+  double* Lf = reinterpret_cast<double*>(ws + L.lf);
+  double* W = reinterpret_cast<double*>(ws + L.w);
+  float* PKh = reinterpret_cast<float*>(ws + L.pkh);
+  float* PKl = reinterpret_cast<float*>(ws + L.pkl);
+  double* Xw = reinterpret_cast<double*>(ws + L.xw);
+  double* R = reinterpret_cast<double*>(ws + L.r);
+  double* Winv = reinterpret_cast<double*>(ws + L.winv);
+  double* norms = reinterpret_cast<double*>(ws + L.norms);
+  const long long lds = L.lds, ldf = L.ldf;
+  EGPU_CUDA_TRY(cudaMemsetAsync(h->dstatus, 0, sizeof(DevStatus), st));
+  {
+    dim3 grid((n + 31) / 32, (n + 31) / 32), block(32, 8);
+    mixed_prepare_kernel<<<grid, block, 0, st>>>(uplo, n, A, lda, As, lds, Af, ldf);
+    count_launch();
+    EGPU_CUDA_TRY(cudaGetLastError());
+  }
+  // ---- factorization
+  for (int k = 0; k < n; k += nb) {
+    const int b = std::min(nb, n - k);
+    const int m = n - k, m2 = m - b;
+    {
+      TraceMark tm(st, kTraceOther, 0.0, 12.0 * m * b);
+      dim3 grid((m + 255) / 256, b);
+      widen_panel_kernel<<<grid, 256, 0, st>>>(m, b, Af + k + (long long)k * ldf, ldf, Lf + k + (long long)k * lds, lds);
+      count_launch();
+      EGPU_CUDA_TRY(cudaGetLastError());
+    }
+    TRY(launch_potrf_diag(st, EGPU_LOWER, Lf + k + (long long)k * lds, lds, b, W, nb, h->dstatus, k));
+    if (m2 == 0) continue;
+    double* L21 = Lf + (k + b) + (long long)k * lds;
+    TRY(launch_dgemm(st, false, false, m2, b, b, 1.0, L21, lds, W, nb, 0.0, L21, lds, 0, true, h->dstatus));
+    TRY(launch_split_tf32(st, m2, b, L21, lds, PKh, PKl, L.ldk));
+    TRY(launch_tc_gemm(st, m2, m2, b, -1.0f, PKh, PKl, PKh, PKl, L.ldk, 1.0f, Af + (k + b) + (long long)(k + b) * ldf,
+                       ldf, 1, 3, h->dstatus));
+  }
+  int info = 0;
+  TRY(read_status_now(h, &info));
+  // ---- refinement
+  TRY(launch_trtri_blocks(st, EGPU_LOWER, 0, Lf, lds, n, nb, Winv, nb));
+  {
+    rowsum_abs_kernel<<<(n + 255) / 256, 256, 0, st>>>(n, As, lds, norms);
+    count_launch();
+    EGPU_CUDA_TRY(cudaGetLastError());
+  }
+  std::vector<double> rs(n);
+  EGPU_CUDA_TRY(cudaMemcpyAsync(rs.data(), norms, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+  EGPU_CUDA_TRY(cudaStreamSynchronize(st));
+  double anorm = 0.0;
+  for (double v : rs) anorm = std::max(anorm, v);
+  dim3 cgrid((n + 255) / 256, nrhs);
+  copy_cols_kernel<<<cgrid, 256, 0, st>>>(n, nrhs, B, ldb, Xw, lds, 0);
+  count_launch();
+  TRY(mixed_solve(h, n, nrhs, Lf, lds, Winv, Xw));
+  int it = 0;
+  double e = INFINITY;
+  for (;;) {
+    copy_cols_kernel<<<cgrid, 256, 0, st>>>(n, nrhs, B, ldb, R, lds, 0);
+    count_launch();
+    TRY(launch_dgemm(st, false, true, n, nrhs, n, -1.0, As, lds, Xw, lds, 1.0, R, lds, 0, false, h->dstatus));
+    TRY(mixed_berr(h, n, nrhs, R, Xw, B, ldb, lds, anorm, norms + n, &e));
+    if (e <= tol || it >= max_iter || !std::isfinite(e)) break;
+    TRY(mixed_solve(h, n, nrhs, Lf, lds, Winv, R));
+    copy_cols_kernel<<<cgrid, 256, 0, st>>>(n, nrhs, R, lds, Xw, lds, 1);
+    count_launch();
+    ++it;
+  }
+  copy_cols_kernel<<<cgrid, 256, 0, st>>>(n, nrhs, Xw, lds, X, ldx, 0);
+  count_launch();
+  EGPU_CUDA_TRY(cudaGetLastError());
+  if (iters) *iters = it;
+  if (berr) *berr = e;
+  TRY(read_status_now(h, &info));
+  return e <= tol ? EGPU_OK : EGPU_NO_CONVERGENCE;
+}
+
+}  // namespace egpu
+
+extern "C" int egpu_dposv_mixed(egpu_handle h, int uplo, int n, int nrhs, const double* dA, int lda,
+                                const double* dB, int ldb, double* dX, int ldx, int max_iter, double tol,
+                                int* iters, double* berr) {
+  if (iters) *iters = 0;
+  if (berr) *berr = 0.0;
+  if (!h) return EGPU_ERR_ARG;
+  if (n < 0 || nrhs < 0 || lda < std::max(1, n) || ldb < std::max(1, n) || ldx < std::max(1, n) ||
+      (uplo != EGPU_LOWER && uplo != EGPU_UPPER) || max_iter < 0)
+    return EGPU_ERR_ARG;
+  if (n == 0 || nrhs == 0) return EGPU_OK;
+  Enter en(h);
+  return egpu::dposv_mixed_core(h, uplo, n, nrhs, dA, lda, dB, ldb, dX, ldx, max_iter, tol, iters, berr);
+}
+
+// Testing entry for the tcgen05 engine: C (FP32) = alpha A B^T + beta C with
+// A (M x K) and B (N x K) given column-major in FP64 and split into TF32 parts.
+extern "C" int egpu_tc_gemm_split(egpu_handle h, int M, int N, int K, double alpha, const double* dA, int lda,
+                                  const double* dB, int ldb, double beta, float* dC, int ldc, int lower, int terms) {
+  if (!h) return EGPU_ERR_ARG;
+  if (M < 0 || N < 0 || K < 1 || lda < std::max(1, M) || ldb < std::max(1, N) || ldc < std::max(1, M))
+    return EGPU_ERR_ARG;
+  if (M == 0 || N == 0) return EGPU_OK;
+  Enter en(h);
+  const long long ldk = ((long long)K + 31) / 32 * 32;
+  const size_t ab = sizeof(float) * (size_t)M * ldk, bb = sizeof(float) * (size_t)N * ldk;
+  auto up = [](size_t x) { return (x + 1023) & ~size_t(1023); };
+  TRY(ensure_ws(h, 2 * up(ab) + 2 * up(bb) + 4096));
+  unsigned char* ws = static_cast<unsigned char*>(h->ws);
+  float* Ah = reinterpret_cast<float*>(ws);
+  float* Al = reinterpret_cast<float*>(ws + up(ab));
+  float* Bh = reinterpret_cast<float*>(ws + 2 * up(ab));
+  float* Bl = reinterpret_cast<float*>(ws + 2 * up(ab) + up(bb));
+  cudaStream_t st = h->stream;
+  EGPU_CUDA_TRY(cudaMemsetAsync(h->dstatus, 0, sizeof(DevStatus), st));
+  TRY(launch_split_tf32(st, M, K, dA, lda, Ah, Al, ldk));
+  TRY(launch_split_tf32(st, N, K, dB, ldb, Bh, Bl, ldk));
+  TRY(launch_tc_gemm(st, M, N, K, (float)alpha, Ah, Al, Bh, Bl, ldk, (float)beta, dC, ldc, lower ? 1 : 0, terms,
+                     h->dstatus));
+  return read_status_now(h, nullptr);
+}

@@ -56,10 +56,7 @@ __global__ void __launch_bounds__(kDiagThreads) potrf_diag_kernel(double* A, lon
   extern __shared__ double S[];
   if (st != nullptr && st->code != 0) return;
   const int tid = threadIdx.x;
-  // all loads in flight at once (a plain load loop waits ~one memory latency per column)
-  for (int c = 0; c < b; ++c)
-    for (int r = c + tid; r < b; r += kDiagThreads)
-      cp_async8(&SE(S, r, c), (UPLO == EGPU_LOWER) ? &A[r + (long long)c * lda] : &A[c + (long long)r * lda]);
+  tri_load_async(S, A, lda, b, UPLO != EGPU_LOWER);
   cp_async_wait_all();
   __syncthreads();
   double* Xl = S + 128 * kLDS + 128;
@@ -71,19 +68,10 @@ __global__ void __launch_bounds__(kDiagThreads) potrf_diag_kernel(double* A, lon
     if (tid == 0) set_status(st, kNotHPD, col_base + f);
     return;
   }
-  for (int c = 0; c < b; ++c)
-    for (int r = c + tid; r < b; r += kDiagThreads) {
-      if (UPLO == EGPU_LOWER) A[r + (long long)c * lda] = SE(S, r, c);
-      else A[c + (long long)r * lda] = SE(S, r, c);
-    }
+  tri_store(S, A, lda, b, UPLO != EGPU_LOWER, false);
   __syncthreads();
   smem_trinv_dmma(S, bp, Xl, T);
-  for (int c = 0; c < b; ++c)
-    for (int r = tid; r < b; r += kDiagThreads) {
-      const double v = (r >= c) ? SE(S, r, c) : 0.0;
-      if (UPLO == EGPU_LOWER) W[r + (long long)c * ldw] = v;
-      else W[c + (long long)r * ldw] = v;  // inv(U) = inv(L)^T
-    }
+  tri_store(S, W, ldw, b, UPLO != EGPU_LOWER, true);  // inv(U) = inv(L)^T
 }
 
 int launch_potrf_diag(cudaStream_t st, int uplo, double* A, long long lda, int b, double* W, int ldw,
@@ -126,9 +114,7 @@ __global__ void __launch_bounds__(kDiagThreads) trtri_blocks_kernel(int uplo, in
   const double* Ab = A + off + (long long)off * lda;
   double* Wb = W + (long long)blk * b * ldw;
   const int tid = threadIdx.x;
-  for (int c = 0; c < bb; ++c)
-    for (int r = c + tid; r < bb; r += kDiagThreads)
-      cp_async8(&SE(S, r, c), (uplo == EGPU_LOWER) ? &Ab[r + (long long)c * lda] : &Ab[c + (long long)r * lda]);
+  tri_load_async(S, Ab, lda, bb, uplo != EGPU_LOWER);
   cp_async_wait_all();
   __syncthreads();
   double* Xl = S + 128 * kLDS + 128;
@@ -140,12 +126,11 @@ __global__ void __launch_bounds__(kDiagThreads) trtri_blocks_kernel(int uplo, in
     warp_trinv16(S, kLDS, 16 * q, unit, Xl + q * 16 * kLeafLD, kLeafLD);
   __syncthreads();
   smem_trinv_dmma(S, bp, Xl, T);
-  for (int c = 0; c < b; ++c)
-    for (int r = tid; r < b; r += kDiagThreads) {
-      double v = 0.0;
-      if (r < bb && c < bb && r >= c) v = SE(S, r, c);
-      if (uplo == EGPU_LOWER) Wb[r + (long long)c * ldw] = v;
-      else Wb[c + (long long)r * ldw] = v;
+  tri_store(S, Wb, ldw, bb, uplo != EGPU_LOWER, true);
+  if (bb < b)  // a short last block: the rest of its b x b slot is zero
+    for (int e = tid; e < b * b; e += kDiagThreads) {
+      const int i = e % b, j = e / b;
+      if (i >= bb || j >= bb) Wb[i + (long long)j * ldw] = 0.0;
     }
 }
 

@@ -35,6 +35,7 @@ extern "C" {
 #define EGPU_NOT_HPD 1    /* non-positive pivot in Cholesky */
 #define EGPU_SINGULAR 2   /* exact zero pivot in LU */
 #define EGPU_TIMEOUT 3    /* a bounded device-side wait ran out */
+#define EGPU_NO_CONVERGENCE 4  /* refinement stopped above its tolerance (result still written) */
 #define EGPU_ERR_ARG (-1)
 #define EGPU_ERR_CUDA (-2)
 #define EGPU_ERR_ALLOC (-3)
@@ -144,6 +145,29 @@ EGPU_API int egpu_dgetrs(egpu_handle h, int orient, int n, int nrhs, const doubl
 
 /* GaussianElimination(A, B), lapack-like/GaussianElimination.hpp:216-232. */
 EGPU_API int egpu_dgesv(egpu_handle h, int n, int nrhs, double* dA, int lda, double* dB, int ldb, int* info);
+
+/* Mixed-precision HPDSolve (HPDSolve.hpp:18-28 computes the same x): no
+ * counterpart in the reference, which factors in the working precision only.
+ * Cholesky with the trailing updates on the tcgen05 tensor cores in TF32 x 3
+ * split precision (FP32 accumulation and FP32 trailing matrix), FP64
+ * diagonal blocks and panel solves, then iterative refinement with FP64
+ * residuals until the normwise backward error
+ *   max_j ||b_j - A x_j||_inf / (||A||_inf ||x_j||_inf + ||b_j||_inf) <= tol
+ * or max_iter corrections.  A (uplo triangle read) and B are inputs only;
+ * X (n x nrhs) receives the solution.  Returns EGPU_OK, EGPU_NOT_HPD,
+ * EGPU_NO_CONVERGENCE (X holds the last iterate) or an error; *iters = the
+ * corrections applied, *berr = the final backward error.  Synchronous. */
+EGPU_API int egpu_dposv_mixed(egpu_handle h, int uplo, int n, int nrhs, const double* dA, int lda,
+                              const double* dB, int ldb, double* dX, int ldx, int max_iter, double tol,
+                              int* iters, double* berr);
+
+/* The tcgen05 engine of egpu_dposv_mixed, for tests and benchmarks:
+ * C (FP32, M x N, column-major) = alpha A B^T + beta C, with A (M x K) and
+ * B (N x K) column-major FP64 split into TF32 hi/lo parts; terms 1 multiplies
+ * the hi parts only, terms 3 adds hi*lo + lo*hi.  lower != 0: only the lower
+ * triangle of a square C is written.  No counterpart in the reference. */
+EGPU_API int egpu_tc_gemm_split(egpu_handle h, int M, int N, int K, double alpha, const double* dA, int lda,
+                                const double* dB, int ldb, double beta, float* dC, int ldc, int lower, int terms);
 
 /* Batched HPDSolve(LOWER, NORMAL, A_i, B_i) (HPDSolve.hpp:18-28) for `count`
  * independent systems of uneven orders n[i] <= 512 with nrhs[i] <= 16, in one

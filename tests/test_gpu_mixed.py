@@ -1,0 +1,91 @@
+"""Mixed-precision path: the tcgen05 TF32 engine against an FP64 product, and
+the mixed HPD solve (TF32 x 3 Cholesky + FP64 iterative refinement) against
+the CPU oracle's FP64 solve.
+
+Tolerances: the TF32 x 3 product keeps ~21 bits, so |C - AB^T| is bounded by
+about 2^-20 * K * max|A| max|B| (terms 3) and 2^-10 * K * max|A| max|B|
+(terms 1, one TF32 product); the refined solve must reach a normwise backward
+error <= 1e-14 and agree with the FP64 oracle solution to kappa * 1e-13."""
+import numpy as np
+import pytest
+import torch
+
+import elemental_b200 as eg
+from elemental_b200 import inputs
+from oracle import pyoracle as orc
+
+pytestmark = pytest.mark.gpu
+
+
+def _bound(A, B, K, bits):
+    return 2.0 ** (-bits) * K * np.abs(A).max() * np.abs(B).max()
+
+
+@pytest.mark.parametrize("M,N,K", [(128, 128, 32), (300, 250, 200), (1000, 77, 128), (129, 513, 45)])
+@pytest.mark.parametrize("terms", [1, 3])
+def test_tc_gemm_split_full(handle, M, N, K, terms):
+    A = inputs.normal(M, K, 11)
+    B = inputs.normal(N, K, 12)
+    C0 = inputs.normal(M, N, 13).astype(np.float32)
+    dC = eg.colmajor_cuda(C0.astype(np.float64)).float().t().contiguous().t()
+    handle.tc_gemm_split(eg.colmajor_cuda(A), eg.colmajor_cuda(B), dC, alpha=-1.0, beta=1.0, terms=terms)
+    torch.cuda.synchronize()
+    ref = C0.astype(np.float64) - A @ B.T
+    err = np.abs(dC.cpu().numpy().astype(np.float64) - ref).max()
+    bits = 20 if terms == 3 else 10
+    assert err <= _bound(A, B, K, bits) + 2.0 ** -22 * np.abs(ref).max(), err
+
+
+def test_tc_gemm_split_lower_leaves_upper(handle):
+    n, K = 384, 128
+    A = inputs.normal(n, K, 21)
+    C0 = np.full((n, n), 7.0, dtype=np.float32)
+    dC = eg.colmajor_cuda(C0.astype(np.float64)).float().t().contiguous().t()
+    dA = eg.colmajor_cuda(A)
+    handle.tc_gemm_split(dA, dA, dC, alpha=1.0, beta=0.0, lower=True, terms=3)
+    torch.cuda.synchronize()
+    out = dC.cpu().numpy().astype(np.float64)
+    low = np.tril(np.ones((n, n), bool))
+    ref = A @ A.T
+    assert np.abs(out[low] - ref[low]).max() <= _bound(A, A, K, 20)
+    assert np.all(out[~low] == 7.0)
+
+
+def _berr(A, X, B):
+    R = B - A @ X
+    return np.max(np.abs(R).max(axis=0) / (np.abs(A).sum(axis=1).max() * np.abs(X).max(axis=0) + np.abs(B).max(axis=0)))
+
+
+@pytest.mark.parametrize("n,nrhs,uplo", [(1000, 4, eg.LOWER), (777, 1, eg.UPPER), (2048, 16, eg.LOWER)])
+def test_hpd_solve_mixed_well_conditioned(handle, n, nrhs, uplo):
+    A = inputs.spd_ggt(n, 31)
+    B = inputs.normal(n, nrhs, 32)
+    X, it, be = handle.hpd_solve_mixed(eg.colmajor_cuda(A), eg.colmajor_cuda(B), uplo=uplo)
+    Xg = X.cpu().numpy()
+    assert be <= 1e-14
+    assert _berr(A, Xg, B) <= 1e-14
+    _, Xr, st = orc.hpd_solve(A, B, orc.LOWER, nb=128)
+    assert st == 0
+    assert np.abs(Xg - Xr).max() <= 1e-12 * np.abs(Xr).max()
+
+
+@pytest.mark.parametrize("kappa", [1e4, 1e6])
+def test_hpd_solve_mixed_ill_conditioned(handle, kappa):
+    n, nrhs = 1024, 8
+    A = inputs.spd_spectrum(n, kappa, 41)
+    B = inputs.normal(n, nrhs, 42)
+    dA = eg.colmajor_cuda(A)
+    X, it, be = handle.hpd_solve_mixed(dA, eg.colmajor_cuda(B))
+    assert be <= 1e-14, (it, be)
+    assert _berr(A, X.cpu().numpy(), B) <= 1e-14
+    _, Xr, st = orc.hpd_solve(A, B, orc.LOWER, nb=128)
+    assert np.abs(X.cpu().numpy() - Xr).max() <= kappa * 1e-13 * np.abs(Xr).max()
+    # inputs are left unchanged
+    assert np.array_equal(dA.cpu().numpy(), A)
+
+
+def test_hpd_solve_mixed_not_hpd(handle):
+    A = inputs.spd_ggt(300, 5)
+    A[150, 150] = -1.0
+    with pytest.raises(eg.NonHPDError):
+        handle.hpd_solve_mixed(eg.colmajor_cuda(A), eg.colmajor_cuda(inputs.normal(300, 2, 6)))
