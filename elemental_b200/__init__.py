@@ -115,6 +115,7 @@ def _declare(L):
         "egpu_dposv_batched": ([H, I, P, P, P, P, P, P, P], I),
         "egpu_dposv_mixed": ([H, I, I, I, P, I, P, I, P, I, I, D, P, P], I),
         "egpu_tc_gemm_split": ([H, I, I, I, D, P, I, P, I, D, P, I, I, I], I),
+        "egpu_host_dposv_mixed": ([H, I, I, I, P, I, P, I, P, I, I, D, P, P], I),
         "egpu_dgesv_batched": ([H, I, P, P, P, P, P, P, P], I),
         "egpu_host_dpotrf": ([H, I, I, P, I, P], I),
         "egpu_host_dpotrs": ([H, I, I, I, I, P, I, P, I], I),

@@ -374,30 +374,79 @@ int trsm_core(egpu_context* h, int side, int uplo, int trans, int unit, int m, i
   return trsm_blocked(st, side, uplo, trans, m, n, A, lda, Winv, nb, B, ldb, h->dstatus);
 }
 
+// Can the one-launch skinny sweep (trsm_skinny.cu) take this right-hand side?
+static bool skinny_ok(egpu_context* h, int nrhs, const double* B, long long ldb) {
+  return nrhs >= 1 && nrhs <= 64 && h->nb <= 128 && h->nb % 2 == 0 && ldb % 2 == 0 &&
+         reinterpret_cast<uintptr_t>(B) % 16 == 0;
+}
+
+// X := inv(T2) inv(T1) X with two skinny sweeps.  Each T is (uplo, unit) for
+// the inverted diagonal blocks and (bwd, amode) for the sweep; Winv areas and
+// the sweep flags are carved at ws_off.
+struct SweepSpec {
+  int uplo, unit, bwd, amode;
+};
+static int skinny_pair(egpu_context* h, int n, int nrhs, const double* A, long long lda, double* B, long long ldb,
+                       SweepSpec t1, SweepSpec t2, size_t ws_off) {
+  const int nb = h->nb;
+  const bool same = t1.uplo == t2.uplo && t1.unit == t2.unit;
+  const size_t wb = align_up(winv_bytes(n, nb), 256);
+  TRY(ensure_ws(h, ws_off + (same ? 1 : 2) * wb + trsm_skinny_flag_bytes(n, nb) + 4096));
+  unsigned char* base = static_cast<unsigned char*>(h->ws) + ws_off;
+  double* W1 = reinterpret_cast<double*>(base);
+  double* W2 = same ? W1 : reinterpret_cast<double*>(base + wb);
+  int* flags = reinterpret_cast<int*>(base + (same ? 1 : 2) * wb);
+  cudaStream_t st = h->stream;
+  EGPU_CUDA_TRY(cudaMemsetAsync(flags, 0, trsm_skinny_flag_bytes(n, nb), st));
+  TRY(launch_trtri_blocks(st, t1.uplo, t1.unit, A, lda, n, nb, W1, nb));
+  if (!same) TRY(launch_trtri_blocks(st, t2.uplo, t2.unit, A, lda, n, nb, W2, nb));
+  TRY(launch_trsm_skinny(st, t1.bwd, t1.amode, n, nrhs, A, lda, W1, nb, B, ldb, flags, 1, h->sm_count, h->dstatus));
+  return launch_trsm_skinny(st, t2.bwd, t2.amode, n, nrhs, A, lda, W2, nb, B, ldb, flags, 2, h->sm_count,
+                            h->dstatus);
+}
+
 int getrs_core(egpu_context* h, int orient, int n, int nrhs, const double* A, long long lda, const int* dp,
                double* B, long long ldb) {
+  // lu::SolveAfter (LU/SolveAfter.hpp:101-146)
   // laswp scratch: perm (n ints) + n*nrhs doubles; placed after the Winv area
   const size_t winv = winv_bytes(n, h->nb);
   const size_t lsw = align_up(sizeof(int) * (size_t)((n + 1) & ~1), 256) + sizeof(double) * (size_t)n * nrhs;
+  const size_t skinny_off = align_up(align_up(winv + 4096, 256) + lsw + 4096, 256);
   TRY(ensure_ws(h, align_up(winv + 4096, 256) + lsw + 4096));
   int* perm = reinterpret_cast<int*>(static_cast<unsigned char*>(h->ws) + align_up(winv + 4096, 256));
   const size_t trsm_off = 0;
+  const bool sk = skinny_ok(h, nrhs, B, ldb);
+  if (sk) {  // reserve now: a later growth of the workspace would move perm
+    TRY(ensure_ws(h, skinny_off + 2 * align_up(winv_bytes(n, h->nb), 256) + trsm_skinny_flag_bytes(n, h->nb) + 8192));
+    perm = reinterpret_cast<int*>(static_cast<unsigned char*>(h->ws) + align_up(winv + 4096, 256));
+  }
   if (orient == EGPU_NORMAL) {
     if (dp) TRY(launch_laswp_seq(h->stream, 0, n, nrhs, B, ldb, dp, n, perm));
-    TRY(trsm_core(h, EGPU_LEFT, EGPU_LOWER, 0, 1, n, nrhs, 1.0, A, lda, B, ldb, trsm_off));
-    TRY(trsm_core(h, EGPU_LEFT, EGPU_UPPER, 0, 0, n, nrhs, 1.0, A, lda, B, ldb, trsm_off));
+    if (sk) {
+      TRY(skinny_pair(h, n, nrhs, A, lda, B, ldb, {EGPU_LOWER, 1, 0, 0}, {EGPU_UPPER, 0, 1, 0}, skinny_off));
+    } else {
+      TRY(trsm_core(h, EGPU_LEFT, EGPU_LOWER, 0, 1, n, nrhs, 1.0, A, lda, B, ldb, trsm_off));
+      TRY(trsm_core(h, EGPU_LEFT, EGPU_UPPER, 0, 0, n, nrhs, 1.0, A, lda, B, ldb, trsm_off));
+    }
   } else {
-    TRY(trsm_core(h, EGPU_LEFT, EGPU_UPPER, 1, 0, n, nrhs, 1.0, A, lda, B, ldb, trsm_off));
-    TRY(trsm_core(h, EGPU_LEFT, EGPU_LOWER, 1, 1, n, nrhs, 1.0, A, lda, B, ldb, trsm_off));
+    if (sk) {
+      TRY(skinny_pair(h, n, nrhs, A, lda, B, ldb, {EGPU_UPPER, 0, 0, 1}, {EGPU_LOWER, 1, 1, 1}, skinny_off));
+    } else {
+      TRY(trsm_core(h, EGPU_LEFT, EGPU_UPPER, 1, 0, n, nrhs, 1.0, A, lda, B, ldb, trsm_off));
+      TRY(trsm_core(h, EGPU_LEFT, EGPU_LOWER, 1, 1, n, nrhs, 1.0, A, lda, B, ldb, trsm_off));
+    }
     if (dp) TRY(launch_laswp_seq(h->stream, 1, n, nrhs, B, ldb, dp, n, perm));
   }
   return EGPU_OK;
 }
-
 int potrs_core(egpu_context* h, int uplo, int n, int nrhs, const double* A, long long lda, double* B,
                long long ldb) {
   // cholesky::SolveAfter (Cholesky/SolveAfter.hpp:20-75); TRANSPOSE only
   // conjugates B, a no-op for real data.
+  if (skinny_ok(h, nrhs, B, ldb)) {
+    if (uplo == EGPU_LOWER) return skinny_pair(h, n, nrhs, A, lda, B, ldb, {EGPU_LOWER, 0, 0, 0}, {EGPU_LOWER, 0, 1, 1}, 0);
+    return skinny_pair(h, n, nrhs, A, lda, B, ldb, {EGPU_UPPER, 0, 0, 1}, {EGPU_UPPER, 0, 1, 0}, 0);
+  }
   if (uplo == EGPU_LOWER) {
     TRY(trsm_core(h, EGPU_LEFT, EGPU_LOWER, 0, 0, n, nrhs, 1.0, A, lda, B, ldb));
     TRY(trsm_core(h, EGPU_LEFT, EGPU_LOWER, 1, 0, n, nrhs, 1.0, A, lda, B, ldb));
@@ -871,6 +920,30 @@ int egpu_host_dpotrs(egpu_handle h, int uplo, int orient, int n, int nrhs, const
   TRY(potrs_core(h, uplo, n, nrhs, dA, la, dB, lb));
   TRY(d2h(h, dB, lb, B, ldb, n, nrhs));
   return read_status(h, nullptr);
+}
+
+// Host-memory form of egpu_dposv_mixed: A and B copied in, X copied out.
+int egpu_host_dposv_mixed(egpu_handle h, int uplo, int n, int nrhs, const double* A, int lda, const double* B,
+                          int ldb, double* X, int ldx, int max_iter, double tol, int* iters, double* berr) {
+  TRY(check_handle(h));
+  if (iters) *iters = 0;
+  if (berr) *berr = 0.0;
+  if (n < 0 || nrhs < 0 || bad_ld(lda, n) || bad_ld(ldb, n) || bad_ld(ldx, n) || max_iter < 0) return EGPU_ERR_ARG;
+  if (n == 0 || nrhs == 0) return EGPU_OK;
+  Enter g(h);
+  SyncScope ss(h);
+  double *dA, *dB, *dX; long long la, lb, lx;
+  TRY(h2d(h, 0, A, lda, n, n, &dA, &la));
+  TRY(h2d(h, 1, B, ldb, n, nrhs, &dB, &lb));
+  TRY(ensure_stage(h, 2, sizeof(double) * (size_t)lb * nrhs));
+  dX = static_cast<double*>(h->stage[2]);
+  lx = lb;
+  int rc = dposv_mixed_core(h, uplo, n, nrhs, dA, la, dB, lb, dX, lx, max_iter, tol, iters, berr);
+  if (rc == EGPU_OK || rc == EGPU_NO_CONVERGENCE) {
+    TRY(d2h(h, dX, lx, X, ldx, n, nrhs));
+    EGPU_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  }
+  return rc;
 }
 
 int egpu_host_dposv(egpu_handle h, int uplo, int orient, int n, int nrhs, double* A, int lda, double* B, int ldb,

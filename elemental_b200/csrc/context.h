@@ -194,6 +194,9 @@ int potrs_core(egpu_context* h, int uplo, int n, int nrhs, const double* A, long
 int trsm_core(egpu_context* h, int side, int uplo, int trans, int unit, int m, int n, double alpha, const double* A,
               long long lda, double* B, long long ldb, size_t ws_offset);
 size_t winv_bytes(int nt, int nb);
+// Mixed-precision HPD solve (mixed.cu).
+int dposv_mixed_core(egpu_context* h, int uplo, int n, int nrhs, const double* A, long long lda, const double* B,
+                     long long ldb, double* X, long long ldx, int max_iter, double tol, int* iters, double* berr);
 int trsm_blocked(cudaStream_t st, int side, int uplo, int trans, int m, int n, const double* A, long long lda,
                  const double* Winv, int nb, double* B, long long ldb, DevStatus* status);
 

@@ -43,7 +43,7 @@ bool make_tma_2d(CUtensorMap* m, int dtype, const void* base, uint64_t inner, ui
 // tcgen05 TF32 GEMM: C (FP32, col-major) = alpha * sum_t A_t B_t^T + beta * C,
 // A_t (M x K) and B_t (N x K) K-major FP32 buffers (row stride ldk elements,
 // ldk % 4 == 0, 16-byte aligned) holding TF32 values; terms 1 uses (Ahi, Bhi),
-// terms 3 adds (Ahi, Blo) and (Alo, Bhi).  tri 1: lower triangle of a square C.
+// terms 3 adds (Ahi, Blo) and (Alo, Bhi).  tri 1: only r >= c is written (M >= N).
 int launch_tc_gemm(cudaStream_t st, int M, int N, int K, float alpha, const float* Ahi, const float* Alo,
                    const float* Bhi, const float* Blo, long long ldk, float beta, float* C, long long ldc, int tri,
                    int terms, DevStatus* status);
@@ -52,6 +52,15 @@ int launch_tc_gemm(cudaStream_t st, int M, int N, int K, float alpha, const floa
 // (hi[r*ldk + c]), columns cols..ldk-1 zero.
 int launch_split_tf32(cudaStream_t st, int rows, int cols, const double* X, long long ldx, float* hi, float* lo,
                       long long ldk);
+
+// X := inv(T) X for nrhs <= 64 in one cooperative launch (trsm_skinny.cu:
+// amode/bwd select T from the stored triangle A, Winv the inverted diagonal
+// blocks).  flags: ceil(n/nb) ints that hold values other than `epoch`.
+// Returns EGPU_ERR_UNSUPPORTED when the shape or alignment does not fit.
+size_t trsm_skinny_flag_bytes(int n, int nb);
+int launch_trsm_skinny(cudaStream_t st, int bwd, int amode, int n, int nrhs, const double* A, long long lda,
+                       const double* Winv, int nb, double* X, long long ldx, int* flags, int epoch, int sm_count,
+                       DevStatus* status);
 
 // Diagonal-block Cholesky (factor in place + triangular inverse into W).
 int launch_potrf_diag(cudaStream_t st, int uplo, double* A, long long lda, int b, double* W, int ldw,

@@ -135,7 +135,7 @@ int launch_split_tf32(cudaStream_t st, int rows, int cols, const double* X, long
 
 // Workspace layout of the mixed solve.
 struct MixedLayout {
-  size_t as, af, lf, w, pkh, pkl, xw, r, winv, norms, total;
+  size_t as, af, lf, w, pkh, pkl, xw, r, winv, norms, flags, total;
   long long lds, ldf, ldk;
 };
 
@@ -150,19 +150,31 @@ static MixedLayout mixed_layout(int n, int nrhs, int nb) {
   L.af = take(sizeof(float) * L.ldf * n);
   L.lf = take(sizeof(double) * L.lds * n);
   L.w = take(sizeof(double) * (size_t)nb * nb);
-  L.pkh = take(sizeof(float) * (size_t)n * L.ldk);
-  L.pkl = take(sizeof(float) * (size_t)n * L.ldk);
+  L.pkh = take(2 * sizeof(float) * (size_t)n * L.ldk);  // two buffers (look-ahead)
+  L.pkl = take(2 * sizeof(float) * (size_t)n * L.ldk);
   L.xw = take(sizeof(double) * L.lds * std::max(nrhs, 1));
   L.r = take(sizeof(double) * L.lds * std::max(nrhs, 1));
   L.winv = take(winv_bytes(n, nb));
   L.norms = take(sizeof(double) * ((size_t)n + 4 * (size_t)std::max(nrhs, 1)));
+  L.flags = take(trsm_skinny_flag_bytes(n, nb));
   L.total = (off + 4095) & ~size_t(4095);
   return L;
 }
 
-// X := Lf^-T Lf^-1 X with the pre-inverted diagonal blocks Winv
+// X := Lf^-T Lf^-1 X with the pre-inverted diagonal blocks Winv: two
+// cooperative sweeps (nrhs <= 64), else the blocked multiply-by-inverse form.
+struct SweepFlags {
+  int* flags;
+  int epoch;
+};
 static int mixed_solve(egpu_context* h, int n, int nrhs, const double* Lf, long long lds, const double* Winv,
-                       double* X) {
+                       double* X, SweepFlags& fl) {
+  int rc = launch_trsm_skinny(h->stream, 0, 0, n, nrhs, Lf, lds, Winv, h->nb, X, lds, fl.flags, ++fl.epoch,
+                              h->sm_count, h->dstatus);
+  if (rc == EGPU_OK)
+    rc = launch_trsm_skinny(h->stream, 1, 1, n, nrhs, Lf, lds, Winv, h->nb, X, lds, fl.flags, ++fl.epoch,
+                            h->sm_count, h->dstatus);
+  if (rc != EGPU_ERR_UNSUPPORTED) return rc;
   TRY(trsm_blocked(h->stream, EGPU_LEFT, EGPU_LOWER, 0, n, nrhs, Lf, lds, Winv, h->nb, X, lds, h->dstatus));
   return trsm_blocked(h->stream, EGPU_LEFT, EGPU_LOWER, 1, n, nrhs, Lf, lds, Winv, h->nb, X, lds, h->dstatus);
 }
@@ -188,7 +200,7 @@ static int mixed_berr(egpu_context* h, int n, int nrhs, const double* R, const d
   return EGPU_OK;
 }
 
-int dposv_mixed_core(egpu_context* h, int uplo, int n, int nrhs, const double* A, long long lda, const double* B,
+int dposv_mixed_core_impl(egpu_context* h, int uplo, int n, int nrhs, const double* A, long long lda, const double* B,
                      long long ldb, double* X, long long ldx, int max_iter, double tol, int* iters, double* berr) {
   const int nb = h->nb;
   cudaStream_t st = h->stream;
@@ -205,6 +217,8 @@ int dposv_mixed_core(egpu_context* h, int uplo, int n, int nrhs, const double* A
   double* R = reinterpret_cast<double*>(ws + L.r);
   double* Winv = reinterpret_cast<double*>(ws + L.winv);
   double* norms = reinterpret_cast<double*>(ws + L.norms);
+  SweepFlags fl{reinterpret_cast<int*>(ws + L.flags), 0};
+  EGPU_CUDA_TRY(cudaMemsetAsync(fl.flags, 0, trsm_skinny_flag_bytes(n, nb), st));
   const long long lds = L.lds, ldf = L.ldf;
   EGPU_CUDA_TRY(cudaMemsetAsync(h->dstatus, 0, sizeof(DevStatus), st));
   {
@@ -213,25 +227,58 @@ int dposv_mixed_core(egpu_context* h, int uplo, int n, int nrhs, const double* A
     count_launch();
     EGPU_CUDA_TRY(cudaGetLastError());
   }
-  // ---- factorization
-  for (int k = 0; k < n; k += nb) {
+  // ---- factorization, look-ahead depth 1: the panel chain of step k+1
+  // (widen, diagonal block, L21, split) runs on the high-priority side stream
+  // as soon as the main stream has updated block column k+1; the rest of
+  // step k's trailing update follows on the main stream.  The split panel is
+  // double-buffered (step parity).
+  float* PKh2[2] = {PKh, PKh + (size_t)n * L.ldk};
+  float* PKl2[2] = {PKl, PKl + (size_t)n * L.ldk};
+  cudaStream_t sd = h->side;
+  auto panel_chain = [&](int k, cudaStream_t s) -> int {
     const int b = std::min(nb, n - k);
     const int m = n - k, m2 = m - b;
     {
-      TraceMark tm(st, kTraceOther, 0.0, 12.0 * m * b);
+      TraceMark tm(s, kTraceOther, 0.0, 12.0 * m * b);
       dim3 grid((m + 255) / 256, b);
-      widen_panel_kernel<<<grid, 256, 0, st>>>(m, b, Af + k + (long long)k * ldf, ldf, Lf + k + (long long)k * lds, lds);
+      widen_panel_kernel<<<grid, 256, 0, s>>>(m, b, Af + k + (long long)k * ldf, ldf, Lf + k + (long long)k * lds, lds);
       count_launch();
       EGPU_CUDA_TRY(cudaGetLastError());
     }
-    TRY(launch_potrf_diag(st, EGPU_LOWER, Lf + k + (long long)k * lds, lds, b, W, nb, h->dstatus, k));
-    if (m2 == 0) continue;
+    TRY(launch_potrf_diag(s, EGPU_LOWER, Lf + k + (long long)k * lds, lds, b, W, nb, h->dstatus, k));
+    if (m2 == 0) return EGPU_OK;
     double* L21 = Lf + (k + b) + (long long)k * lds;
-    TRY(launch_dgemm(st, false, false, m2, b, b, 1.0, L21, lds, W, nb, 0.0, L21, lds, 0, true, h->dstatus));
-    TRY(launch_split_tf32(st, m2, b, L21, lds, PKh, PKl, L.ldk));
-    TRY(launch_tc_gemm(st, m2, m2, b, -1.0f, PKh, PKl, PKh, PKl, L.ldk, 1.0f, Af + (k + b) + (long long)(k + b) * ldf,
-                       ldf, 1, 3, h->dstatus));
+    TRY(launch_dgemm(s, false, false, m2, b, b, 1.0, L21, lds, W, nb, 0.0, L21, lds, 0, true, h->dstatus));
+    const int par = (k / nb) & 1;
+    return launch_split_tf32(s, m2, b, L21, lds, PKh2[par], PKl2[par], L.ldk);
+  };
+  EGPU_CUDA_TRY(cudaEventRecord(h->ev_fork, st));
+  EGPU_CUDA_TRY(cudaStreamWaitEvent(sd, h->ev_fork, 0));
+  TRY(panel_chain(0, sd));
+  for (int k = 0; k < n; k += nb) {
+    const int b = std::min(nb, n - k);
+    const int m2 = n - k - b;
+    const int par = (k / nb) & 1;
+    EGPU_CUDA_TRY(cudaEventRecord(h->ev_panel[par], sd));
+    if (m2 == 0) break;
+    EGPU_CUDA_TRY(cudaStreamWaitEvent(st, h->ev_panel[par], 0));
+    const int b2 = std::min(nb, m2);
+    float* A22 = Af + (k + b) + (long long)(k + b) * ldf;
+    // (a) block column k+1 (lower trapezoid m2 x b2)
+    TRY(launch_tc_gemm(st, m2, b2, b, -1.0f, PKh2[par], PKl2[par], PKh2[par], PKl2[par], L.ldk, 1.0f, A22, ldf, 1, 3,
+                       h->dstatus));
+    EGPU_CUDA_TRY(cudaEventRecord(h->ev_rest[par], st));
+    EGPU_CUDA_TRY(cudaStreamWaitEvent(sd, h->ev_rest[par], 0));
+    TRY(panel_chain(k + b, sd));
+    // (b) the rest of the trailing lower triangle
+    const int m3 = m2 - b2;
+    if (m3 > 0)
+      TRY(launch_tc_gemm(st, m3, m3, b, -1.0f, PKh2[par] + (size_t)b2 * L.ldk, PKl2[par] + (size_t)b2 * L.ldk,
+                         PKh2[par] + (size_t)b2 * L.ldk, PKl2[par] + (size_t)b2 * L.ldk, L.ldk, 1.0f,
+                         A22 + b2 + (long long)b2 * ldf, ldf, 1, 3, h->dstatus));
   }
+  EGPU_CUDA_TRY(cudaEventRecord(h->ev_join, sd));
+  EGPU_CUDA_TRY(cudaStreamWaitEvent(st, h->ev_join, 0));
   int info = 0;
   TRY(read_status_now(h, &info));
   // ---- refinement
@@ -249,7 +296,7 @@ int dposv_mixed_core(egpu_context* h, int uplo, int n, int nrhs, const double* A
   dim3 cgrid((n + 255) / 256, nrhs);
   copy_cols_kernel<<<cgrid, 256, 0, st>>>(n, nrhs, B, ldb, Xw, lds, 0);
   count_launch();
-  TRY(mixed_solve(h, n, nrhs, Lf, lds, Winv, Xw));
+  TRY(mixed_solve(h, n, nrhs, Lf, lds, Winv, Xw, fl));
   int it = 0;
   double e = INFINITY;
   for (;;) {
@@ -258,7 +305,7 @@ int dposv_mixed_core(egpu_context* h, int uplo, int n, int nrhs, const double* A
     TRY(launch_dgemm(st, false, true, n, nrhs, n, -1.0, As, lds, Xw, lds, 1.0, R, lds, 0, false, h->dstatus));
     TRY(mixed_berr(h, n, nrhs, R, Xw, B, ldb, lds, anorm, norms + n, &e));
     if (e <= tol || it >= max_iter || !std::isfinite(e)) break;
-    TRY(mixed_solve(h, n, nrhs, Lf, lds, Winv, R));
+    TRY(mixed_solve(h, n, nrhs, Lf, lds, Winv, R, fl));
     copy_cols_kernel<<<cgrid, 256, 0, st>>>(n, nrhs, R, lds, Xw, lds, 1);
     count_launch();
     ++it;
@@ -285,7 +332,7 @@ extern "C" int egpu_dposv_mixed(egpu_handle h, int uplo, int n, int nrhs, const 
     return EGPU_ERR_ARG;
   if (n == 0 || nrhs == 0) return EGPU_OK;
   Enter en(h);
-  return egpu::dposv_mixed_core(h, uplo, n, nrhs, dA, lda, dB, ldb, dX, ldx, max_iter, tol, iters, berr);
+  return egpu::dposv_mixed_core_impl(h, uplo, n, nrhs, dA, lda, dB, ldb, dX, ldx, max_iter, tol, iters, berr);
 }
 
 // Testing entry for the tcgen05 engine: C (FP32) = alpha A B^T + beta C with
@@ -313,4 +360,9 @@ extern "C" int egpu_tc_gemm_split(egpu_handle h, int M, int N, int K, double alp
   TRY(launch_tc_gemm(st, M, N, K, (float)alpha, Ah, Al, Bh, Bl, ldk, (float)beta, dC, ldc, lower ? 1 : 0, terms,
                      h->dstatus));
   return read_status_now(h, nullptr);
+}
+
+int dposv_mixed_core(egpu_context* h, int uplo, int n, int nrhs, const double* A, long long lda, const double* B,
+                     long long ldb, double* X, long long ldx, int max_iter, double tol, int* iters, double* berr) {
+  return egpu::dposv_mixed_core_impl(h, uplo, n, nrhs, A, lda, B, ldb, X, ldx, max_iter, tol, iters, berr);
 }

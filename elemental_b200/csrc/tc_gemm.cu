@@ -8,15 +8,19 @@
 // hi*hi + hi*lo + lo*hi, which keeps ~21 bits of the FP32 product (the
 // dropped lo*lo term is 2^-22 relative).  terms = 1 is the plain TF32 product.
 //
-// One CTA of 128 threads per 128 x 128 output tile (triangular tile lists for
-// the symmetric rank-k update of a lower triangle):
-//   warp 0 lane 0: TMA producer, 128-byte-swizzled 128 x 32 tiles into a
-//                  ring of stages (mbarrier full/empty pairs, bounded waits);
-//   warp 1 lane 0: MMA issuer, tcgen05.mma.cta_group::1.kind::tf32 128x128x8,
-//                  four per 32-wide k tile and term, tcgen05.commit frees the
-//                  stage;
-//   all 4 warps  : epilogue, tcgen05.ld.32x32b of their 32 TMEM lanes (one
-//                  output row per thread) and a coalesced read-modify-write of C.
+// Persistent kernel, one CTA per SM, 192 threads, output tiles of 128 x 128
+// taken round-robin (triangular tile lists for the symmetric rank-k update of
+// a lower triangle):
+//   warp 4 lane 0: TMA producer, 128-byte-swizzled 128 x 32 tiles into a
+//                  ring of stages that runs across tile boundaries
+//                  (mbarrier full/empty pairs, bounded waits);
+//   warp 5 lane 0: MMA issuer, tcgen05.mma.cta_group::1.kind::tf32 128x128x8,
+//                  four per 32-wide k tile and term, into one of two TMEM
+//                  accumulators (256 columns) so that a tile's epilogue
+//                  overlaps the next tile's MMAs;
+//   warps 0-3    : epilogue, C rows read into registers before the
+//                  accumulator is ready, then tcgen05.ld.32x32b of their 32
+//                  TMEM lanes (one output row per thread) and a coalesced store.
 #include <cudaTypedefs.h>
 
 #include "internal.h"
@@ -26,13 +30,15 @@ namespace egpu {
 namespace {
 
 constexpr int kTcBM = 128, kTcBN = 128, kTcBK = 32;  // BK: 32 TF32 = one 128-byte swizzle row
-constexpr int kTcThreads = 128;
+constexpr int kTcThreads = 320;  // 8 epilogue warps, producer, MMA issuer
+constexpr int kTcEpiWarps = 8;
+constexpr int kTcProdWarp = 8, kTcMmaWarp = 9;
 constexpr int kTcTileBytes = kTcBM * kTcBK * 4;  // 16 KiB per operand tile
 
 template <int NT>
 struct TcShape {
   static constexpr int kOps = NT == 1 ? 2 : 4;  // A_hi, B_hi (+ A_lo, B_lo)
-  static constexpr int kStages = NT == 1 ? 4 : 3;
+  static constexpr int kStages = NT == 1 ? 6 : 3;
   static constexpr int kStageBytes = kOps * kTcTileBytes;
   static constexpr int kSmemBytes = kStages * kStageBytes + 1024 /*align*/ + 256 /*barriers*/;
 };
@@ -42,7 +48,7 @@ struct TcParams {
   long long ldc;
   int M, N, K;
   float alpha, beta;
-  int tri;  // 0 full, 1 lower triangle of a square C (tiles i >= j, diagonal tiles masked)
+  int tri;  // 0 full, 1 lower trapezoid r >= c of C (M >= N; tiles i >= j, diagonal tiles masked)
   int tiles_m, tiles_n;
   DevStatus* status;
 };
@@ -109,34 +115,34 @@ __device__ __forceinline__ void tc_tile_of(const TcParams& p, int bid, int& tm, 
 }  // namespace
 
 template <int NT>
-__global__ void __launch_bounds__(kTcThreads, 1) tc_gemm_kernel(const __grid_constant__ CUtensorMap mah,
+__global__ void __maxnreg__(200) tc_gemm_kernel(const __grid_constant__ CUtensorMap mah,
                                                                  const __grid_constant__ CUtensorMap mbh,
                                                                  const __grid_constant__ CUtensorMap mal,
                                                                  const __grid_constant__ CUtensorMap mbl,
-                                                                 TcParams p) {
+                                                                 TcParams p, int ntiles) {
   using S = TcShape<NT>;
   extern __shared__ unsigned char tc_smem_raw[];
   unsigned char* smem = reinterpret_cast<unsigned char*>(
       (reinterpret_cast<uintptr_t>(tc_smem_raw) + 1023) & ~uintptr_t(1023));  // swizzle atoms: 1 KiB aligned
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + S::kStages * S::kStageBytes);
   uint64_t* empty = full + S::kStages;
-  uint64_t* done = empty + S::kStages;
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
+  uint64_t* tfull = empty + S::kStages;  // [2] accumulator ready
+  uint64_t* tempty = tfull + 2;          // [2] accumulator drained (8 epilogue warps arrive)
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(tempty + 2);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   if (p.status != nullptr && ((volatile DevStatus*)p.status)->code != 0) return;  // uniform
-  int tm, tn;
-  tc_tile_of(p, blockIdx.x, tm, tn);
-  const int m0 = tm * kTcBM, n0 = tn * kTcBN;
   const int KT = (p.K + kTcBK - 1) / kTcBK;
 
   if (tid == 0) {
     for (int s = 0; s < S::kStages; ++s) { mbar_init(&full[s], 1); mbar_init(&empty[s], 1); }
-    mbar_init(done, 1);
+    for (int a = 0; a < 2; ++a) { mbar_init(&tfull[a], 1); mbar_init(&tempty[a], kTcEpiWarps); }
+    *abort_flag = 0;
     fence_mbar_init();
   }
-  if (warp == 1) {  // 128 TMEM columns: the 128 x 128 FP32 accumulator
-    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 128;" ::"r"(smem_u32(tmem_slot))
+  if (warp == kTcMmaWarp) {  // 256 TMEM columns: two 128 x 128 FP32 accumulators
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 256;" ::"r"(smem_u32(tmem_slot))
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
@@ -144,79 +150,114 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_gemm_kernel(const __grid_con
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = *tmem_slot;
-  bool ok = true;
 
-  if (warp == 0 && lane == 0) {
-    // ---- TMA producer
-    tma_prefetch_desc(&mah);
-    tma_prefetch_desc(&mbh);
-    if (NT == 3) { tma_prefetch_desc(&mal); tma_prefetch_desc(&mbl); }
-    for (int kt = 0; kt < KT; ++kt) {
-      const int s = kt % S::kStages;
-      const uint32_t ph = (uint32_t)(kt / S::kStages) & 1u;
-      if (!mbar_wait_bounded(&empty[s], ph ^ 1u)) { ok = false; set_status(p.status, kTimeout, 101); break; }
-      unsigned char* st = smem + s * S::kStageBytes;
-      mbar_expect_tx(&full[s], S::kStageBytes);
-      const int k0 = kt * kTcBK;
-      tma_load_2d(st, &mah, &full[s], k0, m0);
-      tma_load_2d(st + kTcTileBytes, &mbh, &full[s], k0, n0);
-      if (NT == 3) {
-        tma_load_2d(st + 2 * kTcTileBytes, &mal, &full[s], k0, m0);
-        tma_load_2d(st + 3 * kTcTileBytes, &mbl, &full[s], k0, n0);
-      }
-    }
-  } else if (warp == 1 && lane == 0) {
-    // ---- MMA issuer
-    for (int kt = 0; kt < KT; ++kt) {
-      const int s = kt % S::kStages;
-      const uint32_t ph = (uint32_t)(kt / S::kStages) & 1u;
-      if (!mbar_wait_bounded(&full[s], ph)) { ok = false; set_status(p.status, kTimeout, 102); break; }
-      tc_fence_after();
-      const uint32_t st = smem_u32(smem + s * S::kStageBytes);
-      const uint64_t ah = sw128_kmajor_desc(st), bh = sw128_kmajor_desc(st + kTcTileBytes);
-      const uint64_t al = sw128_kmajor_desc(st + 2 * kTcTileBytes), bl = sw128_kmajor_desc(st + 3 * kTcTileBytes);
-#pragma unroll
-      for (int kk = 0; kk < kTcBK / 8; ++kk) {  // 8 TF32 = 32 bytes per MMA along K
-        const uint64_t adv = (uint64_t)((kk * 32) >> 4);
-        tc_mma(tmem, ah + adv, bh + adv, (kt | kk) != 0);
-        if (NT == 3) {
-          tc_mma(tmem, ah + adv, bl + adv, 1u);
-          tc_mma(tmem, al + adv, bh + adv, 1u);
-        }
-      }
-      tc_commit(&empty[s]);  // stage free once these MMAs have read it
-    }
-    tc_commit(done);
-  }
-  __syncwarp();
-  // ---- epilogue: every thread owns output row m0 + 32 warp + lane
-  bool have = mbar_wait_bounded(done, 0);
-  if (!have && tid == 0) set_status(p.status, kTimeout, 103);
-  tc_fence_after();
-  if (have && ok && KT > 0) {
-    const int r = m0 + warp * 32 + lane;
-#pragma unroll 1
-    for (int c0 = 0; c0 < kTcBN; c0 += 32) {
-      float v[32];
-      tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
-      if (r < p.M) {
-        float* crow = p.C + r;
-#pragma unroll
-        for (int j = 0; j < 32; ++j) {
-          const int c = n0 + c0 + j;
-          if (c < p.N && (p.tri == 0 || r >= c)) {
-            float* cp = crow + (long long)c * p.ldc;
-            *cp = (p.beta == 0.0f) ? p.alpha * v[j] : fmaf(p.alpha, v[j], p.beta * *cp);
+  if (warp == kTcProdWarp) {
+    if (lane == 0) {  // ---- TMA producer
+      tma_prefetch_desc(&mah);
+      tma_prefetch_desc(&mbh);
+      if (NT == 3) { tma_prefetch_desc(&mal); tma_prefetch_desc(&mbl); }
+      int g = 0;
+      for (int t = blockIdx.x; t < ntiles && !*abort_flag; t += gridDim.x) {
+        int tm, tn;
+        tc_tile_of(p, t, tm, tn);
+        const int m0 = tm * kTcBM, n0 = tn * kTcBN;
+        for (int kt = 0; kt < KT; ++kt, ++g) {
+          const int s = g % S::kStages;
+          const uint32_t ph = (uint32_t)(g / S::kStages) & 1u;
+          if (!mbar_wait_bounded(&empty[s], ph ^ 1u)) { *abort_flag = 1; set_status(p.status, kTimeout, 101); break; }
+          unsigned char* st = smem + s * S::kStageBytes;
+          mbar_expect_tx(&full[s], S::kStageBytes);
+          const int k0 = kt * kTcBK;
+          tma_load_2d(st, &mah, &full[s], k0, m0);
+          tma_load_2d(st + kTcTileBytes, &mbh, &full[s], k0, n0);
+          if (NT == 3) {
+            tma_load_2d(st + 2 * kTcTileBytes, &mal, &full[s], k0, m0);
+            tma_load_2d(st + 3 * kTcTileBytes, &mbl, &full[s], k0, n0);
           }
         }
       }
     }
+  } else if (warp == kTcMmaWarp) {
+    if (lane == 0) {  // ---- MMA issuer
+      int g = 0, i = 0;
+      for (int t = blockIdx.x; t < ntiles && !*abort_flag; t += gridDim.x, ++i) {
+        const int a = i & 1;
+        const uint32_t acc_addr = tmem + (uint32_t)(a * kTcBN);
+        if (!mbar_wait_bounded(&tempty[a], ((uint32_t)(i >> 1) & 1u) ^ 1u)) {
+          *abort_flag = 1; set_status(p.status, kTimeout, 104); break;
+        }
+        tc_fence_after();
+        for (int kt = 0; kt < KT; ++kt, ++g) {
+          const int s = g % S::kStages;
+          const uint32_t ph = (uint32_t)(g / S::kStages) & 1u;
+          if (!mbar_wait_bounded(&full[s], ph)) { *abort_flag = 1; set_status(p.status, kTimeout, 102); break; }
+          tc_fence_after();
+          const uint32_t st = smem_u32(smem + s * S::kStageBytes);
+          const uint64_t ah = sw128_kmajor_desc(st), bh = sw128_kmajor_desc(st + kTcTileBytes);
+          const uint64_t al = sw128_kmajor_desc(st + 2 * kTcTileBytes), bl = sw128_kmajor_desc(st + 3 * kTcTileBytes);
+#pragma unroll
+          for (int kk = 0; kk < kTcBK / 8; ++kk) {  // 8 TF32 = 32 bytes per MMA along K
+            const uint64_t adv = (uint64_t)((kk * 32) >> 4);
+            tc_mma(acc_addr, ah + adv, bh + adv, (kt | kk) != 0);
+            if (NT == 3) {
+              tc_mma(acc_addr, ah + adv, bl + adv, 1u);
+              tc_mma(acc_addr, al + adv, bh + adv, 1u);
+            }
+          }
+          tc_commit(&empty[s]);  // stage free once these MMAs have read it
+        }
+        tc_commit(&tfull[a]);  // accumulator a complete
+      }
+    }
+  } else {
+    // ---- epilogue: warp e reads TMEM lanes 32 (e % 4) .. (its quarter) and
+    // columns 64 (e / 4) .. of each tile; each thread owns one output row.
+    const int q = warp & 3, half = warp >> 2;
+    int i = 0;
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++i) {
+      int tm, tn;
+      tc_tile_of(p, t, tm, tn);
+      const int m0 = tm * kTcBM, n0 = tn * kTcBN + half * 64;
+      const int r = m0 + q * 32 + lane;
+      const int a = i & 1;
+      // columns n0 + j, j < jmax, of row r are written (bounds, lower triangle)
+      int jmax = r < p.M ? min(64, p.N - n0) : 0;
+      if (p.tri) jmax = min(jmax, r - n0 + 1);
+      float* cbase = p.C + (long long)n0 * p.ldc + (r < p.M ? r : 0);
+      // this thread's 64 C entries in flight while the MMAs run
+      float cv[64];
+      {
+        const float* cp = cbase;
+#pragma unroll
+        for (int j = 0; j < 64; ++j, cp += p.ldc) cv[j] = (p.beta != 0.0f && j < jmax) ? *cp : 0.0f;
+      }
+      const bool have = __all_sync(0xffffffffu, mbar_wait_bounded(&tfull[a], (uint32_t)(i >> 1) & 1u));
+      if (!have) {
+        if (lane == 0) { *abort_flag = 1; set_status(p.status, kTimeout, 103); }
+        break;
+      }
+      tc_fence_after();
+#pragma unroll
+      for (int c0 = 0; c0 < 64; c0 += 32) {
+        float v[32];
+        tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(a * kTcBN + half * 64 + c0), v);
+        float* cp;  // opaque copy of the base: keeps the load addresses from staying live
+        asm volatile("mov.b64 %0, %1;" : "=l"(cp) : "l"(cbase + (long long)c0 * p.ldc));
+#pragma unroll
+        for (int j = 0; j < 32; ++j, cp += p.ldc)
+          if (c0 + j < jmax) *cp = fmaf(p.alpha, v[j], p.beta * cv[c0 + j]);
+      }
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&tempty[a])) : "memory");
+      if (*abort_flag) break;
+    }
   }
   tc_fence_before();
   __syncthreads();
-  if (warp == 1) {
+  if (warp == kTcMmaWarp) {
     tc_fence_after();
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 128;" ::"r"(tmem) : "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 256;" ::"r"(tmem) : "memory");
   }
 }
 
@@ -233,7 +274,10 @@ static cudaError_t tc_launch_variant(cudaStream_t st, const CUtensorMap& mah, co
     if (e != cudaSuccess) return e;
     if (dev < 32) attr_mask |= (1u << dev);
   }
-  kern<<<(unsigned)nblocks, kTcThreads, TcShape<NT>::kSmemBytes, st>>>(mah, mbh, mal, mbl, p);
+  int dev_sms = 148;
+  cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, dev);
+  const unsigned grid = (unsigned)std::min<long long>(nblocks, dev_sms);
+  kern<<<grid, kTcThreads, TcShape<NT>::kSmemBytes, st>>>(mah, mbh, mal, mbl, p, (int)nblocks);
   count_launch();
   return cudaGetLastError();
 }
@@ -243,7 +287,7 @@ int launch_tc_gemm(cudaStream_t st, int M, int N, int K, float alpha, const floa
                    int terms, DevStatus* status) {
   if (M <= 0 || N <= 0 || K <= 0) return M <= 0 || N <= 0 ? EGPU_OK : EGPU_ERR_ARG;
   if (terms != 1 && terms != 3) return EGPU_ERR_ARG;
-  if (tri == 1 && M != N) return EGPU_ERR_ARG;
+  if (tri == 1 && M < N) return EGPU_ERR_ARG;  // lower trapezoid: rows >= columns
   if (ldk < K || ldk % 4 != 0) return EGPU_ERR_ALIGN;
   for (const float* q : {Ahi, Bhi, terms == 3 ? Alo : Ahi, terms == 3 ? Blo : Bhi})
     if (q == nullptr || reinterpret_cast<uintptr_t>(q) % 16 != 0) return EGPU_ERR_ALIGN;
@@ -264,9 +308,12 @@ int launch_tc_gemm(cudaStream_t st, int M, int N, int K, float alpha, const floa
   p.tiles_m = (M + kTcBM - 1) / kTcBM;
   p.tiles_n = (N + kTcBN - 1) / kTcBN;
   p.status = status;
-  const long long nblocks =
-      tri ? (long long)p.tiles_n * (p.tiles_n + 1) / 2 : (long long)p.tiles_m * p.tiles_n;
-  const double flops = (tri ? (double)M * (M + 1) : 2.0 * M * N) * K * terms;
+  long long nblocks = (long long)p.tiles_m * p.tiles_n;
+  if (tri) {  // tiles on or below the diagonal: column j holds tiles j .. tiles_m-1
+    nblocks = 0;
+    for (int j = 0; j < p.tiles_n; ++j) nblocks += p.tiles_m - j;
+  }
+  const double flops = (tri ? (double)N * (N + 1) + 2.0 * (double)(M - N) * N : 2.0 * M * N) * K * terms;
   const double bytes = 4.0 * terms * ((double)M * K + (double)N * K) / (terms == 3 ? 1.5 : 1.0) +
                        4.0 * (beta == 0.0f ? 1.0 : 2.0) * M * N * (tri ? 0.5 : 1.0);
   TraceMark tm(st, kTraceTc, flops, bytes);

@@ -161,6 +161,11 @@ EGPU_API int egpu_dposv_mixed(egpu_handle h, int uplo, int n, int nrhs, const do
                               const double* dB, int ldb, double* dX, int ldx, int max_iter, double tol,
                               int* iters, double* berr);
 
+/* Host-memory form of egpu_dposv_mixed (A, B, X in host memory). */
+EGPU_API int egpu_host_dposv_mixed(egpu_handle h, int uplo, int n, int nrhs, const double* A, int lda,
+                                   const double* B, int ldb, double* X, int ldx, int max_iter, double tol,
+                                   int* iters, double* berr);
+
 /* The tcgen05 engine of egpu_dposv_mixed, for tests and benchmarks:
  * C (FP32, M x N, column-major) = alpha A B^T + beta C, with A (M x K) and
  * B (N x K) column-major FP64 split into TF32 hi/lo parts; terms 1 multiplies
