@@ -1,24 +1,32 @@
 #!/usr/bin/env python
-"""Benchmark: FP64-accurate factor-and-solve throughput on B200.
+"""Benchmark: FP64-accurate solves per second on B200, mixed precision +
+iterative refinement, batched and served forms against plain FP64.
 
-Workload (default, one GPU): LU with partial pivoting + solve of one dense
-system, n = 8192, block size 128, A ~ U[-1,1] (seeded), B = 64 right-hand
-sides ~ N(0,1).  One "step" = restore A and B from pristine device copies,
-factor (egpu_dgetrf), solve (egpu_dgetrs).  metric = solves per second
-(systems factored and solved), whole job.
+Workloads (--workload; the default is the first):
+  mixed    Mixed-precision Cholesky + IR, n = 16384, 32 RHS: A = Q diag(s) Q^T,
+           Q the orthogonal factor of a seeded N(0,1) matrix, s log-spaced over
+           [1, 1e6]; B ~ N(0,1).  One step = egpu_dposv_mixed (tcgen05 TF32 x 3
+           trailing updates, FP64 refinement to backward error <= 1e-14).  The
+           plain FP64 path (egpu_dposv: Cholesky + HPD solve) is timed on the
+           same A and B in the same run and reported beside it.
+  lu       Plain FP64 LU with partial pivoting + solve, n = 8192, 64 RHS,
+           A ~ U[-1,1], B ~ N(0,1): egpu_dgetrf + egpu_dgetrs per step.
+  chol     Plain FP64 Cholesky + HPD solve, n = 2048, 16 RHS, A = G G^T + n I.
+  batched  4096 HPD + 4096 general systems, n ~ U{32..512}, 1-8 RHS, one
+           persistent launch per kind, the step replayed from a CUDA graph.
+  serve    Poisson request stream through the continuous-batching server.
 
   value      device-resident inputs (HBM), CUDA events on the library stream
-  e2e        the same factor-and-solve through the host-memory C ABI entry
-             GaussianElimination (egpu_host_dgesv): pinned host A, B copied in,
-             factored and solved, A and X copied back, every step
-  roofline   the trailing-update kernel (FP64 DMMA GEMM), from per-launch CUDA
-             events recorded inside the timed region
+  e2e        the same solves through the host-memory C ABI entry, pinned host
+             inputs copied in and the solutions copied out every step
+  roofline   the dominant kernel, from per-launch CUDA events recorded inside
+             the timed region
   cpu_baseline  the CPU oracle (the reference's algorithm restated in C,
-             OpenMP over all host cores) on the same input, rank 0 only
+             OpenMP over all host cores), rank 0 only, on a bounded sample
 
 --impl reference runs the oracle arm alone on the host cores.
-Multi-GPU (torchrun, one rank per GPU): every rank factors its own
-independently seeded system; no data-path collective ("scaling": "weak").
+Multi-GPU (torchrun, one rank per GPU): every rank solves its own
+independently seeded problems; no data-path collective ("scaling": "weak").
 """
 from __future__ import annotations
 
@@ -36,16 +44,41 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-N = 8192
-NRHS = 64
 NB = 128
 SEED = 20240
 FP64_PEAK_TFLOPS = 37.15  # measured DMMA peak, profiles/fp64_peak.md
 HBM_PEAK_GBS_FALLBACK = 6650.0
 
+WORKLOADS = {
+    "mixed": {"n": 16384, "nrhs": 32, "kappa": 1e6,
+              "metric": "FP64-accurate solves/sec (HPD solve, n=16384, 32 RHS, kappa 1e6): mixed-precision+IR",
+              "desc": "mixed-precision Cholesky (tcgen05 TF32x3 trailing updates) + FP64 iterative refinement to "
+                      "backward error <= 1e-14, n=16384, nb=128, 32 RHS, A = Q diag(s) Q^T, s log-spaced [1, 1e6]"},
+    "lu": {"n": 8192, "nrhs": 64,
+           "metric": "FP64-accurate solves/sec (LU-PP factor + 64-RHS solve, n=8192)",
+           "desc": "LU partial pivoting + solve, n=8192, nb=128, 64 RHS (plain FP64)"},
+    "batched": {"count": 4096, "nmin": 32, "nmax": 512, "rmin": 1, "rmax": 8, "n": 512, "nrhs": 8,
+                "metric": "FP64-accurate solves/sec (batched uneven: 4096 HPD + 4096 GE systems, n in [32, 512])",
+                "desc": "batched uneven solves: 4096 HPD (G G^T + n I) and 4096 general (U[-1,1]) systems, n ~ U{32..512}, "
+                        "1-8 RHS, FP64, one persistent launch per kind (autotuned grid), the step captured in a CUDA graph"},
+    "serve": {"rate": 2000.0, "window_s": 2.0, "nmin": 64, "nmax": 8192, "kmin": 1e2, "kmax": 1e8, "rmin": 1,
+              "rmax": 64, "pool": 48, "budget": 150 << 30, "slots": 4, "n": 8192, "nrhs": 64,
+              "metric": "FP64-accurate solves/sec and p50/p99 latency (served stream, Poisson 2000 req/s): mixed+IR",
+              "desc": "request server, continuous batching: Poisson arrivals (mean 2000 req/s, 2 s window), 50/50 "
+                      "HPD/GE, n log-uniform [64, 8192], kappa log-uniform [1e2, 1e8] (Q diag(s) Q^T), 1-64 RHS, "
+                      "150 GB HBM budget, 4 slots"},
+    "chol": {"n": 2048, "nrhs": 16,
+             "metric": "FP64-accurate solves/sec (Cholesky + 16-RHS HPD solve, n=2048)",
+             "desc": "Cholesky + HPD solve, lower, n=2048, nb=128, 16 RHS (plain FP64)"},
+}
+
 
 def flops_lu_solve(n, nrhs):
     return 2.0 * n ** 3 / 3.0 + 2.0 * n * n * nrhs
+
+
+def flops_chol_solve(n, nrhs):
+    return n ** 3 / 3.0 + 2.0 * n * n * nrhs
 
 
 def measured_peaks():
@@ -72,7 +105,7 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                 "-lms", "50"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
         except Exception:
@@ -137,97 +170,165 @@ def max_over_ranks(ws, x, device):
     return float(t.item())
 
 
-def cpu_oracle_solve(n, nrhs, seed, threads):
-    """One LU + solve by the CPU oracle; returns seconds."""
+def make_inputs(kind, n, nrhs, seed, device=None):
+    """Seeded inputs of a workload (numpy, column-major; the mixed workload's
+    A is built on the GPU when ``device`` is given)."""
     from elemental_b200 import inputs
+    if kind == "lu":
+        A = inputs.uniform(n, n, seed)
+    elif kind == "chol":
+        A = inputs.spd_ggt(n, seed)
+    else:
+        A = inputs.spd_spectrum(n, WORKLOADS["mixed"]["kappa"], seed, device=device)
+    B = inputs.normal(n, nrhs, seed + 1)
+    return A, B
+
+
+def cpu_oracle_solve(kind, n, nrhs, seed, threads):
+    """One factor + solve by the CPU oracle (FP64: the reference's algorithm);
+    returns seconds."""
     from oracle import pyoracle as orc
     orc.set_threads(threads)
-    A = inputs.uniform(n, n, seed)
-    B = inputs.normal(n, nrhs, seed + 1)
+    A, B = make_inputs(kind if kind != "mixed" else "chol", n, nrhs, seed)
     t0 = time.perf_counter()
-    F, p, st = orc.lu(A, NB)
-    X = orc.lu_solve_after(F, p, B, orc.NORMAL)
+    if kind == "lu":
+        F, p, st = orc.lu(A, NB)
+        X = orc.lu_solve_after(F, p, B, orc.NORMAL)
+    else:
+        _, X, st = orc.hpd_solve(A, B, orc.LOWER, nb=NB)
     dt = time.perf_counter() - t0
     assert st == 0 and np.isfinite(X).all()
     return dt
 
 
+def flops_of(kind, n, nrhs):
+    return flops_lu_solve(n, nrhs) if kind == "lu" else flops_chol_solve(n, nrhs)
+
+
+def cpu_sample(kind, n_full, nrhs, seed, threads, budget_s, reps):
+    """Time the oracle on a bounded sample: the largest n <= n_full (halving)
+    whose `reps` runs fit in about budget_s; returns (seconds per full-size
+    solve, sample description)."""
+    t_probe = cpu_oracle_solve(kind, 1024, nrhs, seed, threads)
+    est = t_probe * flops_of(kind, n_full, nrhs) / flops_of(kind, 1024, nrhs)
+    n_s = n_full
+    while n_s > 1024 and est * flops_of(kind, n_s, nrhs) / flops_of(kind, n_full, nrhs) * reps > budget_s:
+        n_s //= 2
+    times = [cpu_oracle_solve(kind, n_s, nrhs, seed + 7 * i, threads) for i in range(reps)]
+    scale = flops_of(kind, n_s, nrhs) / flops_of(kind, n_full, nrhs)
+    t_full = sum(times) / len(times) / scale
+    what = "Cholesky + HPD solve" if kind != "lu" else "LU + solve"
+    return t_full, f"{reps} FP64 {what} runs at n={n_s}, {nrhs} RHS (flop-scaled to n={n_full})"
+
+
 def reference_arm(args, ws, rank):
     """CPU oracle timed on the host cores (the reference's own algorithm for
     this path, restated in C; the reference itself needs MPI + BLAS and is not
-    built here)."""
+    built here).  For the mixed workload the reference has no mixed-precision
+    path: its FP64 Cholesky + HPD solve is the baseline."""
     if rank != 0:
         return
+    W = WORKLOADS[args.workload]
+    n, nrhs = W["n"], W["nrhs"]
     threads = os.cpu_count() or 1
-    # warm-up: small problems (thread pool, page faults)
+    if args.workload == "batched":
+        return reference_batched(args, W, threads)
+    if args.workload == "serve":
+        return reference_serve(args, W, threads)
     for _ in range(max(args.warmup, 0)):
-        cpu_oracle_solve(512, NRHS, SEED, threads)
-    # size the sample so that the K timed steps stay within ~150 s
-    t_probe = cpu_oracle_solve(2048, NRHS, SEED, threads)
-    est_full = t_probe * flops_lu_solve(N, NRHS) / flops_lu_solve(2048, NRHS)
-    n_s = N
-    while n_s > 1024 and est_full * (n_s / N) ** 3 * args.steps > 150.0:
-        n_s //= 2
-    times = [cpu_oracle_solve(n_s, NRHS, SEED + 7 * i, threads) for i in range(args.steps)]
-    scale = flops_lu_solve(n_s, NRHS) / flops_lu_solve(N, NRHS)
-    t_step = sum(times) / len(times) / scale  # seconds per full-size solve
-    value = 1.0 / t_step
+        cpu_oracle_solve(args.workload, 512, nrhs, SEED, threads)
+    t_full, sample = cpu_sample(args.workload, n, nrhs, SEED, threads, 150.0, args.steps)
+    value = 1.0 / t_full
     line = {
-        "metric": "FP64-accurate solves/sec (LU-PP factor + 64-RHS solve, n=8192)",
-        "value": value, "unit": "solves/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": t_step * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f64", "data": "synthetic (seeded U[-1,1] A, N(0,1) B)", "impl": "reference",
-        "config": {"workload": "LU partial pivoting + solve, n=8192, nb=128, 64 RHS", "n": N, "nrhs": NRHS,
-                   "nb": NB, "parallelism": "host cores"},
-        "cpu_baseline": {"value": value, "unit": "solves/s", "cores": threads, "kind": "port",
-                         "sample": f"{args.steps} LU+solve runs at n={n_s} (flop-scaled to n={N})"},
+        "metric": W["metric"], "value": value, "unit": "solves/s", "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": t_full * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)", "impl": "reference",
+        "config": {"workload": W["desc"], "n": n, "nrhs": nrhs, "nb": NB, "parallelism": "host cores"},
+        "cpu_baseline": {"value": value, "unit": "solves/s", "cores": threads, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
 
 
-def our_arm(args, ws, rank, local):
-    import torch
-    import elemental_b200 as eg
+def reference_batched(args, W, threads):
+    """Oracle HPD solves and GaussianEliminations on systems drawn from the
+    batch (same sizes and right-hand-side counts), all host cores."""
     from elemental_b200 import inputs
+    from oracle import pyoracle as orc
+    orc.set_threads(threads)
+    sizes, rhs = batched_sets(SEED, W)
+    r = np.random.default_rng(SEED + 5)
+    per_step = 16
+    times = []
+    for s in range(args.warmup + args.steps):
+        idx = r.choice(W["count"], per_step, replace=False)
+        mats = [(inputs.spd_ggt(sizes[0][i], int(i)), inputs.normal(sizes[0][i], rhs[0][i], int(i) + 1),
+                 inputs.uniform(sizes[1][i], sizes[1][i], int(i) + 2), inputs.normal(sizes[1][i], rhs[1][i], int(i) + 3))
+                for i in idx]
+        t0 = time.perf_counter()
+        for Ah, Bh, Ag, Bg in mats:
+            orc.hpd_solve(Ah, Bh, orc.LOWER, nb=32)
+            orc.gaussian_elimination(Ag, Bg, nb=32)
+        if s >= args.warmup:
+            times.append(time.perf_counter() - t0)
+    value = 2 * per_step * len(times) / sum(times)
+    line = {
+        "metric": W["metric"], "value": value, "unit": "solves/s", "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * 2 * W["count"] / value, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)", "impl": "reference",
+        "config": {"workload": W["desc"], "count_per_kind": W["count"], "parallelism": "host cores"},
+        "cpu_baseline": {"value": value, "unit": "solves/s", "cores": threads, "kind": "port",
+                         "sample": f"{per_step} HPD + {per_step} GE systems per step drawn from the batch"},
+        "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
 
-    torch.cuda.set_device(local)
-    dev = torch.device("cuda", local)
-    h = eg.Handle(local)
-    h.set_blocksize(NB)
-    stream = torch.cuda.Stream(device=dev)
-    seed = SEED + 1000 * rank
-    A_host = inputs.uniform(N, N, seed)
-    B_host = inputs.normal(N, NRHS, seed + 1)
-    A0 = eg.colmajor_cuda(A_host, device=dev)
-    B0 = eg.colmajor_cuda(B_host, device=dev)
-    A = eg.empty_colmajor(N, N, device=dev)
-    B = eg.empty_colmajor(N, NRHS, device=dev)
-    p = torch.zeros(N, dtype=torch.int32, device=dev)
 
-    def step():
-        A.copy_(A0)
-        B.copy_(B0)
-        h.lu(A, p)
-        h.lu_solve_after(A, p, B, eg.NORMAL)
+def reference_serve(args, W, threads):
+    """The oracle's FP64 rate on the served mix: Cholesky + solve and LU +
+    solve timed at n = 2048 on all host cores, applied to the stream's mean
+    work per request (E[n^3] of the log-uniform size law, 50/50 kinds, mean
+    32 RHS); requests served one after another."""
+    lo, hi = np.log(W["nmin"]), np.log(W["nmax"])
+    en3 = (W["nmax"] ** 3 - W["nmin"] ** 3) / (3.0 * (hi - lo))
+    en2 = (W["nmax"] ** 2 - W["nmin"] ** 2) / (2.0 * (hi - lo))
+    k = 0.5 * (W["rmin"] + W["rmax"])
+    work = 0.5 * (en3 / 3.0 + 2.0 * en2 * k) + 0.5 * (2.0 * en3 / 3.0 + 2.0 * en2 * k)
+    ns = 2048
+    for _ in range(max(args.warmup, 1)):
+        cpu_oracle_solve("chol", 512, 32, SEED, threads)
+    tc = cpu_oracle_solve("chol", ns, 32, SEED, threads)
+    tl = cpu_oracle_solve("lu", ns, 32, SEED, threads)
+    rate = (flops_chol_solve(ns, 32) + flops_lu_solve(ns, 32)) / (tc + tl)  # FP64 flop/s of the oracle
+    value = rate / work
+    line = {
+        "metric": W["metric"], "value": value, "unit": "solves/s", "n_gpus": args.gpus, "steps": 1,
+        "warmup": args.warmup, "ms_per_step": 1e3 / value, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)", "impl": "reference",
+        "config": {"workload": W["desc"], "parallelism": "host cores"},
+        "cpu_baseline": {"value": value, "unit": "solves/s", "cores": threads, "kind": "port",
+                         "sample": f"one Cholesky+solve and one LU+solve at n={ns}, 32 RHS; oracle flop rate "
+                                   f"{rate / 1e9:.1f} GFLOP/s applied to the stream's mean work per request"},
+        "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
 
+
+def timed(args, ws, dev, stream, h, step):
+    """W warm-up steps, then K timed steps between barriers + syncs, with the
+    launch trace and the clock sampler on; returns (ms over K, trace, launches, clocks)."""
+    import torch
     with torch.cuda.stream(stream):
         for _ in range(args.warmup):
             step()
         torch.cuda.synchronize(dev)
-        # accuracy of the last solve (checked, reported)
-        X = B.double()
-        R = torch.from_numpy(B_host).to(dev) - torch.from_numpy(A_host).to(dev) @ X
-        bwd = float(R.abs().sum(0).max() / (torch.from_numpy(A_host).to(dev).abs().sum(0).max() *
-                                            X.abs().sum(0).max() * N * np.finfo(np.float64).eps))
-        del R, X
         barrier(ws)
         torch.cuda.synchronize(dev)
         launches0 = h.launch_count()
         h.trace_enable(True)
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
-        with ClockSampler(local) as clk:
+        with ClockSampler(dev.index) as clk:
             e0.record(stream)
             for _ in range(args.steps):
                 step()
@@ -238,80 +339,483 @@ def our_arm(args, ws, rank, local):
         launches = h.launch_count() - launches0
         barrier(ws)
         ms = max_over_ranks(ws, e0.elapsed_time(e1), dev)
+    return ms, trace, launches, clk.summary()
 
+
+def backward_error(A, X, B):
+    """max_j ||b_j - A x_j||_inf / (||A||_inf ||x_j||_inf + ||b_j||_inf) (torch, on the device)."""
+    R = B - A @ X
+    den = A.abs().sum(1).max() * X.abs().amax(0) + B.abs().amax(0)
+    return float((R.abs().amax(0) / den).max())
+
+
+def roofline_of(trace, kind, peaks):
+    """Roofline line for one traced kernel class."""
+    t = trace.get(kind, {})
+    if not t or not t.get("launches") or t["ms"] <= 0:
+        return None
+    total_ms = sum(v["ms"] for v in trace.values())
+    if kind == "tc":  # FP32 C read-modify-write + split panels: HBM-bound at K = 128
+        peak = peaks.get("hbm_gbs") or HBM_PEAK_GBS_FALLBACK
+        achieved = t["bytes"] / (t["ms"] / 1e3) / 1e9
+        return {"bound": "hbm", "kernel": "tc_gemm_kernel (tcgen05 TF32x3 trailing update)", "achieved": achieved,
+                "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)" if peaks.get("hbm_gbs") else "fallback",
+                "tensor_tflops": t["flops"] / (t["ms"] / 1e3) / 1e12, "traffic": None,
+                "launches": t["launches"], "share_of_traced_time": t["ms"] / total_ms}
+    achieved = t["flops"] / (t["ms"] / 1e3) / 1e12
+    return {"bound": "tensor", "kernel": "dgemm_tma_kernel (FP64 DMMA trailing update)", "achieved": achieved,
+            "peak": FP64_PEAK_TFLOPS, "unit": "TFLOP/s", "frac": achieved / FP64_PEAK_TFLOPS, "traffic": None,
+            "peak_source": "measured FP64 DMMA peak (profiles/fp64_peak.md); MEASURED_PEAKS.json has no FP64 entry",
+            "launches": t["launches"], "share_of_traced_time": t["ms"] / total_ms}
+
+
+def pinned_like(a):
+    import torch
+    t = torch.empty((a.size,), dtype=torch.float64, pin_memory=True).numpy().reshape(a.shape, order="F")
+    np.copyto(t, a)
+    return t
+
+
+def our_arm(args, ws, rank, local):
+    import torch
+    import elemental_b200 as eg
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    h = eg.Handle(local)
+    h.set_blocksize(NB)
+    stream = torch.cuda.Stream(device=dev)
+    kind = args.workload
+    W = WORKLOADS[kind]
+    n, nrhs = W["n"], W["nrhs"]
+    seed = SEED + 1000 * rank
+    A_host, B_host = make_inputs(kind, n, nrhs, seed, device=dev if kind == "mixed" else None)
+    A0 = eg.colmajor_cuda(A_host, device=dev)
+    B0 = eg.colmajor_cuda(B_host, device=dev)
+    A = eg.empty_colmajor(n, n, device=dev)
+    B = eg.empty_colmajor(n, nrhs, device=dev)
+    p = torch.zeros(n, dtype=torch.int32, device=dev)
+    info = {}
+
+    # plain FP64 step (the drop-in path): restore A, B, factor, solve
+    def plain_step():
+        A.copy_(A0)
+        B.copy_(B0)
+        if kind == "lu":
+            h.lu(A, p)
+            h.lu_solve_after(A, p, B, eg.NORMAL)
+        else:
+            h.hpd_solve(A, B, eg.LOWER)
+
+    def mixed_step():
+        X, it, be = h.hpd_solve_mixed(A0, B0, eg.LOWER, 30, 1e-14)
+        info["X"], info["iters"], info["berr"] = X, it, be
+
+    step = mixed_step if kind == "mixed" else plain_step
+    ms, trace, launches, clocks = timed(args, ws, dev, stream, h, step)
     ms_per_step = ms / args.steps
     value = ws * args.steps / (ms / 1e3)
+    with torch.cuda.stream(stream):
+        Xd = info["X"] if kind == "mixed" else B
+        bwd = backward_error(A0, Xd, B0)
+    plain = None
+    if kind == "mixed":
+        # the plain FP64 path on the same inputs, same timing rules
+        pms, ptrace, plaunches, _ = timed(args, ws, dev, stream, h, plain_step)
+        with torch.cuda.stream(stream):
+            pbwd = backward_error(A0, B, B0)
+        plain = {"value": ws * args.steps / (pms / 1e3), "unit": "solves/s", "ms_per_step": pms / args.steps,
+                 "backward_error": pbwd, "api": "egpu_dposv (Cholesky + HPD solve, FP64)",
+                 "roofline": roofline_of(ptrace, "update", measured_peaks()),
+                 "kernels": {k: {"ms": v["ms"], "launches": v["launches"]} for k, v in ptrace.items() if v["launches"]}}
 
-    # ---- end to end through the host-memory C ABI (GaussianElimination)
-    Ah = torch.empty((N * N,), dtype=torch.float64, pin_memory=True).numpy().reshape((N, N), order="F")
-    Bh = torch.empty((N * NRHS,), dtype=torch.float64, pin_memory=True).numpy().reshape((N, NRHS), order="F")
-    e2e_ms = []
-    hs = torch.cuda.ExternalStream(eg.lib().egpu_get_stream(h.h) or 0, device=dev)
+    # ---- end to end through the host-memory C ABI, pinned host buffers
+    Ah, Bh = pinned_like(A_host), pinned_like(B_host)
+    Xh = pinned_like(np.zeros((n, nrhs), order="F"))
     h.set_stream(None)
     hs = torch.cuda.ExternalStream(eg.lib().egpu_get_stream(h.h), device=dev)
+    e2e_ms = []
     for i in range(args.warmup + args.steps):
-        np.copyto(Ah, A_host)
-        np.copyto(Bh, B_host)
+        if kind != "mixed":
+            np.copyto(Ah, A_host)
+            np.copyto(Bh, B_host)
         barrier(ws)
         f0 = torch.cuda.Event(enable_timing=True)
         f1 = torch.cuda.Event(enable_timing=True)
         f0.record(hs)
-        h.host_gaussian_elimination(Ah, Bh)
+        if kind == "mixed":
+            h.host_hpd_solve_mixed(Ah, Bh, Xh)
+        elif kind == "lu":
+            h.host_gaussian_elimination(Ah, Bh)
+        else:
+            h.host_hpd_solve(Ah, Bh)
         f1.record(hs)
         f1.synchronize()
         if i >= args.warmup:
             e2e_ms.append(max_over_ranks(ws, f0.elapsed_time(f1), dev))
     e2e_value = ws * len(e2e_ms) / (sum(e2e_ms) / 1e3)
-    xerr = float(np.max(np.abs(Bh - np.asarray(B.cpu().numpy()))) / max(1e-300, np.max(np.abs(Bh))))
+    Xe = Xh if kind == "mixed" else Bh
+    xref = (info["X"] if kind == "mixed" else B).cpu().numpy()
+    xerr = float(np.max(np.abs(Xe - xref)) / max(1e-300, np.max(np.abs(xref))))
+    in_bytes = 8 * (n * n + n * nrhs)
+    out_bytes = 8 * n * nrhs + (0 if kind == "mixed" else 8 * n * n)
 
     if rank != 0:
         return
-    # ---- roofline of the dominant kernel (trailing-update DMMA GEMM)
-    try:
-        live_peak = h.measure_fp64_peak()
-    except Exception:
-        live_peak = None
-    upd = trace["update"]
-    achieved = upd["flops"] / (upd["ms"] / 1e3) / 1e12 if upd["ms"] > 0 else None
-    traffic = None
-    try:
-        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
-            traffic = json.load(f).get("dgemm_update_bytes_per_launch")
-    except Exception:
-        pass
-    total_ms = sum(v["ms"] for v in trace.values())
-    # ---- CPU baseline (oracle on the host cores, same seeded input)
+    peaks = measured_peaks()
+    roof = roofline_of(trace, "tc" if kind == "mixed" else "update", peaks)
     cpu = None
     if ws == 1 and not args.no_cpu:
         threads = os.cpu_count() or 1
-        t = cpu_oracle_solve(N, NRHS, seed, threads)
-        cpu = {"value": 1.0 / t, "unit": "solves/s", "cores": threads, "kind": "port",
-               "sample": f"one LU+solve at n={N} (the full workload), oracle in C with OpenMP"}
-    clocks = clk.summary()
+        t_full, sample = cpu_sample(kind, n, nrhs, seed, threads, 30.0, 1)
+        cpu = {"value": 1.0 / t_full, "unit": "solves/s", "cores": threads, "kind": "port",
+               "sample": sample + ", oracle in C with OpenMP"}
+    f_useful = flops_of(kind, n, nrhs)
     line = {
-        "metric": "FP64-accurate solves/sec (LU-PP factor + 64-RHS solve, n=8192)",
-        "value": value, "unit": "solves/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f64", "data": "synthetic (seeded U[-1,1] A, N(0,1) B)",
-        "config": {"workload": "LU partial pivoting + solve, n=8192, nb=128, 64 RHS (plain FP64)", "n": N,
-                   "nrhs": NRHS, "nb": NB, "parallelism": f"{ws} independent systems" if ws > 1 else "1 GPU",
-                   "l2": "inputs (512 MiB) larger than L2", "step_includes": "device restore copy of A and B"},
-        "tflops": flops_lu_solve(N, NRHS) / (ms_per_step / 1e3) / 1e12,
+        "metric": W["metric"], "value": value, "unit": "solves/s", "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64" if kind != "mixed" else "f64 (tf32x3 trailing updates)",
+        "data": "synthetic (seeded)",
+        "config": {"workload": W["desc"], "n": n, "nrhs": nrhs, "nb": NB,
+                   "parallelism": f"{ws} independent systems" if ws > 1 else "1 GPU",
+                   "l2": f"inputs ({8 * n * n >> 20} MiB) larger than L2",
+                   "step_includes": "device restore copy of A and B" if kind != "mixed"
+                   else "FP32/FP64 working copies of A made inside egpu_dposv_mixed"},
+        "equiv_fp64_tflops": f_useful / (ms_per_step / 1e3) / 1e12,
         "backward_error": bwd,
-        "e2e": {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": 8 * (N * N + N * NRHS),
-                "d2h_bytes_per_step": 8 * (N * N + N * NRHS), "api": "egpu_host_dgesv (GaussianElimination)",
+        "e2e": {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": in_bytes,
+                "d2h_bytes_per_step": out_bytes,
+                "api": {"mixed": "egpu_host_dposv_mixed", "lu": "egpu_host_dgesv (GaussianElimination)",
+                        "chol": "egpu_host_dposv (HPDSolve)"}[kind],
                 "x_rel_diff_vs_device_path": xerr},
-        "roofline": {"bound": "tensor", "kernel": "dgemm_tma_kernel (trailing update)",
-                     "achieved": achieved, "peak": FP64_PEAK_TFLOPS, "unit": "TFLOP/s",
-                     "frac": (achieved / FP64_PEAK_TFLOPS) if achieved else None,
-                     "peak_source": "measured FP64 DMMA peak (profiles/fp64_peak.md); MEASURED_PEAKS.json has no FP64 entry",
-                     "peak_live_tflops": live_peak,
-                     "traffic": traffic, "launches": upd["launches"],
-                     "share_of_traced_time": upd["ms"] / total_ms if total_ms else None},
+        "roofline": roof,
         "kernels": {k: {"ms": v["ms"], "launches": v["launches"]} for k, v in trace.items() if v["launches"]},
         "gpu_launches": launches,
         "clocks": clocks,
         "cpu_baseline": cpu,
+    }
+    if kind == "mixed":
+        line["refinement"] = {"corrections": info["iters"], "berr": info["berr"], "tol": 1e-14}
+        line["plain_fp64"] = plain
+        line["speedup_vs_plain_fp64"] = value / plain["value"]
+    print(json.dumps(line), flush=True)
+
+
+def batched_sets(seed, W):
+    r = np.random.default_rng(seed)
+    cnt = W["count"]
+    sizes = [r.integers(W["nmin"], W["nmax"] + 1, cnt), r.integers(W["nmin"], W["nmax"] + 1, cnt)]
+    rhs = [r.integers(W["rmin"], W["rmax"] + 1, cnt), r.integers(W["rmin"], W["rmax"] + 1, cnt)]
+    return [[int(x) for x in s] for s in sizes], [[int(x) for x in s] for s in rhs]
+
+
+def arm_batched(args, ws, rank, local):
+    """C4: 4096 HPD + 4096 general systems of uneven order in one persistent
+    launch per kind, the step (refill + both launches, the two kinds on two
+    streams) captured once in a CUDA graph and replayed."""
+    import torch
+    import elemental_b200 as eg
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    W = WORKLOADS["batched"]
+    h = eg.Handle(local)
+    seed = SEED + 1000 * rank
+    sizes, rhs = batched_sets(seed, W)
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(seed)
+    # one arena per kind for A and B (column-major, ld = n rounded up to even)
+    arenas = []
+    for kind in (0, 1):
+        lds = [n + (n & 1) for n in sizes[kind]]
+        offA = np.cumsum([0] + [ld * n for ld, n in zip(lds, sizes[kind])])
+        offB = np.cumsum([0] + [ld * k for ld, k in zip(lds, rhs[kind])])
+        A = torch.empty(int(offA[-1]), dtype=torch.float64, device=dev)
+        B = torch.empty(int(offB[-1]), dtype=torch.float64, device=dev)
+        views_A, views_B = [], []
+        for i, n in enumerate(sizes[kind]):
+            va = torch.as_strided(A, (n, n), (1, lds[i]), int(offA[i]))
+            vb = torch.as_strided(B, (n, rhs[kind][i]), (1, lds[i]), int(offB[i]))
+            if kind == 0:
+                g = torch.randn(n, n, dtype=torch.float64, device=dev, generator=gen)
+                va.copy_(g @ g.T + n * torch.eye(n, dtype=torch.float64, device=dev))
+            else:
+                va.copy_(torch.rand(n, n, dtype=torch.float64, device=dev, generator=gen) * 2 - 1)
+            vb.copy_(torch.randn(n, rhs[kind][i], dtype=torch.float64, device=dev, generator=gen))
+            views_A.append(va)
+            views_B.append(vb)
+        arenas.append({"A": A, "B": B, "A0": A.clone(), "B0": B.clone(), "vA": views_A, "vB": views_B,
+                       "lds": lds, "offA": offA, "offB": offB})
+    torch.cuda.synchronize()
+    plans = [eg.BatchPlan(h, k, arenas[k]["vA"], arenas[k]["vB"]) for k in (0, 1)]
+    s0, s1 = torch.cuda.Stream(device=dev), torch.cuda.Stream(device=dev)
+    tuned = []
+    with torch.cuda.stream(s0):
+        for k in (0, 1):
+            tuned.append(plans[k].autotune(reps=1, stream=s0))
+    torch.cuda.synchronize()
+
+    def refill_and_run():
+        cur = torch.cuda.current_stream()
+        s1.wait_stream(cur)
+        for k, s in ((0, cur), (1, s1)):
+            with torch.cuda.stream(s):
+                arenas[k]["A"].copy_(arenas[k]["A0"])
+                arenas[k]["B"].copy_(arenas[k]["B0"])
+                plans[k].run(s)
+        cur.wait_stream(s1)
+
+    graph = torch.cuda.CUDAGraph()
+    s0.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(s0):
+        refill_and_run()  # untimed warm run outside capture
+    torch.cuda.synchronize()
+    with torch.cuda.graph(graph, stream=s0):
+        refill_and_run()
+    torch.cuda.synchronize()
+
+    def step():
+        graph.replay()
+
+    ms, trace, launches, clocks = timed(args, ws, dev, s0, h, step)
+    total = 2 * W["count"]
+    value = ws * total * args.steps / (ms / 1e3)
+    # one traced (uncaptured) run for the kernel's own time
+    with torch.cuda.stream(s0):
+        for k in (0, 1):
+            arenas[k]["A"].copy_(arenas[k]["A0"])
+            arenas[k]["B"].copy_(arenas[k]["B0"])
+        h.trace_enable(True)
+        for k in (0, 1):
+            plans[k].run(s0)
+        torch.cuda.synchronize()
+        ktrace = h.trace_summary()
+        h.trace_enable(False)
+    infos = [plans[k].info(s0) for k in (0, 1)]
+    assert all(v == 0 for inf in infos for v in inf)
+    # accuracy on a sample of systems (backward error, FP64)
+    r = np.random.default_rng(seed + 5)
+    berr = 0.0
+    for k in (0, 1):
+        for i in r.choice(W["count"], 32, replace=False):
+            a0 = torch.as_strided(arenas[k]["A0"], arenas[k]["vA"][i].shape, arenas[k]["vA"][i].stride(),
+                                  arenas[k]["vA"][i].storage_offset())
+            b0 = torch.as_strided(arenas[k]["B0"], arenas[k]["vB"][i].shape, arenas[k]["vB"][i].stride(),
+                                  arenas[k]["vB"][i].storage_offset())
+            berr = max(berr, backward_error(a0, arenas[k]["vB"][i], b0))
+    # plain FP64 path (one egpu_dposv / egpu_dgesv call per system) on a sample
+    samp = 128
+    t_plain = 0.0
+    with torch.cuda.stream(s0):
+        for k in (0, 1):
+            idx = r.choice(W["count"], samp, replace=False)
+            work = [(torch.as_strided(arenas[k]["A0"], arenas[k]["vA"][i].shape, arenas[k]["vA"][i].stride(),
+                                      arenas[k]["vA"][i].storage_offset()).clone(),
+                     arenas[k]["vB"][i].clone()) for i in idx]
+            work = [(a.t().contiguous().t(), b.t().contiguous().t()) for a, b in work]
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(s0)
+            for A_, B_ in work:
+                if k == 0:
+                    h.hpd_solve(A_, B_, eg.LOWER)
+                else:
+                    h.gaussian_elimination(A_, B_)
+            e1.record(s0)
+            torch.cuda.synchronize()
+            t_plain += e0.elapsed_time(e1) / samp * W["count"]
+    plain_value = total / (t_plain / 1e3)
+    # e2e: pinned host arenas in, both plans, solutions out, every step
+    hostA = [arenas[k]["A0"].cpu().pin_memory() for k in (0, 1)]
+    hostB = [arenas[k]["B0"].cpu().pin_memory() for k in (0, 1)]
+    outB = [torch.empty_like(hostB[k]).pin_memory() for k in (0, 1)]
+    e2e_ms = []
+    with torch.cuda.stream(s0):
+        for i in range(args.warmup + args.steps):
+            barrier(ws)
+            f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            f0.record(s0)
+            for k in (0, 1):
+                arenas[k]["A"].copy_(hostA[k], non_blocking=True)
+                arenas[k]["B"].copy_(hostB[k], non_blocking=True)
+                plans[k].run(s0)
+                outB[k].copy_(arenas[k]["B"], non_blocking=True)
+            f1.record(s0)
+            f1.synchronize()
+            if i >= args.warmup:
+                e2e_ms.append(max_over_ranks(ws, f0.elapsed_time(f1), dev))
+    e2e_value = ws * total * len(e2e_ms) / (sum(e2e_ms) / 1e3)
+    h2d = sum(int(hostA[k].numel() + hostB[k].numel()) * 8 for k in (0, 1))
+    d2h = sum(int(outB[k].numel()) * 8 for k in (0, 1))
+    for p_ in plans:
+        p_.close()
+    if rank != 0:
+        return
+    flops = sum(n ** 3 / 3.0 for n in sizes[0]) + sum(2.0 * n ** 3 / 3.0 for n in sizes[1])
+    t = ktrace.get("other", {})
+    achieved = t["flops"] / (t["ms"] / 1e3) / 1e12 if t.get("ms") else None
+    cpu = None
+    if ws == 1 and not args.no_cpu:
+        from oracle import pyoracle as orc
+        threads = os.cpu_count() or 1
+        orc.set_threads(threads)
+        idx = r.choice(W["count"], 24, replace=False)
+        mats = []
+        for i in idx:
+            for k in (0, 1):
+                n = sizes[k][i]
+                a = arenas[k]["A0"][int(arenas[k]["offA"][i]):int(arenas[k]["offA"][i]) + arenas[k]["lds"][i] * n]
+                b = arenas[k]["B0"][int(arenas[k]["offB"][i]):int(arenas[k]["offB"][i]) + arenas[k]["lds"][i] * rhs[k][i]]
+                Ah_ = np.asfortranarray(a.cpu().numpy().reshape((arenas[k]["lds"][i], n), order="F")[:n])
+                Bh_ = np.asfortranarray(b.cpu().numpy().reshape((arenas[k]["lds"][i], rhs[k][i]), order="F")[:n])
+                mats.append((k, Ah_, Bh_))
+        t0 = time.perf_counter()
+        for k, Ah_, Bh_ in mats:
+            if k == 0:
+                orc.hpd_solve(Ah_, Bh_, orc.LOWER, nb=32)
+            else:
+                orc.gaussian_elimination(Ah_, Bh_, nb=32)
+        dt = time.perf_counter() - t0
+        cpu = {"value": len(mats) / dt, "unit": "solves/s", "cores": threads, "kind": "port",
+               "sample": "24 HPD + 24 GE systems drawn from the batch, oracle in C with OpenMP"}
+    line = {
+        "metric": W["metric"], "value": value, "unit": "solves/s", "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded, generated on the device)",
+        "config": {"workload": W["desc"], "count_per_kind": W["count"], "n_range": [W["nmin"], W["nmax"]],
+                   "rhs_range": [W["rmin"], W["rmax"]], "parallelism": "1 GPU" if ws == 1 else f"{ws} GPUs, own batch each",
+                   "l2": f"arenas ({sum(int(a['A'].numel()) for a in arenas) * 8 >> 20} MiB) larger than L2",
+                   "step_includes": "device refill of every matrix and right-hand side, both batched launches"},
+        "equiv_fp64_tflops": flops / (ms / args.steps / 1e3) / 1e12,
+        "backward_error": berr,
+        "autotuned_grid": {"hpd": tuned[0][1], "ge": tuned[1][1]},
+        "plain_fp64": {"value": plain_value, "unit": "solves/s",
+                       "api": "egpu_dposv / egpu_dgesv, one call per system (sampled, 128 per kind)"},
+        "speedup_vs_plain_fp64": value / plain_value,
+        "e2e": {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "api": "egpu_batch_plan_run with pinned host arenas copied in and solutions copied out"},
+        "roofline": {"bound": "tensor", "kernel": "chol_batched_kernel + lu_batched_kernel (FP64 DMMA)",
+                     "achieved": achieved, "peak": FP64_PEAK_TFLOPS, "unit": "TFLOP/s",
+                     "frac": achieved / FP64_PEAK_TFLOPS if achieved else None,
+                     "peak_source": "measured FP64 DMMA peak (profiles/fp64_peak.md)", "traffic": None},
+        "kernels": {k: {"ms": v["ms"], "launches": v["launches"]} for k, v in ktrace.items() if v["launches"]},
+        "gpu_launches": launches + 2 * args.steps,
+        "gpu_launches_note": "2 persistent batched kernels per step, replayed from the CUDA graph",
+        "clocks": clocks,
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def serve_stream(seed, W, device):
+    """The request stream: a pool of matrices (log-uniform n and kappa) in
+    pinned host memory and a seeded Poisson arrival sequence over the pool."""
+    import torch
+    from elemental_b200 import inputs
+    r = np.random.default_rng(seed)
+    pool = []
+    for i in range(W["pool"]):
+        n = int(np.exp(r.uniform(np.log(W["nmin"]), np.log(W["nmax"]))))
+        kappa = float(np.exp(r.uniform(np.log(W["kmin"]), np.log(W["kmax"]))))
+        A = inputs.spd_spectrum_torch(n, kappa, seed + i, device)
+        Ah = torch.empty((n * n,), dtype=torch.float64, pin_memory=True)
+        Ah.copy_(A.t().reshape(-1))  # symmetric: column-major values
+        Bh = torch.empty((n * W["rmax"],), dtype=torch.float64, pin_memory=True)
+        Bh.copy_(torch.from_numpy(inputs.normal(n, W["rmax"], seed + 500 + i).ravel(order="F")))
+        pool.append((n, kappa, Ah.numpy().reshape((n, n), order="F"), Bh.numpy().reshape((n, W["rmax"]), order="F")))
+        del A
+    torch.cuda.empty_cache()
+    t, reqs = 0.0, []
+    while True:
+        t += r.exponential(1.0 / W["rate"])
+        if t > W["window_s"]:
+            break
+        reqs.append((t, int(r.integers(0, W["pool"])), int(r.integers(W["rmin"], W["rmax"] + 1)), int(r.integers(0, 2))))
+    return pool, reqs
+
+
+def run_stream(eg, W, pool, reqs, mode, device_index):
+    """Replay the arrival sequence against a server; returns per-request records."""
+    srv = eg.Server(device_index, hbm_budget_bytes=W["budget"], slots=W["slots"], mode=mode, tol=1e-14)
+    ids, outs = [], []
+    t0 = time.perf_counter()
+    for (ta, pi, k, kind) in reqs:
+        now = time.perf_counter() - t0
+        if ta > now:
+            time.sleep(ta - now)
+        n, _, Ah, Bh = pool[pi]
+        X = np.zeros((n, k), order="F")
+        ids.append(srv.submit(kind, Ah, Bh[:, :k], X))
+        outs.append(X)
+    srv.drain()
+    t_end = time.perf_counter() - t0
+    recs = [srv.query(i) for i in ids]
+    srv.close()
+    return recs, outs, t_end
+
+
+def arm_serve(args, ws, rank, local):
+    """C5: the served stream through the request server, mixed mode (value)
+    and FP64 mode (plain_fp64) on the same arrivals."""
+    import torch
+    import elemental_b200 as eg
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    W = WORKLOADS["serve"]
+    seed = SEED + 1000 * rank
+    pool, reqs = serve_stream(seed, W, dev)
+    # warm-up: a few requests per mode (kernels loaded, workspaces sized)
+    for mode in (1, 0):
+        run_stream(eg, W, pool, [(0.0, i % len(pool), 4, i % 2) for i in range(max(args.warmup, 3))], mode, local)
+    res = {}
+    clocks = None
+    for mode in (1, 0):
+        barrier(ws)
+        with ClockSampler(local) as clk:
+            recs, outs, t_end = run_stream(eg, W, pool, reqs, mode, local)
+        if mode == 1:
+            clocks = clk.summary()
+        ok = [i for i, r_ in enumerate(recs) if r_ and r_["status"] == 0]
+        lat = np.array([recs[i]["latency_ms"] for i in ok])
+        # backward error on a sample (host FP64)
+        rs = np.random.default_rng(seed + 9)
+        berr = 0.0
+        for i in rs.choice(ok, min(24, len(ok)), replace=False):
+            _, pi, k, _ = reqs[i]
+            n, _, Ah, Bh = pool[pi]
+            R = Bh[:, :k] - Ah @ outs[i]
+            den = np.abs(Ah).sum(axis=1).max() * np.abs(outs[i]).max(axis=0) + np.abs(Bh[:, :k]).max(axis=0)
+            berr = max(berr, float((np.abs(R).max(axis=0) / den).max()))
+        paths = [recs[i]["path"] for i in ok]
+        res[mode] = {"value": len(ok) / t_end, "completed": len(ok), "submitted": len(reqs), "makespan_s": t_end,
+                     "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+                     "backward_error_sampled": berr,
+                     "paths": {"fp64": paths.count(0), "mixed": paths.count(1), "batched": paths.count(2),
+                               "mixed_fell_back": paths.count(3)}}
+    if rank != 0:
+        return
+    m, p = res[1], res[0]
+    line = {
+        "metric": W["metric"], "value": m["value"], "unit": "solves/s", "n_gpus": ws, "steps": 1,
+        "warmup": args.warmup, "ms_per_step": m["makespan_s"] * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64 (mixed tf32x3 + IR for HPD requests)",
+        "data": "synthetic (seeded pool of 48 matrices, seeded Poisson arrivals)",
+        "config": {"workload": W["desc"], "requests": len(reqs), "parallelism": "1 GPU",
+                   "l2": "pool matrices up to 512 MiB, larger than L2",
+                   "step_includes": "the whole stream: host->device copies, solves, device->host copies"},
+        "latency_ms": {"p50": m["p50_ms"], "p99": m["p99_ms"]},
+        "served": m,
+        "plain_fp64": p,
+        "speedup_vs_plain_fp64": m["value"] / p["value"],
+        "e2e": {"value": m["value"], "unit": "solves/s",
+                "h2d_bytes_per_step": int(sum(8 * pool[pi][0] * (pool[pi][0] + k) for _, pi, k, _ in reqs)),
+                "d2h_bytes_per_step": int(sum(8 * pool[pi][0] * k for _, pi, k, _ in reqs)),
+                "api": "egpu_server_submit / egpu_server_query with pinned host buffers"},
+        "roofline": None,
+        "gpu_launches": None,
+        "clocks": clocks,
+        "cpu_baseline": None,
     }
     print(json.dumps(line), flush=True)
 
@@ -390,6 +894,7 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="mixed", choices=sorted(WORKLOADS), help="benchmark configuration")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline leg")
     ap.add_argument("--case", choices=["update", "gemm", "panel", "diag", "peaks"], default=None,
                     help="run one launch of one kernel class (profiling)")
@@ -402,6 +907,10 @@ def main():
     try:
         if args.impl == "reference":
             reference_arm(args, ws, rank)
+        elif args.workload == "batched":
+            arm_batched(args, ws, rank, local)
+        elif args.workload == "serve":
+            arm_serve(args, ws, rank, local)
         else:
             our_arm(args, ws, rank, local)
     finally:

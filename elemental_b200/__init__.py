@@ -116,6 +116,19 @@ def _declare(L):
         "egpu_dposv_mixed": ([H, I, I, I, P, I, P, I, P, I, I, D, P, P], I),
         "egpu_tc_gemm_split": ([H, I, I, I, D, P, I, P, I, D, P, I, I, I], I),
         "egpu_host_dposv_mixed": ([H, I, I, I, P, I, P, I, P, I, I, D, P, P], I),
+        "egpu_batch_plan_create": ([H, I, I, P, P, P, P, P, P, P], I),
+        "egpu_batch_plan_run": ([P, P], I),
+        "egpu_batch_plan_info": ([P, P, P], I),
+        "egpu_batch_plan_autotune": ([P, P, I, P, P], I),
+        "egpu_batch_plan_set_grid": ([P, I], I),
+        "egpu_batch_plan_destroy": ([P], I),
+        "egpu_server_create": ([I, ctypes.c_size_t, I, I, P], I),
+        "egpu_server_set_tolerance": ([P, D], I),
+        "egpu_server_submit": ([P, I, I, I, P, I, P, I, P, I, P], I),
+        "egpu_server_query": ([P, ctypes.c_ulonglong, I, P, P, P, P, P, P], I),
+        "egpu_server_release": ([P, ctypes.c_ulonglong], I),
+        "egpu_server_drain": ([P], I),
+        "egpu_server_destroy": ([P], I),
         "egpu_dgesv_batched": ([H, I, P, P, P, P, P, P, P], I),
         "egpu_host_dpotrf": ([H, I, I, P, I, P], I),
         "egpu_host_dpotrs": ([H, I, I, I, I, P, I, P, I], I),
@@ -200,6 +213,116 @@ def _np_f(a: np.ndarray):
 
 def _np_ptr(a):
     return a.ctypes.data_as(ctypes.c_void_p)
+
+
+class Server:
+    """Continuous-batching request server (egpu_server_*).  Requests reference
+    host arrays (column-major float64, best pinned) that must stay alive until
+    the request completes."""
+
+    HPD, GE = 0, 1
+
+    def __init__(self, device=0, hbm_budget_bytes=150 << 30, slots=4, mode=0, tol=1e-14):
+        self._s = ctypes.c_void_p()
+        _check(lib().egpu_server_create(device, hbm_budget_bytes, slots, mode, ctypes.byref(self._s)))
+        _check(lib().egpu_server_set_tolerance(self._s, tol))
+        self._keep = {}
+
+    def submit(self, kind, A, B, X):
+        A, B, X = _np_f(A), _np_f(B), _np_f(X)
+        rid = ctypes.c_ulonglong(0)
+        _check(lib().egpu_server_submit(self._s, kind, A.shape[0], B.shape[1], _np_ptr(A), max(A.shape[0], 1),
+                                        _np_ptr(B), max(B.shape[0], 1), _np_ptr(X), max(X.shape[0], 1),
+                                        ctypes.byref(rid)))
+        self._keep[rid.value] = (A, B, X)
+        return rid.value
+
+    def query(self, rid, wait=False):
+        """None while pending, else a dict with status, latency_ms, path, iters, berr."""
+        d, st, it, path = ctypes.c_int(0), ctypes.c_int(0), ctypes.c_int(0), ctypes.c_int(0)
+        lat, be = ctypes.c_double(0.0), ctypes.c_double(0.0)
+        _check(lib().egpu_server_query(self._s, rid, 1 if wait else 0, ctypes.byref(d), ctypes.byref(st),
+                                       ctypes.byref(lat), ctypes.byref(path), ctypes.byref(it), ctypes.byref(be)))
+        if not d.value:
+            return None
+        return {"status": st.value, "latency_ms": lat.value, "path": path.value, "iters": it.value,
+                "berr": be.value}
+
+    def release(self, rid):
+        _check(lib().egpu_server_release(self._s, rid))
+        self._keep.pop(rid, None)
+
+    def drain(self):
+        _check(lib().egpu_server_drain(self._s))
+
+    def close(self):
+        if self._s:
+            lib().egpu_server_destroy(self._s)
+            self._s = ctypes.c_void_p()
+            self._keep.clear()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class BatchPlan:
+    """A device-resident batched solve (egpu_batch_plan_*): kind 0 = HPD solves,
+    kind 1 = GaussianElimination.  The matrices stay where they are; run()
+    only enqueues work (capturable in a CUDA graph)."""
+
+    def __init__(self, handle, kind, As, Bs=None):
+        self.handle = handle
+        cnt = len(As)
+        n = (ctypes.c_int * cnt)(*[a.shape[0] for a in As])
+        nr = (ctypes.c_int * cnt)(*[(b.shape[1] if b.dim() > 1 else 1) if Bs is not None else 0
+                                    for b in (Bs if Bs is not None else As)])
+        lda = (ctypes.c_int * cnt)(*[_ld(a) for a in As])
+        ptrA = (ctypes.c_void_p * cnt)(*[a.data_ptr() for a in As])
+        if Bs is not None:
+            ldb = (ctypes.c_int * cnt)(*[_ld(b) for b in Bs])
+            ptrB = (ctypes.c_void_p * cnt)(*[b.data_ptr() for b in Bs])
+        else:
+            ldb, ptrB = None, None
+        self.count = cnt
+        self._p = ctypes.c_void_p()
+        _check(lib().egpu_batch_plan_create(handle._h, kind, cnt, n, nr, ptrA, lda, ptrB, ldb, ctypes.byref(self._p)))
+
+    @staticmethod
+    def _stream(stream):
+        import torch
+        s = stream if stream is not None else torch.cuda.current_stream()
+        return ctypes.c_void_p(s.cuda_stream or 1)  # 0 (legacy default stream) is passed as its handle 1
+
+    def run(self, stream=None):
+        _check(lib().egpu_batch_plan_run(self._p, self._stream(stream)))
+
+    def info(self, stream=None):
+        out = (ctypes.c_int * max(self.count, 1))()
+        _check(lib().egpu_batch_plan_info(self._p, self._stream(stream), out))
+        return list(out)[: self.count]
+
+    def autotune(self, reps=2, stream=None):
+        ms = ctypes.c_double(0.0)
+        g = ctypes.c_int(0)
+        _check(lib().egpu_batch_plan_autotune(self._p, self._stream(stream), reps, ctypes.byref(ms), ctypes.byref(g)))
+        return ms.value, g.value
+
+    def set_grid(self, grid):
+        _check(lib().egpu_batch_plan_set_grid(self._p, grid))
+
+    def close(self):
+        if self._p:
+            lib().egpu_batch_plan_destroy(self._p)
+            self._p = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class Handle:
@@ -481,6 +604,20 @@ class Handle:
         pp = None if p is None else np.ascontiguousarray(p, dtype=np.int32)
         _check(lib().egpu_host_dgetrs(self._h, orient, A.shape[0], B.shape[1], _np_ptr(A), max(A.shape[0], 1),
                                       None if pp is None else _np_ptr(pp), _np_ptr(B), max(B.shape[0], 1)))
+
+    def host_hpd_solve_mixed(self, A, B, X, uplo=LOWER, max_iter=30, tol=1e-14):
+        """Mixed-precision HPD solve on host arrays: X := A^-1 B (A, B unchanged);
+        returns (corrections, backward error)."""
+        A, B, X = _np_f(A), _np_f(B), _np_f(X)
+        it = ctypes.c_int(0)
+        be = ctypes.c_double(0.0)
+        rc = lib().egpu_host_dposv_mixed(self._h, uplo, A.shape[0], B.shape[1], _np_ptr(A), max(A.shape[0], 1),
+                                         _np_ptr(B), max(B.shape[0], 1), _np_ptr(X), max(X.shape[0], 1), max_iter,
+                                         tol, ctypes.byref(it), ctypes.byref(be))
+        if rc == NO_CONVERGENCE:
+            raise ElemGPUError(f"refinement did not reach {tol:g} in {it.value} corrections (berr {be.value:.3e})")
+        _check(rc)
+        return it.value, be.value
 
     def host_gaussian_elimination(self, A, B):
         A, B = _np_f(A), _np_f(B)

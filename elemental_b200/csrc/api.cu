@@ -375,9 +375,9 @@ int trsm_core(egpu_context* h, int side, int uplo, int trans, int unit, int m, i
 }
 
 // Can the one-launch skinny sweep (trsm_skinny.cu) take this right-hand side?
-static bool skinny_ok(egpu_context* h, int nrhs, const double* B, long long ldb) {
-  return nrhs >= 1 && nrhs <= 64 && h->nb <= 128 && h->nb % 2 == 0 && ldb % 2 == 0 &&
-         reinterpret_cast<uintptr_t>(B) % 16 == 0;
+static bool skinny_ok(egpu_context* h, int nrhs, const double* A, long long lda, const double* B, long long ldb) {
+  return nrhs >= 1 && nrhs <= 64 && h->nb <= 128 && h->nb % 2 == 0 && ldb % 2 == 0 && lda % 2 == 0 &&
+         reinterpret_cast<uintptr_t>(B) % 16 == 0 && reinterpret_cast<uintptr_t>(A) % 16 == 0;
 }
 
 // X := inv(T2) inv(T1) X with two skinny sweeps.  Each T is (uplo, unit) for
@@ -415,7 +415,7 @@ int getrs_core(egpu_context* h, int orient, int n, int nrhs, const double* A, lo
   TRY(ensure_ws(h, align_up(winv + 4096, 256) + lsw + 4096));
   int* perm = reinterpret_cast<int*>(static_cast<unsigned char*>(h->ws) + align_up(winv + 4096, 256));
   const size_t trsm_off = 0;
-  const bool sk = skinny_ok(h, nrhs, B, ldb);
+  const bool sk = skinny_ok(h, nrhs, A, lda, B, ldb);
   if (sk) {  // reserve now: a later growth of the workspace would move perm
     TRY(ensure_ws(h, skinny_off + 2 * align_up(winv_bytes(n, h->nb), 256) + trsm_skinny_flag_bytes(n, h->nb) + 8192));
     perm = reinterpret_cast<int*>(static_cast<unsigned char*>(h->ws) + align_up(winv + 4096, 256));
@@ -443,7 +443,7 @@ int potrs_core(egpu_context* h, int uplo, int n, int nrhs, const double* A, long
                long long ldb) {
   // cholesky::SolveAfter (Cholesky/SolveAfter.hpp:20-75); TRANSPOSE only
   // conjugates B, a no-op for real data.
-  if (skinny_ok(h, nrhs, B, ldb)) {
+  if (skinny_ok(h, nrhs, A, lda, B, ldb)) {
     if (uplo == EGPU_LOWER) return skinny_pair(h, n, nrhs, A, lda, B, ldb, {EGPU_LOWER, 0, 0, 0}, {EGPU_LOWER, 0, 1, 1}, 0);
     return skinny_pair(h, n, nrhs, A, lda, B, ldb, {EGPU_UPPER, 0, 0, 1}, {EGPU_UPPER, 0, 1, 0}, 0);
   }
@@ -783,6 +783,64 @@ int egpu_dposv_batched(egpu_handle h, int count, const int* n, const int* nrhs, 
   TRY(ensure_ws(h, egpu_batched_ws_bytes(count, h->sm_count) + 4096));
   return egpu_batched_launch(0, h->stream, h->sm_count, count, n, nrhs, dA, lda, dB, ldb, h->ws, h->ws_bytes,
                              info);
+}
+
+// ---- batch plans (device-resident batched solves, capturable runs) ----
+struct egpu_batch_plan_s {
+  egpu_context* h;
+  egpu::BatchPlan* p;
+};
+
+int egpu_batch_plan_create(egpu_handle h, int kind, int count, const int* n, const int* nrhs, double* const* dA,
+                           const int* lda, double* const* dB, const int* ldb, egpu_batch_plan* out) {
+  TRY(check_handle(h));
+  if (!out || (kind != 0 && kind != 1) || count < 0 || (count > 0 && (!n || !nrhs || !dA || !lda))) return EGPU_ERR_ARG;
+  *out = nullptr;
+  Enter g(h);
+  egpu::BatchPlan* p = nullptr;
+  TRY(egpu::batch_plan_create(h->device, h->sm_count, kind, count, n, nrhs, dA, lda, dB, ldb, &p));
+  auto* w = new (std::nothrow) egpu_batch_plan_s{h, p};
+  if (!w) {
+    egpu::batch_plan_destroy(p);
+    return EGPU_ERR_ALLOC;
+  }
+  *out = w;
+  return EGPU_OK;
+}
+
+int egpu_batch_plan_run(egpu_batch_plan plan, void* stream) {
+  if (!plan) return EGPU_ERR_ARG;
+  Enter g(plan->h);
+  return egpu::batch_plan_run(plan->p, stream ? static_cast<cudaStream_t>(stream) : plan->h->stream);
+}
+
+int egpu_batch_plan_info(egpu_batch_plan plan, void* stream, int* info) {
+  if (!plan || !info) return EGPU_ERR_ARG;
+  Enter g(plan->h);
+  return egpu::batch_plan_info(plan->p, stream ? static_cast<cudaStream_t>(stream) : plan->h->stream, info);
+}
+
+int egpu_batch_plan_autotune(egpu_batch_plan plan, void* stream, int reps, double* best_ms, int* best_grid) {
+  if (!plan) return EGPU_ERR_ARG;
+  Enter g(plan->h);
+  return egpu::batch_plan_autotune(plan->p, stream ? static_cast<cudaStream_t>(stream) : plan->h->stream, reps,
+                                   best_ms, best_grid);
+}
+
+int egpu_batch_plan_set_grid(egpu_batch_plan plan, int grid) {
+  if (!plan || grid < 1) return EGPU_ERR_ARG;
+  egpu::batch_plan_set_grid(plan->p, grid);
+  return EGPU_OK;
+}
+
+int egpu_batch_plan_destroy(egpu_batch_plan plan) {
+  if (!plan) return EGPU_OK;
+  {
+    Enter g(plan->h);
+    egpu::batch_plan_destroy(plan->p);
+  }
+  delete plan;
+  return EGPU_OK;
 }
 
 int egpu_dgesv_batched(egpu_handle h, int count, const int* n, const int* nrhs, double* const* dA, const int* lda,

@@ -13,6 +13,7 @@
 // systems in flight).  The right-hand sides are solved with the same
 // diagonal-block inverses, kept per CTA in a global scratch area.
 #include <algorithm>
+#include <new>
 #include <vector>
 
 #include "internal.h"
@@ -241,15 +242,15 @@ __global__ void __launch_bounds__(kBT, 1) chol_batched_kernel(const BatchItem* i
     for (int ib = 0; ib < nblk; ++ib) {
       const int i0 = ib * kBnb, bi = min(kBnb, n - i0);
       const double* Xi = Xg + (size_t)ib * kBnb * kBnb;
-      if (tid < bi * nrhs) {
-        const int i = tid % bi, q = tid / bi;
+      for (int e = tid; e < bi * nrhs; e += kBT) {  // bi * nrhs can exceed the CTA (32 x 16)
+        const int i = e % bi, q = e / bi;
         double s = 0.0;
         for (int k = 0; k <= i; ++k) s = fma(Xi[i + k * kBnb], BS[q * kBmaxN + i0 + k], s);
         X[i + q * kXLD] = s;  // staging
       }
       __syncthreads();
-      if (tid < bi * nrhs) {
-        const int i = tid % bi, q = tid / bi;
+      for (int e = tid; e < bi * nrhs; e += kBT) {  // bi * nrhs can exceed the CTA (32 x 16)
+        const int i = e % bi, q = e / bi;
         BS[q * kBmaxN + i0 + i] = X[i + q * kXLD];
       }
       __syncthreads();
@@ -273,15 +274,15 @@ __global__ void __launch_bounds__(kBT, 1) chol_batched_kernel(const BatchItem* i
     for (int ib = nblk - 1; ib >= 0; --ib) {
       const int i0 = ib * kBnb, bi = min(kBnb, n - i0);
       const double* Xi = Xg + (size_t)ib * kBnb * kBnb;
-      if (tid < bi * nrhs) {
-        const int i = tid % bi, q = tid / bi;
+      for (int e = tid; e < bi * nrhs; e += kBT) {  // bi * nrhs can exceed the CTA (32 x 16)
+        const int i = e % bi, q = e / bi;
         double s = 0.0;
         for (int k = i; k < bi; ++k) s = fma(Xi[k + i * kBnb], BS[q * kBmaxN + i0 + k], s);
         X[i + q * kXLD] = s;
       }
       __syncthreads();
-      if (tid < bi * nrhs) {
-        const int i = tid % bi, q = tid / bi;
+      for (int e = tid; e < bi * nrhs; e += kBT) {  // bi * nrhs can exceed the CTA (32 x 16)
+        const int i = e % bi, q = e / bi;
         BS[q * kBmaxN + i0 + i] = X[i + q * kXLD];
       }
       __syncthreads();
@@ -559,15 +560,15 @@ __global__ void __launch_bounds__(kBT, 1) lu_batched_kernel(const BatchItem* ite
     for (int ib = nblk - 1; ib >= 0; --ib) {
       const int i0 = ib * kBnb, bi = min(kBnb, n - i0);
       const double* Xi = Xg + (size_t)ib * kBnb * kBnb;
-      if (tid < bi * nrhs) {
-        const int i = tid % bi, q = tid / bi;
+      for (int e = tid; e < bi * nrhs; e += kBT) {  // bi * nrhs can exceed the CTA (32 x 16)
+        const int i = e % bi, q = e / bi;
         double s = 0.0;
         for (int k = i; k < bi; ++k) s = fma(Xi[i + k * kBnb], BS[q * kBmaxN + i0 + k], s);
         X[i + q * kXLD] = s;
       }
       __syncthreads();
-      if (tid < bi * nrhs) {
-        const int i = tid % bi, q = tid / bi;
+      for (int e = tid; e < bi * nrhs; e += kBT) {  // bi * nrhs can exceed the CTA (32 x 16)
+        const int i = e % bi, q = e / bi;
         BS[q * kBmaxN + i0 + i] = X[i + q * kXLD];
       }
       __syncthreads();
@@ -648,6 +649,146 @@ int egpu_batched_launch(int kind, cudaStream_t st, int sm_count, int count, cons
 size_t egpu_batched_ws_bytes(int count, int sm_count) {
   return sizeof(BatchItem) * (size_t)count + sizeof(int) * (size_t)count + 4096 +
          sizeof(double) * (size_t)sm_count * kBmaxN * kBnb;
+}
+
+// ---------------------------------------------------------------------------
+// Batch plans: the size-sorted item list, the queue counter, per-system info
+// and the per-CTA inverse scratch live on the device for the plan's lifetime,
+// so a run is two stream operations (counter reset + the persistent kernel),
+// which a CUDA graph can capture and replay.  The grid (number of persistent
+// CTAs) is the tunable launch shape: egpu_batch_plan_autotune times the
+// candidates on the plan's own systems and keeps the fastest.
+struct BatchPlan {
+  int kind = 0, count = 0, grid = 0, sm_count = 0, device = 0;
+  BatchItem* d_items = nullptr;
+  int* d_counter = nullptr;
+  int* d_info = nullptr;
+  double* d_inv = nullptr;
+  void* block = nullptr;
+  double flops = 0.0;
+};
+
+int batch_plan_create(int device, int sm_count, int kind, int count, const int* n, const int* nrhs,
+                      double* const* A, const int* lda, double* const* B, const int* ldb, BatchPlan** out) {
+  *out = nullptr;
+  for (int i = 0; i < count; ++i)
+    if (n[i] < 0 || n[i] > kBmaxN || nrhs[i] < 0 || nrhs[i] > kBmaxRHS || lda[i] < std::max(1, n[i]) ||
+        (B && nrhs[i] > 0 && ldb[i] < std::max(1, n[i])))
+      return EGPU_ERR_UNSUPPORTED;
+  std::vector<BatchItem> items(count);
+  double flops = 0.0;
+  for (int i = 0; i < count; ++i) {
+    items[i].A = A[i];
+    items[i].B = B ? B[i] : nullptr;
+    items[i].n = n[i];
+    items[i].nrhs = B ? nrhs[i] : 0;
+    items[i].lda = lda[i];
+    items[i].ldb = B ? ldb[i] : 1;
+    items[i].id = i;
+    flops += (kind == 0 ? 1.0 / 3.0 : 2.0 / 3.0) * (double)n[i] * n[i] * n[i];
+  }
+  std::stable_sort(items.begin(), items.end(), [](const BatchItem& a, const BatchItem& b) { return a.n > b.n; });
+  BatchPlan* p = new (std::nothrow) BatchPlan;
+  if (!p) return EGPU_ERR_ALLOC;
+  p->kind = kind; p->count = count; p->grid = sm_count; p->sm_count = sm_count; p->device = device; p->flops = flops;
+  const size_t b_items = ((sizeof(BatchItem) * (size_t)std::max(count, 1)) + 255) & ~size_t(255);
+  const size_t b_info = ((sizeof(int) * (size_t)std::max(count, 1)) + 255) & ~size_t(255);
+  const size_t b_inv = sizeof(double) * (size_t)sm_count * kBmaxN * kBnb;
+  cudaError_t e = cudaMalloc(&p->block, b_items + 256 + b_info + b_inv);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    delete p;
+    return EGPU_ERR_ALLOC;
+  }
+  unsigned char* base = static_cast<unsigned char*>(p->block);
+  p->d_items = reinterpret_cast<BatchItem*>(base);
+  p->d_counter = reinterpret_cast<int*>(base + b_items);
+  p->d_info = reinterpret_cast<int*>(base + b_items + 256);
+  p->d_inv = reinterpret_cast<double*>(base + b_items + 256 + b_info);
+  if (count > 0) e = cudaMemcpy(p->d_items, items.data(), sizeof(BatchItem) * count, cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) {
+    set_last_error(e, "batch plan upload", __FILE__, __LINE__);
+    cudaFree(p->block);
+    delete p;
+    return EGPU_ERR_CUDA;
+  }
+  *out = p;
+  return EGPU_OK;
+}
+
+// Enqueue one run of the plan on `st` (no host synchronisation).
+int batch_plan_run(BatchPlan* p, cudaStream_t st) {
+  if (p->count == 0) return EGPU_OK;
+  const size_t smem = sizeof(double) * kBSmemDoubles;
+  auto kern = (p->kind == 0) ? chol_batched_kernel : lu_batched_kernel;
+  static bool attr[2] = {false, false};
+  if (!attr[p->kind]) {
+    EGPU_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    attr[p->kind] = true;
+  }
+  EGPU_CUDA_TRY(cudaMemsetAsync(p->d_counter, 0, sizeof(int), st));
+  {
+    TraceMark tm(st, kTraceOther, p->flops, 0.0);
+    kern<<<std::max(1, std::min(p->grid, p->sm_count)), kBT, smem, st>>>(p->d_items, p->count, p->d_counter,
+                                                                        p->d_info, p->d_inv);
+    count_launch();
+  }
+  EGPU_CUDA_TRY(cudaGetLastError());
+  return EGPU_OK;
+}
+
+int batch_plan_info(BatchPlan* p, cudaStream_t st, int* info_host) {
+  if (p->count == 0) return EGPU_OK;
+  EGPU_CUDA_TRY(cudaMemcpyAsync(info_host, p->d_info, sizeof(int) * p->count, cudaMemcpyDeviceToHost, st));
+  EGPU_CUDA_TRY(cudaStreamSynchronize(st));
+  return EGPU_OK;
+}
+
+// Time each candidate grid (`reps` runs each, after one untimed run) and keep
+// the fastest.  The runs factor the plan's systems in place.
+int batch_plan_autotune(BatchPlan* p, cudaStream_t st, int reps, double* best_ms, int* best_grid) {
+  const int cands[] = {p->sm_count, (3 * p->sm_count) / 4, p->sm_count / 2, p->sm_count / 4};
+  cudaEvent_t e0, e1;
+  EGPU_CUDA_TRY(cudaEventCreate(&e0));
+  EGPU_CUDA_TRY(cudaEventCreate(&e1));
+  double best = 1e300;
+  int bg = p->sm_count;
+  for (int g : cands) {
+    if (g < 1) continue;
+    p->grid = g;
+    int rc = batch_plan_run(p, st);
+    if (rc != EGPU_OK) { cudaEventDestroy(e0); cudaEventDestroy(e1); return rc; }
+    cudaEventRecord(e0, st);
+    for (int r = 0; r < std::max(1, reps); ++r) {
+      rc = batch_plan_run(p, st);
+      if (rc != EGPU_OK) { cudaEventDestroy(e0); cudaEventDestroy(e1); return rc; }
+    }
+    cudaEventRecord(e1, st);
+    cudaError_t e = cudaEventSynchronize(e1);
+    float ms = 0.f;
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+    if (e != cudaSuccess) {
+      set_last_error(e, "batch plan autotune", __FILE__, __LINE__);
+      cudaEventDestroy(e0); cudaEventDestroy(e1);
+      return EGPU_ERR_CUDA;
+    }
+    const double per = ms / std::max(1, reps);
+    if (per < best) { best = per; bg = g; }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  p->grid = bg;
+  if (best_ms) *best_ms = best;
+  if (best_grid) *best_grid = bg;
+  return EGPU_OK;
+}
+
+void batch_plan_set_grid(BatchPlan* p, int grid) { p->grid = std::max(1, std::min(grid, p->sm_count)); }
+
+void batch_plan_destroy(BatchPlan* p) {
+  if (!p) return;
+  if (p->block) cudaFree(p->block);
+  delete p;
 }
 
 }  // namespace egpu

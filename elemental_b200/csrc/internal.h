@@ -60,7 +60,12 @@ int launch_split_tf32(cudaStream_t st, int rows, int cols, const double* X, long
 size_t trsm_skinny_flag_bytes(int n, int nb);
 int launch_trsm_skinny(cudaStream_t st, int bwd, int amode, int n, int nrhs, const double* A, long long lda,
                        const double* Winv, int nb, double* X, long long ldx, int* flags, int epoch, int sm_count,
-                       DevStatus* status);
+                       DevStatus* status, double* Y = nullptr);
+
+// C += alpha A B for N <= 64 (split-K DMMA, FP64 atomics into C); A, B
+// 16-byte aligned with even leading dimensions, else EGPU_ERR_UNSUPPORTED.
+int launch_dgemm_skinny(cudaStream_t st, int M, int N, int K, double alpha, const double* A, long long lda,
+                        const double* B, long long ldb, double* C, long long ldc, int sm_count, DevStatus* status);
 
 // Diagonal-block Cholesky (factor in place + triangular inverse into W).
 int launch_potrf_diag(cudaStream_t st, int uplo, double* A, long long lda, int b, double* W, int ldw,
@@ -100,6 +105,14 @@ int launch_getrf_diag_nopiv(cudaStream_t st, double* A, long long lda, int b, do
 
 // Batched (one persistent launch) HPDSolve, lower, n <= 512, nrhs <= 16.
 size_t egpu_batched_ws_bytes(int count, int sm_count);
+struct BatchPlan;
+int batch_plan_create(int device, int sm_count, int kind, int count, const int* n, const int* nrhs,
+                      double* const* A, const int* lda, double* const* B, const int* ldb, BatchPlan** out);
+int batch_plan_run(BatchPlan* p, cudaStream_t st);
+int batch_plan_info(BatchPlan* p, cudaStream_t st, int* info_host);
+int batch_plan_autotune(BatchPlan* p, cudaStream_t st, int reps, double* best_ms, int* best_grid);
+void batch_plan_set_grid(BatchPlan* p, int grid);
+void batch_plan_destroy(BatchPlan* p);
 // kind 0: HPDSolve (lower Cholesky + solve); kind 1: GaussianElimination (LU + solve)
 int egpu_batched_launch(int kind, cudaStream_t st, int sm_count, int count, const int* n, const int* nrhs,
                         double* const* A, const int* lda, double* const* B, const int* ldb, void* ws,

@@ -135,7 +135,7 @@ int launch_split_tf32(cudaStream_t st, int rows, int cols, const double* X, long
 
 // Workspace layout of the mixed solve.
 struct MixedLayout {
-  size_t as, af, lf, w, pkh, pkl, xw, r, winv, norms, flags, total;
+  size_t as, af, lf, m2, m3, w, pkh, pkl, xw, r, yt, winv, norms, flags, total;
   long long lds, ldf, ldk;
 };
 
@@ -149,11 +149,14 @@ static MixedLayout mixed_layout(int n, int nrhs, int nb) {
   L.as = take(sizeof(double) * L.lds * n);
   L.af = take(sizeof(float) * L.ldf * n);
   L.lf = take(sizeof(double) * L.lds * n);
+  L.m2 = take(sizeof(double) * L.lds * n);  // L(r, j) inv(L_jj): forward sweep
+  L.m3 = take(sizeof(double) * L.lds * n);  // inv(L_jj) L(j, r): backward sweep
   L.w = take(sizeof(double) * (size_t)nb * nb);
   L.pkh = take(2 * sizeof(float) * (size_t)n * L.ldk);  // two buffers (look-ahead)
   L.pkl = take(2 * sizeof(float) * (size_t)n * L.ldk);
   L.xw = take(sizeof(double) * L.lds * std::max(nrhs, 1));
   L.r = take(sizeof(double) * L.lds * std::max(nrhs, 1));
+  L.yt = take(sizeof(double) * L.lds * std::max(nrhs, 1));
   L.winv = take(winv_bytes(n, nb));
   L.norms = take(sizeof(double) * ((size_t)n + 4 * (size_t)std::max(nrhs, 1)));
   L.flags = take(trsm_skinny_flag_bytes(n, nb));
@@ -161,22 +164,46 @@ static MixedLayout mixed_layout(int n, int nrhs, int nb) {
   return L;
 }
 
-// X := Lf^-T Lf^-1 X with the pre-inverted diagonal blocks Winv: two
-// cooperative sweeps (nrhs <= 64), else the blocked multiply-by-inverse form.
+// X := Lf^-T Lf^-1 X: two cooperative prescaled sweeps over M2 = L D^-1 and
+// M3 = D^-1 L (D the diagonal blocks, nrhs <= 64; Y is scratch), else the
+// blocked multiply-by-inverse form.
 struct SweepFlags {
   int* flags;
   int epoch;
+  double* M2;
+  double* M3;
+  double* Y;
 };
 static int mixed_solve(egpu_context* h, int n, int nrhs, const double* Lf, long long lds, const double* Winv,
                        double* X, SweepFlags& fl) {
-  int rc = launch_trsm_skinny(h->stream, 0, 0, n, nrhs, Lf, lds, Winv, h->nb, X, lds, fl.flags, ++fl.epoch,
-                              h->sm_count, h->dstatus);
+  int rc = launch_trsm_skinny(h->stream, 0, 0, n, nrhs, fl.M2, lds, Winv, h->nb, X, lds, fl.flags, ++fl.epoch,
+                              h->sm_count, h->dstatus, fl.Y);
   if (rc == EGPU_OK)
-    rc = launch_trsm_skinny(h->stream, 1, 1, n, nrhs, Lf, lds, Winv, h->nb, X, lds, fl.flags, ++fl.epoch,
-                            h->sm_count, h->dstatus);
+    rc = launch_trsm_skinny(h->stream, 1, 1, n, nrhs, fl.M3, lds, Winv, h->nb, fl.Y, lds, fl.flags, ++fl.epoch,
+                            h->sm_count, h->dstatus, X);
   if (rc != EGPU_ERR_UNSUPPORTED) return rc;
   TRY(trsm_blocked(h->stream, EGPU_LEFT, EGPU_LOWER, 0, n, nrhs, Lf, lds, Winv, h->nb, X, lds, h->dstatus));
   return trsm_blocked(h->stream, EGPU_LEFT, EGPU_LOWER, 1, n, nrhs, Lf, lds, Winv, h->nb, X, lds, h->dstatus);
+}
+
+// M2(r, j) = L(r, j) W_j and M3(j, r) = W_j L(j, r) for the blocks below the
+// diagonal (W_j = inv(L_jj)), one GEMM per block column / block row.
+static int mixed_prescale(egpu_context* h, int n, const double* Lf, long long lds, const double* Winv, double* M2,
+                          double* M3) {
+  const int nb = h->nb;
+  cudaStream_t st = h->stream;
+  for (int j0 = 0; j0 < n; j0 += nb) {
+    const int bj = std::min(nb, n - j0);
+    const double* Wj = Winv + (size_t)(j0 / nb) * nb * nb;
+    const int below = n - j0 - bj;
+    if (below > 0)
+      TRY(launch_dgemm(st, false, true, below, bj, bj, 1.0, Lf + (j0 + bj) + (long long)j0 * lds, lds, Wj, nb, 0.0,
+                       M2 + (j0 + bj) + (long long)j0 * lds, lds, 0, false, h->dstatus));
+    if (j0 > 0)
+      TRY(launch_dgemm(st, false, true, bj, j0, bj, 1.0, Wj, nb, Lf + j0, lds, 0.0, M3 + j0, lds, 0, false,
+                       h->dstatus));
+  }
+  return EGPU_OK;
 }
 
 // Backward error of the current iterate: max_j ||r_j|| / (||A|| ||x_j|| + ||b_j||), inf-norms.
@@ -217,7 +244,8 @@ int dposv_mixed_core_impl(egpu_context* h, int uplo, int n, int nrhs, const doub
   double* R = reinterpret_cast<double*>(ws + L.r);
   double* Winv = reinterpret_cast<double*>(ws + L.winv);
   double* norms = reinterpret_cast<double*>(ws + L.norms);
-  SweepFlags fl{reinterpret_cast<int*>(ws + L.flags), 0};
+  SweepFlags fl{reinterpret_cast<int*>(ws + L.flags), 0, reinterpret_cast<double*>(ws + L.m2),
+                reinterpret_cast<double*>(ws + L.m3), reinterpret_cast<double*>(ws + L.yt)};
   EGPU_CUDA_TRY(cudaMemsetAsync(fl.flags, 0, trsm_skinny_flag_bytes(n, nb), st));
   const long long lds = L.lds, ldf = L.ldf;
   EGPU_CUDA_TRY(cudaMemsetAsync(h->dstatus, 0, sizeof(DevStatus), st));
@@ -283,6 +311,7 @@ int dposv_mixed_core_impl(egpu_context* h, int uplo, int n, int nrhs, const doub
   TRY(read_status_now(h, &info));
   // ---- refinement
   TRY(launch_trtri_blocks(st, EGPU_LOWER, 0, Lf, lds, n, nb, Winv, nb));
+  if (nrhs <= 64) TRY(mixed_prescale(h, n, Lf, lds, Winv, fl.M2, fl.M3));
   {
     rowsum_abs_kernel<<<(n + 255) / 256, 256, 0, st>>>(n, As, lds, norms);
     count_launch();
@@ -298,13 +327,18 @@ int dposv_mixed_core_impl(egpu_context* h, int uplo, int n, int nrhs, const doub
   count_launch();
   TRY(mixed_solve(h, n, nrhs, Lf, lds, Winv, Xw, fl));
   int it = 0;
-  double e = INFINITY;
+  double e = INFINITY, e_prev = INFINITY;
   for (;;) {
     copy_cols_kernel<<<cgrid, 256, 0, st>>>(n, nrhs, B, ldb, R, lds, 0);
     count_launch();
-    TRY(launch_dgemm(st, false, true, n, nrhs, n, -1.0, As, lds, Xw, lds, 1.0, R, lds, 0, false, h->dstatus));
+    int rg = launch_dgemm_skinny(st, n, nrhs, n, -1.0, As, lds, Xw, lds, R, lds, h->sm_count, h->dstatus);
+    if (rg == EGPU_ERR_UNSUPPORTED)
+      rg = launch_dgemm(st, false, true, n, nrhs, n, -1.0, As, lds, Xw, lds, 1.0, R, lds, 0, false, h->dstatus);
+    TRY(rg);
     TRY(mixed_berr(h, n, nrhs, R, Xw, B, ldb, lds, anorm, norms + n, &e));
     if (e <= tol || it >= max_iter || !std::isfinite(e)) break;
+    if (it >= 2 && e > 0.9 * e_prev) break;  // stagnation: the factor is too far from A
+    e_prev = e;
     TRY(mixed_solve(h, n, nrhs, Lf, lds, Winv, R, fl));
     copy_cols_kernel<<<cgrid, 256, 0, st>>>(n, nrhs, R, lds, Xw, lds, 1);
     count_launch();

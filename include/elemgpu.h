@@ -146,6 +146,55 @@ EGPU_API int egpu_dgetrs(egpu_handle h, int orient, int n, int nrhs, const doubl
 /* GaussianElimination(A, B), lapack-like/GaussianElimination.hpp:216-232. */
 EGPU_API int egpu_dgesv(egpu_handle h, int n, int nrhs, double* dA, int lda, double* dB, int ldb, int* info);
 
+/* Batch plans: a batched HPD solve (kind 0, as egpu_dposv_batched) or
+ * GaussianElimination (kind 1, as egpu_dgesv_batched) whose size-sorted
+ * system list, queue and scratch stay on the device, so that a run is two
+ * stream operations with no host synchronisation (a CUDA graph can capture
+ * and replay it; the device pointers are fixed at creation: refill the
+ * matrices in place between runs).  egpu_batch_plan_autotune times the
+ * candidate persistent-grid sizes on the plan's own systems (the runs factor
+ * them in place) and keeps the fastest; egpu_batch_plan_info copies the
+ * per-system info of the last run to the host and synchronises.  A plan
+ * belongs to the handle that made it and must be destroyed before it.
+ * No counterpart in the reference (it solves one system per call). */
+typedef struct egpu_batch_plan_s* egpu_batch_plan;
+EGPU_API int egpu_batch_plan_create(egpu_handle h, int kind, int count, const int* n, const int* nrhs,
+                                    double* const* dA, const int* lda, double* const* dB, const int* ldb,
+                                    egpu_batch_plan* out);
+EGPU_API int egpu_batch_plan_run(egpu_batch_plan plan, void* stream);
+EGPU_API int egpu_batch_plan_info(egpu_batch_plan plan, void* stream, int* info);
+EGPU_API int egpu_batch_plan_autotune(egpu_batch_plan plan, void* stream, int reps, double* best_ms,
+                                      int* best_grid);
+EGPU_API int egpu_batch_plan_set_grid(egpu_batch_plan plan, int grid);
+EGPU_API int egpu_batch_plan_destroy(egpu_batch_plan plan);
+
+/* Request server (continuous batching on one GPU): no counterpart in the
+ * reference.  A dispatcher thread admits queued requests in arrival order
+ * against an HBM budget (bytes) and hands them to `slots` worker threads,
+ * each with its own handle and stream, so up to `slots` jobs run at once;
+ * all queued small requests (n <= 512, nrhs <= 16) of the kind at the head of
+ * the queue form one batched job.  mode 0: FP64 solves; mode 1: HPD requests
+ * take egpu_dposv_mixed (FP64 fallback when it cannot reach the tolerance),
+ * GE requests stay FP64.  kind 0 = HPDSolve(LOWER) (A lower triangle read),
+ * kind 1 = GaussianElimination.  A, B, X are host buffers (pinned for
+ * speed) that must stay valid until the request completes; A and B are not
+ * modified, X receives the solution.  The per-slot handle workspaces are
+ * outside the budget's accounting. */
+typedef struct egpu_server_s* egpu_server;
+EGPU_API int egpu_server_create(int device, size_t hbm_budget_bytes, int slots, int mode, egpu_server* out);
+EGPU_API int egpu_server_set_tolerance(egpu_server s, double tol);
+EGPU_API int egpu_server_submit(egpu_server s, int kind, int n, int nrhs, const double* A, int lda,
+                                const double* B, int ldb, double* X, int ldx, unsigned long long* id);
+/* *done = 0 while queued or running; once done: *status (EGPU_* code),
+ * *latency_ms (completion - submission), *path (0 FP64, 1 mixed, 2 batched,
+ * 3 mixed fell back to FP64), *iters and *berr (mixed path).  wait != 0
+ * blocks until the request completes. */
+EGPU_API int egpu_server_query(egpu_server s, unsigned long long id, int wait, int* done, int* status,
+                               double* latency_ms, int* path, int* iters, double* berr);
+EGPU_API int egpu_server_release(egpu_server s, unsigned long long id);
+EGPU_API int egpu_server_drain(egpu_server s);
+EGPU_API int egpu_server_destroy(egpu_server s);
+
 /* Mixed-precision HPDSolve (HPDSolve.hpp:18-28 computes the same x): no
  * counterpart in the reference, which factors in the working precision only.
  * Cholesky with the trailing updates on the tcgen05 tensor cores in TF32 x 3

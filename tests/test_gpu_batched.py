@@ -14,7 +14,7 @@ pytestmark = pytest.mark.gpu
 def test_hpd_solve_batched_uneven(handle):
     r = inputs.rng(2024)
     sizes = [1, 2, 31, 32, 33, 64, 127, 128, 129, 300, 511, 512] + list(r.integers(1, 513, 36))
-    nrhs = [int(x) for x in r.integers(1, 9, len(sizes))]
+    nrhs = [int(x) for x in r.integers(1, 17, len(sizes))]  # up to the 16-column limit
     As, Bs, dA, dB = [], [], [], []
     for i, (n, k) in enumerate(zip(sizes, nrhs)):
         A = inputs.spd_ggt(int(n), seed=3000 + i)
@@ -49,7 +49,7 @@ def test_hpd_batched_reports_failures_per_system(handle):
 def test_gaussian_elimination_batched_uneven(handle):
     r = inputs.rng(77)
     sizes = [1, 2, 31, 32, 33, 64, 100, 255, 256, 257, 511, 512] + list(r.integers(1, 513, 24))
-    nrhs = [int(x) for x in r.integers(1, 9, len(sizes))]
+    nrhs = [int(x) for x in r.integers(1, 17, len(sizes))]  # up to the 16-column limit
     As, Bs, dA, dB = [], [], [], []
     for i, (n, k) in enumerate(zip(sizes, nrhs)):
         A = inputs.uniform(int(n), int(n), seed=5000 + i)
@@ -74,3 +74,52 @@ def test_gaussian_elimination_batched_singular(handle):
     dA = [eg.colmajor_cuda(good), eg.colmajor_cuda(bad)]
     dB = [eg.colmajor_cuda(inputs.normal(80, 1, s)) for s in range(2)]
     assert handle.gaussian_elimination_batched(dA, dB) == [0, 46]
+
+
+@pytest.mark.parametrize("kind", [0, 1])
+def test_batch_plan_graph_replay_matches_oracle(handle, kind):
+    """A plan run captured in a CUDA graph and replayed on refilled inputs
+    gives the oracle's per-system solutions; the autotuner keeps a valid grid."""
+    import torch
+    r = inputs.rng(77 + kind)
+    sizes = [int(x) for x in r.integers(1, 513, 24)] + [512, 1, 33]
+    As, Bs, dA, dB = [], [], [], []
+    for i, n in enumerate(sizes):
+        A = inputs.spd_ggt(n, 500 + i) if kind == 0 else inputs.uniform(n, n, 500 + i)
+        B = inputs.normal(n, 1 + i % 16, 600 + i)
+        As.append(A); Bs.append(B)
+        dA.append(eg.colmajor_cuda(A)); dB.append(eg.colmajor_cuda(B))
+    A0 = [a.clone() for a in dA]
+    B0 = [b.clone() for b in dB]
+    plan = eg.BatchPlan(handle, kind, dA, dB)
+    ms, grid = plan.autotune(reps=1)
+    assert ms > 0 and 1 <= grid <= torch.cuda.get_device_properties(0).multi_processor_count
+    s = torch.cuda.Stream()
+    torch.cuda.synchronize()
+    for a, a0 in zip(dA, A0):
+        a.copy_(a0)
+    for b, b0 in zip(dB, B0):
+        b.copy_(b0)
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g, stream=s):
+        plan.run(s)
+    torch.cuda.synchronize()
+    for rep in range(2):  # refill, replay
+        for a, a0 in zip(dA, A0):
+            a.copy_(a0)
+        for b, b0 in zip(dB, B0):
+            b.copy_(b0)
+        torch.cuda.synchronize()
+        g.replay()
+        torch.cuda.synchronize()
+    assert plan.info(s) == [0] * len(sizes)
+    for i, (A, B) in enumerate(zip(As, Bs)):
+        if kind == 0:
+            _, X, st = orc.hpd_solve(A, B, orc.LOWER, nb=32)
+        else:
+            _, X, st = orc.gaussian_elimination(A, B, nb=32)
+        assert st == 0
+        Xg = dB[i].cpu().numpy()
+        assert np.max(np.abs(Xg - X)) <= 1e-8 * max(1.0, np.max(np.abs(X))), i
+    plan.close()

@@ -89,3 +89,19 @@ def test_hpd_solve_mixed_not_hpd(handle):
     A[150, 150] = -1.0
     with pytest.raises(eg.NonHPDError):
         handle.hpd_solve_mixed(eg.colmajor_cuda(A), eg.colmajor_cuda(inputs.normal(300, 2, 6)))
+
+
+def test_host_hpd_solve_mixed_matches_device():
+    """The host-memory entry gives the device entry's solution."""
+    h = eg.Handle(0)
+    n, k = 700, 5
+    A = inputs.spd_spectrum(n, 1e5, 51)
+    B = inputs.normal(n, k, 52)
+    X = np.zeros((n, k), order="F")
+    it, be = h.host_hpd_solve_mixed(A, B, X)
+    Xd, it2, be2 = h.hpd_solve_mixed(eg.colmajor_cuda(A), eg.colmajor_cuda(B))
+    assert be <= 1e-14 and be2 <= 1e-14
+    assert _berr(A, X, B) <= 1e-14
+    # both at backward error <= 1e-14: forward errors within kappa * 1e-14 of each other
+    assert np.abs(X - Xd.cpu().numpy()).max() <= 1e5 * 1e-14 * np.abs(X).max()
+    h.close()

@@ -223,10 +223,12 @@ def test_lu_nopiv(handle):
 
 # --------------------------------------------------------------- solves --
 
+# nrhs <= 64 with an even leading dimension takes the one-launch skinny
+# sweep; odd leading dimensions and wider right-hand sides the blocked form
 @pytest.mark.parametrize("uplo", [eg.LOWER, eg.UPPER])
-@pytest.mark.parametrize("nrhs", [1, 16])
-def test_hpd_solve(handle, uplo, nrhs):
-    n = 1030
+@pytest.mark.parametrize("nrhs", [1, 16, 65])
+@pytest.mark.parametrize("n", [1030, 1031])
+def test_hpd_solve(handle, uplo, nrhs, n):
     A = inputs.spd_ggt(n, 21)
     B = inputs.normal(n, nrhs, 22)
     dA, dB = cuda(A), cuda(B)
@@ -239,10 +241,10 @@ def test_hpd_solve(handle, uplo, nrhs):
 
 
 @pytest.mark.parametrize("orient", [eg.NORMAL, eg.TRANSPOSE])
-@pytest.mark.parametrize("nrhs", [1, 64])
-def test_lu_solve_after(handle, orient, nrhs):
+@pytest.mark.parametrize("nrhs", [1, 64, 65])
+@pytest.mark.parametrize("n", [999, 1000])
+def test_lu_solve_after(handle, orient, nrhs, n):
     import torch
-    n = 999
     A = inputs.uniform(n, n, 31)
     B = inputs.normal(n, nrhs, 32)
     dA = cuda(A)
