@@ -404,7 +404,7 @@ class Handle:
     def launch_count(self) -> int:
         return int(lib().egpu_launch_count(self._h))
 
-    TRACE_KINDS = {"update": 0, "trsm": 1, "diag": 2, "panel": 3, "swap": 4, "other": 5, "tc": 6}
+    TRACE_KINDS = {"update": 0, "trsm": 1, "diag": 2, "panel": 3, "swap": 4, "other": 5, "tc": 6, "solve": 7}
 
     def trace_enable(self, on: bool = True):
         """Bracket every launch with CUDA events on its stream (clears old records)."""

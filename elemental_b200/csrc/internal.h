@@ -18,7 +18,7 @@ bool tma_compatible(const void* p, long long ld);
 
 // ---- launch tracing (per-kernel-class CUDA-event timing on the launch stream)
 enum TraceKind { kTraceUpdate = 0, kTraceTrsm = 1, kTraceDiag = 2, kTracePanel = 3, kTraceSwap = 4,
-                 kTraceOther = 5, kTraceTc = 6, kTraceKinds = 7 };
+                 kTraceOther = 5, kTraceTc = 6, kTraceSolve = 7, kTraceKinds = 8 };
 struct Trace;
 // Records an event pair around one launch when the calling thread has an
 // active trace; no-op otherwise.

@@ -186,23 +186,21 @@ static int mixed_solve(egpu_context* h, int n, int nrhs, const double* Lf, long 
   return trsm_blocked(h->stream, EGPU_LEFT, EGPU_LOWER, 1, n, nrhs, Lf, lds, Winv, h->nb, X, lds, h->dstatus);
 }
 
-// M2(r, j) = L(r, j) W_j and M3(j, r) = W_j L(j, r) for the blocks below the
-// diagonal (W_j = inv(L_jj)), one GEMM per block column / block row.
-static int mixed_prescale(egpu_context* h, int n, const double* Lf, long long lds, const double* Winv, double* M2,
-                          double* M3) {
+// Prescaled copies of block column / row block j0 for the solve sweeps:
+// M2(r, j) = L(r, j) W_j below the diagonal block and M3(j, r) = W_j L(j, r)
+// left of it (W_j = inv(L_jj)).
+static int mixed_prescale_step(egpu_context* h, cudaStream_t st, int n, int j0, const double* Lf, long long lds,
+                               const double* Winv, double* M2, double* M3) {
   const int nb = h->nb;
-  cudaStream_t st = h->stream;
-  for (int j0 = 0; j0 < n; j0 += nb) {
-    const int bj = std::min(nb, n - j0);
-    const double* Wj = Winv + (size_t)(j0 / nb) * nb * nb;
-    const int below = n - j0 - bj;
-    if (below > 0)
-      TRY(launch_dgemm(st, false, true, below, bj, bj, 1.0, Lf + (j0 + bj) + (long long)j0 * lds, lds, Wj, nb, 0.0,
-                       M2 + (j0 + bj) + (long long)j0 * lds, lds, 0, false, h->dstatus));
-    if (j0 > 0)
-      TRY(launch_dgemm(st, false, true, bj, j0, bj, 1.0, Wj, nb, Lf + j0, lds, 0.0, M3 + j0, lds, 0, false,
-                       h->dstatus));
-  }
+  const int bj = std::min(nb, n - j0);
+  const double* Wj = Winv + (size_t)(j0 / nb) * nb * nb;
+  const int below = n - j0 - bj;
+  if (below > 0)
+    TRY(launch_dgemm(st, false, true, below, bj, bj, 1.0, Lf + (j0 + bj) + (long long)j0 * lds, lds, Wj, nb, 0.0,
+                     M2 + (j0 + bj) + (long long)j0 * lds, lds, 0, false, h->dstatus));
+  if (j0 > 0)
+    TRY(launch_dgemm(st, false, true, bj, j0, bj, 1.0, Wj, nb, Lf + j0, lds, 0.0, M3 + j0, lds, 0, false,
+                     h->dstatus));
   return EGPU_OK;
 }
 
@@ -263,6 +261,7 @@ int dposv_mixed_core_impl(egpu_context* h, int uplo, int n, int nrhs, const doub
   float* PKh2[2] = {PKh, PKh + (size_t)n * L.ldk};
   float* PKl2[2] = {PKl, PKl + (size_t)n * L.ldk};
   cudaStream_t sd = h->side;
+  const bool prescale = nrhs <= 64;
   auto panel_chain = [&](int k, cudaStream_t s) -> int {
     const int b = std::min(nb, n - k);
     const int m = n - k, m2 = m - b;
@@ -273,10 +272,11 @@ int dposv_mixed_core_impl(egpu_context* h, int uplo, int n, int nrhs, const doub
       count_launch();
       EGPU_CUDA_TRY(cudaGetLastError());
     }
-    TRY(launch_potrf_diag(s, EGPU_LOWER, Lf + k + (long long)k * lds, lds, b, W, nb, h->dstatus, k));
+    double* Wk = Winv + (size_t)(k / nb) * nb * nb;  // this block's inverse, kept for the solves
+    TRY(launch_potrf_diag(s, EGPU_LOWER, Lf + k + (long long)k * lds, lds, b, Wk, nb, h->dstatus, k));
     if (m2 == 0) return EGPU_OK;
     double* L21 = Lf + (k + b) + (long long)k * lds;
-    TRY(launch_dgemm(s, false, false, m2, b, b, 1.0, L21, lds, W, nb, 0.0, L21, lds, 0, true, h->dstatus));
+    TRY(launch_dgemm(s, false, false, m2, b, b, 1.0, L21, lds, Wk, nb, 0.0, L21, lds, 0, true, h->dstatus));
     const int par = (k / nb) & 1;
     return launch_split_tf32(s, m2, b, L21, lds, PKh2[par], PKl2[par], L.ldk);
   };
@@ -304,14 +304,16 @@ int dposv_mixed_core_impl(egpu_context* h, int uplo, int n, int nrhs, const doub
       TRY(launch_tc_gemm(st, m3, m3, b, -1.0f, PKh2[par] + (size_t)b2 * L.ldk, PKl2[par] + (size_t)b2 * L.ldk,
                          PKh2[par] + (size_t)b2 * L.ldk, PKl2[par] + (size_t)b2 * L.ldk, L.ldk, 1.0f,
                          A22 + b2 + (long long)b2 * ldf, ldf, 1, 3, h->dstatus));
+    // prescaled copies for the solve sweeps, off the panel chain: M2 of block
+    // column k, M3 of row block k (its row block of L is final by now)
+    if (prescale) TRY(mixed_prescale_step(h, st, n, k, Lf, lds, Winv, fl.M2, fl.M3));
   }
   EGPU_CUDA_TRY(cudaEventRecord(h->ev_join, sd));
   EGPU_CUDA_TRY(cudaStreamWaitEvent(st, h->ev_join, 0));
+  if (prescale) TRY(mixed_prescale_step(h, st, n, (n - 1) / nb * nb, Lf, lds, Winv, fl.M2, fl.M3));  // last block
   int info = 0;
   TRY(read_status_now(h, &info));
   // ---- refinement
-  TRY(launch_trtri_blocks(st, EGPU_LOWER, 0, Lf, lds, n, nb, Winv, nb));
-  if (nrhs <= 64) TRY(mixed_prescale(h, n, Lf, lds, Winv, fl.M2, fl.M3));
   {
     rowsum_abs_kernel<<<(n + 255) / 256, 256, 0, st>>>(n, As, lds, norms);
     count_launch();

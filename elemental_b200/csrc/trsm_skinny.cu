@@ -300,7 +300,7 @@ int launch_trsm_skinny(cudaStream_t st, int bwd, int amode, int n, int nrhs, con
     attr = true;
   }
   const int grid = std::min(p.nblk, sm_count);
-  TraceMark tm(st, kTraceTrsm, (double)n * n * nrhs, 4.0 * (double)n * n + 16.0 * n * nrhs);
+  TraceMark tm(st, kTraceSolve, (double)n * n * nrhs, 4.0 * (double)n * n + 16.0 * n * nrhs);
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(grid);
   cfg.blockDim = dim3(kTsThreads);

@@ -104,7 +104,8 @@ EGPU_API long long egpu_launch_count(egpu_handle h);
  * every kernel launch issued through this handle is bracketed by CUDA events
  * on its own stream.  Kinds: 0 trailing update (Gemm/Herk), 1 triangular
  * multiply by an inverted diagonal block (Trsm), 2 diagonal-block kernels,
- * 3 LU panel, 4 row interchanges, 5 other.  enable() clears the records;
+ * 3 LU panel, 4 row interchanges, 5 other (batched kernels, conversions),
+ * 6 tcgen05 tensor-core updates, 7 one-launch solve sweeps.  enable() clears the records;
  * summary() waits for the recorded launches and sums their device time,
  * algorithmic flops and algorithmic bytes. */
 EGPU_API int egpu_trace_enable(egpu_handle h, int on);
