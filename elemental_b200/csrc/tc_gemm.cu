@@ -8,19 +8,20 @@
 // hi*hi + hi*lo + lo*hi, which keeps ~21 bits of the FP32 product (the
 // dropped lo*lo term is 2^-22 relative).  terms = 1 is the plain TF32 product.
 //
-// Persistent kernel, one CTA per SM, 192 threads, output tiles of 128 x 128
-// taken round-robin (triangular tile lists for the symmetric rank-k update of
-// a lower triangle):
-//   warp 4 lane 0: TMA producer, 128-byte-swizzled 128 x 32 tiles into a
+// Each CTA (one per SM at a time, 320 threads) takes a contiguous run of up
+// to 8 output tiles of 128 x 128 (triangular tile lists for the symmetric
+// rank-k update of a lower triangle):
+//   warp 8 lane 0: TMA producer, 128-byte-swizzled 128 x 32 tiles into a
 //                  ring of stages that runs across tile boundaries
 //                  (mbarrier full/empty pairs, bounded waits);
-//   warp 5 lane 0: MMA issuer, tcgen05.mma.cta_group::1.kind::tf32 128x128x8,
+//   warp 9 lane 0: MMA issuer, tcgen05.mma.cta_group::1.kind::tf32 128x128x8,
 //                  four per 32-wide k tile and term, into one of two TMEM
 //                  accumulators (256 columns) so that a tile's epilogue
 //                  overlaps the next tile's MMAs;
-//   warps 0-3    : epilogue, C rows read into registers before the
+//   warps 0-7    : epilogue, C rows read into registers before the
 //                  accumulator is ready, then tcgen05.ld.32x32b of their 32
-//                  TMEM lanes (one output row per thread) and a coalesced store.
+//                  TMEM lanes (warp e: lanes 32 (e % 4).., columns 64 (e / 4)..)
+//                  and a coalesced store, one output row per thread.
 #include <cudaTypedefs.h>
 
 #include "internal.h"
@@ -119,7 +120,7 @@ __global__ void __maxnreg__(200) tc_gemm_kernel(const __grid_constant__ CUtensor
                                                                  const __grid_constant__ CUtensorMap mbh,
                                                                  const __grid_constant__ CUtensorMap mal,
                                                                  const __grid_constant__ CUtensorMap mbl,
-                                                                 TcParams p, int ntiles) {
+                                                                 TcParams p, int ntiles, int per_cta) {
   using S = TcShape<NT>;
   extern __shared__ unsigned char tc_smem_raw[];
   unsigned char* smem = reinterpret_cast<unsigned char*>(
@@ -134,6 +135,10 @@ __global__ void __maxnreg__(200) tc_gemm_kernel(const __grid_constant__ CUtensor
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   if (p.status != nullptr && ((volatile DevStatus*)p.status)->code != 0) return;  // uniform
   const int KT = (p.K + kTcBK - 1) / kTcBK;
+  // a contiguous run of `per_cta` tiles per CTA: CTAs retire every few tiles,
+  // so kernels of a higher-priority stream (the look-ahead panel chain) get
+  // SMs between them instead of waiting for the whole update
+  const int t_first = blockIdx.x * per_cta, t_end = min(ntiles, t_first + per_cta);
 
   if (tid == 0) {
     for (int s = 0; s < S::kStages; ++s) { mbar_init(&full[s], 1); mbar_init(&empty[s], 1); }
@@ -157,7 +162,7 @@ __global__ void __maxnreg__(200) tc_gemm_kernel(const __grid_constant__ CUtensor
       tma_prefetch_desc(&mbh);
       if (NT == 3) { tma_prefetch_desc(&mal); tma_prefetch_desc(&mbl); }
       int g = 0;
-      for (int t = blockIdx.x; t < ntiles && !*abort_flag; t += gridDim.x) {
+      for (int t = t_first; t < t_end && !*abort_flag; ++t) {
         int tm, tn;
         tc_tile_of(p, t, tm, tn);
         const int m0 = tm * kTcBM, n0 = tn * kTcBN;
@@ -180,7 +185,7 @@ __global__ void __maxnreg__(200) tc_gemm_kernel(const __grid_constant__ CUtensor
   } else if (warp == kTcMmaWarp) {
     if (lane == 0) {  // ---- MMA issuer
       int g = 0, i = 0;
-      for (int t = blockIdx.x; t < ntiles && !*abort_flag; t += gridDim.x, ++i) {
+      for (int t = t_first; t < t_end && !*abort_flag; ++t, ++i) {
         const int a = i & 1;
         const uint32_t acc_addr = tmem + (uint32_t)(a * kTcBN);
         if (!mbar_wait_bounded(&tempty[a], ((uint32_t)(i >> 1) & 1u) ^ 1u)) {
@@ -214,7 +219,7 @@ __global__ void __maxnreg__(200) tc_gemm_kernel(const __grid_constant__ CUtensor
     // columns 64 (e / 4) .. of each tile; each thread owns one output row.
     const int q = warp & 3, half = warp >> 2;
     int i = 0;
-    for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++i) {
+    for (int t = t_first; t < t_end; ++t, ++i) {
       int tm, tn;
       tc_tile_of(p, t, tm, tn);
       const int m0 = tm * kTcBM, n0 = tn * kTcBN + half * 64;
@@ -276,8 +281,9 @@ static cudaError_t tc_launch_variant(cudaStream_t st, const CUtensorMap& mah, co
   }
   int dev_sms = 148;
   cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, dev);
-  const unsigned grid = (unsigned)std::min<long long>(nblocks, dev_sms);
-  kern<<<grid, kTcThreads, TcShape<NT>::kSmemBytes, st>>>(mah, mbh, mal, mbl, p, (int)nblocks);
+  const int per_cta = (int)std::max<long long>(1, std::min<long long>(8, nblocks / (4LL * dev_sms)));
+  const unsigned grid = (unsigned)((nblocks + per_cta - 1) / per_cta);
+  kern<<<grid, kTcThreads, TcShape<NT>::kSmemBytes, st>>>(mah, mbh, mal, mbl, p, (int)nblocks, per_cta);
   count_launch();
   return cudaGetLastError();
 }

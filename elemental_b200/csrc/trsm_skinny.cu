@@ -25,10 +25,10 @@
 // inverse on the dependency chain: a CTA publishes z_r (in X) as soon as the
 // sum is done and forms Y_r = inv(T_rr) z_r afterwards.
 //
-// Products are 16 x 8 x 8 DMMA fragments from shared memory: the 128 x 32
-// chunk of the block (ld 132, or its transpose with ld 36: conflict-free
-// fragment loads) and the 32 x nrhs chunk of X_j (ld 36), two cp.async stages
-// of 16-byte copies.  Requires nrhs <= 64, nb <= 128 even, lda and ldx even,
+// Products are 16 x 8 x 8 DMMA fragments from shared memory: the whole
+// off-diagonal block (ld 132, or its transpose with ld 132: conflict-free
+// fragment loads) and the matching X block, 16-byte cp.async copies in four
+// 32-deep groups that all are in flight at once.  Requires nrhs <= 64, nb <= 128 even, lda and ldx even,
 // A, Winv, X (and Y) 16-byte aligned.
 #include "internal.h"
 
@@ -37,16 +37,12 @@ namespace egpu {
 namespace {
 
 constexpr int kTsThreads = 256;  // 8 warps: warp w owns rows 16w .. 16w+15 of the block
-constexpr int kTsKC = 32;        // k chunk
-constexpr int kTsLDA = 132;      // column-major chunk [a + k * 132]
-constexpr int kTsLDK = 36;       // transposed chunk [k + a * 36]
-constexpr int kTsLDX = 36;
+constexpr int kTsKC = 32;        // k chunk (one cp.async group each)
+constexpr int kTsLD = 132;       // leading dimension of the staged blocks (conflict-free fragment loads)
 constexpr int kTsMaxRhs = 64;
-constexpr int kTsStageA = 128 * kTsLDK > kTsKC * kTsLDA ? 128 * kTsLDK : kTsKC * kTsLDA;  // doubles
-constexpr int kTsStageX = kTsMaxRhs * kTsLDX;       // doubles: the X chunk, [k + c * 36]
-constexpr int kTsStage = kTsStageA + kTsStageX;
-constexpr int kTsAccLD = 132;                       // acc staging [a + c * 132]
-constexpr int kTsSmemDoubles = 2 * kTsStage + kTsMaxRhs * kTsAccLD;
+constexpr int kTsA = 128 * kTsLD;          // doubles: a whole off-diagonal block, [a + k*132] or [k + a*132]
+constexpr int kTsX = kTsMaxRhs * kTsLD;    // doubles: the matching X block, [k + c*132]
+constexpr int kTsSmemDoubles = kTsA + kTsX;
 
 struct TsParams {
   const double* L;
@@ -56,6 +52,7 @@ struct TsParams {
   long long ldx;
   double* Y;  // prescaled form: X_r receives the unscaled block (published), Y_r = inv(T_rr) X_r
   int n, nrhs, nb, nblk, bwd, amode;
+  int strips, hs;  // tasks per block row and their height (prescaled form: 2)
   int* flags;
   int epoch;
   DevStatus* status;
@@ -65,61 +62,67 @@ struct TsParams {
 __device__ __forceinline__ int ts_block(const TsParams& p, int s) { return p.bwd ? p.nblk - 1 - s : s; }
 
 // Stage the k chunk [k0, k0+32) of an m x K operand A (m <= 128 rows) into
-// shared memory with 16-byte .cg copies.  amode 0: A(a, k) = G[a + k lda]
-// (column-major block), kept as sA[a + k * 132]; amode 1: A(a, k) =
-// G[k + a lda] (the transpose of a column-major block), kept as
-// sA[k + a * 36].  Out-of-range entries are zero.  lda even, G 16-byte
+// the whole-block buffer with 16-byte .cg copies.  amode 0: A(a, k) =
+// G[a + k lda] (column-major block), kept as sA[a + k * 132]; amode 1:
+// A(a, k) = G[k + a lda] (the transpose of a column-major block), kept as
+// sA[k + a * 132].  Out-of-range entries are zero.  lda even, G 16-byte
 // aligned, k0 even.
 __device__ __forceinline__ void ts_stage_a(double* sA, const double* G, long long lda, int amode, int m, int K,
                                            int k0) {
   const int tid = threadIdx.x;
   if (amode == 0) {
     for (int e = tid; e < 64 * kTsKC; e += kTsThreads) {  // row pairs
-      const int a = 2 * (e & 63), k = e >> 6;
-      double* d = &sA[a + k * kTsLDA];
-      const double* src = &G[a + (long long)(k0 + k) * lda];
-      if (k0 + k < K && a + 1 < m) cp_async16_cg(d, src);
+      const int a = 2 * (e & 63), k = k0 + (e >> 6);
+      double* d = &sA[a + k * kTsLD];
+      const double* src = &G[a + (long long)k * lda];
+      if (k < K && a + 1 < m) cp_async16_cg(d, src);
       else {
-        d[0] = (k0 + k < K && a < m) ? src[0] : 0.0;
+        d[0] = (k < K && a < m) ? src[0] : 0.0;
         d[1] = 0.0;
       }
     }
   } else {
     for (int e = tid; e < 128 * (kTsKC / 2); e += kTsThreads) {  // k pairs
-      const int k = 2 * (e & 15), a = e >> 4;
-      double* d = &sA[k + a * kTsLDK];
-      const double* src = &G[(k0 + k) + (long long)a * lda];
-      if (a < m && k0 + k + 1 < K) cp_async16_cg(d, src);
+      const int k = k0 + 2 * (e & 15), a = e >> 4;
+      double* d = &sA[k + a * kTsLD];
+      const double* src = &G[k + (long long)a * lda];
+      if (a < m && k + 1 < K) cp_async16_cg(d, src);
       else {
-        d[0] = (a < m && k0 + k < K) ? src[0] : 0.0;
+        d[0] = (a < m && k < K) ? src[0] : 0.0;
         d[1] = 0.0;
       }
     }
   }
 }
 
-// The matching rows [k0, k0+32) of X (K x nrhs) into sX[k + c * 36].
-__device__ __forceinline__ void ts_stage_x(double* sX, int K, int k0, const double* Xg, long long ldx, int nrhs,
-                                           bool x_shared) {
-  // X rows in pairs: 16-byte .cg copies (L2, never a stale L1 line of a block
-  // another CTA has just published); ldx even and X 16-byte aligned
+// The matching rows [k0, k0+32) of X (K x nrhs) into sX[k + c * 132]:
+// 16-byte .cg copies (L2, never a stale L1 line of a block another CTA has
+// just published); ldx even and X 16-byte aligned.
+__device__ __forceinline__ void ts_stage_x(double* sX, int K, int k0, const double* Xg, long long ldx, int nrhs) {
   for (int e = threadIdx.x; e < (kTsKC / 2) * nrhs; e += kTsThreads) {
-    const int k = 2 * (e & 15), c = e >> 4;
-    double* d = &sX[k + c * kTsLDX];
-    const double* src = &Xg[(k0 + k) + (long long)c * ldx];
-    if (x_shared) {  // operand staged in this CTA's shared memory
-      d[0] = (k0 + k < K) ? src[0] : 0.0;
-      d[1] = (k0 + k + 1 < K) ? src[1] : 0.0;
-    } else if (k0 + k + 1 < K) {
+    const int k = k0 + 2 * (e & 15), c = e >> 4;
+    double* d = &sX[k + c * kTsLD];
+    const double* src = &Xg[k + (long long)c * ldx];
+    if (k + 1 < K) {
       cp_async16_cg(d, src);
     } else {
-      d[0] = (k0 + k < K) ? __ldcg(src) : 0.0;
+      d[0] = (k < K) ? __ldcg(src) : 0.0;
       d[1] = 0.0;
     }
   }
 }
 
-// Bounded wait (thread 0) for *flag == epoch, then a CTA barrier.  Returns
+__device__ __forceinline__ void ts_wait_groups(int pending) {
+  switch (pending) {  // cp.async.wait_group takes an immediate
+    case 0: asm volatile("cp.async.wait_group 0;" ::: "memory"); break;
+    case 1: asm volatile("cp.async.wait_group 1;" ::: "memory"); break;
+    case 2: asm volatile("cp.async.wait_group 2;" ::: "memory"); break;
+    default: asm volatile("cp.async.wait_group 3;" ::: "memory"); break;
+  }
+}
+
+// Bounded wait (thread 0) for the arrival counter *flag to reach `epoch`
+// (strips x sweep number), then a CTA barrier.  Returns
 // false (all threads) when the wait ran out.
 __device__ __forceinline__ bool ts_wait_flag(const int* flag, int epoch, DevStatus* status) {
   __shared__ int s_ok;
@@ -129,7 +132,7 @@ __device__ __forceinline__ bool ts_wait_flag(const int* flag, int epoch, DevStat
     while (true) {
       int v;
       asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(flag) : "memory");
-      if (v == epoch) break;
+      if (v >= epoch) break;
       if (++it > kSpinLimit) { ok = 0; set_status(status, kTimeout, 201); break; }
       if (it > 16) __nanosleep(64);
     }
@@ -139,50 +142,51 @@ __device__ __forceinline__ bool ts_wait_flag(const int* flag, int epoch, DevStat
   return s_ok != 0;
 }
 
-// acc[nt] (16 x 8 fragments, rows 16 warp.., columns 8 nt..) += sign * A(m x K) * Xg(K x nrhs).
-// With `flag` set, the first A chunk is requested before waiting for X to be published.
+// acc[nt] (16 x 8 fragments, rows 16 warp.., columns 8 nt..) += sign * A(m x K) * X(K x nrhs), K <= 128.
+// Every chunk of A is requested at once (one cp.async group each) before the
+// wait for X to be published (`flag`), then every chunk of X, so one product
+// costs one memory round trip plus its DMMAs.  x_in_smem: X already sits in
+// the X buffer (the staged accumulator).
 __device__ bool ts_product(double (&acc)[8][4], double sign, double* sm, const double* G, long long lda, int amode,
-                           int m, int K, const double* Xg, long long ldx, int nrhs, bool x_shared,
+                           int m, int K, const double* Xg, long long ldx, int nrhs, bool x_in_smem,
                            const int* flag = nullptr, int epoch = 0, DevStatus* status = nullptr) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int g = lane >> 2, t = lane & 3;
-  const int nchunks = (K + kTsKC - 1) / kTsKC;
+  const int nch = (K + kTsKC - 1) / kTsKC;
   const int ntn = (nrhs + 7) / 8;
-  ts_stage_a(sm, G, lda, amode, m, K, 0);
+  double* sA = sm;
+  double* sX = sm + kTsA;
+  for (int c = 0; c < nch; ++c) {
+    ts_stage_a(sA, G, lda, amode, m, K, c * kTsKC);
+    asm volatile("cp.async.commit_group;" ::: "memory");
+  }
   if (flag != nullptr && !ts_wait_flag(flag, epoch, status)) {
-    asm volatile("cp.async.commit_group;\n cp.async.wait_group 0;" ::: "memory");
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
     return false;
   }
-  ts_stage_x(sm + kTsStageA, K, 0, Xg, ldx, nrhs, x_shared);
-  asm volatile("cp.async.commit_group;" ::: "memory");
-  for (int ch = 0; ch < nchunks; ++ch) {
-    double* cur = sm + (ch & 1) * kTsStage;
-    if (ch + 1 < nchunks) {
-      double* nxt = sm + ((ch + 1) & 1) * kTsStage;
-      ts_stage_a(nxt, G, lda, amode, m, K, (ch + 1) * kTsKC);
-      ts_stage_x(nxt + kTsStageA, K, (ch + 1) * kTsKC, Xg, ldx, nrhs, x_shared);
+  if (!x_in_smem)
+    for (int c = 0; c < nch; ++c) {
+      ts_stage_x(sX, K, c * kTsKC, Xg, ldx, nrhs);
       asm volatile("cp.async.commit_group;" ::: "memory");
-      asm volatile("cp.async.wait_group 1;" ::: "memory");
-    } else {
-      asm volatile("cp.async.wait_group 0;" ::: "memory");
     }
+  for (int c = 0; c < nch; ++c) {
+    ts_wait_groups(nch - 1 - c);  // A chunk c (and X chunk c) landed for this thread
     __syncthreads();
-    const double* sA = cur;
-    const double* sX = cur + kTsStageA;
 #pragma unroll
     for (int kk = 0; kk < kTsKC; kk += 8) {
+      const int k = c * kTsKC + kk;
       double a[4];
       const int ra = 16 * warp + g;
       if (amode == 0) {
-        a[0] = sA[ra + (kk + t) * kTsLDA];
-        a[1] = sA[ra + 8 + (kk + t) * kTsLDA];
-        a[2] = sA[ra + (kk + t + 4) * kTsLDA];
-        a[3] = sA[ra + 8 + (kk + t + 4) * kTsLDA];
+        a[0] = sA[ra + (k + t) * kTsLD];
+        a[1] = sA[ra + 8 + (k + t) * kTsLD];
+        a[2] = sA[ra + (k + t + 4) * kTsLD];
+        a[3] = sA[ra + 8 + (k + t + 4) * kTsLD];
       } else {
-        a[0] = sA[(kk + t) + ra * kTsLDK];
-        a[1] = sA[(kk + t) + (ra + 8) * kTsLDK];
-        a[2] = sA[(kk + t + 4) + ra * kTsLDK];
-        a[3] = sA[(kk + t + 4) + (ra + 8) * kTsLDK];
+        a[0] = sA[(k + t) + ra * kTsLD];
+        a[1] = sA[(k + t) + (ra + 8) * kTsLD];
+        a[2] = sA[(k + t + 4) + ra * kTsLD];
+        a[3] = sA[(k + t + 4) + (ra + 8) * kTsLD];
       }
 #pragma unroll
       for (int q = 0; q < 4; ++q) a[q] *= sign;
@@ -190,14 +194,14 @@ __device__ bool ts_product(double (&acc)[8][4], double sign, double* sm, const d
       for (int nt = 0; nt < 8; ++nt) {
         if (nt < ntn) {
           double bf[2];
-          bf[0] = sX[(kk + t) + (8 * nt + g) * kTsLDX];
-          bf[1] = sX[(kk + t + 4) + (8 * nt + g) * kTsLDX];
+          bf[0] = sX[(k + t) + (8 * nt + g) * kTsLD];
+          bf[1] = sX[(k + t + 4) + (8 * nt + g) * kTsLD];
           dmma_16x8x8(acc[nt], a, bf);
         }
       }
     }
-    __syncthreads();
   }
+  __syncthreads();  // the buffers are free for the next product
   return true;
 }
 
@@ -205,78 +209,102 @@ __device__ bool ts_product(double (&acc)[8][4], double sign, double* sm, const d
 
 __global__ void __launch_bounds__(kTsThreads, 1) trsm_skinny_kernel(TsParams p) {
   extern __shared__ double sm[];
-  double* accS = sm + 2 * kTsStage;
+  double* accS = sm + kTsA;  // the X buffer: the accumulator is the next product's right operand
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int g = lane >> 2, t = lane & 3;
   const int ntn = (p.nrhs + 7) / 8;
+  const bool pre = p.Y != nullptr;
+  const int S = p.strips, hs = p.hs, target = p.strips * p.epoch;
   if (p.status != nullptr && ((volatile DevStatus*)p.status)->code != 0) return;
-  for (int s = blockIdx.x; s < p.nblk; s += gridDim.x) {
+  for (int task = blockIdx.x; task < p.nblk * S; task += gridDim.x) {
+    const int s = task / S, q = task - s * S;
     const int r = ts_block(p, s);
-    const int r0 = r * p.nb, mr = min(p.nb, p.n - r0);
+    const int rb0 = r * p.nb, mb = min(p.nb, p.n - rb0);  // the block row
+    const int r0 = rb0 + q * hs, mr = min(hs, mb - q * hs);  // this task's strip of it (may be empty)
     double acc[8][4];
-    // acc = B_r
 #pragma unroll
     for (int nt = 0; nt < 8; ++nt)
 #pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const int row = 16 * warp + g + ((q >= 2) ? 8 : 0), col = 8 * nt + 2 * t + (q & 1);
-        acc[nt][q] = (nt < ntn && row < mr && col < p.nrhs) ? __ldcg(&p.X[(r0 + row) + (long long)col * p.ldx]) : 0.0;
-      }
-    // acc -= T(r, j) X_j for the blocks j solved before r
-    for (int sj = 0; sj < s; ++sj) {
-      const int j = ts_block(p, sj);
-      const int j0 = j * p.nb, mj = min(p.nb, p.n - j0);
-      const double* G = p.amode == 0 ? p.L + r0 + (long long)j0 * p.lda   // A(r, j)
-                                     : p.L + j0 + (long long)r0 * p.lda;  // A(j, r)^T
-      if (!ts_product(acc, -1.0, sm, G, p.lda, p.amode, mr, mj, p.X + j0, p.ldx, p.nrhs, false, &p.flags[j], p.epoch,
-                      p.status))
-        return;
-    }
-    if (p.Y != nullptr) {
-      // prescaled form: publish z_r = acc first (the others need only z), then Y_r = inv(T_rr) z_r
+      for (int e = 0; e < 4; ++e) acc[nt][e] = 0.0;
+    if (mr > 0) {
+      // acc = B(strip)
 #pragma unroll
       for (int nt = 0; nt < 8; ++nt)
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
-          const int row = 16 * warp + g + ((q >= 2) ? 8 : 0), col = 8 * nt + 2 * t + (q & 1);
-          if (nt < ntn && row < mr && col < p.nrhs) p.X[(r0 + row) + (long long)col * p.ldx] = acc[nt][q];
+        for (int e = 0; e < 4; ++e) {
+          const int row = 16 * warp + g + ((e >= 2) ? 8 : 0), col = 8 * nt + 2 * t + (e & 1);
+          if (nt < ntn && row < mr && col < p.nrhs) acc[nt][e] = __ldcg(&p.X[(r0 + row) + (long long)col * p.ldx]);
         }
-      __threadfence();
-      __syncthreads();
-      if (tid == 0) asm volatile("st.release.gpu.global.s32 [%0], %1;" ::"l"(&p.flags[r]), "r"(p.epoch) : "memory");
+      // acc -= T(strip, j) X_j for the blocks j solved before r
+      for (int sj = 0; sj < s; ++sj) {
+        const int j = ts_block(p, sj);
+        const int j0 = j * p.nb, mj = min(p.nb, p.n - j0);
+        const double* G = p.amode == 0 ? p.L + r0 + (long long)j0 * p.lda   // A(strip, j)
+                                       : p.L + j0 + (long long)r0 * p.lda;  // A(j, strip)^T
+        if (!ts_product(acc, -1.0, sm, G, p.lda, p.amode, mr, mj, p.X + j0, p.ldx, p.nrhs, false, &p.flags[j], target,
+                        p.status))
+          return;
+      }
     }
-    // inv(T_rr) acc  (amode 1: inv(A_rr)^T = Winv_r^T)
+    if (pre) {
+      // prescaled form: publish the strip of z_r = acc first (the others need only z) ...
+      if (mr > 0)
 #pragma unroll
-    for (int nt = 0; nt < 8; ++nt)
+        for (int nt = 0; nt < 8; ++nt)
 #pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const int row = 16 * warp + g + ((q >= 2) ? 8 : 0), col = 8 * nt + 2 * t + (q & 1);
-        if (nt < ntn) accS[row + col * kTsAccLD] = acc[nt][q];
-        acc[nt][q] = 0.0;
-      }
-    __syncthreads();
-    const double* Wr = p.Winv + (long long)r * p.nb * p.nb;
-    ts_product(acc, 1.0, sm, Wr, p.nb, p.amode, mr, mr, accS, kTsAccLD, p.nrhs, true);
-    double* out = p.Y != nullptr ? p.Y : p.X;
-#pragma unroll
-    for (int nt = 0; nt < 8; ++nt)
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const int row = 16 * warp + g + ((q >= 2) ? 8 : 0), col = 8 * nt + 2 * t + (q & 1);
-        if (nt < ntn && row < mr && col < p.nrhs) out[(r0 + row) + (long long)col * p.ldx] = acc[nt][q];
-      }
-    if (p.Y == nullptr) {
+          for (int e = 0; e < 4; ++e) {
+            const int row = 16 * warp + g + ((e >= 2) ? 8 : 0), col = 8 * nt + 2 * t + (e & 1);
+            if (nt < ntn && row < mr && col < p.nrhs) p.X[(r0 + row) + (long long)col * p.ldx] = acc[nt][e];
+          }
       __threadfence();
       __syncthreads();
-      if (tid == 0) asm volatile("st.release.gpu.global.s32 [%0], %1;" ::"l"(&p.flags[r]), "r"(p.epoch) : "memory");
+      if (tid == 0) asm volatile("red.release.gpu.global.add.s32 [%0], 1;" ::"l"(&p.flags[r]) : "memory");
+      if (mr <= 0) continue;
+      // ... then Y(strip) = inv(T_rr)(strip rows, :) z_r once every strip of z_r is out
+#pragma unroll
+      for (int nt = 0; nt < 8; ++nt)
+#pragma unroll
+        for (int e = 0; e < 4; ++e) acc[nt][e] = 0.0;
+      const double* Wr = p.Winv + (long long)r * p.nb * p.nb;
+      const double* G = p.amode == 0 ? Wr + q * hs : Wr + (long long)q * hs * p.nb;
+      if (!ts_product(acc, 1.0, sm, G, p.nb, p.amode, mr, mb, p.X + rb0, p.ldx, p.nrhs, false, &p.flags[r], target,
+                      p.status))
+        return;
+    } else {
+      // X_r = inv(T_rr) acc (one strip per block: the whole accumulator is in this CTA)
+#pragma unroll
+      for (int nt = 0; nt < 8; ++nt)
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          const int row = 16 * warp + g + ((e >= 2) ? 8 : 0), col = 8 * nt + 2 * t + (e & 1);
+          if (nt < ntn) accS[row + col * kTsLD] = acc[nt][e];
+          acc[nt][e] = 0.0;
+        }
+      __syncthreads();
+      const double* Wr = p.Winv + (long long)r * p.nb * p.nb;
+      ts_product(acc, 1.0, sm, Wr, p.nb, p.amode, mr, mr, accS, kTsLD, p.nrhs, true);
+    }
+    double* out = pre ? p.Y : p.X;
+#pragma unroll
+    for (int nt = 0; nt < 8; ++nt)
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const int row = 16 * warp + g + ((e >= 2) ? 8 : 0), col = 8 * nt + 2 * t + (e & 1);
+        if (nt < ntn && row < mr && col < p.nrhs) out[(r0 + row) + (long long)col * p.ldx] = acc[nt][e];
+      }
+    if (!pre) {
+      __threadfence();
+      __syncthreads();
+      if (tid == 0) asm volatile("red.release.gpu.global.add.s32 [%0], 1;" ::"l"(&p.flags[r]) : "memory");
     }
   }
 }
 
 size_t trsm_skinny_flag_bytes(int n, int nb) { return sizeof(int) * (size_t)((n + nb - 1) / nb) + 256; }
 
-// flags: device array of ceil(n/nb) ints that persists across calls; epoch
-// must differ from every value the flags hold (the caller counts calls).
+// flags: device array of ceil(n/nb) arrival counters, zero before the first
+// sweep of a sequence; sweep number `epoch` (1, 2, ...) of the sequence
+// waits for counters to reach strips x epoch.
 int launch_trsm_skinny(cudaStream_t st, int bwd, int amode, int n, int nrhs, const double* L, long long lda,
                        const double* Winv, int nb, double* X, long long ldx, int* flags, int epoch, int sm_count,
                        DevStatus* status, double* Y) {
@@ -288,6 +316,10 @@ int launch_trsm_skinny(cudaStream_t st, int bwd, int amode, int n, int nrhs, con
   TsParams p;
   p.L = L; p.lda = lda; p.Winv = Winv; p.X = X; p.ldx = ldx; p.Y = Y;
   p.n = n; p.nrhs = nrhs; p.nb = nb; p.nblk = (n + nb - 1) / nb; p.bwd = bwd; p.amode = amode;
+  // prescaled form: two strips per block row, so the dependency chain's product is half a block,
+  // when every strip still gets a CTA of its own (a CTA that holds two tasks starts its second late)
+  p.strips = (Y != nullptr && nb >= 32 && 2 * ((n + nb - 1) / nb) <= sm_count) ? 2 : 1;
+  p.hs = p.strips == 1 ? nb : ((nb + 1) / 2 + 15) / 16 * 16;
   p.flags = flags; p.epoch = epoch; p.status = status;
   const size_t smem = sizeof(double) * kTsSmemDoubles;
   static bool attr = false;
@@ -299,7 +331,7 @@ int launch_trsm_skinny(cudaStream_t st, int bwd, int amode, int n, int nrhs, con
     }
     attr = true;
   }
-  const int grid = std::min(p.nblk, sm_count);
+  const int grid = std::min(p.nblk * p.strips, sm_count);
   TraceMark tm(st, kTraceSolve, (double)n * n * nrhs, 4.0 * (double)n * n + 16.0 * n * nrhs);
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(grid);
