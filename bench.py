@@ -881,6 +881,12 @@ def kernel_case(args):
             del g, spd
         print(json.dumps(out))
         return
+    elif args.case == "mixed":
+        # one mixed-precision HPD solve (kappa 1e6, 32 RHS) at order --n
+        A = inputs.spd_spectrum_torch(n, 1e6, 7, "cuda")
+        B = torch.randn(32, n, dtype=torch.float64, device="cuda").t()
+        X, it, be = h.hpd_solve_mixed(A, B)
+        assert be <= 1e-14
     elif args.case == "diag":
         A = eg.colmajor_cuda(inputs.spd_ggt(NB, 1))
         h.cholesky(A, eg.LOWER)
@@ -896,7 +902,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="mixed", choices=sorted(WORKLOADS), help="benchmark configuration")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline leg")
-    ap.add_argument("--case", choices=["update", "gemm", "panel", "diag", "peaks"], default=None,
+    ap.add_argument("--case", choices=["update", "gemm", "panel", "diag", "peaks", "mixed"], default=None,
                     help="run one launch of one kernel class (profiling)")
     ap.add_argument("--n", type=int, default=6144, help="size for --case")
     args = ap.parse_args()

@@ -116,6 +116,7 @@ def _declare(L):
         "egpu_dposv_mixed": ([H, I, I, I, P, I, P, I, P, I, I, D, P, P], I),
         "egpu_tc_gemm_split": ([H, I, I, I, D, P, I, P, I, D, P, I, I, I], I),
         "egpu_host_dposv_mixed": ([H, I, I, I, P, I, P, I, P, I, I, D, P, P], I),
+        "egpu_mixed_gmres_iterations": ([H], I),
         "egpu_batch_plan_create": ([H, I, I, P, P, P, P, P, P, P], I),
         "egpu_batch_plan_run": ([P, P], I),
         "egpu_batch_plan_info": ([P, P, P], I),
@@ -124,6 +125,7 @@ def _declare(L):
         "egpu_batch_plan_destroy": ([P], I),
         "egpu_server_create": ([I, ctypes.c_size_t, I, I, P], I),
         "egpu_server_set_tolerance": ([P, D], I),
+        "egpu_server_set_mixed_min_n": ([P, I], I),
         "egpu_server_submit": ([P, I, I, I, P, I, P, I, P, I, P], I),
         "egpu_server_query": ([P, ctypes.c_ulonglong, I, P, P, P, P, P, P], I),
         "egpu_server_release": ([P, ctypes.c_ulonglong], I),
@@ -222,10 +224,12 @@ class Server:
 
     HPD, GE = 0, 1
 
-    def __init__(self, device=0, hbm_budget_bytes=150 << 30, slots=4, mode=0, tol=1e-14):
+    def __init__(self, device=0, hbm_budget_bytes=150 << 30, slots=4, mode=0, tol=1e-14, mixed_min_n=None):
         self._s = ctypes.c_void_p()
         _check(lib().egpu_server_create(device, hbm_budget_bytes, slots, mode, ctypes.byref(self._s)))
         _check(lib().egpu_server_set_tolerance(self._s, tol))
+        if mixed_min_n is not None:
+            _check(lib().egpu_server_set_mixed_min_n(self._s, mixed_min_n))
         self._keep = {}
 
     def submit(self, kind, A, B, X):
@@ -533,6 +537,10 @@ class Handle:
             raise ElemGPUError(f"refinement did not reach {tol:g} in {it.value} corrections (berr {be.value:.3e})")
         _check(rc)
         return X, it.value, be.value
+
+    def mixed_gmres_iterations(self):
+        """GMRES iterations of the last mixed solve (0 when plain refinement converged)."""
+        return lib().egpu_mixed_gmres_iterations(self._h)
 
     def tc_gemm_split(self, A, B, C, alpha=1.0, beta=0.0, lower=False, terms=3):
         """C (float32, column-major) = alpha A B^T + beta C on the tcgen05 tensor cores

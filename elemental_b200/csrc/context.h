@@ -68,6 +68,7 @@ struct egpu_context {
   cudaEvent_t ev_panel[2] = {nullptr, nullptr}, ev_rest[2] = {nullptr, nullptr};
   int lookahead = 1;
   int async = 0;  // device API: enqueue only; status read by egpu_get_status
+  int gmres_inner = 0;  // GMRES iterations of the last mixed solve
 };
 
 struct DeviceGuard {

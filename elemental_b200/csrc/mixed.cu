@@ -121,6 +121,43 @@ __global__ void copy_cols_kernel(int n, int ncols, const double* X, long long ld
   }
 }
 
+// out[j * nrhs + c] = sum_i V_j[i, c] W[i, c] for j < nv (V_j = V + j * vstride); one block per (j, c)
+__global__ void block_dots_kernel(int n, const double* V, long long ldv, long long vstride, const double* W,
+                                  long long ldw, double* out, int nrhs) {
+  const int j = blockIdx.x, c = blockIdx.y;
+  const double* v = V + j * vstride + (long long)c * ldv;
+  const double* w = W + (long long)c * ldw;
+  double s = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) s = fma(v[i], w[i], s);
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  __shared__ double red[32];
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    s = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (threadIdx.x == 0) out[j * nrhs + c] = s;
+  }
+}
+
+// W[:, c] -= sum_{j < nv} coef[j * nrhs + c] V_j[:, c]
+__global__ void block_axpy_kernel(int n, int nv, const double* V, long long ldv, long long vstride,
+                                  const double* coef, double* W, long long ldw, int nrhs) {
+  const int c = blockIdx.y;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    double acc = 0.0;
+    for (int j = 0; j < nv; ++j) acc = fma(coef[j * nrhs + c], V[j * vstride + (long long)c * ldv + i], acc);
+    W[(long long)c * ldw + i] -= acc;
+  }
+}
+
+// Y[:, c] = s[c] X[:, c]
+__global__ void col_scale_kernel(int n, const double* X, long long ldx, const double* s, double* Y, long long ldy) {
+  const int c = blockIdx.y;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    Y[(long long)c * ldy + i] = s[c] * X[(long long)c * ldx + i];
+}
+
 }  // namespace
 
 int launch_split_tf32(cudaStream_t st, int rows, int cols, const double* X, long long ldx, float* hi, float* lo,
@@ -133,9 +170,11 @@ int launch_split_tf32(cudaStream_t st, int rows, int cols, const double* X, long
   return EGPU_OK;
 }
 
+constexpr int kGmresRestart = 20;  // Krylov vectors per GMRES cycle
+
 // Workspace layout of the mixed solve.
 struct MixedLayout {
-  size_t as, af, lf, m2, m3, w, pkh, pkl, xw, r, yt, winv, norms, flags, total;
+  size_t as, af, lf, m2, m3, w, pkh, pkl, xw, r, yt, winv, norms, flags, gv, gw, gc, total;
   long long lds, ldf, ldk;
 };
 
@@ -160,6 +199,9 @@ static MixedLayout mixed_layout(int n, int nrhs, int nb) {
   L.winv = take(winv_bytes(n, nb));
   L.norms = take(sizeof(double) * ((size_t)n + 4 * (size_t)std::max(nrhs, 1)));
   L.flags = take(trsm_skinny_flag_bytes(n, nb));
+  L.gv = take(sizeof(double) * L.lds * std::max(nrhs, 1) * (kGmresRestart + 1));  // GMRES basis
+  L.gw = take(sizeof(double) * L.lds * std::max(nrhs, 1));                        // GMRES work vector
+  L.gc = take(sizeof(double) * (size_t)std::max(nrhs, 1) * (kGmresRestart + 2));  // coefficients
   L.total = (off + 4095) & ~size_t(4095);
   return L;
 }
@@ -225,11 +267,138 @@ static int mixed_berr(egpu_context* h, int n, int nrhs, const double* R, const d
   return EGPU_OK;
 }
 
+// GMRES-IR correction: solve A d = r with GMRES left-preconditioned by the
+// low-precision factor (M = Lf Lf^T applied by mixed_solve), FP64 everywhere
+// else, one Krylov basis per right-hand side advanced in lockstep; classical
+// Gram-Schmidt applied twice, Givens rotations on the host.  Stops when every
+// column's preconditioned residual fell below inner_tol times its start, or
+// after kGmresRestart vectors.  R is consumed; D receives the correction.
+struct GmresWork {
+  double* V;      // kGmresRestart + 1 basis blocks of lds x nrhs
+  double* W;      // work block
+  double* coef;   // (kGmresRestart + 2) x nrhs device coefficients
+  double* dots;   // device scratch for dot products ((kGmresRestart + 1) x nrhs)
+};
+static int gmres_correction(egpu_context* h, int n, int nrhs, const double* As, long long lds, const double* Lf,
+                            const double* Winv, SweepFlags& fl, double* R, double* D, GmresWork& gw,
+                            double inner_tol, int* inner_iters) {
+  cudaStream_t st = h->stream;
+  const long long vs = lds * nrhs;  // stride between basis blocks
+  const int m = kGmresRestart;
+  dim3 vgrid((n + 255) / 256, nrhs);
+  auto dots = [&](int nv, const double* W, std::vector<double>& out) -> int {  // out[j*nrhs+c] = <V_j, W>
+    block_dots_kernel<<<dim3(nv, nrhs), 256, 0, st>>>(n, gw.V, lds, vs, W, lds, gw.dots, nrhs);
+    count_launch();
+    EGPU_CUDA_TRY(cudaGetLastError());
+    out.resize((size_t)nv * nrhs);
+    EGPU_CUDA_TRY(cudaMemcpyAsync(out.data(), gw.dots, sizeof(double) * nv * nrhs, cudaMemcpyDeviceToHost, st));
+    EGPU_CUDA_TRY(cudaStreamSynchronize(st));
+    return EGPU_OK;
+  };
+  auto self_norms = [&](const double* W, std::vector<double>& out) -> int {  // ||W[:, c]||
+    block_dots_kernel<<<dim3(1, nrhs), 256, 0, st>>>(n, W, lds, 0, W, lds, gw.dots, nrhs);
+    count_launch();
+    EGPU_CUDA_TRY(cudaGetLastError());
+    out.resize(nrhs);
+    EGPU_CUDA_TRY(cudaMemcpyAsync(out.data(), gw.dots, sizeof(double) * nrhs, cudaMemcpyDeviceToHost, st));
+    EGPU_CUDA_TRY(cudaStreamSynchronize(st));
+    for (double& v : out) v = std::sqrt(std::max(v, 0.0));
+    return EGPU_OK;
+  };
+  auto scale_into = [&](const double* X, const std::vector<double>& s, double* Y) -> int {
+    EGPU_CUDA_TRY(cudaMemcpyAsync(gw.coef, s.data(), sizeof(double) * nrhs, cudaMemcpyHostToDevice, st));
+    col_scale_kernel<<<vgrid, 256, 0, st>>>(n, X, lds, gw.coef, Y, lds);
+    count_launch();
+    EGPU_CUDA_TRY(cudaGetLastError());
+    return EGPU_OK;
+  };
+  auto axpy = [&](int nv, const std::vector<double>& c, double* W) -> int {  // W -= sum_j c_j V_j
+    EGPU_CUDA_TRY(cudaMemcpyAsync(gw.coef, c.data(), sizeof(double) * nv * nrhs, cudaMemcpyHostToDevice, st));
+    block_axpy_kernel<<<vgrid, 256, 0, st>>>(n, nv, gw.V, lds, vs, gw.coef, W, lds, nrhs);
+    count_launch();
+    EGPU_CUDA_TRY(cudaGetLastError());
+    return EGPU_OK;
+  };
+  // z = M^-1 r, beta = ||z||, V_0 = z / beta
+  TRY(mixed_solve(h, n, nrhs, Lf, lds, Winv, R, fl));
+  std::vector<double> beta, inv(nrhs), hv, nrm;
+  TRY(self_norms(R, beta));
+  for (int c = 0; c < nrhs; ++c) inv[c] = beta[c] > 0.0 ? 1.0 / beta[c] : 0.0;
+  TRY(scale_into(R, inv, gw.V));
+  // per column: Hessenberg (column-major (m+1) x m), rotations, rhs g
+  std::vector<double> H((size_t)nrhs * (m + 1) * m, 0.0), cs((size_t)nrhs * m), sn((size_t)nrhs * m),
+      g((size_t)nrhs * (m + 1), 0.0);
+  auto Hc = [&](int c, int i, int j) -> double& { return H[((size_t)c * m + j) * (m + 1) + i]; };
+  for (int c = 0; c < nrhs; ++c) g[(size_t)c * (m + 1)] = beta[c];
+  int k = 0;
+  for (int i = 0; i < m; ++i) {
+    double* Vi = gw.V + i * vs;
+    // W = M^-1 A V_i
+    EGPU_CUDA_TRY(cudaMemsetAsync(gw.W, 0, sizeof(double) * vs, st));
+    int rg = launch_dgemm_skinny(st, n, nrhs, n, 1.0, As, lds, Vi, lds, gw.W, lds, h->sm_count, h->dstatus);
+    if (rg == EGPU_ERR_UNSUPPORTED)
+      rg = launch_dgemm(st, false, true, n, nrhs, n, 1.0, As, lds, Vi, lds, 0.0, gw.W, lds, 0, false, h->dstatus);
+    TRY(rg);
+    TRY(mixed_solve(h, n, nrhs, Lf, lds, Winv, gw.W, fl));
+    for (int pass = 0; pass < 2; ++pass) {  // classical Gram-Schmidt, twice
+      TRY(dots(i + 1, gw.W, hv));
+      TRY(axpy(i + 1, hv, gw.W));
+      for (int c = 0; c < nrhs; ++c)
+        for (int j = 0; j <= i; ++j) Hc(c, j, i) += hv[(size_t)j * nrhs + c];
+    }
+    TRY(self_norms(gw.W, nrm));
+    for (int c = 0; c < nrhs; ++c) {
+      Hc(c, i + 1, i) = nrm[c];
+      inv[c] = nrm[c] > 0.0 ? 1.0 / nrm[c] : 0.0;
+    }
+    TRY(scale_into(gw.W, inv, gw.V + (i + 1) * vs));
+    bool done = true;
+    for (int c = 0; c < nrhs; ++c) {
+      double* cc = &cs[(size_t)c * m];
+      double* ss = &sn[(size_t)c * m];
+      double* gg = &g[(size_t)c * (m + 1)];
+      for (int j = 0; j < i; ++j) {  // earlier rotations on the new column
+        const double a = Hc(c, j, i), b = Hc(c, j + 1, i);
+        Hc(c, j, i) = cc[j] * a + ss[j] * b;
+        Hc(c, j + 1, i) = -ss[j] * a + cc[j] * b;
+      }
+      const double a = Hc(c, i, i), b = Hc(c, i + 1, i);
+      const double rr = std::hypot(a, b);
+      cc[i] = rr > 0.0 ? a / rr : 1.0;
+      ss[i] = rr > 0.0 ? b / rr : 0.0;
+      Hc(c, i, i) = rr;
+      Hc(c, i + 1, i) = 0.0;
+      gg[i + 1] = -ss[i] * gg[i];
+      gg[i] = cc[i] * gg[i];
+      if (beta[c] > 0.0 && std::fabs(gg[i + 1]) > inner_tol * beta[c]) done = false;
+    }
+    k = i + 1;
+    if (done) break;
+  }
+  // y = H(0:k, 0:k)^-1 g(0:k) per column; D = sum_j y_j V_j
+  std::vector<double> y((size_t)k * nrhs, 0.0);
+  for (int c = 0; c < nrhs; ++c) {
+    const double* gg = &g[(size_t)c * (m + 1)];
+    for (int j = k - 1; j >= 0; --j) {
+      double s = gg[j];
+      for (int l = j + 1; l < k; ++l) s -= Hc(c, j, l) * y[(size_t)l * nrhs + c];
+      const double d = Hc(c, j, j);
+      y[(size_t)j * nrhs + c] = d != 0.0 ? s / d : 0.0;
+    }
+  }
+  for (double& v : y) v = -v;  // axpy subtracts
+  EGPU_CUDA_TRY(cudaMemsetAsync(D, 0, sizeof(double) * vs, st));
+  TRY(axpy(k, y, D));
+  if (inner_iters) *inner_iters += k;
+  return EGPU_OK;
+}
+
 int dposv_mixed_core_impl(egpu_context* h, int uplo, int n, int nrhs, const double* A, long long lda, const double* B,
                      long long ldb, double* X, long long ldx, int max_iter, double tol, int* iters, double* berr) {
   const int nb = h->nb;
   cudaStream_t st = h->stream;
   const MixedLayout L = mixed_layout(n, nrhs, nb);
+  h->gmres_inner = 0;
   TRY(ensure_ws(h, L.total + 4096));
   unsigned char* ws = static_cast<unsigned char*>(h->ws);
   double* As = reinterpret_cast<double*>(ws + L.as);
@@ -330,6 +499,7 @@ int dposv_mixed_core_impl(egpu_context* h, int uplo, int n, int nrhs, const doub
   TRY(mixed_solve(h, n, nrhs, Lf, lds, Winv, Xw, fl));
   int it = 0;
   double e = INFINITY, e_prev = INFINITY;
+  h->gmres_inner = 0;
   for (;;) {
     copy_cols_kernel<<<cgrid, 256, 0, st>>>(n, nrhs, B, ldb, R, lds, 0);
     count_launch();
@@ -339,12 +509,37 @@ int dposv_mixed_core_impl(egpu_context* h, int uplo, int n, int nrhs, const doub
     TRY(rg);
     TRY(mixed_berr(h, n, nrhs, R, Xw, B, ldb, lds, anorm, norms + n, &e));
     if (e <= tol || it >= max_iter || !std::isfinite(e)) break;
-    if (it >= 2 && e > 0.9 * e_prev) break;  // stagnation: the factor is too far from A
+    // slow contraction (the factor is too far from A): continue with GMRES-IR below
+    if (it >= 2 && e > 0.25 * e_prev) break;
     e_prev = e;
     TRY(mixed_solve(h, n, nrhs, Lf, lds, Winv, R, fl));
     copy_cols_kernel<<<cgrid, 256, 0, st>>>(n, nrhs, R, lds, Xw, lds, 1);
     count_launch();
     ++it;
+  }
+  // GMRES-IR when plain refinement contracts slowly (the factor is good enough
+  // to precondition but too far from A to contract): R holds the residual of Xw
+  if (e > tol && std::isfinite(e) && it < max_iter) {
+    GmresWork gw{reinterpret_cast<double*>(ws + L.gv), reinterpret_cast<double*>(ws + L.gw),
+                 reinterpret_cast<double*>(ws + L.gc), reinterpret_cast<double*>(ws + L.gc) + nrhs};
+    int inner = 0;
+    double e_best = e;
+    while (it < max_iter) {
+      TRY(gmres_correction(h, n, nrhs, As, lds, Lf, Winv, fl, R, R, gw, 1e-10, &inner));
+      copy_cols_kernel<<<cgrid, 256, 0, st>>>(n, nrhs, R, lds, Xw, lds, 1);
+      count_launch();
+      ++it;
+      copy_cols_kernel<<<cgrid, 256, 0, st>>>(n, nrhs, B, ldb, R, lds, 0);
+      count_launch();
+      int rg = launch_dgemm_skinny(st, n, nrhs, n, -1.0, As, lds, Xw, lds, R, lds, h->sm_count, h->dstatus);
+      if (rg == EGPU_ERR_UNSUPPORTED)
+        rg = launch_dgemm(st, false, true, n, nrhs, n, -1.0, As, lds, Xw, lds, 1.0, R, lds, 0, false, h->dstatus);
+      TRY(rg);
+      TRY(mixed_berr(h, n, nrhs, R, Xw, B, ldb, lds, anorm, norms + n, &e));
+      if (e <= tol || !std::isfinite(e) || e > 0.9 * e_best) break;
+      e_best = e;
+    }
+    h->gmres_inner = inner;
   }
   copy_cols_kernel<<<cgrid, 256, 0, st>>>(n, nrhs, Xw, lds, X, ldx, 0);
   count_launch();
@@ -370,6 +565,8 @@ extern "C" int egpu_dposv_mixed(egpu_handle h, int uplo, int n, int nrhs, const 
   Enter en(h);
   return egpu::dposv_mixed_core_impl(h, uplo, n, nrhs, dA, lda, dB, ldb, dX, ldx, max_iter, tol, iters, berr);
 }
+
+extern "C" int egpu_mixed_gmres_iterations(egpu_handle h) { return h ? h->gmres_inner : -1; }
 
 // Testing entry for the tcgen05 engine: C (FP32) = alpha A B^T + beta C with
 // A (M x K) and B (N x K) given column-major in FP64 and split into TF32 parts.

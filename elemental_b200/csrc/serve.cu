@@ -8,10 +8,11 @@
 // overlaps on the device.  When a worker frees up, every queued small
 // request (n <= 512, nrhs <= 16) of the kind at the head of the queue is
 // taken as one job and solved in one batched launch; a larger request is a
-// job of its own.  Mode 1 solves HPD requests with the mixed-precision
-// solver (egpu_dposv_mixed) and falls back to the FP64 path for a request it
-// cannot bring to the tolerance; GE requests always take the FP64 path
-// (egpu_dgesv).  Completion times are recorded per request (latency =
+// job of its own.  Mode 1 solves HPD requests of order >= mixed_min_n with
+// the mixed-precision solver (egpu_dposv_mixed) and falls back to the FP64
+// path for a request it cannot bring to the tolerance; smaller HPD requests
+// (where the FP64 path is faster on this hardware) and GE requests take the
+// FP64 path (egpu_dgesv).  Completion times are recorded per request (latency =
 // completion - submission, host steady clock).
 #include <chrono>
 #include <condition_variable>
@@ -58,6 +59,7 @@ struct egpu_server_s {
   int device = 0, slots = 1, mode = 0;
   size_t budget = 0, in_use = 0;
   double tol = 1e-14;
+  int mixed_min_n = 10240;  // mode 1: smaller HPD requests take the FP64 path (faster there)
   std::mutex mu;
   std::condition_variable cv_dispatch, cv_done;
   std::deque<Request*> queue;
@@ -160,7 +162,7 @@ void run_job(egpu_server_s* s, egpu_server_s::Worker* w, std::vector<Request*>& 
                     cudaMemcpyHostToDevice, st);
   int rc, info = 0;
   double* sol = dB;
-  if (r->kind == 0 && s->mode == 1) {
+  if (r->kind == 0 && s->mode == 1 && n >= s->mixed_min_n) {
     rc = egpu_dposv_mixed(h, EGPU_LOWER, n, r->nrhs, dA, ldd, dB, ldd, dX, ldd, 30, s->tol, &r->iters, &r->berr);
     r->path = 1;
     sol = dX;
@@ -295,6 +297,13 @@ int egpu_server_create(int device, size_t hbm_budget_bytes, int slots, int mode,
   for (auto* w : s->workers) w->th = std::thread(worker_main, s, w);
   s->dispatcher = std::thread(dispatcher_main, s);
   *out = s;
+  return EGPU_OK;
+}
+
+int egpu_server_set_mixed_min_n(egpu_server s, int n) {
+  if (!s || n < 0) return EGPU_ERR_ARG;
+  std::lock_guard<std::mutex> lk(s->mu);
+  s->mixed_min_n = n;
   return EGPU_OK;
 }
 

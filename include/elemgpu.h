@@ -175,8 +175,8 @@ EGPU_API int egpu_batch_plan_destroy(egpu_batch_plan plan);
  * each with its own handle and stream, so up to `slots` jobs run at once;
  * all queued small requests (n <= 512, nrhs <= 16) of the kind at the head of
  * the queue form one batched job.  mode 0: FP64 solves; mode 1: HPD requests
- * take egpu_dposv_mixed (FP64 fallback when it cannot reach the tolerance),
- * GE requests stay FP64.  kind 0 = HPDSolve(LOWER) (A lower triangle read),
+ * of order >= the mixed threshold take egpu_dposv_mixed (FP64 fallback when
+ * it cannot reach the tolerance), the rest stay FP64.  kind 0 = HPDSolve(LOWER) (A lower triangle read),
  * kind 1 = GaussianElimination.  A, B, X are host buffers (pinned for
  * speed) that must stay valid until the request completes; A and B are not
  * modified, X receives the solution.  The per-slot handle workspaces are
@@ -184,6 +184,9 @@ EGPU_API int egpu_batch_plan_destroy(egpu_batch_plan plan);
 typedef struct egpu_server_s* egpu_server;
 EGPU_API int egpu_server_create(int device, size_t hbm_budget_bytes, int slots, int mode, egpu_server* out);
 EGPU_API int egpu_server_set_tolerance(egpu_server s, double tol);
+/* Mode 1 sends HPD requests of order >= n to the mixed solver (default
+ * 10240: below it the FP64 path is the faster one on B200). */
+EGPU_API int egpu_server_set_mixed_min_n(egpu_server s, int n);
 EGPU_API int egpu_server_submit(egpu_server s, int kind, int n, int nrhs, const double* A, int lda,
                                 const double* B, int ldb, double* X, int ldx, unsigned long long* id);
 /* *done = 0 while queued or running; once done: *status (EGPU_* code),
@@ -210,6 +213,14 @@ EGPU_API int egpu_server_destroy(egpu_server s);
 EGPU_API int egpu_dposv_mixed(egpu_handle h, int uplo, int n, int nrhs, const double* dA, int lda,
                               const double* dB, int ldb, double* dX, int ldx, int max_iter, double tol,
                               int* iters, double* berr);
+
+/* GMRES iterations spent by the handle's last mixed solve: when plain
+ * refinement stagnates (the low-precision factor is too far from A to
+ * contract, typically kappa >~ 1e7), egpu_dposv_mixed continues with GMRES-IR
+ * (GMRES on M^-1 A d = M^-1 r, M the low-precision factor, FP64 residuals and
+ * Krylov vectors, 20 vectors per cycle, one cycle per correction); its
+ * corrections count in *iters. */
+EGPU_API int egpu_mixed_gmres_iterations(egpu_handle h);
 
 /* Host-memory form of egpu_dposv_mixed (A, B, X in host memory). */
 EGPU_API int egpu_host_dposv_mixed(egpu_handle h, int uplo, int n, int nrhs, const double* A, int lda,

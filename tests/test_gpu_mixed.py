@@ -105,3 +105,16 @@ def test_host_hpd_solve_mixed_matches_device():
     # both at backward error <= 1e-14: forward errors within kappa * 1e-14 of each other
     assert np.abs(X - Xd.cpu().numpy()).max() <= 1e5 * 1e-14 * np.abs(X).max()
     h.close()
+
+
+@pytest.mark.parametrize("kappa", [1e8, 1e9])
+def test_hpd_solve_mixed_gmres_ir(handle, kappa):
+    """Beyond kappa ~ 1e7 the TF32x3 factor no longer contracts plain
+    refinement quickly; GMRES-IR preconditioned by it reaches 1e-14."""
+    n, nrhs = 1024, 4
+    A = inputs.spd_spectrum(n, kappa, 61)
+    B = inputs.normal(n, nrhs, 62)
+    X, it, be = handle.hpd_solve_mixed(eg.colmajor_cuda(A), eg.colmajor_cuda(B))
+    assert be <= 1e-14
+    assert _berr(A, X.cpu().numpy(), B) <= 1e-14
+    assert handle.mixed_gmres_iterations() > 0

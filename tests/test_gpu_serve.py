@@ -74,7 +74,7 @@ def test_server_budget_admission():
 
 
 def test_server_mixed_mode_and_fallback():
-    srv = eg.Server(0, hbm_budget_bytes=8 << 30, slots=2, mode=1)
+    srv = eg.Server(0, hbm_budget_bytes=8 << 30, slots=2, mode=1, mixed_min_n=0)
     good = inputs.spd_spectrum(1024, 1e4, 11)
     hard = inputs.spd_spectrum(1024, 1e12, 12)
     B = inputs.normal(1024, 3, 13)
