@@ -63,6 +63,9 @@ __device__ __forceinline__ void sg_stage(double* sA, double* sB, const SgParams&
 
 }  // namespace
 
+// NT: 8-column tiles of B and C (compile-time: a DMMA skipped under a
+// run-time predicate still costs its issue slots).
+template <int NT>
 __global__ void __launch_bounds__(kSgThreads, 1) dgemm_skinny_kernel(SgParams p) {
   extern __shared__ double sm[];
   if (p.status != nullptr && ((volatile DevStatus*)p.status)->code != 0) return;
@@ -72,10 +75,9 @@ __global__ void __launch_bounds__(kSgThreads, 1) dgemm_skinny_kernel(SgParams p)
   const int kbeg = blockIdx.y * p.kslice, kend = min(p.K, kbeg + p.kslice);
   if (kbeg >= kend) return;
   const int nch = (kend - kbeg + kSgKC - 1) / kSgKC;
-  const int ntn = (p.N + 7) / 8;
-  double acc[8][4];
+  double acc[NT][4];
 #pragma unroll
-  for (int nt = 0; nt < 8; ++nt)
+  for (int nt = 0; nt < NT; ++nt)
 #pragma unroll
     for (int q = 0; q < 4; ++q) acc[nt][q] = 0.0;
   // prologue: stages 0 .. S-2 in flight
@@ -105,22 +107,21 @@ __global__ void __launch_bounds__(kSgThreads, 1) dgemm_skinny_kernel(SgParams p)
       a[2] = sA[ra + (kk + t + 4) * kSgLDA];
       a[3] = sA[ra + 8 + (kk + t + 4) * kSgLDA];
 #pragma unroll
-      for (int nt = 0; nt < 8; ++nt)
-        if (nt < ntn) {
-          double bf[2];
-          bf[0] = sB[(kk + t) + (8 * nt + g) * kSgLDB];
-          bf[1] = sB[(kk + t + 4) + (8 * nt + g) * kSgLDB];
-          dmma_16x8x8(acc[nt], a, bf);
-        }
+      for (int nt = 0; nt < NT; ++nt) {
+        double bf[2];
+        bf[0] = sB[(kk + t) + (8 * nt + g) * kSgLDB];
+        bf[1] = sB[(kk + t + 4) + (8 * nt + g) * kSgLDB];
+        dmma_16x8x8(acc[nt], a, bf);
+      }
     }
   }
   asm volatile("cp.async.wait_group 0;" ::: "memory");
 #pragma unroll
-  for (int nt = 0; nt < 8; ++nt)
+  for (int nt = 0; nt < NT; ++nt)
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
       const int row = m0 + 16 * warp + g + ((q >= 2) ? 8 : 0), col = 8 * nt + 2 * t + (q & 1);
-      if (nt < ntn && row < p.M && col < p.N) atomicAdd(&p.C[row + (long long)col * p.ldc], p.alpha * acc[nt][q]);
+      if (row < p.M && col < p.N) atomicAdd(&p.C[row + (long long)col * p.ldc], p.alpha * acc[nt][q]);
     }
 }
 
@@ -131,14 +132,18 @@ int launch_dgemm_skinny(cudaStream_t st, int M, int N, int K, double alpha, cons
       reinterpret_cast<uintptr_t>(B) % 16)
     return EGPU_ERR_UNSUPPORTED;
   const size_t smem = sizeof(double) * kSgSmemDoubles;
-  static bool attr = false;
-  if (!attr) {
-    if (cudaFuncSetAttribute(dgemm_skinny_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
-        cudaSuccess) {
+  const int nt = N <= 8 ? 1 : N <= 16 ? 2 : N <= 32 ? 4 : 8;
+  const int ai = nt == 1 ? 0 : nt == 2 ? 1 : nt == 4 ? 2 : 3;
+  void (*kern)(SgParams) = nt == 1 ? dgemm_skinny_kernel<1>
+                           : nt == 2 ? dgemm_skinny_kernel<2>
+                           : nt == 4 ? dgemm_skinny_kernel<4> : dgemm_skinny_kernel<8>;
+  static bool attr[4] = {false, false, false, false};
+  if (!attr[ai]) {
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
       cudaGetLastError();
       return EGPU_ERR_UNSUPPORTED;
     }
-    attr = true;
+    attr[ai] = true;
   }
   const int mt = (M + 127) / 128;
   // about four CTAs per SM in total, K slices a multiple of the chunk
@@ -148,7 +153,7 @@ int launch_dgemm_skinny(cudaStream_t st, int M, int N, int K, double alpha, cons
   splits = (K + kslice - 1) / kslice;
   SgParams p{A, lda, B, ldb, C, ldc, M, N, K, kslice, alpha, status};
   TraceMark tm(st, kTraceUpdate, 2.0 * M * N * K, 8.0 * ((double)M * K + (double)K * N * mt + 2.0 * M * N * splits));
-  dgemm_skinny_kernel<<<dim3(mt, splits), kSgThreads, smem, st>>>(p);
+  kern<<<dim3(mt, splits), kSgThreads, smem, st>>>(p);
   count_launch();
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) {

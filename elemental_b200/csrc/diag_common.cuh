@@ -7,8 +7,10 @@ namespace egpu {
 
 // ---------------------------------------------------------------------------
 // Diagonal-block kernels.  The nb x nb block (nb <= 128) lives in shared
-// memory with leading dimension kLDS = 129 (odd: row and column sweeps are
-// both bank-conflict free), always as a LOWER triangle (an upper triangle is
+// memory with leading dimension kLDS = 132 (4 mod 16: the 8-byte DMMA
+// fragment loads, rows g + 8.. x columns t + 4.., hit 16 distinct bank pairs
+// per half warp; even, so every column starts on a 16-byte boundary for
+// 16-byte copies), always as a LOWER triangle (an upper triangle is
 // handled as the lower triangle of its transpose: UVar3Unb and LVar3Unb
 // perform the same operations on A and A^T).
 //
@@ -24,7 +26,7 @@ namespace egpu {
 // X21 = -inv(L22) (L21 X11), with 4x4-blocked mini-GEMMs.
 // All loops are rolled: straight-line unrolled code run by one warp stalls
 // on instruction fetch.
-constexpr int kLDS = 129;
+constexpr int kLDS = 132;
 constexpr int kSP = 16;  // sub-panel width
 constexpr int kDiagSmemBase = (128 * kLDS + 128) * (int)sizeof(double);
 
@@ -211,19 +213,25 @@ __device__ inline void smem_trinv(double* S, int b, int unit) {
 // DMMA building blocks on shared-memory operands (all column-major).
 //
 // C = alpha * A * op(B) + beta * C for M % 16 == 0, N % 8 == 0, K % 8 == 0.
+// The 16 x 8 output tiles go round-robin to warps w_first .. w_first +
+// w_count - 1 (default: all warps); skip_top_left leaves the top-left 16 x 16
+// block of C to someone else.
 // A_LOWER: A[r][k] = 0 for k > r.  B_TRANS: op(B)[k][c] = B[c][k] (B stored
 // N x K).  B_LOWER: op(B)[k][c] = 0 for c > k.  C_LOWER: only r >= c is
 // written.  C must not alias A or B.  All warps of the CTA share the 16x8
 // output tiles; the caller synchronises afterwards.
 template <bool A_LOWER, bool B_TRANS, bool B_LOWER, bool C_LOWER>
 __device__ inline void smem_dmma_gemm(const double* A, int lda, const double* B, int ldb, double* C, int ldc,
-                                      int M, int N, int K, double alpha, double beta) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+                                      int M, int N, int K, double alpha, double beta, int w_first = 0,
+                                      int w_count = -1, bool skip_top_left = false) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int nw = w_count > 0 ? w_count : (blockDim.x >> 5);
   const int g = lane >> 2, t = lane & 3;
   const int tm = M / 16, tn = N / 8;
-  for (int tile = warp; tile < tm * tn; tile += nw) {
+  for (int tile = warp - w_first; tile < tm * tn; tile += nw) {
     const int r0 = (tile % tm) * 16, c0 = (tile / tm) * 8;
     if (C_LOWER && r0 + 15 < c0) continue;
+    if (skip_top_left && r0 < 16 && c0 < 16) continue;  // another warp owns that block
     double acc[4] = {0.0, 0.0, 0.0, 0.0};
     const int kend = A_LOWER ? min(K, r0 + 16) : K;  // A is zero right of its diagonal
     const int kbeg = B_LOWER ? (c0 / 8) * 8 : 0;      // op(B) is zero above its diagonal
@@ -337,20 +345,51 @@ constexpr int kDiagSmem = kDiagSmemBase + kDiagTmpDoubles * (int)sizeof(double);
 // (S(r, c) = G[c + r ld]); consecutive threads always take consecutive
 // global addresses.
 __device__ inline void tri_load_async(double* S, const double* G, long long ld, int b, bool upper) {
-  for (int e = threadIdx.x; e < b * b; e += blockDim.x) {
-    const int i = e % b, j = e / b;  // G row i, column j
-    if (!upper && i >= j) cp_async8(&S[i + j * kLDS], &G[i + (long long)j * ld]);
-    if (upper && j >= i) cp_async8(&S[j + i * kLDS], &G[i + (long long)j * ld]);
+  // a warp per column j, lanes over rows; 16-byte copies when G's columns are
+  // 16-byte aligned (the copy may start one row above the diagonal: S's
+  // strict upper triangle is never read)
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const bool vec = !upper && (ld % 2 == 0) && (reinterpret_cast<uintptr_t>(G) % 16 == 0);
+  for (int j = warp; j < b; j += nw) {
+    const double* g = G + (long long)j * ld;
+    if (vec) {
+      for (int i = (j & ~1) + 2 * lane; i < b; i += 64) {
+        if (i + 1 < b) cp_async16_cg(&S[i + j * kLDS], &g[i]);
+        else cp_async8(&S[i + j * kLDS], &g[i]);
+      }
+    } else if (!upper) {
+      for (int i = j + lane; i < b; i += 32) cp_async8(&S[i + j * kLDS], &g[i]);
+    } else {
+      for (int i = lane; i <= j; i += 32) cp_async8(&S[j + i * kLDS], &g[i]);  // G(i, j), i <= j
+    }
   }
 }
 // Lower triangle of S (r >= c) into G; the other triangle of the b x b block
 // is written as zero when `zero_other`, else left alone.
 __device__ inline void tri_store(const double* S, double* G, long long ld, int b, bool upper, bool zero_other) {
-  for (int e = threadIdx.x; e < b * b; e += blockDim.x) {
-    const int i = e % b, j = e / b;
-    const int r = upper ? j : i, c = upper ? i : j;  // S coordinates
-    if (r >= c) G[i + (long long)j * ld] = S[r + c * kLDS];
-    else if (zero_other) G[i + (long long)j * ld] = 0.0;
+  // a warp per column j of G, lanes over rows i; 16-byte stores when aligned
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const bool vec = !upper && (ld % 2 == 0) && (reinterpret_cast<uintptr_t>(G) % 16 == 0);
+  for (int j = warp; j < b; j += nw) {
+    double* g = G + (long long)j * ld;
+    if (vec) {
+      const double* s = S + j * kLDS;
+      for (int i = (zero_other ? 0 : (j & ~1)) + 2 * lane; i < b; i += 64) {
+        const double v0 = i >= j ? s[i] : 0.0;
+        if (i + 1 < b && (i >= j || zero_other)) {
+          *reinterpret_cast<double2*>(&g[i]) = make_double2(v0, i + 1 >= j ? s[i + 1] : 0.0);
+        } else {
+          if (i >= j || zero_other) g[i] = v0;
+          if (i + 1 < b) g[i + 1] = s[i + 1];  // i + 1 == j: on the diagonal
+        }
+      }
+    } else {
+      for (int i = lane; i < b; i += 32) {
+        const int r = upper ? j : i, c = upper ? i : j;  // S coordinates
+        if (r >= c) g[i] = S[r + c * kLDS];
+        else if (zero_other) g[i] = 0.0;
+      }
+    }
   }
 }
 
@@ -391,42 +430,74 @@ __device__ inline void smem_trinv_dmma(double* S, int bp, const double* Xl, doub
   }
 }
 
-// Lower Cholesky of the bp x bp block in S (bp a multiple of 16; the caller
-// pads with identity) in 16-column steps: warp 0 factors the 16 x 16 diagonal
-// block and inverts it (Xl), all warps form L21 = A21 X11^T and the trailing
-// update A22 -= L21 L21^T on the tensor cores.  Returns 0 or the 1-based column
-// of a non-positive pivot (uniform).
-__device__ inline int smem_chol_dmma(double* S, int bp, double* Xl, double* T) {
-  __shared__ int s_fail;
-  for (int o = 0; o < bp; o += 16) {
-    double* X11 = Xl + (o / 16) * 16 * kLeafLD;
-    if (threadIdx.x < 32) {
-      const int f = warp_chol16(S, kLDS, o, X11, kLeafLD);
-      if (threadIdx.x == 0) s_fail = f ? o + f : 0;
+// L21 := A21 * X11^T in place (A21: m2 x 16 at P, ld kLDS, m2 % 16 == 0;
+// X11: 16 x 16, ld kLeafLD): warp w takes 16-row tiles w, w + nw, ...; both
+// 8-column halves stay in registers until the whole row tile is read.
+__device__ inline void smem_l21_inplace(double* P, int m2, const double* X11) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int g = lane >> 2, t = lane & 3;
+  for (int rt = warp; rt < m2 / 16; rt += nw) {
+    const int r0 = rt * 16;
+    double acc0[4] = {0.0, 0.0, 0.0, 0.0}, acc1[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+    for (int k0 = 0; k0 < 16; k0 += 8) {
+      double a[4], b0[2], b1[2];
+      a[0] = P[(r0 + g) + (k0 + t) * kLDS];
+      a[1] = P[(r0 + g + 8) + (k0 + t) * kLDS];
+      a[2] = P[(r0 + g) + (k0 + t + 4) * kLDS];
+      a[3] = P[(r0 + g + 8) + (k0 + t + 4) * kLDS];
+      b0[0] = X11[g + (k0 + t) * kLeafLD];  // op(B)[k][c] = X11[c][k]
+      b0[1] = X11[g + (k0 + t + 4) * kLeafLD];
+      b1[0] = X11[(g + 8) + (k0 + t) * kLeafLD];
+      b1[1] = X11[(g + 8) + (k0 + t + 4) * kLeafLD];
+      dmma_16x8x8(acc0, a, b0);
+      dmma_16x8x8(acc1, a, b1);
     }
-    __syncthreads();
-    if (s_fail) return s_fail;
-    const int m2 = bp - o - 16;
-    if (m2 > 0) {
-      // L21 = A21 * X11^T into T (m2 x 16), then back into S
-      for (int r0 = 0; r0 < m2; r0 += 64) {
-        const int mr = min(64, m2 - r0);
-        smem_dmma_gemm<false, true, false, false>(S + (o + 16 + r0) + o * kLDS, kLDS, X11, kLeafLD, T, kTmpLD,
-                                                  mr, 16, 16, 1.0, 0.0);
-        __syncthreads();
-        for (int e = threadIdx.x; e < mr * 16; e += blockDim.x) {
-          const int r = e % mr, c = e / mr;
-          S[(o + 16 + r0 + r) + (o + c) * kLDS] = T[r + c * kTmpLD];
-        }
-        __syncthreads();
-      }
-      // A22 -= L21 L21^T (lower part)
-      smem_dmma_gemm<false, true, false, true>(S + (o + 16) + o * kLDS, kLDS, S + (o + 16) + o * kLDS, kLDS,
-                                               S + (o + 16) + (o + 16) * kLDS, kLDS, m2, m2, 16, -1.0, 1.0);
-      __syncthreads();
+    __syncwarp();
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int r = r0 + g + ((q >= 2) ? 8 : 0), c = 2 * t + (q & 1);
+      P[r + c * kLDS] = acc0[q];
+      P[r + (c + 8) * kLDS] = acc1[q];
     }
   }
-  return 0;
+}
+
+// Lower Cholesky of the bp x bp block in S (bp a multiple of 16; the caller
+// pads with identity) in 16-column steps, the diagonal 16 x 16 leaves
+// factored and inverted by one warp (X11 into Xl), L21 = A21 X11^T and the
+// trailing update A22 -= L21 L21^T on the tensor cores.  Look-ahead: while
+// warps 1.. update the rest of A22, warp 0 updates the next diagonal leaf
+// first and factors it.  Returns 0 or the 1-based column of a non-positive
+// pivot (uniform).
+__device__ inline int smem_chol_dmma(double* S, int bp, double* Xl, double* /*T*/) {
+  __shared__ int s_fail;
+  const int warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  if (warp == 0) {
+    const int f = warp_chol16(S, kLDS, 0, Xl, kLeafLD);
+    if (threadIdx.x == 0) s_fail = f;
+  }
+  __syncthreads();
+  for (int o = 0; o < bp; o += 16) {
+    if (s_fail) return s_fail;
+    const int m2 = bp - o - 16;
+    if (m2 <= 0) break;
+    double* L21 = S + (o + 16) + o * kLDS;
+    double* A22 = S + (o + 16) + (o + 16) * kLDS;
+    smem_l21_inplace(L21, m2, Xl + (o / 16) * 16 * kLeafLD);
+    __syncthreads();
+    if (warp == 0) {
+      smem_dmma_gemm<false, true, false, true>(L21, kLDS, L21, kLDS, A22, kLDS, 16, 16, 16, -1.0, 1.0, 0, 1);
+      __syncwarp();
+      const int f = warp_chol16(S, kLDS, o + 16, Xl + ((o + 16) / 16) * 16 * kLeafLD, kLeafLD);
+      if (threadIdx.x == 0) s_fail = f ? o + 16 + f : 0;
+    } else {
+      smem_dmma_gemm<false, true, false, true>(L21, kLDS, L21, kLDS, A22, kLDS, m2, m2, 16, -1.0, 1.0, 1, nw - 1,
+                                               true);
+    }
+    __syncthreads();
+  }
+  return s_fail;
 }
 
 }  // namespace egpu

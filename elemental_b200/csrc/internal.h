@@ -56,11 +56,13 @@ int launch_split_tf32(cudaStream_t st, int rows, int cols, const double* X, long
 // X := inv(T) X for nrhs <= 64 in one cooperative launch (trsm_skinny.cu:
 // amode/bwd select T from the stored triangle A, Winv the inverted diagonal
 // blocks).  flags: ceil(n/nb) ints that hold values other than `epoch`.
+// Y != NULL selects a prescaled A: column-prescaled (X: b in, z out; Y :=
+// inv(T_rr) z_r) or, with row_prescaled, row-prescaled (Y: b in, X := x).
 // Returns EGPU_ERR_UNSUPPORTED when the shape or alignment does not fit.
 size_t trsm_skinny_flag_bytes(int n, int nb);
 int launch_trsm_skinny(cudaStream_t st, int bwd, int amode, int n, int nrhs, const double* A, long long lda,
                        const double* Winv, int nb, double* X, long long ldx, int* flags, int epoch, int sm_count,
-                       DevStatus* status, double* Y = nullptr);
+                       DevStatus* status, double* Y = nullptr, bool row_prescaled = false);
 
 // C += alpha A B for N <= 64 (split-K DMMA, FP64 atomics into C); A, B
 // 16-byte aligned with even leading dimensions, else EGPU_ERR_UNSUPPORTED.
@@ -69,7 +71,7 @@ int launch_dgemm_skinny(cudaStream_t st, int M, int N, int K, double alpha, cons
 
 // Diagonal-block Cholesky (factor in place + triangular inverse into W).
 int launch_potrf_diag(cudaStream_t st, int uplo, double* A, long long lda, int b, double* W, int ldw,
-                      DevStatus* status, int col_base);
+                      DevStatus* status, int col_base, bool store_factor = true);
 
 // Batched triangular inverse of `count` diagonal blocks of size b (the last
 // one may be smaller: n total), block i at A + i*b*(lda+1), into W + i*b*ldw.

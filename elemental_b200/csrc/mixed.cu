@@ -174,7 +174,7 @@ constexpr int kGmresRestart = 20;  // Krylov vectors per GMRES cycle
 
 // Workspace layout of the mixed solve.
 struct MixedLayout {
-  size_t as, af, lf, m2, m3, w, pkh, pkl, xw, r, yt, winv, norms, flags, gv, gw, gc, total;
+  size_t as, af, lf, pkh, pkl, xw, r, yt, winv, norms, flags, gv, gw, gc, total;
   long long lds, ldf, ldk;
 };
 
@@ -188,9 +188,6 @@ static MixedLayout mixed_layout(int n, int nrhs, int nb) {
   L.as = take(sizeof(double) * L.lds * n);
   L.af = take(sizeof(float) * L.ldf * n);
   L.lf = take(sizeof(double) * L.lds * n);
-  L.m2 = take(sizeof(double) * L.lds * n);  // L(r, j) inv(L_jj): forward sweep
-  L.m3 = take(sizeof(double) * L.lds * n);  // inv(L_jj) L(j, r): backward sweep
-  L.w = take(sizeof(double) * (size_t)nb * nb);
   L.pkh = take(2 * sizeof(float) * (size_t)n * L.ldk);  // two buffers (look-ahead)
   L.pkl = take(2 * sizeof(float) * (size_t)n * L.ldk);
   L.xw = take(sizeof(double) * L.lds * std::max(nrhs, 1));
@@ -206,43 +203,42 @@ static MixedLayout mixed_layout(int n, int nrhs, int nb) {
   return L;
 }
 
-// X := Lf^-T Lf^-1 X: two cooperative prescaled sweeps over M2 = L D^-1 and
-// M3 = D^-1 L (D the diagonal blocks, nrhs <= 64; Y is scratch), else the
-// blocked multiply-by-inverse form.
+// X := Lf^-T Lf^-1 X.  Prescaled (nrhs <= 64): the off-diagonal blocks of Lf
+// hold M2 = L D^-1 (D the diagonal blocks, W their inverses), and the two
+// cooperative sweeps are the column-prescaled forward sweep over M2 (z in X,
+// Y := W z) and the row-prescaled backward sweep over M2^T (Y in, X out).
+// Otherwise Lf holds L and the blocked multiply-by-inverse form runs.
 struct SweepFlags {
   int* flags;
   int epoch;
-  double* M2;
-  double* M3;
+  bool prescaled;
   double* Y;
 };
 static int mixed_solve(egpu_context* h, int n, int nrhs, const double* Lf, long long lds, const double* Winv,
                        double* X, SweepFlags& fl) {
-  int rc = launch_trsm_skinny(h->stream, 0, 0, n, nrhs, fl.M2, lds, Winv, h->nb, X, lds, fl.flags, ++fl.epoch,
-                              h->sm_count, h->dstatus, fl.Y);
-  if (rc == EGPU_OK)
-    rc = launch_trsm_skinny(h->stream, 1, 1, n, nrhs, fl.M3, lds, Winv, h->nb, fl.Y, lds, fl.flags, ++fl.epoch,
-                            h->sm_count, h->dstatus, X);
-  if (rc != EGPU_ERR_UNSUPPORTED) return rc;
+  if (fl.prescaled) {
+    TRY(launch_trsm_skinny(h->stream, 0, 0, n, nrhs, Lf, lds, Winv, h->nb, X, lds, fl.flags, ++fl.epoch,
+                           h->sm_count, h->dstatus, fl.Y));
+    return launch_trsm_skinny(h->stream, 1, 1, n, nrhs, Lf, lds, Winv, h->nb, X, lds, fl.flags, ++fl.epoch,
+                              h->sm_count, h->dstatus, fl.Y, true);
+  }
   TRY(trsm_blocked(h->stream, EGPU_LEFT, EGPU_LOWER, 0, n, nrhs, Lf, lds, Winv, h->nb, X, lds, h->dstatus));
   return trsm_blocked(h->stream, EGPU_LEFT, EGPU_LOWER, 1, n, nrhs, Lf, lds, Winv, h->nb, X, lds, h->dstatus);
 }
 
-// Prescaled copies of block column / row block j0 for the solve sweeps:
-// M2(r, j) = L(r, j) W_j below the diagonal block and M3(j, r) = W_j L(j, r)
-// left of it (W_j = inv(L_jj)).
-static int mixed_prescale_step(egpu_context* h, cudaStream_t st, int n, int j0, const double* Lf, long long lds,
-                               const double* Winv, double* M2, double* M3) {
+// M2 for block column j0 in place: Lf(r, j) := L(r, j) W_j below the
+// diagonal block (the 128-wide tile keeps each row panel in one CTA).  The
+// panel's TF32 split was taken from L before this runs.
+static int mixed_prescale_step(egpu_context* h, cudaStream_t st, int n, int j0, double* Lf, long long lds,
+                               const double* Winv) {
   const int nb = h->nb;
   const int bj = std::min(nb, n - j0);
   const double* Wj = Winv + (size_t)(j0 / nb) * nb * nb;
   const int below = n - j0 - bj;
-  if (below > 0)
-    TRY(launch_dgemm(st, false, true, below, bj, bj, 1.0, Lf + (j0 + bj) + (long long)j0 * lds, lds, Wj, nb, 0.0,
-                     M2 + (j0 + bj) + (long long)j0 * lds, lds, 0, false, h->dstatus));
-  if (j0 > 0)
-    TRY(launch_dgemm(st, false, true, bj, j0, bj, 1.0, Wj, nb, Lf + j0, lds, 0.0, M3 + j0, lds, 0, false,
-                     h->dstatus));
+  if (below > 0) {
+    double* P = Lf + (j0 + bj) + (long long)j0 * lds;
+    TRY(launch_dgemm(st, false, true, below, bj, bj, 1.0, P, lds, Wj, nb, 0.0, P, lds, 0, true, h->dstatus));
+  }
   return EGPU_OK;
 }
 
@@ -404,15 +400,15 @@ int dposv_mixed_core_impl(egpu_context* h, int uplo, int n, int nrhs, const doub
   double* As = reinterpret_cast<double*>(ws + L.as);
   float* Af = reinterpret_cast<float*>(ws + L.af);
   double* Lf = reinterpret_cast<double*>(ws + L.lf);
-  double* W = reinterpret_cast<double*>(ws + L.w);
   float* PKh = reinterpret_cast<float*>(ws + L.pkh);
   float* PKl = reinterpret_cast<float*>(ws + L.pkl);
   double* Xw = reinterpret_cast<double*>(ws + L.xw);
   double* R = reinterpret_cast<double*>(ws + L.r);
   double* Winv = reinterpret_cast<double*>(ws + L.winv);
   double* norms = reinterpret_cast<double*>(ws + L.norms);
-  SweepFlags fl{reinterpret_cast<int*>(ws + L.flags), 0, reinterpret_cast<double*>(ws + L.m2),
-                reinterpret_cast<double*>(ws + L.m3), reinterpret_cast<double*>(ws + L.yt)};
+  // prescaled sweeps where the one-launch sweep kernel takes the shape
+  const bool prescale = nrhs <= 64 && nb >= 8 && nb <= 128 && nb % 2 == 0;
+  SweepFlags fl{reinterpret_cast<int*>(ws + L.flags), 0, prescale, reinterpret_cast<double*>(ws + L.yt)};
   EGPU_CUDA_TRY(cudaMemsetAsync(fl.flags, 0, trsm_skinny_flag_bytes(n, nb), st));
   const long long lds = L.lds, ldf = L.ldf;
   EGPU_CUDA_TRY(cudaMemsetAsync(h->dstatus, 0, sizeof(DevStatus), st));
@@ -430,7 +426,6 @@ int dposv_mixed_core_impl(egpu_context* h, int uplo, int n, int nrhs, const doub
   float* PKh2[2] = {PKh, PKh + (size_t)n * L.ldk};
   float* PKl2[2] = {PKl, PKl + (size_t)n * L.ldk};
   cudaStream_t sd = h->side;
-  const bool prescale = nrhs <= 64;
   auto panel_chain = [&](int k, cudaStream_t s) -> int {
     const int b = std::min(nb, n - k);
     const int m = n - k, m2 = m - b;
@@ -442,7 +437,8 @@ int dposv_mixed_core_impl(egpu_context* h, int uplo, int n, int nrhs, const doub
       EGPU_CUDA_TRY(cudaGetLastError());
     }
     double* Wk = Winv + (size_t)(k / nb) * nb * nb;  // this block's inverse, kept for the solves
-    TRY(launch_potrf_diag(s, EGPU_LOWER, Lf + k + (long long)k * lds, lds, b, Wk, nb, h->dstatus, k));
+    // the solves read only Winv and the off-diagonal blocks: L_kk itself is not stored
+    TRY(launch_potrf_diag(s, EGPU_LOWER, Lf + k + (long long)k * lds, lds, b, Wk, nb, h->dstatus, k, false));
     if (m2 == 0) return EGPU_OK;
     double* L21 = Lf + (k + b) + (long long)k * lds;
     TRY(launch_dgemm(s, false, false, m2, b, b, 1.0, L21, lds, Wk, nb, 0.0, L21, lds, 0, true, h->dstatus));
@@ -473,13 +469,13 @@ int dposv_mixed_core_impl(egpu_context* h, int uplo, int n, int nrhs, const doub
       TRY(launch_tc_gemm(st, m3, m3, b, -1.0f, PKh2[par] + (size_t)b2 * L.ldk, PKl2[par] + (size_t)b2 * L.ldk,
                          PKh2[par] + (size_t)b2 * L.ldk, PKl2[par] + (size_t)b2 * L.ldk, L.ldk, 1.0f,
                          A22 + b2 + (long long)b2 * ldf, ldf, 1, 3, h->dstatus));
-    // prescaled copies for the solve sweeps, off the panel chain: M2 of block
-    // column k, M3 of row block k (its row block of L is final by now)
-    if (prescale) TRY(mixed_prescale_step(h, st, n, k, Lf, lds, Winv, fl.M2, fl.M3));
+    // M2 of block column k for the solve sweeps, off the panel chain (the
+    // split of panel k, on the side stream, came before (a) above)
+    if (prescale) TRY(mixed_prescale_step(h, st, n, k, Lf, lds, Winv));
   }
   EGPU_CUDA_TRY(cudaEventRecord(h->ev_join, sd));
   EGPU_CUDA_TRY(cudaStreamWaitEvent(st, h->ev_join, 0));
-  if (prescale) TRY(mixed_prescale_step(h, st, n, (n - 1) / nb * nb, Lf, lds, Winv, fl.M2, fl.M3));  // last block
+
   int info = 0;
   TRY(read_status_now(h, &info));
   // ---- refinement

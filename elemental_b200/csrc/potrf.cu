@@ -52,7 +52,8 @@ __device__ void tri_inverse_smem(double* S, int b, int uplo, int unit) {
 // then the inverse of the factor into W (other triangle zeroed).
 template <int UPLO>
 __global__ void __launch_bounds__(kDiagThreads) potrf_diag_kernel(double* A, long long lda, int b, double* W,
-                                                                   int ldw, DevStatus* st, int col_base) {
+                                                                   int ldw, DevStatus* st, int col_base,
+                                                                   int store_factor) {
   extern __shared__ double S[];
   if (st != nullptr && st->code != 0) return;
   const int tid = threadIdx.x;
@@ -68,14 +69,14 @@ __global__ void __launch_bounds__(kDiagThreads) potrf_diag_kernel(double* A, lon
     if (tid == 0) set_status(st, kNotHPD, col_base + f);
     return;
   }
-  tri_store(S, A, lda, b, UPLO != EGPU_LOWER, false);
+  if (store_factor) tri_store(S, A, lda, b, UPLO != EGPU_LOWER, false);
   __syncthreads();
   smem_trinv_dmma(S, bp, Xl, T);
   tri_store(S, W, ldw, b, UPLO != EGPU_LOWER, true);  // inv(U) = inv(L)^T
 }
 
 int launch_potrf_diag(cudaStream_t st, int uplo, double* A, long long lda, int b, double* W, int ldw,
-                      DevStatus* status, int col_base) {
+                      DevStatus* status, int col_base, bool store_factor) {
   if (b <= 0) return EGPU_OK;
   if (b > kMaxNB) return EGPU_ERR_ARG;
   const size_t smem = kDiagSmem;
@@ -85,13 +86,15 @@ int launch_potrf_diag(cudaStream_t st, int uplo, double* A, long long lda, int b
     e = cudaFuncSetAttribute(potrf_diag_kernel<EGPU_LOWER>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              kDiagSmem);
     if (e == cudaSuccess)
-      potrf_diag_kernel<EGPU_LOWER><<<1, kDiagThreads, smem, st>>>(A, lda, b, W, ldw, status, col_base);
+      potrf_diag_kernel<EGPU_LOWER><<<1, kDiagThreads, smem, st>>>(A, lda, b, W, ldw, status, col_base,
+                                                            store_factor ? 1 : 0);
       count_launch();
   } else {
     e = cudaFuncSetAttribute(potrf_diag_kernel<EGPU_UPPER>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              kDiagSmem);
     if (e == cudaSuccess)
-      potrf_diag_kernel<EGPU_UPPER><<<1, kDiagThreads, smem, st>>>(A, lda, b, W, ldw, status, col_base);
+      potrf_diag_kernel<EGPU_UPPER><<<1, kDiagThreads, smem, st>>>(A, lda, b, W, ldw, status, col_base,
+                                                            store_factor ? 1 : 0);
       count_launch();
   }
   if (e == cudaSuccess) e = cudaGetLastError();

@@ -19,11 +19,18 @@
 // off-diagonal block is requested before the wait for the X block it
 // multiplies.
 //
-// Prescaled form (Y != NULL): A holds the off-diagonal blocks already
+// Column-prescaled form (mode 1): A holds the off-diagonal blocks already
 // multiplied by the inverse of the diagonal block of the column they act on,
 // M(r, j) = T(r, j) inv(T_jj).  Then z_r = b_r - sum_j M(r, j) z_j needs no
 // inverse on the dependency chain: a CTA publishes z_r (in X) as soon as the
 // sum is done and forms Y_r = inv(T_rr) z_r afterwards.
+//
+// Row-prescaled form (mode 2): the blocks are M(r, j) = inv(T_rr) T(r, j), so
+// x_r = inv(T_rr) b_r - sum_j M(r, j) x_j: every task forms inv(T_rr) b_r
+// (b read from Y) before its first wait, and publishes x_r (in X) with no
+// inverse after the sum.  With M2 = L D^-1 stored, L y = b is the
+// column-prescaled sweep over M2 and L^T x = y the row-prescaled sweep over
+// M2^T (amode 1): inv(L_rr^T) L_jr^T = (L_jr inv(L_rr))^T = M2(j, r)^T.
 //
 // Products are 16 x 8 x 8 DMMA fragments from shared memory: the whole
 // off-diagonal block (ld 132, or its transpose with ld 132: conflict-free
@@ -42,7 +49,17 @@ constexpr int kTsLD = 132;       // leading dimension of the staged blocks (conf
 constexpr int kTsMaxRhs = 64;
 constexpr int kTsA = 128 * kTsLD;          // doubles: a whole off-diagonal block, [a + k*132] or [k + a*132]
 constexpr int kTsX = kTsMaxRhs * kTsLD;    // doubles: the matching X block, [k + c*132]
-constexpr int kTsSmemDoubles = kTsA + kTsX;
+// The off-diagonal products of a block row run through a ring of kTsStages
+// k chunks: stage = A chunk (amode 0: [a + k*132], amode 1: [k + a*36]) and
+// X chunk ([k + c*36]); ld 132 and 36 are both 4 mod 16 (conflict-free
+// 8-byte fragment loads).
+constexpr int kTsStages = 4;
+constexpr int kTsCT = 36;                        // ld of the chunk-transposed layouts
+constexpr int kTsRA = 128 * kTsCT;               // doubles: A chunk (the larger of 32*132 and 128*36)
+constexpr int kTsRX = kTsMaxRhs * kTsCT;         // doubles: X chunk
+constexpr int kTsRStage = kTsRA + kTsRX;
+constexpr int kTsSmemDoubles = (kTsA + kTsX) > kTsStages * kTsRStage ? (kTsA + kTsX) : kTsStages * kTsRStage;
+static_assert(32 * kTsLD <= kTsRA, "A chunk fits its stage");
 
 struct TsParams {
   const double* L;
@@ -50,8 +67,9 @@ struct TsParams {
   const double* Winv;  // block i at Winv + i*nb*nb, ld nb
   double* X;
   long long ldx;
-  double* Y;  // prescaled form: X_r receives the unscaled block (published), Y_r = inv(T_rr) X_r
+  double* Y;  // mode 1: Y_r = inv(T_rr) z_r (z published in X); mode 2: the right-hand side (X receives x)
   int n, nrhs, nb, nblk, bwd, amode;
+  int mode;        // 0 plain, 1 column-prescaled, 2 row-prescaled
   int strips, hs;  // tasks per block row and their height (prescaled form: 2)
   int* flags;
   int epoch;
@@ -134,7 +152,7 @@ __device__ __forceinline__ bool ts_wait_flag(const int* flag, int epoch, DevStat
       asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(flag) : "memory");
       if (v >= epoch) break;
       if (++it > kSpinLimit) { ok = 0; set_status(status, kTimeout, 201); break; }
-      if (it > 16) __nanosleep(64);
+      if (it > 4096) __nanosleep(64);
     }
     s_ok = ok;
   }
@@ -142,18 +160,177 @@ __device__ __forceinline__ bool ts_wait_flag(const int* flag, int epoch, DevStat
   return s_ok != 0;
 }
 
+__device__ __forceinline__ void ts_wait_upto(int pending) {
+  switch (pending) {  // immediates only
+    case 0: asm volatile("cp.async.wait_group 0;" ::: "memory"); break;
+    case 1: asm volatile("cp.async.wait_group 1;" ::: "memory"); break;
+    case 2: asm volatile("cp.async.wait_group 2;" ::: "memory"); break;
+    case 3: asm volatile("cp.async.wait_group 3;" ::: "memory"); break;
+    case 4: asm volatile("cp.async.wait_group 4;" ::: "memory"); break;
+    case 5: asm volatile("cp.async.wait_group 5;" ::: "memory"); break;
+    case 6: asm volatile("cp.async.wait_group 6;" ::: "memory"); break;
+    default: asm volatile("cp.async.wait_group 7;" ::: "memory"); break;
+  }
+}
+
+// One poll (thread 0) of an arrival counter, the answer uniform over the CTA
+// (the reduction is also a barrier).
+__device__ __forceinline__ bool ts_poll_flag(const int* flag, int epoch) {
+  int v = 0;
+  if (threadIdx.x == 0) {
+    int f;
+    asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(f) : "l"(flag) : "memory");
+    v = f >= epoch;
+  }
+  return __syncthreads_or(v) != 0;
+}
+
+// Chunk [k0, k0+32) of the m x K operand A into a ring stage (local k index).
+// amode 0: A(a, k) = G[a + k lda] kept as sA[a + kl*132]; amode 1: A(a, k) =
+// G[k + a lda] kept as sA[kl + a*36].  Entries outside m x K are zero.
+__device__ __forceinline__ void ts_ring_a(double* sA, const double* G, long long lda, int amode, int m, int K,
+                                          int k0) {
+  const int tid = threadIdx.x;
+  if (amode == 0) {
+    for (int e = tid; e < 64 * kTsKC; e += kTsThreads) {
+      const int a = 2 * (e & 63), kl = e >> 6, k = k0 + kl;
+      double* d = &sA[a + kl * kTsLD];
+      const double* src = &G[a + (long long)k * lda];
+      if (k < K && a + 1 < m) cp_async16_cg(d, src);
+      else {
+        d[0] = (k < K && a < m) ? src[0] : 0.0;
+        d[1] = 0.0;
+      }
+    }
+  } else {
+    for (int e = tid; e < 128 * (kTsKC / 2); e += kTsThreads) {
+      const int kl = 2 * (e & 15), a = e >> 4, k = k0 + kl;
+      double* d = &sA[kl + a * kTsCT];
+      const double* src = &G[k + (long long)a * lda];
+      if (a < m && k + 1 < K) cp_async16_cg(d, src);
+      else {
+        d[0] = (a < m && k < K) ? src[0] : 0.0;
+        d[1] = 0.0;
+      }
+    }
+  }
+}
+
+// Rows [k0, k0+32) of X (K x nrhs) into a ring stage: sX[kl + c*36], .cg copies.
+__device__ __forceinline__ void ts_ring_x(double* sX, int K, int k0, const double* Xg, long long ldx, int nrhs) {
+  for (int e = threadIdx.x; e < (kTsKC / 2) * nrhs; e += kTsThreads) {
+    const int kl = 2 * (e & 15), c = e >> 4, k = k0 + kl;
+    double* d = &sX[kl + c * kTsCT];
+    const double* src = &Xg[k + (long long)c * ldx];
+    if (k + 1 < K) {
+      cp_async16_cg(d, src);
+    } else {
+      d[0] = (k < K) ? __ldcg(src) : 0.0;
+      d[1] = 0.0;
+    }
+  }
+}
+
+// acc -= sum over solve steps sj < s of T(strip, j) X_j (j = the block row of
+// step sj): every product's k chunks stream through the kTsStages-deep ring
+// as one sequence, so the loads of the next chunks (and of the next product)
+// overlap the DMMAs of the current one.  A chunks need no flag and are
+// requested up to kTsStages chunks ahead; the X chunks of product sj wait for
+// X_j to be published: a poll while loaded chunks remain, a bounded wait when
+// nothing else is left.  Each piece (A chunk, X chunk) is one cp.async group;
+// xg[] remembers the group of each stage's X piece (the later of the two).
+// Returns false when a wait ran out.
+template <int NT>
+__device__ bool ts_ring_products(double (&acc)[8][4], double* sm, const TsParams& p, int s, int r0, int mr,
+                                 int target) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int g = lane >> 2, t = lane & 3;
+  const int cpp = (p.nb + kTsKC - 1) / kTsKC;  // chunks per product
+  const int Q = s * cpp;
+  int a_issued = 0, x_issued = 0, ready = 0, ncommit = 0;
+  int ag[kTsStages], xg[kTsStages];
+#pragma unroll
+  for (int i = 0; i < kTsStages; ++i) ag[i] = xg[i] = 0;
+  for (int qc = 0; qc < Q; ++qc) {
+    // X pieces first: a fresh A piece committed before the X piece of chunk
+    // qc would make the wait for that X piece wait for it too
+    for (; x_issued < Q && x_issued < qc + kTsStages; ++x_issued) {
+      const int sj = x_issued / cpp, c = x_issued - sj * cpp;
+      const int j = ts_block(p, sj), j0 = j * p.nb, mj = min(p.nb, p.n - j0);
+      if (sj >= ready) {
+        if (x_issued > qc) {
+          if (!ts_poll_flag(&p.flags[j], target)) break;
+        } else if (!ts_wait_flag(&p.flags[j], target, p.status)) {
+          asm volatile("cp.async.wait_group 0;" ::: "memory");
+          return false;
+        }
+        ready = sj + 1;
+      }
+      if (c * kTsKC < mj)
+        ts_ring_x(sm + (x_issued % kTsStages) * kTsRStage + kTsRA, mj, c * kTsKC, p.X + j0, p.ldx, p.nrhs);
+      asm volatile("cp.async.commit_group;" ::: "memory");
+      xg[x_issued % kTsStages] = ncommit++;
+    }
+    // A pieces (no flag) up to kTsStages chunks ahead
+    for (; a_issued < Q && a_issued < qc + kTsStages; ++a_issued) {
+      const int sj = a_issued / cpp, c = a_issued - sj * cpp;
+      const int j = ts_block(p, sj), j0 = j * p.nb, mj = min(p.nb, p.n - j0);
+      if (c * kTsKC < mj) {
+        const double* G = p.amode == 0 ? p.L + r0 + (long long)j0 * p.lda : p.L + j0 + (long long)r0 * p.lda;
+        ts_ring_a(sm + (a_issued % kTsStages) * kTsRStage, G, p.lda, p.amode, mr, mj, c * kTsKC);
+      }
+      asm volatile("cp.async.commit_group;" ::: "memory");
+      ag[a_issued % kTsStages] = ncommit++;
+    }
+    const int slot = qc % kTsStages;
+    ts_wait_upto(ncommit - 1 - max(ag[slot], xg[slot]));  // this thread's pieces of chunk qc landed
+    __syncthreads();
+    const int sj = qc / cpp, c = qc - sj * cpp;
+    const int mj = min(p.nb, p.n - ts_block(p, sj) * p.nb);
+    if (c * kTsKC < mj && 16 * warp < mr) {
+      const double* sA = sm + slot * kTsRStage;
+      const double* sX = sA + kTsRA;
+      const int ra = 16 * warp + g;
+#pragma unroll
+      for (int kk = 0; kk < kTsKC; kk += 8) {
+        double a[4];
+        if (p.amode == 0) {
+          a[0] = -sA[ra + (kk + t) * kTsLD];
+          a[1] = -sA[ra + 8 + (kk + t) * kTsLD];
+          a[2] = -sA[ra + (kk + t + 4) * kTsLD];
+          a[3] = -sA[ra + 8 + (kk + t + 4) * kTsLD];
+        } else {
+          a[0] = -sA[(kk + t) + ra * kTsCT];
+          a[1] = -sA[(kk + t) + (ra + 8) * kTsCT];
+          a[2] = -sA[(kk + t + 4) + ra * kTsCT];
+          a[3] = -sA[(kk + t + 4) + (ra + 8) * kTsCT];
+        }
+#pragma unroll
+        for (int nt = 0; nt < NT; ++nt) {
+          double bf[2];
+          bf[0] = sX[(kk + t) + (8 * nt + g) * kTsCT];
+          bf[1] = sX[(kk + t + 4) + (8 * nt + g) * kTsCT];
+          dmma_16x8x8(acc[nt], a, bf);
+        }
+      }
+    }
+    __syncthreads();  // the stage is free for chunk qc + kTsStages
+  }
+  return true;
+}
+
 // acc[nt] (16 x 8 fragments, rows 16 warp.., columns 8 nt..) += sign * A(m x K) * X(K x nrhs), K <= 128.
 // Every chunk of A is requested at once (one cp.async group each) before the
 // wait for X to be published (`flag`), then every chunk of X, so one product
 // costs one memory round trip plus its DMMAs.  x_in_smem: X already sits in
 // the X buffer (the staged accumulator).
+template <int NT>
 __device__ bool ts_product(double (&acc)[8][4], double sign, double* sm, const double* G, long long lda, int amode,
                            int m, int K, const double* Xg, long long ldx, int nrhs, bool x_in_smem,
                            const int* flag = nullptr, int epoch = 0, DevStatus* status = nullptr) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int g = lane >> 2, t = lane & 3;
   const int nch = (K + kTsKC - 1) / kTsKC;
-  const int ntn = (nrhs + 7) / 8;
   double* sA = sm;
   double* sX = sm + kTsA;
   for (int c = 0; c < nch; ++c) {
@@ -191,13 +368,11 @@ __device__ bool ts_product(double (&acc)[8][4], double sign, double* sm, const d
 #pragma unroll
       for (int q = 0; q < 4; ++q) a[q] *= sign;
 #pragma unroll
-      for (int nt = 0; nt < 8; ++nt) {
-        if (nt < ntn) {
-          double bf[2];
-          bf[0] = sX[(k + t) + (8 * nt + g) * kTsLD];
-          bf[1] = sX[(k + t + 4) + (8 * nt + g) * kTsLD];
-          dmma_16x8x8(acc[nt], a, bf);
-        }
+      for (int nt = 0; nt < NT; ++nt) {
+        double bf[2];
+        bf[0] = sX[(k + t) + (8 * nt + g) * kTsLD];
+        bf[1] = sX[(k + t + 4) + (8 * nt + g) * kTsLD];
+        dmma_16x8x8(acc[nt], a, bf);
       }
     }
   }
@@ -207,13 +382,15 @@ __device__ bool ts_product(double (&acc)[8][4], double sign, double* sm, const d
 
 }  // namespace
 
+// NT: 8-column tiles of the right-hand side (a compile-time count: a DMMA
+// skipped under a run-time predicate still costs its issue slots).
+template <int NT>
 __global__ void __launch_bounds__(kTsThreads, 1) trsm_skinny_kernel(TsParams p) {
   extern __shared__ double sm[];
   double* accS = sm + kTsA;  // the X buffer: the accumulator is the next product's right operand
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int g = lane >> 2, t = lane & 3;
-  const int ntn = (p.nrhs + 7) / 8;
-  const bool pre = p.Y != nullptr;
+  const int mode = p.mode;
   const int S = p.strips, hs = p.hs, target = p.strips * p.epoch;
   if (p.status != nullptr && ((volatile DevStatus*)p.status)->code != 0) return;
   for (int task = blockIdx.x; task < p.nblk * S; task += gridDim.x) {
@@ -227,37 +404,35 @@ __global__ void __launch_bounds__(kTsThreads, 1) trsm_skinny_kernel(TsParams p) 
 #pragma unroll
       for (int e = 0; e < 4; ++e) acc[nt][e] = 0.0;
     if (mr > 0) {
-      // acc = B(strip)
+      if (mode == 2) {
+        // acc = inv(T_rr)(strip rows, :) b_r, before the first wait
+        const double* Wr = p.Winv + (long long)r * p.nb * p.nb;
+        const double* G = p.amode == 0 ? Wr + q * hs : Wr + (long long)q * hs * p.nb;
+        ts_product<NT>(acc, 1.0, sm, G, p.nb, p.amode, mr, mb, p.Y + rb0, p.ldx, p.nrhs, false);
+      } else {
+        // acc = B(strip)
 #pragma unroll
-      for (int nt = 0; nt < 8; ++nt)
+        for (int nt = 0; nt < 8; ++nt)
 #pragma unroll
-        for (int e = 0; e < 4; ++e) {
-          const int row = 16 * warp + g + ((e >= 2) ? 8 : 0), col = 8 * nt + 2 * t + (e & 1);
-          if (nt < ntn && row < mr && col < p.nrhs) acc[nt][e] = __ldcg(&p.X[(r0 + row) + (long long)col * p.ldx]);
-        }
-      // acc -= T(strip, j) X_j for the blocks j solved before r
-      for (int sj = 0; sj < s; ++sj) {
-        const int j = ts_block(p, sj);
-        const int j0 = j * p.nb, mj = min(p.nb, p.n - j0);
-        const double* G = p.amode == 0 ? p.L + r0 + (long long)j0 * p.lda   // A(strip, j)
-                                       : p.L + j0 + (long long)r0 * p.lda;  // A(j, strip)^T
-        if (!ts_product(acc, -1.0, sm, G, p.lda, p.amode, mr, mj, p.X + j0, p.ldx, p.nrhs, false, &p.flags[j], target,
-                        p.status))
-          return;
+          for (int e = 0; e < 4; ++e) {
+            const int row = 16 * warp + g + ((e >= 2) ? 8 : 0), col = 8 * nt + 2 * t + (e & 1);
+            if (nt < NT && row < mr && col < p.nrhs) acc[nt][e] = __ldcg(&p.X[(r0 + row) + (long long)col * p.ldx]);
+          }
       }
+      // acc -= T(strip, j) X_j for the blocks j solved before r
+      if (!ts_ring_products<NT>(acc, sm, p, s, r0, mr, target)) return;
     }
-    if (pre) {
-      // prescaled form: publish the strip of z_r = acc first (the others need only z) ...
+    if (mode == 1) {
+      // column-prescaled form: publish the strip of z_r = acc first (the others need only z) ...
       if (mr > 0)
 #pragma unroll
         for (int nt = 0; nt < 8; ++nt)
 #pragma unroll
           for (int e = 0; e < 4; ++e) {
             const int row = 16 * warp + g + ((e >= 2) ? 8 : 0), col = 8 * nt + 2 * t + (e & 1);
-            if (nt < ntn && row < mr && col < p.nrhs) p.X[(r0 + row) + (long long)col * p.ldx] = acc[nt][e];
+            if (nt < NT && row < mr && col < p.nrhs) p.X[(r0 + row) + (long long)col * p.ldx] = acc[nt][e];
           }
-      __threadfence();
-      __syncthreads();
+      __syncthreads();  // the block's stores happen before thread 0's release (barrier + cumulative release)
       if (tid == 0) asm volatile("red.release.gpu.global.add.s32 [%0], 1;" ::"l"(&p.flags[r]) : "memory");
       if (mr <= 0) continue;
       // ... then Y(strip) = inv(T_rr)(strip rows, :) z_r once every strip of z_r is out
@@ -267,34 +442,33 @@ __global__ void __launch_bounds__(kTsThreads, 1) trsm_skinny_kernel(TsParams p) 
         for (int e = 0; e < 4; ++e) acc[nt][e] = 0.0;
       const double* Wr = p.Winv + (long long)r * p.nb * p.nb;
       const double* G = p.amode == 0 ? Wr + q * hs : Wr + (long long)q * hs * p.nb;
-      if (!ts_product(acc, 1.0, sm, G, p.nb, p.amode, mr, mb, p.X + rb0, p.ldx, p.nrhs, false, &p.flags[r], target,
+      if (!ts_product<NT>(acc, 1.0, sm, G, p.nb, p.amode, mr, mb, p.X + rb0, p.ldx, p.nrhs, false, &p.flags[r], target,
                       p.status))
         return;
-    } else {
+    } else if (mode == 0) {
       // X_r = inv(T_rr) acc (one strip per block: the whole accumulator is in this CTA)
 #pragma unroll
       for (int nt = 0; nt < 8; ++nt)
 #pragma unroll
         for (int e = 0; e < 4; ++e) {
           const int row = 16 * warp + g + ((e >= 2) ? 8 : 0), col = 8 * nt + 2 * t + (e & 1);
-          if (nt < ntn) accS[row + col * kTsLD] = acc[nt][e];
+          if (nt < NT) accS[row + col * kTsLD] = acc[nt][e];
           acc[nt][e] = 0.0;
         }
       __syncthreads();
       const double* Wr = p.Winv + (long long)r * p.nb * p.nb;
-      ts_product(acc, 1.0, sm, Wr, p.nb, p.amode, mr, mr, accS, kTsLD, p.nrhs, true);
+      ts_product<NT>(acc, 1.0, sm, Wr, p.nb, p.amode, mr, mr, accS, kTsLD, p.nrhs, true);
     }
-    double* out = pre ? p.Y : p.X;
+    double* out = mode == 1 ? p.Y : p.X;
 #pragma unroll
     for (int nt = 0; nt < 8; ++nt)
 #pragma unroll
       for (int e = 0; e < 4; ++e) {
         const int row = 16 * warp + g + ((e >= 2) ? 8 : 0), col = 8 * nt + 2 * t + (e & 1);
-        if (nt < ntn && row < mr && col < p.nrhs) out[(r0 + row) + (long long)col * p.ldx] = acc[nt][e];
+        if (nt < NT && row < mr && col < p.nrhs) out[(r0 + row) + (long long)col * p.ldx] = acc[nt][e];
       }
-    if (!pre) {
-      __threadfence();
-      __syncthreads();
+    if (mode != 1) {
+      __syncthreads();  // the block's stores happen before thread 0's release (barrier + cumulative release)
       if (tid == 0) asm volatile("red.release.gpu.global.add.s32 [%0], 1;" ::"l"(&p.flags[r]) : "memory");
     }
   }
@@ -307,7 +481,7 @@ size_t trsm_skinny_flag_bytes(int n, int nb) { return sizeof(int) * (size_t)((n 
 // waits for counters to reach strips x epoch.
 int launch_trsm_skinny(cudaStream_t st, int bwd, int amode, int n, int nrhs, const double* L, long long lda,
                        const double* Winv, int nb, double* X, long long ldx, int* flags, int epoch, int sm_count,
-                       DevStatus* status, double* Y) {
+                       DevStatus* status, double* Y, bool row_prescaled) {
   if (n <= 0 || nrhs <= 0) return EGPU_OK;
   if (nrhs > kTsMaxRhs || nb > 128 || nb < 8 || nb % 2 != 0 || ldx % 2 != 0 || lda % 2 != 0 ||
       reinterpret_cast<uintptr_t>(X) % 16 != 0 || reinterpret_cast<uintptr_t>(L) % 16 != 0 ||
@@ -316,20 +490,26 @@ int launch_trsm_skinny(cudaStream_t st, int bwd, int amode, int n, int nrhs, con
   TsParams p;
   p.L = L; p.lda = lda; p.Winv = Winv; p.X = X; p.ldx = ldx; p.Y = Y;
   p.n = n; p.nrhs = nrhs; p.nb = nb; p.nblk = (n + nb - 1) / nb; p.bwd = bwd; p.amode = amode;
+  p.mode = Y == nullptr ? 0 : row_prescaled ? 2 : 1;
   // prescaled form: two strips per block row, so the dependency chain's product is half a block,
-  // when every strip still gets a CTA of its own (a CTA that holds two tasks starts its second late)
-  p.strips = (Y != nullptr && nb >= 32 && 2 * ((n + nb - 1) / nb) <= sm_count) ? 2 : 1;
+  // while a CTA holds at most two tasks (its second task starts after the first and still has to
+  // catch up with all the products of its block row)
+  p.strips = (p.mode != 0 && nb >= 32 && (n + nb - 1) / nb <= sm_count) ? 2 : 1;
   p.hs = p.strips == 1 ? nb : ((nb + 1) / 2 + 15) / 16 * 16;
   p.flags = flags; p.epoch = epoch; p.status = status;
   const size_t smem = sizeof(double) * kTsSmemDoubles;
-  static bool attr = false;
-  if (!attr) {
-    if (cudaFuncSetAttribute(trsm_skinny_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
-        cudaSuccess) {
+  const int nt = nrhs <= 8 ? 1 : nrhs <= 16 ? 2 : nrhs <= 32 ? 4 : 8;
+  void (*kern)(TsParams) = nt == 1 ? trsm_skinny_kernel<1>
+                           : nt == 2 ? trsm_skinny_kernel<2>
+                           : nt == 4 ? trsm_skinny_kernel<4> : trsm_skinny_kernel<8>;
+  static bool attr[4] = {false, false, false, false};
+  const int ai = nt == 1 ? 0 : nt == 2 ? 1 : nt == 4 ? 2 : 3;
+  if (!attr[ai]) {
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
       cudaGetLastError();
       return EGPU_ERR_UNSUPPORTED;
     }
-    attr = true;
+    attr[ai] = true;
   }
   const int grid = std::min(p.nblk * p.strips, sm_count);
   TraceMark tm(st, kTraceSolve, (double)n * n * nrhs, 4.0 * (double)n * n + 16.0 * n * nrhs);
@@ -343,7 +523,7 @@ int launch_trsm_skinny(cudaStream_t st, int bwd, int amode, int n, int nrhs, con
   attr1[0].val.cooperative = 1;
   cfg.attrs = attr1;
   cfg.numAttrs = 1;
-  cudaError_t e = cudaLaunchKernelEx(&cfg, trsm_skinny_kernel, p);
+  cudaError_t e = cudaLaunchKernelEx(&cfg, kern, p);
   count_launch();
   if (e != cudaSuccess) {
     set_last_error(e, "trsm_skinny launch", __FILE__, __LINE__);
