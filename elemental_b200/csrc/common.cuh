@@ -15,7 +15,7 @@ enum StatusCode : int {
   kOk = 0,
   kNotHPD = 1,     // Cholesky: non-positive pivot (std::logic_error in the reference)
   kSingular = 2,   // LU: exact zero pivot (SingularMatrixException)
-  kTimeout = 3,    // a bounded device-side wait ran out
+  kTimeout = 3,    // a bounded device-side wait ran out (or a kernel refused a launch shape; info: site)
 };
 
 struct DevStatus {
@@ -77,6 +77,29 @@ __device__ __forceinline__ void tma_load_2d(void* smem_dst, const CUtensorMap* m
       "[%4];" ::"r"(smem_u32(smem_dst)),
       "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(smem_u32(bar))
       : "memory");
+}
+
+// Untiled bulk copy, global -> this CTA's shared memory: both addresses
+// 16-byte aligned, size a multiple of 16 bytes; completion is counted on the
+// mbarrier's transaction count.
+__device__ __forceinline__ void bulk_load(void* smem_dst, const void* gsrc, uint32_t bytes, uint64_t* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+               ::"r"(smem_u32(smem_dst)), "l"(gsrc), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
+
+// The executing thread's earlier cp.async copies arrive on `bar` when they
+// complete (the arrival is counted in the barrier's initial count).
+__device__ __forceinline__ void cp_async_arrive_noinc(uint64_t* bar) {
+  asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+// Order this thread's generic-proxy view before its later async-proxy (bulk
+// copy) accesses: global data acquired from another CTA, or shared memory
+// last written by ordinary stores.
+__device__ __forceinline__ void fence_proxy_async_global() { asm volatile("fence.proxy.async.global;" ::: "memory"); }
+__device__ __forceinline__ void fence_proxy_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
 
 __device__ __forceinline__ void tma_prefetch_desc(const CUtensorMap* map) {

@@ -160,131 +160,117 @@ __device__ __forceinline__ bool ts_wait_flag(const int* flag, int epoch, DevStat
   return s_ok != 0;
 }
 
-__device__ __forceinline__ void ts_wait_upto(int pending) {
-  switch (pending) {  // immediates only
-    case 0: asm volatile("cp.async.wait_group 0;" ::: "memory"); break;
-    case 1: asm volatile("cp.async.wait_group 1;" ::: "memory"); break;
-    case 2: asm volatile("cp.async.wait_group 2;" ::: "memory"); break;
-    case 3: asm volatile("cp.async.wait_group 3;" ::: "memory"); break;
-    case 4: asm volatile("cp.async.wait_group 4;" ::: "memory"); break;
-    case 5: asm volatile("cp.async.wait_group 5;" ::: "memory"); break;
-    case 6: asm volatile("cp.async.wait_group 6;" ::: "memory"); break;
-    default: asm volatile("cp.async.wait_group 7;" ::: "memory"); break;
-  }
+// Chunk [k0, k0+32) of the strip's A operand into a ring stage: one TMA box
+// issued by thread 0, completing on `bar`.  amode 0: the box is rows r0 ..
+// r0+hs+3 x columns j0+k0 .. +31 of the stored matrix, landing as
+// sA[a + kl*(hs+4)]; amode 1: rows j0+k0 .. +35 x columns r0 .. r0+hs-1,
+// landing as sA[kl + a*36].  Both pitches are 4 mod 16 (conflict-free
+// fragment loads); the extra rows are read and ignored, and the parts of the
+// box past the matrix (a short last block) arrive as zeros.
+__device__ __forceinline__ void ts_tma_a(double* sA, const CUtensorMap* map, const TsParams& p, int r0, int j0,
+                                         int k0, uint64_t* bar) {
+  if (threadIdx.x != 0) return;
+  const uint32_t bytes = p.amode == 0 ? (uint32_t)((p.hs + 4) * kTsKC * 8) : (uint32_t)(kTsCT * p.hs * 8);
+  mbar_expect_tx(bar, bytes);
+  if (p.amode == 0) tma_load_2d(sA, map, bar, r0, j0 + k0);
+  else tma_load_2d(sA, map, bar, j0 + k0, r0);
 }
 
-// One poll (thread 0) of an arrival counter, the answer uniform over the CTA
-// (the reduction is also a barrier).
-__device__ __forceinline__ bool ts_poll_flag(const int* flag, int epoch) {
-  int v = 0;
-  if (threadIdx.x == 0) {
-    int f;
-    asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(f) : "l"(flag) : "memory");
-    v = f >= epoch;
-  }
-  return __syncthreads_or(v) != 0;
-}
-
-// Chunk [k0, k0+32) of the m x K operand A into a ring stage (local k index).
-// amode 0: A(a, k) = G[a + k lda] kept as sA[a + kl*132]; amode 1: A(a, k) =
-// G[k + a lda] kept as sA[kl + a*36].  Entries outside m x K are zero.
-__device__ __forceinline__ void ts_ring_a(double* sA, const double* G, long long lda, int amode, int m, int K,
-                                          int k0) {
-  const int tid = threadIdx.x;
-  if (amode == 0) {
-    for (int e = tid; e < 64 * kTsKC; e += kTsThreads) {
-      const int a = 2 * (e & 63), kl = e >> 6, k = k0 + kl;
-      double* d = &sA[a + kl * kTsLD];
-      const double* src = &G[a + (long long)k * lda];
-      if (k < K && a + 1 < m) cp_async16_cg(d, src);
-      else {
-        d[0] = (k < K && a < m) ? src[0] : 0.0;
-        d[1] = 0.0;
-      }
-    }
-  } else {
-    for (int e = tid; e < 128 * (kTsKC / 2); e += kTsThreads) {
-      const int kl = 2 * (e & 15), a = e >> 4, k = k0 + kl;
-      double* d = &sA[kl + a * kTsCT];
-      const double* src = &G[k + (long long)a * lda];
-      if (a < m && k + 1 < K) cp_async16_cg(d, src);
-      else {
-        d[0] = (a < m && k < K) ? src[0] : 0.0;
-        d[1] = 0.0;
-      }
-    }
-  }
-}
-
-// Rows [k0, k0+32) of X (K x nrhs) into a ring stage: sX[kl + c*36], .cg copies.
-__device__ __forceinline__ void ts_ring_x(double* sX, int K, int k0, const double* Xg, long long ldx, int nrhs) {
+// Rows [k0, k0+32) of X (K x nrhs) into a ring stage, sX[kl + c*36]: 16-byte
+// .cg copies by every thread (X was published by other CTAs and acquired
+// through a flag: read through L2 in the generic proxy), each thread's copies
+// arriving on `bar` (initial count: the block size).  Rows past K are zero.
+__device__ __forceinline__ void ts_async_x(double* sX, int K, int k0, const double* Xg, long long ldx, int nrhs,
+                                           uint64_t* bar) {
   for (int e = threadIdx.x; e < (kTsKC / 2) * nrhs; e += kTsThreads) {
     const int kl = 2 * (e & 15), c = e >> 4, k = k0 + kl;
-    double* d = &sX[kl + c * kTsCT];
+    double* dd = &sX[kl + c * kTsCT];
     const double* src = &Xg[k + (long long)c * ldx];
     if (k + 1 < K) {
-      cp_async16_cg(d, src);
+      cp_async16_cg(dd, src);
     } else {
-      d[0] = (k < K) ? __ldcg(src) : 0.0;
-      d[1] = 0.0;
+      dd[0] = (k < K) ? __ldcg(src) : 0.0;
+      dd[1] = 0.0;
     }
   }
+  cp_async_arrive_noinc(bar);
+}
+
+// Error exit: wait (bounded) for the copies of every piece already issued,
+// chunks [from, a_end) of A and [from, x_end) of X, so no copy still targets
+// this CTA's shared memory when it returns.
+__device__ __forceinline__ void ts_ring_drain(uint64_t* barA, uint64_t* barX, int gq, int from, int a_end, int x_end) {
+  for (int q = from; q < a_end; ++q)
+    (void)mbar_wait_bounded(&barA[(gq + q) % kTsStages], (uint32_t)((gq + q) / kTsStages) & 1u);
+  for (int q = from; q < x_end; ++q)
+    (void)mbar_wait_bounded(&barX[(gq + q) % kTsStages], (uint32_t)((gq + q) / kTsStages) & 1u);
+}
+
+// Both pieces of ring chunk `gq` (this CTA's running chunk count) landed:
+// every thread waits on the stage's two mbarrier phases (bounded).
+__device__ __forceinline__ bool ts_ring_wait(uint64_t* barA, uint64_t* barX, int gq, DevStatus* status) {
+  const int slot = gq % kTsStages;
+  const uint32_t par = (uint32_t)(gq / kTsStages) & 1u;
+  if (mbar_wait_bounded(&barA[slot], par) && mbar_wait_bounded(&barX[slot], par)) return true;
+  set_status(status, kTimeout, 202);
+  return false;
 }
 
 // acc -= sum over solve steps sj < s of T(strip, j) X_j (j = the block row of
 // step sj): every product's k chunks stream through the kTsStages-deep ring
 // as one sequence, so the loads of the next chunks (and of the next product)
-// overlap the DMMAs of the current one.  A chunks need no flag and are
-// requested up to kTsStages chunks ahead; the X chunks of product sj wait for
-// X_j to be published: a poll while loaded chunks remain, a bounded wait when
-// nothing else is left.  Each piece (A chunk, X chunk) is one cp.async group;
-// xg[] remembers the group of each stage's X piece (the later of the two).
-// Returns false when a wait ran out.
+// overlap the DMMAs of the current one.  A pieces are single TMA boxes
+// (thread 0) issued up to kTsStages chunks ahead with no flag; X pieces are
+// small copies by every thread once X_j is published:
+// a poll that runs behind the DMMAs while loaded chunks remain, a bounded
+// wait when nothing else is left.  gq: the CTA's running chunk count (the
+// stage mbarriers' phases).  Returns false when a wait ran out.
 template <int NT>
-__device__ bool ts_ring_products(double (&acc)[8][4], double* sm, const TsParams& p, int s, int r0, int mr,
-                                 int target) {
+__device__ bool ts_ring_products(double (&acc)[8][4], double* sm, uint64_t* barA, uint64_t* barX, int& gq,
+                                 const CUtensorMap* mapA, const TsParams& p, int s, int r0, int mr, int target) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int g = lane >> 2, t = lane & 3;
   const int cpp = (p.nb + kTsKC - 1) / kTsKC;  // chunks per product
   const int Q = s * cpp;
-  int a_issued = 0, x_issued = 0, ready = 0, ncommit = 0;
-  int ag[kTsStages], xg[kTsStages];
-#pragma unroll
-  for (int i = 0; i < kTsStages; ++i) ag[i] = xg[i] = 0;
+  int a_issued = 0, x_issued = 0, ready = 0;
+  int pv_prev = 0, pidx_prev = -1;  // the previous chunk's poll (thread 0)
+  if (threadIdx.x == 0) fence_proxy_async_smem();  // the stages were last written in the generic proxy
+  const int ldA = p.amode == 0 ? p.hs + 4 : kTsCT;  // A stage pitch
   for (int qc = 0; qc < Q; ++qc) {
-    // X pieces first: a fresh A piece committed before the X piece of chunk
-    // qc would make the wait for that X piece wait for it too
+    // X pieces first (they gate the next chunks)
     for (; x_issued < Q && x_issued < qc + kTsStages; ++x_issued) {
       const int sj = x_issued / cpp, c = x_issued - sj * cpp;
       const int j = ts_block(p, sj), j0 = j * p.nb, mj = min(p.nb, p.n - j0);
       if (sj >= ready) {
-        if (x_issued > qc) {
-          if (!ts_poll_flag(&p.flags[j], target)) break;
-        } else if (!ts_wait_flag(&p.flags[j], target, p.status)) {
-          asm volatile("cp.async.wait_group 0;" ::: "memory");
+        if (x_issued > qc) break;  // loaded chunks remain: the poll below runs behind them
+        if (!ts_wait_flag(&p.flags[j], target, p.status)) {
+          ts_ring_drain(barA, barX, gq, qc, a_issued, x_issued);
           return false;
         }
         ready = sj + 1;
       }
-      if (c * kTsKC < mj)
-        ts_ring_x(sm + (x_issued % kTsStages) * kTsRStage + kTsRA, mj, c * kTsKC, p.X + j0, p.ldx, p.nrhs);
-      asm volatile("cp.async.commit_group;" ::: "memory");
-      xg[x_issued % kTsStages] = ncommit++;
+      const int sl = (gq + x_issued) % kTsStages;
+      ts_async_x(sm + sl * kTsRStage + kTsRA, mj, c * kTsKC, p.X + j0, p.ldx, p.nrhs, &barX[sl]);
     }
     // A pieces (no flag) up to kTsStages chunks ahead
     for (; a_issued < Q && a_issued < qc + kTsStages; ++a_issued) {
       const int sj = a_issued / cpp, c = a_issued - sj * cpp;
-      const int j = ts_block(p, sj), j0 = j * p.nb, mj = min(p.nb, p.n - j0);
-      if (c * kTsKC < mj) {
-        const double* G = p.amode == 0 ? p.L + r0 + (long long)j0 * p.lda : p.L + j0 + (long long)r0 * p.lda;
-        ts_ring_a(sm + (a_issued % kTsStages) * kTsRStage, G, p.lda, p.amode, mr, mj, c * kTsKC);
-      }
-      asm volatile("cp.async.commit_group;" ::: "memory");
-      ag[a_issued % kTsStages] = ncommit++;
+      const int sl = (gq + a_issued) % kTsStages;
+      ts_tma_a(sm + sl * kTsRStage, mapA, p, r0, ts_block(p, sj) * p.nb, c * kTsKC, &barA[sl]);
     }
-    const int slot = qc % kTsStages;
-    ts_wait_upto(ncommit - 1 - max(ag[slot], xg[slot]));  // this thread's pieces of chunk qc landed
-    __syncthreads();
+    // poll for the first product not yet known published: a relaxed load
+    // issued now and read at the next chunk's closing barrier, so its round
+    // trip hides behind the DMMAs
+    int pv = 0;
+    const int pidx = ready < s ? ready : -1;
+    if (pidx >= 0 && threadIdx.x == 0)
+      asm volatile("ld.relaxed.gpu.global.s32 %0, [%1];" : "=r"(pv) : "l"(&p.flags[ts_block(p, pidx)]) : "memory");
+    const int slot = (gq + qc) % kTsStages;
+    if (!ts_ring_wait(barA, barX, gq + qc, p.status)) {
+      ts_ring_drain(barA, barX, gq, qc + 1, a_issued, x_issued);
+      return false;
+    }
+    __syncthreads();  // the X pieces' ordinary-store parts (zero rows) are visible
     const int sj = qc / cpp, c = qc - sj * cpp;
     const int mj = min(p.nb, p.n - ts_block(p, sj) * p.nb);
     if (c * kTsKC < mj && 16 * warp < mr) {
@@ -295,10 +281,10 @@ __device__ bool ts_ring_products(double (&acc)[8][4], double* sm, const TsParams
       for (int kk = 0; kk < kTsKC; kk += 8) {
         double a[4];
         if (p.amode == 0) {
-          a[0] = -sA[ra + (kk + t) * kTsLD];
-          a[1] = -sA[ra + 8 + (kk + t) * kTsLD];
-          a[2] = -sA[ra + (kk + t + 4) * kTsLD];
-          a[3] = -sA[ra + 8 + (kk + t + 4) * kTsLD];
+          a[0] = -sA[ra + (kk + t) * ldA];
+          a[1] = -sA[ra + 8 + (kk + t) * ldA];
+          a[2] = -sA[ra + (kk + t + 4) * ldA];
+          a[3] = -sA[ra + 8 + (kk + t + 4) * ldA];
         } else {
           a[0] = -sA[(kk + t) + ra * kTsCT];
           a[1] = -sA[(kk + t) + (ra + 8) * kTsCT];
@@ -314,8 +300,19 @@ __device__ bool ts_ring_products(double (&acc)[8][4], double* sm, const TsParams
         }
       }
     }
-    __syncthreads();  // the stage is free for chunk qc + kTsStages
+    // the stage is free for chunk qc + kTsStages; the previous chunk's poll
+    // answer, made an acquire by thread 0's fence before the barrier that
+    // publishes it
+    int seen = 0;
+    if (threadIdx.x == 0 && pidx_prev >= 0 && pidx_prev == ready && pv_prev >= target) {
+      asm volatile("fence.acq_rel.gpu;" ::: "memory");
+      seen = 1;
+    }
+    if (__syncthreads_or(seen)) ready = ready + 1;
+    pv_prev = pv;
+    pidx_prev = pidx;
   }
+  gq += Q;
   return true;
 }
 
@@ -385,14 +382,31 @@ __device__ bool ts_product(double (&acc)[8][4], double sign, double* sm, const d
 // NT: 8-column tiles of the right-hand side (a compile-time count: a DMMA
 // skipped under a run-time predicate still costs its issue slots).
 template <int NT>
-__global__ void __launch_bounds__(kTsThreads, 1) trsm_skinny_kernel(TsParams p) {
-  extern __shared__ double sm[];
+__global__ void __launch_bounds__(kTsThreads, 1) trsm_skinny_kernel(const __grid_constant__ CUtensorMap mapA,
+                                                                    TsParams p) {
+  // TMA boxes land at stage starts: the dynamic region must be 128-byte
+  // aligned (it follows the static barriers)
+  extern __shared__ __align__(128) double sm[];
   double* accS = sm + kTsA;  // the X buffer: the accumulator is the next product's right operand
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int g = lane >> 2, t = lane & 3;
+  __shared__ __align__(8) uint64_t barA[kTsStages], barX[kTsStages];
+  if (tid == 0) {
+    for (int i = 0; i < kTsStages; ++i) {
+      mbar_init(&barA[i], 1);
+      mbar_init(&barX[i], kTsThreads);
+    }
+    fence_mbar_init();
+  }
+  __syncthreads();
+  int gq = 0;  // ring chunks issued by this CTA so far
   const int mode = p.mode;
   const int S = p.strips, hs = p.hs, target = p.strips * p.epoch;
   if (p.status != nullptr && ((volatile DevStatus*)p.status)->code != 0) return;
+  if (smem_u32(sm) % 128 != 0) {  // no TMA into a misaligned stage: report and stop
+    if (tid == 0) set_status(p.status, kTimeout, 203);
+    return;
+  }
   for (int task = blockIdx.x; task < p.nblk * S; task += gridDim.x) {
     const int s = task / S, q = task - s * S;
     const int r = ts_block(p, s);
@@ -420,7 +434,7 @@ __global__ void __launch_bounds__(kTsThreads, 1) trsm_skinny_kernel(TsParams p) 
           }
       }
       // acc -= T(strip, j) X_j for the blocks j solved before r
-      if (!ts_ring_products<NT>(acc, sm, p, s, r0, mr, target)) return;
+      if (!ts_ring_products<NT>(acc, sm, barA, barX, gq, &mapA, p, s, r0, mr, target)) return;
     }
     if (mode == 1) {
       // column-prescaled form: publish the strip of z_r = acc first (the others need only z) ...
@@ -452,7 +466,9 @@ __global__ void __launch_bounds__(kTsThreads, 1) trsm_skinny_kernel(TsParams p) 
 #pragma unroll
         for (int e = 0; e < 4; ++e) {
           const int row = 16 * warp + g + ((e >= 2) ? 8 : 0), col = 8 * nt + 2 * t + (e & 1);
-          if (nt < NT) accS[row + col * kTsLD] = acc[nt][e];
+          // rows past the strip hold products of stale stage rows: they are the
+          // product's zero K tail here
+          if (nt < NT) accS[row + col * kTsLD] = row < mr ? acc[nt][e] : 0.0;
           acc[nt][e] = 0.0;
         }
       __syncthreads();
@@ -497,9 +513,16 @@ int launch_trsm_skinny(cudaStream_t st, int bwd, int amode, int n, int nrhs, con
   p.strips = (p.mode != 0 && nb >= 32 && (n + nb - 1) / nb <= sm_count) ? 2 : 1;
   p.hs = p.strips == 1 ? nb : ((nb + 1) / 2 + 15) / 16 * 16;
   p.flags = flags; p.epoch = epoch; p.status = status;
+  // A's ring pieces: TMA boxes over the stored n x n matrix (see ts_tma_a)
+  CUtensorMap mapA;
+  const bool mok = amode == 0 ? make_tma_2d(&mapA, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, L, n, n, 8ull * lda,
+                                            (uint32_t)(p.hs + 4), kTsKC, false)
+                              : make_tma_2d(&mapA, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, L, n, n, 8ull * lda, kTsCT,
+                                            (uint32_t)p.hs, false);
+  if (!mok) return EGPU_ERR_UNSUPPORTED;
   const size_t smem = sizeof(double) * kTsSmemDoubles;
   const int nt = nrhs <= 8 ? 1 : nrhs <= 16 ? 2 : nrhs <= 32 ? 4 : 8;
-  void (*kern)(TsParams) = nt == 1 ? trsm_skinny_kernel<1>
+  void (*kern)(const CUtensorMap, TsParams) = nt == 1 ? trsm_skinny_kernel<1>
                            : nt == 2 ? trsm_skinny_kernel<2>
                            : nt == 4 ? trsm_skinny_kernel<4> : trsm_skinny_kernel<8>;
   static bool attr[4] = {false, false, false, false};
@@ -523,7 +546,7 @@ int launch_trsm_skinny(cudaStream_t st, int bwd, int amode, int n, int nrhs, con
   attr1[0].val.cooperative = 1;
   cfg.attrs = attr1;
   cfg.numAttrs = 1;
-  cudaError_t e = cudaLaunchKernelEx(&cfg, kern, p);
+  cudaError_t e = cudaLaunchKernelEx(&cfg, kern, mapA, p);
   count_launch();
   if (e != cudaSuccess) {
     set_last_error(e, "trsm_skinny launch", __FILE__, __LINE__);
