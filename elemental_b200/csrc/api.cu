@@ -532,11 +532,14 @@ int egpu_create(egpu_handle* out, int device) {
     int lo = 0, hi = 0;
     cudaDeviceGetStreamPriorityRange(&lo, &hi);  // hi = greatest priority
     bool ok = cudaStreamCreateWithPriority(&h->side, cudaStreamNonBlocking, hi) == cudaSuccess;
+    ok = ok && cudaStreamCreateWithPriority(&h->aux, cudaStreamNonBlocking, lo) == cudaSuccess;
+    ok = ok && cudaEventCreateWithFlags(&h->ev_aux, cudaEventDisableTiming) == cudaSuccess;
     ok = ok && cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming) == cudaSuccess;
     ok = ok && cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming) == cudaSuccess;
     for (int i = 0; i < 2; ++i) {
       ok = ok && cudaEventCreateWithFlags(&h->ev_panel[i], cudaEventDisableTiming) == cudaSuccess;
       ok = ok && cudaEventCreateWithFlags(&h->ev_rest[i], cudaEventDisableTiming) == cudaSuccess;
+      ok = ok && cudaEventCreateWithFlags(&h->ev_split[i], cudaEventDisableTiming) == cudaSuccess;
     }
     if (!ok) {
       set_last_error(cudaGetLastError(), "egpu_create streams", __FILE__, __LINE__);
@@ -559,9 +562,12 @@ int egpu_destroy(egpu_handle h) {
   if (h->dstatus) cudaFree(h->dstatus);
   if (h->hstatus) cudaFreeHost(h->hstatus);
   if (h->side) cudaStreamSynchronize(h->side);
-  for (cudaEvent_t e : {h->ev_fork, h->ev_join, h->ev_panel[0], h->ev_panel[1], h->ev_rest[0], h->ev_rest[1]})
+  if (h->aux) cudaStreamSynchronize(h->aux);
+  for (cudaEvent_t e : {h->ev_fork, h->ev_join, h->ev_panel[0], h->ev_panel[1], h->ev_rest[0], h->ev_rest[1],
+                        h->ev_split[0], h->ev_split[1], h->ev_aux})
     if (e) cudaEventDestroy(e);
   if (h->side) cudaStreamDestroy(h->side);
+  if (h->aux) cudaStreamDestroy(h->aux);
   if (h->own_stream) cudaStreamDestroy(h->own_stream);
   delete h;
   return EGPU_OK;

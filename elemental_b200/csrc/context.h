@@ -66,6 +66,10 @@ struct egpu_context {
   cudaStream_t side = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   cudaEvent_t ev_panel[2] = {nullptr, nullptr}, ev_rest[2] = {nullptr, nullptr};
+  // a lowest-priority stream for work that only fills idle SMs (the mixed
+  // path's prescaled solve copies), joined before its results are read
+  cudaStream_t aux = nullptr;
+  cudaEvent_t ev_split[2] = {nullptr, nullptr}, ev_aux = nullptr;
   int lookahead = 1;
   int async = 0;  // device API: enqueue only; status read by egpu_get_status
   int gmres_inner = 0;  // GMRES iterations of the last mixed solve

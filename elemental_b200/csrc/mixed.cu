@@ -443,7 +443,9 @@ int dposv_mixed_core_impl(egpu_context* h, int uplo, int n, int nrhs, const doub
     double* L21 = Lf + (k + b) + (long long)k * lds;
     TRY(launch_dgemm(s, false, false, m2, b, b, 1.0, L21, lds, Wk, nb, 0.0, L21, lds, 0, true, h->dstatus));
     const int par = (k / nb) & 1;
-    return launch_split_tf32(s, m2, b, L21, lds, PKh2[par], PKl2[par], L.ldk);
+    TRY(launch_split_tf32(s, m2, b, L21, lds, PKh2[par], PKl2[par], L.ldk));
+    if (prescale) EGPU_CUDA_TRY(cudaEventRecord(h->ev_split[par], s));  // L21 final: its M2 may start
+    return EGPU_OK;
   };
   EGPU_CUDA_TRY(cudaEventRecord(h->ev_fork, st));
   EGPU_CUDA_TRY(cudaStreamWaitEvent(sd, h->ev_fork, 0));
@@ -469,12 +471,20 @@ int dposv_mixed_core_impl(egpu_context* h, int uplo, int n, int nrhs, const doub
       TRY(launch_tc_gemm(st, m3, m3, b, -1.0f, PKh2[par] + (size_t)b2 * L.ldk, PKl2[par] + (size_t)b2 * L.ldk,
                          PKh2[par] + (size_t)b2 * L.ldk, PKl2[par] + (size_t)b2 * L.ldk, L.ldk, 1.0f,
                          A22 + b2 + (long long)b2 * ldf, ldf, 1, 3, h->dstatus));
-    // M2 of block column k for the solve sweeps, off the panel chain (the
-    // split of panel k, on the side stream, came before (a) above)
-    if (prescale) TRY(mixed_prescale_step(h, st, n, k, Lf, lds, Winv));
+    // M2 of block column k for the solve sweeps, on the lowest-priority
+    // stream: it needs only panel k's chain (split done) and fills SMs the
+    // updates and the chain leave idle
+    if (prescale) {
+      EGPU_CUDA_TRY(cudaStreamWaitEvent(h->aux, h->ev_split[par], 0));
+      TRY(mixed_prescale_step(h, h->aux, n, k, Lf, lds, Winv));
+    }
   }
   EGPU_CUDA_TRY(cudaEventRecord(h->ev_join, sd));
   EGPU_CUDA_TRY(cudaStreamWaitEvent(st, h->ev_join, 0));
+  if (prescale) {
+    EGPU_CUDA_TRY(cudaEventRecord(h->ev_aux, h->aux));
+    EGPU_CUDA_TRY(cudaStreamWaitEvent(st, h->ev_aux, 0));
+  }
 
   int info = 0;
   TRY(read_status_now(h, &info));

@@ -73,6 +73,11 @@ __global__ void __launch_bounds__(kDiagThreads) potrf_diag_kernel(double* A, lon
   __syncthreads();
   smem_trinv_dmma(S, bp, Xl, T);
   tri_store(S, W, ldw, b, UPLO != EGPU_LOWER, true);  // inv(U) = inv(L)^T
+  if (b < ldw)  // a short last block: the rest of its ldw x ldw slot is zero (whole-slot readers)
+    for (int e = tid; e < ldw * ldw; e += kDiagThreads) {
+      const int i = e % ldw, j = e / ldw;
+      if (i >= b || j >= b) W[i + (long long)j * ldw] = 0.0;
+    }
 }
 
 int launch_potrf_diag(cudaStream_t st, int uplo, double* A, long long lda, int b, double* W, int ldw,
