@@ -106,6 +106,13 @@ __device__ __forceinline__ void tma_prefetch_desc(const CUtensorMap* map) {
   asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(map)) : "memory");
 }
 
+// Round-to-nearest (ties away) FP32 -> TF32 (low 13 mantissa bits zero).
+__device__ __forceinline__ float tf32_rna(float x) {
+  uint32_t r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+  return __uint_as_float(r);
+}
+
 // ------------------------------------------------------------------ DMMA --
 // D = A(16x8) * B(8x8) + D, FP64 tensor-core MMA (legacy warp-level form;
 // tcgen05 has no f64 kind).

@@ -49,9 +49,13 @@ int launch_tc_gemm(cudaStream_t st, int M, int N, int K, float alpha, const floa
                    int terms, DevStatus* status);
 
 // X (rows x cols, column-major FP64) -> TF32 hi/lo parts in K-major rows
-// (hi[r*ldk + c]), columns cols..ldk-1 zero.
+// (hi[r*ldk + c], row stride ldk), columns cols..width-1 zero (width: ldk
+// when negative).
 int launch_split_tf32(cudaStream_t st, int rows, int cols, const double* X, long long ldx, float* hi, float* lo,
-                      long long ldk);
+                      long long ldk, int width = -1);
+// The same from a column-major FP32 X (width ldk).
+int launch_split_tf32_f32(cudaStream_t st, int rows, int cols, const float* X, long long ldx, float* hi, float* lo,
+                          long long ldk);
 
 // X := inv(T) X for nrhs <= 64 in one cooperative launch (trsm_skinny.cu:
 // amode/bwd select T from the stored triangle A, Winv the inverted diagonal
@@ -72,6 +76,13 @@ int launch_dgemm_skinny(cudaStream_t st, int M, int N, int K, double alpha, cons
 // Diagonal-block Cholesky (factor in place + triangular inverse into W).
 int launch_potrf_diag(cudaStream_t st, int uplo, double* A, long long lda, int b, double* W, int ldw,
                       DevStatus* status, int col_base, bool store_factor = true);
+// The mixed path's diagonal block: lower Cholesky of the FP32 b x b block at
+// Af (computed in FP64), its inverse into W (FP64, zero-padded ldw x ldw
+// slot) and the TF32 hi/lo split of that inverse in row-major 128 x ldk form
+// (Wh[j*ldk + k] = inv(L)[j][k], zero outside b x b): the K-major B operand
+// of L21 = A21 inv(L)^T on the tensor cores.
+int launch_potrf_diag_f32(cudaStream_t st, const float* Af, long long ldf, int b, double* W, int ldw, float* Wh,
+                          float* Wl, long long ldk, DevStatus* status, int col_base);
 
 // Batched triangular inverse of `count` diagonal blocks of size b (the last
 // one may be smaller: n total), block i at A + i*b*(lda+1), into W + i*b*ldw.

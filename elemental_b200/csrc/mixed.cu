@@ -50,33 +50,30 @@ __global__ void mixed_prepare_kernel(int uplo, int n, const double* A, long long
   }
 }
 
-// Lf[k+i, k+c] = Af[k+i, k+c] for the panel (rows i in [0, m), cols c in [0, b), lower part)
+// Lf[i, c] = Af[i, c] for the whole m x b block (a panel's L21)
 __global__ void widen_panel_kernel(int m, int b, const float* Af, long long ldf, double* Lf, long long ldl) {
   const int c = blockIdx.y;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x)
-    if (i >= c) Lf[i + (long long)c * ldl] = (double)Af[i + (long long)c * ldf];
+    Lf[i + (long long)c * ldl] = (double)Af[i + (long long)c * ldf];
 }
 
-__device__ __forceinline__ float tf32_rna(float x) {
-  uint32_t r;
-  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
-  return __uint_as_float(r);
-}
 
-// X (rows x cols, column-major FP64) -> hi/lo TF32 in K-major rows: hi[r*ldk + c]
-__global__ void split_tf32_kernel(int rows, int cols, const double* X, long long ldx, float* hi, float* lo,
-                                  long long ldk) {
+// X (rows x cols, column-major FP64 or FP32) -> hi/lo TF32 in K-major rows:
+// hi[r*ldk + c] for c < width (zero for c >= cols)
+template <typename T>
+__global__ void split_tf32_kernel(int rows, int cols, const T* X, long long ldx, float* hi, float* lo,
+                                  long long ldk, int width) {
   __shared__ double tile[32][33];
   const int r0 = blockIdx.x * 32, c0 = blockIdx.y * 32;
   const int tx = threadIdx.x, ty = threadIdx.y;
   for (int q = ty; q < 32; q += 8) {
     const int r = r0 + tx, c = c0 + q;
-    tile[q][tx] = (r < rows && c < cols) ? X[r + (long long)c * ldx] : 0.0;
+    tile[q][tx] = (r < rows && c < cols) ? (double)X[r + (long long)c * ldx] : 0.0;
   }
   __syncthreads();
   for (int q = ty; q < 32; q += 8) {
     const int r = r0 + q, c = c0 + tx;
-    if (r < rows && c < ldk) {
+    if (r < rows && c < width) {
       const double x = (c < cols) ? tile[tx][q] : 0.0;
       const float h = tf32_rna((float)x);
       hi[(long long)r * ldk + c] = h;
@@ -161,10 +158,21 @@ __global__ void col_scale_kernel(int n, const double* X, long long ldx, const do
 }  // namespace
 
 int launch_split_tf32(cudaStream_t st, int rows, int cols, const double* X, long long ldx, float* hi, float* lo,
-                      long long ldk) {
+                      long long ldk, int width) {
+  if (rows <= 0 || cols <= 0) return EGPU_OK;
+  if (width < 0) width = (int)ldk;
+  dim3 grid((rows + 31) / 32, (width + 31) / 32), block(32, 8);
+  split_tf32_kernel<double><<<grid, block, 0, st>>>(rows, cols, X, ldx, hi, lo, ldk, width);
+  count_launch();
+  EGPU_CUDA_TRY(cudaGetLastError());
+  return EGPU_OK;
+}
+
+int launch_split_tf32_f32(cudaStream_t st, int rows, int cols, const float* X, long long ldx, float* hi, float* lo,
+                          long long ldk) {
   if (rows <= 0 || cols <= 0) return EGPU_OK;
   dim3 grid((rows + 31) / 32, (int)((ldk + 31) / 32)), block(32, 8);
-  split_tf32_kernel<<<grid, block, 0, st>>>(rows, cols, X, ldx, hi, lo, ldk);
+  split_tf32_kernel<float><<<grid, block, 0, st>>>(rows, cols, X, ldx, hi, lo, ldk, (int)ldk);
   count_launch();
   EGPU_CUDA_TRY(cudaGetLastError());
   return EGPU_OK;
@@ -174,7 +182,7 @@ constexpr int kGmresRestart = 20;  // Krylov vectors per GMRES cycle
 
 // Workspace layout of the mixed solve.
 struct MixedLayout {
-  size_t as, af, lf, pkh, pkl, xw, r, yt, winv, norms, flags, gv, gw, gc, total;
+  size_t as, af, lf, pkh, pkl, wsh, wsl, xw, r, yt, winv, norms, flags, gv, gw, gc, total;
   long long lds, ldf, ldk;
 };
 
@@ -190,6 +198,8 @@ static MixedLayout mixed_layout(int n, int nrhs, int nb) {
   L.lf = take(sizeof(double) * L.lds * n);
   L.pkh = take(2 * sizeof(float) * (size_t)n * L.ldk);  // two buffers (look-ahead)
   L.pkl = take(2 * sizeof(float) * (size_t)n * L.ldk);
+  L.wsh = take(sizeof(float) * 128 * (size_t)L.ldk);  // TF32 split of the current diagonal inverse
+  L.wsl = take(sizeof(float) * 128 * (size_t)L.ldk);
   L.xw = take(sizeof(double) * L.lds * std::max(nrhs, 1));
   L.r = take(sizeof(double) * L.lds * std::max(nrhs, 1));
   L.yt = take(sizeof(double) * L.lds * std::max(nrhs, 1));
@@ -402,6 +412,8 @@ int dposv_mixed_core_impl(egpu_context* h, int uplo, int n, int nrhs, const doub
   double* Lf = reinterpret_cast<double*>(ws + L.lf);
   float* PKh = reinterpret_cast<float*>(ws + L.pkh);
   float* PKl = reinterpret_cast<float*>(ws + L.pkl);
+  float* Wsh = reinterpret_cast<float*>(ws + L.wsh);
+  float* Wsl = reinterpret_cast<float*>(ws + L.wsl);
   double* Xw = reinterpret_cast<double*>(ws + L.xw);
   double* R = reinterpret_cast<double*>(ws + L.r);
   double* Winv = reinterpret_cast<double*>(ws + L.winv);
@@ -411,83 +423,108 @@ int dposv_mixed_core_impl(egpu_context* h, int uplo, int n, int nrhs, const doub
   SweepFlags fl{reinterpret_cast<int*>(ws + L.flags), 0, prescale, reinterpret_cast<double*>(ws + L.yt)};
   EGPU_CUDA_TRY(cudaMemsetAsync(fl.flags, 0, trsm_skinny_flag_bytes(n, nb), st));
   const long long lds = L.lds, ldf = L.ldf;
-  EGPU_CUDA_TRY(cudaMemsetAsync(h->dstatus, 0, sizeof(DevStatus), st));
-  {
-    dim3 grid((n + 31) / 32, (n + 31) / 32), block(32, 8);
-    mixed_prepare_kernel<<<grid, block, 0, st>>>(uplo, n, A, lda, As, lds, Af, ldf);
-    count_launch();
-    EGPU_CUDA_TRY(cudaGetLastError());
-  }
-  // ---- factorization, look-ahead depth 1: the panel chain of step k+1
-  // (widen, diagonal block, L21, split) runs on the high-priority side stream
-  // as soon as the main stream has updated block column k+1; the rest of
-  // step k's trailing update follows on the main stream.  The split panel is
-  // double-buffered (step parity).
-  float* PKh2[2] = {PKh, PKh + (size_t)n * L.ldk};
-  float* PKl2[2] = {PKl, PKl + (size_t)n * L.ldk};
-  cudaStream_t sd = h->side;
-  auto panel_chain = [&](int k, cudaStream_t s) -> int {
-    const int b = std::min(nb, n - k);
-    const int m = n - k, m2 = m - b;
+  // The factorization: the fast form computes every panel's L21 on the
+  // tensor cores (TF32 x 3); `accurate` keeps L21 in FP64 (DMMA), a second
+  // attempt for matrices whose fast factorization meets a non-positive pivot.
+  auto factor = [&](bool accurate) -> int {
+    EGPU_CUDA_TRY(cudaMemsetAsync(h->dstatus, 0, sizeof(DevStatus), st));
     {
-      TraceMark tm(s, kTraceOther, 0.0, 12.0 * m * b);
-      dim3 grid((m + 255) / 256, b);
-      widen_panel_kernel<<<grid, 256, 0, s>>>(m, b, Af + k + (long long)k * ldf, ldf, Lf + k + (long long)k * lds, lds);
+      dim3 grid((n + 31) / 32, (n + 31) / 32), block(32, 8);
+      mixed_prepare_kernel<<<grid, block, 0, st>>>(uplo, n, A, lda, As, lds, Af, ldf);
       count_launch();
       EGPU_CUDA_TRY(cudaGetLastError());
     }
-    double* Wk = Winv + (size_t)(k / nb) * nb * nb;  // this block's inverse, kept for the solves
-    // the solves read only Winv and the off-diagonal blocks: L_kk itself is not stored
-    TRY(launch_potrf_diag(s, EGPU_LOWER, Lf + k + (long long)k * lds, lds, b, Wk, nb, h->dstatus, k, false));
-    if (m2 == 0) return EGPU_OK;
-    double* L21 = Lf + (k + b) + (long long)k * lds;
-    TRY(launch_dgemm(s, false, false, m2, b, b, 1.0, L21, lds, Wk, nb, 0.0, L21, lds, 0, true, h->dstatus));
-    const int par = (k / nb) & 1;
-    TRY(launch_split_tf32(s, m2, b, L21, lds, PKh2[par], PKl2[par], L.ldk));
-    if (prescale) EGPU_CUDA_TRY(cudaEventRecord(h->ev_split[par], s));  // L21 final: its M2 may start
-    return EGPU_OK;
-  };
-  EGPU_CUDA_TRY(cudaEventRecord(h->ev_fork, st));
-  EGPU_CUDA_TRY(cudaStreamWaitEvent(sd, h->ev_fork, 0));
-  TRY(panel_chain(0, sd));
-  for (int k = 0; k < n; k += nb) {
-    const int b = std::min(nb, n - k);
-    const int m2 = n - k - b;
-    const int par = (k / nb) & 1;
-    EGPU_CUDA_TRY(cudaEventRecord(h->ev_panel[par], sd));
-    if (m2 == 0) break;
-    EGPU_CUDA_TRY(cudaStreamWaitEvent(st, h->ev_panel[par], 0));
-    const int b2 = std::min(nb, m2);
-    float* A22 = Af + (k + b) + (long long)(k + b) * ldf;
-    // (a) block column k+1 (lower trapezoid m2 x b2)
-    TRY(launch_tc_gemm(st, m2, b2, b, -1.0f, PKh2[par], PKl2[par], PKh2[par], PKl2[par], L.ldk, 1.0f, A22, ldf, 1, 3,
-                       h->dstatus));
-    EGPU_CUDA_TRY(cudaEventRecord(h->ev_rest[par], st));
-    EGPU_CUDA_TRY(cudaStreamWaitEvent(sd, h->ev_rest[par], 0));
-    TRY(panel_chain(k + b, sd));
-    // (b) the rest of the trailing lower triangle
-    const int m3 = m2 - b2;
-    if (m3 > 0)
-      TRY(launch_tc_gemm(st, m3, m3, b, -1.0f, PKh2[par] + (size_t)b2 * L.ldk, PKl2[par] + (size_t)b2 * L.ldk,
-                         PKh2[par] + (size_t)b2 * L.ldk, PKl2[par] + (size_t)b2 * L.ldk, L.ldk, 1.0f,
-                         A22 + b2 + (long long)b2 * ldf, ldf, 1, 3, h->dstatus));
-    // M2 of block column k for the solve sweeps, on the lowest-priority
-    // stream: it needs only panel k's chain (split done) and fills SMs the
-    // updates and the chain leave idle
-    if (prescale) {
+    // ---- factorization, look-ahead depth 1: the panel chain of step k+1
+    // (diagonal block, L21, split) runs on the high-priority side stream
+    // as soon as the main stream has updated block column k+1; the rest of
+    // step k's trailing update follows on the main stream.  The split panel is
+    // double-buffered (step parity).
+    float* PKh2[2] = {PKh, PKh + (size_t)n * L.ldk};
+    float* PKl2[2] = {PKl, PKl + (size_t)n * L.ldk};
+    cudaStream_t sd = h->side;
+    // The panel chain, all on the TF32 x 3 tensor-core path except the
+    // diagonal block: the FP32 diagonal block is factored and inverted in FP64
+    // (inverse kept for the solves, its TF32 split for the next product), then
+    // L21 = A21 inv(L11)^T on the tensor cores, in place in the FP32 panel, and
+    // its TF32 split for the trailing updates.
+    auto panel_chain = [&](int k, cudaStream_t s) -> int {
+      const int b = std::min(nb, n - k);
+      const int m2 = n - k - b;
+      const int par = (k / nb) & 1;
+      double* Wk = Winv + (size_t)(k / nb) * nb * nb;
+      TRY(launch_potrf_diag_f32(s, Af + k + (long long)k * ldf, ldf, b, Wk, nb, Wsh, Wsl, L.ldk, h->dstatus, k));
+      if (m2 == 0) return EGPU_OK;
+      float* A21 = Af + (k + b) + (long long)k * ldf;
+      if (accurate) {  // L21 = A21 inv(L11)^T in FP64 (DMMA) from the widened panel
+        double* L21 = Lf + (k + b) + (long long)k * lds;
+        dim3 grid((m2 + 255) / 256, b);
+        widen_panel_kernel<<<grid, 256, 0, s>>>(m2, b, A21, ldf, L21, lds);
+        count_launch();
+        EGPU_CUDA_TRY(cudaGetLastError());
+        TRY(launch_dgemm(s, false, false, m2, b, b, 1.0, L21, lds, Wk, nb, 0.0, L21, lds, 0, true, h->dstatus));
+        TRY(launch_split_tf32(s, m2, b, L21, lds, PKh2[par], PKl2[par], L.ldk));
+      } else {
+        TRY(launch_split_tf32_f32(s, m2, b, A21, ldf, PKh2[par], PKl2[par], L.ldk));
+        TRY(launch_tc_gemm(s, m2, b, b, 1.0f, PKh2[par], PKl2[par], Wsh, Wsl, L.ldk, 0.0f, A21, ldf, 0, 3,
+                           h->dstatus));
+        TRY(launch_split_tf32_f32(s, m2, b, A21, ldf, PKh2[par], PKl2[par], L.ldk));
+      }
+      EGPU_CUDA_TRY(cudaEventRecord(h->ev_split[par], s));  // L21 final: its FP64 copy may start
+      return EGPU_OK;
+    };
+    // Off the chain, on the lowest-priority stream: the FP64 copy of panel k's
+    // L21 for the solves, and M2 in place over it when prescaled
+    auto l21_copy = [&](int k, int par) -> int {
+      const int b = std::min(nb, n - k), m2 = n - k - b;
+      if (m2 <= 0) return EGPU_OK;
       EGPU_CUDA_TRY(cudaStreamWaitEvent(h->aux, h->ev_split[par], 0));
-      TRY(mixed_prescale_step(h, h->aux, n, k, Lf, lds, Winv));
+      if (!accurate) {  // the FP32 panel holds L21
+        TraceMark tm(h->aux, kTraceOther, 0.0, 12.0 * m2 * b);
+        dim3 grid((m2 + 255) / 256, b);
+        widen_panel_kernel<<<grid, 256, 0, h->aux>>>(m2, b, Af + (k + b) + (long long)k * ldf, ldf,
+                                                     Lf + (k + b) + (long long)k * lds, lds);
+        count_launch();
+        EGPU_CUDA_TRY(cudaGetLastError());
+      }
+      if (prescale) TRY(mixed_prescale_step(h, h->aux, n, k, Lf, lds, Winv));
+      return EGPU_OK;
+    };
+    EGPU_CUDA_TRY(cudaEventRecord(h->ev_fork, st));
+    EGPU_CUDA_TRY(cudaStreamWaitEvent(sd, h->ev_fork, 0));
+    TRY(panel_chain(0, sd));
+    for (int k = 0; k < n; k += nb) {
+      const int b = std::min(nb, n - k);
+      const int m2 = n - k - b;
+      const int par = (k / nb) & 1;
+      EGPU_CUDA_TRY(cudaEventRecord(h->ev_panel[par], sd));
+      if (m2 == 0) break;
+      EGPU_CUDA_TRY(cudaStreamWaitEvent(st, h->ev_panel[par], 0));
+      const int b2 = std::min(nb, m2);
+      float* A22 = Af + (k + b) + (long long)(k + b) * ldf;
+      // (a) block column k+1 (lower trapezoid m2 x b2)
+      TRY(launch_tc_gemm(st, m2, b2, b, -1.0f, PKh2[par], PKl2[par], PKh2[par], PKl2[par], L.ldk, 1.0f, A22, ldf, 1, 3,
+                         h->dstatus));
+      EGPU_CUDA_TRY(cudaEventRecord(h->ev_rest[par], st));
+      EGPU_CUDA_TRY(cudaStreamWaitEvent(sd, h->ev_rest[par], 0));
+      TRY(panel_chain(k + b, sd));
+      // (b) the rest of the trailing lower triangle
+      const int m3 = m2 - b2;
+      if (m3 > 0)
+        TRY(launch_tc_gemm(st, m3, m3, b, -1.0f, PKh2[par] + (size_t)b2 * L.ldk, PKl2[par] + (size_t)b2 * L.ldk,
+                           PKh2[par] + (size_t)b2 * L.ldk, PKl2[par] + (size_t)b2 * L.ldk, L.ldk, 1.0f,
+                           A22 + b2 + (long long)b2 * ldf, ldf, 1, 3, h->dstatus));
+      TRY(l21_copy(k, par));
     }
-  }
-  EGPU_CUDA_TRY(cudaEventRecord(h->ev_join, sd));
-  EGPU_CUDA_TRY(cudaStreamWaitEvent(st, h->ev_join, 0));
-  if (prescale) {
+    EGPU_CUDA_TRY(cudaEventRecord(h->ev_join, sd));
+    EGPU_CUDA_TRY(cudaStreamWaitEvent(st, h->ev_join, 0));
     EGPU_CUDA_TRY(cudaEventRecord(h->ev_aux, h->aux));
     EGPU_CUDA_TRY(cudaStreamWaitEvent(st, h->ev_aux, 0));
-  }
 
-  int info = 0;
-  TRY(read_status_now(h, &info));
+    return read_status_now(h, nullptr);
+  };
+  int frc = factor(false);
+  if (frc == EGPU_NOT_HPD) frc = factor(true);
+  TRY(frc);  // the status word (pivot column) stays readable by the caller
   // ---- refinement
   {
     rowsum_abs_kernel<<<(n + 255) / 256, 256, 0, st>>>(n, As, lds, norms);
@@ -552,7 +589,7 @@ int dposv_mixed_core_impl(egpu_context* h, int uplo, int n, int nrhs, const doub
   EGPU_CUDA_TRY(cudaGetLastError());
   if (iters) *iters = it;
   if (berr) *berr = e;
-  TRY(read_status_now(h, &info));
+  TRY(read_status_now(h, nullptr));
   return e <= tol ? EGPU_OK : EGPU_NO_CONVERGENCE;
 }
 

@@ -80,6 +80,83 @@ __global__ void __launch_bounds__(kDiagThreads) potrf_diag_kernel(double* A, lon
     }
 }
 
+// The mixed path's diagonal block (lower): the FP32 block of the trailing
+// matrix, widened on load, factored and inverted in FP64 as above; the
+// inverse goes to W (FP64, for the solves) and, split into TF32 hi/lo rows,
+// to Wh/Wl (the B operand of the panel's L21 product on the tensor cores).
+__global__ void __launch_bounds__(kDiagThreads) potrf_diag_f32_kernel(const float* Af, long long ldf, int b,
+                                                                       double* W, int ldw, float* Wh, float* Wl,
+                                                                       long long ldk, DevStatus* st, int col_base) {
+  extern __shared__ double S[];
+  if (st != nullptr && st->code != 0) return;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  static_assert(kDiagThreads == 256, "a warp per 16 columns of the 128 x 128 block");
+  {  // lower triangle: warp w holds columns w, w + 8, ..; every load issued before any is used
+    float v[16][4];
+#pragma unroll
+    for (int u = 0; u < 16; ++u)
+#pragma unroll
+      for (int t = 0; t < 4; ++t) {
+        const int j = warp + 8 * u, i = lane + 32 * t;
+        v[u][t] = (j < b && i >= j && i < b) ? Af[i + (long long)j * ldf] : 0.0f;
+      }
+#pragma unroll
+    for (int u = 0; u < 16; ++u)
+#pragma unroll
+      for (int t = 0; t < 4; ++t) {
+        const int j = warp + 8 * u, i = lane + 32 * t;
+        if (j < b && i >= j && i < b) S[i + j * kLDS] = (double)v[u][t];
+      }
+  }
+  __syncthreads();
+  double* Xl = S + 128 * kLDS + 128;
+  double* T = Xl + 8 * 16 * kLeafLD;
+  const int bp = pad16_identity(S, b);
+  __syncthreads();
+  const int f = smem_chol_dmma(S, bp, Xl, T);
+  if (f) {
+    if (tid == 0) set_status(st, kNotHPD, col_base + f);
+    return;
+  }
+  __syncthreads();
+  smem_trinv_dmma(S, bp, Xl, T);
+  __syncthreads();
+  tri_store(S, W, ldw, b, false, true);
+  if (b < ldw)  // a short last block: the rest of its ldw x ldw slot is zero (whole-slot readers)
+    for (int e = tid; e < ldw * ldw; e += kDiagThreads) {
+      const int i = e % ldw, j = e / ldw;
+      if (i >= b || j >= b) W[i + (long long)j * ldw] = 0.0;
+    }
+  for (int j = warp; j < 128; j += kDiagThreads / 32) {  // row j of inv(L), a warp per row
+    float* wh = Wh + (long long)j * ldk;
+    float* wl = Wl + (long long)j * ldk;
+    for (int k = lane; k < (int)ldk; k += 32) {
+      const double v = (j < b && k <= j) ? S[j + k * kLDS] : 0.0;
+      const float hv = tf32_rna((float)v);
+      wh[k] = hv;
+      wl[k] = tf32_rna((float)(v - (double)hv));
+    }
+  }
+}
+
+int launch_potrf_diag_f32(cudaStream_t st, const float* Af, long long ldf, int b, double* W, int ldw, float* Wh,
+                          float* Wl, long long ldk, DevStatus* status, int col_base) {
+  if (b <= 0) return EGPU_OK;
+  if (b > kMaxNB || ldk < b) return EGPU_ERR_ARG;
+  TraceMark tm(st, kTraceDiag, (double)b * b * b / 3.0 * 2.0, 12.0 * b * b);
+  cudaError_t e = cudaFuncSetAttribute(potrf_diag_f32_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kDiagSmem);
+  if (e == cudaSuccess) {
+    potrf_diag_f32_kernel<<<1, kDiagThreads, kDiagSmem, st>>>(Af, ldf, b, W, ldw, Wh, Wl, ldk, status, col_base);
+    count_launch();
+    e = cudaGetLastError();
+  }
+  if (e != cudaSuccess) {
+    set_last_error(e, "potrf_diag_f32 launch", __FILE__, __LINE__);
+    return EGPU_ERR_CUDA;
+  }
+  return EGPU_OK;
+}
+
 int launch_potrf_diag(cudaStream_t st, int uplo, double* A, long long lda, int b, double* W, int ldw,
                       DevStatus* status, int col_base, bool store_factor) {
   if (b <= 0) return EGPU_OK;
