@@ -7,17 +7,14 @@
 //   bwd    : T is upper triangular (solve from the last block up)
 // so lower L x = b is (fwd, 0), L^T x = b is (bwd, 1), U^T x = b is (fwd, 1)
 // and U x = b is (bwd, 0).  Winv holds inv(A_rr) of every diagonal block
-// (transposed on use when amode is 1).
+// (transposed on use when amode is 1), each in a zero-padded nb x nb slot.
 //
-// Block rows of X (nb rows each) are owned round-robin by the CTAs; a CTA
-// processes its block rows in solve order, left-looking: acc = B_r -
-// sum_j T(r, j) X_j over the blocks j already solved, then X_r = inv(T_rr)
-// acc with the pre-inverted diagonal block, and publishes X_r with a release
-// flag.  Each off-diagonal block is read once, so the sweep streams the
-// triangle from HBM once while the dependency chain only waits on flags
-// (bounded spins), not on kernel boundaries.  The first chunk of each
-// off-diagonal block is requested before the wait for the X block it
-// multiplies.
+// Block rows of X (nb rows each, optionally split into two strips) are owned
+// by the CTAs in solve order, left-looking: acc = B_r - sum_j T(r, j) X_j
+// over the blocks j already solved, then X_r = inv(T_rr) acc, published with
+// a release counter.  Each off-diagonal block is read once, so the sweep
+// streams the triangle from HBM once while the dependency chain only waits
+// on counters (bounded spins), not on kernel boundaries.
 //
 // Column-prescaled form (mode 1): A holds the off-diagonal blocks already
 // multiplied by the inverse of the diagonal block of the column they act on,
@@ -27,39 +24,42 @@
 //
 // Row-prescaled form (mode 2): the blocks are M(r, j) = inv(T_rr) T(r, j), so
 // x_r = inv(T_rr) b_r - sum_j M(r, j) x_j: every task forms inv(T_rr) b_r
-// (b read from Y) before its first wait, and publishes x_r (in X) with no
-// inverse after the sum.  With M2 = L D^-1 stored, L y = b is the
+// (b read from Y) first, with no counter to wait for, and publishes x_r (in
+// X) with no inverse after the sum.  With M2 = L D^-1 stored, L y = b is the
 // column-prescaled sweep over M2 and L^T x = y the row-prescaled sweep over
 // M2^T (amode 1): inv(L_rr^T) L_jr^T = (L_jr inv(L_rr))^T = M2(j, r)^T.
 //
-// Products are 16 x 8 x 8 DMMA fragments from shared memory: the whole
-// off-diagonal block (ld 132, or its transpose with ld 132: conflict-free
-// fragment loads) and the matching X block, 16-byte cp.async copies in four
-// 32-deep groups that all are in flight at once.  Requires nrhs <= 64, nb <= 128 even, lda and ldx even,
-// A, Winv, X (and Y) 16-byte aligned.
+// Warp-specialized: every product (an off-diagonal block times X_j, or the
+// diagonal inverse times a block of X) streams through a ring of kTsStages
+// k chunks of 32.  A producer warp issues each chunk's A piece as one TMA box
+// (up to kTsStages chunks ahead) and its X piece as 16-byte copies once X_j
+// is published (it alone spins on the counters), both completing on the
+// stage's full barriers; eight consumer warps only wait, multiply (16 x 8 x 8
+// DMMA fragments from shared memory) and release the stage.  Requires
+// nrhs <= 64, nb <= 128 even, lda and ldx even, A, Winv, X (and Y) 16-byte
+// aligned.
 #include "internal.h"
 
 namespace egpu {
 
 namespace {
 
-constexpr int kTsThreads = 256;  // 8 warps: warp w owns rows 16w .. 16w+15 of the block
-constexpr int kTsKC = 32;        // k chunk (one cp.async group each)
-constexpr int kTsLD = 132;       // leading dimension of the staged blocks (conflict-free fragment loads)
+constexpr int kTsConsumers = 256;              // 8 warps: warp w owns rows 16w .. 16w+15 of the strip
+constexpr int kTsThreads = kTsConsumers + 32;  // + the producer warp
+constexpr int kTsKC = 32;                      // k chunk
 constexpr int kTsMaxRhs = 64;
-constexpr int kTsA = 128 * kTsLD;          // doubles: a whole off-diagonal block, [a + k*132] or [k + a*132]
-constexpr int kTsX = kTsMaxRhs * kTsLD;    // doubles: the matching X block, [k + c*132]
-// The off-diagonal products of a block row run through a ring of kTsStages
-// k chunks: stage = A chunk (amode 0: [a + k*132], amode 1: [k + a*36]) and
-// X chunk ([k + c*36]); ld 132 and 36 are both 4 mod 16 (conflict-free
-// 8-byte fragment loads).
+// A ring stage holds an A chunk (amode 0: [a + kl*(hs+4)], amode 1:
+// [kl + a*36]) and an X chunk ([kl + c*36]); both pitches are 4 mod 16
+// (conflict-free 8-byte fragment loads) and every stage starts on a
+// 128-byte boundary (TMA destination).
 constexpr int kTsStages = 4;
-constexpr int kTsCT = 36;                        // ld of the chunk-transposed layouts
-constexpr int kTsRA = 128 * kTsCT;               // doubles: A chunk (the larger of 32*132 and 128*36)
-constexpr int kTsRX = kTsMaxRhs * kTsCT;         // doubles: X chunk
+constexpr int kTsCT = 36;                 // pitch of the k-contiguous layouts
+constexpr int kTsRA = 128 * kTsCT;        // doubles: A chunk (>= 32 * 132 and 36 * 128)
+constexpr int kTsRX = kTsMaxRhs * kTsCT;  // doubles: X chunk
 constexpr int kTsRStage = kTsRA + kTsRX;
-constexpr int kTsSmemDoubles = (kTsA + kTsX) > kTsStages * kTsRStage ? (kTsA + kTsX) : kTsStages * kTsRStage;
-static_assert(32 * kTsLD <= kTsRA, "A chunk fits its stage");
+constexpr int kTsSmemDoubles = kTsStages * kTsRStage;
+static_assert(32 * 132 <= kTsRA, "A chunk fits its stage");
+static_assert((kTsRStage * 8) % 128 == 0 && (kTsRA * 8) % 128 == 0, "stage starts are 128-byte aligned");
 
 struct TsParams {
   const double* L;
@@ -70,7 +70,7 @@ struct TsParams {
   double* Y;  // mode 1: Y_r = inv(T_rr) z_r (z published in X); mode 2: the right-hand side (X receives x)
   int n, nrhs, nb, nblk, bwd, amode;
   int mode;        // 0 plain, 1 column-prescaled, 2 row-prescaled
-  int strips, hs;  // tasks per block row and their height (prescaled form: 2)
+  int strips, hs;  // tasks per block row and their height
   int* flags;
   int epoch;
   DevStatus* status;
@@ -79,415 +79,316 @@ struct TsParams {
 // block row of solve step s
 __device__ __forceinline__ int ts_block(const TsParams& p, int s) { return p.bwd ? p.nblk - 1 - s : s; }
 
-// Stage the k chunk [k0, k0+32) of an m x K operand A (m <= 128 rows) into
-// the whole-block buffer with 16-byte .cg copies.  amode 0: A(a, k) =
-// G[a + k lda] (column-major block), kept as sA[a + k * 132]; amode 1:
-// A(a, k) = G[k + a lda] (the transpose of a column-major block), kept as
-// sA[k + a * 132].  Out-of-range entries are zero.  lda even, G 16-byte
-// aligned, k0 even.
-__device__ __forceinline__ void ts_stage_a(double* sA, const double* G, long long lda, int amode, int m, int K,
-                                           int k0) {
-  const int tid = threadIdx.x;
-  if (amode == 0) {
-    for (int e = tid; e < 64 * kTsKC; e += kTsThreads) {  // row pairs
-      const int a = 2 * (e & 63), k = k0 + (e >> 6);
-      double* d = &sA[a + k * kTsLD];
-      const double* src = &G[a + (long long)k * lda];
-      if (k < K && a + 1 < m) cp_async16_cg(d, src);
-      else {
-        d[0] = (k < K && a < m) ? src[0] : 0.0;
-        d[1] = 0.0;
-      }
-    }
+// One task: strip q of the block row r solved at step s.
+struct TsTask {
+  int s, q, r, rb0, mb, r0, mr;
+};
+__device__ __forceinline__ TsTask ts_task(const TsParams& p, int task) {
+  TsTask t;
+  t.s = task / p.strips;
+  t.q = task - t.s * p.strips;
+  t.r = ts_block(p, t.s);
+  t.rb0 = t.r * p.nb;
+  t.mb = min(p.nb, p.n - t.rb0);
+  t.r0 = t.rb0 + t.q * p.hs;
+  t.mr = min(p.hs, t.mb - t.q * p.hs);  // may be empty
+  return t;
+}
+
+// Product pi of a task: the s off-diagonal products (solve steps, sign -1)
+// and one diagonal product inv(T_rr)(strip rows, :) times a block of X (sign
+// +1): last in modes 0 and 1, first in mode 2.  Its X: block j of X
+// (counter j), the staged accumulator (mode 0), z_r (mode 1: counter r, all
+// strips) or b_r from Y (mode 2, no counter).
+struct TsProd {
+  int step;            // off-diagonal solve step, or -1 for the diagonal product
+  int j0, K;           // first row of the X block, its height
+  const double* xsrc;  // X block (global), or null: staged by the consumers
+  const int* flag;     // counter to wait for, or null
+};
+__device__ __forceinline__ TsProd ts_prod(const TsParams& p, const TsTask& t, int pi) {
+  TsProd d;
+  const bool diag = p.mode == 2 ? pi == 0 : pi == t.s;
+  d.step = diag ? -1 : (p.mode == 2 ? pi - 1 : pi);
+  if (!diag) {
+    const int j = ts_block(p, d.step);
+    d.j0 = j * p.nb;
+    d.K = min(p.nb, p.n - d.j0);
+    d.xsrc = p.X + d.j0;
+    d.flag = &p.flags[j];
   } else {
-    for (int e = tid; e < 128 * (kTsKC / 2); e += kTsThreads) {  // k pairs
-      const int k = k0 + 2 * (e & 15), a = e >> 4;
-      double* d = &sA[k + a * kTsLD];
-      const double* src = &G[k + (long long)a * lda];
-      if (a < m && k + 1 < K) cp_async16_cg(d, src);
-      else {
-        d[0] = (a < m && k < K) ? src[0] : 0.0;
-        d[1] = 0.0;
-      }
-    }
+    d.j0 = t.rb0;
+    d.K = t.mb;
+    d.xsrc = p.mode == 0 ? nullptr : (p.mode == 1 ? p.X : p.Y) + t.rb0;
+    d.flag = p.mode == 1 ? &p.flags[t.r] : nullptr;
   }
+  return d;
 }
 
-// The matching rows [k0, k0+32) of X (K x nrhs) into sX[k + c * 132]:
-// 16-byte .cg copies (L2, never a stale L1 line of a block another CTA has
-// just published); ldx even and X 16-byte aligned.
-__device__ __forceinline__ void ts_stage_x(double* sX, int K, int k0, const double* Xg, long long ldx, int nrhs) {
-  for (int e = threadIdx.x; e < (kTsKC / 2) * nrhs; e += kTsThreads) {
-    const int k = k0 + 2 * (e & 15), c = e >> 4;
-    double* d = &sX[k + c * kTsLD];
-    const double* src = &Xg[k + (long long)c * ldx];
-    if (k + 1 < K) {
-      cp_async16_cg(d, src);
-    } else {
-      d[0] = (k < K) ? __ldcg(src) : 0.0;
-      d[1] = 0.0;
-    }
+// Bounded wait on an mbarrier phase for the chunk pipeline: spins (the
+// try_wait itself suspends briefly) before it starts to sleep.
+__device__ __forceinline__ bool ts_mbar_wait(uint64_t* bar, uint32_t parity) {
+  for (long long it = 0; it < kSpinLimit; ++it) {
+    if (mbar_try_wait(bar, parity)) return true;
+    if (it > 4096) __nanosleep(64);
   }
-}
-
-__device__ __forceinline__ void ts_wait_groups(int pending) {
-  switch (pending) {  // cp.async.wait_group takes an immediate
-    case 0: asm volatile("cp.async.wait_group 0;" ::: "memory"); break;
-    case 1: asm volatile("cp.async.wait_group 1;" ::: "memory"); break;
-    case 2: asm volatile("cp.async.wait_group 2;" ::: "memory"); break;
-    default: asm volatile("cp.async.wait_group 3;" ::: "memory"); break;
-  }
-}
-
-// Bounded wait (thread 0) for the arrival counter *flag to reach `epoch`
-// (strips x sweep number), then a CTA barrier.  Returns
-// false (all threads) when the wait ran out.
-__device__ __forceinline__ bool ts_wait_flag(const int* flag, int epoch, DevStatus* status) {
-  __shared__ int s_ok;
-  if (threadIdx.x == 0) {
-    int ok = 1;
-    long long it = 0;
-    while (true) {
-      int v;
-      asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(flag) : "memory");
-      if (v >= epoch) break;
-      if (++it > kSpinLimit) { ok = 0; set_status(status, kTimeout, 201); break; }
-      if (it > 4096) __nanosleep(64);
-    }
-    s_ok = ok;
-  }
-  __syncthreads();
-  return s_ok != 0;
-}
-
-// Chunk [k0, k0+32) of the strip's A operand into a ring stage: one TMA box
-// issued by thread 0, completing on `bar`.  amode 0: the box is rows r0 ..
-// r0+hs+3 x columns j0+k0 .. +31 of the stored matrix, landing as
-// sA[a + kl*(hs+4)]; amode 1: rows j0+k0 .. +35 x columns r0 .. r0+hs-1,
-// landing as sA[kl + a*36].  Both pitches are 4 mod 16 (conflict-free
-// fragment loads); the extra rows are read and ignored, and the parts of the
-// box past the matrix (a short last block) arrive as zeros.
-__device__ __forceinline__ void ts_tma_a(double* sA, const CUtensorMap* map, const TsParams& p, int r0, int j0,
-                                         int k0, uint64_t* bar) {
-  if (threadIdx.x != 0) return;
-  const uint32_t bytes = p.amode == 0 ? (uint32_t)((p.hs + 4) * kTsKC * 8) : (uint32_t)(kTsCT * p.hs * 8);
-  mbar_expect_tx(bar, bytes);
-  if (p.amode == 0) tma_load_2d(sA, map, bar, r0, j0 + k0);
-  else tma_load_2d(sA, map, bar, j0 + k0, r0);
-}
-
-// Rows [k0, k0+32) of X (K x nrhs) into a ring stage, sX[kl + c*36]: 16-byte
-// .cg copies by every thread (X was published by other CTAs and acquired
-// through a flag: read through L2 in the generic proxy), each thread's copies
-// arriving on `bar` (initial count: the block size).  Rows past K are zero.
-__device__ __forceinline__ void ts_async_x(double* sX, int K, int k0, const double* Xg, long long ldx, int nrhs,
-                                           uint64_t* bar) {
-  for (int e = threadIdx.x; e < (kTsKC / 2) * nrhs; e += kTsThreads) {
-    const int kl = 2 * (e & 15), c = e >> 4, k = k0 + kl;
-    double* dd = &sX[kl + c * kTsCT];
-    const double* src = &Xg[k + (long long)c * ldx];
-    if (k + 1 < K) {
-      cp_async16_cg(dd, src);
-    } else {
-      dd[0] = (k < K) ? __ldcg(src) : 0.0;
-      dd[1] = 0.0;
-    }
-  }
-  cp_async_arrive_noinc(bar);
-}
-
-// Error exit: wait (bounded) for the copies of every piece already issued,
-// chunks [from, a_end) of A and [from, x_end) of X, so no copy still targets
-// this CTA's shared memory when it returns.
-__device__ __forceinline__ void ts_ring_drain(uint64_t* barA, uint64_t* barX, int gq, int from, int a_end, int x_end) {
-  for (int q = from; q < a_end; ++q)
-    (void)mbar_wait_bounded(&barA[(gq + q) % kTsStages], (uint32_t)((gq + q) / kTsStages) & 1u);
-  for (int q = from; q < x_end; ++q)
-    (void)mbar_wait_bounded(&barX[(gq + q) % kTsStages], (uint32_t)((gq + q) / kTsStages) & 1u);
-}
-
-// Both pieces of ring chunk `gq` (this CTA's running chunk count) landed:
-// every thread waits on the stage's two mbarrier phases (bounded).
-__device__ __forceinline__ bool ts_ring_wait(uint64_t* barA, uint64_t* barX, int gq, DevStatus* status) {
-  const int slot = gq % kTsStages;
-  const uint32_t par = (uint32_t)(gq / kTsStages) & 1u;
-  if (mbar_wait_bounded(&barA[slot], par) && mbar_wait_bounded(&barX[slot], par)) return true;
-  set_status(status, kTimeout, 202);
   return false;
 }
 
-// acc -= sum over solve steps sj < s of T(strip, j) X_j (j = the block row of
-// step sj): every product's k chunks stream through the kTsStages-deep ring
-// as one sequence, so the loads of the next chunks (and of the next product)
-// overlap the DMMAs of the current one.  A pieces are single TMA boxes
-// (thread 0) issued up to kTsStages chunks ahead with no flag; X pieces are
-// small copies by every thread once X_j is published:
-// a poll that runs behind the DMMAs while loaded chunks remain, a bounded
-// wait when nothing else is left.  gq: the CTA's running chunk count (the
-// stage mbarriers' phases).  Returns false when a wait ran out.
-template <int NT>
-__device__ bool ts_ring_products(double (&acc)[8][4], double* sm, uint64_t* barA, uint64_t* barX, int& gq,
-                                 const CUtensorMap* mapA, const TsParams& p, int s, int r0, int mr, int target) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int g = lane >> 2, t = lane & 3;
-  const int cpp = (p.nb + kTsKC - 1) / kTsKC;  // chunks per product
-  const int Q = s * cpp;
-  int a_issued = 0, x_issued = 0, ready = 0;
-  int pv_prev = 0, pidx_prev = -1;  // the previous chunk's poll (thread 0)
-  if (threadIdx.x == 0) fence_proxy_async_smem();  // the stages were last written in the generic proxy
-  const int ldA = p.amode == 0 ? p.hs + 4 : kTsCT;  // A stage pitch
-  for (int qc = 0; qc < Q; ++qc) {
-    // X pieces first (they gate the next chunks)
-    for (; x_issued < Q && x_issued < qc + kTsStages; ++x_issued) {
-      const int sj = x_issued / cpp, c = x_issued - sj * cpp;
-      const int j = ts_block(p, sj), j0 = j * p.nb, mj = min(p.nb, p.n - j0);
-      if (sj >= ready) {
-        if (x_issued > qc) break;  // loaded chunks remain: the poll below runs behind them
-        if (!ts_wait_flag(&p.flags[j], target, p.status)) {
-          ts_ring_drain(barA, barX, gq, qc, a_issued, x_issued);
-          return false;
-        }
-        ready = sj + 1;
-      }
-      const int sl = (gq + x_issued) % kTsStages;
-      ts_async_x(sm + sl * kTsRStage + kTsRA, mj, c * kTsKC, p.X + j0, p.ldx, p.nrhs, &barX[sl]);
-    }
-    // A pieces (no flag) up to kTsStages chunks ahead
-    for (; a_issued < Q && a_issued < qc + kTsStages; ++a_issued) {
-      const int sj = a_issued / cpp, c = a_issued - sj * cpp;
-      const int sl = (gq + a_issued) % kTsStages;
-      ts_tma_a(sm + sl * kTsRStage, mapA, p, r0, ts_block(p, sj) * p.nb, c * kTsKC, &barA[sl]);
-    }
-    // poll for the first product not yet known published: a relaxed load
-    // issued now and read at the next chunk's closing barrier, so its round
-    // trip hides behind the DMMAs
-    int pv = 0;
-    const int pidx = ready < s ? ready : -1;
-    if (pidx >= 0 && threadIdx.x == 0)
-      asm volatile("ld.relaxed.gpu.global.s32 %0, [%1];" : "=r"(pv) : "l"(&p.flags[ts_block(p, pidx)]) : "memory");
-    const int slot = (gq + qc) % kTsStages;
-    if (!ts_ring_wait(barA, barX, gq + qc, p.status)) {
-      ts_ring_drain(barA, barX, gq, qc + 1, a_issued, x_issued);
-      return false;
-    }
-    __syncthreads();  // the X pieces' ordinary-store parts (zero rows) are visible
-    const int sj = qc / cpp, c = qc - sj * cpp;
-    const int mj = min(p.nb, p.n - ts_block(p, sj) * p.nb);
-    if (c * kTsKC < mj && 16 * warp < mr) {
-      const double* sA = sm + slot * kTsRStage;
-      const double* sX = sA + kTsRA;
-      const int ra = 16 * warp + g;
-#pragma unroll
-      for (int kk = 0; kk < kTsKC; kk += 8) {
-        double a[4];
-        if (p.amode == 0) {
-          a[0] = -sA[ra + (kk + t) * ldA];
-          a[1] = -sA[ra + 8 + (kk + t) * ldA];
-          a[2] = -sA[ra + (kk + t + 4) * ldA];
-          a[3] = -sA[ra + 8 + (kk + t + 4) * ldA];
-        } else {
-          a[0] = -sA[(kk + t) + ra * kTsCT];
-          a[1] = -sA[(kk + t) + (ra + 8) * kTsCT];
-          a[2] = -sA[(kk + t + 4) + ra * kTsCT];
-          a[3] = -sA[(kk + t + 4) + (ra + 8) * kTsCT];
-        }
-#pragma unroll
-        for (int nt = 0; nt < NT; ++nt) {
-          double bf[2];
-          bf[0] = sX[(kk + t) + (8 * nt + g) * kTsCT];
-          bf[1] = sX[(kk + t + 4) + (8 * nt + g) * kTsCT];
-          dmma_16x8x8(acc[nt], a, bf);
-        }
-      }
-    }
-    // the stage is free for chunk qc + kTsStages; the previous chunk's poll
-    // answer, made an acquire by thread 0's fence before the barrier that
-    // publishes it
-    int seen = 0;
-    if (threadIdx.x == 0 && pidx_prev >= 0 && pidx_prev == ready && pv_prev >= target) {
-      asm volatile("fence.acq_rel.gpu;" ::: "memory");
-      seen = 1;
-    }
-    if (__syncthreads_or(seen)) ready = ready + 1;
-    pv_prev = pv;
-    pidx_prev = pidx;
-  }
-  gq += Q;
-  return true;
-}
-
-// acc[nt] (16 x 8 fragments, rows 16 warp.., columns 8 nt..) += sign * A(m x K) * X(K x nrhs), K <= 128.
-// Every chunk of A is requested at once (one cp.async group each) before the
-// wait for X to be published (`flag`), then every chunk of X, so one product
-// costs one memory round trip plus its DMMAs.  x_in_smem: X already sits in
-// the X buffer (the staged accumulator).
-template <int NT>
-__device__ bool ts_product(double (&acc)[8][4], double sign, double* sm, const double* G, long long lda, int amode,
-                           int m, int K, const double* Xg, long long ldx, int nrhs, bool x_in_smem,
-                           const int* flag = nullptr, int epoch = 0, DevStatus* status = nullptr) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int g = lane >> 2, t = lane & 3;
-  const int nch = (K + kTsKC - 1) / kTsKC;
-  double* sA = sm;
-  double* sX = sm + kTsA;
-  for (int c = 0; c < nch; ++c) {
-    ts_stage_a(sA, G, lda, amode, m, K, c * kTsKC);
-    asm volatile("cp.async.commit_group;" ::: "memory");
-  }
-  if (flag != nullptr && !ts_wait_flag(flag, epoch, status)) {
-    asm volatile("cp.async.wait_group 0;" ::: "memory");
-    return false;
-  }
-  if (!x_in_smem)
-    for (int c = 0; c < nch; ++c) {
-      ts_stage_x(sX, K, c * kTsKC, Xg, ldx, nrhs);
-      asm volatile("cp.async.commit_group;" ::: "memory");
-    }
-  for (int c = 0; c < nch; ++c) {
-    ts_wait_groups(nch - 1 - c);  // A chunk c (and X chunk c) landed for this thread
-    __syncthreads();
-#pragma unroll
-    for (int kk = 0; kk < kTsKC; kk += 8) {
-      const int k = c * kTsKC + kk;
-      double a[4];
-      const int ra = 16 * warp + g;
-      if (amode == 0) {
-        a[0] = sA[ra + (k + t) * kTsLD];
-        a[1] = sA[ra + 8 + (k + t) * kTsLD];
-        a[2] = sA[ra + (k + t + 4) * kTsLD];
-        a[3] = sA[ra + 8 + (k + t + 4) * kTsLD];
-      } else {
-        a[0] = sA[(k + t) + ra * kTsLD];
-        a[1] = sA[(k + t) + (ra + 8) * kTsLD];
-        a[2] = sA[(k + t + 4) + ra * kTsLD];
-        a[3] = sA[(k + t + 4) + (ra + 8) * kTsLD];
-      }
-#pragma unroll
-      for (int q = 0; q < 4; ++q) a[q] *= sign;
-#pragma unroll
-      for (int nt = 0; nt < NT; ++nt) {
-        double bf[2];
-        bf[0] = sX[(k + t) + (8 * nt + g) * kTsLD];
-        bf[1] = sX[(k + t + 4) + (8 * nt + g) * kTsLD];
-        dmma_16x8x8(acc[nt], a, bf);
-      }
-    }
-  }
-  __syncthreads();  // the buffers are free for the next product
-  return true;
-}
+// Consumers only (warps 0..7): named barrier 1.
+__device__ __forceinline__ void ts_consumer_sync() { asm volatile("bar.sync 1, %0;" ::"n"(kTsConsumers) : "memory"); }
 
 }  // namespace
+
+// Barrier counts: fullA completes on thread 0's expect_tx arrival plus the
+// TMA bytes; fullX on two arrivals per producer lane (its copies' completion,
+// and an ordinary release arrival covering its zero stores); empty on one
+// arrival per consumer warp.
+constexpr uint32_t kTsFullXCount = 64;
+constexpr uint32_t kTsEmptyCount = kTsConsumers / 32;
+
+// The producer warp: every chunk of every product of this CTA's tasks, A
+// pieces up to kTsStages chunks ahead of the X pieces (a stage is reused
+// once its consumers released it), X pieces once their block is published.
+// Nothing here blocks: the loop polls stage releases and counters and idles
+// (bounded) only when neither moves.
+__device__ void ts_producer(const CUtensorMap* mapL, const CUtensorMap* mapW, const TsParams& p, double* sm,
+                            uint64_t* fullA, uint64_t* fullX, uint64_t* empty) {
+  const int lane = threadIdx.x & 31;
+  const int cpp = (p.nb + kTsKC - 1) / kTsKC;  // chunks per product
+  const int target = p.strips * p.epoch;
+  const uint32_t a_bytes = p.amode == 0 ? (uint32_t)((p.hs + 4) * kTsKC * 8) : (uint32_t)(kTsCT * p.hs * 8);
+  if (lane == 0) {
+    tma_prefetch_desc(mapL);
+    tma_prefetch_desc(mapW);
+  }
+  int gq = 0;  // chunks of this CTA so far
+  for (int task = blockIdx.x; task < p.nblk * p.strips; task += gridDim.x) {
+    const TsTask t = ts_task(p, task);
+    if (t.mr <= 0) continue;
+    const int Q = (t.s + 1) * cpp;
+    int a_next = 0, x_next = 0, known = -1;
+    long long idle = 0;
+    // one polling loop: A pieces whose stage is free (tested, never waited
+    // for), and the next X piece as soon as its stage is ours and its block
+    // is published, so no X piece queues behind a stage release
+    while (x_next < Q) {
+      bool progress = false;
+      while (a_next < Q && a_next < x_next + kTsStages) {
+        const int g = gq + a_next, slot = g % kTsStages;
+        if (g >= kTsStages) {  // lane 0's test decides for the warp
+          const int freed = mbar_test(&empty[slot], ((uint32_t)(g / kTsStages) & 1u) ^ 1u);
+          if (!__shfl_sync(0xffffffffu, freed, 0)) break;
+        }
+        if (lane == 0) {
+          const int pi = a_next / cpp, k0 = (a_next - pi * cpp) * kTsKC;
+          const TsProd d = ts_prod(p, t, pi);
+          double* sA = sm + slot * kTsRStage;
+          mbar_expect_tx(&fullA[slot], a_bytes);
+          if (d.step >= 0) {  // rows of the strip x columns of block j of the stored matrix (or its transpose)
+            if (p.amode == 0) tma_load_2d(sA, mapL, &fullA[slot], t.r0, d.j0 + k0);
+            else tma_load_2d(sA, mapL, &fullA[slot], d.j0 + k0, t.r0);
+          } else {  // the strip's rows of inv(T_rr): slot r of the Winv tensor (columns r*nb ..)
+            const int wc = t.r * p.nb;
+            if (p.amode == 0) tma_load_2d(sA, mapW, &fullA[slot], t.q * p.hs, wc + k0);
+            else tma_load_2d(sA, mapW, &fullA[slot], k0, wc + t.q * p.hs);
+          }
+        }
+        ++a_next;
+        progress = true;
+      }
+      while (x_next < a_next) {  // X pieces whose stage holds their A piece
+        const int pi = x_next / cpp, c = x_next - pi * cpp;
+        const TsProd d = ts_prod(p, t, pi);
+        if (d.xsrc != nullptr && d.flag != nullptr && known != pi) {
+          int v = 0;
+          if (lane == 0) asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(d.flag) : "memory");
+          v = __shfl_sync(0xffffffffu, v, 0);  // lane 0's acquire, then every lane's copies
+          if (v < target) break;
+          known = pi;
+        }
+        const int slot = (gq + x_next) % kTsStages;
+        if (d.xsrc != nullptr) {
+          double* sX = sm + slot * kTsRStage + kTsRA;
+          const int k0 = c * kTsKC;
+          for (int e = lane; e < (kTsKC / 2) * p.nrhs; e += 32) {
+            const int kl = 2 * (e & 15), col = e >> 4, k = k0 + kl;
+            double* dd = &sX[kl + col * kTsCT];
+            const double* src = &d.xsrc[k + (long long)col * p.ldx];
+            if (k + 1 < d.K) {
+              cp_async16_cg(dd, src);
+            } else {
+              dd[0] = (k < d.K) ? __ldcg(src) : 0.0;
+              dd[1] = 0.0;
+            }
+          }
+        }
+        // staged pieces (written by the consumers) still complete the phase
+        cp_async_arrive_noinc(&fullX[slot]);
+        asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&fullX[slot])) : "memory");
+        ++x_next;
+        progress = true;
+      }
+      if (progress) {
+        idle = 0;
+      } else if (++idle > kSpinLimit) {
+        if (lane == 0) set_status(p.status, kTimeout, 212);
+        return;
+      } else if (idle > 4096) {
+        __nanosleep(64);
+      }
+    }
+    gq += Q;
+  }
+}
+
+// The consumer warps: acc for the task's strip through all its products,
+// then the store and the release of the block's counter.
+template <int NT>
+__device__ void ts_consumers(const TsParams& p, double* sm, uint64_t* fullA, uint64_t* fullX, uint64_t* empty) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int g8 = lane >> 2, t4 = lane & 3;
+  const int cpp = (p.nb + kTsKC - 1) / kTsKC;
+  const int ldA = p.amode == 0 ? p.hs + 4 : kTsCT;  // A stage pitch
+  int gq = 0;
+  for (int task = blockIdx.x; task < p.nblk * p.strips; task += gridDim.x) {
+    const TsTask t = ts_task(p, task);
+    double acc[NT][4];
+#pragma unroll
+    for (int nt = 0; nt < NT; ++nt)
+#pragma unroll
+      for (int e = 0; e < 4; ++e) acc[nt][e] = 0.0;
+    if (t.mr > 0) {
+      if (p.mode != 2) {  // acc = B(strip)
+#pragma unroll
+        for (int nt = 0; nt < NT; ++nt)
+#pragma unroll
+          for (int e = 0; e < 4; ++e) {
+            const int row = 16 * warp + g8 + ((e >= 2) ? 8 : 0), col = 8 * nt + 2 * t4 + (e & 1);
+            if (row < t.mr && col < p.nrhs) acc[nt][e] = __ldcg(&p.X[(t.r0 + row) + (long long)col * p.ldx]);
+          }
+      }
+      const int P = t.s + 1;
+      for (int pi = 0; pi < P; ++pi) {
+        const TsProd d = ts_prod(p, t, pi);
+        if (d.step < 0 && p.mode == 1) {
+          // column-prescaled form: publish the strip of z_r = acc (the other
+          // tasks need only z), then Y(strip) = inv(T_rr)(strip, :) z_r
+#pragma unroll
+          for (int nt = 0; nt < NT; ++nt)
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+              const int row = 16 * warp + g8 + ((e >= 2) ? 8 : 0), col = 8 * nt + 2 * t4 + (e & 1);
+              if (row < t.mr && col < p.nrhs) p.X[(t.r0 + row) + (long long)col * p.ldx] = acc[nt][e];
+              acc[nt][e] = 0.0;
+            }
+          ts_consumer_sync();  // the consumers' stores happen before thread 0's (cumulative) release
+          if (tid == 0) asm volatile("red.release.gpu.global.add.s32 [%0], 1;" ::"l"(&p.flags[t.r]) : "memory");
+        }
+        if (d.xsrc == nullptr) {
+          // plain form: X_r = inv(T_rr) acc; the accumulator is the product's
+          // X, staged in the X slots of its chunks (row k in the slot of
+          // chunk k / 32; rows past the strip are the zero K tail) once every
+          // consumer is done with the earlier chunks
+          ts_consumer_sync();
+          const int gd = gq + pi * cpp;
+#pragma unroll
+          for (int nt = 0; nt < NT; ++nt)
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+              const int row = 16 * warp + g8 + ((e >= 2) ? 8 : 0), col = 8 * nt + 2 * t4 + (e & 1);
+              double* sXr = sm + ((gd + row / kTsKC) % kTsStages) * kTsRStage + kTsRA;
+              sXr[(row % kTsKC) + col * kTsCT] = row < t.mr ? acc[nt][e] : 0.0;
+              acc[nt][e] = 0.0;
+            }
+          ts_consumer_sync();
+        }
+        const double sgn = d.step >= 0 ? -1.0 : 1.0;
+        for (int c = 0; c < cpp; ++c) {
+          const int g = gq + pi * cpp + c, slot = g % kTsStages;
+          const uint32_t par = (uint32_t)(g / kTsStages) & 1u;
+          if (!ts_mbar_wait(&fullA[slot], par) || !ts_mbar_wait(&fullX[slot], par)) {
+            if (lane == 0) set_status(p.status, kTimeout, 213);
+            return;
+          }
+          if (c * kTsKC < d.K && 16 * warp < t.mr) {
+            const double* sA = sm + slot * kTsRStage;
+            const double* sX = sA + kTsRA;
+            const int ra = 16 * warp + g8;
+#pragma unroll
+            for (int kk = 0; kk < kTsKC; kk += 8) {
+              double a[4];
+              if (p.amode == 0) {
+                a[0] = sgn * sA[ra + (kk + t4) * ldA];
+                a[1] = sgn * sA[ra + 8 + (kk + t4) * ldA];
+                a[2] = sgn * sA[ra + (kk + t4 + 4) * ldA];
+                a[3] = sgn * sA[ra + 8 + (kk + t4 + 4) * ldA];
+              } else {
+                a[0] = sgn * sA[(kk + t4) + ra * kTsCT];
+                a[1] = sgn * sA[(kk + t4) + (ra + 8) * kTsCT];
+                a[2] = sgn * sA[(kk + t4 + 4) + ra * kTsCT];
+                a[3] = sgn * sA[(kk + t4 + 4) + (ra + 8) * kTsCT];
+              }
+#pragma unroll
+              for (int nt = 0; nt < NT; ++nt) {
+                double bf[2];
+                bf[0] = sX[(kk + t4) + (8 * nt + g8) * kTsCT];
+                bf[1] = sX[(kk + t4 + 4) + (8 * nt + g8) * kTsCT];
+                dmma_16x8x8(acc[nt], a, bf);
+              }
+            }
+          }
+          __syncwarp();
+          if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&empty[slot])) : "memory");
+        }
+      }
+      gq += P * cpp;
+      double* out = p.mode == 1 ? p.Y : p.X;
+#pragma unroll
+      for (int nt = 0; nt < NT; ++nt)
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          const int row = 16 * warp + g8 + ((e >= 2) ? 8 : 0), col = 8 * nt + 2 * t4 + (e & 1);
+          if (row < t.mr && col < p.nrhs) out[(t.r0 + row) + (long long)col * p.ldx] = acc[nt][e];
+        }
+    }
+    if (p.mode != 1 || t.mr <= 0) {  // publish x_r (every strip releases once, an empty one too)
+      ts_consumer_sync();
+      if (tid == 0) asm volatile("red.release.gpu.global.add.s32 [%0], 1;" ::"l"(&p.flags[t.r]) : "memory");
+    }
+  }
+}
 
 // NT: 8-column tiles of the right-hand side (a compile-time count: a DMMA
 // skipped under a run-time predicate still costs its issue slots).
 template <int NT>
-__global__ void __launch_bounds__(kTsThreads, 1) trsm_skinny_kernel(const __grid_constant__ CUtensorMap mapA,
+__global__ void __launch_bounds__(kTsThreads, 1) trsm_skinny_kernel(const __grid_constant__ CUtensorMap mapL,
+                                                                    const __grid_constant__ CUtensorMap mapW,
                                                                     TsParams p) {
   // TMA boxes land at stage starts: the dynamic region must be 128-byte
   // aligned (it follows the static barriers)
   extern __shared__ __align__(128) double sm[];
-  double* accS = sm + kTsA;  // the X buffer: the accumulator is the next product's right operand
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int g = lane >> 2, t = lane & 3;
-  __shared__ __align__(8) uint64_t barA[kTsStages], barX[kTsStages];
+  __shared__ __align__(8) uint64_t fullA[kTsStages], fullX[kTsStages], empty[kTsStages];
+  __shared__ int s_go;
+  const int tid = threadIdx.x;
   if (tid == 0) {
     for (int i = 0; i < kTsStages; ++i) {
-      mbar_init(&barA[i], 1);
-      mbar_init(&barX[i], kTsThreads);
+      mbar_init(&fullA[i], 1);
+      mbar_init(&fullX[i], kTsFullXCount);
+      mbar_init(&empty[i], kTsEmptyCount);
     }
     fence_mbar_init();
+    int go = p.status == nullptr || ((volatile DevStatus*)p.status)->code == 0;
+    if (go && smem_u32(sm) % 128 != 0) {  // no TMA into a misaligned stage: report and stop
+      set_status(p.status, kTimeout, 203);
+      go = 0;
+    }
+    s_go = go;
   }
   __syncthreads();
-  int gq = 0;  // ring chunks issued by this CTA so far
-  const int mode = p.mode;
-  const int S = p.strips, hs = p.hs, target = p.strips * p.epoch;
-  if (p.status != nullptr && ((volatile DevStatus*)p.status)->code != 0) return;
-  if (smem_u32(sm) % 128 != 0) {  // no TMA into a misaligned stage: report and stop
-    if (tid == 0) set_status(p.status, kTimeout, 203);
-    return;
-  }
-  for (int task = blockIdx.x; task < p.nblk * S; task += gridDim.x) {
-    const int s = task / S, q = task - s * S;
-    const int r = ts_block(p, s);
-    const int rb0 = r * p.nb, mb = min(p.nb, p.n - rb0);  // the block row
-    const int r0 = rb0 + q * hs, mr = min(hs, mb - q * hs);  // this task's strip of it (may be empty)
-    double acc[8][4];
-#pragma unroll
-    for (int nt = 0; nt < 8; ++nt)
-#pragma unroll
-      for (int e = 0; e < 4; ++e) acc[nt][e] = 0.0;
-    if (mr > 0) {
-      if (mode == 2) {
-        // acc = inv(T_rr)(strip rows, :) b_r, before the first wait
-        const double* Wr = p.Winv + (long long)r * p.nb * p.nb;
-        const double* G = p.amode == 0 ? Wr + q * hs : Wr + (long long)q * hs * p.nb;
-        ts_product<NT>(acc, 1.0, sm, G, p.nb, p.amode, mr, mb, p.Y + rb0, p.ldx, p.nrhs, false);
-      } else {
-        // acc = B(strip)
-#pragma unroll
-        for (int nt = 0; nt < 8; ++nt)
-#pragma unroll
-          for (int e = 0; e < 4; ++e) {
-            const int row = 16 * warp + g + ((e >= 2) ? 8 : 0), col = 8 * nt + 2 * t + (e & 1);
-            if (nt < NT && row < mr && col < p.nrhs) acc[nt][e] = __ldcg(&p.X[(r0 + row) + (long long)col * p.ldx]);
-          }
-      }
-      // acc -= T(strip, j) X_j for the blocks j solved before r
-      if (!ts_ring_products<NT>(acc, sm, barA, barX, gq, &mapA, p, s, r0, mr, target)) return;
-    }
-    if (mode == 1) {
-      // column-prescaled form: publish the strip of z_r = acc first (the others need only z) ...
-      if (mr > 0)
-#pragma unroll
-        for (int nt = 0; nt < 8; ++nt)
-#pragma unroll
-          for (int e = 0; e < 4; ++e) {
-            const int row = 16 * warp + g + ((e >= 2) ? 8 : 0), col = 8 * nt + 2 * t + (e & 1);
-            if (nt < NT && row < mr && col < p.nrhs) p.X[(r0 + row) + (long long)col * p.ldx] = acc[nt][e];
-          }
-      __syncthreads();  // the block's stores happen before thread 0's release (barrier + cumulative release)
-      if (tid == 0) asm volatile("red.release.gpu.global.add.s32 [%0], 1;" ::"l"(&p.flags[r]) : "memory");
-      if (mr <= 0) continue;
-      // ... then Y(strip) = inv(T_rr)(strip rows, :) z_r once every strip of z_r is out
-#pragma unroll
-      for (int nt = 0; nt < 8; ++nt)
-#pragma unroll
-        for (int e = 0; e < 4; ++e) acc[nt][e] = 0.0;
-      const double* Wr = p.Winv + (long long)r * p.nb * p.nb;
-      const double* G = p.amode == 0 ? Wr + q * hs : Wr + (long long)q * hs * p.nb;
-      if (!ts_product<NT>(acc, 1.0, sm, G, p.nb, p.amode, mr, mb, p.X + rb0, p.ldx, p.nrhs, false, &p.flags[r], target,
-                      p.status))
-        return;
-    } else if (mode == 0) {
-      // X_r = inv(T_rr) acc (one strip per block: the whole accumulator is in this CTA)
-#pragma unroll
-      for (int nt = 0; nt < 8; ++nt)
-#pragma unroll
-        for (int e = 0; e < 4; ++e) {
-          const int row = 16 * warp + g + ((e >= 2) ? 8 : 0), col = 8 * nt + 2 * t + (e & 1);
-          // rows past the strip hold products of stale stage rows: they are the
-          // product's zero K tail here
-          if (nt < NT) accS[row + col * kTsLD] = row < mr ? acc[nt][e] : 0.0;
-          acc[nt][e] = 0.0;
-        }
-      __syncthreads();
-      const double* Wr = p.Winv + (long long)r * p.nb * p.nb;
-      ts_product<NT>(acc, 1.0, sm, Wr, p.nb, p.amode, mr, mr, accS, kTsLD, p.nrhs, true);
-    }
-    double* out = mode == 1 ? p.Y : p.X;
-#pragma unroll
-    for (int nt = 0; nt < 8; ++nt)
-#pragma unroll
-      for (int e = 0; e < 4; ++e) {
-        const int row = 16 * warp + g + ((e >= 2) ? 8 : 0), col = 8 * nt + 2 * t + (e & 1);
-        if (nt < NT && row < mr && col < p.nrhs) out[(r0 + row) + (long long)col * p.ldx] = acc[nt][e];
-      }
-    if (mode != 1) {
-      __syncthreads();  // the block's stores happen before thread 0's release (barrier + cumulative release)
-      if (tid == 0) asm volatile("red.release.gpu.global.add.s32 [%0], 1;" ::"l"(&p.flags[r]) : "memory");
-    }
-  }
+  if (!s_go) return;
+  if (tid >= kTsConsumers) ts_producer(&mapL, &mapW, p, sm, fullA, fullX, empty);
+  else ts_consumers<NT>(p, sm, fullA, fullX, empty);
 }
 
 size_t trsm_skinny_flag_bytes(int n, int nb) { return sizeof(int) * (size_t)((n + nb - 1) / nb) + 256; }
@@ -507,24 +408,27 @@ int launch_trsm_skinny(cudaStream_t st, int bwd, int amode, int n, int nrhs, con
   p.L = L; p.lda = lda; p.Winv = Winv; p.X = X; p.ldx = ldx; p.Y = Y;
   p.n = n; p.nrhs = nrhs; p.nb = nb; p.nblk = (n + nb - 1) / nb; p.bwd = bwd; p.amode = amode;
   p.mode = Y == nullptr ? 0 : row_prescaled ? 2 : 1;
-  // prescaled form: two strips per block row, so the dependency chain's product is half a block,
+  // prescaled forms: two strips per block row, so the dependency chain's product is half a block,
   // while a CTA holds at most two tasks (its second task starts after the first and still has to
   // catch up with all the products of its block row)
-  p.strips = (p.mode != 0 && nb >= 32 && (n + nb - 1) / nb <= sm_count) ? 2 : 1;
+  p.strips = (p.mode != 0 && nb >= 32 && p.nblk <= sm_count) ? 2 : 1;
   p.hs = p.strips == 1 ? nb : ((nb + 1) / 2 + 15) / 16 * 16;
   p.flags = flags; p.epoch = epoch; p.status = status;
-  // A's ring pieces: TMA boxes over the stored n x n matrix (see ts_tma_a)
-  CUtensorMap mapA;
-  const bool mok = amode == 0 ? make_tma_2d(&mapA, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, L, n, n, 8ull * lda,
-                                            (uint32_t)(p.hs + 4), kTsKC, false)
-                              : make_tma_2d(&mapA, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, L, n, n, 8ull * lda, kTsCT,
-                                            (uint32_t)p.hs, false);
-  if (!mok) return EGPU_ERR_UNSUPPORTED;
+  // the A pieces: TMA boxes over the stored n x n matrix and over the Winv
+  // slots (nb rows x nblk*nb columns), the same box for both
+  const uint32_t bi = amode == 0 ? (uint32_t)(p.hs + 4) : (uint32_t)kTsCT;
+  const uint32_t bo = amode == 0 ? (uint32_t)kTsKC : (uint32_t)p.hs;
+  CUtensorMap mapL, mapW;
+  if (!make_tma_2d(&mapL, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, L, n, n, 8ull * lda, bi, bo, false) ||
+      !make_tma_2d(&mapW, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, Winv, nb, (uint64_t)p.nblk * nb, 8ull * nb, bi, bo,
+                   false))
+    return EGPU_ERR_UNSUPPORTED;
   const size_t smem = sizeof(double) * kTsSmemDoubles;
   const int nt = nrhs <= 8 ? 1 : nrhs <= 16 ? 2 : nrhs <= 32 ? 4 : 8;
-  void (*kern)(const CUtensorMap, TsParams) = nt == 1 ? trsm_skinny_kernel<1>
-                           : nt == 2 ? trsm_skinny_kernel<2>
-                           : nt == 4 ? trsm_skinny_kernel<4> : trsm_skinny_kernel<8>;
+  void (*kern)(const CUtensorMap, const CUtensorMap, TsParams) = nt == 1   ? trsm_skinny_kernel<1>
+                                                                 : nt == 2 ? trsm_skinny_kernel<2>
+                                                                 : nt == 4 ? trsm_skinny_kernel<4>
+                                                                           : trsm_skinny_kernel<8>;
   static bool attr[4] = {false, false, false, false};
   const int ai = nt == 1 ? 0 : nt == 2 ? 1 : nt == 4 ? 2 : 3;
   if (!attr[ai]) {
@@ -542,11 +446,11 @@ int launch_trsm_skinny(cudaStream_t st, int bwd, int amode, int n, int nrhs, con
   cfg.dynamicSmemBytes = smem;
   cfg.stream = st;
   cudaLaunchAttribute attr1[1];
-  attr1[0].id = cudaLaunchAttributeCooperative;  // every CTA resident: the flag waits always end
+  attr1[0].id = cudaLaunchAttributeCooperative;  // every CTA resident: the counter waits always end
   attr1[0].val.cooperative = 1;
   cfg.attrs = attr1;
   cfg.numAttrs = 1;
-  cudaError_t e = cudaLaunchKernelEx(&cfg, kern, mapA, p);
+  cudaError_t e = cudaLaunchKernelEx(&cfg, kern, mapL, mapW, p);
   count_launch();
   if (e != cudaSuccess) {
     set_last_error(e, "trsm_skinny launch", __FILE__, __LINE__);
