@@ -100,6 +100,7 @@ def _declare(L):
         "egpu_launch_count": ([H], LL),
         "egpu_trace_enable": ([H, I], I),
         "egpu_trace_summary": ([H, I, P, P, P, P], I),
+        "egpu_trace_events": ([H, I, P, P, P, P], I),
         "egpu_dpotrf": ([H, I, I, P, I, P], I),
         "egpu_dpotrs": ([H, I, I, I, I, P, I, P, I], I),
         "egpu_dposv": ([H, I, I, I, I, P, I, P, I, P], I),
@@ -413,6 +414,25 @@ class Handle:
     def trace_enable(self, on: bool = True):
         """Bracket every launch with CUDA events on its stream (clears old records)."""
         _check(lib().egpu_trace_enable(self._h, int(on)))
+
+    def trace_events(self):
+        """Traced launches in order: list of (kind name, stream, start ms, duration ms);
+        stream 0 is the handle's stream, 1 the look-ahead side stream, 2 the
+        lowest-priority auxiliary stream."""
+        import numpy as np
+        n = lib().egpu_trace_events(self._h, 0, None, None, None, None)
+        if n < 0:
+            _check(n)
+        kinds = np.zeros(max(n, 1), dtype=np.int32)
+        streams = np.zeros(max(n, 1), dtype=np.int32)
+        st = np.zeros(max(n, 1), dtype=np.float64)
+        du = np.zeros(max(n, 1), dtype=np.float64)
+        lib().egpu_trace_events(self._h, n, kinds.ctypes.data_as(ctypes.c_void_p),
+                                streams.ctypes.data_as(ctypes.c_void_p), st.ctypes.data_as(ctypes.c_void_p),
+                                du.ctypes.data_as(ctypes.c_void_p))
+        names = {v: k for k, v in self.TRACE_KINDS.items()}
+        return [(names.get(int(kinds[i]), str(int(kinds[i]))), int(streams[i]), float(st[i]), float(du[i]))
+                for i in range(n)]
 
     def trace_summary(self) -> dict:
         """{kind: {"ms", "flops", "bytes", "launches"}} over the traced launches."""

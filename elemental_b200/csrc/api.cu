@@ -26,7 +26,7 @@ TraceMark::TraceMark(cudaStream_t s, int kind, double flops, double bytes) {
   if (t_trace == nullptr || !t_trace->on) return;
   cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
   if (cudaStreamIsCapturing(s, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) return;
-  Trace::Rec r{kind, flops, bytes, t_trace->get(), t_trace->get()};
+  Trace::Rec r{kind, flops, bytes, t_trace->get(), t_trace->get(), s};
   if (!r.e0 || !r.e1) return;
   t = t_trace;
   st = s;
@@ -658,6 +658,26 @@ int egpu_trace_summary(egpu_handle h, int kind, double* total_ms, double* total_
   if (total_bytes) *total_bytes = by;
   if (launches) *launches = n;
   return EGPU_OK;
+}
+
+int egpu_trace_events(egpu_handle h, int max, int* kind, int* stream_tag, double* start_ms, double* dur_ms) {
+  TRY(check_handle(h));
+  Enter g(h);
+  const int n = (int)h->trace.recs.size();
+  if (n == 0) return 0;
+  const cudaEvent_t base = h->trace.recs[0].e0;
+  for (int i = 0; i < n && i < max; ++i) {
+    const auto& r = h->trace.recs[i];
+    EGPU_CUDA_TRY(cudaEventSynchronize(r.e1));
+    float t0 = 0, t = 0;
+    EGPU_CUDA_TRY(cudaEventElapsedTime(&t0, base, r.e0));
+    EGPU_CUDA_TRY(cudaEventElapsedTime(&t, r.e0, r.e1));
+    if (kind) kind[i] = r.kind;
+    if (stream_tag) stream_tag[i] = r.st == h->stream ? 0 : r.st == h->side ? 1 : r.st == h->aux ? 2 : 3;
+    if (start_ms) start_ms[i] = t0;
+    if (dur_ms) dur_ms[i] = t;
+  }
+  return n;
 }
 
 const char* egpu_error_string(int code) {

@@ -14,6 +14,7 @@ struct Trace {
     int kind;
     double flops, bytes;
     cudaEvent_t e0, e1;
+    cudaStream_t st;  // the launch's stream (timeline dumps)
   };
   bool on = false;
   std::vector<Rec> recs;

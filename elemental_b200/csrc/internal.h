@@ -44,9 +44,13 @@ bool make_tma_2d(CUtensorMap* m, int dtype, const void* base, uint64_t inner, ui
 // A_t (M x K) and B_t (N x K) K-major FP32 buffers (row stride ldk elements,
 // ldk % 4 == 0, 16-byte aligned) holding TF32 values; terms 1 uses (Ahi, Bhi),
 // terms 3 adds (Ahi, Blo) and (Alo, Bhi).  tri 1: only r >= c is written (M >= N).
+// Sh/Sl (optional): also the TF32 hi/lo split of the result's rows r >= srow0,
+// K-major with row stride sldk (% 32 == 0), columns [0, swidth) (zero past N;
+// N <= swidth <= sldk), 16-byte aligned; the A buffers may be the same rows.
 int launch_tc_gemm(cudaStream_t st, int M, int N, int K, float alpha, const float* Ahi, const float* Alo,
                    const float* Bhi, const float* Blo, long long ldk, float beta, float* C, long long ldc, int tri,
-                   int terms, DevStatus* status);
+                   int terms, DevStatus* status, float* Sh = nullptr, float* Sl = nullptr, long long sldk = 0,
+                   int srow0 = 0, int swidth = 0);
 
 // X (rows x cols, column-major FP64) -> TF32 hi/lo parts in K-major rows
 // (hi[r*ldk + c], row stride ldk), columns cols..width-1 zero (width: ldk

@@ -99,12 +99,18 @@ __global__ void colmax_kernel(int n, int ncols, const double* X, long long ldx, 
 }
 
 // ||As||_inf = max_i sum_j |As[i, j]| : per-row sums, one thread per row
+// rows[j] = sum_i |As[i, j]|: the row sums of the symmetric As, as column
+// sums (a warp per column, contiguous loads, fixed summation order)
 __global__ void rowsum_abs_kernel(int n, const double* As, long long lds, double* rows) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
+  const int lane = threadIdx.x & 31;
+  const int j = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (j >= n) return;
+  const double* col = As + (long long)j * lds;
   double s = 0.0;
-  for (int j = 0; j < n; ++j) s += fabs(As[i + (long long)j * lds]);
-  rows[i] = s;
+  for (int i = lane; i < n; i += 32) s += fabs(col[i]);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if (lane == 0) rows[j] = s;
 }
 
 // Y = X (n x ncols) ; Y += X
@@ -161,6 +167,7 @@ int launch_split_tf32(cudaStream_t st, int rows, int cols, const double* X, long
                       long long ldk, int width) {
   if (rows <= 0 || cols <= 0) return EGPU_OK;
   if (width < 0) width = (int)ldk;
+  TraceMark tm(st, kTraceOther, 0.0, (double)rows * (8.0 * cols + 8.0 * width));
   dim3 grid((rows + 31) / 32, (width + 31) / 32), block(32, 8);
   split_tf32_kernel<double><<<grid, block, 0, st>>>(rows, cols, X, ldx, hi, lo, ldk, width);
   count_launch();
@@ -171,6 +178,7 @@ int launch_split_tf32(cudaStream_t st, int rows, int cols, const double* X, long
 int launch_split_tf32_f32(cudaStream_t st, int rows, int cols, const float* X, long long ldx, float* hi, float* lo,
                           long long ldk) {
   if (rows <= 0 || cols <= 0) return EGPU_OK;
+  TraceMark tm(st, kTraceOther, 0.0, (double)rows * (4.0 * cols + 8.0 * ldk));
   dim3 grid((rows + 31) / 32, (int)((ldk + 31) / 32)), block(32, 8);
   split_tf32_kernel<float><<<grid, block, 0, st>>>(rows, cols, X, ldx, hi, lo, ldk, (int)ldk);
   count_launch();
@@ -464,10 +472,12 @@ int dposv_mixed_core_impl(egpu_context* h, int uplo, int n, int nrhs, const doub
         TRY(launch_dgemm(s, false, false, m2, b, b, 1.0, L21, lds, Wk, nb, 0.0, L21, lds, 0, true, h->dstatus));
         TRY(launch_split_tf32(s, m2, b, L21, lds, PKh2[par], PKl2[par], L.ldk));
       } else {
-        TRY(launch_split_tf32_f32(s, m2, b, A21, ldf, PKh2[par], PKl2[par], L.ldk));
+        // A21's split: from the previous step's block-column update (its
+        // epilogue), or here for the first panel; L21's split is written by the
+        // product's epilogue over it (a tile's output rows are the rows it read)
+        if (k == 0) TRY(launch_split_tf32_f32(s, m2, b, A21, ldf, PKh2[par], PKl2[par], L.ldk));
         TRY(launch_tc_gemm(s, m2, b, b, 1.0f, PKh2[par], PKl2[par], Wsh, Wsl, L.ldk, 0.0f, A21, ldf, 0, 3,
-                           h->dstatus));
-        TRY(launch_split_tf32_f32(s, m2, b, A21, ldf, PKh2[par], PKl2[par], L.ldk));
+                           h->dstatus, PKh2[par], PKl2[par], L.ldk, 0, (int)L.ldk));
       }
       EGPU_CUDA_TRY(cudaEventRecord(h->ev_split[par], s));  // L21 final: its FP64 copy may start
       return EGPU_OK;
@@ -501,9 +511,10 @@ int dposv_mixed_core_impl(egpu_context* h, int uplo, int n, int nrhs, const doub
       EGPU_CUDA_TRY(cudaStreamWaitEvent(st, h->ev_panel[par], 0));
       const int b2 = std::min(nb, m2);
       float* A22 = Af + (k + b) + (long long)(k + b) * ldf;
-      // (a) block column k+1 (lower trapezoid m2 x b2)
+      // (a) block column k+1 (lower trapezoid m2 x b2); its rows below the
+      // next diagonal block are the next panel's A21, split into the other buffer
       TRY(launch_tc_gemm(st, m2, b2, b, -1.0f, PKh2[par], PKl2[par], PKh2[par], PKl2[par], L.ldk, 1.0f, A22, ldf, 1, 3,
-                         h->dstatus));
+                         h->dstatus, PKh2[par ^ 1], PKl2[par ^ 1], L.ldk, b2, (int)L.ldk));
       EGPU_CUDA_TRY(cudaEventRecord(h->ev_rest[par], st));
       EGPU_CUDA_TRY(cudaStreamWaitEvent(sd, h->ev_rest[par], 0));
       TRY(panel_chain(k + b, sd));
@@ -527,7 +538,7 @@ int dposv_mixed_core_impl(egpu_context* h, int uplo, int n, int nrhs, const doub
   TRY(frc);  // the status word (pivot column) stays readable by the caller
   // ---- refinement
   {
-    rowsum_abs_kernel<<<(n + 255) / 256, 256, 0, st>>>(n, As, lds, norms);
+    rowsum_abs_kernel<<<(n + 7) / 8, 256, 0, st>>>(n, As, lds, norms);
     count_launch();
     EGPU_CUDA_TRY(cudaGetLastError());
   }

@@ -52,6 +52,12 @@ struct TcParams {
   int tri;  // 0 full, 1 lower trapezoid r >= c of C (M >= N; tiles i >= j, diagonal tiles masked)
   int tiles_m, tiles_n;
   DevStatus* status;
+  // optional TF32 split of the result (sh == null: none): rows r >= srow0 of
+  // C land in K-major rows sh[(r - srow0) * sldk + c], c < swidth (zero past N)
+  float* sh;
+  float* sl;
+  long long sldk;
+  int srow0, swidth;
 };
 
 __device__ __forceinline__ uint64_t sw128_kmajor_desc(uint32_t saddr) {
@@ -242,6 +248,7 @@ __global__ void __maxnreg__(200) tc_gemm_kernel(const __grid_constant__ CUtensor
         break;
       }
       tc_fence_after();
+      const bool split = p.sh != nullptr && r >= p.srow0 && r < p.M;
 #pragma unroll
       for (int c0 = 0; c0 < 64; c0 += 32) {
         float v[32];
@@ -249,8 +256,24 @@ __global__ void __maxnreg__(200) tc_gemm_kernel(const __grid_constant__ CUtensor
         float* cp;  // opaque copy of the base: keeps the load addresses from staying live
         asm volatile("mov.b64 %0, %1;" : "=l"(cp) : "l"(cbase + (long long)c0 * p.ldc));
 #pragma unroll
-        for (int j = 0; j < 32; ++j, cp += p.ldc)
-          if (c0 + j < jmax) *cp = fmaf(p.alpha, v[j], p.beta * cv[c0 + j]);
+        for (int j = 0; j < 32; ++j, cp += p.ldc) {
+          v[j] = c0 + j < jmax ? fmaf(p.alpha, v[j], p.beta * cv[c0 + j]) : 0.0f;
+          if (c0 + j < jmax) *cp = v[j];
+        }
+        if (split && n0 + c0 < p.swidth) {  // the result's TF32 hi/lo split, 16-byte stores
+          float* sh = p.sh + (long long)(r - p.srow0) * p.sldk + (n0 + c0);
+          float* sl = p.sl + (long long)(r - p.srow0) * p.sldk + (n0 + c0);
+#pragma unroll
+          for (int j4 = 0; j4 < 32; j4 += 4) {
+            float4 h4, l4;
+            h4.x = tf32_rna(v[j4]);     l4.x = tf32_rna(v[j4] - h4.x);
+            h4.y = tf32_rna(v[j4 + 1]); l4.y = tf32_rna(v[j4 + 1] - h4.y);
+            h4.z = tf32_rna(v[j4 + 2]); l4.z = tf32_rna(v[j4 + 2] - h4.z);
+            h4.w = tf32_rna(v[j4 + 3]); l4.w = tf32_rna(v[j4 + 3] - h4.w);
+            *reinterpret_cast<float4*>(sh + j4) = h4;
+            *reinterpret_cast<float4*>(sl + j4) = l4;
+          }
+        }
       }
       tc_fence_before();
       __syncwarp();
@@ -290,9 +313,13 @@ static cudaError_t tc_launch_variant(cudaStream_t st, const CUtensorMap& mah, co
 
 int launch_tc_gemm(cudaStream_t st, int M, int N, int K, float alpha, const float* Ahi, const float* Alo,
                    const float* Bhi, const float* Blo, long long ldk, float beta, float* C, long long ldc, int tri,
-                   int terms, DevStatus* status) {
+                   int terms, DevStatus* status, float* Sh, float* Sl, long long sldk, int srow0, int swidth) {
   if (M <= 0 || N <= 0 || K <= 0) return M <= 0 || N <= 0 ? EGPU_OK : EGPU_ERR_ARG;
   if (terms != 1 && terms != 3) return EGPU_ERR_ARG;
+  if (Sh != nullptr &&
+      (Sl == nullptr || sldk % 32 != 0 || swidth > sldk || swidth < std::min(N, (int)sldk) ||
+       reinterpret_cast<uintptr_t>(Sh) % 16 != 0 || reinterpret_cast<uintptr_t>(Sl) % 16 != 0))
+    return EGPU_ERR_ARG;
   if (tri == 1 && M < N) return EGPU_ERR_ARG;  // lower trapezoid: rows >= columns
   if (ldk < K || ldk % 4 != 0) return EGPU_ERR_ALIGN;
   for (const float* q : {Ahi, Bhi, terms == 3 ? Alo : Ahi, terms == 3 ? Blo : Bhi})
@@ -314,6 +341,7 @@ int launch_tc_gemm(cudaStream_t st, int M, int N, int K, float alpha, const floa
   p.tiles_m = (M + kTcBM - 1) / kTcBM;
   p.tiles_n = (N + kTcBN - 1) / kTcBN;
   p.status = status;
+  p.sh = Sh; p.sl = Sl; p.sldk = sldk; p.srow0 = srow0; p.swidth = swidth;
   long long nblocks = (long long)p.tiles_m * p.tiles_n;
   if (tri) {  // tiles on or below the diagonal: column j holds tiles j .. tiles_m-1
     nblocks = 0;

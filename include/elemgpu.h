@@ -111,6 +111,13 @@ EGPU_API long long egpu_launch_count(egpu_handle h);
 EGPU_API int egpu_trace_enable(egpu_handle h, int on);
 EGPU_API int egpu_trace_summary(egpu_handle h, int kind, double* total_ms, double* total_flops,
                                 double* total_bytes, long long* launches);
+/* The traced launches in order: kind (as egpu_trace_summary), stream (0 the
+   handle's stream, 1 the look-ahead side stream, 2 the lowest-priority
+   auxiliary stream, 3 another), start relative to the first traced launch
+   and duration, both in ms.  Fills at most `max` entries; returns the number
+   of traced launches (or a negative error code). */
+EGPU_API int egpu_trace_events(egpu_handle h, int max, int* kind, int* stream_tag, double* start_ms,
+                               double* dur_ms);
 
 /* Roofline denominator: measured FP64 tensor-core (DMMA) throughput of the
  * handle's GPU in TFLOP/s (in-register mma.sync loop, ~30 ms). */
