@@ -540,6 +540,7 @@ int egpu_create(egpu_handle* out, int device) {
       ok = ok && cudaEventCreateWithFlags(&h->ev_panel[i], cudaEventDisableTiming) == cudaSuccess;
       ok = ok && cudaEventCreateWithFlags(&h->ev_rest[i], cudaEventDisableTiming) == cudaSuccess;
       ok = ok && cudaEventCreateWithFlags(&h->ev_split[i], cudaEventDisableTiming) == cudaSuccess;
+      ok = ok && cudaEventCreateWithFlags(&h->ev_a21[i], cudaEventDisableTiming) == cudaSuccess;
     }
     if (!ok) {
       set_last_error(cudaGetLastError(), "egpu_create streams", __FILE__, __LINE__);
@@ -564,7 +565,7 @@ int egpu_destroy(egpu_handle h) {
   if (h->side) cudaStreamSynchronize(h->side);
   if (h->aux) cudaStreamSynchronize(h->aux);
   for (cudaEvent_t e : {h->ev_fork, h->ev_join, h->ev_panel[0], h->ev_panel[1], h->ev_rest[0], h->ev_rest[1],
-                        h->ev_split[0], h->ev_split[1], h->ev_aux})
+                        h->ev_split[0], h->ev_split[1], h->ev_aux, h->ev_a21[0], h->ev_a21[1]})
     if (e) cudaEventDestroy(e);
   if (h->side) cudaStreamDestroy(h->side);
   if (h->aux) cudaStreamDestroy(h->aux);

@@ -71,6 +71,9 @@ struct egpu_context {
   // path's prescaled solve copies), joined before its results are read
   cudaStream_t aux = nullptr;
   cudaEvent_t ev_split[2] = {nullptr, nullptr}, ev_aux = nullptr;
+  // the mixed chain: a block column's rows below its diagonal block updated
+  // (and split) -- the next panel's L21 product waits for it
+  cudaEvent_t ev_a21[2] = {nullptr, nullptr};
   int lookahead = 1;
   int async = 0;  // device API: enqueue only; status read by egpu_get_status
   int gmres_inner = 0;  // GMRES iterations of the last mixed solve

@@ -476,6 +476,7 @@ int dposv_mixed_core_impl(egpu_context* h, int uplo, int n, int nrhs, const doub
         // epilogue), or here for the first panel; L21's split is written by the
         // product's epilogue over it (a tile's output rows are the rows it read)
         if (k == 0) TRY(launch_split_tf32_f32(s, m2, b, A21, ldf, PKh2[par], PKl2[par], L.ldk));
+        else EGPU_CUDA_TRY(cudaStreamWaitEvent(s, h->ev_a21[par], 0));
         TRY(launch_tc_gemm(s, m2, b, b, 1.0f, PKh2[par], PKl2[par], Wsh, Wsl, L.ldk, 0.0f, A21, ldf, 0, 3,
                            h->dstatus, PKh2[par], PKl2[par], L.ldk, 0, (int)L.ldk));
       }
@@ -511,12 +512,19 @@ int dposv_mixed_core_impl(egpu_context* h, int uplo, int n, int nrhs, const doub
       EGPU_CUDA_TRY(cudaStreamWaitEvent(st, h->ev_panel[par], 0));
       const int b2 = std::min(nb, m2);
       float* A22 = Af + (k + b) + (long long)(k + b) * ldf;
-      // (a) block column k+1 (lower trapezoid m2 x b2); its rows below the
-      // next diagonal block are the next panel's A21, split into the other buffer
-      TRY(launch_tc_gemm(st, m2, b2, b, -1.0f, PKh2[par], PKl2[par], PKh2[par], PKl2[par], L.ldk, 1.0f, A22, ldf, 1, 3,
-                         h->dstatus, PKh2[par ^ 1], PKl2[par ^ 1], L.ldk, b2, (int)L.ldk));
+      // (a) block column k+1: its diagonal block first (releases the next
+      // diagonal factorization), then the rows below it, which are the next
+      // panel's A21 (split into the other buffer; its L21 product waits for it)
+      TRY(launch_tc_gemm(st, b2, b2, b, -1.0f, PKh2[par], PKl2[par], PKh2[par], PKl2[par], L.ldk, 1.0f, A22, ldf, 1,
+                         3, h->dstatus));
       EGPU_CUDA_TRY(cudaEventRecord(h->ev_rest[par], st));
       EGPU_CUDA_TRY(cudaStreamWaitEvent(sd, h->ev_rest[par], 0));
+      if (m2 > b2) {
+        TRY(launch_tc_gemm(st, m2 - b2, b2, b, -1.0f, PKh2[par] + (size_t)b2 * L.ldk, PKl2[par] + (size_t)b2 * L.ldk,
+                           PKh2[par], PKl2[par], L.ldk, 1.0f, A22 + b2, ldf, 0, 3, h->dstatus, PKh2[par ^ 1],
+                           PKl2[par ^ 1], L.ldk, 0, (int)L.ldk));
+        EGPU_CUDA_TRY(cudaEventRecord(h->ev_a21[par ^ 1], st));
+      }
       TRY(panel_chain(k + b, sd));
       // (b) the rest of the trailing lower triangle
       const int m3 = m2 - b2;
