@@ -84,22 +84,49 @@ __global__ void __launch_bounds__(kDiagThreads) potrf_diag_kernel(double* A, lon
 // matrix, widened on load, factored and inverted in FP64 as above; the
 // inverse goes to W (FP64, for the solves) and, split into TF32 hi/lo rows,
 // to Wh/Wl (the B operand of the panel's L21 product on the tensor cores).
-__global__ void __launch_bounds__(kDiagThreads) potrf_diag_f32_kernel(const float* Af, long long ldf, int b,
-                                                                       double* W, int ldw, float* Wh, float* Wl,
-                                                                       long long ldk, DevStatus* st, int col_base) {
-  extern __shared__ double S[];
-  if (st != nullptr && st->code != 0) return;
+// Both big transfers go through the TMA engine: the block arrives as one
+// 128 x 128 FP32 box (staged in S's first 64 KB, widened in place: every
+// thread reads its values before any writes), and W leaves as one 132 x 128
+// FP64 box straight from S (pitch 132; the rows past the slot are clipped)
+// while the threads write the split.
+__global__ void __launch_bounds__(kDiagThreads) potrf_diag_f32_kernel(const __grid_constant__ CUtensorMap mapA,
+                                                                       const __grid_constant__ CUtensorMap mapW,
+                                                                       int b, float* Wh, float* Wl, long long ldk,
+                                                                       DevStatus* st, int col_base) {
+  extern __shared__ __align__(128) double S[];
+  __shared__ __align__(8) uint64_t bar;
+  __shared__ int s_go;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   static_assert(kDiagThreads == 256, "a warp per 16 columns of the 128 x 128 block");
-  {  // lower triangle: warp w holds columns w, w + 8, ..; every load issued before any is used
+  float* stage = reinterpret_cast<float*>(S);  // the FP32 box, [i + j * 128]
+  if (tid == 0) {
+    int go = st == nullptr || st->code == 0;
+    if (go && smem_u32(S) % 128 != 0) {  // no TMA into a misaligned buffer
+      set_status(st, kTimeout, 205);
+      go = 0;
+    }
+    if (go) {
+      mbar_init(&bar, 1);
+      fence_mbar_init();
+      mbar_expect_tx(&bar, 128u * 128u * 4u);
+      tma_load_2d(stage, &mapA, &bar, 0, 0);
+      if (!mbar_wait_bounded(&bar, 0)) {  // the box never landed: report, do not touch it
+        set_status(st, kTimeout, 206);
+        go = 0;
+      }
+    }
+    s_go = go;
+  }
+  __syncthreads();
+  if (!s_go) return;
+  (void)mbar_wait_bounded(&bar, 0);  // completed: every thread observes the box's arrival
+  {  // widen the lower triangle: warp w holds columns w, w + 8, ..
     float v[16][4];
 #pragma unroll
     for (int u = 0; u < 16; ++u)
 #pragma unroll
-      for (int t = 0; t < 4; ++t) {
-        const int j = warp + 8 * u, i = lane + 32 * t;
-        v[u][t] = (j < b && i >= j && i < b) ? Af[i + (long long)j * ldf] : 0.0f;
-      }
+      for (int t = 0; t < 4; ++t) v[u][t] = stage[(lane + 32 * t) + (warp + 8 * u) * 128];
+    __syncthreads();
 #pragma unroll
     for (int u = 0; u < 16; ++u)
 #pragma unroll
@@ -121,32 +148,43 @@ __global__ void __launch_bounds__(kDiagThreads) potrf_diag_f32_kernel(const floa
   __syncthreads();
   smem_trinv_dmma(S, bp, Xl, T);
   __syncthreads();
-  tri_store(S, W, ldw, b, false, true);
-  if (b < ldw)  // a short last block: the rest of its ldw x ldw slot is zero (whole-slot readers)
-    for (int e = tid; e < ldw * ldw; e += kDiagThreads) {
-      const int i = e % ldw, j = e / ldw;
-      if (i >= b || j >= b) W[i + (long long)j * ldw] = 0.0;
-    }
+  // W's slot: inv(L) below and on the diagonal, zero above it and outside b x b
+  for (int j = warp; j < 128; j += kDiagThreads / 32)
+    for (int i = lane; i < 128; i += 32)
+      if (i < j || i >= b || j >= b) S[i + j * kLDS] = 0.0;
+  fence_proxy_async_smem();  // the zeros (and the inverse) are read by the TMA store
+  __syncthreads();
+  if (tid == 0) {
+    tma_store_2d(&mapW, S, 0, 0);
+    bulk_commit();
+  }
   for (int j = warp; j < 128; j += kDiagThreads / 32) {  // row j of inv(L), a warp per row
     float* wh = Wh + (long long)j * ldk;
     float* wl = Wl + (long long)j * ldk;
     for (int k = lane; k < (int)ldk; k += 32) {
-      const double v = (j < b && k <= j) ? S[j + k * kLDS] : 0.0;
-      const float hv = tf32_rna((float)v);
+      const double vv = k < 128 ? S[j + k * kLDS] : 0.0;  // zero above the diagonal and outside b x b
+      const float hv = tf32_rna((float)vv);
       wh[k] = hv;
-      wl[k] = tf32_rna((float)(v - (double)hv));
+      wl[k] = tf32_rna((float)(vv - (double)hv));
     }
   }
+  if (tid == 0) bulk_wait_all();  // the store has read S and landed before the block retires
 }
 
 int launch_potrf_diag_f32(cudaStream_t st, const float* Af, long long ldf, int b, double* W, int ldw, float* Wh,
                           float* Wl, long long ldk, DevStatus* status, int col_base) {
   if (b <= 0) return EGPU_OK;
-  if (b > kMaxNB || ldk < b) return EGPU_ERR_ARG;
+  if (b > kMaxNB || ldk < b || ldw > 128 || ldw < b || ldk % 4 != 0 || ldf % 4 != 0 ||
+      reinterpret_cast<uintptr_t>(Af) % 16 != 0 || reinterpret_cast<uintptr_t>(W) % 16 != 0)
+    return EGPU_ERR_ARG;
+  CUtensorMap mapA, mapW;
+  if (!make_tma_2d(&mapA, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, Af, b, b, 4ull * ldf, 128, 128, false) ||
+      !make_tma_2d(&mapW, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, W, ldw, ldw, 8ull * ldw, kLDS, 128, false))
+    return EGPU_ERR_TMA;
   TraceMark tm(st, kTraceDiag, (double)b * b * b / 3.0 * 2.0, 12.0 * b * b);
   cudaError_t e = cudaFuncSetAttribute(potrf_diag_f32_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kDiagSmem);
   if (e == cudaSuccess) {
-    potrf_diag_f32_kernel<<<1, kDiagThreads, kDiagSmem, st>>>(Af, ldf, b, W, ldw, Wh, Wl, ldk, status, col_base);
+    potrf_diag_f32_kernel<<<1, kDiagThreads, kDiagSmem, st>>>(mapA, mapW, b, Wh, Wl, ldk, status, col_base);
     count_launch();
     e = cudaGetLastError();
   }
