@@ -208,9 +208,11 @@ EGPU_API int egpu_server_destroy(egpu_server s);
 
 /* Mixed-precision HPDSolve (HPDSolve.hpp:18-28 computes the same x): no
  * counterpart in the reference, which factors in the working precision only.
- * Cholesky with the trailing updates on the tcgen05 tensor cores in TF32 x 3
- * split precision (FP32 accumulation and FP32 trailing matrix), FP64
- * diagonal blocks and panel solves, then iterative refinement with FP64
+ * Cholesky with the trailing updates and the panel solves (L21) on the
+ * tcgen05 tensor cores in TF32 x 3 split precision (FP32 accumulation and
+ * FP32 trailing matrix) and FP64 diagonal blocks (a factorization that meets
+ * a non-positive pivot is redone once with FP64 panel solves before
+ * EGPU_NOT_HPD is returned), then iterative refinement with FP64
  * residuals until the normwise backward error
  *   max_j ||b_j - A x_j||_inf / (||A||_inf ||x_j||_inf + ||b_j||_inf) <= tol
  * or max_iter corrections.  A (uplo triangle read) and B are inputs only;
