@@ -59,7 +59,7 @@ struct egpu_server_s {
   int device = 0, slots = 1, mode = 0;
   size_t budget = 0, in_use = 0;
   double tol = 1e-14;
-  int mixed_min_n = 10240;  // mode 1: smaller HPD requests take the FP64 path (faster there)
+  int mixed_min_n = 6144;  // mode 1: smaller HPD requests take the FP64 path (faster there on average)
   std::mutex mu;
   std::condition_variable cv_dispatch, cv_done;
   std::deque<Request*> queue;

@@ -192,7 +192,8 @@ typedef struct egpu_server_s* egpu_server;
 EGPU_API int egpu_server_create(int device, size_t hbm_budget_bytes, int slots, int mode, egpu_server* out);
 EGPU_API int egpu_server_set_tolerance(egpu_server s, double tol);
 /* Mode 1 sends HPD requests of order >= n to the mixed solver (default
- * 10240: below it the FP64 path is the faster one on B200). */
+ * 6144: below it the FP64 path is faster on B200 for kappa spread
+ * log-uniformly up to 1e8, where GMRES-IR makes the mixed solve slower). */
 EGPU_API int egpu_server_set_mixed_min_n(egpu_server s, int n);
 EGPU_API int egpu_server_submit(egpu_server s, int kind, int n, int nrhs, const double* A, int lda,
                                 const double* B, int ldb, double* X, int ldx, unsigned long long* id);
