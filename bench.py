@@ -824,7 +824,8 @@ def kernel_case(args):
     """One launch of a single kernel class at a chosen size, for profiler
     captures (ncu -k ...): 'update' = one lower Herk trailing update
     (n x n, K = 128), 'gemm' = one Gemm trailing update, 'panel' = one LU panel
-    (n x 128), 'diag' = one diagonal-block Cholesky (128 x 128)."""
+    (n x 128), 'diag' = one diagonal-block Cholesky (128 x 128), 'mixed' = one
+    mixed-precision HPD solve, 'tc' = the tcgen05 trailing update alone."""
     import torch
     import elemental_b200 as eg
     from elemental_b200 import inputs
@@ -890,6 +891,25 @@ def kernel_case(args):
     elif args.case == "diag":
         A = eg.colmajor_cuda(inputs.spd_ggt(NB, 1))
         h.cholesky(A, eg.LOWER)
+    elif args.case == "tc":
+        # the mixed factorization's trailing update alone: C (n x n FP32, lower
+        # triangle) -= L L^T with L n x 128, TF32 x 3 on tcgen05; three timed
+        # launches (the trace separates the kernel from the operand splits)
+        L = eg.empty_colmajor(n, NB).normal_()
+        C = eg.empty_colmajor(n, n).normal_().float().t().contiguous().t()
+        h.tc_gemm_split(L, L, C, alpha=-1.0, beta=1.0, lower=True, terms=3)
+        torch.cuda.synchronize()
+        h.trace_enable(True)
+        for _ in range(3):
+            h.tc_gemm_split(L, L, C, alpha=-1.0, beta=1.0, lower=True, terms=3)
+        torch.cuda.synchronize()
+        s = h.trace_summary()
+        h.trace_enable(False)
+        ms = s["tc"]["ms"] / max(1, s["tc"]["launches"])
+        cbytes = 8.0 * n * (n + 1) / 2  # FP32 lower triangle read + written
+        print(json.dumps({"case": "tc", "n": n, "ms_per_launch": ms, "c_gbs": cbytes / ms / 1e6,
+                          "tf32_tflops": 3 * 2.0 * n * (n + 1) / 2 * NB / ms / 1e9}))
+        return
     torch.cuda.synchronize()
     print(json.dumps({"case": args.case, "n": n, "ok": True}))
 
@@ -902,7 +922,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="mixed", choices=sorted(WORKLOADS), help="benchmark configuration")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline leg")
-    ap.add_argument("--case", choices=["update", "gemm", "panel", "diag", "peaks", "mixed"], default=None,
+    ap.add_argument("--case", choices=["update", "gemm", "panel", "diag", "peaks", "mixed", "tc"], default=None,
                     help="run one launch of one kernel class (profiling)")
     ap.add_argument("--n", type=int, default=6144, help="size for --case")
     args = ap.parse_args()

@@ -396,7 +396,10 @@ class Handle:
         _check(lib().egpu_reserve(self._h, int(nbytes)))
 
     def set_lookahead(self, depth: int):
-        """0: one stream, steps in order; 1 (default): panel k+1 overlaps update k."""
+        """0: one stream, steps in order; 1: panel k+1 overlaps update k;
+        G >= 2 (Cholesky): trailing updates deferred over groups of G panels,
+        the side stream factoring each group's panels just in time; -1
+        (default): G chosen per group from the trailing order."""
         _check(lib().egpu_set_lookahead(self._h, depth))
 
     def set_stream(self, stream_ptr: int | None):

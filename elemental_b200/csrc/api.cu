@@ -227,11 +227,69 @@ int potrf_lookahead(egpu_context* h, int uplo, int n, double* A, long long lda, 
   return EGPU_OK;
 }
 
+// Look-ahead over groups of G panels, so that the trailing update reads and
+// writes the matrix once per G panels (K = G nb: the DMMA update's fixed cost
+// per pass -- tile fill, C read-modify-write -- amortised over G times the
+// flops; FP64 throughout, so the deferral changes only summation order).
+//   side:  per panel kb of group g = [g0, g1): update block column kb by the
+//          group's earlier panels [g0, kb) (one product, K = (kb - g0) nb),
+//          then factor it; after the last panel -> ev_panel(g)
+//   main:  wait ev_panel(g); update by the whole group the next group's first
+//          block column (-> ev_next), its other block columns (-> ev_rest),
+//          then everything beyond it
+// Group g+1's first panel waits for ev_next(g), its later panels for
+// ev_rest(g); the main stream alone writes columns beyond the group the side
+// stream is factoring, so no column is written by both streams at once.
+// G <= 0 selects the group size per group from the order of the trailing
+// matrix: deep groups while the main-stream update dominates, single panels
+// once the side chain (diag + Trsm + column update per panel) is the longer.
+static int auto_group(int m_left) {
+  return m_left > 10240 ? 8 : m_left > 6144 ? 4 : m_left > 4096 ? 2 : 1;
+}
+
+int potrf_grouped(egpu_context* h, int uplo, int n, double* A, long long lda, double* W, int G) {
+  const int nb = h->nb;
+  const int nblk = (n + nb - 1) / nb;
+  cudaStream_t M = h->stream, P = h->side;
+  EGPU_CUDA_TRY(cudaEventRecord(h->ev_fork, M));
+  EGPU_CUDA_TRY(cudaStreamWaitEvent(P, h->ev_fork, 0));
+  int Gn = 1;  // the current group's size
+  for (int g0 = 0, gi = 0; g0 < nblk; g0 += Gn, ++gi) {
+    Gn = G > 0 ? G : auto_group(n - g0 * nb);
+    const int g1 = std::min(nblk, g0 + Gn);
+    const int kg = g0 * nb, kend = std::min(n, g1 * nb), Kg = kend - kg;  // the group's columns
+    for (int kb = g0; kb < g1; ++kb) {
+      const int k = kb * nb, b = std::min(nb, n - k);
+      if (kb == g0 && gi >= 1) EGPU_CUDA_TRY(cudaStreamWaitEvent(P, h->ev_next[(gi - 1) & 1], 0));
+      if (kb == g0 + 1 && gi >= 1) EGPU_CUDA_TRY(cudaStreamWaitEvent(P, h->ev_rest[(gi - 1) & 1], 0));
+      if (kb > g0) TRY(potrf_update_cols(h, P, uplo, n, A, lda, kg, k - kg, k, k + b));
+      TRY(potrf_panel(h, P, uplo, n, A, lda, k, b, W));
+    }
+    if (g1 == nblk) break;
+    EGPU_CUDA_TRY(cudaEventRecord(h->ev_panel[gi & 1], P));
+    EGPU_CUDA_TRY(cudaStreamWaitEvent(M, h->ev_panel[gi & 1], 0));
+    // the next group's columns [c1, c3): its size decides which of them the
+    // main stream updates before ev_rest
+    const int Gnext = G > 0 ? G : auto_group(n - kend);
+    const int c1 = kend, c2 = std::min(n, c1 + nb), c3 = std::min(n, c1 + Gnext * nb);
+    TRY(potrf_update_cols(h, M, uplo, n, A, lda, kg, Kg, c1, c2));
+    EGPU_CUDA_TRY(cudaEventRecord(h->ev_next[gi & 1], M));
+    TRY(potrf_update_cols(h, M, uplo, n, A, lda, kg, Kg, c2, c3));
+    EGPU_CUDA_TRY(cudaEventRecord(h->ev_rest[gi & 1], M));
+    TRY(potrf_update_cols(h, M, uplo, n, A, lda, kg, Kg, c3, n));
+  }
+  EGPU_CUDA_TRY(cudaEventRecord(h->ev_join, P));
+  EGPU_CUDA_TRY(cudaStreamWaitEvent(M, h->ev_join, 0));
+  return EGPU_OK;
+}
+
 int potrf_core(egpu_context* h, int uplo, int n, double* A, long long lda) {
   const int nb = h->nb;
   TRY(ensure_ws(h, sizeof(double) * (size_t)nb * nb + 4096));
   Carve cv(h->ws);
   double* W = cv.take<double>((size_t)nb * nb);
+  if ((h->lookahead < 0 || h->lookahead >= 2) && n > 2 * nb)
+    return potrf_grouped(h, uplo, n, A, lda, W, h->lookahead);
   if (h->lookahead && n > nb) return potrf_lookahead(h, uplo, n, A, lda, W);
   return potrf_seq(h, uplo, n, A, lda, W);
 }
@@ -541,6 +599,7 @@ int egpu_create(egpu_handle* out, int device) {
       ok = ok && cudaEventCreateWithFlags(&h->ev_rest[i], cudaEventDisableTiming) == cudaSuccess;
       ok = ok && cudaEventCreateWithFlags(&h->ev_split[i], cudaEventDisableTiming) == cudaSuccess;
       ok = ok && cudaEventCreateWithFlags(&h->ev_a21[i], cudaEventDisableTiming) == cudaSuccess;
+      ok = ok && cudaEventCreateWithFlags(&h->ev_next[i], cudaEventDisableTiming) == cudaSuccess;
     }
     if (!ok) {
       set_last_error(cudaGetLastError(), "egpu_create streams", __FILE__, __LINE__);
@@ -565,7 +624,8 @@ int egpu_destroy(egpu_handle h) {
   if (h->side) cudaStreamSynchronize(h->side);
   if (h->aux) cudaStreamSynchronize(h->aux);
   for (cudaEvent_t e : {h->ev_fork, h->ev_join, h->ev_panel[0], h->ev_panel[1], h->ev_rest[0], h->ev_rest[1],
-                        h->ev_split[0], h->ev_split[1], h->ev_aux, h->ev_a21[0], h->ev_a21[1]})
+                        h->ev_split[0], h->ev_split[1], h->ev_aux, h->ev_a21[0], h->ev_a21[1], h->ev_next[0],
+                        h->ev_next[1]})
     if (e) cudaEventDestroy(e);
   if (h->side) cudaStreamDestroy(h->side);
   if (h->aux) cudaStreamDestroy(h->aux);
@@ -625,8 +685,8 @@ int egpu_reserve(egpu_handle h, size_t bytes) {
 
 int egpu_set_lookahead(egpu_handle h, int depth) {
   TRY(check_handle(h));
-  if (depth < 0) return EGPU_ERR_ARG;
-  h->lookahead = depth > 0 ? 1 : 0;
+  if (depth < -1) return EGPU_ERR_ARG;
+  h->lookahead = std::min(depth, 16);
   return EGPU_OK;
 }
 

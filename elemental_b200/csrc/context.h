@@ -74,7 +74,9 @@ struct egpu_context {
   // the mixed chain: a block column's rows below its diagonal block updated
   // (and split) -- the next panel's L21 product waits for it
   cudaEvent_t ev_a21[2] = {nullptr, nullptr};
-  int lookahead = 1;
+  // grouped FP64 Cholesky: the next group's first block column updated
+  cudaEvent_t ev_next[2] = {nullptr, nullptr};
+  int lookahead = -1;  // -1 auto groups, 0 sequential, 1 per-panel, G >= 2 fixed groups (Cholesky)
   int async = 0;  // device API: enqueue only; status read by egpu_get_status
   int gmres_inner = 0;  // GMRES iterations of the last mixed solve
 };

@@ -79,9 +79,14 @@ EGPU_API int egpu_synchronize(egpu_handle h);
  * the panel width; values are rounded to an even number in [2, 128]. */
 EGPU_API int egpu_set_blocksize(egpu_handle h, int nb);
 EGPU_API int egpu_get_blocksize(egpu_handle h);
-/* Panel look-ahead depth (0 = sequential steps on one stream, 1 = default:
- * the next panel is factored on a high-priority side stream while the current
- * trailing update runs).  Results are identical either way. */
+/* Panel look-ahead (0 = sequential steps on one stream; 1 = the next panel is
+ * factored on a high-priority side stream while the current trailing update
+ * runs; G >= 2, Cholesky: the trailing update is applied once per group of G
+ * panels (a G*nb-deep product) while the side stream factors the next group's
+ * panels, each updated just in time; -1 = default: Cholesky picks G per group
+ * from the trailing order (8 above 10240, 4 above 6144, 2 above 4096, else 1).
+ * LU treats any nonzero value as 1; values above 16 are clamped.)  Results
+ * agree to rounding. */
 EGPU_API int egpu_set_lookahead(egpu_handle h, int depth);
 /* Asynchronous mode for the device-memory API: calls only enqueue work on the
  * handle's stream and return EGPU_OK; a failure status (not HPD, singular,

@@ -310,14 +310,17 @@ def test_cholesky_lookahead_matches_sequential(handle, uplo):
     n = 1500
     A = inputs.spd_ggt(n, 61)
     out = []
-    for depth in (0, 1):
+    # 0 sequential, 1 per-panel look-ahead, 2/4 grouped (12 block columns, the
+    # last one 92 wide: groups 4+4+4 and 2x6), 5 ragged groups 5+5+2
+    for depth in (0, 1, 2, 4, 5, -1):
         handle.set_lookahead(depth)
         dA = cuda(A)
         handle.cholesky(dA, uplo)
         out.append(host(dA))
-    handle.set_lookahead(1)
+    handle.set_lookahead(-1)
     tri = np.tril if uplo == eg.LOWER else np.triu
-    assert np.max(np.abs(tri(out[0]) - tri(out[1]))) <= 1e-13 * np.max(np.abs(out[0]))
+    for o in out[1:]:
+        assert np.max(np.abs(tri(out[0]) - tri(o))) <= 1e-13 * np.max(np.abs(out[0]))
 
 
 def test_lu_lookahead_matches_sequential(handle):
@@ -331,7 +334,7 @@ def test_lu_lookahead_matches_sequential(handle):
         dp = torch.zeros(n, dtype=torch.int32, device="cuda")
         handle.lu(dA, dp)
         res.append((host(dA), dp.cpu().numpy()))
-    handle.set_lookahead(1)
+    handle.set_lookahead(-1)
     assert np.array_equal(res[0][1], res[1][1])
     assert np.max(np.abs(res[0][0] - res[1][0])) <= 1e-12 * np.max(np.abs(res[0][0]))
 
