@@ -825,20 +825,36 @@ def kernel_case(args):
     captures (ncu -k ...): 'update' = one lower Herk trailing update
     (n x n, K = 128), 'gemm' = one Gemm trailing update, 'panel' = one LU panel
     (n x 128), 'diag' = one diagonal-block Cholesky (128 x 128), 'mixed' = one
-    mixed-precision HPD solve, 'tc' = the tcgen05 trailing update alone."""
+    mixed-precision HPD solve, 'tc' = the tcgen05 trailing update alone,
+    'chol' = one plain FP64 Cholesky (warm-up call first).  --k sets the inner
+    dimension of 'update' and 'gemm' (default 128)."""
     import torch
     import elemental_b200 as eg
     from elemental_b200 import inputs
     h = eg.Handle(0)
     n = args.n
     if args.case in ("update", "gemm"):
-        A = eg.empty_colmajor(n, NB).normal_()
+        A = eg.empty_colmajor(n, args.k).normal_()
         C = eg.empty_colmajor(n, n).normal_()
         if args.case == "update":
             h.herk(eg.LOWER, eg.NORMAL, -1.0, A, 1.0, C)
         else:
-            Bm = eg.empty_colmajor(NB, n).normal_()
+            Bm = eg.empty_colmajor(args.k, n).normal_()
             h.gemm(eg.NORMAL, eg.NORMAL, -1.0, A, Bm, 1.0, C)
+    elif args.case == "chol":
+        A0 = inputs.spd_spectrum_torch(n, 1e3, SEED, "cuda")
+        A = A0.clone()
+        h.cholesky(A)  # warm-up
+        A.copy_(A0)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        h.cholesky(A)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        print(json.dumps({"case": "chol", "n": n, "ms": ms, "tflops": n ** 3 / 3 / ms / 1e9}))
+        return
     elif args.case == "panel":
         A = eg.colmajor_cuda(inputs.uniform(n, NB, 1))
         p = torch.zeros(NB, dtype=torch.int32, device="cuda")
@@ -922,9 +938,11 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="mixed", choices=sorted(WORKLOADS), help="benchmark configuration")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline leg")
-    ap.add_argument("--case", choices=["update", "gemm", "panel", "diag", "peaks", "mixed", "tc"], default=None,
+    ap.add_argument("--case", choices=["update", "gemm", "panel", "diag", "peaks", "mixed", "tc", "chol"],
+                    default=None,
                     help="run one launch of one kernel class (profiling)")
     ap.add_argument("--n", type=int, default=6144, help="size for --case")
+    ap.add_argument("--k", type=int, default=NB, help="inner dimension for --case update/gemm")
     args = ap.parse_args()
     if args.case:
         kernel_case(args)

@@ -92,8 +92,10 @@ int launch_dgemm(cudaStream_t st, bool a_kmajor, bool b_kmajor, int M, int N, in
   if (tri != 0 && wide) return EGPU_ERR_ARG;
   const int BM = 128, BN = wide ? 128 : 64;
   CUtensorMap ma, mb;
-  bool ok = a_kmajor ? make_map(&ma, A, K, M, lda, kBK, BM, true) : make_map(&ma, A, M, K, lda, BM, kBK, false);
-  ok = ok && (b_kmajor ? make_map(&mb, B, K, N, ldb, kBK, BN, true) : make_map(&mb, B, N, K, ldb, BN, kBK, false));
+  // K-major: one {16 k, BM} box per stage; MN-major: BM / 16 boxes of
+  // {16 m, 16 k} (both 128B-swizzled, see dgemm.cuh)
+  bool ok = a_kmajor ? make_map(&ma, A, K, M, lda, kBK, BM, true) : make_map(&ma, A, M, K, lda, 16, kBK, true);
+  ok = ok && (b_kmajor ? make_map(&mb, B, K, N, ldb, kBK, BN, true) : make_map(&mb, B, N, K, ldb, 16, kBK, true));
   if (!ok) return EGPU_ERR_TMA;
   GemmParams p;
   p.C = C; p.ldc = ldc; p.M = M; p.N = N; p.K = K; p.alpha = alpha; p.beta = beta; p.tri = tri;

@@ -15,9 +15,13 @@
 // DMMA reaches the FP64 peak (37.2 TFLOP/s measured, DFMA 34.1).
 //
 // Shared-memory layouts (no bank conflicts on any fragment load):
-//   MN-major operand (m or n contiguous in global): smem [16 k][BM] plain;
-//     one 16-byte load gives two adjacent rows -> feeds two m16 tiles
-//     (row-interleaved tile pairs).
+//   MN-major operand (m or n contiguous in global): BM/16 boxes of 16 m x
+//     16 k, each [16 k][16 m] (128 B per k row) with the 128B swizzle (16-byte
+//     chunk c of row k at chunk c ^ (k & 7)); one 16-byte load gives two
+//     adjacent rows -> feeds two m16 tiles (row-interleaved tile pairs).  The
+//     four lanes of a quad read k rows 2t (+1) of the same chunk, which the
+//     swizzle spreads over distinct banks (plain [16 k][BM] rows, 8 BM bytes
+//     apart, would put all four in the same banks).
 //   K-major operand (k contiguous in global): smem [BM][16 k], 128B swizzle;
 //     one 16-byte load gives the k pair (2t, 2t+1) of one row.
 // The k index inside each k8 step is permuted (logical t <-> physical 2t,
@@ -47,7 +51,7 @@ struct GemmShape {
   static constexpr int BN = 32 * WARPS_N;
   static constexpr int kThreads = 32 * WARPS_M * WARPS_N;
   static constexpr int kStageBytes = (BM + BN) * kBK * 8;
-  static constexpr int kSmemBytes = kStages * kStageBytes + 1024 /*align*/ + 64 /*barriers*/;
+  static constexpr int kSmemBytes = kStages * kStageBytes + 1024 /*align*/ + 16 * kStages /*barriers*/;
 };
 
 // Map a linear CTA index onto (tile_m, tile_n) for the triangular modes with
@@ -100,6 +104,7 @@ __global__ void __launch_bounds__(32 * WARPS_M * WARPS_N, (WARPS_M * WARPS_N <= 
   extern __shared__ unsigned char smem_raw[];
   unsigned char* smem = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + kStages * S::kStageBytes);
+  uint64_t* empty = full + kStages;  // one arrival per warp when it is done with a stage
 
   int ti, tj;
   if (!map_tile(p, ti, tj)) return;
@@ -115,7 +120,10 @@ __global__ void __launch_bounds__(32 * WARPS_M * WARPS_N, (WARPS_M * WARPS_N <= 
   if (tid == 0) {
     tma_prefetch_desc(&tmA);
     tma_prefetch_desc(&tmB);
-    for (int s = 0; s < kStages; ++s) mbar_init(&full[s], 1);
+    for (int s = 0; s < kStages; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], S::kThreads / 32);
+    }
     fence_mbar_init();
   }
   __syncthreads();
@@ -125,14 +133,25 @@ __global__ void __launch_bounds__(32 * WARPS_M * WARPS_N, (WARPS_M * WARPS_N <= 
     double* sA = reinterpret_cast<double*>(smem + s * S::kStageBytes);
     double* sB = sA + BM * kBK;
     mbar_expect_tx(&full[s], S::kStageBytes);
-    if (AK) tma_load_2d(sA, &tmA, &full[s], kt * kBK, row0);
-    else    tma_load_2d(sA, &tmA, &full[s], row0, kt * kBK);
-    if (BK) tma_load_2d(sB, &tmB, &full[s], kt * kBK, col0);
-    else    tma_load_2d(sB, &tmB, &full[s], col0, kt * kBK);
+    if (AK) {
+      tma_load_2d(sA, &tmA, &full[s], kt * kBK, row0);
+    } else {
+#pragma unroll
+      for (int b = 0; b < BM / 16; ++b) tma_load_2d(sA + b * 256, &tmA, &full[s], row0 + 16 * b, kt * kBK);
+    }
+    if (BK) {
+      tma_load_2d(sB, &tmB, &full[s], kt * kBK, col0);
+    } else {
+#pragma unroll
+      for (int b = 0; b < BN / 16; ++b) tma_load_2d(sB + b * 256, &tmB, &full[s], col0 + 16 * b, kt * kBK);
+    }
   };
 
-  if (tid == 0)
+  int issued = 0;  // k-tiles whose loads thread 0 has issued
+  if (tid == 0) {
     for (int kt = 0; kt < kStages && kt < KT; ++kt) issue(kt);
+    issued = min(kStages, KT);
+  }
   // Pull this tile of C into L2 while the main loop runs, so the epilogue's
   // read-modify-write does not wait on HBM (one bulk prefetch per column).
   if (p.beta != 0.0 && p.cvec) {
@@ -157,7 +176,8 @@ __global__ void __launch_bounds__(32 * WARPS_M * WARPS_N, (WARPS_M * WARPS_N <= 
   for (int kt = 0; kt < KT; ++kt) {
     const int s = kt % kStages;
     const uint32_t parity = (kt / kStages) & 1;
-    if (ok) ok = mbar_wait_bounded(&full[s], parity);
+    // warp-uniform outcome: the DMMAs below need the whole warp converged
+    ok = __all_sync(0xffffffffu, ok && mbar_wait_bounded(&full[s], parity));
     const double* sA = reinterpret_cast<const double*>(smem + s * S::kStageBytes);
     const double* sB = sA + BM * kBK;
 #pragma unroll
@@ -175,13 +195,15 @@ __global__ void __launch_bounds__(32 * WARPS_M * WARPS_N, (WARPS_M * WARPS_N <= 
           af[i][0] = v0.x; af[i][2] = v0.y; af[i][1] = v1.x; af[i][3] = v1.y;
         }
       } else {
+        // box (wm * 64 + pr * 32) / 16 (+1 for rows +16), chunk g of rows ke, ke + 1
+        const int c0 = (g ^ (ke & 7)) << 1, c1 = (g ^ ((ke + 1) & 7)) << 1;
 #pragma unroll
         for (int pr = 0; pr < 2; ++pr) {
-          const int m0 = wm * 64 + pr * 32 + 2 * g;
-          const double2 v00 = *reinterpret_cast<const double2*>(sA + ke * BM + m0);
-          const double2 v01 = *reinterpret_cast<const double2*>(sA + (ke + 1) * BM + m0);
-          const double2 v10 = *reinterpret_cast<const double2*>(sA + ke * BM + m0 + 16);
-          const double2 v11 = *reinterpret_cast<const double2*>(sA + (ke + 1) * BM + m0 + 16);
+          const double* bx = sA + (wm * 4 + pr * 2) * 256;
+          const double2 v00 = *reinterpret_cast<const double2*>(bx + ke * 16 + c0);
+          const double2 v01 = *reinterpret_cast<const double2*>(bx + (ke + 1) * 16 + c1);
+          const double2 v10 = *reinterpret_cast<const double2*>(bx + 256 + ke * 16 + c0);
+          const double2 v11 = *reinterpret_cast<const double2*>(bx + 256 + (ke + 1) * 16 + c1);
           af[2 * pr][0] = v00.x; af[2 * pr][1] = v10.x; af[2 * pr][2] = v01.x; af[2 * pr][3] = v11.x;
           af[2 * pr + 1][0] = v00.y; af[2 * pr + 1][1] = v10.y; af[2 * pr + 1][2] = v01.y; af[2 * pr + 1][3] = v11.y;
         }
@@ -195,11 +217,12 @@ __global__ void __launch_bounds__(32 * WARPS_M * WARPS_N, (WARPS_M * WARPS_N <= 
           bf[j][0] = v.x; bf[j][1] = v.y;
         }
       } else {
+        const int c0 = (g ^ (ke & 7)) << 1, c1 = (g ^ ((ke + 1) & 7)) << 1;
 #pragma unroll
         for (int q = 0; q < 2; ++q) {
-          const int n0 = wn * 32 + q * 16 + 2 * g;
-          const double2 v0 = *reinterpret_cast<const double2*>(sB + ke * BN + n0);
-          const double2 v1 = *reinterpret_cast<const double2*>(sB + (ke + 1) * BN + n0);
+          const double* bx = sB + (wn * 2 + q) * 256;  // box of n rows wn * 32 + q * 16 ..
+          const double2 v0 = *reinterpret_cast<const double2*>(bx + ke * 16 + c0);
+          const double2 v1 = *reinterpret_cast<const double2*>(bx + (ke + 1) * 16 + c1);
           bf[2 * q][0] = v0.x; bf[2 * q][1] = v1.x;
           bf[2 * q + 1][0] = v0.y; bf[2 * q + 1][1] = v1.y;
         }
@@ -209,17 +232,34 @@ __global__ void __launch_bounds__(32 * WARPS_M * WARPS_N, (WARPS_M * WARPS_N <= 
 #pragma unroll
         for (int j = 0; j < 4; ++j) dmma_16x8x8(acc[i][j], af[i], bf[j]);
     }
-    // Every warp is done with stage s: refill it (tid 0) for k-tile kt+kStages.
-    ok = __syncthreads_and(ok);
+    // This warp is done with stage s.  The refill is a TMA write into the
+    // same bytes, and an mbarrier release alone does not order this warp's
+    // generic-proxy reads before an async-proxy write: lane 0 fences (after
+    // the warp has converged) and arrives.  Warp 0 refills the stage for
+    // k-tile kt + kStages once every warp has arrived (the whole warp waits,
+    // lane 0 issues, so warp 0 stays converged); the other warps run ahead
+    // into the stages already loaded instead of meeting at a CTA barrier.
+    __syncwarp();
+    if (lane == 0) {
+      fence_proxy_async_smem();
+      mbar_arrive(&empty[s]);
+    }
+    if (warp == 0 && kt + kStages < KT) {
+      ok = __all_sync(0xffffffffu, ok && mbar_wait_bounded(&empty[s], parity));
+      if (ok && lane == 0) issue(kt + kStages);
+      if (ok) issued = kt + kStages + 1;
+      __syncwarp();
+    }
     if (!ok) break;
-    if (tid == 0 && kt + kStages < KT) issue(kt + kStages);
   }
 
-  if (!ok) {
+  // a warp that gave up (bounded wait) leaves early; all meet here
+  if (!__syncthreads_and(ok)) {
     if (tid == 0) {
       set_status(p.status, kTimeout, 100);
       // Drain copies still in flight before the CTA's shared memory goes away.
-      for (int kt = 0; kt < KT && kt < kStages; ++kt) (void)mbar_wait_bounded(&full[kt % kStages], 0);
+      for (int r = max(0, issued - kStages); r < issued; ++r)
+        (void)mbar_wait_bounded(&full[r % kStages], (r / kStages) & 1);
     }
     __syncthreads();
     return;

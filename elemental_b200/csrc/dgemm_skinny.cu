@@ -119,7 +119,11 @@ __global__ void __launch_bounds__(kSgThreads, 1)
       }
     }
     __syncwarp();
-    if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&empty[slot])) : "memory");
+    // the slot's refill is a TMA write: order this warp's reads of it first
+    if (lane == 0) {
+      fence_proxy_async_smem();
+      mbar_arrive(&empty[slot]);
+    }
   }
 #pragma unroll
   for (int nt = 0; nt < NT; ++nt)

@@ -339,7 +339,11 @@ __device__ void ts_consumers(const TsParams& p, double* sm, uint64_t* fullA, uin
             }
           }
           __syncwarp();
-          if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&empty[slot])) : "memory");
+          // the slot's refill is a TMA write: order this warp's reads of it first
+          if (lane == 0) {
+            fence_proxy_async_smem();
+            mbar_arrive(&empty[slot]);
+          }
         }
       }
       gq += P * cpp;
