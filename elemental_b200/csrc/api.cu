@@ -244,7 +244,7 @@ int potrf_lookahead(egpu_context* h, int uplo, int n, double* A, long long lda, 
 // matrix: deep groups while the main-stream update dominates, single panels
 // once the side chain (diag + Trsm + column update per panel) is the longer.
 static int auto_group(int m_left) {
-  return m_left > 10240 ? 8 : m_left > 6144 ? 4 : m_left > 4096 ? 2 : 1;
+  return m_left > 12288 ? 16 : m_left > 7168 ? 8 : m_left > 5120 ? 4 : m_left > 3072 ? 2 : 1;
 }
 
 int potrf_grouped(egpu_context* h, int uplo, int n, double* A, long long lda, double* W, int G) {

@@ -54,6 +54,17 @@ bool make_tma_2d(CUtensorMap* m, int dtype, const void* base, uint64_t inner, ui
   return r == CUDA_SUCCESS;
 }
 
+static int sm_count_of_current_device() {
+  static int cache[32] = {0};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev >= 0 && dev < 32 && cache[dev] > 0) return cache[dev];
+  int n = 0;
+  if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0) n = 148;
+  if (dev >= 0 && dev < 32) cache[dev] = n;
+  return n;
+}
+
 bool tma_compatible(const void* p, long long ld) {
   return (reinterpret_cast<uintptr_t>(p) % 16 == 0) && (ld % 2 == 0) && ld > 0;
 }
@@ -81,8 +92,10 @@ static cudaError_t launch_variant(cudaStream_t st, const CUtensorMap& ma, const 
 //   a_kmajor = true : A stored K x M column-major (op = TRANSPOSE)
 //   b_kmajor = true : B stored K x N column-major (op = NORMAL)
 //   b_kmajor = false: B stored N x K column-major (op = TRANSPOSE)
-// wide = true selects the 128x128 tile (8 warps), which keeps whole 128-wide
-// row panels inside one CTA (in-place multiply by an inverted triangle).
+// wide = true selects a 128-column tile, which keeps whole 128-wide row panels
+// inside one CTA (in-place multiply by an inverted triangle): 128 x 128 (8
+// warps), or 64 x 128 (4 warps, 2 CTAs/SM) when A is MN-major and 128-row
+// tiles would not fill the SMs twice over.
 int launch_dgemm(cudaStream_t st, bool a_kmajor, bool b_kmajor, int M, int N, int K, double alpha,
                  const double* A, long long lda, const double* B, long long ldb, double beta, double* C,
                  long long ldc, int tri, bool wide, DevStatus* status) {
@@ -90,7 +103,8 @@ int launch_dgemm(cudaStream_t st, bool a_kmajor, bool b_kmajor, int M, int N, in
   if (K <= 0) return launch_scale(st, M, N, beta, C, ldc, tri);
   if (!tma_compatible(A, lda) || !tma_compatible(B, ldb)) return EGPU_ERR_ALIGN;
   if (tri != 0 && wide) return EGPU_ERR_ARG;
-  const int BM = 128, BN = wide ? 128 : 64;
+  const bool half = wide && !a_kmajor && (M + 127) / 128 < 2 * sm_count_of_current_device();
+  const int BM = half ? 64 : 128, BN = wide ? 128 : 64;
   CUtensorMap ma, mb;
   // K-major: one {16 k, BM} box per stage; MN-major: BM / 16 boxes of
   // {16 m, 16 k} (both 128B-swizzled, see dgemm.cuh)
@@ -118,7 +132,10 @@ int launch_dgemm(cudaStream_t st, bool a_kmajor, bool b_kmajor, int M, int N, in
   const double bytes = 8.0 * ((double)M * K + (double)N * K + (beta == 0.0 ? 1.0 : 2.0) * M * N * (tri ? 0.5 : 1.0));
   TraceMark tm(st, beta == 0.0 ? kTraceTrsm : kTraceUpdate, flops, bytes);
   cudaError_t e;
-  if (wide) {
+  if (half) {
+    if (!b_kmajor) e = launch_variant<false, false, 1, 4>(st, ma, mb, p, nblocks);
+    else e = launch_variant<false, true, 1, 4>(st, ma, mb, p, nblocks);
+  } else if (wide) {
     if (!a_kmajor && !b_kmajor) e = launch_variant<false, false, 2, 4>(st, ma, mb, p, nblocks);
     else if (!a_kmajor && b_kmajor) e = launch_variant<false, true, 2, 4>(st, ma, mb, p, nblocks);
     else if (a_kmajor && !b_kmajor) e = launch_variant<true, false, 2, 4>(st, ma, mb, p, nblocks);
