@@ -243,6 +243,11 @@ int potrf_lookahead(egpu_context* h, int uplo, int n, double* A, long long lda, 
 // G <= 0 selects the group size per group from the order of the trailing
 // matrix: deep groups while the main-stream update dominates, single panels
 // once the side chain (diag + Trsm + column update per panel) is the longer.
+// The first groups are kept short (2, then 8 panels): until a group is
+// factored the main stream has nothing to update, and the first update (K =
+// 2 nb over the whole matrix) is long enough to hide the next group's chain.
+static const int kRamp[4] = {2, 8, 16, 16};
+
 static int auto_group(int m_left) {
   return m_left > 12288 ? 16 : m_left > 7168 ? 8 : m_left > 5120 ? 4 : m_left > 3072 ? 2 : 1;
 }
@@ -255,7 +260,7 @@ int potrf_grouped(egpu_context* h, int uplo, int n, double* A, long long lda, do
   EGPU_CUDA_TRY(cudaStreamWaitEvent(P, h->ev_fork, 0));
   int Gn = 1;  // the current group's size
   for (int g0 = 0, gi = 0; g0 < nblk; g0 += Gn, ++gi) {
-    Gn = G > 0 ? G : auto_group(n - g0 * nb);
+    Gn = G > 0 ? G : std::min(auto_group(n - g0 * nb), kRamp[std::min(gi, 3)]);
     const int g1 = std::min(nblk, g0 + Gn);
     const int kg = g0 * nb, kend = std::min(n, g1 * nb), Kg = kend - kg;  // the group's columns
     for (int kb = g0; kb < g1; ++kb) {
@@ -270,7 +275,7 @@ int potrf_grouped(egpu_context* h, int uplo, int n, double* A, long long lda, do
     EGPU_CUDA_TRY(cudaStreamWaitEvent(M, h->ev_panel[gi & 1], 0));
     // the next group's columns [c1, c3): its size decides which of them the
     // main stream updates before ev_rest
-    const int Gnext = G > 0 ? G : auto_group(n - kend);
+    const int Gnext = G > 0 ? G : std::min(auto_group(n - kend), kRamp[std::min(gi + 1, 3)]);
     const int c1 = kend, c2 = std::min(n, c1 + nb), c3 = std::min(n, c1 + Gnext * nb);
     TRY(potrf_update_cols(h, M, uplo, n, A, lda, kg, Kg, c1, c2));
     EGPU_CUDA_TRY(cudaEventRecord(h->ev_next[gi & 1], M));

@@ -85,7 +85,7 @@ EGPU_API int egpu_get_blocksize(egpu_handle h);
  * panels (a G*nb-deep product) while the side stream factors the next group's
  * panels, each updated just in time; -1 = default: Cholesky picks G per group
  * from the trailing order (16 above 12288, 8 above 7168, 4 above 5120, 2 above
- * 3072, else 1).
+ * 3072, else 1; the first two groups at most 2 and 8 panels).
  * LU treats any nonzero value as 1; values above 16 are clamped.)  Results
  * agree to rounding. */
 EGPU_API int egpu_set_lookahead(egpu_handle h, int depth);
