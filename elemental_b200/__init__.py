@@ -144,6 +144,16 @@ def _declare(L):
         "egpu_host_dgemm": ([H, I, I, I, I, I, D, P, I, P, I, D, P, I], I),
         "egpu_host_dherk": ([H, I, I, I, I, D, P, I, D, P, I], I),
         "egpu_host_dlaswp": ([H, I, I, I, P, I, P, I], I),
+        "egpu_dtrtri": ([H, I, I, I, P, I], I),
+        "egpu_dgetri": ([H, I, P, I, P], I),
+        "egpu_dpotri": ([H, I, I, P, I, P], I),
+        "egpu_dsafe_det": ([H, I, P, I, I, P, P], I),
+        "egpu_dsafe_hpd_det": ([H, I, I, P, I, I, P, P], I),
+        "egpu_host_dtrtri": ([H, I, I, I, P, I], I),
+        "egpu_host_dgetri": ([H, I, P, I, P], I),
+        "egpu_host_dpotri": ([H, I, I, P, I, P], I),
+        "egpu_host_dsafe_det": ([H, I, P, I, I, P, P], I),
+        "egpu_host_dsafe_hpd_det": ([H, I, I, P, I, I, P, P], I),
     }
     for name, (args, res) in sig.items():
         if hasattr(L, name):
@@ -471,6 +481,83 @@ class Handle:
         info = ctypes.c_int(0)
         rc = lib().egpu_dgetrf(self._h, A.shape[0], A.shape[1], _ptr(A), _ld(A), _ptr(p), ctypes.byref(info))
         _check(rc, info.value)
+
+    # ---- TriangularInverse / Inverse / HPDInverse / (Safe)Determinant ----
+
+    def triangular_inverse(self, A, uplo=LOWER, diag=NON_UNIT):
+        """TriangularInverse(uplo, diag, A) in place (the other triangle untouched)."""
+        self._bind_stream()
+        _check(lib().egpu_dtrtri(self._h, uplo, diag, A.shape[0], _ptr(A), _ld(A)))
+
+    def inverse(self, A):
+        """Inverse(A) in place via LU with partial pivoting."""
+        self._bind_stream()
+        info = ctypes.c_int(0)
+        rc = lib().egpu_dgetri(self._h, A.shape[0], _ptr(A), _ld(A), ctypes.byref(info))
+        _check(rc, info.value)
+
+    def hpd_inverse(self, A, uplo=LOWER):
+        """HPDInverse(uplo, A): the uplo triangle of A := that of inv(A)."""
+        self._bind_stream()
+        info = ctypes.c_int(0)
+        rc = lib().egpu_dpotri(self._h, uplo, A.shape[0], _ptr(A), _ld(A), ctypes.byref(info))
+        _check(rc, info.value)
+
+    def safe_determinant(self, A, overwrite=False):
+        """SafeDeterminant(A): (rho, kappa, n) with det(A) = rho * exp(kappa * n)."""
+        self._bind_stream()
+        rho, kappa = ctypes.c_double(0), ctypes.c_double(0)
+        _check(lib().egpu_dsafe_det(self._h, A.shape[0], _ptr(A), _ld(A), int(bool(overwrite)),
+                                    ctypes.byref(rho), ctypes.byref(kappa)))
+        return rho.value, kappa.value, A.shape[0]
+
+    def safe_hpd_determinant(self, A, uplo=LOWER, overwrite=False):
+        """SafeHPDDeterminant(uplo, A): (rho, kappa, n), rho = 1 (0 if not HPD)."""
+        self._bind_stream()
+        rho, kappa = ctypes.c_double(0), ctypes.c_double(0)
+        _check(lib().egpu_dsafe_hpd_det(self._h, uplo, A.shape[0], _ptr(A), _ld(A), int(bool(overwrite)),
+                                        ctypes.byref(rho), ctypes.byref(kappa)))
+        return rho.value, kappa.value, A.shape[0]
+
+    def determinant(self, A):
+        """Determinant(A) = rho * exp(kappa * n) (Determinant.hpp)."""
+        rho, kappa, n = self.safe_determinant(A)
+        return rho * float(np.exp(kappa * n))
+
+    def hpd_determinant(self, A, uplo=LOWER):
+        """HPDDeterminant(uplo, A) = exp(kappa * n)."""
+        _, kappa, n = self.safe_hpd_determinant(A, uplo)
+        return float(np.exp(kappa * n))
+
+    def host_triangular_inverse(self, A: np.ndarray, uplo=LOWER, diag=NON_UNIT):
+        A = _np_f(A)
+        _check(lib().egpu_host_dtrtri(self._h, uplo, diag, A.shape[0], _np_ptr(A), max(A.shape[0], 1)))
+
+    def host_inverse(self, A: np.ndarray):
+        A = _np_f(A)
+        info = ctypes.c_int(0)
+        rc = lib().egpu_host_dgetri(self._h, A.shape[0], _np_ptr(A), max(A.shape[0], 1), ctypes.byref(info))
+        _check(rc, info.value)
+
+    def host_hpd_inverse(self, A: np.ndarray, uplo=LOWER):
+        A = _np_f(A)
+        info = ctypes.c_int(0)
+        rc = lib().egpu_host_dpotri(self._h, uplo, A.shape[0], _np_ptr(A), max(A.shape[0], 1), ctypes.byref(info))
+        _check(rc, info.value)
+
+    def host_safe_determinant(self, A: np.ndarray, overwrite=False):
+        A = _np_f(A)
+        rho, kappa = ctypes.c_double(0), ctypes.c_double(0)
+        _check(lib().egpu_host_dsafe_det(self._h, A.shape[0], _np_ptr(A), max(A.shape[0], 1), int(bool(overwrite)),
+                                         ctypes.byref(rho), ctypes.byref(kappa)))
+        return rho.value, kappa.value, A.shape[0]
+
+    def host_safe_hpd_determinant(self, A: np.ndarray, uplo=LOWER, overwrite=False):
+        A = _np_f(A)
+        rho, kappa = ctypes.c_double(0), ctypes.c_double(0)
+        _check(lib().egpu_host_dsafe_hpd_det(self._h, uplo, A.shape[0], _np_ptr(A), max(A.shape[0], 1),
+                                             int(bool(overwrite)), ctypes.byref(rho), ctypes.byref(kappa)))
+        return rho.value, kappa.value, A.shape[0]
 
     def lu_nopiv(self, A):
         self._bind_stream()

@@ -536,6 +536,92 @@ int gesv_core(egpu_context* h, int n, int nrhs, double* A, long long lda, double
   return trsm_core(h, EGPU_LEFT, EGPU_UPPER, 0, 0, n, nrhs, 1.0, A, lda, B, ldb);
 }
 
+// TriangularInverse (lapack-like/TriangularInverse.hpp:56-64): the uplo
+// triangle of A := its inverse, by the blocked Trsm against the identity in
+// staging slot 3; the other triangle (and, for UNIT, the diagonal) is not
+// touched.
+int trtri_core(egpu_context* h, int uplo, int unit, int n, double* A, long long lda) {
+  const long long ldx = ld_aligned(n);
+  TRY(ensure_stage(h, 3, sizeof(double) * (size_t)ldx * n));
+  double* X = static_cast<double*>(h->stage[3]);
+  TRY(launch_set_identity(h->stream, n, X, ldx));
+  TRY(trsm_core(h, EGPU_LEFT, uplo, 0, unit, n, n, 1.0, A, lda, X, ldx));
+  return launch_copy_triangle(h->stream, uplo, unit != 0, n, X, ldx, A, lda);
+}
+
+// Inverse (Inverse.hpp:17-23 -> inverse::LUPartialPiv, Inverse/LUPartialPiv.hpp):
+// P A = L U, then A := inv(A) as the solution of A X = I (lu::SolveAfter on
+// the identity).  A singular pivot stops with EGPU_SINGULAR (SingularMatrix-
+// Exception from lu::Panel), A then holding the partial factorization.
+int getri_core(egpu_context* h, int n, double* A, long long lda, int* info) {
+  int* dp = static_cast<int*>(h->stage[2]);
+  TRY(getrf_core(h, n, n, A, lda, dp));
+  TRY(read_status(h, info));
+  const long long ldx = ld_aligned(n);
+  TRY(ensure_stage(h, 3, sizeof(double) * (size_t)ldx * n));
+  double* X = static_cast<double*>(h->stage[3]);
+  TRY(launch_set_identity(h->stream, n, X, ldx));
+  TRY(getrs_core(h, EGPU_NORMAL, n, n, A, lda, dp, X, ldx));
+  return launch_copy(h->stream, n, n, X, ldx, A, lda);
+}
+
+// HPDInverse (Inverse.hpp:25-35 -> hpd_inverse::CholeskyLVar2 / UVar2): the
+// uplo triangle of A := that of inv(A), from the Cholesky factor and
+// cholesky::SolveAfter on the identity; the other triangle is not touched.
+// A non-HPD input stops with EGPU_NOT_HPD.
+int potri_core(egpu_context* h, int uplo, int n, double* A, long long lda, int* info) {
+  TRY(potrf_core(h, uplo, n, A, lda));
+  TRY(read_status(h, info));
+  const long long ldx = ld_aligned(n);
+  TRY(ensure_stage(h, 3, sizeof(double) * (size_t)ldx * n));
+  double* X = static_cast<double*>(h->stage[3]);
+  TRY(launch_set_identity(h->stream, n, X, ldx));
+  TRY(potrs_core(h, uplo, n, n, A, lda, X, ldx));
+  return launch_copy_triangle(h->stream, uplo, false, n, X, ldx, A, lda);
+}
+
+// SafeDeterminant (Determinant.hpp, determinant::LUPartialPiv,
+// Determinant/LUPartialPiv.hpp:17-67) and SafeHPDDeterminant
+// (hpd_determinant::Cholesky, Determinant/Cholesky.hpp:17-55) on the work
+// matrix W (factored in place): det = rho exp(kappa n).  LU: rho = the signs
+// of U's diagonal times (-1)^(pivot parity, PivotParity.hpp:17-33), kappa =
+// sum log|u_ii| / n.  Cholesky: rho = 1, kappa = sum log l_ii / (n / 2).  A
+// singular (LU) or non-HPD (Cholesky) matrix gives rho = kappa = 0, as the
+// reference catches its exception.  Always synchronous: the values return to
+// the host.
+int safe_det_core(egpu_context* h, int hpd, int uplo, int n, double* W, long long ldw, double* rho,
+                  double* kappa) {
+  *rho = 1.0;
+  *kappa = 0.0;
+  if (n == 0) return EGPU_OK;
+  const size_t piv_bytes = align_up(sizeof(int) * (size_t)n, 256);
+  TRY(ensure_stage(h, 2, piv_bytes + 64));
+  int* dp = static_cast<int*>(h->stage[2]);
+  double* dout = reinterpret_cast<double*>(static_cast<unsigned char*>(h->stage[2]) + piv_bytes);
+  EGPU_CUDA_TRY(cudaMemsetAsync(h->dstatus, 0, sizeof(DevStatus), h->stream));
+  if (hpd) TRY(potrf_core(h, uplo, n, W, ldw));
+  else TRY(getrf_core(h, n, n, W, ldw, dp));
+  int rc = read_status_now(h, nullptr);
+  if (rc == (hpd ? EGPU_NOT_HPD : EGPU_SINGULAR)) {
+    EGPU_CUDA_TRY(cudaMemsetAsync(h->dstatus, 0, sizeof(DevStatus), h->stream));
+    *rho = 0.0;
+    return EGPU_OK;
+  }
+  TRY(rc);
+  TRY(launch_diag_logsum(h->stream, n, W, ldw, hpd ? nullptr : dp, dout));
+  double out[3];
+  EGPU_CUDA_TRY(cudaMemcpyAsync(out, dout, sizeof(out), cudaMemcpyDeviceToHost, h->stream));
+  EGPU_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  if (hpd) {
+    *kappa = out[0] / (0.5 * n);
+  } else {
+    *kappa = out[0] / n;
+    const long long flips = (long long)out[1] + (long long)out[2];
+    *rho = (flips & 1) ? -1.0 : 1.0;
+  }
+  return EGPU_OK;
+}
+
 // ----- operand repacking for TMA alignment -----
 
 int pack(egpu_context* h, int slot, Operand& op, bool copy_in) {
@@ -622,7 +708,7 @@ int egpu_destroy(egpu_handle h) {
   Enter g(h);
   if (h->stream) cudaStreamSynchronize(h->stream);
   if (h->ws) cudaFree(h->ws);
-  for (int i = 0; i < 3; ++i)
+  for (int i = 0; i < egpu_context::kStageSlots; ++i)
     if (h->stage[i]) cudaFree(h->stage[i]);
   if (h->dstatus) cudaFree(h->dstatus);
   if (h->hstatus) cudaFreeHost(h->hstatus);
@@ -1012,6 +1098,83 @@ int egpu_dlaswp(egpu_handle h, int inverse, int m, int n, double* dA, int lda, c
   return EGPU_OK;
 }
 
+int egpu_dtrtri(egpu_handle h, int uplo, int diag, int n, double* dA, int lda) {
+  TRY(check_handle(h));
+  if (n < 0 || (uplo != EGPU_LOWER && uplo != EGPU_UPPER) || bad_ld(lda, n)) return EGPU_ERR_ARG;
+  if (n == 0) return EGPU_OK;
+  Enter g(h);
+  Operand A = make_op(dA, lda, n, n);
+  TRY(pack(h, 0, A, true));
+  TRY(reset_status(h));
+  TRY(trtri_core(h, uplo, diag == EGPU_UNIT, n, A.ptr, A.ld));
+  TRY(unpack(h, A));
+  return read_status(h, nullptr);
+}
+
+int egpu_dgetri(egpu_handle h, int n, double* dA, int lda, int* info) {
+  TRY(check_handle(h));
+  if (info) *info = 0;
+  if (n < 0 || bad_ld(lda, n)) return EGPU_ERR_ARG;
+  if (n == 0) return EGPU_OK;
+  Enter g(h);
+  TRY(ensure_stage(h, 2, sizeof(int) * (size_t)n));
+  Operand A = make_op(dA, lda, n, n);
+  TRY(pack(h, 0, A, true));
+  TRY(reset_status(h));
+  int rc = getri_core(h, n, A.ptr, A.ld, info);
+  TRY(unpack(h, A));
+  TRY(rc);
+  return read_status(h, info);
+}
+
+int egpu_dpotri(egpu_handle h, int uplo, int n, double* dA, int lda, int* info) {
+  TRY(check_handle(h));
+  if (info) *info = 0;
+  if (n < 0 || (uplo != EGPU_LOWER && uplo != EGPU_UPPER) || bad_ld(lda, n)) return EGPU_ERR_ARG;
+  if (n == 0) return EGPU_OK;
+  Enter g(h);
+  Operand A = make_op(dA, lda, n, n);
+  TRY(pack(h, 0, A, true));
+  TRY(reset_status(h));
+  int rc = potri_core(h, uplo, n, A.ptr, A.ld, info);
+  TRY(unpack(h, A));
+  TRY(rc);
+  return read_status(h, info);
+}
+
+// The determinant's work matrix: A itself when overwrite (factored in place),
+// else a copy in staging slot 3.
+static int safe_det_device(egpu_handle h, int hpd, int uplo, int n, double* dA, int lda, int overwrite, double* rho,
+                           double* kappa) {
+  TRY(check_handle(h));
+  if (!rho || !kappa || n < 0 || bad_ld(lda, n) || (hpd && uplo != EGPU_LOWER && uplo != EGPU_UPPER))
+    return EGPU_ERR_ARG;
+  Enter g(h);
+  if (n == 0) return safe_det_core(h, hpd, uplo, n, dA, lda, rho, kappa);
+  if (overwrite) {
+    Operand A = make_op(dA, lda, n, n);
+    TRY(pack(h, 0, A, true));
+    TRY(safe_det_core(h, hpd, uplo, n, A.ptr, A.ld, rho, kappa));
+    TRY(unpack(h, A));
+    EGPU_CUDA_TRY(cudaStreamSynchronize(h->stream));
+    return EGPU_OK;
+  }
+  const long long ldw = ld_aligned(n);
+  TRY(ensure_stage(h, 3, sizeof(double) * (size_t)ldw * n));
+  double* W = static_cast<double*>(h->stage[3]);
+  TRY(launch_copy(h->stream, n, n, dA, lda, W, ldw));
+  return safe_det_core(h, hpd, uplo, n, W, ldw, rho, kappa);
+}
+
+int egpu_dsafe_det(egpu_handle h, int n, double* dA, int lda, int overwrite, double* rho, double* kappa) {
+  return safe_det_device(h, 0, EGPU_LOWER, n, dA, lda, overwrite, rho, kappa);
+}
+
+int egpu_dsafe_hpd_det(egpu_handle h, int uplo, int n, double* dA, int lda, int overwrite, double* rho,
+                       double* kappa) {
+  return safe_det_device(h, 1, uplo, n, dA, lda, overwrite, rho, kappa);
+}
+
 // ------------------------------------------------------------ host API --
 // Copy host column-major buffers into handle staging memory (ld multiple of
 // 32), run the device path, copy results back.
@@ -1265,6 +1428,81 @@ int egpu_host_dlaswp(egpu_handle h, int inverse, int m, int n, double* A, int ld
   TRY(d2h(h, dA, la, A, lda, m, n));
   EGPU_CUDA_TRY(cudaStreamSynchronize(h->stream));
   return EGPU_OK;
+}
+
+int egpu_host_dtrtri(egpu_handle h, int uplo, int diag, int n, double* A, int lda) {
+  TRY(check_handle(h));
+  if (n < 0 || (uplo != EGPU_LOWER && uplo != EGPU_UPPER) || bad_ld(lda, n)) return EGPU_ERR_ARG;
+  if (n == 0) return EGPU_OK;
+  Enter g(h);
+  SyncScope ss(h);
+  double* d; long long ld;
+  TRY(h2d(h, 0, A, lda, n, n, &d, &ld));
+  TRY(reset_status(h));
+  TRY(trtri_core(h, uplo, diag == EGPU_UNIT, n, d, ld));
+  TRY(d2h(h, d, ld, A, lda, n, n));
+  return read_status(h, nullptr);
+}
+
+int egpu_host_dgetri(egpu_handle h, int n, double* A, int lda, int* info) {
+  TRY(check_handle(h));
+  if (info) *info = 0;
+  if (n < 0 || bad_ld(lda, n)) return EGPU_ERR_ARG;
+  if (n == 0) return EGPU_OK;
+  Enter g(h);
+  SyncScope ss(h);
+  double* d; long long ld;
+  TRY(h2d(h, 0, A, lda, n, n, &d, &ld));
+  if (!stage_ints(h, 2, n)) return EGPU_ERR_ALLOC;
+  TRY(reset_status(h));
+  int rc = getri_core(h, n, d, ld, info);
+  if (rc < 0) return rc;
+  TRY(d2h(h, d, ld, A, lda, n, n));
+  TRY(rc);
+  return read_status(h, info);
+}
+
+int egpu_host_dpotri(egpu_handle h, int uplo, int n, double* A, int lda, int* info) {
+  TRY(check_handle(h));
+  if (info) *info = 0;
+  if (n < 0 || (uplo != EGPU_LOWER && uplo != EGPU_UPPER) || bad_ld(lda, n)) return EGPU_ERR_ARG;
+  if (n == 0) return EGPU_OK;
+  Enter g(h);
+  SyncScope ss(h);
+  double* d; long long ld;
+  TRY(h2d(h, 0, A, lda, n, n, &d, &ld));
+  TRY(reset_status(h));
+  int rc = potri_core(h, uplo, n, d, ld, info);
+  if (rc < 0) return rc;
+  TRY(d2h(h, d, ld, A, lda, n, n));
+  TRY(rc);
+  return read_status(h, info);
+}
+
+static int safe_det_host(egpu_handle h, int hpd, int uplo, int n, double* A, int lda, int overwrite, double* rho,
+                         double* kappa) {
+  TRY(check_handle(h));
+  if (!rho || !kappa || n < 0 || bad_ld(lda, n) || (hpd && uplo != EGPU_LOWER && uplo != EGPU_UPPER))
+    return EGPU_ERR_ARG;
+  Enter g(h);
+  SyncScope ss(h);
+  double* d = nullptr; long long ld = 1;
+  if (n > 0) TRY(h2d(h, 0, A, lda, n, n, &d, &ld));
+  TRY(safe_det_core(h, hpd, uplo, n, d, ld, rho, kappa));
+  if (overwrite && n > 0) {  // canOverwrite: A receives the factorization
+    TRY(d2h(h, d, ld, A, lda, n, n));
+    EGPU_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  }
+  return EGPU_OK;
+}
+
+int egpu_host_dsafe_det(egpu_handle h, int n, double* A, int lda, int overwrite, double* rho, double* kappa) {
+  return safe_det_host(h, 0, EGPU_LOWER, n, A, lda, overwrite, rho, kappa);
+}
+
+int egpu_host_dsafe_hpd_det(egpu_handle h, int uplo, int n, double* A, int lda, int overwrite, double* rho,
+                            double* kappa) {
+  return safe_det_host(h, 1, uplo, n, A, lda, overwrite, rho, kappa);
 }
 
 }  // extern "C"

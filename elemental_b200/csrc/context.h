@@ -59,8 +59,11 @@ struct egpu_context {
   DevStatus* dstatus = nullptr;
   DevStatus* hstatus = nullptr;  // pinned
   // host-API staging buffers
-  void* stage[3] = {nullptr, nullptr, nullptr};
-  size_t stage_bytes[3] = {0, 0, 0};
+  // staging slots: 0, 1 operand copies; 2 pivots (+ small results); 3 the
+  // n x n right-hand side of the inverses / the determinant's copy of A
+  static constexpr int kStageSlots = 4;
+  void* stage[kStageSlots] = {nullptr, nullptr, nullptr, nullptr};
+  size_t stage_bytes[kStageSlots] = {0, 0, 0, 0};
   Trace trace;
   // look-ahead: a high-priority side stream for the panel chain and events
   // joining it with the update chain on `stream`

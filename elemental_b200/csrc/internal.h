@@ -135,6 +135,15 @@ int egpu_batched_launch(int kind, cudaStream_t st, int sm_count, int count, cons
                         double* const* A, const int* lda, double* const* B, const int* ldb, void* ws,
                         size_t ws_bytes, int* info_host);
 
+// TriangularInverse / Inverse / Determinant helpers (inverse.cu).
+int launch_set_identity(cudaStream_t st, int n, double* X, long long ldx);
+// D's uplo triangle (strict: below/above the diagonal only) := S's.
+int launch_copy_triangle(cudaStream_t st, int uplo, bool strict, int n, const double* S, long long lds, double* D,
+                         long long ldd);
+// out[0..2] = sum log|a_ii|, count of a_ii < 0, count of p[i] != i (p may be
+// null); one deterministic block reduction.
+int launch_diag_logsum(cudaStream_t st, int n, const double* A, long long lda, const int* p, double* out);
+
 // Copy between strided device matrices.
 int launch_copy(cudaStream_t st, int m, int n, const double* src, long long lds, double* dst, long long ldd);
 

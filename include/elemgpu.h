@@ -290,6 +290,40 @@ EGPU_API int egpu_dherk(egpu_handle h, int uplo, int orient, int n, int k, doubl
  * lapack-like/ApplyRowPivots.hpp:17-79 (sequential swaps i <-> p[i]). */
 EGPU_API int egpu_dlaswp(egpu_handle h, int inverse, int m, int n, double* dA, int lda, const int* dp, int npiv);
 
+/* TriangularInverse(uplo, diag, A), lapack-like/TriangularInverse.hpp:56-64
+ * (triangular_inverse::LVar3 / UVar3): the uplo triangle of A := its inverse;
+ * the other triangle, and for diag = EGPU_UNIT the diagonal, are not
+ * touched.  No singularity check (as the reference). */
+EGPU_API int egpu_dtrtri(egpu_handle h, int uplo, int diag, int n, double* dA, int lda);
+
+/* Inverse(A), lapack-like/Inverse.hpp:17-23 (inverse::LUPartialPiv,
+ * Inverse/LUPartialPiv.hpp): A := inv(A) from P A = L U.  Returns
+ * EGPU_SINGULAR (info = the 1-based column of the zero pivot, lu::Panel's
+ * SingularMatrixException) with A holding the partial factorization. */
+EGPU_API int egpu_dgetri(egpu_handle h, int n, double* dA, int lda, int* info);
+
+/* HPDInverse(uplo, A), lapack-like/Inverse.hpp:25-35 (hpd_inverse::
+ * CholeskyLVar2 / CholeskyUVar2): the uplo triangle of A := that of inv(A);
+ * the other triangle is not touched.  EGPU_NOT_HPD as egpu_dpotrf. */
+EGPU_API int egpu_dpotri(egpu_handle h, int uplo, int n, double* dA, int lda, int* info);
+
+/* SafeDeterminant(A[, canOverwrite]), lapack-like/Determinant.hpp (
+ * determinant::LUPartialPiv, Determinant/LUPartialPiv.hpp:17-67 with
+ * PivotParity.hpp:17-33): det(A) = rho * exp(kappa * n), rho = +-1, kappa =
+ * sum log|u_ii| / n.  A singular matrix gives rho = kappa = 0 and EGPU_OK (the
+ * reference catches SingularMatrixException).  overwrite != 0 factors A in
+ * place (canOverwrite); otherwise A is copied first and left unchanged.
+ * Synchronous in either handle mode (the values return to the host); it
+ * clears the handle's device status. */
+EGPU_API int egpu_dsafe_det(egpu_handle h, int n, double* dA, int lda, int overwrite, double* rho, double* kappa);
+
+/* SafeHPDDeterminant(uplo, A[, canOverwrite]), Determinant.hpp
+ * (hpd_determinant::Cholesky, Determinant/Cholesky.hpp:17-55): rho = 1, kappa
+ * = sum log l_ii / (n / 2); a matrix that is not numerically HPD gives rho =
+ * kappa = 0 and EGPU_OK.  Otherwise as egpu_dsafe_det. */
+EGPU_API int egpu_dsafe_hpd_det(egpu_handle h, int uplo, int n, double* dA, int lda, int overwrite, double* rho,
+                                double* kappa);
+
 /* Cholesky factorization that allocates no device memory (no counterpart in
  * the reference).  For callers that cannot let a library allocate: a process
  * that gives all device memory to its own pool at start-up and must not see an
@@ -321,6 +355,14 @@ EGPU_API int egpu_host_dgemm(egpu_handle h, int orientA, int orientB, int m, int
 EGPU_API int egpu_host_dherk(egpu_handle h, int uplo, int orient, int n, int k, double alpha, const double* A, int lda,
                     double beta, double* C, int ldc);
 EGPU_API int egpu_host_dlaswp(egpu_handle h, int inverse, int m, int n, double* A, int lda, const int* p, int npiv);
+EGPU_API int egpu_host_dtrtri(egpu_handle h, int uplo, int diag, int n, double* A, int lda);
+EGPU_API int egpu_host_dgetri(egpu_handle h, int n, double* A, int lda, int* info);
+EGPU_API int egpu_host_dpotri(egpu_handle h, int uplo, int n, double* A, int lda, int* info);
+/* overwrite != 0 (canOverwrite): A receives the factorization; otherwise A is
+ * only read. */
+EGPU_API int egpu_host_dsafe_det(egpu_handle h, int n, double* A, int lda, int overwrite, double* rho, double* kappa);
+EGPU_API int egpu_host_dsafe_hpd_det(egpu_handle h, int uplo, int n, double* A, int lda, int overwrite, double* rho,
+                                     double* kappa);
 
 #ifdef __cplusplus
 }

@@ -25,6 +25,7 @@
 #pragma once
 
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <memory>
 #include <stack>
@@ -521,6 +522,111 @@ inline void ApplyInverseRowPivots(Matrix<F>& A, const Matrix<int>& p) {
   a.WriteBack(A);
 }
 
+// ------------------------------ inverses and determinants (next rows) -----
+
+// SafeProduct<F> (core/types_decl.hpp:24-31): det = rho * exp(kappa * n).
+template <typename F>
+struct SafeProduct {
+  F rho;
+  F kappa;
+  int n;
+  explicit SafeProduct(int numEntries) : rho(1), kappa(0), n(numEntries) {}
+};
+
+// TriangularInverse(uplo, diag, A), lapack-like/TriangularInverse.hpp:56-64.
+template <typename F>
+inline void TriangularInverse(UpperOrLower uplo, UnitOrNonUnit diag, Matrix<F>& A) {
+  static_assert(detail::IsSupported<F>::value, "elemgpu supports float and double");
+  if (A.Height() != A.Width()) throw std::logic_error("Nonsquare matrices cannot be triangular");
+  detail::AsDouble<F> a(A, true);
+  int rc = egpu_host_dtrtri(detail::handle(), uplo == LOWER ? EGPU_LOWER : EGPU_UPPER,
+                            diag == UNIT ? EGPU_UNIT : EGPU_NON_UNIT, A.Height(), a.p, a.ld);
+  a.WriteBack(A);
+  detail::check(rc);
+}
+
+// Inverse(A), lapack-like/Inverse.hpp:17-23 (inverse::LUPartialPiv).  Throws
+// SingularMatrixException on an exact zero pivot.
+template <typename F>
+inline void Inverse(Matrix<F>& A) {
+  static_assert(detail::IsSupported<F>::value, "elemgpu supports float and double");
+  if (A.Height() != A.Width()) throw std::logic_error("Cannot invert non-square matrices");
+  detail::AsDouble<F> a(A, true);
+  int info = 0;
+  int rc = egpu_host_dgetri(detail::handle(), A.Height(), a.p, a.ld, &info);
+  a.WriteBack(A);
+  detail::check(rc, info);
+}
+
+// HPDInverse(uplo, A), lapack-like/Inverse.hpp:25-35 (hpd_inverse::
+// CholeskyLVar2 / UVar2): only the uplo triangle of A is written.
+template <typename F>
+inline void HPDInverse(UpperOrLower uplo, Matrix<F>& A) {
+  static_assert(detail::IsSupported<F>::value, "elemgpu supports float and double");
+  if (A.Height() != A.Width()) throw std::logic_error("Nonsquare matrices cannot be triangular");
+  detail::AsDouble<F> a(A, true);
+  int info = 0;
+  int rc = egpu_host_dpotri(detail::handle(), uplo == LOWER ? EGPU_LOWER : EGPU_UPPER, A.Height(), a.p, a.ld, &info);
+  a.WriteBack(A);
+  detail::check(rc, info);
+}
+
+namespace detail {
+template <typename F>
+inline SafeProduct<F> safe_det(int hpd, UpperOrLower uplo, Matrix<F>& A, bool canOverwrite) {
+  static_assert(IsSupported<F>::value, "elemgpu supports float and double");
+  if (A.Height() != A.Width()) throw std::logic_error("Cannot compute determinant of nonsquare matrix");
+  AsDouble<F> a(A, true);
+  double rho = 1.0, kappa = 0.0;
+  int rc = hpd ? egpu_host_dsafe_hpd_det(handle(), uplo == LOWER ? EGPU_LOWER : EGPU_UPPER, A.Height(), a.p, a.ld,
+                                         canOverwrite ? 1 : 0, &rho, &kappa)
+               : egpu_host_dsafe_det(handle(), A.Height(), a.p, a.ld, canOverwrite ? 1 : 0, &rho, &kappa);
+  if (canOverwrite) a.WriteBack(A);
+  check(rc);
+  SafeProduct<F> det(A.Height());
+  det.rho = F(rho);
+  det.kappa = F(kappa);
+  return det;
+}
+}  // namespace detail
+
+// SafeDeterminant(A[, canOverwrite]), lapack-like/Determinant.hpp
+// (determinant::LUPartialPiv): rho = kappa = 0 for a singular matrix.
+template <typename F>
+inline SafeProduct<F> SafeDeterminant(const Matrix<F>& A) {
+  Matrix<F> B(A);
+  return detail::safe_det(0, LOWER, B, false);
+}
+template <typename F>
+inline SafeProduct<F> SafeDeterminant(Matrix<F>& A, bool canOverwrite = false) {
+  return detail::safe_det(0, LOWER, A, canOverwrite);
+}
+
+// SafeHPDDeterminant(uplo, A[, canOverwrite]), Determinant.hpp
+// (hpd_determinant::Cholesky): rho = kappa = 0 if A is not numerically HPD.
+template <typename F>
+inline SafeProduct<F> SafeHPDDeterminant(UpperOrLower uplo, const Matrix<F>& A) {
+  Matrix<F> B(A);
+  return detail::safe_det(1, uplo, B, false);
+}
+template <typename F>
+inline SafeProduct<F> SafeHPDDeterminant(UpperOrLower uplo, Matrix<F>& A, bool canOverwrite = false) {
+  return detail::safe_det(1, uplo, A, canOverwrite);
+}
+
+// Determinant(A) = rho exp(kappa n); HPDDeterminant(uplo, A) = exp(kappa n)
+// (Determinant.hpp).
+template <typename F>
+inline F Determinant(const Matrix<F>& A) {
+  SafeProduct<F> s = SafeDeterminant(A);
+  return s.rho * std::exp(s.kappa * s.n);
+}
+template <typename F>
+inline F HPDDeterminant(UpperOrLower uplo, const Matrix<F>& A) {
+  SafeProduct<F> s = SafeHPDDeterminant(uplo, A);
+  return std::exp(s.kappa * s.n);
+}
+
 // ------------------------------------------- 1 x 1 DistMatrix overloads --
 // Cholesky.hpp:79-101, LU.hpp:220-321, HPDSolve.hpp:30-41,
 // Cholesky/SolveAfter.hpp:77-134, LU/SolveAfter.hpp:148-195,
@@ -572,5 +678,31 @@ inline void Herk(UpperOrLower uplo, Orientation orientation, T alpha, const Dist
                  DistMatrix<T>& C) {
   Herk(uplo, orientation, alpha, A.LockedMatrix(), beta, C.Matrix());
 }
+template <typename F>
+inline void TriangularInverse(UpperOrLower uplo, UnitOrNonUnit diag, DistMatrix<F>& A) {
+  TriangularInverse(uplo, diag, A.Matrix());
+}
+template <typename F>
+inline void Inverse(DistMatrix<F>& A) { Inverse(A.Matrix()); }
+template <typename F>
+inline void HPDInverse(UpperOrLower uplo, DistMatrix<F>& A) { HPDInverse(uplo, A.Matrix()); }
+template <typename F>
+inline SafeProduct<F> SafeDeterminant(const DistMatrix<F>& A) { return SafeDeterminant(A.LockedMatrix()); }
+template <typename F>
+inline SafeProduct<F> SafeDeterminant(DistMatrix<F>& A, bool canOverwrite = false) {
+  return SafeDeterminant(A.Matrix(), canOverwrite);
+}
+template <typename F>
+inline SafeProduct<F> SafeHPDDeterminant(UpperOrLower uplo, const DistMatrix<F>& A) {
+  return SafeHPDDeterminant(uplo, A.LockedMatrix());
+}
+template <typename F>
+inline SafeProduct<F> SafeHPDDeterminant(UpperOrLower uplo, DistMatrix<F>& A, bool canOverwrite = false) {
+  return SafeHPDDeterminant(uplo, A.Matrix(), canOverwrite);
+}
+template <typename F>
+inline F Determinant(const DistMatrix<F>& A) { return Determinant(A.LockedMatrix()); }
+template <typename F>
+inline F HPDDeterminant(UpperOrLower uplo, const DistMatrix<F>& A) { return HPDDeterminant(uplo, A.LockedMatrix()); }
 
 }  // namespace elem

@@ -207,3 +207,108 @@ def syrk(uplo, trans, alpha, A, beta, C):
     getattr(lib(), f"oref_{_pfx(C)}syrk")(
         uplo.encode(), trans.encode(), n, k, alpha, _p(_f(A)), _ld(A), beta, _p(C), _ld(C))
     return C
+
+
+# ---- TriangularInverse / Inverse / HPDInverse / (Safe)Determinant ----------
+# Compositions of the routines above, in the reference's order of operations.
+
+
+def triangular_inverse(A, uplo=LOWER, unit=False):
+    """TriangularInverse(uplo, diag, A) (lapack-like/TriangularInverse.hpp:56-64):
+    the uplo triangle of a copy of A := its inverse (the diagonal too unless
+    unit); the other triangle is left as it was.  Computed as Trsm(LEFT, uplo,
+    NORMAL, diag, 1, T, I), which is the same inverse as the reference's
+    blocked LVar3/UVar3 up to rounding."""
+    A = _f(A).copy(order="F")
+    n = A.shape[0]
+    X = trsm("L", "L" if uplo == LOWER else "U", "N", "U" if unit else "N", 1.0, A, np.eye(n, order="F"))
+    tri = np.tril if uplo == LOWER else np.triu
+    mask = tri(np.ones((n, n), dtype=bool), -1 if (unit and uplo == LOWER) else (1 if unit else 0))
+    A[mask] = X[mask]
+    return A
+
+
+def inverse(A, nb=128):
+    """Inverse(A) (Inverse.hpp:17-23) by inverse::LUPartialPiv
+    (Inverse/LUPartialPiv.hpp:17-80): P A = L U; TriangularInverse(UPPER,
+    NON_UNIT) of U in place; then, over diagonal blocks from the bottom up,
+    A1 -= A2 L21 (Gemm) and A1 := A1 inv(L11) (Trsm RIGHT LOWER NORMAL UNIT)
+    with L11/L21 copied out and zeroed; finally inv(A) := inv(A) P
+    (ApplyInverseColumnPivots).  Returns (inverse, status)."""
+    F, p, st = lu(A, nb)
+    if st:
+        return F, st
+    n = F.shape[0]
+    F = triangular_inverse(F, UPPER, unit=False)
+    ends = list(range(n, 0, -nb))  # blocks aligned to the bottom-right corner
+    for e in ends:
+        k = max(0, e - nb)
+        L11 = F[k:e, k:e].copy(order="F")
+        L21 = F[e:, k:e].copy(order="F")
+        F[k:e, k:e] = np.triu(F[k:e, k:e])
+        F[e:, k:e] = 0.0
+        A1 = np.asfortranarray(F[:, k:e])
+        if e < n:
+            A1 = gemm("N", "N", -1.0, np.asfortranarray(F[:, e:]), L21, 1.0, A1)
+        A1 = trsm("R", "L", "N", "U", 1.0, L11, A1)
+        F[:, k:e] = A1
+    # inv(A) P: the column swaps i <-> p[i] undone in reverse order
+    for i in range(n - 1, -1, -1):
+        j = int(p[i])
+        if j != i:
+            F[:, [i, j]] = F[:, [j, i]]
+    return F, 0
+
+
+def hpd_inverse(A, uplo=LOWER, nb=128):
+    """HPDInverse(uplo, A) (Inverse.hpp:25-35): the uplo triangle of a copy of
+    A := that of inv(A), the other triangle as it was.  Computed from the
+    Cholesky factor and cholesky::SolveAfter on the identity (the same inverse
+    as hpd_inverse::CholeskyLVar2 / UVar2 up to rounding).  Returns (result,
+    status)."""
+    F, st = cholesky(A, uplo, nb)
+    if st:
+        return F, st
+    n = F.shape[0]
+    X = cholesky_solve_after(F, np.eye(n, order="F"), uplo)
+    out = _f(A).copy(order="F")
+    tri = np.tril if uplo == LOWER else np.triu
+    mask = tri(np.ones((n, n), dtype=bool))
+    out[mask] = X[mask]
+    return out, 0
+
+
+def safe_determinant(A, nb=128):
+    """SafeDeterminant(A) -> (rho, kappa, n), det = rho exp(kappa n)
+    (determinant::LUPartialPiv / AfterLUPartialPiv,
+    Determinant/LUPartialPiv.hpp:17-67, PivotParity.hpp:17-33); a singular
+    matrix gives rho = kappa = 0."""
+    F, p, st = lu(A, nb)
+    n = F.shape[0]
+    if st:
+        return 0.0, 0.0, n
+    rho, kappa = 1.0, 0.0
+    scale = float(n)
+    for i in range(n):
+        delta = F[i, i]
+        alpha = abs(delta)
+        rho *= delta / alpha
+        kappa += np.log(alpha) / scale
+    odd = sum(1 for i in range(n) if p[i] != i) % 2 == 1
+    return (-rho if odd else rho), float(kappa), n
+
+
+def safe_hpd_determinant(A, uplo=LOWER, nb=128):
+    """SafeHPDDeterminant(uplo, A) -> (rho, kappa, n) (hpd_determinant::
+    Cholesky / AfterCholesky, Determinant/Cholesky.hpp:17-55): rho = 1, kappa =
+    sum log l_ii / (n / 2); a matrix that is not numerically HPD gives rho =
+    kappa = 0."""
+    F, st = cholesky(A, uplo, nb)
+    n = F.shape[0]
+    if st:
+        return 0.0, 0.0, n
+    kappa = 0.0
+    scale = n / 2.0
+    for i in range(n):
+        kappa += np.log(F[i, i]) / scale
+    return 1.0, float(kappa), n

@@ -163,6 +163,72 @@ int main(int argc, char** argv) {
     try { LU(S, p); } catch (SingularMatrixException&) { caught = true; }
     Check(caught, "LU throws SingularMatrixException", 0);
   }
+  // Inverse / HPDInverse / TriangularInverse / (Safe)Determinant, checked by
+  // identities: A inv(A) = I, det(A) det(inv(A)) = 1, SafeHPDDeterminant and
+  // SafeDeterminant agree on an HPD matrix, a unit triangular inverse keeps
+  // the diagonal and the other triangle.
+  {
+    const int m = 300;
+    Matrix<double> A, Ai;
+    Uniform(A, m, m);
+    for (int i = 0; i < m; ++i) A.Update(i, i, 4.0);
+    Ai = A;
+    Inverse(Ai);
+    Matrix<double> I(m, m);
+    Gemm(NORMAL, NORMAL, 1.0, A, Ai, 0.0, I);
+    double e = 0;
+    for (int j = 0; j < m; ++j)
+      for (int i = 0; i < m; ++i) e = std::max(e, std::fabs(I.Get(i, j) - (i == j ? 1.0 : 0.0)));
+    Check(e < 1e-12, "Inverse: A inv(A) = I", e);
+    SafeProduct<double> d1 = SafeDeterminant(A), d2 = SafeDeterminant(Ai);
+    const double s = d1.kappa * d1.n + d2.kappa * d2.n;
+    Check(d1.rho * d2.rho == 1.0 && std::fabs(s) < 1e-9, "SafeDeterminant: det(A) det(inv(A)) = 1", s);
+
+    Matrix<double> G, S(m, m), Si;
+    Uniform(G, m, m);
+    Gemm(NORMAL, TRANSPOSE, 1.0, G, G, 0.0, S);
+    for (int i = 0; i < m; ++i) S.Update(i, i, (double)m);
+    SafeProduct<double> h = SafeHPDDeterminant(LOWER, S), g = SafeDeterminant(S);
+    Check(h.rho == 1.0 && g.rho == 1.0 && std::fabs(h.kappa - g.kappa) < 1e-12 * std::fabs(g.kappa),
+          "SafeHPDDeterminant = SafeDeterminant on HPD", std::fabs(h.kappa - g.kappa));
+    Si = S;
+    HPDInverse(UPPER, Si);
+    double eh = 0;  // (S inv(S))_ij from the upper triangle of inv(S) mirrored
+    Matrix<double> Sym(m, m);
+    for (int j = 0; j < m; ++j)
+      for (int i = 0; i < m; ++i) Sym.Set(i, j, i <= j ? Si.Get(i, j) : Si.Get(j, i));
+    Gemm(NORMAL, NORMAL, 1.0, S, Sym, 0.0, I);
+    for (int j = 0; j < m; ++j)
+      for (int i = 0; i < m; ++i) eh = std::max(eh, std::fabs(I.Get(i, j) - (i == j ? 1.0 : 0.0)));
+    bool lower_kept = true;
+    for (int j = 0; j < m; ++j)
+      for (int i = j + 1; i < m; ++i) lower_kept = lower_kept && Si.Get(i, j) == S.Get(i, j);
+    Check(eh < 1e-12 && lower_kept, "HPDInverse(UPPER): S inv(S) = I, lower kept", eh);
+
+    Matrix<double> T = A, Ti;  // strictly lower part scaled by 1/m: well conditioned
+    for (int j = 0; j < m; ++j)
+      for (int i = j + 1; i < m; ++i) T.Set(i, j, A.Get(i, j) / m);
+    Ti = T;
+    TriangularInverse(LOWER, UNIT, Ti);
+    bool kept = true;
+    for (int j = 0; j < m; ++j)
+      for (int i = 0; i <= j; ++i) kept = kept && Ti.Get(i, j) == T.Get(i, j);
+    double et = 0;  // (unit L) inv(unit L) = I
+    for (int j = 0; j < m; ++j)
+      for (int i = j; i < m; ++i) {
+        double acc = 0;
+        for (int k = j; k <= i; ++k)
+          acc += (k == i ? 1.0 : T.Get(i, k)) * (k == j ? 1.0 : Ti.Get(k, j));
+        et = std::max(et, std::fabs(acc - (i == j ? 1.0 : 0.0)));
+      }
+    Check(kept && et < 1e-10, "TriangularInverse(LOWER, UNIT)", et);
+
+    Matrix<double> Z;
+    Uniform(Z, 20, 20);
+    for (int i = 0; i < 20; ++i) Z.Set(i, 5, 0.0);
+    SafeProduct<double> z = SafeDeterminant(Z);
+    Check(z.rho == 0.0 && z.kappa == 0.0, "SafeDeterminant of a singular matrix is 0", 0);
+  }
   Finalize();
   std::printf("%s\n", failures ? "FAILED" : "PASSED");
   return failures ? 1 : 0;

@@ -206,3 +206,63 @@ def test_float_variant():
     assert st == 0
     ref = sla.cholesky(A.astype(np.float64), lower=True)
     assert np.max(np.abs(np.tril(F) - ref)) < 1e-4 * np.max(np.abs(ref))
+
+
+# ---- TriangularInverse / Inverse / HPDInverse / (Safe)Determinant ----------
+
+@pytest.mark.parametrize("n", [1, 7, 130])
+def test_inverse_and_determinant_vs_numpy(n):
+    rs = np.random.default_rng(40 + n)
+    A = np.asfortranarray(rs.uniform(-1, 1, (n, n)))
+    X, st = orc.inverse(A, nb=32)
+    assert st == 0
+    assert np.abs(X @ A - np.eye(n)).max() <= 1e-10
+    rho, kappa, nn = orc.safe_determinant(A, nb=32)
+    sign, logabs = np.linalg.slogdet(A)
+    assert nn == n and rho == sign
+    assert abs(kappa * n - logabs) <= 1e-11 * max(1.0, abs(logabs))
+
+
+def test_inverse_and_determinant_singular():
+    A = np.asfortranarray(np.random.default_rng(3).uniform(-1, 1, (9, 9)))
+    A[:, 4] = 0.0
+    _, st = orc.inverse(A)
+    assert st == 5
+    assert orc.safe_determinant(A) == (0.0, 0.0, 9)
+
+
+@pytest.mark.parametrize("uplo", [orc.LOWER, orc.UPPER])
+def test_hpd_inverse_and_determinant_vs_numpy(uplo):
+    rs = np.random.default_rng(8)
+    n = 90
+    G = rs.standard_normal((n, n))
+    S = np.asfortranarray(G @ G.T + n * np.eye(n))
+    H, st = orc.hpd_inverse(S, uplo, nb=32)
+    assert st == 0
+    tri = np.tril if uplo == orc.LOWER else np.triu
+    other = (lambda M: np.triu(M, 1)) if uplo == orc.LOWER else (lambda M: np.tril(M, -1))
+    Si = np.linalg.inv(S)
+    assert np.abs(tri(H) - tri(Si)).max() <= 1e-12 * np.abs(Si).max()
+    assert np.array_equal(other(H), other(S))
+    rho, kappa, _ = orc.safe_hpd_determinant(S, uplo, nb=32)
+    assert rho == 1.0 and abs(kappa * n - np.linalg.slogdet(S)[1]) <= 1e-11 * n
+    S[3, 3] = -1.0
+    assert orc.safe_hpd_determinant(S, uplo) == (0.0, 0.0, n)
+
+
+@pytest.mark.parametrize("uplo", [orc.LOWER, orc.UPPER])
+@pytest.mark.parametrize("unit", [False, True])
+def test_triangular_inverse_vs_numpy(uplo, unit):
+    rs = np.random.default_rng(5)
+    n = 60
+    T = np.asfortranarray(rs.standard_normal((n, n)) * 0.1 + np.diag(rs.uniform(1, 2, n)))
+    X = orc.triangular_inverse(T, uplo, unit)
+    tri = np.tril if uplo == orc.LOWER else np.triu
+    k = -1 if uplo == orc.LOWER else 1
+    Tt = (tri(T, k) + np.eye(n)) if unit else tri(T)
+    Xt = (tri(X, k) + np.eye(n)) if unit else tri(X)
+    assert np.abs(Xt @ Tt - np.eye(n)).max() <= 1e-13
+    other = (lambda M: np.triu(M, 1)) if uplo == orc.LOWER else (lambda M: np.tril(M, -1))
+    assert np.array_equal(other(X), other(T))
+    if unit:
+        assert np.array_equal(np.diag(X), np.diag(T))
