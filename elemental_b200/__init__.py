@@ -144,6 +144,8 @@ def _declare(L):
         "egpu_host_dgemm": ([H, I, I, I, I, I, D, P, I, P, I, D, P, I], I),
         "egpu_host_dherk": ([H, I, I, I, I, D, P, I, D, P, I], I),
         "egpu_host_dlaswp": ([H, I, I, I, P, I, P, I], I),
+        "egpu_dpotrf_reverse": ([H, I, I, P, I, P], I),
+        "egpu_host_dpotrf_reverse": ([H, I, I, P, I, P], I),
         "egpu_dtrtri": ([H, I, I, I, P, I], I),
         "egpu_dgetri": ([H, I, P, I, P], I),
         "egpu_dpotri": ([H, I, I, P, I, P], I),
@@ -480,6 +482,20 @@ class Handle:
         self._bind_stream()
         info = ctypes.c_int(0)
         rc = lib().egpu_dgetrf(self._h, A.shape[0], A.shape[1], _ptr(A), _ld(A), _ptr(p), ctypes.byref(info))
+        _check(rc, info.value)
+
+    def reverse_cholesky(self, A, uplo=LOWER):
+        """ReverseCholesky(uplo, A): A = L^T L (LOWER) or U U^T (UPPER), in place."""
+        self._bind_stream()
+        info = ctypes.c_int(0)
+        rc = lib().egpu_dpotrf_reverse(self._h, uplo, A.shape[0], _ptr(A), _ld(A), ctypes.byref(info))
+        _check(rc, info.value)
+
+    def host_reverse_cholesky(self, A: np.ndarray, uplo=LOWER):
+        A = _np_f(A)
+        info = ctypes.c_int(0)
+        rc = lib().egpu_host_dpotrf_reverse(self._h, uplo, A.shape[0], _np_ptr(A), max(A.shape[0], 1),
+                                            ctypes.byref(info))
         _check(rc, info.value)
 
     # ---- TriangularInverse / Inverse / HPDInverse / (Safe)Determinant ----

@@ -580,6 +580,29 @@ int potri_core(egpu_context* h, int uplo, int n, double* A, long long lda, int* 
   return launch_copy_triangle(h->stream, uplo, false, n, X, ldx, A, lda);
 }
 
+// ReverseCholesky (lapack-like/Cholesky.hpp:64-76 -> cholesky::ReverseLVar3 /
+// ReverseUVar3, Cholesky/LVar3.hpp:125-165): LOWER: A = L^T L, L lower;
+// UPPER: A = U U^T, U upper, swept from the bottom-right corner.  With J the
+// reversal permutation, the reverse factor of A is J chol(J A J) J with the
+// other triangle: the uplo triangle is rotated by 180 degrees into staging
+// slot 3 (where it becomes the opposite triangle), factored forward, and the
+// factor rotated back.  Only the uplo triangle of A is read or written.
+// EGPU_NOT_HPD's info is the 1-based column of A where the reverse sweep
+// stopped.
+int reverse_potrf_core(egpu_context* h, int uplo, int n, double* A, long long lda, int* info) {
+  const long long ldx = ld_aligned(n);
+  TRY(ensure_stage(h, 3, sizeof(double) * (size_t)ldx * n));
+  double* X = static_cast<double*>(h->stage[3]);
+  const int other = uplo == EGPU_LOWER ? EGPU_UPPER : EGPU_LOWER;
+  TRY(launch_rotate_triangle(h->stream, uplo, n, A, lda, X, ldx));
+  TRY(potrf_core(h, other, n, X, ldx));
+  int col = 0;
+  const int rc = read_status(h, &col);
+  if (rc == EGPU_NOT_HPD && info) *info = n + 1 - col;
+  TRY(rc);
+  return launch_rotate_triangle(h->stream, other, n, X, ldx, A, lda);
+}
+
 // SafeDeterminant (Determinant.hpp, determinant::LUPartialPiv,
 // Determinant/LUPartialPiv.hpp:17-67) and SafeHPDDeterminant
 // (hpd_determinant::Cholesky, Determinant/Cholesky.hpp:17-55) on the work
@@ -1142,6 +1165,16 @@ int egpu_dpotri(egpu_handle h, int uplo, int n, double* dA, int lda, int* info) 
   return read_status(h, info);
 }
 
+int egpu_dpotrf_reverse(egpu_handle h, int uplo, int n, double* dA, int lda, int* info) {
+  TRY(check_handle(h));
+  if (info) *info = 0;
+  if (n < 0 || (uplo != EGPU_LOWER && uplo != EGPU_UPPER) || bad_ld(lda, n)) return EGPU_ERR_ARG;
+  if (n == 0) return EGPU_OK;
+  Enter g(h);
+  TRY(reset_status(h));
+  return reverse_potrf_core(h, uplo, n, dA, lda, info);
+}
+
 // The determinant's work matrix: A itself when overwrite (factored in place),
 // else a copy in staging slot 3.
 static int safe_det_device(egpu_handle h, int hpd, int uplo, int n, double* dA, int lda, int overwrite, double* rho,
@@ -1477,6 +1510,23 @@ int egpu_host_dpotri(egpu_handle h, int uplo, int n, double* A, int lda, int* in
   TRY(d2h(h, d, ld, A, lda, n, n));
   TRY(rc);
   return read_status(h, info);
+}
+
+int egpu_host_dpotrf_reverse(egpu_handle h, int uplo, int n, double* A, int lda, int* info) {
+  TRY(check_handle(h));
+  if (info) *info = 0;
+  if (n < 0 || (uplo != EGPU_LOWER && uplo != EGPU_UPPER) || bad_ld(lda, n)) return EGPU_ERR_ARG;
+  if (n == 0) return EGPU_OK;
+  Enter g(h);
+  SyncScope ss(h);
+  double* d; long long ld;
+  TRY(h2d(h, 0, A, lda, n, n, &d, &ld));
+  TRY(reset_status(h));
+  int rc = reverse_potrf_core(h, uplo, n, d, ld, info);
+  if (rc < 0) return rc;
+  TRY(d2h(h, d, ld, A, lda, n, n));
+  EGPU_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  return rc;
 }
 
 static int safe_det_host(egpu_handle h, int hpd, int uplo, int n, double* A, int lda, int overwrite, double* rho,

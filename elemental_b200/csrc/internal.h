@@ -140,6 +140,9 @@ int launch_set_identity(cudaStream_t st, int n, double* X, long long ldx);
 // D's uplo triangle (strict: below/above the diagonal only) := S's.
 int launch_copy_triangle(cudaStream_t st, int uplo, bool strict, int n, const double* S, long long lds, double* D,
                          long long ldd);
+// D[n-1-i, n-1-j] := S[i, j] over S's uplo triangle.
+int launch_rotate_triangle(cudaStream_t st, int uplo, int n, const double* S, long long lds, double* D,
+                           long long ldd);
 // out[0..2] = sum log|a_ii|, count of a_ii < 0, count of p[i] != i (p may be
 // null); one deterministic block reduction.
 int launch_diag_logsum(cudaStream_t st, int n, const double* A, long long lda, const int* p, double* out);

@@ -1,8 +1,9 @@
-// Small kernels behind TriangularInverse / Inverse / HPDInverse and the
-// (Safe)Determinant entry points: an identity fill (the right-hand side the
-// inverses are solved against), a triangle copy (the inverse written back
-// over the caller's triangle only) and one deterministic reduction over the
-// diagonal of a factor.
+// Small kernels behind TriangularInverse / Inverse / HPDInverse, the
+// (Safe)Determinant entry points and ReverseCholesky: an identity fill (the
+// right-hand side the inverses are solved against), a triangle copy (the
+// inverse written back over the caller's triangle only), a 180-degree
+// triangle rotation (the reverse factorization as a forward one) and one
+// deterministic reduction over the diagonal of a factor.
 #include "internal.h"
 
 namespace egpu {
@@ -65,6 +66,17 @@ __global__ void __launch_bounds__(kDiagReduceThreads) diag_logsum_kernel(int n, 
   }
 }
 
+// D[n-1-i, n-1-j] := S[i, j] for (i, j) in S's uplo triangle (a 180-degree
+// rotation, which maps S's uplo triangle onto D's other triangle).
+__global__ void rotate_triangle_kernel(int uplo, int n, const double* S, long long lds, double* D, long long ldd) {
+  const long long total = (long long)n * n;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+       e += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(e % n), j = (int)(e / n);
+    if (uplo == EGPU_LOWER ? i >= j : i <= j) D[(n - 1 - i) + (long long)(n - 1 - j) * ldd] = S[i + j * lds];
+  }
+}
+
 int grid_for(long long elems) {
   return (int)std::max<long long>(1, std::min<long long>((elems + 255) / 256, 148 * 16));
 }
@@ -91,6 +103,19 @@ int launch_copy_triangle(cudaStream_t st, int uplo, bool strict, int n, const do
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) {
     set_last_error(e, "copy_triangle launch", __FILE__, __LINE__);
+    return EGPU_ERR_CUDA;
+  }
+  return EGPU_OK;
+}
+
+int launch_rotate_triangle(cudaStream_t st, int uplo, int n, const double* S, long long lds, double* D,
+                           long long ldd) {
+  if (n <= 0) return EGPU_OK;
+  rotate_triangle_kernel<<<grid_for((long long)n * n), 256, 0, st>>>(uplo, n, S, lds, D, ldd);
+  count_launch();
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    set_last_error(e, "rotate_triangle launch", __FILE__, __LINE__);
     return EGPU_ERR_CUDA;
   }
   return EGPU_OK;

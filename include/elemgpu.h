@@ -307,6 +307,14 @@ EGPU_API int egpu_dgetri(egpu_handle h, int n, double* dA, int lda, int* info);
  * the other triangle is not touched.  EGPU_NOT_HPD as egpu_dpotrf. */
 EGPU_API int egpu_dpotri(egpu_handle h, int uplo, int n, double* dA, int lda, int* info);
 
+/* ReverseCholesky(uplo, A), lapack-like/Cholesky.hpp:64-76
+ * (cholesky::ReverseLVar3 / ReverseUVar3, Cholesky/LVar3.hpp:125-165): LOWER
+ * factors A = L^T L with L lower, UPPER A = U U^T with U upper, in the uplo
+ * triangle (the other triangle is not touched).  EGPU_NOT_HPD with info = the
+ * 1-based column where the reverse sweep met a non-positive pivot.  dA needs
+ * no alignment (the triangle is staged). */
+EGPU_API int egpu_dpotrf_reverse(egpu_handle h, int uplo, int n, double* dA, int lda, int* info);
+
 /* SafeDeterminant(A[, canOverwrite]), lapack-like/Determinant.hpp (
  * determinant::LUPartialPiv, Determinant/LUPartialPiv.hpp:17-67 with
  * PivotParity.hpp:17-33): det(A) = rho * exp(kappa * n), rho = +-1, kappa =
@@ -355,6 +363,7 @@ EGPU_API int egpu_host_dgemm(egpu_handle h, int orientA, int orientB, int m, int
 EGPU_API int egpu_host_dherk(egpu_handle h, int uplo, int orient, int n, int k, double alpha, const double* A, int lda,
                     double beta, double* C, int ldc);
 EGPU_API int egpu_host_dlaswp(egpu_handle h, int inverse, int m, int n, double* A, int lda, const int* p, int npiv);
+EGPU_API int egpu_host_dpotrf_reverse(egpu_handle h, int uplo, int n, double* A, int lda, int* info);
 EGPU_API int egpu_host_dtrtri(egpu_handle h, int uplo, int diag, int n, double* A, int lda);
 EGPU_API int egpu_host_dgetri(egpu_handle h, int n, double* A, int lda, int* info);
 EGPU_API int egpu_host_dpotri(egpu_handle h, int uplo, int n, double* A, int lda, int* info);

@@ -413,6 +413,20 @@ inline void Cholesky(UpperOrLower uplo, Matrix<F>& A) {
   detail::check(rc, info);
 }
 
+// ReverseCholesky(uplo, A), lapack-like/Cholesky.hpp:64-76: A = L^H L (LOWER)
+// or U U^H (UPPER), swept from the bottom-right corner.
+template <typename F>
+inline void ReverseCholesky(UpperOrLower uplo, Matrix<F>& A) {
+  static_assert(detail::IsSupported<F>::value, "elemgpu supports float and double");
+  if (A.Height() != A.Width()) throw std::logic_error("A must be square");
+  detail::AsDouble<F> a(A, true);
+  int info = 0;
+  int rc = egpu_host_dpotrf_reverse(detail::handle(), uplo == LOWER ? EGPU_LOWER : EGPU_UPPER, A.Height(), a.p, a.ld,
+                                    &info);
+  a.WriteBack(A);
+  detail::check(rc, info);
+}
+
 namespace cholesky {
 // cholesky::SolveAfter(uplo, orientation, A, B), lapack-like/Cholesky/SolveAfter.hpp:20-75.
 template <typename F>
@@ -682,6 +696,8 @@ template <typename F>
 inline void TriangularInverse(UpperOrLower uplo, UnitOrNonUnit diag, DistMatrix<F>& A) {
   TriangularInverse(uplo, diag, A.Matrix());
 }
+template <typename F>
+inline void ReverseCholesky(UpperOrLower uplo, DistMatrix<F>& A) { ReverseCholesky(uplo, A.Matrix()); }
 template <typename F>
 inline void Inverse(DistMatrix<F>& A) { Inverse(A.Matrix()); }
 template <typename F>

@@ -312,3 +312,28 @@ def safe_hpd_determinant(A, uplo=LOWER, nb=128):
     for i in range(n):
         kappa += np.log(F[i, i]) / scale
     return 1.0, float(kappa), n
+
+
+def reverse_cholesky(A, uplo=LOWER):
+    """ReverseCholesky(uplo, A) (lapack-like/Cholesky.hpp:64-76): LOWER follows
+    cholesky::ReverseLVar3Unb (Cholesky/LVar3.hpp:53-81) -- from the last
+    column back: alpha = sqrt(a_jj), row j left of the diagonal scaled by
+    1/alpha, then A00 -= a10^T a10 on its lower triangle -- giving A = L^T L;
+    UPPER is the transpose of the same sweep (A = U U^T).  Unblocked (the
+    blocked ReverseLVar3, :125-165, performs the same eliminations).  Returns
+    (copy with the factor in the uplo triangle, status): status is the
+    1-based column of a non-positive pivot, else 0."""
+    A = _f(A).copy(order="F")
+    n = A.shape[0]
+    W = A if uplo == LOWER else A.T  # the upper case on the transpose: a lower sweep
+    for j in range(n - 1, -1, -1):
+        alpha = W[j, j]
+        if not alpha > 0.0:
+            return A, j + 1
+        alpha = np.sqrt(alpha)
+        W[j, j] = alpha
+        W[j, :j] /= alpha
+        r = W[j, :j].copy()
+        # A00[i, k] -= r[i] r[k] for i >= k (lower triangle of A00)
+        W[:j, :j] -= np.tril(np.outer(r, r))
+    return A, 0

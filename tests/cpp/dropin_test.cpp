@@ -223,6 +223,17 @@ int main(int argc, char** argv) {
       }
     Check(kept && et < 1e-10, "TriangularInverse(LOWER, UNIT)", et);
 
+    Matrix<double> R = S;  // ReverseCholesky(LOWER): S = L^T L
+    ReverseCholesky(LOWER, R);
+    double er = 0;
+    for (int j = 0; j < m; ++j)
+      for (int i = j; i < m; ++i) {
+        double acc = 0;
+        for (int k = i; k < m; ++k) acc += R.Get(k, i) * R.Get(k, j);
+        er = std::max(er, std::fabs(acc - S.Get(i, j)));
+      }
+    Check(er < 1e-9 * m, "ReverseCholesky(LOWER): L^T L = S", er);
+
     Matrix<double> Z;
     Uniform(Z, 20, 20);
     for (int i = 0; i < 20; ++i) Z.Set(i, 5, 0.0);

@@ -175,3 +175,40 @@ def test_host_entry_points(handle):
     assert r == rr and abs(k - kr) <= 1e-12 * max(1.0, abs(kr))
     r, k, _ = handle.host_safe_hpd_determinant(S, eg.LOWER)
     assert r == 1.0 and abs(k - orc.safe_hpd_determinant(S)[1]) <= 1e-12 * max(1.0, abs(k))
+
+
+# ---------------------------------------------------------- ReverseCholesky --
+
+@pytest.mark.parametrize("n", [1, 5, 128, 129, 600])
+@pytest.mark.parametrize("uplo", [eg.LOWER, eg.UPPER])
+def test_reverse_cholesky(handle, n, uplo):
+    A = inputs.spd_ggt(n, 600 + n)
+    ref, st = orc.reverse_cholesky(A, uplo)
+    assert st == 0
+    dA = cuda(A)
+    handle.reverse_cholesky(dA, uplo)
+    F = host(dA)
+    tri = np.tril if uplo == eg.LOWER else np.triu
+    assert np.max(np.abs(tri(F) - tri(ref))) <= 1e-11 * np.max(np.abs(ref))
+    assert np.array_equal(other_triangle(F, uplo), other_triangle(A, uplo))
+    L = tri(F)
+    R = L.T @ L if uplo == eg.LOWER else L @ L.T
+    assert np.linalg.norm(A - R, 1) / (n * EPS * np.linalg.norm(A, 1)) <= 4.0
+
+
+@pytest.mark.parametrize("uplo", [eg.LOWER, eg.UPPER])
+def test_reverse_cholesky_not_hpd_column(handle, uplo):
+    A = inputs.spd_ggt(200, 5)
+    A[150, 150] = -1.0
+    _, st = orc.reverse_cholesky(A, uplo)
+    with pytest.raises(eg.NonHPDError) as e:
+        handle.reverse_cholesky(cuda(A), uplo)
+    assert e.value.column == st
+
+
+def test_reverse_cholesky_host(handle):
+    A = inputs.spd_ggt(300, 6)
+    F = A.copy(order="F")
+    handle.host_reverse_cholesky(F, eg.LOWER)
+    ref, _ = orc.reverse_cholesky(A, eg.LOWER)
+    assert np.max(np.abs(np.tril(F) - np.tril(ref))) <= 1e-11 * np.max(np.abs(ref))
