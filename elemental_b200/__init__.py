@@ -144,6 +144,8 @@ def _declare(L):
         "egpu_host_dgemm": ([H, I, I, I, I, I, D, P, I, P, I, D, P, I], I),
         "egpu_host_dherk": ([H, I, I, I, I, D, P, I, D, P, I], I),
         "egpu_host_dlaswp": ([H, I, I, I, P, I, P, I], I),
+        "egpu_dldl": ([H, I, I, P, I, P, P], I),
+        "egpu_host_dldl": ([H, I, I, P, I, P, P], I),
         "egpu_dpotrf_reverse": ([H, I, I, P, I, P], I),
         "egpu_host_dpotrf_reverse": ([H, I, I, P, I, P], I),
         "egpu_dtrtri": ([H, I, I, I, P, I], I),
@@ -483,6 +485,25 @@ class Handle:
         info = ctypes.c_int(0)
         rc = lib().egpu_dgetrf(self._h, A.shape[0], A.shape[1], _ptr(A), _ld(A), _ptr(p), ctypes.byref(info))
         _check(rc, info.value)
+
+    def ldl(self, A, d=None, orient=TRANSPOSE):
+        """LDLT / LDLH(A[, d]): A = L D L^T without pivoting on the lower
+        triangle (L strictly below the diagonal, D on it; d, a CUDA tensor of
+        n doubles, also receives D)."""
+        self._bind_stream()
+        info = ctypes.c_int(0)
+        rc = lib().egpu_dldl(self._h, orient, A.shape[0], _ptr(A), _ld(A), None if d is None else _ptr(d),
+                             ctypes.byref(info))
+        _check(rc, info.value)
+
+    def host_ldl(self, A: np.ndarray, orient=TRANSPOSE) -> np.ndarray:
+        A = _np_f(A)
+        d = np.zeros(A.shape[0])
+        info = ctypes.c_int(0)
+        rc = lib().egpu_host_dldl(self._h, orient, A.shape[0], _np_ptr(A), max(A.shape[0], 1), _np_ptr(d),
+                                  ctypes.byref(info))
+        _check(rc, info.value)
+        return d
 
     def reverse_cholesky(self, A, uplo=LOWER):
         """ReverseCholesky(uplo, A): A = L^T L (LOWER) or U U^T (UPPER), in place."""

@@ -603,6 +603,41 @@ int reverse_potrf_core(egpu_context* h, int uplo, int n, double* A, long long ld
   return launch_rotate_triangle(h->stream, other, n, X, ldx, A, lda);
 }
 
+// LDLT / LDLH (lapack-like/LDL.hpp -> ldl::Var3, LDL/Var3.hpp): blocked
+// LDL^T without pivoting on the lower triangle (the upper one is not read or
+// written).  Per block column: the symmetric diagonal block, staged from the
+// lower triangle, is factored by the unpivoted LU kernel (a symmetric block
+// has U11 = D11 L11^T), L11 and D11 are written back (d receives D when
+// given); S21 = A21 inv(L11)^T (= L21 D11) before A21 := L21 = A21 inv(U11)
+// (Trsm as a multiply, in place), then A22 -= S21 L21^T on the lower
+// triangle.  An exact zero pivot stops with EGPU_SINGULAR
+// (SingularMatrixException, LDL/Var3.hpp:44-45).
+int ldl_core(egpu_context* h, int n, double* A, long long lda, double* d) {
+  const int nb = h->nb;
+  cudaStream_t st = h->stream;
+  const long long lds = ld_aligned(n);
+  TRY(ensure_ws(h, 3 * align_up(sizeof(double) * (size_t)nb * nb, 256) + sizeof(double) * (size_t)lds * nb + 4096));
+  Carve cv(h->ws);
+  double* W = cv.take<double>((size_t)nb * nb);    // inv(L11), unit lower
+  double* W2 = cv.take<double>((size_t)nb * nb);   // inv(U11)
+  double* Blk = cv.take<double>((size_t)nb * nb);  // the symmetric diagonal block, ld nb
+  double* S21 = cv.take<double>((size_t)lds * nb);
+  for (int k = 0; k < n; k += nb) {
+    const int b = std::min(nb, n - k), m2 = n - k - b;
+    double* A11 = A + k + (size_t)k * lda;
+    TRY(launch_sym_from_lower(st, b, A11, lda, Blk, nb));
+    TRY(launch_getrf_diag_nopiv(st, Blk, nb, b, W, nb, W2, h->dstatus, k));
+    TRY(launch_ldl_block_writeback(st, b, Blk, nb, A11, lda, d ? d + k : nullptr));
+    if (m2 == 0) continue;
+    double* A21 = A + (k + b) + (size_t)k * lda;
+    double* A22 = A + (k + b) + (size_t)(k + b) * lda;
+    TRY(launch_dgemm(st, false, false, m2, b, b, 1.0, A21, lda, W, nb, 0.0, S21, lds, 0, false, h->dstatus));
+    TRY(launch_dgemm(st, false, true, m2, b, b, 1.0, A21, lda, W2, nb, 0.0, A21, lda, 0, true, h->dstatus));
+    TRY(launch_dgemm(st, false, false, m2, m2, b, -1.0, S21, lds, A21, lda, 1.0, A22, lda, 1, false, h->dstatus));
+  }
+  return EGPU_OK;
+}
+
 // SafeDeterminant (Determinant.hpp, determinant::LUPartialPiv,
 // Determinant/LUPartialPiv.hpp:17-67) and SafeHPDDeterminant
 // (hpd_determinant::Cholesky, Determinant/Cholesky.hpp:17-55) on the work
@@ -1175,6 +1210,20 @@ int egpu_dpotrf_reverse(egpu_handle h, int uplo, int n, double* dA, int lda, int
   return reverse_potrf_core(h, uplo, n, dA, lda, info);
 }
 
+int egpu_dldl(egpu_handle h, int orient, int n, double* dA, int lda, double* dd, int* info) {
+  TRY(check_handle(h));
+  if (info) *info = 0;
+  if (n < 0 || orient == EGPU_NORMAL || bad_ld(lda, n)) return EGPU_ERR_ARG;
+  if (n == 0) return EGPU_OK;
+  Enter g(h);
+  Operand A = make_op(dA, lda, n, n);
+  TRY(pack(h, 0, A, true));
+  TRY(reset_status(h));
+  TRY(ldl_core(h, n, A.ptr, A.ld, dd));
+  TRY(unpack(h, A));
+  return read_status(h, info);
+}
+
 // The determinant's work matrix: A itself when overwrite (factored in place),
 // else a copy in staging slot 3.
 static int safe_det_device(egpu_handle h, int hpd, int uplo, int n, double* dA, int lda, int overwrite, double* rho,
@@ -1509,6 +1558,25 @@ int egpu_host_dpotri(egpu_handle h, int uplo, int n, double* A, int lda, int* in
   if (rc < 0) return rc;
   TRY(d2h(h, d, ld, A, lda, n, n));
   TRY(rc);
+  return read_status(h, info);
+}
+
+int egpu_host_dldl(egpu_handle h, int orient, int n, double* A, int lda, double* d, int* info) {
+  TRY(check_handle(h));
+  if (info) *info = 0;
+  if (n < 0 || orient == EGPU_NORMAL || bad_ld(lda, n)) return EGPU_ERR_ARG;
+  if (n == 0) return EGPU_OK;
+  Enter g(h);
+  SyncScope ss(h);
+  double* dA; long long ld;
+  TRY(h2d(h, 0, A, lda, n, n, &dA, &ld));
+  TRY(ensure_stage(h, 2, sizeof(double) * (size_t)n));
+  double* dd = static_cast<double*>(h->stage[2]);
+  TRY(reset_status(h));
+  int rc = ldl_core(h, n, dA, ld, dd);
+  if (rc < 0) return rc;
+  TRY(d2h(h, dA, ld, A, lda, n, n));
+  if (d) EGPU_CUDA_TRY(cudaMemcpyAsync(d, dd, sizeof(double) * n, cudaMemcpyDeviceToHost, h->stream));
   return read_status(h, info);
 }
 

@@ -143,6 +143,11 @@ int launch_copy_triangle(cudaStream_t st, int uplo, bool strict, int n, const do
 // D[n-1-i, n-1-j] := S[i, j] over S's uplo triangle.
 int launch_rotate_triangle(cudaStream_t st, int uplo, int n, const double* S, long long lds, double* D,
                            long long ldd);
+// LDL diagonal blocks: the symmetric b x b block from A11's lower triangle;
+// and back: A11's strict lower := L, diagonal (and d) := D from an L\U block.
+int launch_sym_from_lower(cudaStream_t st, int b, const double* A, long long lda, double* Blk, long long ldb);
+int launch_ldl_block_writeback(cudaStream_t st, int b, const double* Blk, long long ldb, double* A, long long lda,
+                               double* d);
 // out[0..2] = sum log|a_ii|, count of a_ii < 0, count of p[i] != i (p may be
 // null); one deterministic block reduction.
 int launch_diag_logsum(cudaStream_t st, int n, const double* A, long long lda, const int* p, double* out);

@@ -1,8 +1,9 @@
 // Small kernels behind TriangularInverse / Inverse / HPDInverse, the
-// (Safe)Determinant entry points and ReverseCholesky: an identity fill (the
+// (Safe)Determinant entry points, ReverseCholesky and LDL: an identity fill (the
 // right-hand side the inverses are solved against), a triangle copy (the
 // inverse written back over the caller's triangle only), a 180-degree
-// triangle rotation (the reverse factorization as a forward one) and one
+// triangle rotation (the reverse factorization as a forward one), the
+// symmetric staging and write-back of LDL's diagonal blocks and one
 // deterministic reduction over the diagonal of a factor.
 #include "internal.h"
 
@@ -77,6 +78,28 @@ __global__ void rotate_triangle_kernel(int uplo, int n, const double* S, long lo
   }
 }
 
+// The b x b symmetric block whose lower triangle is A11's: Blk[i][j] =
+// A11[max(i,j)][min(i,j)] (A11's upper triangle is not read).
+__global__ void sym_from_lower_kernel(int b, const double* A, long long lda, double* Blk, long long ldb) {
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < b * b; e += gridDim.x * blockDim.x) {
+    const int i = e % b, j = e / b;
+    Blk[i + (long long)j * ldb] = i >= j ? A[i + (long long)j * lda] : A[j + (long long)i * lda];
+  }
+}
+
+// From the unpivoted LU L\U of a symmetric block: A11's strict lower
+// triangle := L's, its diagonal (and d, when given) := U's diagonal (D).
+__global__ void ldl_block_writeback_kernel(int b, const double* Blk, long long ldb, double* A, long long lda,
+                                           double* d) {
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < b * b; e += gridDim.x * blockDim.x) {
+    const int i = e % b, j = e / b;
+    if (i < j) continue;
+    const double v = Blk[i + (long long)j * ldb];
+    A[i + (long long)j * lda] = v;
+    if (i == j && d != nullptr) d[i] = v;
+  }
+}
+
 int grid_for(long long elems) {
   return (int)std::max<long long>(1, std::min<long long>((elems + 255) / 256, 148 * 16));
 }
@@ -116,6 +139,31 @@ int launch_rotate_triangle(cudaStream_t st, int uplo, int n, const double* S, lo
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) {
     set_last_error(e, "rotate_triangle launch", __FILE__, __LINE__);
+    return EGPU_ERR_CUDA;
+  }
+  return EGPU_OK;
+}
+
+int launch_sym_from_lower(cudaStream_t st, int b, const double* A, long long lda, double* Blk, long long ldb) {
+  if (b <= 0) return EGPU_OK;
+  sym_from_lower_kernel<<<grid_for((long long)b * b), 256, 0, st>>>(b, A, lda, Blk, ldb);
+  count_launch();
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    set_last_error(e, "sym_from_lower launch", __FILE__, __LINE__);
+    return EGPU_ERR_CUDA;
+  }
+  return EGPU_OK;
+}
+
+int launch_ldl_block_writeback(cudaStream_t st, int b, const double* Blk, long long ldb, double* A, long long lda,
+                               double* d) {
+  if (b <= 0) return EGPU_OK;
+  ldl_block_writeback_kernel<<<grid_for((long long)b * b), 256, 0, st>>>(b, Blk, ldb, A, lda, d);
+  count_launch();
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    set_last_error(e, "ldl_block_writeback launch", __FILE__, __LINE__);
     return EGPU_ERR_CUDA;
   }
   return EGPU_OK;

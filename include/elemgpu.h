@@ -307,6 +307,15 @@ EGPU_API int egpu_dgetri(egpu_handle h, int n, double* dA, int lda, int* info);
  * the other triangle is not touched.  EGPU_NOT_HPD as egpu_dpotrf. */
 EGPU_API int egpu_dpotri(egpu_handle h, int uplo, int n, double* dA, int lda, int* info);
 
+/* LDLT(A[, d]) / LDLH(A[, d]), lapack-like/LDL.hpp (ldl::Var3,
+ * LDL/Var3.hpp): A = L D L^T without pivoting, orient EGPU_TRANSPOSE or
+ * EGPU_ADJOINT (the same for real F; EGPU_NORMAL is EGPU_ERR_ARG, "Can only
+ * perform LDL^T or LDL^H").  Only the lower triangle is read and written:
+ * strictly below the diagonal L (unit diagonal implied), on the diagonal D;
+ * dd (device, n doubles, or NULL) also receives D.  EGPU_SINGULAR with info =
+ * the 1-based column of an exact zero pivot. */
+EGPU_API int egpu_dldl(egpu_handle h, int orient, int n, double* dA, int lda, double* dd, int* info);
+
 /* ReverseCholesky(uplo, A), lapack-like/Cholesky.hpp:64-76
  * (cholesky::ReverseLVar3 / ReverseUVar3, Cholesky/LVar3.hpp:125-165): LOWER
  * factors A = L^T L with L lower, UPPER A = U U^T with U upper, in the uplo
@@ -363,6 +372,7 @@ EGPU_API int egpu_host_dgemm(egpu_handle h, int orientA, int orientB, int m, int
 EGPU_API int egpu_host_dherk(egpu_handle h, int uplo, int orient, int n, int k, double alpha, const double* A, int lda,
                     double beta, double* C, int ldc);
 EGPU_API int egpu_host_dlaswp(egpu_handle h, int inverse, int m, int n, double* A, int lda, const int* p, int npiv);
+EGPU_API int egpu_host_dldl(egpu_handle h, int orient, int n, double* A, int lda, double* d, int* info);
 EGPU_API int egpu_host_dpotrf_reverse(egpu_handle h, int uplo, int n, double* A, int lda, int* info);
 EGPU_API int egpu_host_dtrtri(egpu_handle h, int uplo, int diag, int n, double* A, int lda);
 EGPU_API int egpu_host_dgetri(egpu_handle h, int n, double* A, int lda, int* info);

@@ -413,6 +413,38 @@ inline void Cholesky(UpperOrLower uplo, Matrix<F>& A) {
   detail::check(rc, info);
 }
 
+// LDLT(A[, d]) / LDLH(A[, d]), lapack-like/LDL.hpp (ldl::Var3): A = L D L^T
+// without pivoting on the lower triangle; d (resized to n x 1 unless a view)
+// receives D.  SingularMatrixException on an exact zero pivot.
+namespace detail {
+template <typename F>
+inline void ldl(Orientation orientation, Matrix<F>& A, Matrix<F>* d) {
+  static_assert(IsSupported<F>::value, "elemgpu supports float and double");
+  if (A.Height() != A.Width()) throw std::logic_error("A must be square");
+  if (orientation == NORMAL) throw std::logic_error("Can only perform LDL^T or LDL^H");
+  const int n = A.Height();
+  if (d && d->Viewing() && (d->Height() != n || d->Width() != 1))
+    throw std::logic_error("d must be a column vector the same height as A");
+  if (d && !d->Viewing()) d->ResizeTo(n, 1);
+  AsDouble<F> a(A, true);
+  std::vector<double> dv(std::max(n, 1));
+  int info = 0;
+  int rc = egpu_host_dldl(handle(), Ori(orientation), n, a.p, a.ld, dv.data(), &info);
+  a.WriteBack(A);
+  if (d)
+    for (int i = 0; i < n; ++i) d->Set(i, 0, (F)dv[i]);
+  check(rc, info);
+}
+}  // namespace detail
+template <typename F>
+inline void LDLT(Matrix<F>& A) { detail::ldl(TRANSPOSE, A, (Matrix<F>*)nullptr); }
+template <typename F>
+inline void LDLT(Matrix<F>& A, Matrix<F>& d) { detail::ldl(TRANSPOSE, A, &d); }
+template <typename F>
+inline void LDLH(Matrix<F>& A) { detail::ldl(ADJOINT, A, (Matrix<F>*)nullptr); }
+template <typename F>
+inline void LDLH(Matrix<F>& A, Matrix<F>& d) { detail::ldl(ADJOINT, A, &d); }
+
 // ReverseCholesky(uplo, A), lapack-like/Cholesky.hpp:64-76: A = L^H L (LOWER)
 // or U U^H (UPPER), swept from the bottom-right corner.
 template <typename F>
@@ -698,6 +730,10 @@ inline void TriangularInverse(UpperOrLower uplo, UnitOrNonUnit diag, DistMatrix<
 }
 template <typename F>
 inline void ReverseCholesky(UpperOrLower uplo, DistMatrix<F>& A) { ReverseCholesky(uplo, A.Matrix()); }
+template <typename F>
+inline void LDLT(DistMatrix<F>& A) { LDLT(A.Matrix()); }
+template <typename F>
+inline void LDLH(DistMatrix<F>& A) { LDLH(A.Matrix()); }
 template <typename F>
 inline void Inverse(DistMatrix<F>& A) { Inverse(A.Matrix()); }
 template <typename F>

@@ -337,3 +337,26 @@ def reverse_cholesky(A, uplo=LOWER):
         # A00[i, k] -= r[i] r[k] for i >= k (lower triangle of A00)
         W[:j, :j] -= np.tril(np.outer(r, r))
     return A, 0
+
+
+def ldl(A):
+    """LDLT / LDLH(A, d) without pivoting (lapack-like/LDL.hpp), following
+    ldl::Var3Unb (LDL/Var3.hpp:19-67) column by column -- d_j = alpha11 (an
+    exact zero is SingularMatrixException), A22 -= a21 (a21 / alpha11)^T on its
+    lower triangle, a21 /= alpha11 -- which the blocked Var3 reorders only.
+    Returns (copy with L strictly below the diagonal and D on it, d, status):
+    status is the 1-based column of a zero pivot, else 0.  The upper triangle
+    is left as it was."""
+    A = _f(A).copy(order="F")
+    n = A.shape[0]
+    d = np.zeros(n)
+    for j in range(n):
+        alpha = A[j, j]
+        if alpha == 0.0:
+            return A, d, j + 1
+        d[j] = alpha
+        a21 = A[j + 1:, j].copy()
+        beta = a21 / alpha
+        A[j + 1:, j + 1:] -= np.tril(np.outer(a21, beta))
+        A[j + 1:, j] = beta
+    return A, d, 0

@@ -234,6 +234,19 @@ int main(int argc, char** argv) {
       }
     Check(er < 1e-9 * m, "ReverseCholesky(LOWER): L^T L = S", er);
 
+    Matrix<double> Ld = S, dd;  // LDLT of the HPD S: D > 0 and L D L^T = S
+    LDLT(Ld, dd);
+    double el = 0;
+    bool dpos = dd.Height() == m;
+    for (int i = 0; i < m && dpos; ++i) dpos = dd.Get(i, 0) > 0 && dd.Get(i, 0) == Ld.Get(i, i);
+    for (int j = 0; j < m; j += 7)
+      for (int i = j; i < m; ++i) {
+        double acc = 0;
+        for (int k = 0; k <= j; ++k) acc += (k == i ? 1.0 : Ld.Get(i, k)) * dd.Get(k, 0) * (k == j ? 1.0 : Ld.Get(j, k));
+        el = std::max(el, std::fabs(acc - S.Get(i, j)));
+      }
+    Check(dpos && el < 1e-9 * m, "LDLT: L D L^T = S, d = diag", el);
+
     Matrix<double> Z;
     Uniform(Z, 20, 20);
     for (int i = 0; i < 20; ++i) Z.Set(i, 5, 0.0);

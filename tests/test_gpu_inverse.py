@@ -212,3 +212,57 @@ def test_reverse_cholesky_host(handle):
     handle.host_reverse_cholesky(F, eg.LOWER)
     ref, _ = orc.reverse_cholesky(A, eg.LOWER)
     assert np.max(np.abs(np.tril(F) - np.tril(ref))) <= 1e-11 * np.max(np.abs(ref))
+
+
+# ----------------------------------------------------------------- LDL^T --
+
+def ldl_input(n, seed, garbage_above=True):
+    """A = L0 D0 L0^T with L0 unit lower (off-diagonal scaled by 0.5/n) and D0
+    of mixed sign (|D0| in [1, 2]): symmetric indefinite with safe unpivoted
+    pivots.  The strict upper triangle is overwritten with 7.0, which the
+    factorization must neither read nor write."""
+    rs = np.random.default_rng(seed)
+    L0 = np.tril(rs.standard_normal((n, n)) * (0.5 / max(n, 1)), -1) + np.eye(n)
+    D0 = rs.uniform(1.0, 2.0, n) * rs.choice([-1.0, 1.0], n)
+    A = np.asfortranarray(L0 @ np.diag(D0) @ L0.T)
+    if garbage_above:
+        A[np.triu_indices(n, 1)] = 7.0
+    return A, L0, D0
+
+
+@pytest.mark.parametrize("n", [1, 7, 128, 129, 400, 1000])
+@pytest.mark.parametrize("orient", [eg.TRANSPOSE, eg.ADJOINT])
+def test_ldl(handle, n, orient):
+    import torch
+    A, L0, D0 = ldl_input(n, 700 + n)
+    ref, dref, st = orc.ldl(A)
+    assert st == 0
+    dA = cuda(A)
+    dd = torch.zeros(n, dtype=torch.float64, device="cuda")
+    handle.ldl(dA, dd, orient)
+    F = host(dA)
+    assert np.max(np.abs(np.tril(F) - np.tril(ref))) <= 1e-12 * np.max(np.abs(np.tril(ref)))
+    assert np.max(np.abs(dd.cpu().numpy() - dref)) <= 1e-12 * np.max(np.abs(dref))
+    assert np.array_equal(np.triu(F, 1), np.triu(A, 1))
+    assert np.max(np.abs(np.tril(F, -1) + np.eye(n) - L0)) <= 1e-12
+
+
+def test_ldl_singular_column_and_normal_rejected(handle):
+    A, _, _ = ldl_input(300, 8)
+    A[200, :] = 0.0
+    A[:, 200] = 0.0
+    _, _, st = orc.ldl(A)
+    with pytest.raises(eg.SingularMatrixError) as e:
+        handle.ldl(cuda(A))
+    assert e.value.column == st == 201
+    with pytest.raises(eg.ElemGPUError):
+        handle.ldl(cuda(A), None, eg.NORMAL)
+
+
+def test_ldl_host(handle):
+    A, _, _ = ldl_input(260, 9)
+    F = A.copy(order="F")
+    d = handle.host_ldl(F)
+    ref, dref, _ = orc.ldl(A)
+    assert np.max(np.abs(np.tril(F) - np.tril(ref))) <= 1e-12 * np.max(np.abs(np.tril(ref)))
+    assert np.max(np.abs(d - dref)) <= 1e-12 * np.max(np.abs(dref))

@@ -266,3 +266,18 @@ def test_triangular_inverse_vs_numpy(uplo, unit):
     assert np.array_equal(other(X), other(T))
     if unit:
         assert np.array_equal(np.diag(X), np.diag(T))
+
+
+def test_ldl_and_reverse_cholesky_oracle():
+    rs = np.random.default_rng(12)
+    n = 40
+    L0 = np.tril(rs.standard_normal((n, n)) * (0.5 / n), -1) + np.eye(n)
+    D0 = rs.uniform(1, 2, n) * rs.choice([-1.0, 1.0], n)
+    A = np.asfortranarray(L0 @ np.diag(D0) @ L0.T)
+    F, d, st = orc.ldl(A)
+    assert st == 0 and np.abs(np.tril(F, -1) + np.eye(n) - L0).max() <= 1e-13 and np.abs(d - D0).max() <= 1e-13
+    G = rs.standard_normal((n, n))
+    S = np.asfortranarray(G @ G.T + n * np.eye(n))
+    R, st = orc.reverse_cholesky(S, orc.LOWER)
+    L = np.tril(R)
+    assert st == 0 and np.abs(L.T @ L - S).max() <= 1e-12 * np.abs(S).max()
