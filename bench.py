@@ -144,13 +144,16 @@ class ClockSampler:
 
 
 def dist_setup():
+    """One process per GPU (torchrun's RANK / LOCAL_RANK / WORLD_SIZE).  The
+    process group is NCCL; EGPU_BENCH_BACKEND=gloo selects gloo for the
+    host-side tests of this plumbing."""
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if ws > 1:
         import datetime
         import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        dist.init_process_group(os.environ.get("EGPU_BENCH_BACKEND", "nccl"), timeout=datetime.timedelta(seconds=300))
     return ws, rank, local
 
 
