@@ -46,3 +46,15 @@ def test_library_has_no_unresolved_own_symbols():
     out = subprocess.run(["nm", "-D", eg.LIB_PATH], capture_output=True, text=True).stdout
     undefined = [l.split()[-1] for l in out.splitlines() if " U " in l and "egpu" in l]
     assert not undefined, undefined
+
+
+def test_header_is_plain_c(tmp_path):
+    # bindings from C (cgo, JNI, ctypes users) include the header as C99
+    import os
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    src = tmp_path / "uses_header.c"
+    calls = "\n".join(f"  (void)&{n};" for n in eg.exported_symbols())
+    src.write_text('#include "elemgpu.h"\nint main(void) {\n' + calls + "\n  return 0;\n}\n")
+    subprocess.run(["gcc", "-std=c99", "-Wall", "-Wextra", "-pedantic", "-Werror", "-I",
+                    os.path.join(root, "include"), "-c", str(src), "-o", str(tmp_path / "uses_header.o")],
+                   check=True, capture_output=True)
