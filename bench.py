@@ -829,8 +829,10 @@ def kernel_case(args):
     (n x n, K = 128), 'gemm' = one Gemm trailing update, 'panel' = one LU panel
     (n x 128), 'diag' = one diagonal-block Cholesky (128 x 128), 'mixed' = one
     mixed-precision HPD solve, 'tc' = the tcgen05 trailing update alone,
-    'chol' = one plain FP64 Cholesky (warm-up call first).  --k sets the inner
-    dimension of 'update' and 'gemm' (default 128)."""
+    'chol' = one plain FP64 Cholesky (warm-up call first); 'inverse',
+    'hpdinverse', 'trtri', 'ldl', 'revchol', 'det' time those entry points
+    (best of three, flops: 2n^3, n^3, n^3/3, n^3/3, n^3/3, 2n^3/3).  --k sets
+    the inner dimension of 'update' and 'gemm' (default 128)."""
     import torch
     import elemental_b200 as eg
     from elemental_b200 import inputs
@@ -929,6 +931,37 @@ def kernel_case(args):
         print(json.dumps({"case": "tc", "n": n, "ms_per_launch": ms, "c_gbs": cbytes / ms / 1e6,
                           "tf32_tflops": 3 * 2.0 * n * (n + 1) / 2 * NB / ms / 1e9}))
         return
+    elif args.case in ("inverse", "hpdinverse", "trtri", "ldl", "revchol", "det"):
+        # the next rows (inverses, determinants, LDL, ReverseCholesky) at order
+        # n: one warm-up call, then three timed calls on fresh copies of A
+        if args.case in ("inverse", "det"):
+            A0 = eg.colmajor_cuda(inputs.uniform(n, n, SEED))
+        elif args.case == "trtri":
+            rs = np.random.default_rng(SEED)
+            A0 = eg.colmajor_cuda(rs.standard_normal((n, n)) * (0.5 / n) + np.diag(rs.uniform(1.0, 2.0, n)))
+        else:
+            A0 = inputs.spd_spectrum_torch(n, 1e3, SEED, "cuda")
+        flops = {"inverse": 2.0 * n ** 3, "hpdinverse": 1.0 * n ** 3, "trtri": n ** 3 / 3.0, "ldl": n ** 3 / 3.0,
+                 "revchol": n ** 3 / 3.0, "det": 2.0 * n ** 3 / 3.0}[args.case]
+        call = {"inverse": lambda A: h.inverse(A), "hpdinverse": lambda A: h.hpd_inverse(A),
+                "trtri": lambda A: h.triangular_inverse(A), "ldl": lambda A: h.ldl(A),
+                "revchol": lambda A: h.reverse_cholesky(A), "det": lambda A: h.safe_determinant(A, overwrite=True)}
+        A = A0.clone()
+        call[args.case](A)
+        times = []
+        for _ in range(3):
+            A.copy_(A0)
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            call[args.case](A)
+            e1.record()
+            torch.cuda.synchronize()
+            times.append(e0.elapsed_time(e1))
+        ms = min(times)
+        print(json.dumps({"case": args.case, "n": n, "ms": ms, "algorithmic_gflop": flops / 1e9,
+                          "tflops": flops / ms / 1e9, "frac_of_dmma_peak": flops / ms / 1e9 / FP64_PEAK_TFLOPS}))
+        return
     torch.cuda.synchronize()
     print(json.dumps({"case": args.case, "n": n, "ok": True}))
 
@@ -941,7 +974,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="mixed", choices=sorted(WORKLOADS), help="benchmark configuration")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline leg")
-    ap.add_argument("--case", choices=["update", "gemm", "panel", "diag", "peaks", "mixed", "tc", "chol"],
+    ap.add_argument("--case", choices=["update", "gemm", "panel", "diag", "peaks", "mixed", "tc", "chol", "inverse",
+                                       "hpdinverse", "trtri", "ldl", "revchol", "det"],
                     default=None,
                     help="run one launch of one kernel class (profiling)")
     ap.add_argument("--n", type=int, default=6144, help="size for --case")
