@@ -217,6 +217,22 @@ def _ptr(t):
     return ctypes.c_void_p(t.data_ptr())
 
 
+def _device_vec(t, count: int, dtype: str):
+    """Pointer to a device-vector argument: a contiguous CUDA tensor of
+    ``dtype`` ("int32" or "float64") with at least ``count`` elements, the
+    number the library reads or writes.  Checked here because a short or
+    mistyped buffer would otherwise be written out of bounds on the device."""
+    import torch
+    want = {"int32": torch.int32, "float64": torch.float64}[dtype]
+    if not isinstance(t, torch.Tensor) or t.device.type != "cuda":
+        raise TypeError(f"expected a CUDA tensor of {dtype}")
+    if t.dtype != want:
+        raise TypeError(f"expected a {dtype} tensor, got {t.dtype}")
+    if not t.is_contiguous() or t.numel() < count:
+        raise ValueError(f"expected a contiguous vector of at least {count} elements, got shape {tuple(t.shape)}")
+    return ctypes.c_void_p(t.data_ptr())
+
+
 def _np_f(a: np.ndarray):
     a = np.asarray(a)
     if a.dtype != np.float64:
@@ -483,7 +499,8 @@ class Handle:
     def lu(self, A, p):
         self._bind_stream()
         info = ctypes.c_int(0)
-        rc = lib().egpu_dgetrf(self._h, A.shape[0], A.shape[1], _ptr(A), _ld(A), _ptr(p), ctypes.byref(info))
+        pp = _device_vec(p, min(A.shape[0], A.shape[1]), "int32")
+        rc = lib().egpu_dgetrf(self._h, A.shape[0], A.shape[1], _ptr(A), _ld(A), pp, ctypes.byref(info))
         _check(rc, info.value)
 
     def ldl(self, A, d=None, orient=TRANSPOSE):
@@ -492,8 +509,8 @@ class Handle:
         n doubles, also receives D)."""
         self._bind_stream()
         info = ctypes.c_int(0)
-        rc = lib().egpu_dldl(self._h, orient, A.shape[0], _ptr(A), _ld(A), None if d is None else _ptr(d),
-                             ctypes.byref(info))
+        dd = None if d is None else _device_vec(d, A.shape[0], "float64")
+        rc = lib().egpu_dldl(self._h, orient, A.shape[0], _ptr(A), _ld(A), dd, ctypes.byref(info))
         _check(rc, info.value)
 
     def host_ldl(self, A: np.ndarray, orient=TRANSPOSE) -> np.ndarray:
@@ -604,8 +621,9 @@ class Handle:
 
     def lu_solve_after(self, A, p, B, orient=NORMAL):
         self._bind_stream()
+        pp = None if p is None else _device_vec(p, A.shape[0], "int32")
         _check(lib().egpu_dgetrs(self._h, orient, A.shape[0], B.shape[1] if B.dim() > 1 else 1, _ptr(A), _ld(A),
-                                 None if p is None else _ptr(p), _ptr(B), _ld(B)))
+                                 pp, _ptr(B), _ld(B)))
 
     def gaussian_elimination(self, A, B):
         self._bind_stream()
@@ -641,7 +659,8 @@ class Handle:
     def apply_row_pivots(self, B, p, inverse=False):
         self._bind_stream()
         m, n = B.shape[0], (B.shape[1] if B.dim() > 1 else 1)
-        _check(lib().egpu_dlaswp(self._h, int(inverse), m, n, _ptr(B), _ld(B), _ptr(p), p.shape[0]))
+        pp = _device_vec(p, p.shape[0], "int32")
+        _check(lib().egpu_dlaswp(self._h, int(inverse), m, n, _ptr(B), _ld(B), pp, p.shape[0]))
 
     def _batched(self, fn, As, Bs):
         self._bind_stream()

@@ -58,3 +58,15 @@ def test_header_is_plain_c(tmp_path):
     subprocess.run(["gcc", "-std=c99", "-Wall", "-Wextra", "-pedantic", "-Werror", "-I",
                     os.path.join(root, "include"), "-c", str(src), "-o", str(tmp_path / "uses_header.o")],
                    check=True, capture_output=True)
+
+
+def test_device_vector_arguments_are_checked_before_any_call():
+    import pytest
+    import torch
+    from elemental_b200 import _device_vec
+    with pytest.raises(TypeError):
+        _device_vec(torch.zeros(8, dtype=torch.int32), 8, "int32")  # host tensor
+    with pytest.raises(TypeError):
+        _device_vec([0] * 8, 8, "int32")
+    with pytest.raises(KeyError):
+        _device_vec(torch.zeros(8, dtype=torch.int32), 8, "int64")
