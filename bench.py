@@ -81,6 +81,19 @@ def flops_chol_solve(n, nrhs):
     return n ** 3 / 3.0 + 2.0 * n * n * nrhs
 
 
+def fp64_peak_probe():
+    """FP64 DMMA throughput of the current GPU (TFLOP/s) from the
+    benchmark-only library (elemental_b200/bench_csrc/fp64_peak.cu)."""
+    import ctypes
+    from elemental_b200 import build as _b
+    L = ctypes.CDLL(_b.BENCH_LIB)
+    v = ctypes.c_double()
+    rc = L.egpu_bench_fp64_peak(ctypes.byref(v))
+    if rc != 0:
+        raise RuntimeError(f"FP64 peak probe failed (cudaError {rc})")
+    return v.value
+
+
 def measured_peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -338,6 +351,7 @@ def timed(args, ws, dev, stream, h, step):
             e1.record(stream)
             torch.cuda.synchronize(dev)
         trace = h.trace_summary()
+        trace["_busy_ms"] = h.trace_busy_ms()
         h.trace_enable(False)
         launches = h.launch_count() - launches0
         barrier(ws)
@@ -352,25 +366,39 @@ def backward_error(A, X, B):
     return float((R.abs().amax(0) / den).max())
 
 
-def roofline_of(trace, kind, peaks):
-    """Roofline line for one traced kernel class."""
+def roofline_of(trace, kind, peaks, busy_total_ms):
+    """Roofline line for one traced kernel class.  Its time is the class's
+    busy time on the device (the union of its launches' intervals across the
+    concurrent streams, egpu_trace_busy), not the sum of per-launch spans,
+    which counts overlapped launches twice."""
     t = trace.get(kind, {})
-    if not t or not t.get("launches") or t["ms"] <= 0:
+    if not t or not t.get("launches") or t["busy_ms"] <= 0:
         return None
-    total_ms = sum(v["ms"] for v in trace.values())
+    ms = t["busy_ms"]
+    common = {"launches": t["launches"], "time_ms": ms, "time_basis": "busy time of the kernel class (union of "
+              "its launch intervals across streams, CUDA events on each launch's stream)",
+              "share_of_busy_time": t["share_ms"] / busy_total_ms if busy_total_ms > 0 else None}
     if kind == "tc":  # FP32 C read-modify-write + split panels: HBM-bound at K = 128
         peak = peaks.get("hbm_gbs") or HBM_PEAK_GBS_FALLBACK
-        achieved = t["bytes"] / (t["ms"] / 1e3) / 1e9
+        achieved = t["bytes"] / (ms / 1e3) / 1e9
         return {"bound": "hbm", "kernel": "tc_gemm_kernel (tcgen05 TF32x3 trailing update)", "achieved": achieved,
                 "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)" if peaks.get("hbm_gbs") else "fallback",
-                "tensor_tflops": t["flops"] / (t["ms"] / 1e3) / 1e12, "traffic": None,
-                "launches": t["launches"], "share_of_traced_time": t["ms"] / total_ms}
-    achieved = t["flops"] / (t["ms"] / 1e3) / 1e12
+                "tensor_tflops": t["flops"] / (ms / 1e3) / 1e12, "traffic": None, **common}
+    achieved = t["flops"] / (ms / 1e3) / 1e12
     return {"bound": "tensor", "kernel": "dgemm_tma_kernel (FP64 DMMA trailing update)", "achieved": achieved,
             "peak": FP64_PEAK_TFLOPS, "unit": "TFLOP/s", "frac": achieved / FP64_PEAK_TFLOPS, "traffic": None,
             "peak_source": "measured FP64 DMMA peak (profiles/fp64_peak.md); MEASURED_PEAKS.json has no FP64 entry",
-            "launches": t["launches"], "share_of_traced_time": t["ms"] / total_ms}
+            **common}
+
+
+def kernel_table(trace, steps):
+    """Per-class device time per step: busy (union across streams) and share
+    (overlapped time split among the classes in flight; the shares add up to
+    the traced busy time, which is at most the step time)."""
+    return {k: {"busy_ms_per_step": v["busy_ms"] / steps, "share_ms_per_step": v["share_ms"] / steps,
+                "launches_per_step": v["launches"] / steps}
+            for k, v in trace.items() if v["launches"]}
 
 
 def pinned_like(a):
@@ -430,8 +458,8 @@ def our_arm(args, ws, rank, local):
             pbwd = backward_error(A0, B, B0)
         plain = {"value": ws * args.steps / (pms / 1e3), "unit": "solves/s", "ms_per_step": pms / args.steps,
                  "backward_error": pbwd, "api": "egpu_dposv (Cholesky + HPD solve, FP64)",
-                 "roofline": roofline_of(ptrace, "update", measured_peaks()),
-                 "kernels": {k: {"ms": v["ms"], "launches": v["launches"]} for k, v in ptrace.items() if v["launches"]}}
+                 "roofline": roofline_of(ptrace, "update", measured_peaks(), ptrace.pop("_busy_ms")),
+                 "kernels": kernel_table(ptrace, args.steps)}
 
     # ---- end to end through the host-memory C ABI, pinned host buffers
     Ah, Bh = pinned_like(A_host), pinned_like(B_host)
@@ -467,7 +495,8 @@ def our_arm(args, ws, rank, local):
     if rank != 0:
         return
     peaks = measured_peaks()
-    roof = roofline_of(trace, "tc" if kind == "mixed" else "update", peaks)
+    busy = trace.pop("_busy_ms")
+    roof = roofline_of(trace, "tc" if kind == "mixed" else "update", peaks, busy)
     cpu = None
     if ws == 1 and not args.no_cpu:
         threads = os.cpu_count() or 1
@@ -493,7 +522,8 @@ def our_arm(args, ws, rank, local):
                         "chol": "egpu_host_dposv (HPDSolve)"}[kind],
                 "x_rel_diff_vs_device_path": xerr},
         "roofline": roof,
-        "kernels": {k: {"ms": v["ms"], "launches": v["launches"]} for k, v in trace.items() if v["launches"]},
+        "kernels": kernel_table(trace, args.steps),
+        "traced_busy_ms_per_step": busy / args.steps,
         "gpu_launches": launches,
         "clocks": clocks,
         "cpu_baseline": cpu,
@@ -866,7 +896,7 @@ def kernel_case(args):
         h.lu(A, p)
     elif args.case == "peaks":
         # roofline denominators and vendor reference points on this GPU
-        out = {"dmma_peak_tflops": h.measure_fp64_peak()}
+        out = {"dmma_peak_tflops": fp64_peak_probe()}
         torch.backends.cuda.matmul.allow_tf32 = False
         for m in (4096, 8192):
             a = torch.randn(m, m, dtype=torch.float64, device="cuda")

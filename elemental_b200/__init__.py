@@ -94,12 +94,12 @@ def _declare(L):
         "egpu_set_async": ([H, I], I),
         "egpu_get_status": ([H, P], I),
         "egpu_reserve": ([H, ctypes.c_size_t], I),
-        "egpu_measure_fp64_peak": ([H, P], I),
         "egpu_error_string": ([I], ctypes.c_char_p),
         "egpu_last_error_detail": ([], ctypes.c_char_p),
         "egpu_launch_count": ([H], LL),
         "egpu_trace_enable": ([H, I], I),
         "egpu_trace_summary": ([H, I, P, P, P, P], I),
+        "egpu_trace_busy": ([H, I, P, P], I),
         "egpu_trace_events": ([H, I, P, P, P, P], I),
         "egpu_dpotrf": ([H, I, I, P, I, P], I),
         "egpu_dpotrs": ([H, I, I, I, I, P, I, P, I], I),
@@ -217,15 +217,18 @@ def _ptr(t):
     return ctypes.c_void_p(t.data_ptr())
 
 
-def _device_vec(t, count: int, dtype: str):
+def _device_vec(t, count: int, dtype: str, device: int):
     """Pointer to a device-vector argument: a contiguous CUDA tensor of
-    ``dtype`` ("int32" or "float64") with at least ``count`` elements, the
-    number the library reads or writes.  Checked here because a short or
-    mistyped buffer would otherwise be written out of bounds on the device."""
+    ``dtype`` ("int32" or "float64") on GPU ``device`` (the handle's) with at
+    least ``count`` elements, the number the library reads or writes.  Checked
+    here because a short, mistyped or other-GPU buffer would otherwise be
+    written out of bounds (or through another device's pointer) by a kernel."""
     import torch
     want = {"int32": torch.int32, "float64": torch.float64}[dtype]
     if not isinstance(t, torch.Tensor) or t.device.type != "cuda":
         raise TypeError(f"expected a CUDA tensor of {dtype}")
+    if t.device.index != device:
+        raise ValueError(f"expected a tensor on cuda:{device} (the handle's GPU), got {t.device}")
     if t.dtype != want:
         raise TypeError(f"expected a {dtype} tensor, got {t.dtype}")
     if not t.is_contiguous() or t.numel() < count:
@@ -416,12 +419,6 @@ class Handle:
         info = ctypes.c_int(0)
         _check(lib().egpu_get_status(self._h, ctypes.byref(info)), info.value)
 
-    def measure_fp64_peak(self) -> float:
-        """FP64 DMMA throughput of this GPU (TFLOP/s), the FP64 roofline peak."""
-        v = ctypes.c_double()
-        _check(lib().egpu_measure_fp64_peak(self._h, ctypes.byref(v)))
-        return v.value
-
     def reserve(self, nbytes: int):
         _check(lib().egpu_reserve(self._h, int(nbytes)))
 
@@ -468,14 +465,27 @@ class Handle:
                 for i in range(n)]
 
     def trace_summary(self) -> dict:
-        """{kind: {"ms", "flops", "bytes", "launches"}} over the traced launches."""
+        """{kind: {"ms", "flops", "bytes", "launches", "busy_ms", "share_ms"}} over
+        the traced launches: "ms" sums per-launch durations; "busy_ms" is the
+        union of the kind's launch intervals across streams; "share_ms" splits
+        overlapped time evenly among the kinds in flight (the shares add up to
+        the traced busy time)."""
         out = {}
         for name, k in self.TRACE_KINDS.items():
             ms, fl, by, n = ctypes.c_double(), ctypes.c_double(), ctypes.c_double(), ctypes.c_longlong()
             _check(lib().egpu_trace_summary(self._h, k, ctypes.byref(ms), ctypes.byref(fl), ctypes.byref(by),
                                             ctypes.byref(n)))
-            out[name] = {"ms": ms.value, "flops": fl.value, "bytes": by.value, "launches": n.value}
+            busy, share = ctypes.c_double(), ctypes.c_double()
+            _check(lib().egpu_trace_busy(self._h, k, ctypes.byref(busy), ctypes.byref(share)))
+            out[name] = {"ms": ms.value, "flops": fl.value, "bytes": by.value, "launches": n.value,
+                         "busy_ms": busy.value, "share_ms": share.value}
         return out
+
+    def trace_busy_ms(self) -> float:
+        """Busy time of the traced region (any kind in flight), ms."""
+        busy = ctypes.c_double()
+        _check(lib().egpu_trace_busy(self._h, -1, ctypes.byref(busy), None))
+        return busy.value
 
     # ---------------- device API (torch CUDA tensors, column-major) ----
     def cholesky(self, A, uplo=LOWER):
@@ -499,7 +509,7 @@ class Handle:
     def lu(self, A, p):
         self._bind_stream()
         info = ctypes.c_int(0)
-        pp = _device_vec(p, min(A.shape[0], A.shape[1]), "int32")
+        pp = _device_vec(p, min(A.shape[0], A.shape[1]), "int32", self.device)
         rc = lib().egpu_dgetrf(self._h, A.shape[0], A.shape[1], _ptr(A), _ld(A), pp, ctypes.byref(info))
         _check(rc, info.value)
 
@@ -509,7 +519,7 @@ class Handle:
         n doubles, also receives D)."""
         self._bind_stream()
         info = ctypes.c_int(0)
-        dd = None if d is None else _device_vec(d, A.shape[0], "float64")
+        dd = None if d is None else _device_vec(d, A.shape[0], "float64", self.device)
         rc = lib().egpu_dldl(self._h, orient, A.shape[0], _ptr(A), _ld(A), dd, ctypes.byref(info))
         _check(rc, info.value)
 
@@ -621,7 +631,7 @@ class Handle:
 
     def lu_solve_after(self, A, p, B, orient=NORMAL):
         self._bind_stream()
-        pp = None if p is None else _device_vec(p, A.shape[0], "int32")
+        pp = None if p is None else _device_vec(p, A.shape[0], "int32", self.device)
         _check(lib().egpu_dgetrs(self._h, orient, A.shape[0], B.shape[1] if B.dim() > 1 else 1, _ptr(A), _ld(A),
                                  pp, _ptr(B), _ld(B)))
 
@@ -659,7 +669,7 @@ class Handle:
     def apply_row_pivots(self, B, p, inverse=False):
         self._bind_stream()
         m, n = B.shape[0], (B.shape[1] if B.dim() > 1 else 1)
-        pp = _device_vec(p, p.shape[0], "int32")
+        pp = _device_vec(p, p.shape[0], "int32", self.device)
         _check(lib().egpu_dlaswp(self._h, int(inverse), m, n, _ptr(B), _ld(B), pp, p.shape[0]))
 
     def _batched(self, fn, As, Bs):

@@ -1,8 +1,15 @@
-// Roofline denominator: FP64 tensor-core (DMMA) throughput of this GPU,
-// measured with an in-register mma.sync m16n8k8 loop (no memory traffic).
-#include "internal.h"
+// Benchmark-only library (libegpu_bench.so, not part of libelemgpu.so): the
+// FP64 roofline denominator of this GPU.  The FP64 tensor path on sm_100a is
+// warp-level DMMA (mma.sync m16n8k8 f64; tcgen05 has no f64 kind), so the
+// peak is an in-register m16n8k8 loop with no memory traffic, 8 CTAs of 256
+// threads per SM.  bench.py --case peaks loads this library by itself.
+#include <cuda_runtime.h>
 
-namespace egpu {
+#include <algorithm>
+
+#include "../csrc/common.cuh"
+
+namespace {
 
 __global__ void __launch_bounds__(256) dmma_peak_kernel(double* sink, int iters) {
   double a[4] = {threadIdx.x * 1e-3, 2e-3, 3e-3, 4e-3};
@@ -14,7 +21,7 @@ __global__ void __launch_bounds__(256) dmma_peak_kernel(double* sink, int iters)
     for (int j = 0; j < 4; ++j) c[i][j] = 0.0;
   for (int it = 0; it < iters; ++it) {
 #pragma unroll
-    for (int i = 0; i < 4; ++i) dmma_16x8x8(c[i], a, b);
+    for (int i = 0; i < 4; ++i) egpu::dmma_16x8x8(c[i], a, b);
   }
   double r = 0.0;
 #pragma unroll
@@ -24,18 +31,19 @@ __global__ void __launch_bounds__(256) dmma_peak_kernel(double* sink, int iters)
   sink[blockIdx.x * blockDim.x + threadIdx.x] = r;
 }
 
-}  // namespace egpu
+}  // namespace
 
-using namespace egpu;
-
-extern "C" int egpu_measure_fp64_peak(egpu_handle h, double* tflops) {
-  if (!h || !tflops) return EGPU_ERR_ARG;
+// DMMA throughput of the current device in TFLOP/s (best of two timed
+// launches after one warm-up).  Returns 0, or the failing cudaError_t.
+extern "C" __attribute__((visibility("default"))) int egpu_bench_fp64_peak(double* tflops) {
+  if (!tflops) return (int)cudaErrorInvalidValue;
   int dev = 0, sms = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   const int blocks = sms * 8, threads = 256, iters = 2000;
   double* sink = nullptr;
-  EGPU_CUDA_TRY(cudaMalloc(&sink, sizeof(double) * blocks * threads));
+  cudaError_t e = cudaMalloc(&sink, sizeof(double) * blocks * threads);
+  if (e != cudaSuccess) return (int)e;
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
@@ -49,16 +57,13 @@ extern "C" int egpu_measure_fp64_peak(egpu_handle h, double* tflops) {
     cudaEventElapsedTime(&ms, e0, e1);
     if (rep > 0) best = std::min(best, ms);
   }
-  cudaError_t e = cudaGetLastError();
+  e = cudaGetLastError();
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   cudaFree(sink);
-  if (e != cudaSuccess) {
-    set_last_error(e, "dmma_peak", __FILE__, __LINE__);
-    return EGPU_ERR_CUDA;
-  }
-  // per warp per iteration: 4 MMAs of 16x8x8 = 4 * 2 * 1024 flops
+  if (e != cudaSuccess) return (int)e;
+  // per warp per iteration: 4 MMAs of 16 x 8 x 8 = 4 * 2 * 1024 flops
   const double flops = 4.0 * 2.0 * 16 * 8 * 8 * (double)iters * blocks * (threads / 32);
   *tflops = flops / (best * 1e-3) / 1e12;
-  return EGPU_OK;
+  return 0;
 }

@@ -14,6 +14,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libelemgpu.so")
+BENCH_LIB = os.path.join(HERE, "libegpu_bench.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -27,10 +28,10 @@ def sources() -> list[str]:
 
 
 def needs_build() -> bool:
-    if not os.path.exists(LIB):
+    if not os.path.exists(LIB) or not os.path.exists(BENCH_LIB):
         return True
-    t = os.path.getmtime(LIB)
-    deps = sources() + glob.glob(os.path.join(CSRC, "*.cuh")) + glob.glob(os.path.join(CSRC, "*.h"))
+    t = min(os.path.getmtime(LIB), os.path.getmtime(BENCH_LIB))
+    deps = sources() + glob.glob(os.path.join(CSRC, "*.cuh")) + glob.glob(os.path.join(HERE, "bench_csrc", "*.cu")) + glob.glob(os.path.join(CSRC, "*.h"))
     deps += glob.glob(os.path.join(HERE, "..", "include", "*.h"))
     return any(os.path.getmtime(d) > t for d in deps)
 
@@ -63,10 +64,23 @@ def build(force: bool = False, verbose: bool = False, jobs: int | None = None) -
     if failed:
         raise RuntimeError("nvcc failed")
     tmp = LIB + ".tmp"
-    subprocess.run([nvcc()] + ARCH + ["-shared", "-o", tmp] + objs + ["-lcuda" if False else "-lcudart_static", "-lrt", "-ldl", "-lpthread"],
+    subprocess.run([nvcc()] + ARCH + ["-shared", "-o", tmp] + objs + ["-lcudart_static", "-lrt", "-ldl", "-lpthread"],
                    check=True)
     os.replace(tmp, LIB)
+    build_bench(flags)
     return LIB
+
+
+def build_bench(flags: list[str]) -> str:
+    """The benchmark-only library (bench_csrc/*.cu -> libegpu_bench.so): the
+    FP64 peak probe that bench.py uses as its roofline denominator.  It is not
+    linked into libelemgpu.so."""
+    srcs = sorted(glob.glob(os.path.join(HERE, "bench_csrc", "*.cu")))
+    tmp = BENCH_LIB + ".tmp"
+    subprocess.run([nvcc()] + flags + ["-shared", "-o", tmp] + srcs + ["-lcudart_static", "-lrt", "-ldl", "-lpthread"],
+                   check=True)
+    os.replace(tmp, BENCH_LIB)
+    return BENCH_LIB
 
 
 if __name__ == "__main__":

@@ -1,5 +1,6 @@
 // C-ABI entry points: handle, workspace, and the blocked right-looking
 // drivers that sequence the sm_100a kernels for Cholesky, LU and the solves.
+#include <algorithm>
 #include <atomic>
 #include <cstring>
 #include <vector>
@@ -867,6 +868,59 @@ int egpu_trace_summary(egpu_handle h, int kind, double* total_ms, double* total_
   if (total_flops) *total_flops = fl;
   if (total_bytes) *total_bytes = by;
   if (launches) *launches = n;
+  return EGPU_OK;
+}
+
+int egpu_trace_busy(egpu_handle h, int kind, double* busy_ms, double* share_ms) {
+  TRY(check_handle(h));
+  Enter g(h);
+  if (kind < -1 || kind >= kTraceKinds) return EGPU_ERR_ARG;
+  // every launch as an interval on one time axis (the first launch's start)
+  struct Iv { double t0, t1; int kind; };
+  std::vector<Iv> iv;
+  const int n = (int)h->trace.recs.size();
+  if (n > 0) {
+    const cudaEvent_t base = h->trace.recs[0].e0;
+    iv.reserve(n);
+    for (const auto& r : h->trace.recs) {
+      EGPU_CUDA_TRY(cudaEventSynchronize(r.e1));
+      float a = 0, b = 0;
+      EGPU_CUDA_TRY(cudaEventElapsedTime(&a, base, r.e0));
+      EGPU_CUDA_TRY(cudaEventElapsedTime(&b, base, r.e1));
+      iv.push_back({a, std::max(a, b), r.kind});
+    }
+  }
+  // sweep over the interval end points: a segment counts toward `busy` when a
+  // launch of `kind` (any kind for -1) is in flight, and toward `share` by
+  // 1 / (number of distinct kinds in flight) when `kind` is one of them
+  std::vector<std::pair<double, int>> ev;  // (time, +-(index + 1))
+  ev.reserve(2 * iv.size());
+  for (int i = 0; i < (int)iv.size(); ++i) {
+    ev.push_back({iv[i].t0, i + 1});
+    ev.push_back({iv[i].t1, -(i + 1)});
+  }
+  std::sort(ev.begin(), ev.end(), [](const std::pair<double, int>& a, const std::pair<double, int>& b) {
+    return a.first < b.first || (a.first == b.first && a.second < b.second);  // ends before starts
+  });
+  int active[kTraceKinds] = {0};
+  double busy = 0, share = 0, prev = ev.empty() ? 0.0 : ev[0].first;
+  for (const auto& e : ev) {
+    const double dt = e.first - prev;
+    if (dt > 0) {
+      int kinds = 0, any = 0;
+      for (int k = 0; k < kTraceKinds; ++k) kinds += active[k] > 0, any += active[k];
+      const bool mine = kind < 0 ? any > 0 : active[kind] > 0;
+      if (mine) {
+        busy += dt;
+        share += kind < 0 ? dt : dt / kinds;
+      }
+    }
+    prev = e.first;
+    const Iv& x = iv[std::abs(e.second) - 1];
+    active[x.kind] += e.second > 0 ? 1 : -1;
+  }
+  if (busy_ms) *busy_ms = busy;
+  if (share_ms) *share_ms = share;
   return EGPU_OK;
 }
 

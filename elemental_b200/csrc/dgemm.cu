@@ -128,8 +128,13 @@ int launch_dgemm(cudaStream_t st, bool a_kmajor, bool b_kmajor, int M, int N, in
       nblocks += std::max(0, hi - lo);
     }
   }
-  const double flops = (tri == 0 ? 2.0 * M * N : (double)M * (M + 1)) * K;
-  const double bytes = 8.0 * ((double)M * K + (double)N * K + (beta == 0.0 ? 1.0 : 2.0) * M * N * (tri ? 0.5 : 1.0));
+  // entries of C the product touches: the whole M x N block, or the lower
+  // (tri 1) / upper (tri 2) trapezoid -- a launch over rows [c0, n) of block
+  // columns [c0, c1) is a triangle on top of a rectangle
+  const double lo_n = std::min(M, N), rect = tri == 1 ? std::max(0, M - N) : std::max(0, N - M);
+  const double entries = tri == 0 ? (double)M * N : lo_n * (lo_n + 1) / 2 + rect * lo_n;
+  const double flops = 2.0 * entries * K;
+  const double bytes = 8.0 * ((double)M * K + (double)N * K + (beta == 0.0 ? 1.0 : 2.0) * entries);
   TraceMark tm(st, beta == 0.0 ? kTraceTrsm : kTraceUpdate, flops, bytes);
   cudaError_t e;
   if (half) {

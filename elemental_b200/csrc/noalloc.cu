@@ -14,6 +14,12 @@
 // call's contents; the status word is cleared at the start of each call and
 // the inverse block is always written before it is read.  Calls whose work
 // overlaps on the GPU (other streams, other host threads) race on the array.
+// Under CUDA's lazy module loading (the default) the driver loads this file's
+// module, and with it the array, and the kernels' modules on the first call on
+// a device: that call is where device memory is taken, so callers make one
+// small call at start-up (or run with CUDA_MODULE_LOADING=EAGER).  An odd nb
+// is rounded down to the next even value (the diagonal kernels work on column
+// pairs), as egpu_set_blocksize does for a handle.
 #include <mutex>
 
 #include "internal.h"

@@ -112,11 +112,20 @@ EGPU_API long long egpu_launch_count(egpu_handle h);
  * multiply by an inverted diagonal block (Trsm), 2 diagonal-block kernels,
  * 3 LU panel, 4 row interchanges, 5 other (batched kernels, conversions),
  * 6 tcgen05 tensor-core updates, 7 one-launch solve sweeps.  enable() clears the records;
- * summary() waits for the recorded launches and sums their device time,
- * algorithmic flops and algorithmic bytes. */
+ * summary() waits for the recorded launches and sums their per-launch device
+ * times (start-to-end on each launch's own stream), algorithmic flops and
+ * algorithmic bytes. */
 EGPU_API int egpu_trace_enable(egpu_handle h, int on);
 EGPU_API int egpu_trace_summary(egpu_handle h, int kind, double* total_ms, double* total_flops,
                                 double* total_bytes, long long* launches);
+/* Device time of one launch kind (-1: any kind) on one time axis, the
+ * concurrent streams merged: *busy_ms = the time during which at least one
+ * traced launch of that kind was in flight (the union of the launches'
+ * intervals; with kind -1 the traced region's busy time); *share_ms = that
+ * time with every moment split evenly among the kinds in flight, so the
+ * shares of all kinds add up to the busy time of kind -1.  Sums of per-launch
+ * durations (egpu_trace_summary) count overlapped launches twice. */
+EGPU_API int egpu_trace_busy(egpu_handle h, int kind, double* busy_ms, double* share_ms);
 /* The traced launches in order: kind (as egpu_trace_summary), stream (0 the
    handle's stream, 1 the look-ahead side stream, 2 the lowest-priority
    auxiliary stream, 3 another), start relative to the first traced launch
@@ -124,10 +133,6 @@ EGPU_API int egpu_trace_summary(egpu_handle h, int kind, double* total_ms, doubl
    of traced launches (or a negative error code). */
 EGPU_API int egpu_trace_events(egpu_handle h, int max, int* kind, int* stream_tag, double* start_ms,
                                double* dur_ms);
-
-/* Roofline denominator: measured FP64 tensor-core (DMMA) throughput of the
- * handle's GPU in TFLOP/s (in-register mma.sync loop, ~30 ms). */
-EGPU_API int egpu_measure_fp64_peak(egpu_handle h, double* tflops);
 
 /* ---- device-memory API ---- */
 
@@ -347,10 +352,16 @@ EGPU_API int egpu_dsafe_hpd_det(egpu_handle h, int uplo, int n, double* dA, int 
  * allocation fail or synchronise the device mid-run.  Same result as
  * egpu_dpotrf with lookahead 0, on the caller's stream (NULL = the legacy
  * default stream), no handle.  dA must be 16-byte aligned with an even lda
- * (EGPU_ERR_ALIGN otherwise); nb in [2, 128] (EGPU_ERR_UNSUPPORTED otherwise).
+ * (EGPU_ERR_ALIGN otherwise); nb in [2, 128] (EGPU_ERR_UNSUPPORTED otherwise),
+ * an odd nb rounded down to the next even value as egpu_set_blocksize does.
  * Scratch: a file-scope 128 KiB + 256 B __device__ array on every GPU that
  * loads the library, held until exit; its device address is looked up on the
  * first call on each device (make that first call before any stream capture).
+ * With CUDA's default lazy module loading that first call is also where the
+ * driver loads the kernels it launches and places the array, which takes
+ * device memory: make one small call at start-up (or set
+ * CUDA_MODULE_LOADING=EAGER) so that later calls allocate nothing.  Each call
+ * ends by waiting for the caller's stream (the status word is read back).
  * All calls share the array: calls that overlap on the GPU race. */
 EGPU_API int egpu_dpotrf_noalloc(void* stream, int uplo, int n, double* dA, int lda, int nb, int* info);
 

@@ -191,6 +191,15 @@ def trsm(side, uplo, orient, diag, alpha, A, B):
     return B
 
 
+def trsv(uplo, orient, diag, A, x):
+    """Trsv(uplo, orientation, diag, A, x) (blas-like/level2/Trsv.hpp:20-44,
+    dtrsv_ at src/core/imports/blas.cpp:901-904): x := op(A)^-1 x."""
+    x = np.array(x, dtype=A.dtype, copy=True).reshape(-1)
+    n = x.shape[0]
+    getattr(lib(), f"oref_{_pfx(x)}trsv")(uplo.encode(), orient.encode(), diag.encode(), n, _p(_f(A)), _ld(A), _p(x))
+    return x
+
+
 def gemm(ta, tb, alpha, A, B, beta, C):
     C = _f(C).copy(order="F")
     m, n = C.shape

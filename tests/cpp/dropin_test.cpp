@@ -9,6 +9,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <random>
+#include <string>
 
 #include "elemgpu/elemental.hpp"
 
@@ -101,8 +102,83 @@ void TestLU(int m, double tol) {
   Check(e3 < tol * m, "GaussianElimination recovers X", e3);
 }
 
+// --dist-dump DIR: run the 1 x 1 DistMatrix overloads (and Trsv on a
+// Matrix) on the inputs DIR/spd.bin, DIR/ge.bin (n x n) and DIR/rhs.bin
+// (n x k), each a header {rows, cols} of int32 followed by the column-major
+// doubles, and write every result to DIR/<name>.bin in the same format; the
+// Python side compares them with the oracle.
+static Matrix<double> ReadBin(const std::string& path) {
+  FILE* f = std::fopen(path.c_str(), "rb");
+  if (!f) { std::printf("cannot open %s\n", path.c_str()); std::exit(2); }
+  int hw[2] = {0, 0};
+  if (std::fread(hw, sizeof(int), 2, f) != 2) std::exit(2);
+  Matrix<double> A(hw[0], hw[1]);
+  for (int j = 0; j < hw[1]; ++j)
+    if (std::fread(A.Buffer(0, j), sizeof(double), hw[0], f) != (size_t)hw[0]) std::exit(2);
+  std::fclose(f);
+  return A;
+}
+
+template <typename T>
+static void WriteBin(const std::string& path, const Matrix<T>& A) {
+  FILE* f = std::fopen(path.c_str(), "wb");
+  if (!f) std::exit(2);
+  const int hw[2] = {A.Height(), A.Width()};
+  std::fwrite(hw, sizeof(int), 2, f);
+  for (int j = 0; j < A.Width(); ++j) std::fwrite(A.LockedBuffer(0, j), sizeof(T), A.Height(), f);
+  std::fclose(f);
+}
+
+static int DistDump(const std::string& dir) {
+  Grid g;
+  const Matrix<double> spd = ReadBin(dir + "/spd.bin"), ge = ReadBin(dir + "/ge.bin"), rhs = ReadBin(dir + "/rhs.bin");
+  for (UpperOrLower uplo : {LOWER, UPPER}) {
+    const char* u = uplo == LOWER ? "L" : "U";
+    DistMatrix<double> A(g), B(g), X(g);
+    A.Matrix() = spd;
+    Cholesky(uplo, A);  // Cholesky.hpp:79-101
+    WriteBin(dir + "/chol_" + u + ".bin", A.LockedMatrix());
+    X.Matrix() = rhs;
+    cholesky::SolveAfter(uplo, NORMAL, A, X);  // Cholesky/SolveAfter.hpp:77-134
+    WriteBin(dir + "/solveafter_" + u + ".bin", X.LockedMatrix());
+    A.Matrix() = spd;
+    B.Matrix() = rhs;
+    HPDSolve(uplo, NORMAL, A, B);  // HPDSolve.hpp:30-41
+    WriteBin(dir + "/hpdsolve_" + u + ".bin", B.LockedMatrix());
+  }
+  {
+    DistMatrix<double> A(g), B(g);
+    DistMatrix<int, VC, STAR> p(g);
+    A.Matrix() = ge;
+    LU(A, p);  // LU.hpp:220-321
+    WriteBin(dir + "/lu.bin", A.LockedMatrix());
+    WriteBin(dir + "/lu_p.bin", p.LockedMatrix());
+    B.Matrix() = rhs;
+    lu::SolveAfter(NORMAL, A, p, B);  // LU/SolveAfter.hpp:148-195
+    WriteBin(dir + "/lusolve.bin", B.LockedMatrix());
+    A.Matrix() = ge;
+    B.Matrix() = rhs;
+    GaussianElimination(A, B);  // GaussianElimination.hpp:234-252
+    WriteBin(dir + "/gauss.bin", B.LockedMatrix());
+  }
+  for (UpperOrLower uplo : {LOWER, UPPER})
+    for (Orientation o : {NORMAL, TRANSPOSE}) {
+      Matrix<double> x(rhs.Height(), 1);
+      for (int i = 0; i < rhs.Height(); ++i) x.Set(i, 0, rhs.Get(i, 0));
+      Trsv(uplo, o, NON_UNIT, spd, x);  // Trsv.hpp:20-44
+      WriteBin(dir + "/trsv_" + (uplo == LOWER ? "L" : "U") + (o == NORMAL ? "N" : "T") + ".bin", x);
+    }
+  std::printf("DUMPED\n");
+  return 0;
+}
+
 int main(int argc, char** argv) {
   Initialize(argc, argv);
+  if (argc == 3 && std::string(argv[1]) == "--dist-dump") {
+    const int rc = DistDump(argv[2]);
+    Finalize();
+    return rc;
+  }
   PushBlocksizeStack(96);
   TestCholesky<double>(LOWER, 500, 1e-12);
   TestCholesky<double>(UPPER, 333, 1e-12);

@@ -65,8 +65,8 @@ def test_device_vector_arguments_are_checked_before_any_call():
     import torch
     from elemental_b200 import _device_vec
     with pytest.raises(TypeError):
-        _device_vec(torch.zeros(8, dtype=torch.int32), 8, "int32")  # host tensor
+        _device_vec(torch.zeros(8, dtype=torch.int32), 8, "int32", 0)  # host tensor
     with pytest.raises(TypeError):
-        _device_vec([0] * 8, 8, "int32")
+        _device_vec([0] * 8, 8, "int32", 0)
     with pytest.raises(KeyError):
-        _device_vec(torch.zeros(8, dtype=torch.int32), 8, "int64")
+        _device_vec(torch.zeros(8, dtype=torch.int32), 8, "int64", 0)

@@ -118,3 +118,24 @@ def test_hpd_solve_mixed_gmres_ir(handle, kappa):
     assert be <= 1e-14
     assert _berr(A, X.cpu().numpy(), B) <= 1e-14
     assert handle.mixed_gmres_iterations() > 0
+
+
+def test_hpd_solve_mixed_config_n16384_kappa1e6(handle):
+    # The benchmark configuration: n = 16384, A = Q diag(s) Q^T with s
+    # log-spaced over [1, 1e6], 32 right-hand sides ~ N(0,1).  The mixed solve
+    # reaches backward error <= 1e-14, and its X agrees with the plain FP64
+    # solve (egpu_dposv) on the same A and B to kappa * 1e-13.
+    n, k, kappa = 16384, 32, 1e6
+    A = inputs.spd_spectrum_torch(n, kappa, 20240, "cuda")
+    B = torch.from_numpy(inputs.normal(n, k, 20241)).cuda().t().contiguous().t()
+    X, iters, berr = handle.hpd_solve_mixed(A, B, eg.LOWER, 30, 1e-14)
+    torch.cuda.synchronize()
+    R = B - A @ X
+    den = A.abs().sum(1).max() * X.abs().amax(0) + B.abs().amax(0)
+    be = float((R.abs().amax(0) / den).max())
+    assert be <= 1e-14 and berr <= 1e-14, (be, berr, iters)
+    A2, X2 = A.clone(), B.clone()
+    handle.hpd_solve(A2, X2, eg.LOWER)
+    del A2
+    rel = float((X - X2).abs().max() / X2.abs().max())
+    assert rel <= kappa * 1e-13, rel

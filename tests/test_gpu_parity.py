@@ -12,6 +12,8 @@ Tolerances (floating point, FP64):
   * solves: ||A X - B||_1 / (||A||_1 ||X||_1 n eps) <= 4 and X within 1e-9
     relative of the oracle's X.
 """
+import os
+
 import numpy as np
 import pytest
 
@@ -104,6 +106,26 @@ def test_trsm(handle, side, uplo, orient, diag):
     assert np.max(np.abs(host(dB) - ref)) <= 1e-12 * np.max(np.abs(ref))
 
 
+@pytest.mark.parametrize("uplo", [eg.LOWER, eg.UPPER])
+@pytest.mark.parametrize("orient", [eg.NORMAL, eg.TRANSPOSE])
+@pytest.mark.parametrize("diag", [eg.NON_UNIT, eg.UNIT])
+@pytest.mark.parametrize("n", [1, 257, 1030])
+def test_trsv(handle, uplo, orient, diag, n):
+    # Trsv(uplo, orientation, diag, A, x), blas-like/level2/Trsv.hpp:20-44
+    r = inputs.rng(n + 16 * uplo + 4 * orient + diag)
+    A = np.asfortranarray(r.uniform(-1, 1, (n, n)) / np.sqrt(n) + 2 * np.eye(n))
+    x = r.standard_normal(n)
+    dA = cuda(A)
+    import torch
+    dx = torch.from_numpy(x.copy()).cuda()
+    handle.trsv(uplo, orient, diag, dA, dx)
+    ref = orc.trsv("L" if uplo == eg.LOWER else "U", "N" if orient == eg.NORMAL else "T",
+                   "U" if diag == eg.UNIT else "N", A, x)
+    got = dx.cpu().numpy()
+    assert np.max(np.abs(got - ref)) <= 1e-12 * np.max(np.abs(ref))
+    assert np.array_equal(host(dA), A)  # A is read only
+
+
 # ------------------------------------------------------------- Cholesky --
 
 @pytest.mark.parametrize("n", [1, 2, 7, 127, 128, 129, 300, 1000, 2048])
@@ -183,6 +205,54 @@ def test_lu_pivots_and_factors(handle, n):
     assert np.array_equal(p, pref), np.nonzero(p != pref)[0][:10]
     assert np.max(np.abs(F - ref)) <= 1e-10 * max(1.0, np.max(np.abs(ref)))
     assert lu_bwd(A, F, p) <= BWD
+
+
+def test_lu_config_n8192_64rhs(handle):
+    # LU with partial pivoting + lu::SolveAfter at the benchmark configuration
+    # (n = 8192, nb = 128, A ~ U[-1,1] seeded, 64 right-hand sides ~ N(0,1)):
+    # the pivot vector index for index, the factors, the backward error and X
+    # against the oracle on the same inputs (LU.hpp:144-218, LU/Panel.hpp:52-64,
+    # LU/SolveAfter.hpp:101-146)
+    import torch
+    n, k = 8192, 64
+    A = inputs.uniform(n, n, 20240)
+    B = inputs.normal(n, k, 20241)
+    dA = cuda(A)
+    dp = torch.zeros(n, dtype=torch.int32, device="cuda")
+    handle.lu(dA, dp)
+    dB = cuda(B)
+    handle.lu_solve_after(dA, dp, dB, eg.NORMAL)
+    F, p, X = host(dA), dp.cpu().numpy(), host(dB)
+    orc.set_threads(os.cpu_count() or 1)
+    ref, pref, st = orc.lu(A, 128)
+    assert st == 0
+    assert np.array_equal(p, pref), np.nonzero(p != pref)[0][:10]
+    assert np.max(np.abs(F - ref)) <= 1e-9 * max(1.0, np.max(np.abs(ref)))
+    Xref = orc.lu_solve_after(ref, pref, B, orc.NORMAL)
+    assert np.max(np.abs(X - Xref)) <= 1e-7 * np.max(np.abs(Xref))
+    # backward error through A X - B (the n^3 product of L U is left to the
+    # factor comparison above)
+    assert solve_bwd(A, X, B) <= BWD * 4
+
+
+def test_lu_tall_panel_grid_form(handle):
+    # m = 20000 rows: taller than one cluster holds (16 x 1024), so the panel
+    # runs the cooperative grid form; pivots, factors and solve vs the oracle
+    import torch
+    m, n = 20000, 320
+    A = inputs.uniform(m, n, 4242)
+    dA = cuda(A)
+    dp = torch.zeros(n, dtype=torch.int32, device="cuda")
+    handle.trace_enable(True)
+    handle.lu(dA, dp)
+    ev = handle.trace_events()
+    handle.trace_enable(False)
+    assert sum(1 for e in ev if e[0] == "panel") == 3
+    ref, pref, st = orc.lu(A, 128)
+    assert st == 0
+    assert np.array_equal(dp.cpu().numpy(), pref)
+    assert np.max(np.abs(host(dA) - ref)) <= 1e-10 * max(1.0, np.max(np.abs(ref)))
+    assert lu_bwd(A, host(dA), dp.cpu().numpy()) <= BWD
 
 
 @pytest.mark.parametrize("shape", [(500, 300), (300, 500), (1000, 129)])

@@ -56,6 +56,30 @@ def test_noalloc_matches_handle_entry_point_twice(uplo):
             assert np.array_equal(dA.cpu().numpy()[other], A[other])
 
 
+def test_noalloc_second_call_takes_no_device_memory():
+    # after a first call on the device (module loading and the scratch array
+    # placed), a call on a new size leaves the free device memory unchanged
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    f = _noalloc()
+    info = ctypes.c_int(0)
+    # both sizes launch the same kernels (one diagonal-block kernel, the 64 x
+    # 128 panel multiply and the triangular update), so the first call has
+    # loaded everything the second one runs
+    A1 = eg.empty_colmajor(777, 777, ld=778)
+    A1.copy_(torch.from_numpy(inputs.spd_ggt(777, 31)))
+    A2 = eg.empty_colmajor(1300, 1300)
+    A2.copy_(torch.from_numpy(inputs.spd_ggt(1300, 32)))
+    torch.cuda.synchronize()
+    assert f(None, eg.LOWER, 777, ctypes.c_void_p(A1.data_ptr()), 778, 128, ctypes.byref(info)) == eg.OK
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    assert f(None, eg.LOWER, 1300, ctypes.c_void_p(A2.data_ptr()), 1300, 128, ctypes.byref(info)) == eg.OK
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info()[0] == free0
+
+
 def test_noalloc_rejects_and_reports():
     import torch
     if not torch.cuda.is_available():
