@@ -200,18 +200,34 @@ def make_inputs(kind, n, nrhs, seed, device=None):
     return A, B
 
 
-def cpu_oracle_solve(kind, n, nrhs, seed, threads):
-    """One factor + solve by the CPU oracle (FP64: the reference's algorithm);
-    returns seconds."""
+def cpu_checker():
+    """The CPU implementation timed beside the GPU: the reference's own code
+    (oracle/_ref/libelemref.so: Elemental compiled from its sources, level-3
+    flops in the scipy wheel's OpenBLAS on every host core) when it is built,
+    else the C restatement (oracle/liboracle.so, OpenMP).  Returns (module,
+    kind, description)."""
+    from oracle import ref
+    if ref.available():
+        return ref, "reference", "Elemental's own code (oracle/_ref, OpenBLAS on all host cores)"
     from oracle import pyoracle as orc
-    orc.set_threads(threads)
-    A, B = make_inputs(kind if kind != "mixed" else "chol", n, nrhs, seed)
+    orc.set_threads(os.cpu_count() or 1)
+    return orc, "port", "the C restatement of the reference (oracle/liboracle.so, OpenMP on all host cores)"
+
+
+def cpu_solve(kind, n, nrhs, seed):
+    """One FP64 factor + solve on the host cores by the CPU checker (Cholesky +
+    HPDSolve for chol/mixed, LU + lu::SolveAfter for lu); returns seconds.
+    The mixed workload's matrix is timed as G G^T + n I of the same order
+    (the factorization's cost does not depend on the spectrum, and the
+    Q diag(s) Q^T construction needs an n^3 QR on the host)."""
+    M, _, _ = cpu_checker()
+    A, B = make_inputs("lu" if kind == "lu" else "chol", n, nrhs, seed)
     t0 = time.perf_counter()
     if kind == "lu":
-        F, p, st = orc.lu(A, NB)
-        X = orc.lu_solve_after(F, p, B, orc.NORMAL)
+        F, p, st = M.lu(A, NB)
+        X = M.lu_solve_after(F, p, B, 0)
     else:
-        _, X, st = orc.hpd_solve(A, B, orc.LOWER, nb=NB)
+        _, X, st = M.hpd_solve(A, B, 0, nb=NB)
     dt = time.perf_counter() - t0
     assert st == 0 and np.isfinite(X).all()
     return dt
@@ -221,87 +237,94 @@ def flops_of(kind, n, nrhs):
     return flops_lu_solve(n, nrhs) if kind == "lu" else flops_chol_solve(n, nrhs)
 
 
-def cpu_sample(kind, n_full, nrhs, seed, threads, budget_s, reps):
-    """Time the oracle on a bounded sample: the largest n <= n_full (halving)
-    whose `reps` runs fit in about budget_s; returns (seconds per full-size
-    solve, sample description)."""
-    t_probe = cpu_oracle_solve(kind, 1024, nrhs, seed, threads)
-    est = t_probe * flops_of(kind, n_full, nrhs) / flops_of(kind, 1024, nrhs)
+def cpu_sample(kind, n_full, nrhs, seed, budget_s, reps):
+    """Time the CPU checker on the full-size solve when `reps` of them fit in
+    about budget_s (estimated from one run at a quarter of the order), else on the largest
+    n <= n_full (halving) that fits, flop-scaled and labelled so.  Returns
+    (seconds per full-size solve, reps timed, sample description)."""
+    n_probe = max(512, n_full // 4)
+    t_probe = cpu_solve(kind, n_probe, nrhs, seed)
+    est = t_probe * flops_of(kind, n_full, nrhs) / flops_of(kind, n_probe, nrhs)
+    reps = max(1, min(reps, int(budget_s / max(est, 1e-9))))
     n_s = n_full
     while n_s > 1024 and est * flops_of(kind, n_s, nrhs) / flops_of(kind, n_full, nrhs) * reps > budget_s:
         n_s //= 2
-    times = [cpu_oracle_solve(kind, n_s, nrhs, seed + 7 * i, threads) for i in range(reps)]
+    times = [cpu_solve(kind, n_s, nrhs, seed + 7 * i) for i in range(reps)]
     scale = flops_of(kind, n_s, nrhs) / flops_of(kind, n_full, nrhs)
     t_full = sum(times) / len(times) / scale
     what = "Cholesky + HPD solve" if kind != "lu" else "LU + solve"
-    return t_full, f"{reps} FP64 {what} runs at n={n_s}, {nrhs} RHS (flop-scaled to n={n_full})"
+    if n_s == n_full:
+        return t_full, reps, f"{reps} full-size FP64 {what} runs at n={n_full}, {nrhs} RHS"
+    return t_full, reps, f"{reps} FP64 {what} runs at n={n_s}, {nrhs} RHS (flop-scaled to n={n_full})"
 
 
-def reference_arm(args, ws, rank):
-    """CPU oracle timed on the host cores (the reference's own algorithm for
-    this path, restated in C; the reference itself needs MPI + BLAS and is not
-    built here).  For the mixed workload the reference has no mixed-precision
-    path: its FP64 Cholesky + HPD solve is the baseline."""
-    if rank != 0:
-        return
-    W = WORKLOADS[args.workload]
-    n, nrhs = W["n"], W["nrhs"]
+def reference_record(args, workload):
+    """The reference arm for one workload on the host cores: the reference's
+    own code (oracle/_ref) with OpenBLAS on every core, or the restatement
+    where the reference was not built.  The reference has no mixed-precision
+    path: for the mixed workload its FP64 Cholesky + HPD solve is the
+    baseline.  Each step is one full-size solve when `steps` of them fit in
+    about two minutes, else the run is cut to what fits (at least one step;
+    `steps` reports the number timed)."""
+    W = WORKLOADS[workload]
+    _, kind, what = cpu_checker()
     threads = os.cpu_count() or 1
-    if args.workload == "batched":
-        return reference_batched(args, W, threads)
-    if args.workload == "serve":
-        return reference_serve(args, W, threads)
-    for _ in range(max(args.warmup, 0)):
-        cpu_oracle_solve(args.workload, 512, nrhs, SEED, threads)
-    t_full, sample = cpu_sample(args.workload, n, nrhs, SEED, threads, 150.0, args.steps)
+    if workload == "batched":
+        return reference_batched(args, W, kind, what, threads)
+    if workload == "serve":
+        return reference_serve(args, W, kind, what, threads)
+    n, nrhs = W["n"], W["nrhs"]
+    cpu_solve(workload, 512, nrhs, SEED)  # warm-up: library load, thread pool
+    t_full, reps, sample = cpu_sample(workload, n, nrhs, SEED, 120.0, max(args.steps, 1))
     value = 1.0 / t_full
-    line = {
-        "metric": W["metric"], "value": value, "unit": "solves/s", "n_gpus": args.gpus, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": t_full * 1e3, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)", "impl": "reference",
-        "config": {"workload": W["desc"], "n": n, "nrhs": nrhs, "nb": NB, "parallelism": "host cores"},
-        "cpu_baseline": {"value": value, "unit": "solves/s", "cores": threads, "kind": "port", "sample": sample},
+    return {
+        "metric": W["metric"], "value": value, "unit": "solves/s", "n_gpus": args.gpus, "steps": reps,
+        "steps_requested": args.steps, "warmup": 1, "ms_per_step": t_full * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)", "impl": "reference",
+        "config": {"workload": W["desc"], "n": n, "nrhs": nrhs, "nb": NB, "parallelism": f"{threads} host cores"},
+        "cpu_baseline": {"value": value, "unit": "solves/s", "cores": threads, "kind": kind,
+                         "sample": sample + ", " + what},
         "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
-    print(json.dumps(line), flush=True)
 
 
-def reference_batched(args, W, threads):
-    """Oracle HPD solves and GaussianEliminations on systems drawn from the
-    batch (same sizes and right-hand-side counts), all host cores."""
+def reference_batched(args, W, kind, what, threads):
+    """The reference's HPD solves and GaussianEliminations (1 x 1 Grid form)
+    on systems drawn from the batch (same sizes and right-hand-side counts),
+    one after another, OpenBLAS on all host cores."""
     from elemental_b200 import inputs
-    from oracle import pyoracle as orc
-    orc.set_threads(threads)
+    M, _, _ = cpu_checker()
     sizes, rhs = batched_sets(SEED, W)
     r = np.random.default_rng(SEED + 5)
     per_step = 16
     times = []
-    for s in range(args.warmup + args.steps):
+    steps = max(1, min(args.steps, 10))
+    for s in range(1 + steps):
         idx = r.choice(W["count"], per_step, replace=False)
         mats = [(inputs.spd_ggt(sizes[0][i], int(i)), inputs.normal(sizes[0][i], rhs[0][i], int(i) + 1),
                  inputs.uniform(sizes[1][i], sizes[1][i], int(i) + 2), inputs.normal(sizes[1][i], rhs[1][i], int(i) + 3))
                 for i in idx]
         t0 = time.perf_counter()
         for Ah, Bh, Ag, Bg in mats:
-            orc.hpd_solve(Ah, Bh, orc.LOWER, nb=32)
-            orc.gaussian_elimination(Ag, Bg, nb=32)
-        if s >= args.warmup:
+            M.hpd_solve(Ah, Bh, 0, nb=NB)
+            M.gaussian_elimination(Ag, Bg, nb=NB)
+        if s >= 1:
             times.append(time.perf_counter() - t0)
     value = 2 * per_step * len(times) / sum(times)
-    line = {
-        "metric": W["metric"], "value": value, "unit": "solves/s", "n_gpus": args.gpus, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": 1e3 * 2 * W["count"] / value, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)", "impl": "reference",
-        "config": {"workload": W["desc"], "count_per_kind": W["count"], "parallelism": "host cores"},
-        "cpu_baseline": {"value": value, "unit": "solves/s", "cores": threads, "kind": "port",
-                         "sample": f"{per_step} HPD + {per_step} GE systems per step drawn from the batch"},
+    return {
+        "metric": W["metric"], "value": value, "unit": "solves/s", "n_gpus": args.gpus, "steps": len(times),
+        "steps_requested": args.steps, "warmup": 1, "ms_per_step": 1e3 * 2 * W["count"] / value,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+        "impl": "reference", "config": {"workload": W["desc"], "count_per_kind": W["count"],
+                                        "parallelism": f"{threads} host cores"},
+        "cpu_baseline": {"value": value, "unit": "solves/s", "cores": threads, "kind": kind,
+                         "sample": f"{per_step} HPD + {per_step} GE systems per step drawn from the batch, " + what},
         "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
-    print(json.dumps(line), flush=True)
 
 
-def reference_serve(args, W, threads):
-    """The oracle's FP64 rate on the served mix: Cholesky + solve and LU +
+def reference_serve(args, W, kind, what, threads):
+    """The reference's FP64 rate on the served mix: Cholesky + solve and LU +
     solve timed at n = 2048 on all host cores, applied to the stream's mean
     work per request (E[n^3] of the log-uniform size law, 50/50 kinds, mean
     32 RHS); requests served one after another."""
@@ -311,23 +334,21 @@ def reference_serve(args, W, threads):
     k = 0.5 * (W["rmin"] + W["rmax"])
     work = 0.5 * (en3 / 3.0 + 2.0 * en2 * k) + 0.5 * (2.0 * en3 / 3.0 + 2.0 * en2 * k)
     ns = 2048
-    for _ in range(max(args.warmup, 1)):
-        cpu_oracle_solve("chol", 512, 32, SEED, threads)
-    tc = cpu_oracle_solve("chol", ns, 32, SEED, threads)
-    tl = cpu_oracle_solve("lu", ns, 32, SEED, threads)
-    rate = (flops_chol_solve(ns, 32) + flops_lu_solve(ns, 32)) / (tc + tl)  # FP64 flop/s of the oracle
+    cpu_solve("chol", 512, 32, SEED)
+    tc = cpu_solve("chol", ns, 32, SEED)
+    tl = cpu_solve("lu", ns, 32, SEED)
+    rate = (flops_chol_solve(ns, 32) + flops_lu_solve(ns, 32)) / (tc + tl)  # FP64 flop/s on the host
     value = rate / work
-    line = {
+    return {
         "metric": W["metric"], "value": value, "unit": "solves/s", "n_gpus": args.gpus, "steps": 1,
-        "warmup": args.warmup, "ms_per_step": 1e3 / value, "higher_is_better": True, "scaling": "weak",
+        "warmup": 1, "ms_per_step": 1e3 / value, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)", "impl": "reference",
-        "config": {"workload": W["desc"], "parallelism": "host cores"},
-        "cpu_baseline": {"value": value, "unit": "solves/s", "cores": threads, "kind": "port",
-                         "sample": f"one Cholesky+solve and one LU+solve at n={ns}, 32 RHS; oracle flop rate "
+        "config": {"workload": W["desc"], "parallelism": f"{threads} host cores"},
+        "cpu_baseline": {"value": value, "unit": "solves/s", "cores": threads, "kind": kind,
+                         "sample": f"one Cholesky+solve and one LU+solve at n={ns}, 32 RHS ({what}); host flop rate "
                                    f"{rate / 1e9:.1f} GFLOP/s applied to the stream's mean work per request"},
         "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
-    print(json.dumps(line), flush=True)
 
 
 def timed(args, ws, dev, stream, h, step):
@@ -408,7 +429,7 @@ def pinned_like(a):
     return t
 
 
-def our_arm(args, ws, rank, local):
+def our_arm(args, ws, rank, local, kind):
     import torch
     import elemental_b200 as eg
 
@@ -417,7 +438,6 @@ def our_arm(args, ws, rank, local):
     h = eg.Handle(local)
     h.set_blocksize(NB)
     stream = torch.cuda.Stream(device=dev)
-    kind = args.workload
     W = WORKLOADS[kind]
     n, nrhs = W["n"], W["nrhs"]
     seed = SEED + 1000 * rank
@@ -499,10 +519,10 @@ def our_arm(args, ws, rank, local):
     roof = roofline_of(trace, "tc" if kind == "mixed" else "update", peaks, busy)
     cpu = None
     if ws == 1 and not args.no_cpu:
-        threads = os.cpu_count() or 1
-        t_full, sample = cpu_sample(kind, n, nrhs, seed, threads, 30.0, 1)
-        cpu = {"value": 1.0 / t_full, "unit": "solves/s", "cores": threads, "kind": "port",
-               "sample": sample + ", oracle in C with OpenMP"}
+        _, ckind, cwhat = cpu_checker()
+        t_full, _, sample = cpu_sample(kind, n, nrhs, seed, 30.0, 1)
+        cpu = {"value": 1.0 / t_full, "unit": "solves/s", "cores": os.cpu_count() or 1, "kind": ckind,
+               "sample": sample + ", " + cwhat}
     f_useful = flops_of(kind, n, nrhs)
     line = {
         "metric": W["metric"], "value": value, "unit": "solves/s", "n_gpus": ws, "steps": args.steps,
@@ -532,7 +552,7 @@ def our_arm(args, ws, rank, local):
         line["refinement"] = {"corrections": info["iters"], "berr": info["berr"], "tol": 1e-14}
         line["plain_fp64"] = plain
         line["speedup_vs_plain_fp64"] = value / plain["value"]
-    print(json.dumps(line), flush=True)
+    return line
 
 
 def batched_sets(seed, W):
@@ -690,9 +710,7 @@ def arm_batched(args, ws, rank, local):
     achieved = t["flops"] / (t["ms"] / 1e3) / 1e12 if t.get("ms") else None
     cpu = None
     if ws == 1 and not args.no_cpu:
-        from oracle import pyoracle as orc
-        threads = os.cpu_count() or 1
-        orc.set_threads(threads)
+        M, ckind, cwhat = cpu_checker()
         idx = r.choice(W["count"], 24, replace=False)
         mats = []
         for i in idx:
@@ -703,15 +721,16 @@ def arm_batched(args, ws, rank, local):
                 Ah_ = np.asfortranarray(a.cpu().numpy().reshape((arenas[k]["lds"][i], n), order="F")[:n])
                 Bh_ = np.asfortranarray(b.cpu().numpy().reshape((arenas[k]["lds"][i], rhs[k][i]), order="F")[:n])
                 mats.append((k, Ah_, Bh_))
+        M.hpd_solve(mats[0][1], mats[0][2], 0, nb=NB)  # warm-up
         t0 = time.perf_counter()
         for k, Ah_, Bh_ in mats:
             if k == 0:
-                orc.hpd_solve(Ah_, Bh_, orc.LOWER, nb=32)
+                M.hpd_solve(Ah_, Bh_, 0, nb=NB)
             else:
-                orc.gaussian_elimination(Ah_, Bh_, nb=32)
+                M.gaussian_elimination(Ah_, Bh_, nb=NB)
         dt = time.perf_counter() - t0
-        cpu = {"value": len(mats) / dt, "unit": "solves/s", "cores": threads, "kind": "port",
-               "sample": "24 HPD + 24 GE systems drawn from the batch, oracle in C with OpenMP"}
+        cpu = {"value": len(mats) / dt, "unit": "solves/s", "cores": os.cpu_count() or 1, "kind": ckind,
+               "sample": "24 HPD + 24 GE systems drawn from the batch, one after another, " + cwhat}
     line = {
         "metric": W["metric"], "value": value, "unit": "solves/s", "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -738,7 +757,7 @@ def arm_batched(args, ws, rank, local):
         "clocks": clocks,
         "cpu_baseline": cpu,
     }
-    print(json.dumps(line), flush=True)
+    return line
 
 
 def serve_stream(seed, W, device):
@@ -850,7 +869,11 @@ def arm_serve(args, ws, rank, local):
         "clocks": clocks,
         "cpu_baseline": None,
     }
-    print(json.dumps(line), flush=True)
+    if ws == 1 and not args.no_cpu:
+        _, ckind, cwhat = cpu_checker()
+        rec = reference_serve(args, W, ckind, cwhat, os.cpu_count() or 1)
+        line["cpu_baseline"] = rec["cpu_baseline"]
+    return line
 
 
 def kernel_case(args):
@@ -996,6 +1019,22 @@ def kernel_case(args):
     print(json.dumps({"case": args.case, "n": n, "ok": True}))
 
 
+NESTED = {"chol": "C1", "lu": "C2", "mixed": "C3", "batched": "C4", "serve": "C5"}
+NESTED_KEYS = ("metric", "value", "unit", "ms_per_step", "steps", "backward_error", "latency_ms", "roofline", "e2e",
+               "cpu_baseline", "plain_fp64", "speedup_vs_plain_fp64", "refinement", "kernels", "gpu_launches",
+               "clocks", "config", "impl", "steps_requested")
+
+
+def run_workload(args, ws, rank, local, workload):
+    if args.impl == "reference":
+        return reference_record(args, workload) if rank == 0 else None
+    if workload == "batched":
+        return arm_batched(args, ws, rank, local)
+    if workload == "serve":
+        return arm_serve(args, ws, rank, local)
+    return our_arm(args, ws, rank, local, workload)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -1003,7 +1042,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="mixed", choices=sorted(WORKLOADS), help="benchmark configuration")
-    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline leg")
+    ap.add_argument("--no-nested", action="store_true",
+                    help="time only --workload (by default the mixed line also carries the other configurations)")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline legs")
     ap.add_argument("--case", choices=["update", "gemm", "panel", "diag", "peaks", "mixed", "tc", "chol", "inverse",
                                        "hpdinverse", "trtri", "ldl", "revchol", "det"],
                     default=None,
@@ -1016,14 +1057,24 @@ def main():
         return
     ws, rank, local = dist_setup()
     try:
-        if args.impl == "reference":
-            reference_arm(args, ws, rank)
-        elif args.workload == "batched":
-            arm_batched(args, ws, rank, local)
-        elif args.workload == "serve":
-            arm_serve(args, ws, rank, local)
-        else:
-            our_arm(args, ws, rank, local)
+        if args.impl == "reference" and ws > 1 and rank != 0:
+            return  # the reference arm runs on rank 0 alone
+        line = run_workload(args, ws, rank, local, args.workload)
+        if args.workload == "mixed" and not args.no_nested:
+            # every other benchmark configuration, timed in the same run under
+            # the same rules, as nested records (the top-level line stays the
+            # mixed-precision headline)
+            line_cfgs = {}
+            for wl in ("chol", "lu", "batched", "serve"):
+                rec = run_workload(args, ws, rank, local, wl)
+                if rec is not None:
+                    line_cfgs[NESTED[wl] + "_" + wl] = {k: rec[k] for k in NESTED_KEYS if k in rec}
+            if line is not None:
+                line["configs"] = line_cfgs
+        if line is not None and rank == 0:
+            if args.workload == "mixed":
+                line["config"]["benchmark_config"] = "C3"
+            print(json.dumps(line), flush=True)
     finally:
         if ws > 1:
             import torch.distributed as dist

@@ -6,7 +6,7 @@
  * tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg load this
  * library, and only as the checker; the GPU product never calls it.
  *
- * Parity: unpinned (see oref_impl.h header).  Built by oracle/Makefile into
+ * Parity: pinned to the reference's own code (see oref_impl.h header).  Built by oracle/Makefile into
  * oracle/liboracle.so; exported names: oref_d* (double) and oref_s* (float).
  */
 #include <math.h>

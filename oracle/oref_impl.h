@@ -6,12 +6,20 @@
  * bench.py's cpu_baseline / reference arm as the checker.  Nothing in the
  * product (libelemgpu.so, the elem:: headers) links or calls it.
  *
- * Parity status: UNPINNED.  The reference ships no golden vectors or
- * known-answer tests for this path (its tests print residual norms from a
- * wall-clock-seeded drand48), and the reference itself cannot be built here
- * (it needs MPI, a BLAS/LAPACK and a CMake-generated config.h).  This file is
- * cross-checked instead against LAPACK (scipy's dpotrf/dgetrf) and against
- * exact constructions (A = L0 L0^T, P A = L0 U0) in tests/test_oracle.py.
+ * Parity status: PINNED to the reference's own code.  The reference ships no
+ * golden vectors or known-answer tests for this path (its tests print residual
+ * norms from a wall-clock-seeded drand48), so oracle/refbuild/Makefile compiles
+ * the reference's sources into oracle/_ref/libelemref.so (a single-process
+ * MPI, a hand-written config.h, the scipy wheel's OpenBLAS), and
+ * tests/test_oracle_ref.py checks this restatement against it on seeded
+ * inputs (pivots index for index, factors and solves to rounding) and against
+ * golden vectors it produced (tests/golden/ref_golden.npz).  Two recorded
+ * deviations: the reference's sequential RowEchelon crashes (its distributed
+ * form, which a 1 x 1 Grid runs, is what GaussianElimination restates), and
+ * its blocked ReverseLVar3/UVar3 does not factor A for n > Blocksize() (the
+ * restatement follows ReverseLVar3Unb, which it matches exactly for
+ * n <= Blocksize()).  tests/test_oracle.py also checks it against LAPACK and
+ * exact constructions.
  *
  * The level-3/level-2 arithmetic of the reference lives in whatever external
  * BLAS the build links (Elemental CMakeLists.txt:289-313; call sites

@@ -5,9 +5,9 @@ this module, and only as the checker.  Every routine mirrors an Elemental
 entry point (citations in oracle/oref_impl.h); matrices are numpy arrays in
 column-major (Fortran) order, indices are 0-based as in Elemental.
 
-Parity status: unpinned (the reference ships no golden vectors and cannot be
-built here); the oracle is cross-checked against LAPACK and exact
-constructions in tests/test_oracle.py.
+Parity status: pinned -- tests/test_oracle_ref.py checks every routine here
+against the reference's own code compiled from its sources (oracle/ref.py,
+oracle/_ref) and against the golden vectors it produced (tests/golden/).
 """
 from __future__ import annotations
 
