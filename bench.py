@@ -186,6 +186,27 @@ def max_over_ranks(ws, x, device):
     return float(t.item())
 
 
+def shard_of(ws, rank, sizes, kinds):
+    """The systems this rank owns when `ws` ranks share one list of
+    independent systems (egpu_partition_systems: largest first to the least
+    loaded rank, cost n^3/3 HPD, 2n^3/3 GE).  Every rank computes the same
+    partition; returns (owned indices in list order, per-rank loads)."""
+    import elemental_b200 as eg
+    owner, load = eg.partition_systems(sizes, kinds, ws)
+    return [i for i in range(len(sizes)) if owner[i] == rank], load
+
+
+def gather_to_host(ws, obj):
+    """Every rank's `obj` on every rank (host-side exchange of statuses and
+    results; the data path itself has no collective)."""
+    if ws == 1:
+        return [obj]
+    import torch.distributed as dist
+    out = [None] * ws
+    dist.all_gather_object(out, obj)
+    return out
+
+
 def make_inputs(kind, n, nrhs, seed, device=None):
     """Seeded inputs of a workload (numpy, column-major; the mixed workload's
     A is built on the GPU when ``device`` is given)."""
@@ -574,10 +595,17 @@ def arm_batched(args, ws, rank, local):
     dev = torch.device("cuda", local)
     W = WORKLOADS["batched"]
     h = eg.Handle(local)
-    seed = SEED + 1000 * rank
+    # one list of 2 x count systems shared by all ranks (multi-GPU: each rank
+    # factors the systems the partition gives it; no data-path collective)
+    seed = SEED
     sizes, rhs = batched_sets(seed, W)
+    mine, shard_load = shard_of(ws, rank, sizes[0] + sizes[1], [0] * W["count"] + [1] * W["count"])
+    own = [[i for i in mine if i < W["count"]], [i - W["count"] for i in mine if i >= W["count"]]]
+    sizes = [[sizes[k][i] for i in own[k]] for k in (0, 1)]
+    rhs = [[rhs[k][i] for i in own[k]] for k in (0, 1)]
+    cnt = [len(sizes[0]), len(sizes[1])]
     gen = torch.Generator(device=dev)
-    gen.manual_seed(seed)
+    gen.manual_seed(seed + rank)
     # one arena per kind for A and B (column-major, ld = n rounded up to even)
     arenas = []
     for kind in (0, 1):
@@ -632,8 +660,8 @@ def arm_batched(args, ws, rank, local):
         graph.replay()
 
     ms, trace, launches, clocks = timed(args, ws, dev, s0, h, step)
-    total = 2 * W["count"]
-    value = ws * total * args.steps / (ms / 1e3)
+    total = 2 * W["count"]  # the whole list, all ranks together
+    value = total * args.steps / (ms / 1e3)
     # one traced (uncaptured) run for the kernel's own time
     with torch.cuda.stream(s0):
         for k in (0, 1):
@@ -651,7 +679,7 @@ def arm_batched(args, ws, rank, local):
     r = np.random.default_rng(seed + 5)
     berr = 0.0
     for k in (0, 1):
-        for i in r.choice(W["count"], 32, replace=False):
+        for i in r.choice(cnt[k], min(32, cnt[k]), replace=False):
             a0 = torch.as_strided(arenas[k]["A0"], arenas[k]["vA"][i].shape, arenas[k]["vA"][i].stride(),
                                   arenas[k]["vA"][i].storage_offset())
             b0 = torch.as_strided(arenas[k]["B0"], arenas[k]["vB"][i].shape, arenas[k]["vB"][i].stride(),
@@ -662,7 +690,7 @@ def arm_batched(args, ws, rank, local):
     t_plain = 0.0
     with torch.cuda.stream(s0):
         for k in (0, 1):
-            idx = r.choice(W["count"], samp, replace=False)
+            idx = r.choice(cnt[k], min(samp, cnt[k]), replace=False)
             work = [(torch.as_strided(arenas[k]["A0"], arenas[k]["vA"][i].shape, arenas[k]["vA"][i].stride(),
                                       arenas[k]["vA"][i].storage_offset()).clone(),
                      arenas[k]["vB"][i].clone()) for i in idx]
@@ -677,7 +705,7 @@ def arm_batched(args, ws, rank, local):
                     h.gaussian_elimination(A_, B_)
             e1.record(s0)
             torch.cuda.synchronize()
-            t_plain += e0.elapsed_time(e1) / samp * W["count"]
+            t_plain += e0.elapsed_time(e1) / len(idx) * W["count"]
     plain_value = total / (t_plain / 1e3)
     # e2e: pinned host arenas in, both plans, solutions out, every step
     hostA = [arenas[k]["A0"].cpu().pin_memory() for k in (0, 1)]
@@ -698,7 +726,7 @@ def arm_batched(args, ws, rank, local):
             f1.synchronize()
             if i >= args.warmup:
                 e2e_ms.append(max_over_ranks(ws, f0.elapsed_time(f1), dev))
-    e2e_value = ws * total * len(e2e_ms) / (sum(e2e_ms) / 1e3)
+    e2e_value = total * len(e2e_ms) / (sum(e2e_ms) / 1e3)
     h2d = sum(int(hostA[k].numel() + hostB[k].numel()) * 8 for k in (0, 1))
     d2h = sum(int(outB[k].numel()) * 8 for k in (0, 1))
     for p_ in plans:
@@ -711,7 +739,7 @@ def arm_batched(args, ws, rank, local):
     cpu = None
     if ws == 1 and not args.no_cpu:
         M, ckind, cwhat = cpu_checker()
-        idx = r.choice(W["count"], 24, replace=False)
+        idx = r.choice(min(cnt), 24, replace=False)
         mats = []
         for i in idx:
             for k in (0, 1):
@@ -736,12 +764,14 @@ def arm_batched(args, ws, rank, local):
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded, generated on the device)",
         "config": {"workload": W["desc"], "count_per_kind": W["count"], "n_range": [W["nmin"], W["nmax"]],
-                   "rhs_range": [W["rmin"], W["rmax"]], "parallelism": "1 GPU" if ws == 1 else f"{ws} GPUs, own batch each",
+                   "rhs_range": [W["rmin"], W["rmax"]], "parallelism": "1 GPU" if ws == 1 else f"{ws} GPUs, one list sharded by egpu_partition_systems (greedy n^3 balance)",
                    "l2": f"arenas ({sum(int(a['A'].numel()) for a in arenas) * 8 >> 20} MiB) larger than L2",
                    "step_includes": "device refill of every matrix and right-hand side, both batched launches"},
         "equiv_fp64_tflops": flops / (ms / args.steps / 1e3) / 1e12,
         "backward_error": berr,
         "autotuned_grid": {"hpd": tuned[0][1], "ge": tuned[1][1]},
+        "shard": {"systems_per_rank": cnt, "load_balance": float(max(shard_load) / (sum(shard_load) / ws))}
+        if ws > 1 else None,
         "plain_fp64": {"value": plain_value, "unit": "solves/s",
                        "api": "egpu_dposv / egpu_dgesv, one call per system (sampled, 128 per kind)"},
         "speedup_vs_plain_fp64": value / plain_value,
@@ -984,6 +1014,34 @@ def kernel_case(args):
         print(json.dumps({"case": "tc", "n": n, "ms_per_launch": ms, "c_gbs": cbytes / ms / 1e6,
                           "tf32_tflops": 3 * 2.0 * n * (n + 1) / 2 * NB / ms / 1e9}))
         return
+    elif args.case == "sweep32":
+        # the mixed solver's FP32 super-block sweeps alone at order n, 32 RHS:
+        # one forward + backward launch, three timed repetitions (the trace
+        # separates the super-block inverses ("other") from the sweeps)
+        A = torch.randn(n, n, dtype=torch.float64, device="cuda")
+        A = A @ A.T + n * torch.eye(n, dtype=torch.float64, device="cuda")
+        L = torch.linalg.cholesky(A)
+        del A
+        ld = (n + 31) // 32 * 32
+        store = torch.zeros((n, ld), dtype=torch.float32, device="cuda")
+        L32 = torch.as_strided(store, (n, n), (1, ld))
+        L32.copy_(L.float())
+        del L
+        X = eg.colmajor_cuda(torch.randn(n, 32, dtype=torch.float64, device="cuda"))
+        h.sweep32_solve(L32, X, 2)  # warm-up
+        torch.cuda.synchronize()
+        h.trace_enable(True)
+        for _ in range(3):
+            h.sweep32_solve(L32, X, 2)  # forward + backward, one launch
+        torch.cuda.synchronize()
+        s = h.trace_summary()
+        h.trace_enable(False)
+        sw = s["solve"]
+        ms = sw["busy_ms"] / sw["launches"]
+        print(json.dumps({"case": "sweep32", "n": n, "nrhs": 32, "ms_per_solve": ms, "ms_per_sweep": ms / 2,
+                          "triangle_gbs": 2 * 2.0 * n * n / ms / 1e6,
+                          "prepare_ms": s["other"]["busy_ms"] / max(1, s["other"]["launches"])}))
+        return
     elif args.case in ("inverse", "hpdinverse", "trtri", "ldl", "revchol", "det"):
         # the next rows (inverses, determinants, LDL, ReverseCholesky) at order
         # n: one warm-up call, then three timed calls on fresh copies of A
@@ -1046,7 +1104,7 @@ def main():
                     help="time only --workload (by default the mixed line also carries the other configurations)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline legs")
     ap.add_argument("--case", choices=["update", "gemm", "panel", "diag", "peaks", "mixed", "tc", "chol", "inverse",
-                                       "hpdinverse", "trtri", "ldl", "revchol", "det"],
+                                       "hpdinverse", "trtri", "ldl", "revchol", "det", "sweep32"],
                     default=None,
                     help="run one launch of one kernel class (profiling)")
     ap.add_argument("--n", type=int, default=6144, help="size for --case")

@@ -100,6 +100,8 @@ def _declare(L):
         "egpu_trace_enable": ([H, I], I),
         "egpu_trace_summary": ([H, I, P, P, P, P], I),
         "egpu_trace_busy": ([H, I, P, P], I),
+        "egpu_partition_systems": ([I, P, P, I, P, P], I),
+        "egpu_sweep32_solve": ([H, I, I, I, P, I, P, I], I),
         "egpu_trace_events": ([H, I, P, P, P, P], I),
         "egpu_dpotrf": ([H, I, I, P, I, P], I),
         "egpu_dpotrs": ([H, I, I, I, I, P, I, P, I], I),
@@ -234,6 +236,20 @@ def _device_vec(t, count: int, dtype: str, device: int):
     if not t.is_contiguous() or t.numel() < count:
         raise ValueError(f"expected a contiguous vector of at least {count} elements, got shape {tuple(t.shape)}")
     return ctypes.c_void_p(t.data_ptr())
+
+
+def partition_systems(n, kind, parts: int):
+    """Owner part of each independent system (egpu_partition_systems): the
+    systems are dealt largest first (cost n^3/3 HPD, 2n^3/3 GE) to the least
+    loaded of `parts` parts.  Returns (owner int32 array, per-part load)."""
+    n = np.ascontiguousarray(n, dtype=np.int32)
+    k = None if kind is None else np.ascontiguousarray(kind, dtype=np.int32)
+    owner = np.zeros(max(len(n), 1), dtype=np.int32)
+    load = np.zeros(parts, dtype=np.float64)
+    _check(lib().egpu_partition_systems(len(n), n.ctypes.data_as(ctypes.c_void_p),
+                                        None if k is None else k.ctypes.data_as(ctypes.c_void_p), int(parts),
+                                        owner.ctypes.data_as(ctypes.c_void_p), load.ctypes.data_as(ctypes.c_void_p)))
+    return owner[:len(n)], load
 
 
 def _np_f(a: np.ndarray):
@@ -717,6 +733,16 @@ class Handle:
     def mixed_gmres_iterations(self):
         """GMRES iterations of the last mixed solve (0 when plain refinement converged)."""
         return lib().egpu_mixed_gmres_iterations(self._h)
+
+    def sweep32_solve(self, L32, X, trans=0):
+        """X := L^-1 X (trans 0), L^-T X (trans 1) or L^-T L^-1 X (trans 2) by the mixed solver's FP32
+        super-block sweep (L: lower-triangular float32 CUDA tensor,
+        column-major; X: float64, n x nrhs with nrhs <= 64)."""
+        self._bind_stream()
+        n = L32.shape[0]
+        nrhs = X.shape[1] if X.dim() > 1 else 1
+        ldl = L32.stride(1) if L32.dim() == 2 else max(n, 1)
+        _check(lib().egpu_sweep32_solve(self._h, trans, n, nrhs, _ptr(L32), ldl, _ptr(X), _ld(X)))
 
     def tc_gemm_split(self, A, B, C, alpha=1.0, beta=0.0, lower=False, terms=3):
         """C (float32, column-major) = alpha A B^T + beta C on the tcgen05 tensor cores

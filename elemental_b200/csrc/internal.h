@@ -77,6 +77,18 @@ int launch_trsm_skinny(cudaStream_t st, int bwd, int amode, int n, int nrhs, con
 int launch_dgemm_skinny(cudaStream_t st, int M, int N, int K, double alpha, const double* A, long long lda,
                         const double* B, long long ldb, double* C, long long ldc, int sm_count, DevStatus* status);
 
+// FP32 super-block sweeps (sweep32.cu), the correction solves of the mixed
+// refinement: sweep32_prepare builds the inverses of the 512 x 512 diagonal
+// super-blocks of the lower factor L (FP32, ld ldl) from the 128 x 128 panel
+// inverses Winv (FP64, nb = 128); sweep32_solve then applies X := L^-1 X
+// (trans 0), L^-T X (trans 1) or L^-T L^-1 X (trans 2) to X (FP64, n x nrhs)
+// in one cooperative launch.  ws: sweep32_ws_bytes(n, nrhs) bytes, 256-byte
+// aligned.
+size_t sweep32_ws_bytes(int n, int nrhs);
+int sweep32_prepare(cudaStream_t st, int n, const float* L, long long ldl, const double* Winv, void* ws);
+int sweep32_solve(cudaStream_t st, int trans, int n, int nrhs, const float* L, long long ldl, double* X,
+                  long long ldx, void* ws, int sm_count, DevStatus* status);
+
 // Diagonal-block Cholesky (factor in place + triangular inverse into W).
 int launch_potrf_diag(cudaStream_t st, int uplo, double* A, long long lda, int b, double* W, int ldw,
                       DevStatus* status, int col_base, bool store_factor = true);

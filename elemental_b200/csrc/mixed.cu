@@ -190,7 +190,7 @@ constexpr int kGmresRestart = 20;  // Krylov vectors per GMRES cycle
 
 // Workspace layout of the mixed solve.
 struct MixedLayout {
-  size_t as, af, lf, pkh, pkl, wsh, wsl, xw, r, yt, winv, norms, flags, gv, gw, gc, total;
+  size_t as, af, lf, pkh, pkl, wsh, wsl, xw, r, yt, winv, norms, flags, gv, gw, gc, sw, total;
   long long lds, ldf, ldk;
 };
 
@@ -217,6 +217,7 @@ static MixedLayout mixed_layout(int n, int nrhs, int nb) {
   L.gv = take(sizeof(double) * L.lds * std::max(nrhs, 1) * (kGmresRestart + 1));  // GMRES basis
   L.gw = take(sizeof(double) * L.lds * std::max(nrhs, 1));                        // GMRES work vector
   L.gc = take(sizeof(double) * (size_t)std::max(nrhs, 1) * (kGmresRestart + 2));  // coefficients
+  L.sw = take(sweep32_ws_bytes(n, nrhs));  // FP32 sweeps: super-block inverses, work vectors
   L.total = (off + 4095) & ~size_t(4095);
   return L;
 }
@@ -231,9 +232,13 @@ struct SweepFlags {
   int epoch;
   bool prescaled;
   double* Y;
+  const float* Lf32;  // non-null: the FP32 super-block sweeps over this factor
+  long long ldf;
+  void* sw;           // their workspace (super-block inverses prepared)
 };
 static int mixed_solve(egpu_context* h, int n, int nrhs, const double* Lf, long long lds, const double* Winv,
                        double* X, SweepFlags& fl) {
+  if (fl.Lf32) return sweep32_solve(h->stream, 2, n, nrhs, fl.Lf32, fl.ldf, X, lds, fl.sw, h->sm_count, h->dstatus);
   if (fl.prescaled) {
     TRY(launch_trsm_skinny(h->stream, 0, 0, n, nrhs, Lf, lds, Winv, h->nb, X, lds, fl.flags, ++fl.epoch,
                            h->sm_count, h->dstatus, fl.Y));
@@ -428,7 +433,13 @@ int dposv_mixed_core_impl(egpu_context* h, int uplo, int n, int nrhs, const doub
   double* norms = reinterpret_cast<double*>(ws + L.norms);
   // prescaled sweeps where the one-launch sweep kernel takes the shape
   const bool prescale = nrhs <= 64 && nb >= 8 && nb <= 128 && nb % 2 == 0;
-  SweepFlags fl{reinterpret_cast<int*>(ws + L.flags), 0, prescale, reinterpret_cast<double*>(ws + L.yt)};
+  SweepFlags fl{reinterpret_cast<int*>(ws + L.flags), 0, prescale, reinterpret_cast<double*>(ws + L.yt), nullptr,
+                0, ws + L.sw};
+  // the FP32 super-block sweeps take the corrections when the panels are 128
+  // wide and the FP32 factor is TMA-addressable; the FP64 copy of L (and its
+  // prescaled M2 form) is then only built if GMRES-IR needs it
+  const bool use32 = nb == 128 && nrhs <= 64 && L.ldf % 4 == 0;
+  bool have_lf = false;  // Lf holds the FP64 copy (prescaled when `prescale`)
   EGPU_CUDA_TRY(cudaMemsetAsync(fl.flags, 0, trsm_skinny_flag_bytes(n, nb), st));
   const long long lds = L.lds, ldf = L.ldf;
   // The factorization: the fast form computes every panel's L21 on the
@@ -532,7 +543,7 @@ int dposv_mixed_core_impl(egpu_context* h, int uplo, int n, int nrhs, const doub
         TRY(launch_tc_gemm(st, m3, m3, b, -1.0f, PKh2[par] + (size_t)b2 * L.ldk, PKl2[par] + (size_t)b2 * L.ldk,
                            PKh2[par] + (size_t)b2 * L.ldk, PKl2[par] + (size_t)b2 * L.ldk, L.ldk, 1.0f,
                            A22 + b2 + (long long)b2 * ldf, ldf, 1, 3, h->dstatus));
-      TRY(l21_copy(k, par));
+      if (accurate || !use32) TRY(l21_copy(k, par));
     }
     EGPU_CUDA_TRY(cudaEventRecord(h->ev_join, sd));
     EGPU_CUDA_TRY(cudaStreamWaitEvent(st, h->ev_join, 0));
@@ -541,9 +552,39 @@ int dposv_mixed_core_impl(egpu_context* h, int uplo, int n, int nrhs, const doub
 
     return read_status_now(h, nullptr);
   };
+  bool accurate = false;
   int frc = factor(false);
-  if (frc == EGPU_NOT_HPD) frc = factor(true);
+  if (frc == EGPU_NOT_HPD) {
+    accurate = true;
+    frc = factor(true);
+  }
   TRY(frc);  // the status word (pivot column) stays readable by the caller
+  if (use32 && !accurate) {  // L in the FP32 working matrix: super-block inverses
+    TRY(sweep32_prepare(st, n, Af, ldf, Winv, fl.sw));
+    fl.Lf32 = Af;
+    fl.ldf = ldf;
+  } else {
+    have_lf = true;
+  }
+  // The FP64 copy of L (M2 when prescaled) on demand, for GMRES-IR: widen the
+  // FP32 factor's panels and prescale them (the same work the factorization
+  // does on its auxiliary stream when the FP32 sweeps are not used).
+  auto materialize_lf = [&]() -> int {
+    if (have_lf) return EGPU_OK;
+    for (int k = 0; k + nb < n; k += nb) {
+      const int b = std::min(nb, n - k), m2 = n - k - b;
+      TraceMark tm(st, kTraceOther, 0.0, 12.0 * m2 * b);
+      dim3 grid((m2 + 255) / 256, b);
+      widen_panel_kernel<<<grid, 256, 0, st>>>(m2, b, Af + (k + b) + (long long)k * ldf, ldf,
+                                               Lf + (k + b) + (long long)k * lds, lds);
+      count_launch();
+      EGPU_CUDA_TRY(cudaGetLastError());
+      if (prescale) TRY(mixed_prescale_step(h, st, n, k, Lf, lds, Winv));
+    }
+    have_lf = true;
+    fl.Lf32 = nullptr;
+    return EGPU_OK;
+  };
   // ---- refinement
   {
     rowsum_abs_kernel<<<(n + 7) / 8, 256, 0, st>>>(n, As, lds, norms);
@@ -582,6 +623,7 @@ int dposv_mixed_core_impl(egpu_context* h, int uplo, int n, int nrhs, const doub
   // GMRES-IR when plain refinement contracts slowly (the factor is good enough
   // to precondition but too far from A to contract): R holds the residual of Xw
   if (e > tol && std::isfinite(e) && it < max_iter) {
+    TRY(materialize_lf());
     GmresWork gw{reinterpret_cast<double*>(ws + L.gv), reinterpret_cast<double*>(ws + L.gw),
                  reinterpret_cast<double*>(ws + L.gc), reinterpret_cast<double*>(ws + L.gc) + nrhs};
     int inner = 0;

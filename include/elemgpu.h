@@ -256,6 +256,14 @@ EGPU_API int egpu_host_dposv_mixed(egpu_handle h, int uplo, int n, int nrhs, con
 EGPU_API int egpu_tc_gemm_split(egpu_handle h, int M, int N, int K, double alpha, const double* dA, int lda,
                                 const double* dB, int ldb, double beta, float* dC, int ldc, int lower, int terms);
 
+/* The FP32 correction sweep of egpu_dposv_mixed, for tests and profiling (no
+ * counterpart in the reference): X := L^-1 X (trans 0), L^-T X (trans 1) or
+ * L^-T L^-1 X (trans 2, one launch) with L lower triangular, FP32, column-major (16-byte aligned, ldl a
+ * multiple of 4), through 512 x 512 super-block inverses built from L's 128 x
+ * 128 diagonal-block inverses; X FP64, nrhs <= 64.  Synchronous. */
+EGPU_API int egpu_sweep32_solve(egpu_handle h, int trans, int n, int nrhs, const float* dL, int ldl, double* dX,
+                                int ldx);
+
 /* Batched HPDSolve(LOWER, NORMAL, A_i, B_i) (HPDSolve.hpp:18-28) for `count`
  * independent systems of uneven orders n[i] <= 512 with nrhs[i] <= 16, in one
  * persistent launch (one CTA per system at a time, largest first).  n, nrhs,
@@ -264,6 +272,15 @@ EGPU_API int egpu_tc_gemm_split(egpu_handle h, int M, int N, int K, double alpha
  * numerically HPD (that system's B_i is left unsolved).  Synchronous. */
 EGPU_API int egpu_dposv_batched(egpu_handle h, int count, const int* n, const int* nrhs, double* const* dA,
                                 const int* lda, double* const* dB, const int* ldb, int* info);
+
+/* Sharding of independent systems across GPUs (no counterpart in the
+ * reference, which distributes one matrix over a process grid instead): owner[i]
+ * in [0, parts) for each of `count` systems of order n[i] (kind[i] 0 = HPD
+ * solve, cost n^3 / 3; 1 = GaussianElimination, cost 2 n^3 / 3; kind NULL =
+ * all HPD), dealt largest first to the least-loaded part.  Deterministic, so
+ * every rank computes the same partition; load (optional, `parts` doubles)
+ * receives each part's summed cost.  Host-only: no device is touched. */
+EGPU_API int egpu_partition_systems(int count, const int* n, const int* kind, int parts, int* owner, double* load);
 
 /* Batched GaussianElimination(A_i, B_i) (GaussianElimination.hpp:216-232) for
  * `count` independent systems, n[i] <= 512, nrhs[i] <= 16, one persistent

@@ -139,3 +139,32 @@ def test_hpd_solve_mixed_config_n16384_kappa1e6(handle):
     del A2
     rel = float((X - X2).abs().max() / X2.abs().max())
     assert rel <= kappa * 1e-13, rel
+
+
+@pytest.mark.parametrize("n", [1, 100, 511, 512, 513, 1000, 2049, 4100])
+@pytest.mark.parametrize("nrhs", [1, 7, 32, 33, 64])
+@pytest.mark.parametrize("trans", [0, 1, 2])
+def test_sweep32_solve_matches_fp64_triangular_solve(handle, n, nrhs, trans):
+    # the FP32 super-block sweep (egpu_sweep32_solve) against an FP64
+    # triangular solve of the same FP32 factor: the Cholesky factor of a
+    # well-conditioned HPD matrix, so the FP32 solve is accurate to ~1e-6
+    if n > 1000 and nrhs not in (32, 64):
+        pytest.skip("large orders with the bench's right-hand-side counts only")
+    A = torch.from_numpy(inputs.spd_ggt(n, 90 + n)).cuda()
+    L = torch.linalg.cholesky(A)
+    ld = (n + 31) // 32 * 32
+    store = torch.zeros((n, ld), dtype=torch.float32, device="cuda")
+    L32 = torch.as_strided(store, (n, n), (1, ld))  # column-major, ld a multiple of 32
+    L32.copy_(L.float())
+    Bh = inputs.normal(n, nrhs, 91)
+    B = torch.from_numpy(Bh).cuda()
+    X = eg.colmajor_cuda(Bh)  # column-major FP64
+    handle.sweep32_solve(L32, X, trans)
+    torch.cuda.synchronize()
+    L64 = L32.double().tril()
+    if trans == 2:
+        ref = torch.linalg.solve_triangular(L64.t(), torch.linalg.solve_triangular(L64, B, upper=False), upper=True)
+    else:
+        ref = torch.linalg.solve_triangular(L64.t() if trans else L64, B, upper=bool(trans))
+    err = float((X - ref).abs().max() / ref.abs().max())
+    assert err <= 2e-5, err
