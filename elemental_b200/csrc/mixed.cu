@@ -438,7 +438,7 @@ int dposv_mixed_core_impl(egpu_context* h, int uplo, int n, int nrhs, const doub
   // the FP32 super-block sweeps take the corrections when the panels are 128
   // wide and the FP32 factor is TMA-addressable; the FP64 copy of L (and its
   // prescaled M2 form) is then only built if GMRES-IR needs it
-  const bool use32 = nb == 128 && nrhs <= 64 && L.ldf % 4 == 0;
+  const bool use32 = nb == 128 && nrhs <= 32 && L.ldf % 4 == 0;
   bool have_lf = false;  // Lf holds the FP64 copy (prescaled when `prescale`)
   EGPU_CUDA_TRY(cudaMemsetAsync(fl.flags, 0, trsm_skinny_flag_bytes(n, nb), st));
   const long long lds = L.lds, ldf = L.ldf;

@@ -1,29 +1,37 @@
 // FP32 triangular sweeps for the correction solves of the mixed-precision
-// refinement: X := L^-1 X (forward) or X := L^-T X (backward) with L the
-// low-precision Cholesky factor (FP32, lower triangle of the working matrix).
+// refinement: X := L^-1 X (forward), L^-T X (backward) or L^-T L^-1 X with L
+// the low-precision Cholesky factor (FP32, lower triangle of the working
+// matrix).
 //
 // The refinement's residual is FP64 and its corrections only need the
 // accuracy of the factor itself (FP32), so the sweeps read L in FP32 and
 // compute in FP32 (half the bytes of an FP64 copy, twice the SIMT rate).  The
 // dependency chain of a triangular solve is cut to n / S steps by explicit
 // inverses of the S x S diagonal super-blocks (S = 4 panels = 512):
-//   forward, super-block R:  y_R = W_R z_R              (phase A)
-//                            z_i -= L_iR y_R, i > R      (phase B)
-//   backward, R downwards:   x_R = W_R^T v_R            (phase A)
-//                            v_j -= L_Rj^T x_R, j < R    (phase B)
-// One cooperative launch runs all super-steps with two bounded grid
-// barriers each.  Phase A spreads the rows of W_R over the grid (a warp per
-// row, W_R's rows read contiguously from the copy laid out for the
-// direction); phase B deals 128-row (forward) or 128-column (backward) tiles
-// of L out to the CTAs, each streaming its 128 x 512 block of L through a
-// TMA ring (32 columns or rows per stage) against y_R / x_R held in shared
-// memory, 4 x 4 register tiles per thread.
+//   forward, super-block R:  y_R = W_R (z0_R + dz_R)          (phase A)
+//                            dz_Q -= L_QR y_R, Q > R          (phase B)
+//   backward, R downwards:   x_R = W_R^T (v_R + dv_R)          (phase A)
+//                            dv_Q -= L_RQ^T x_R, Q < R        (phase B)
+// Every piece of work is a tile item -- out(128 x 32) += T(128 x k) v(k x 32)
+// with T a 128-row tile of W_R or of L read through TMA -- and one
+// cooperative launch works through a queue of items in an order that
+// respects their dependencies (phase A of R, then the phase-B items of R
+// that feed R + 1, then the rest of R's phase B, then phase A of R + 1, ...).
+// CTAs take items from an atomic counter, start the item's TMA tile loads at
+// once, then wait (bounded) only for the counters of the items it depends on:
+// phase A of Q waits for all phase-B items that target Q, phase B of R for the
+// phase-A items of R.  No grid barrier separates the steps, so the serial
+// chain is the true dependency chain and the bulk of phase B overlaps it.
+// All results are accumulated with FP32 vector reductions into arrays zeroed
+// at the start.
 //
 // The super-block inverses are built once per factorization from the 128 x
 // 128 diagonal-block inverses W_k (FP64, from the diagonal kernels) and the
 // off-diagonal blocks of L: X_kk = W_k, X_ij = -W_i sum_{k=j}^{i-1} L_ik X_kj
 // (block rows i = 1..3 of each super-block, one launch per i, all
 // super-blocks at once).
+#include <vector>
+
 #include "context.h"
 
 namespace egpu {
@@ -32,29 +40,48 @@ namespace {
 
 constexpr int kS = 512;          // super-block order
 constexpr int kPB = 128;         // panel (block) order inside a super-block
-constexpr int kTM = 128;         // phase-B tile: rows (forward) / columns (backward)
+constexpr int kTM = 128;         // tile: rows (M-contiguous) or columns (K-contiguous) of T
 constexpr int kTK = 32;          // k per TMA stage
 constexpr int kStages = 4;
 constexpr int kThreads = 256;
-constexpr int kRhs = 32;         // right-hand sides per pass
+constexpr int kRhs = 32;         // right-hand sides (nrhs <= 32 per launch)
 
 // shared-memory carve (floats), 1024-byte aligned pieces
-constexpr int kStageFloats = kTM * kTK;                 // 4096 floats = 16 KB
+constexpr int kStageFloats = kTM * kTK;                     // 4096 floats = 16 KB
 constexpr int kOffStages = 0;
-constexpr int kOffY = kOffStages + kStages * kStageFloats;  // kS x kRhs floats = 64 KB
-constexpr int kSmemFloats = kOffY + kS * kRhs;
-constexpr int kSmemBytes = kSmemFloats * 4 + 1024 + 64;  // + alignment slack + mbarriers
+constexpr int kOffV = kOffStages + kStages * kStageFloats;  // kS x kRhs floats = 64 KB
+constexpr int kSmemFloats = kOffV + kS * kRhs;
+constexpr int kSmemBytes = kSmemFloats * 4 + 1024 + 128;  // + alignment slack + mbarriers / scalars
 
-struct Sweep32Params {
-  int n, nrhs, trans, nsuper;
-  const float* Wc;   // W_R column-major (S x S per super-block, stride S*S)
-  const float* Wr;   // W_R row-major
-  float* Z;          // n x ldz row-major work (right-hand sides contiguous)
-  int ldz;
-  float* Yb;         // S x ldz row-major: y_R / x_R of the current super-block
-  double* X;         // in: right-hand side, out: solution (FP64, column-major)
+// An item: out[out_row .. +128) (+/-)= T[tile] * v[v_row + kbeg .. v_row + kend)
+struct Item {
+  short map;      // 0 L (rows contiguous), 1 L (columns), 2 W (rows contiguous), 3 W (columns)
+  short dir;      // 0 forward arrays, 1 backward arrays
+  short kind;     // 0 phase A (out: y/x of super-block, +), 1 phase B (out: deltas, -)
+  short nk;       // TMA stages
+  int tm;         // tile coordinate along M (row of T, or column of T for maps 1/3)
+  int tk;         // coordinate of k = kbeg along K in the tensor
+  int vrow;       // first row of v for k = kbeg
+  int orow;       // first output row
+  int orows;      // output rows valid (from orow)
+  int dep0, need0;  // counter index and the count it must reach
+  int dep1, need1;  // second dependency (or -1)
+  int done;       // counter incremented on completion
+};
+
+struct SweepDF {
+  int n, nrhs, items;
+  const Item* table;
+  float* Z0;   // n x 32: the right-hand side (X converted)
+  float* Df;   // forward deltas
+  float* Yf;   // forward results y
+  float* Db;   // backward deltas
+  float* Yb;   // backward results x
+  double* X;   // in / out, FP64 column-major
   long long ldx;
-  unsigned* counter; // grid barrier counter, zero at launch
+  int out_backward;  // X := Yb (else Yf)
+  int* counters;     // [0] queue, [1] abort, [2...] item counters; zeroed before launch
+  unsigned* bar;     // grid barrier counter, zeroed before launch
   DevStatus* status;
 };
 
@@ -62,249 +89,198 @@ __device__ __forceinline__ float* align1024(float* p) {
   return reinterpret_cast<float*>((reinterpret_cast<uintptr_t>(p) + 1023) & ~uintptr_t(1023));
 }
 
-// Phase A: rows of the current super-block, a warp per row.  out = Wrow * zs
-// over k in [klo, khi); zs = the super-block's right-hand sides (sb x 32).
-// The row's W values are loaded first (up to 16 per lane, all in flight at
-// once), then broadcast with shuffles.  Results go to Yb (and to X when
-// write_x).
-__device__ void phase_a(const Sweep32Params& p, const float* Wrow_base, bool lower_rows, int r0, int sb, int pass,
-                        const float* zs, bool write_x) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int gw = blockIdx.x * (kThreads / 32) + warp, nw = gridDim.x * (kThreads / 32);
-  const int c = pass * kRhs + lane;
-  for (int i = gw; i < sb; i += nw) {
-    // forward: W_R row i, k = 0..i (W_R lower); backward: W_R^T row i = W_R
-    // column i, k = i..sb-1
-    const int klo = lower_rows ? 0 : i, khi = lower_rows ? i + 1 : sb;
-    const float* w = Wrow_base + (size_t)i * kS;
-    float wl[kS / 32];
-#pragma unroll
-    for (int q = 0; q < kS / 32; ++q) {
-      const int k = q * 32 + lane;
-      wl[q] = (k >= klo && k < khi) ? w[k] : 0.f;
-    }
-    float acc = 0.f, acc2 = 0.f;  // two chains: even and odd k
-#pragma unroll
-    for (int q = 0; q < kS / 32; ++q) {
-      if (q * 32 >= khi || q * 32 + 32 <= klo) continue;
-#pragma unroll
-      for (int t = 0; t < 32; t += 2) {
-        acc = fmaf(__shfl_sync(0xffffffffu, wl[q], t), zs[(q * 32 + t) * kRhs + lane], acc);
-        acc2 = fmaf(__shfl_sync(0xffffffffu, wl[q], t + 1), zs[(q * 32 + t + 1) * kRhs + lane], acc2);
-      }
-    }
-    acc += acc2;
-    p.Yb[(size_t)i * p.ldz + c] = acc;
-    if (write_x && c < p.nrhs) p.X[(r0 + i) + (long long)c * p.ldx] = (double)acc;
+// Bounded wait until *c >= need (thread 0).  false: timed out or aborted.
+__device__ bool wait_counter(const int* c, int need, const int* abort) {
+  for (long long it = 0; it < kSpinLimit; ++it) {
+    int v;
+    asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(c) : "memory");
+    if (v >= need) return true;
+    int a;
+    asm volatile("ld.relaxed.gpu.global.s32 %0, [%1];" : "=r"(a) : "l"(abort) : "memory");
+    if (a) return false;
+    if (it > 16) __nanosleep(32);
   }
+  return false;
 }
 
-// Stage rows [0, rows) x 32 columns (pass) of a row-major array into smem
-// (rows beyond `rows` up to kS are zero).
-__device__ void stage_rows(float* dst, const float* src, int ldz, int rows, int pass) {
-  for (int e = threadIdx.x; e < kS * (kRhs / 4); e += kThreads) {
-    const int r = e / (kRhs / 4), q = e % (kRhs / 4);
-    float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-    if (r < rows) v = __ldcg(reinterpret_cast<const float4*>(src + (size_t)r * ldz + pass * kRhs) + q);
-    reinterpret_cast<float4*>(dst + r * kRhs)[q] = v;
-  }
-}
-
-// The phase-B work items of one super-step: tiles of 128 rows (forward) or
-// columns (backward) of the trailing part, each tile's k range split into
-// `ksplit` parts when there are few tiles.
-struct BItems {
-  int lo, hi, ntiles, ksplit, kchunk, items;
-};
-__device__ __forceinline__ BItems b_items(int fwd, int n, int r0, int r1, int G) {
-  BItems b;
-  b.lo = fwd ? r1 : 0;
-  b.hi = fwd ? n : r0;
-  b.ntiles = b.hi > b.lo ? (b.hi - b.lo + kTM - 1) / kTM : 0;
-  b.ksplit = 1;
-  while (b.ksplit < 4 && b.ntiles * b.ksplit * 2 <= G) b.ksplit *= 2;
-  b.kchunk = kS / b.ksplit;
-  b.items = b.ntiles * b.ksplit;
-  return b;
-}
-
-// Issue the TMA loads of k-stage `kn` of an item into ring slot `s`.
-__device__ __forceinline__ void issue_stage(const CUtensorMap* mapF, const CUtensorMap* mapB, int fwd, float* stages,
-                                            uint64_t* full, int s, int m0, int kglob) {
+__device__ __forceinline__ void issue(const CUtensorMap* map, bool mcontig, float* stages, uint64_t* full, int s,
+                                      int tm, int kc) {
   mbar_expect_tx(&full[s], kStageFloats * 4);
-  if (fwd) {
+  if (mcontig) {  // M-contiguous: 4 boxes of {32 rows, 32 k}
     for (int b = 0; b < kTM / 32; ++b)
-      tma_load_2d(stages + s * kStageFloats + b * 32 * kTK, mapF, &full[s], m0 + 32 * b, kglob);
-  } else {
-    tma_load_2d(stages + s * kStageFloats, mapB, &full[s], kglob, m0);
+      tma_load_2d(stages + s * kStageFloats + b * 32 * kTK, map, &full[s], tm + 32 * b, kc);
+  } else {  // K-contiguous: one box {32 k, 128 columns}, 128-byte swizzle
+    tma_load_2d(stages + s * kStageFloats, map, &full[s], kc, tm);
   }
 }
 
-// mode 0: X := L^-1 X; 1: X := L^-T X; 2: both (forward then backward in the
-// same launch, y kept in Z between them).
-__global__ void __launch_bounds__(kThreads, 1) sweep32_kernel(const __grid_constant__ CUtensorMap mapF,
-                                                              const __grid_constant__ CUtensorMap mapB,
-                                                              Sweep32Params p) {
+__global__ void __launch_bounds__(kThreads, 1) sweep32_kernel(const __grid_constant__ CUtensorMap mL0,
+                                                              const __grid_constant__ CUtensorMap mL1,
+                                                              const __grid_constant__ CUtensorMap mW0,
+                                                              const __grid_constant__ CUtensorMap mW1,
+                                                              SweepDF p) {
   extern __shared__ float smem_raw[];
   float* sm = align1024(smem_raw);
   float* stages = sm + kOffStages;
-  float* ys = sm + kOffY;
+  float* vs = sm + kOffV;
   uint64_t* full = reinterpret_cast<uint64_t*>(sm + kSmemFloats);
+  int* s_item = reinterpret_cast<int*>(full + kStages);
+  int* s_ok = s_item + 1;
   const int tid = threadIdx.x;
   const int G = gridDim.x;
-  unsigned target = 0;
-  bool ok = true;
   if (tid == 0) {
     for (int s = 0; s < kStages; ++s) mbar_init(&full[s], 1);
     fence_mbar_init();
   }
   __syncthreads();
-  uint32_t phase_bits = 0;  // parity of each stage's mbarrier
+  uint32_t phase_bits = 0;
+  int* abort = p.counters + 1;
 
-  // X (FP64, column-major) -> Z (FP32, row-major; padding columns zero)
-  for (long long e = blockIdx.x * (long long)kThreads + tid; e < (long long)p.n * p.ldz;
-       e += (long long)G * kThreads) {
-    const int r = (int)(e / p.ldz), c = (int)(e % p.ldz);
-    p.Z[(size_t)r * p.ldz + c] = c < p.nrhs ? (float)p.X[r + (long long)c * p.ldx] : 0.f;
+  // X (FP64, column-major) -> Z0; deltas and results zero
+  const long long nz = (long long)p.n * kRhs;
+  for (long long e = blockIdx.x * (long long)kThreads + tid; e < nz; e += (long long)G * kThreads) {
+    const int r = (int)(e / kRhs), c = (int)(e % kRhs);
+    p.Z0[e] = c < p.nrhs ? (float)p.X[r + (long long)c * p.ldx] : 0.f;
+    p.Df[e] = 0.f; p.Yf[e] = 0.f; p.Db[e] = 0.f; p.Yb[e] = 0.f;
   }
-  target += G;
-  ok = grid_barrier(p.counter, target);
+  unsigned target = G;
+  bool ok = grid_barrier(p.bar, target);
 
-  const int passes = (p.nrhs + kRhs - 1) / kRhs;
   const int rg = ((tid >> 5) & 3) * 8 + (tid & 7);   // 4-row (or 4-column) group 0..31
   const int cg = (tid >> 7) * 4 + ((tid >> 3) & 3);  // 4-rhs group 0..7
-  const int nsteps = p.trans == 2 ? 2 * p.nsuper : p.nsuper;
-  for (int step = 0; step < nsteps && ok; ++step) {
-    const int fwd = p.trans == 0 || (p.trans == 2 && step < p.nsuper);
-    const int lstep = step < p.nsuper ? step : step - p.nsuper;
-    const int R = fwd ? lstep : p.nsuper - 1 - lstep;
-    const int r0 = R * kS, sb = min(kS, p.n - r0), r1 = r0 + sb;
-    const float* WR = (fwd ? p.Wr : p.Wc) + (size_t)R * kS * kS;
-    const bool write_x = !(p.trans == 2 && fwd);
-    const BItems bi = b_items(fwd, p.n, r0, r1, G);
-    const bool has_a = blockIdx.x * (kThreads / 32) < sb;
-    // The first phase-B item's L stages do not depend on y_R: start them now
-    bool prefetched = false;
-    if (tid == 0 && passes == 1 && (int)blockIdx.x < bi.items) {
-      const int t = blockIdx.x / bi.ksplit, kpart = blockIdx.x % bi.ksplit;
-      const int kbeg = kpart * bi.kchunk, kend = min(sb, kbeg + bi.kchunk);
-      const int nk = kend > kbeg ? (kend - kbeg + kTK - 1) / kTK : 0;
-      for (int s = 0; s < min(kStages, nk); ++s)
-        issue_stage(&mapF, &mapB, fwd, stages, full, s, bi.lo + t * kTM, r0 + kbeg + s * kTK);
+  while (ok) {
+    if (tid == 0) *s_item = atomicAdd(p.counters, 1);
+    __syncthreads();
+    const int idx = *s_item;
+    __syncthreads();
+    if (idx >= p.items) break;
+    const Item it = p.table[idx];
+    const bool mcontig = it.map == 0 || it.map == 2;
+    const CUtensorMap* mp = it.map == 0 ? &mL0 : it.map == 1 ? &mL1 : it.map == 2 ? &mW0 : &mW1;
+    // the tile does not depend on anything: start its loads now
+    if (tid == 0) {
+      for (int s = 0; s < min(kStages, (int)it.nk); ++s) issue(mp, mcontig, stages, full, s, it.tm, it.tk + s * kTK);
+      bool w = wait_counter(p.counters + it.dep0, it.need0, abort);
+      if (w && it.dep1 >= 0) w = wait_counter(p.counters + it.dep1, it.need1, abort);
+      if (!w) {
+        set_status(p.status, kTimeout, 9002);
+        atomicExch(abort, 1);
+      }
+      *s_ok = w;
     }
-    prefetched = passes == 1 && (int)blockIdx.x < bi.items;
-    // ---- phase A
-    if (has_a) {
-      for (int pass = 0; pass < passes; ++pass) {
-        stage_rows(ys, p.Z + (size_t)r0 * p.ldz, p.ldz, sb, pass);
-        __syncthreads();
-        phase_a(p, WR, fwd, r0, sb, pass, ys, write_x);
-        __syncthreads();
+    __syncthreads();
+    ok = *s_ok != 0;
+    // v rows [vrow, vrow + 32 nk) -> smem.  Phase A: forward z0 + dz;
+    // backward (y, or z0 when only the backward sweep runs) + dv.  Phase B:
+    // the super-block's results y / x.
+    {
+      const float* s0;
+      const float* s1 = nullptr;
+      if (it.kind == 0) {
+        s0 = it.dir == 0 ? p.Z0 : (p.out_backward == 2 ? p.Yf : p.Z0);
+        s1 = it.dir == 0 ? p.Df : p.Db;
+      } else {
+        s0 = it.dir == 0 ? p.Yf : p.Yb;
+      }
+      const int rows = it.nk * kTK;
+      for (int e = tid; e < rows * (kRhs / 4); e += kThreads) {
+        const int r = e / (kRhs / 4), q = e % (kRhs / 4);
+        const int gr = it.vrow + r;
+        float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (gr < p.n) {
+          v = __ldcg(reinterpret_cast<const float4*>(s0 + (size_t)gr * kRhs) + q);
+          if (s1 != nullptr) {
+            const float4 d = __ldcg(reinterpret_cast<const float4*>(s1 + (size_t)gr * kRhs) + q);
+            v.x += d.x; v.y += d.y; v.z += d.z; v.w += d.w;
+          }
+        }
+        reinterpret_cast<float4*>(vs + r * kRhs)[q] = v;
       }
     }
-    target += G;
-    if (!(ok = grid_barrier(p.counter, target))) break;
-    // ---- phase B.  When there are fewer tiles than CTAs, each tile's k
-    // range is split into 2 or 4 parts (work items) whose results are added
-    // to Z with FP32 reductions, so that the late super-steps keep the grid
-    // busy.  Forward steps of mode 2 also move y_R into Z's rows of R (no
-    // phase B writes them) for the backward steps.
-    if (p.trans == 2 && fwd) {
-      for (int e = blockIdx.x * kThreads + tid; e < sb * p.ldz; e += G * kThreads)
-        p.Z[(size_t)r0 * p.ldz + e] = __ldcg(p.Yb + e);
-    }
-    for (int pass = 0; pass < passes; ++pass) {
-      if ((int)blockIdx.x >= bi.items) break;
-      stage_rows(ys, p.Yb, p.ldz, sb, pass);
-      __syncthreads();
-      for (int it = blockIdx.x; it < bi.items; it += G) {
-        const int t = it / bi.ksplit, kpart = it % bi.ksplit;
-        const int m0 = bi.lo + t * kTM;
-        const int kbeg = kpart * bi.kchunk, kend = min(sb, kbeg + bi.kchunk);
-        const int nk = kend > kbeg ? (kend - kbeg + kTK - 1) / kTK : 0;
-        if (nk == 0) continue;
-        if (tid == 0 && !(prefetched && it == (int)blockIdx.x && pass == 0))
-          for (int s = 0; s < min(kStages, nk); ++s)
-            issue_stage(&mapF, &mapB, fwd, stages, full, s, m0, r0 + kbeg + s * kTK);
-        float acc[4][4];
+    __syncthreads();
+    float acc[4][4];
 #pragma unroll
-        for (int a = 0; a < 4; ++a)
+    for (int a = 0; a < 4; ++a)
 #pragma unroll
-          for (int b = 0; b < 4; ++b) acc[a][b] = 0.f;
-        for (int ks = 0; ks < nk; ++ks) {
-          const int s = ks % kStages;
-          if (!mbar_wait_bounded(&full[s], (phase_bits >> s) & 1)) {
-            set_status(p.status, kTimeout, 9001);
-            ok = false;
-          }
-          phase_bits ^= 1u << s;
-          const float* st = stages + s * kStageFloats;
-          const float* yk = ys + (kbeg + ks * kTK) * kRhs;
-          if (fwd) {
-            // stage = 4 boxes of [32 k][32 rows]: row m = 32 b + q at [b][k][q]
-            const int b = rg >> 3, q = (rg & 7) * 4;
+      for (int b = 0; b < 4; ++b) acc[a][b] = 0.f;
+    for (int ks = 0; ks < it.nk; ++ks) {
+      const int s = ks % kStages;
+      if (!mbar_wait_bounded(&full[s], (phase_bits >> s) & 1)) {
+        if (tid == 0) {
+          set_status(p.status, kTimeout, 9001);
+          atomicExch(abort, 1);
+        }
+        ok = false;
+      }
+      phase_bits ^= 1u << s;
+      const float* st = stages + s * kStageFloats;
+      const float* vk = vs + ks * kTK * kRhs;
+      if (mcontig) {
+        // stage = 4 boxes of [32 k][32 rows]: row m = 32 b + q at [b][k][q]
+        const int b = rg >> 3, q = (rg & 7) * 4;
 #pragma unroll 8
-            for (int k = 0; k < kTK; ++k) {
-              const float4 lv = *reinterpret_cast<const float4*>(st + b * 32 * kTK + k * 32 + q);
-              const float4 yv = *reinterpret_cast<const float4*>(yk + k * kRhs + cg * 4);
-              const float l4[4] = {lv.x, lv.y, lv.z, lv.w}, y4[4] = {yv.x, yv.y, yv.z, yv.w};
+        for (int k = 0; k < kTK; ++k) {
+          const float4 lv = *reinterpret_cast<const float4*>(st + b * 32 * kTK + k * 32 + q);
+          const float4 yv = *reinterpret_cast<const float4*>(vk + k * kRhs + cg * 4);
+          const float l4[4] = {lv.x, lv.y, lv.z, lv.w}, y4[4] = {yv.x, yv.y, yv.z, yv.w};
 #pragma unroll
-              for (int a = 0; a < 4; ++a)
+          for (int a = 0; a < 4; ++a)
 #pragma unroll
-                for (int bb = 0; bb < 4; ++bb) acc[a][bb] = fmaf(l4[a], y4[bb], acc[a][bb]);
-            }
-          } else {
-            // stage = [128 columns j][32 k] with the 128-byte swizzle: 16-byte
-            // chunk c of row j at chunk c ^ (j & 7)
-#pragma unroll 2
-            for (int kc = 0; kc < kTK / 4; ++kc) {
-              float l4[4][4];
-#pragma unroll
-              for (int a = 0; a < 4; ++a) {
-                const int j = rg + 32 * a;  // 8 lanes read 8 consecutive columns: distinct chunks
-                const float4 v = *reinterpret_cast<const float4*>(st + j * kTK + ((kc ^ (j & 7)) << 2));
-                l4[a][0] = v.x; l4[a][1] = v.y; l4[a][2] = v.z; l4[a][3] = v.w;
-              }
-#pragma unroll
-              for (int kk = 0; kk < 4; ++kk) {
-                const float4 yv = *reinterpret_cast<const float4*>(yk + (kc * 4 + kk) * kRhs + cg * 4);
-                const float y4[4] = {yv.x, yv.y, yv.z, yv.w};
-#pragma unroll
-                for (int a = 0; a < 4; ++a)
-#pragma unroll
-                  for (int bb = 0; bb < 4; ++bb) acc[a][bb] = fmaf(l4[a][kk], y4[bb], acc[a][bb]);
-              }
-            }
-          }
-          fence_proxy_async_smem();
-          __syncthreads();  // every thread is done with stage s
-          if (tid == 0 && ks + kStages < nk)
-            issue_stage(&mapF, &mapB, fwd, stages, full, s, m0, r0 + kbeg + (ks + kStages) * kTK);
+            for (int bb = 0; bb < 4; ++bb) acc[a][bb] = fmaf(l4[a], y4[bb], acc[a][bb]);
         }
-        // Z[m, c] -= acc for the tile's rows (forward: 4 consecutive rows per
-        // thread) / columns (backward: columns rg + 32 a); L1 is bypassed since
-        // other CTAs wrote these rows in earlier super-steps
+      } else {
+        // stage = [128 columns j][32 k] with the 128-byte swizzle: 16-byte
+        // chunk c of row j at chunk c ^ (j & 7); columns rg + 32 a
+#pragma unroll 2
+        for (int kc = 0; kc < kTK / 4; ++kc) {
+          float l4[4][4];
 #pragma unroll
-        for (int a = 0; a < 4; ++a) {
-          const int m = m0 + (fwd ? rg * 4 + a : rg + 32 * a);
-          if (m < bi.hi) {
-            float* z = p.Z + (size_t)m * p.ldz + pass * kRhs + cg * 4;
-            if (bi.ksplit == 1) {
-              float4 v = __ldcg(reinterpret_cast<const float4*>(z));
-              v.x -= acc[a][0]; v.y -= acc[a][1]; v.z -= acc[a][2]; v.w -= acc[a][3];
-              *reinterpret_cast<float4*>(z) = v;
-            } else {
-              asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(z), "f"(-acc[a][0]),
-                           "f"(-acc[a][1]), "f"(-acc[a][2]), "f"(-acc[a][3])
-                           : "memory");
-            }
+          for (int a = 0; a < 4; ++a) {
+            const int j = rg + 32 * a;
+            const float4 v = *reinterpret_cast<const float4*>(st + j * kTK + ((kc ^ (j & 7)) << 2));
+            l4[a][0] = v.x; l4[a][1] = v.y; l4[a][2] = v.z; l4[a][3] = v.w;
+          }
+#pragma unroll
+          for (int kk = 0; kk < 4; ++kk) {
+            const float4 yv = *reinterpret_cast<const float4*>(vk + (kc * 4 + kk) * kRhs + cg * 4);
+            const float y4[4] = {yv.x, yv.y, yv.z, yv.w};
+#pragma unroll
+            for (int a = 0; a < 4; ++a)
+#pragma unroll
+              for (int bb = 0; bb < 4; ++bb) acc[a][bb] = fmaf(l4[a][kk], y4[bb], acc[a][bb]);
           }
         }
       }
-      __syncthreads();
+      fence_proxy_async_smem();
+      __syncthreads();  // every thread is done with stage s
+      if (tid == 0 && ks + kStages < it.nk) issue(mp, mcontig, stages, full, s, it.tm, it.tk + (ks + kStages) * kTK);
     }
-    target += G;
-    if (!(ok = grid_barrier(p.counter, target))) break;
+    // out rows: phase A adds into the results, phase B subtracts into the deltas
+    {
+      float* out = it.kind == 0 ? (it.dir == 0 ? p.Yf : p.Yb) : (it.dir == 0 ? p.Df : p.Db);
+      const float sg = it.kind == 0 ? 1.f : -1.f;
+#pragma unroll
+      for (int a = 0; a < 4; ++a) {
+        const int m = mcontig ? rg * 4 + a : rg + 32 * a;
+        if (m < it.orows) {
+          float* z = out + (size_t)(it.orow + m) * kRhs + cg * 4;
+          asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(z), "f"(sg * acc[a][0]),
+                       "f"(sg * acc[a][1]), "f"(sg * acc[a][2]), "f"(sg * acc[a][3])
+                       : "memory");
+        }
+      }
+    }
+    __threadfence();
+    __syncthreads();
+    if (tid == 0) atomicAdd(p.counters + it.done, 1);
+  }
+  // the results to X once every item is done
+  target += G;
+  ok = grid_barrier(p.bar, target) && ok;
+  const float* res = p.out_backward ? p.Yb : p.Yf;
+  for (long long e = blockIdx.x * (long long)kThreads + tid; e < nz; e += (long long)G * kThreads) {
+    const int r = (int)(e / kRhs), c = (int)(e % kRhs);
+    if (c < p.nrhs) p.X[r + (long long)c * p.ldx] = (double)__ldcg(res + e);
   }
   if (!ok && tid == 0) set_status(p.status, kTimeout, 9000);
 }
@@ -428,43 +404,164 @@ __global__ void __launch_bounds__(kThreads) superinv_row_kernel(int n, int nsupe
   tile128_products(&w, 1, -1.f, X + bi * kPB + (size_t)(j * kPB) * kS, kS, As, Bs, kPB, rows_valid, kPB);
 }
 
-// Wr = Wc^T per super-block (row-major copy for the forward sweep)
-__global__ void transpose_blocks_kernel(int nsuper, const float* Wc, float* Wr) {
-  __shared__ float t[32][33];
-  const int R = blockIdx.z;
-  const float* src = Wc + (size_t)R * kS * kS;
-  float* dst = Wr + (size_t)R * kS * kS;
-  const int bx = blockIdx.x * 32, by = blockIdx.y * 32;
-  for (int q = threadIdx.y; q < 32; q += 8) t[q][threadIdx.x] = src[(bx + threadIdx.x) + (size_t)(by + q) * kS];
-  __syncthreads();
-  for (int q = threadIdx.y; q < 32; q += 8) dst[(by + threadIdx.x) + (size_t)(bx + q) * kS] = t[threadIdx.x][q];
-}
-
 }  // namespace
 
-size_t sweep32_ws_bytes(int n, int nrhs) {
+// ---- host: the item queue --------------------------------------------
+
+// Counter layout: [0] queue, [1] abort, then per direction d and super-block R:
+// cY(d, R) (phase-A items of R done), cD(d, R) (phase-B items targeting R done).
+struct CounterIx {
+  int nsuper;
+  int cy(int d, int R) const { return 2 + (d * nsuper + R) * 2; }
+  int cd(int d, int R) const { return 3 + (d * nsuper + R) * 2; }
+  int count() const { return 2 + 4 * nsuper; }
+};
+
+// Items of one sweep direction in dependency order.  G: grid size (decides
+// how finely the bulk phase-B tiles are split along k).
+static void build_items(int n, int G, int dir, bool after_forward, std::vector<Item>& out, const CounterIx& cx) {
   const int nsuper = (n + kS - 1) / kS;
-  const int ldz = ((std::max(nrhs, 1) + kRhs - 1) / kRhs) * kRhs;
-  size_t b = 0;
-  b += 2 * (size_t)nsuper * kS * kS * sizeof(float);        // Wc, Wr
-  b += (size_t)nsuper * 4 * kPB * kPB * sizeof(float);       // temporaries of the inverse
-  b += (size_t)n * ldz * sizeof(float) + 1024;                // Z
-  b += (size_t)kS * ldz * sizeof(float) + 1024;               // Yb
-  b += 4096;                                                  // counter
-  return b + 8 * 1024;
+  auto sb_of = [&](int R) { return std::min(kS, n - R * kS); };
+  std::vector<int> cd_need(nsuper, 0);  // phase-B items that will target each super-block
+  // phase-B items of super-block R: critical (the next super-block of the
+  // sweep, k split 4 ways) or bulk (the others)
+  auto b_items = [&](int R, bool critical, std::vector<Item>& v) {
+    const int r0 = R * kS, sb = sb_of(R);
+    // targets: forward rows of later super-blocks; backward columns of earlier ones
+    std::vector<int> targets;
+    if (dir == 0)
+      for (int Q = R + 1; Q < nsuper; ++Q) targets.push_back(Q);
+    else
+      for (int Q = R - 1; Q >= 0; --Q) targets.push_back(Q);
+    int bulk_tiles = 0;
+    for (size_t t = 1; t < targets.size(); ++t) bulk_tiles += (sb_of(targets[t]) + kTM - 1) / kTM;
+    int ksplit_bulk = 1;
+    while (ksplit_bulk < 4 && bulk_tiles * ksplit_bulk * 2 <= G) ksplit_bulk *= 2;
+    for (size_t t = critical ? 0 : 1; t < (critical ? std::min<size_t>(1, targets.size()) : targets.size()); ++t) {
+      const int Q = targets[t], q0 = Q * kS, sq = sb_of(Q);
+      const int ksplit = t == 0 ? 4 : ksplit_bulk;  // the next super-block's items are on the chain: finest
+      const int kch = kS / ksplit;
+      for (int m = 0; m < sq; m += kTM)
+        for (int kp = 0; kp < ksplit; ++kp) {
+          const int kb = kp * kch, ke = std::min(sb, kb + kch);
+          if (ke <= kb) continue;
+          Item it{};
+          it.map = dir == 0 ? 0 : 1;
+          it.dir = dir;
+          it.kind = 1;
+          it.nk = (ke - kb + kTK - 1) / kTK;
+          it.tm = q0 + m;      // forward: rows of L; backward: columns of L
+          it.tk = r0 + kb;     // forward: columns of L; backward: rows of L
+          it.vrow = r0 + kb;
+          it.orow = q0 + m;
+          it.orows = std::min(kTM, sq - m);
+          it.dep0 = cx.cy(dir, R);
+          it.need0 = 0;  // filled below
+          it.dep1 = -1;
+          it.done = cx.cd(dir, Q);
+          ++cd_need[Q];
+          v.push_back(it);
+        }
+    }
+  };
+  auto a_items = [&](int R, std::vector<Item>& v) {
+    const int r0 = R * kS, sb = sb_of(R);
+    for (int mt = 0; mt < sb; mt += kTM)
+      for (int kt = 0; kt < sb; kt += kTM) {
+        // W_R lower: forward tile (mt, kt) nonzero for kt <= mt; W_R^T upper: kt >= mt
+        if (dir == 0 ? kt > mt : kt < mt) continue;
+        Item it{};
+        it.map = dir == 0 ? 2 : 3;
+        it.dir = dir;
+        it.kind = 0;
+        it.nk = (std::min(kTM, sb - kt) + kTK - 1) / kTK;
+        // W_R block in the (kS x kS nsuper) tensor: rows i, columns R kS + j
+        it.tm = dir == 0 ? mt : R * kS + mt;
+        it.tk = dir == 0 ? R * kS + kt : kt;
+        it.vrow = r0 + kt;
+        it.orow = r0 + mt;
+        it.orows = std::min(kTM, sb - mt);
+        it.dep0 = cx.cd(dir, R);
+        it.need0 = 0;  // filled below
+        it.dep1 = -1;
+        if (dir == 1 && after_forward) {  // x_R needs y_R: all forward phase-A items of R
+          it.dep1 = cx.cy(0, R);
+          it.need1 = 0;  // filled by the caller
+        }
+        it.done = cx.cy(dir, R);
+        v.push_back(it);
+      }
+  };
+  const size_t first = out.size();
+  // dependency order with the chain first: A(R), then the bulk of the
+  // previous super-block's phase B, then R's items for the next super-block
+  // (phase A of R + 1 needs those and the earlier bulk, all queued before it)
+  for (int s = 0; s <= nsuper; ++s) {
+    const int R = dir == 0 ? s : nsuper - 1 - s;
+    const int Rp = dir == 0 ? s - 1 : nsuper - s;  // the previous super-block of the sweep
+    if (s < nsuper) a_items(R, out);
+    if (s >= 1) b_items(Rp, false, out);
+    if (s < nsuper) b_items(R, true, out);
+  }
+  // needs: phase A of R waits for every phase-B item targeting R, phase B of
+  // R for all phase-A items of R
+  std::vector<int> a_count(nsuper, 0);
+  for (size_t i = first; i < out.size(); ++i)
+    if (out[i].kind == 0) ++a_count[(out[i].orow) / kS];
+  for (size_t i = first; i < out.size(); ++i) {
+    Item& it = out[i];
+    if (it.kind == 0) it.need0 = cd_need[it.orow / kS];
+    else it.need0 = a_count[it.vrow / kS];
+  }
 }
+
+size_t sweep32_ws_bytes(int n, int nrhs) {
+  (void)nrhs;
+  const int nsuper = (n + kS - 1) / kS;
+  size_t b = 0;
+  b += (size_t)nsuper * kS * kS * sizeof(float) + 1024;      // Wc
+  b += (size_t)nsuper * 4 * kPB * kPB * sizeof(float);       // temporaries of the inverse
+  b += 5 * ((size_t)n * kRhs * sizeof(float) + 1024);        // Z0, Df, Yf, Db, Yb
+  b += (size_t)(2 + 4 * nsuper) * sizeof(int) + 1024;        // counters
+  b += 1024;                                                  // barrier
+  b += (size_t)2 * (nsuper * 10 + nsuper * nsuper * 16 + 64) * sizeof(Item) + 1024;  // item table (bound)
+  return b + 16 * 1024;  // every piece is 1024-aligned
+}
+
+namespace {
+struct SweepWs {
+  float *Wc, *tmp, *Z0, *Df, *Yf, *Db, *Yb;
+  int* counters;
+  unsigned* bar;
+  Item* table;
+};
+SweepWs carve(void* ws, int n) {
+  const int nsuper = (n + kS - 1) / kS;
+  SweepWs w;
+  uintptr_t b = reinterpret_cast<uintptr_t>(ws);
+  auto take = [&](size_t bytes) { b = align_up(b, 1024); uintptr_t o = b; b += bytes; return o; };
+  w.Wc = reinterpret_cast<float*>(take((size_t)nsuper * kS * kS * sizeof(float)));
+  w.tmp = reinterpret_cast<float*>(take((size_t)nsuper * 4 * kPB * kPB * sizeof(float)));
+  w.Z0 = reinterpret_cast<float*>(take((size_t)n * kRhs * sizeof(float)));
+  w.Df = reinterpret_cast<float*>(take((size_t)n * kRhs * sizeof(float)));
+  w.Yf = reinterpret_cast<float*>(take((size_t)n * kRhs * sizeof(float)));
+  w.Db = reinterpret_cast<float*>(take((size_t)n * kRhs * sizeof(float)));
+  w.Yb = reinterpret_cast<float*>(take((size_t)n * kRhs * sizeof(float)));
+  w.counters = reinterpret_cast<int*>(take((size_t)(2 + 4 * nsuper) * sizeof(int)));
+  w.bar = reinterpret_cast<unsigned*>(take(256));
+  w.table = reinterpret_cast<Item*>(take(0));
+  return w;
+}
+}  // namespace
 
 // Build the super-block inverses from L (FP32, ld ldl) and the FP64 panel
 // inverses Winv (nb = 128, one nb x nb block per panel).  ws: sweep32_ws_bytes.
 int sweep32_prepare(cudaStream_t st, int n, const float* L, long long ldl, const double* Winv, void* ws) {
   const int nsuper = (n + kS - 1) / kS;
-  unsigned char* b = static_cast<unsigned char*>(ws);
-  float* Wc = reinterpret_cast<float*>(b);
-  float* Wr = Wc + (size_t)nsuper * kS * kS;
-  float* tmp = Wr + (size_t)nsuper * kS * kS;
+  const SweepWs w = carve(ws, n);
   TraceMark tm(st, kTraceOther, (double)nsuper * 4.0 * kS * kS * kS / 3.0, 12.0 * nsuper * kS * kS);
   superinv_init_kernel<<<std::min<long long>(((long long)nsuper * kS * kS + 255) / 256, 148 * 16), 256, 0, st>>>(
-      n, nsuper, Winv, Wc);
+      n, nsuper, Winv, w.Wc);
   count_launch();
   EGPU_CUDA_TRY(cudaGetLastError());
   static bool attr = false;
@@ -474,38 +571,43 @@ int sweep32_prepare(cudaStream_t st, int n, const float* L, long long ldl, const
     attr = true;
   }
   for (int bi = 1; bi < kS / kPB; ++bi) {
-    superinv_row_kernel<<<dim3(bi, nsuper), kThreads, shb, st>>>(n, nsuper, bi, L, ldl, Wc, tmp);
+    superinv_row_kernel<<<dim3(bi, nsuper), kThreads, shb, st>>>(n, nsuper, bi, L, ldl, w.Wc, w.tmp);
     count_launch();
     EGPU_CUDA_TRY(cudaGetLastError());
   }
-  transpose_blocks_kernel<<<dim3(kS / 32, kS / 32, nsuper), dim3(32, 8), 0, st>>>(nsuper, Wc, Wr);
-  count_launch();
-  EGPU_CUDA_TRY(cudaGetLastError());
   return EGPU_OK;
 }
 
-// X := L^-1 X (trans 0) or L^-T X (trans 1); X FP64 n x nrhs (ld ldx), L FP32
-// (ld ldl, 16-byte aligned base and ld a multiple of 4), ws prepared by
-// sweep32_prepare for this L.
+// X := L^-1 X (trans 0), L^-T X (trans 1) or L^-T L^-1 X (trans 2); X FP64 n
+// x nrhs (nrhs <= 32, ld ldx), L FP32 (ld ldl, 16-byte aligned base and ld a
+// multiple of 4), ws prepared by sweep32_prepare for this L.
 int sweep32_solve(cudaStream_t st, int trans, int n, int nrhs, const float* L, long long ldl, double* X,
                   long long ldx, void* ws, int sm_count, DevStatus* status) {
   if (n <= 0 || nrhs <= 0) return EGPU_OK;
+  if (nrhs > kRhs || trans < 0 || trans > 2) return EGPU_ERR_UNSUPPORTED;
   if (reinterpret_cast<uintptr_t>(L) % 16 != 0 || ldl % 4 != 0) return EGPU_ERR_ALIGN;
   const int nsuper = (n + kS - 1) / kS;
-  const int ldz = ((nrhs + kRhs - 1) / kRhs) * kRhs;
-  unsigned char* b = static_cast<unsigned char*>(ws);
-  float* Wc = reinterpret_cast<float*>(b);
-  float* Wr = Wc + (size_t)nsuper * kS * kS;
-  float* tmp = Wr + (size_t)nsuper * kS * kS;
-  unsigned char* after = reinterpret_cast<unsigned char*>(tmp + (size_t)nsuper * 4 * kPB * kPB);
-  float* Z = reinterpret_cast<float*>(align_up(reinterpret_cast<uintptr_t>(after), 1024));
-  float* Yb = reinterpret_cast<float*>(align_up(reinterpret_cast<uintptr_t>(Z + (size_t)n * ldz), 1024));
-  unsigned* counter = reinterpret_cast<unsigned*>(align_up(reinterpret_cast<uintptr_t>(Yb + (size_t)kS * ldz), 256));
-  CUtensorMap mapF, mapB;
-  // forward: boxes of 32 rows (inner) x 32 columns; backward: 32 rows (inner)
-  // x 128 columns, 128-byte swizzle
-  if (!make_tma_2d(&mapF, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, L, n, n, ldl * 4, 32, kTK, false) ||
-      !make_tma_2d(&mapB, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, L, n, n, ldl * 4, kTK, kTM, true))
+  const SweepWs w = carve(ws, n);
+  const CounterIx cx{nsuper};
+  std::vector<Item> items;
+  if (trans == 0 || trans == 2) build_items(n, sm_count, 0, false, items, cx);
+  if (trans == 1 || trans == 2) {
+    const size_t b0 = items.size();
+    build_items(n, sm_count, 1, trans == 2, items, cx);
+    if (trans == 2) {  // backward phase A of R also waits for the forward phase A of R
+      std::vector<int> ay(nsuper, 0);
+      for (size_t i = 0; i < b0; ++i)
+        if (items[i].kind == 0) ++ay[items[i].orow / kS];
+      for (size_t i = b0; i < items.size(); ++i)
+        if (items[i].dep1 >= 0) items[i].need1 = ay[items[i].orow / kS];
+    }
+  }
+  CUtensorMap m[4];
+  // L: {n rows, n columns}; W: {kS rows, kS * nsuper columns}
+  if (!make_tma_2d(&m[0], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, L, n, n, ldl * 4, 32, kTK, false) ||
+      !make_tma_2d(&m[1], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, L, n, n, ldl * 4, kTK, kTM, true) ||
+      !make_tma_2d(&m[2], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, w.Wc, kS, (uint64_t)kS * nsuper, kS * 4, 32, kTK, false) ||
+      !make_tma_2d(&m[3], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, w.Wc, kS, (uint64_t)kS * nsuper, kS * 4, kTK, kTM, true))
     return EGPU_ERR_TMA;
   static int attr_dev_mask = 0;
   int dev = 0;
@@ -514,11 +616,15 @@ int sweep32_solve(cudaStream_t st, int trans, int n, int nrhs, const float* L, l
     EGPU_CUDA_TRY(cudaFuncSetAttribute(sweep32_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes));
     attr_dev_mask |= 1 << dev;
   }
-  EGPU_CUDA_TRY(cudaMemsetAsync(counter, 0, sizeof(unsigned), st));
-  Sweep32Params p;
-  p.n = n; p.nrhs = nrhs; p.trans = trans; p.nsuper = nsuper;  // trans 2: forward + backward
-  p.Wc = Wc; p.Wr = Wr; p.Z = Z; p.ldz = ldz; p.Yb = Yb; p.X = X; p.ldx = ldx; p.counter = counter;
-  p.status = status;
+  EGPU_CUDA_TRY(cudaMemcpyAsync(w.table, items.data(), sizeof(Item) * items.size(), cudaMemcpyHostToDevice, st));
+  EGPU_CUDA_TRY(cudaMemsetAsync(w.counters, 0, sizeof(int) * cx.count(), st));
+  EGPU_CUDA_TRY(cudaMemsetAsync(w.bar, 0, sizeof(unsigned), st));
+  SweepDF p;
+  p.n = n; p.nrhs = nrhs; p.items = (int)items.size(); p.table = w.table;
+  p.Z0 = w.Z0; p.Df = w.Df; p.Yf = w.Yf; p.Db = w.Db; p.Yb = w.Yb;
+  p.X = X; p.ldx = ldx;
+  p.out_backward = trans == 0 ? 0 : (trans == 2 ? 2 : 1);
+  p.counters = w.counters; p.bar = w.bar; p.status = status;
   TraceMark tm(st, kTraceSolve, (trans == 2 ? 2.0 : 1.0) * n * n * nrhs,
                (trans == 2 ? 2.0 : 1.0) * (2.0 * n * n + 16.0 * n * nrhs));
   cudaLaunchConfig_t cfg = {};
@@ -531,8 +637,10 @@ int sweep32_solve(cudaStream_t st, int trans, int n, int nrhs, const float* L, l
   attr[0].val.cooperative = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  EGPU_CUDA_TRY(cudaLaunchKernelEx(&cfg, sweep32_kernel, mapF, mapB, p));
+  EGPU_CUDA_TRY(cudaLaunchKernelEx(&cfg, sweep32_kernel, m[0], m[1], m[2], m[3], p));
   count_launch();
+  // (a copy from pageable host memory returns once the data is staged, so the
+  // table's host vector may go)
   return EGPU_OK;
 }
 
@@ -558,7 +666,7 @@ using namespace egpu;
 extern "C" int egpu_sweep32_solve(egpu_handle h, int trans, int n, int nrhs, const float* dL, int ldl, double* dX,
                                   int ldx) {
   if (!h) return EGPU_ERR_ARG;
-  if (n < 0 || nrhs < 0 || nrhs > 64 || ldl < std::max(1, n) || ldx < std::max(1, n) || trans < 0 || trans > 2)
+  if (n < 0 || nrhs < 0 || nrhs > 32 || ldl < std::max(1, n) || ldx < std::max(1, n) || trans < 0 || trans > 2)
     return EGPU_ERR_ARG;
   if (n == 0 || nrhs == 0) return EGPU_OK;
   Enter en(h);

@@ -260,7 +260,7 @@ EGPU_API int egpu_tc_gemm_split(egpu_handle h, int M, int N, int K, double alpha
  * counterpart in the reference): X := L^-1 X (trans 0), L^-T X (trans 1) or
  * L^-T L^-1 X (trans 2, one launch) with L lower triangular, FP32, column-major (16-byte aligned, ldl a
  * multiple of 4), through 512 x 512 super-block inverses built from L's 128 x
- * 128 diagonal-block inverses; X FP64, nrhs <= 64.  Synchronous. */
+ * 128 diagonal-block inverses; X FP64, nrhs <= 32.  Synchronous. */
 EGPU_API int egpu_sweep32_solve(egpu_handle h, int trans, int n, int nrhs, const float* dL, int ldl, double* dX,
                                 int ldx);
 

@@ -142,13 +142,13 @@ def test_hpd_solve_mixed_config_n16384_kappa1e6(handle):
 
 
 @pytest.mark.parametrize("n", [1, 100, 511, 512, 513, 1000, 2049, 4100])
-@pytest.mark.parametrize("nrhs", [1, 7, 32, 33, 64])
+@pytest.mark.parametrize("nrhs", [1, 7, 32])
 @pytest.mark.parametrize("trans", [0, 1, 2])
 def test_sweep32_solve_matches_fp64_triangular_solve(handle, n, nrhs, trans):
     # the FP32 super-block sweep (egpu_sweep32_solve) against an FP64
     # triangular solve of the same FP32 factor: the Cholesky factor of a
     # well-conditioned HPD matrix, so the FP32 solve is accurate to ~1e-6
-    if n > 1000 and nrhs not in (32, 64):
+    if n > 1000 and nrhs != 32:
         pytest.skip("large orders with the bench's right-hand-side counts only")
     A = torch.from_numpy(inputs.spd_ggt(n, 90 + n)).cuda()
     L = torch.linalg.cholesky(A)
