@@ -120,6 +120,8 @@ def _declare(L):
         "egpu_tc_gemm_split": ([H, I, I, I, D, P, I, P, I, D, P, I, I, I], I),
         "egpu_host_dposv_mixed": ([H, I, I, I, P, I, P, I, P, I, I, D, P, P], I),
         "egpu_mixed_gmres_iterations": ([H], I),
+        "egpu_set_mixed_policy": ([H, I], I),
+        "egpu_mixed_condition_estimate": ([H, P], I),
         "egpu_batch_plan_create": ([H, I, I, P, P, P, P, P, P, P], I),
         "egpu_batch_plan_run": ([P, P], I),
         "egpu_batch_plan_info": ([P, P, P], I),
@@ -729,6 +731,17 @@ class Handle:
             raise ElemGPUError(f"refinement did not reach {tol:g} in {it.value} corrections (berr {be.value:.3e})")
         _check(rc)
         return X, it.value, be.value
+
+    def set_mixed_policy(self, policy: int):
+        """0: adaptive (condition estimate only when refinement contracts
+        slowly); 1: estimate after every factorization and pick IR or GMRES-IR."""
+        _check(lib().egpu_set_mixed_policy(self._h, int(policy)))
+
+    def mixed_condition_estimate(self) -> float:
+        """kappa_1(A) estimated by the last mixed solve (-1 when it needed none)."""
+        v = ctypes.c_double()
+        _check(lib().egpu_mixed_condition_estimate(self._h, ctypes.byref(v)))
+        return v.value
 
     def mixed_gmres_iterations(self):
         """GMRES iterations of the last mixed solve (0 when plain refinement converged)."""

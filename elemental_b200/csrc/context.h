@@ -82,6 +82,10 @@ struct egpu_context {
   int lookahead = -1;  // -1 auto groups, 0 sequential, 1 per-panel, G >= 2 fixed groups (Cholesky)
   int async = 0;  // device API: enqueue only; status read by egpu_get_status
   int gmres_inner = 0;  // GMRES iterations of the last mixed solve
+  // mixed solve: 0 adaptive (condition estimate when the first correction
+  // contracts slowly), 1 estimate after every factorization
+  int mixed_policy = 0;
+  double mixed_kappa = -1.0;  // last 1-norm condition estimate (-1: none)
 };
 
 struct DeviceGuard {

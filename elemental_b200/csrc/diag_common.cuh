@@ -30,28 +30,30 @@ constexpr int kLDS = 132;
 constexpr int kSP = 16;  // sub-panel width
 constexpr int kDiagSmemBase = (128 * kLDS + 128) * (int)sizeof(double);
 
-__device__ __forceinline__ double& SE(double* S, int r, int c) { return S[r + c * kLDS]; }
+template <typename T>
+__device__ __forceinline__ T& SE(T* S, int r, int c) { return S[r + c * kLDS]; }
 
 // C[r0.., c0..] (nr x nc, lower part r >= c when tri) -= A[r0.., k0..k0+K) * B[c0.., k0..k0+K)^T
 // reading A and B from S; 4x4 register tiles per thread.  sign = +1 or -1 for
 // "-=" or "+=" (the inverse uses the opposite sign).
-__device__ inline void smem_syrk_tiles(double* S, int r0, int nr, int c0, int nc, int k0, int K, bool tri) {
+template <typename T>
+__device__ inline void smem_syrk_tiles(T* S, int r0, int nr, int c0, int nc, int k0, int K, bool tri) {
   const int tr = (nr + 3) / 4, tc = (nc + 3) / 4;
   for (int t = threadIdx.x; t < tr * tc; t += blockDim.x) {
     const int ti = t % tr, tj = t / tr;
     const int rb = r0 + 4 * ti, cb = c0 + 4 * tj;
     if (tri && rb + 3 < cb) continue;  // tile strictly above the diagonal
-    double acc[4][4];
+    T acc[4][4];
 #pragma unroll
     for (int a = 0; a < 4; ++a)
 #pragma unroll
-      for (int b = 0; b < 4; ++b) acc[a][b] = 0.0;
+      for (int b = 0; b < 4; ++b) acc[a][b] = T(0);
     for (int k = k0; k < k0 + K; ++k) {
-      double x[4], y[4];
+      T x[4], y[4];
 #pragma unroll
       for (int a = 0; a < 4; ++a) {
-        x[a] = (rb + a < r0 + nr) ? SE(S, rb + a, k) : 0.0;
-        y[a] = (cb + a < c0 + nc) ? SE(S, cb + a, k) : 0.0;
+        x[a] = (rb + a < r0 + nr) ? SE(S, rb + a, k) : T(0);
+        y[a] = (cb + a < c0 + nc) ? SE(S, cb + a, k) : T(0);
       }
 #pragma unroll
       for (int a = 0; a < 4; ++a)
@@ -68,23 +70,25 @@ __device__ inline void smem_syrk_tiles(double* S, int r0, int nr, int c0, int nc
   }
 }
 
-// Lower Cholesky of the b x b block in S.  Returns 0 or the 1-based column
-// of a non-positive pivot ("A was not numerically HPD", LVar3.hpp:37-38); the
-// decision is uniform across the block (every thread reads the same a_jj).
-__device__ inline int smem_chol(double* S, int b) {
-  __shared__ double s_alpha[128];
+// Lower Cholesky of the b x b block in S (T = float or double).  Returns 0 or
+// the 1-based column of a non-positive pivot ("A was not numerically HPD",
+// LVar3.hpp:37-38); the decision is uniform across the block (every thread
+// reads the same a_jj).
+template <typename T>
+__device__ inline int smem_chol(T* S, int b) {
+  __shared__ T s_alpha[128];
   const int tid = threadIdx.x;
   const int row = tid & 127, half = tid >> 7;  // two threads per row
   for (int c0 = 0; c0 < b; c0 += kSP) {
     const int c1 = min(b, c0 + kSP);
     for (int j = c0; j < c1; ++j) {
-      const double ajj = SE(S, j, j);
-      if (ajj <= 0.0) return j + 1;
+      const T ajj = SE(S, j, j);
+      if (!(ajj > T(0))) return j + 1;  // non-positive or NaN
       if (tid == 0) s_alpha[j] = sqrt(ajj);
       // column j-1 is read by nobody in this phase: scale it now
       if (j > c0 && half == 1 && row >= j && row < b) SE(S, row, j - 1) /= s_alpha[j - 1];
       if (row > j && row < b) {
-        const double lij = SE(S, row, j) / ajj;
+        const T lij = SE(S, row, j) / ajj;
         for (int k = j + 1 + half; k < c1 && k <= row; k += 2) SE(S, row, k) -= lij * SE(S, k, j);
       }
       __syncthreads();
@@ -103,7 +107,8 @@ __device__ inline int smem_chol(double* S, int b) {
 // In-place inverse of the lower b x b triangle in S (unit: diagonal taken as 1
 // and written as 1).  Uses Xs (16 x 16 scratch per warp would not fit; the
 // diagonal blocks are inverted in place column by column by their warp).
-__device__ inline void smem_trinv(double* S, int b, int unit) {
+template <typename T>
+__device__ inline void smem_trinv(T* S, int b, int unit) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int nblk = (b + kSP - 1) / kSP;
   // 1. 16 x 16 diagonal blocks, one warp each: lane c (< 16) computes column c
@@ -111,15 +116,15 @@ __device__ inline void smem_trinv(double* S, int b, int unit) {
   //    so results go to registers first, then back to S.
   for (int blk = warp; blk < nblk; blk += blockDim.x / 32) {
     const int o = blk * kSP, w = min(kSP, b - o);
-    double x[kSP];
+    T x[kSP];
     const int c = lane;
 #pragma unroll
-    for (int i = 0; i < kSP; ++i) x[i] = 0.0;
+    for (int i = 0; i < kSP; ++i) x[i] = T(0);
     if (c < w) {
 #pragma unroll
       for (int i = 0; i < kSP; ++i) {
         if (i < w && i >= c) {
-          double acc = (i == c) ? 1.0 : 0.0;
+          T acc = (i == c) ? T(1) : T(0);
 #pragma unroll
           for (int m = 0; m < kSP; ++m)
             if (m >= c && m < i) acc = fma(-SE(S, o + i, o + m), x[m], acc);
@@ -131,7 +136,7 @@ __device__ inline void smem_trinv(double* S, int b, int unit) {
     if (c < w) {
 #pragma unroll
       for (int i = 0; i < kSP; ++i)
-        if (i < w && i >= c) SE(S, o + i, o + c) = (unit && i == c) ? 1.0 : x[i];
+        if (i < w && i >= c) SE(S, o + i, o + c) = (unit && i == c) ? T(1) : x[i];
     }
   }
   __syncthreads();
@@ -141,24 +146,24 @@ __device__ inline void smem_trinv(double* S, int b, int unit) {
     // T = L21 * X11 (R x w), computed into registers, written over L21
     {
       const int tr = (R + 3) / 4;
-      double acc[4][4];
+      T acc[4][4];
       const int t = tid;
       const bool act = t < tr * 4;  // tiles: 4 rows x 4 cols, w <= 16 -> 4 col tiles
       const int ti = t % max(tr, 1), tj = t / max(tr, 1);
 #pragma unroll
       for (int a = 0; a < 4; ++a)
 #pragma unroll
-        for (int q = 0; q < 4; ++q) acc[a][q] = 0.0;
+        for (int q = 0; q < 4; ++q) acc[a][q] = T(0);
       if (act) {
         for (int k = 0; k < w; ++k) {
 #pragma unroll
           for (int a = 0; a < 4; ++a) {
             const int r = r0 + 4 * ti + a;
-            const double l = (r < b) ? SE(S, r, o + k) : 0.0;
+            const T l = (r < b) ? SE(S, r, o + k) : T(0);
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
               const int cc = 4 * tj + q;
-              const double xv = (cc < w && k >= cc) ? SE(S, o + k, o + cc) : 0.0;
+              const T xv = (cc < w && k >= cc) ? SE(S, o + k, o + cc) : T(0);
               acc[a][q] = fma(l, xv, acc[a][q]);
             }
           }
@@ -179,16 +184,16 @@ __device__ inline void smem_trinv(double* S, int b, int unit) {
 #pragma unroll
         for (int a = 0; a < 4; ++a)
 #pragma unroll
-          for (int q = 0; q < 4; ++q) acc[a][q] = 0.0;
+          for (int q = 0; q < 4; ++q) acc[a][q] = T(0);
         const int rmax = min(b - 1, r0 + 4 * ti + 3);
         for (int m = r0; m <= rmax; ++m) {
-          double tv[4];
+          T tv[4];
 #pragma unroll
-          for (int q = 0; q < 4; ++q) tv[q] = (4 * tj + q < w) ? SE(S, m, o + 4 * tj + q) : 0.0;
+          for (int q = 0; q < 4; ++q) tv[q] = (4 * tj + q < w) ? SE(S, m, o + 4 * tj + q) : T(0);
 #pragma unroll
           for (int a = 0; a < 4; ++a) {
             const int r = r0 + 4 * ti + a;
-            const double xv = (r < b && m <= r) ? (unit && m == r ? 1.0 : SE(S, r, m)) : 0.0;
+            const T xv = (r < b && m <= r) ? (unit && m == r ? T(1) : SE(S, r, m)) : T(0);
 #pragma unroll
             for (int q = 0; q < 4; ++q) acc[a][q] = fma(xv, tv[q], acc[a][q]);
           }

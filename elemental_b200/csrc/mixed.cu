@@ -412,6 +412,74 @@ static int gmres_correction(egpu_context* h, int n, int nrhs, const double* As, 
   return EGPU_OK;
 }
 
+// 1-norm condition estimate of the HPD A from its low-precision factor:
+// kappa_1 = ||A||_1 ||A^-1||_1 with ||A^-1||_1 estimated by Hager's method
+// (W. W. Hager, "Condition estimates", SIAM J. Sci. Stat. Comput. 5, 1984, as
+// refined by N. J. Higham, ACM TOMS 14, 1988: the algorithm of LAPACK's
+// dlacon), with A^-1 applied as the factor's solve (A symmetric, so A^-T =
+// A^-1).  At most 5 iterations of two solves each, plus the closing test with
+// the alternating vector; the small vector logic runs on the host.  V: two
+// work columns of ld lds on the device.
+static int cond1_estimate(egpu_context* h, int n, const double* Lf, long long lds, const double* Winv,
+                          SweepFlags& fl, double anorm, double* V, double* kappa) {
+  cudaStream_t st = h->stream;
+  std::vector<double> x(n), y(n), z(n), xi(n), xi_old(n, 0.0);
+  auto apply = [&](std::vector<double>& v) -> int {  // v := A^-1 v
+    EGPU_CUDA_TRY(cudaMemcpyAsync(V, v.data(), sizeof(double) * n, cudaMemcpyHostToDevice, st));
+    TRY(mixed_solve(h, n, 1, Lf, lds, Winv, V, fl));
+    EGPU_CUDA_TRY(cudaMemcpyAsync(v.data(), V, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+    EGPU_CUDA_TRY(cudaStreamSynchronize(st));
+    return EGPU_OK;
+  };
+  auto norm1 = [&](const std::vector<double>& v) {
+    double t = 0.0;
+    for (double a : v) t += std::fabs(a);
+    return t;
+  };
+  for (int i = 0; i < n; ++i) x[i] = 1.0 / n;
+  double est = 0.0;
+  for (int k = 1; k <= 5; ++k) {
+    y = x;
+    TRY(apply(y));
+    const double ny = norm1(y);
+    if (k > 1 && ny <= est) break;  // no increase
+    est = ny;
+    bool same = k > 1;
+    for (int i = 0; i < n; ++i) {
+      xi[i] = y[i] >= 0.0 ? 1.0 : -1.0;
+      same = same && xi[i] == xi_old[i];
+    }
+    if (same) break;  // the sign pattern repeats: converged
+    z = xi;
+    TRY(apply(z));
+    int j = 0;
+    double zx = 0.0;
+    for (int i = 0; i < n; ++i) {
+      if (std::fabs(z[i]) > std::fabs(z[j])) j = i;
+      zx += z[i] * x[i];
+    }
+    if (k > 1 && std::fabs(z[j]) <= zx) break;  // no better column
+    std::fill(x.begin(), x.end(), 0.0);
+    x[j] = 1.0;
+    xi_old = xi;
+  }
+  // the alternating test vector guards against the method's known failures
+  for (int i = 0; i < n; ++i) x[i] = (i % 2 ? -1.0 : 1.0) * (1.0 + (n > 1 ? (double)i / (n - 1) : 0.0));
+  TRY(apply(x));
+  est = std::max(est, 2.0 * norm1(x) / (3.0 * n));
+  *kappa = anorm * est;
+  return EGPU_OK;
+}
+
+// Refinement mode from a 1-norm condition estimate and the low-precision
+// factor's unit roundoff u (2^-24 for the FP32-accurate factor): plain
+// refinement contracts while kappa_1 u stays below kGmresAbove (kappa_1
+// overestimates the 2-norm condition that governs the contraction, by up to
+// ~sqrt(n) on the matrices measured), GMRES-IR preconditioned by the same
+// factor beyond that.
+constexpr double kFactorU = 5.9604644775390625e-08;
+constexpr double kGmresAbove = 50.0;
+
 int dposv_mixed_core_impl(egpu_context* h, int uplo, int n, int nrhs, const double* A, long long lda, const double* B,
                      long long ldb, double* X, long long ldx, int max_iter, double tol, int* iters, double* berr) {
   const int nb = h->nb;
@@ -603,6 +671,15 @@ int dposv_mixed_core_impl(egpu_context* h, int uplo, int n, int nrhs, const doub
   int it = 0;
   double e = INFINITY, e_prev = INFINITY;
   h->gmres_inner = 0;
+  h->mixed_kappa = -1.0;
+  bool to_gmres = false;
+  double* V = reinterpret_cast<double*>(ws + L.gv);  // the GMRES basis is free until GMRES-IR runs
+  auto estimate = [&]() -> int {
+    TRY(cond1_estimate(h, n, Lf, lds, Winv, fl, anorm, V, &h->mixed_kappa));
+    to_gmres = h->mixed_kappa * kFactorU > kGmresAbove;
+    return EGPU_OK;
+  };
+  if (h->mixed_policy == 1) TRY(estimate());
   for (;;) {
     copy_cols_kernel<<<cgrid, 256, 0, st>>>(n, nrhs, B, ldb, R, lds, 0);
     count_launch();
@@ -612,7 +689,11 @@ int dposv_mixed_core_impl(egpu_context* h, int uplo, int n, int nrhs, const doub
     TRY(rg);
     TRY(mixed_berr(h, n, nrhs, R, Xw, B, ldb, lds, anorm, norms + n, &e));
     if (e <= tol || it >= max_iter || !std::isfinite(e)) break;
-    // slow contraction (the factor is too far from A): continue with GMRES-IR below
+    // the condition estimate sends ill-conditioned systems to GMRES-IR: at
+    // once (policy 1), or when the first correction contracted slowly
+    if (h->mixed_policy == 0 && it == 1 && e > 0.2 * e_prev && h->mixed_kappa < 0) TRY(estimate());
+    if (to_gmres) break;
+    // a safety net for estimates that were too low: slow contraction later on
     if (it >= 2 && e > 0.25 * e_prev) break;
     e_prev = e;
     TRY(mixed_solve(h, n, nrhs, Lf, lds, Winv, R, fl));
@@ -671,6 +752,18 @@ extern "C" int egpu_dposv_mixed(egpu_handle h, int uplo, int n, int nrhs, const 
 }
 
 extern "C" int egpu_mixed_gmres_iterations(egpu_handle h) { return h ? h->gmres_inner : -1; }
+
+extern "C" int egpu_set_mixed_policy(egpu_handle h, int policy) {
+  if (!h || policy < 0 || policy > 1) return EGPU_ERR_ARG;
+  h->mixed_policy = policy;
+  return EGPU_OK;
+}
+
+extern "C" int egpu_mixed_condition_estimate(egpu_handle h, double* kappa1) {
+  if (!h || !kappa1) return EGPU_ERR_ARG;
+  *kappa1 = h->mixed_kappa;
+  return EGPU_OK;
+}
 
 // Testing entry for the tcgen05 engine: C (FP32) = alpha A B^T + beta C with
 // A (M x K) and B (N x K) given column-major in FP64 and split into TF32 parts.

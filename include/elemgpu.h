@@ -243,6 +243,19 @@ EGPU_API int egpu_dposv_mixed(egpu_handle h, int uplo, int n, int nrhs, const do
  * corrections count in *iters. */
 EGPU_API int egpu_mixed_gmres_iterations(egpu_handle h);
 
+/* Refinement policy of egpu_dposv_mixed (no counterpart in the reference):
+ * 0 (default) adaptive -- plain iterative refinement, and when the first
+ * correction contracts slowly a 1-norm condition estimate of A (Hager's method
+ * with A^-1 applied through the low-precision factor) decides between
+ * continuing and GMRES-IR; 1 -- the estimate runs after every factorization
+ * and an ill-conditioned A goes to GMRES-IR at once.  A matrix the
+ * FP32-accurate factorization reports not numerically HPD is refactored with
+ * FP64 panel solves (see egpu_dposv_mixed) before any refinement. */
+EGPU_API int egpu_set_mixed_policy(egpu_handle h, int policy);
+/* The last mixed solve's 1-norm condition estimate kappa_1(A) = ||A||_1
+ * ||A^-1||_1 (-1 when that solve did not need one). */
+EGPU_API int egpu_mixed_condition_estimate(egpu_handle h, double* kappa1);
+
 /* Host-memory form of egpu_dposv_mixed (A, B, X in host memory). */
 EGPU_API int egpu_host_dposv_mixed(egpu_handle h, int uplo, int n, int nrhs, const double* A, int lda,
                                    const double* B, int ldb, double* X, int ldx, int max_iter, double tol,

@@ -168,3 +168,39 @@ def test_sweep32_solve_matches_fp64_triangular_solve(handle, n, nrhs, trans):
         ref = torch.linalg.solve_triangular(L64.t() if trans else L64, B, upper=bool(trans))
     err = float((X - ref).abs().max() / ref.abs().max())
     assert err <= 2e-5, err
+
+
+@pytest.mark.parametrize("kappa", [1e4, 1e8])
+def test_condition_estimate_picks_the_refinement_mode(handle, kappa):
+    # policy 1: Hager's 1-norm estimate after the factorization picks plain
+    # refinement (kappa 1e4) or GMRES-IR (kappa 1e8); both reach backward
+    # error <= 1e-14 and the oracle's FP64 solution to kappa * 1e-13
+    n, k = 1024, 4
+    A = inputs.spd_spectrum(n, kappa, 33)
+    B = inputs.normal(n, k, 34)
+    handle.set_mixed_policy(1)
+    try:
+        X, iters, berr = handle.hpd_solve_mixed(eg.colmajor_cuda(A), eg.colmajor_cuda(B), eg.LOWER, 30, 1e-14)
+        est = handle.mixed_condition_estimate()
+        gm = handle.mixed_gmres_iterations()
+    finally:
+        handle.set_mixed_policy(0)
+    X = X.cpu().numpy()
+    k1 = np.abs(A).sum(0).max() * np.abs(np.linalg.inv(A)).sum(0).max()
+    assert k1 / 10 <= est <= k1 * 10, (est, k1)
+    assert (gm > 0) == (kappa >= 1e8), (gm, est)
+    assert berr <= 1e-14 and _berr(A, X, B) <= 1e-14
+    _, Xref, st = orc.hpd_solve(A, B, eg.LOWER, nb=128)
+    assert st == 0
+    assert np.abs(X - Xref).max() <= kappa * 1e-13 * np.abs(Xref).max()
+
+
+def test_condition_estimate_skipped_when_refinement_contracts(handle):
+    # the default adaptive policy estimates nothing for a well-conditioned A
+    n = 800
+    A = inputs.spd_spectrum(n, 1e3, 35)
+    B = inputs.normal(n, 2, 36)
+    X, iters, berr = handle.hpd_solve_mixed(eg.colmajor_cuda(A), eg.colmajor_cuda(B), eg.LOWER, 30, 1e-14)
+    assert berr <= 1e-14
+    assert handle.mixed_condition_estimate() == -1.0
+    assert handle.mixed_gmres_iterations() == 0
