@@ -121,6 +121,8 @@ def _declare(L):
         "egpu_host_dposv_mixed": ([H, I, I, I, P, I, P, I, P, I, I, D, P, P], I),
         "egpu_mixed_gmres_iterations": ([H], I),
         "egpu_set_mixed_policy": ([H, I], I),
+        "egpu_dgesv_mixed": ([H, I, I, P, I, P, I, P, I, I, D, P, P], I),
+        "egpu_mixed_mode": ([H], I),
         "egpu_mixed_condition_estimate": ([H, P], I),
         "egpu_batch_plan_create": ([H, I, I, P, P, P, P, P, P, P], I),
         "egpu_batch_plan_run": ([P, P], I),
@@ -731,6 +733,31 @@ class Handle:
             raise ElemGPUError(f"refinement did not reach {tol:g} in {it.value} corrections (berr {be.value:.3e})")
         _check(rc)
         return X, it.value, be.value
+
+    def gaussian_elimination_mixed(self, A, B, max_iter=30, tol=1e-14):
+        """Mixed-precision GaussianElimination: returns (X, corrections,
+        backward error); A and B (column-major float64 CUDA tensors) are left
+        unchanged."""
+        import torch
+        self._bind_stream()
+        nrhs = B.shape[1] if B.dim() > 1 else 1
+        X = empty_colmajor(A.shape[0], nrhs, torch.float64, A.device)
+        it = ctypes.c_int(0)
+        be = ctypes.c_double(0.0)
+        rc = lib().egpu_dgesv_mixed(self._h, A.shape[0], nrhs, _ptr(A), _ld(A), _ptr(B), _ld(B), _ptr(X), _ld(X),
+                                    max_iter, tol, ctypes.byref(it), ctypes.byref(be))
+        if rc == NO_CONVERGENCE:
+            raise ElemGPUError(f"refinement did not reach {tol:g} in {it.value} corrections (berr {be.value:.3e})")
+        if rc == SINGULAR:
+            info = ctypes.c_int(0)
+            lib().egpu_get_status(self._h, ctypes.byref(info))
+            raise SingularMatrixError(info.value)
+        _check(rc)
+        return X, it.value, be.value
+
+    def mixed_mode(self) -> int:
+        """How the last mixed solve finished: 0 refinement, 1 GMRES-IR, 2 FP64 factors."""
+        return int(lib().egpu_mixed_mode(self._h))
 
     def set_mixed_policy(self, policy: int):
         """0: adaptive (condition estimate only when refinement contracts

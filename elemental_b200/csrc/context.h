@@ -85,7 +85,8 @@ struct egpu_context {
   // mixed solve: 0 adaptive (condition estimate when the first correction
   // contracts slowly), 1 estimate after every factorization
   int mixed_policy = 0;
-  double mixed_kappa = -1.0;  // last 1-norm condition estimate (-1: none)
+  double mixed_kappa = -1.0;
+  int mixed_mode = 0;  // how the last mixed solve finished: 0 refinement, 1 GMRES-IR, 2 FP64 factors  // last 1-norm condition estimate (-1: none)
 };
 
 struct DeviceGuard {

@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <functional>
 
 #include "../../include/elemgpu.h"
 #include "common.cuh"
@@ -76,6 +77,34 @@ int launch_trsm_skinny(cudaStream_t st, int bwd, int amode, int n, int nrhs, con
 // 16-byte aligned with even leading dimensions, else EGPU_ERR_UNSUPPORTED.
 int launch_dgemm_skinny(cudaStream_t st, int M, int N, int K, double alpha, const double* A, long long lda,
                         const double* B, long long ldb, double* C, long long ldc, int sm_count, DevStatus* status);
+
+// ---- iterative-refinement helpers shared by the mixed solvers (mixed.cu) --
+constexpr int kGmresRestart = 20;  // Krylov vectors per GMRES cycle
+struct GmresWork {
+  double* V;      // kGmresRestart + 1 basis blocks of lds x nrhs
+  double* W;      // work block
+  double* coef;   // (kGmresRestart + 2) x nrhs device coefficients
+  double* dots;   // device scratch for dot products ((kGmresRestart + 1) x nrhs)
+};
+// apply_a(V, W): W := A V (n x nrhs blocks, ld lds); precond(W): W := M^-1 W.
+using BlockOp = std::function<int(const double*, double*)>;
+using BlockSolve = std::function<int(double*)>;
+// One GMRES-IR correction: GMRES on M^-1 A d = M^-1 r (one basis per
+// right-hand side, advanced in lockstep); R is consumed, D receives d.
+int gmres_correction(egpu_context* h, int n, int nrhs, long long lds, const BlockOp& apply_a,
+                     const BlockSolve& precond, double* R, double* D, GmresWork& gw, double inner_tol,
+                     int* inner_iters);
+// 1-norm condition estimate (Hager / Higham): solve(V, trans) applies A^-1
+// (trans 0) or A^-T (trans 1) to one device column V.
+int cond1_estimate(egpu_context* h, int n, const std::function<int(double*, int)>& solve, double anorm, double* V,
+                   double* kappa);
+// Normwise backward error max_j ||r_j||_inf / (||A||_inf ||x_j||_inf + ||b_j||_inf);
+// norms: device scratch of 3 nrhs doubles.  Synchronizes.
+int mixed_berr(egpu_context* h, int n, int nrhs, const double* R, const double* Xw, const double* B, long long ldb,
+               long long lds, double anorm, double* norms, double* berr);
+// Y (n x ncols) := X, or += X when add.
+int launch_copy_cols(cudaStream_t st, int n, int ncols, const double* X, long long ldx, double* Y, long long ldy,
+                     int add);
 
 // FP32 super-block sweeps (sweep32.cu), the correction solves of the mixed
 // refinement: sweep32_prepare builds the inverses of the 512 x 512 diagonal

@@ -299,16 +299,39 @@ __global__ void __launch_bounds__(kRpThreads, 1) lu_panel_rp_kernel(int m, int b
     };
     const int ntr = b - c1;  // trailing panel columns
     {
+      // all of a thread's gathers are issued before any is stored, so their
+      // L2 latencies overlap
       const int cc = tid & 127;
-      for (int mv = tid >> 7; mv < 2 * w; mv += 2)
-        if (cc < nout && move_live(mv)) {
+      double g[kRpW];
+#pragma unroll
+      for (int q = 0; q < kRpW; ++q) {
+        const int mv = 2 * q + (tid >> 7);
+        g[q] = 0.0;
+        if (mv < 2 * w && cc < nout && move_live(mv)) {
           const int col = cc < c0 ? cc : cc + w;
           const int d = move_dst(mv);
-          if (!(col >= c1 && d < c1)) MV[mv * 128 + cc] = __ldcg(&A[(long long)col * lda + move_src(mv)]);
+          if (!(col >= c1 && d < c1)) g[q] = __ldcg(&A[(long long)col * lda + move_src(mv)]);
         }
-      for (int idx = tid; idx < w * ntr; idx += kRpThreads) {
-        const int i = idx / ntr, cc = idx - i * ntr;
-        U12[i * 128 + cc] = __ldcg(&A[(long long)(c1 + cc) * lda + c0 + s_pre[i]]);
+      }
+      double gu[kRpW * 128 / kRpThreads];
+#pragma unroll
+      for (int q = 0; q < kRpW * 128 / kRpThreads; ++q) {
+        const int idx = tid + q * kRpThreads, i = idx >> 7, c = idx & 127;
+        gu[q] = (i < w && c < ntr) ? __ldcg(&A[(long long)(c1 + c) * lda + c0 + s_pre[i]]) : 0.0;
+      }
+#pragma unroll
+      for (int q = 0; q < kRpW; ++q) {
+        const int mv = 2 * q + (tid >> 7);
+        if (mv < 2 * w && cc < nout && move_live(mv)) {
+          const int col = cc < c0 ? cc : cc + w;
+          const int d = move_dst(mv);
+          if (!(col >= c1 && d < c1)) MV[mv * 128 + cc] = g[q];
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < kRpW * 128 / kRpThreads; ++q) {
+        const int idx = tid + q * kRpThreads, i = idx >> 7, c = idx & 127;
+        if (i < w && c < ntr) U12[i * 128 + c] = gu[q];
       }
     }
     // every source read (and CTA 0's sub-panel, with L11, written) cluster-wide
@@ -351,19 +374,36 @@ __global__ void __launch_bounds__(kRpThreads, 1) lu_panel_rp_kernel(int m, int b
           }
       }
       __syncthreads();
-      // A[r, c1:b) -= L[r, c0:c1) U12 for own rows r >= c1 (L in registers)
+      // A[r, c1:b) -= L[r, c0:c1) U12 for own rows r >= c1 (L in registers),
+      // kB columns at a time: every load of a batch is in flight before the
+      // first multiply
+      constexpr int kB = RT >= 4 ? 4 : 8;
+      for (int cb = 0; cb < ntr; cb += kB) {
+        double x[RT][kB];
 #pragma unroll
-      for (int s = 0; s < RT; ++s) {
-        const int lr = s * kRpThreads + tid, r = r0 + lr;
-        if (lr < rows && r >= c1) {
-          double* arow = &A[r0 + lr];
-          for (int cc = 0; cc < ntr; ++cc) {
-            double x = __ldcg(&arow[(long long)(c1 + cc) * lda]);
+        for (int s = 0; s < RT; ++s) {
+          const int lr = s * kRpThreads + tid, r = r0 + lr;
 #pragma unroll
-            for (int k = 0; k < kRpW; ++k)
-              if (k < w) x = fma(-v[s][k], U12[k * 128 + cc], x);
-            arow[(long long)(c1 + cc) * lda] = x;
+          for (int q = 0; q < kB; ++q)
+            x[s][q] = (lr < rows && r >= c1 && cb + q < ntr) ? __ldcg(&A[(long long)(c1 + cb + q) * lda + r]) : 0.0;
+        }
+#pragma unroll
+        for (int q = 0; q < kB; ++q) {
+          if (cb + q < ntr) {
+#pragma unroll
+            for (int k = 0; k < kRpW; ++k) {
+              const double u = k < w ? U12[k * 128 + cb + q] : 0.0;
+#pragma unroll
+              for (int s = 0; s < RT; ++s) x[s][q] = fma(-v[s][k], u, x[s][q]);
+            }
           }
+        }
+#pragma unroll
+        for (int s = 0; s < RT; ++s) {
+          const int lr = s * kRpThreads + tid, r = r0 + lr;
+#pragma unroll
+          for (int q = 0; q < kB; ++q)
+            if (lr < rows && r >= c1 && cb + q < ntr) A[(long long)(c1 + cb + q) * lda + r] = x[s][q];
         }
       }
     }

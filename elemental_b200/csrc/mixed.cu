@@ -18,6 +18,7 @@
 // is above the tolerance: r = b - A x (FP64 GEMM on a full symmetric copy of
 // A), d = Lf^-T Lf^-1 r, x += d.
 #include <cmath>
+#include <functional>
 #include <vector>
 
 #include "context.h"
@@ -116,12 +117,12 @@ __global__ void rowsum_abs_kernel(int n, const double* As, long long lds, double
 // Y = X (n x ncols) ; Y += X
 __global__ void copy_cols_kernel(int n, int ncols, const double* X, long long ldx, double* Y, long long ldy,
                                  int add) {
-  const int j = blockIdx.y;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    const double x = X[i + (long long)j * ldx];
-    double* y = &Y[i + (long long)j * ldy];
-    *y = add ? *y + x : x;
-  }
+  for (int j = blockIdx.y; j < ncols; j += gridDim.y)
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+      const double x = X[i + (long long)j * ldx];
+      double* y = &Y[i + (long long)j * ldy];
+      *y = add ? *y + x : x;
+    }
 }
 
 // out[j * nrhs + c] = sum_i V_j[i, c] W[i, c] for j < nv (V_j = V + j * vstride); one block per (j, c)
@@ -163,6 +164,15 @@ __global__ void col_scale_kernel(int n, const double* X, long long ldx, const do
 
 }  // namespace
 
+int launch_copy_cols(cudaStream_t st, int n, int ncols, const double* X, long long ldx, double* Y, long long ldy,
+                     int add) {
+  if (n <= 0 || ncols <= 0) return EGPU_OK;
+  copy_cols_kernel<<<dim3((n + 255) / 256, std::min(ncols, 65535)), 256, 0, st>>>(n, ncols, X, ldx, Y, ldy, add);
+  count_launch();
+  EGPU_CUDA_TRY(cudaGetLastError());
+  return EGPU_OK;
+}
+
 int launch_split_tf32(cudaStream_t st, int rows, int cols, const double* X, long long ldx, float* hi, float* lo,
                       long long ldk, int width) {
   if (rows <= 0 || cols <= 0) return EGPU_OK;
@@ -186,7 +196,6 @@ int launch_split_tf32_f32(cudaStream_t st, int rows, int cols, const float* X, l
   return EGPU_OK;
 }
 
-constexpr int kGmresRestart = 20;  // Krylov vectors per GMRES cycle
 
 // Workspace layout of the mixed solve.
 struct MixedLayout {
@@ -266,7 +275,7 @@ static int mixed_prescale_step(egpu_context* h, cudaStream_t st, int n, int j0, 
 }
 
 // Backward error of the current iterate: max_j ||r_j|| / (||A|| ||x_j|| + ||b_j||), inf-norms.
-static int mixed_berr(egpu_context* h, int n, int nrhs, const double* R, const double* Xw, const double* B,
+int mixed_berr(egpu_context* h, int n, int nrhs, const double* R, const double* Xw, const double* B,
                       long long ldb, long long lds, double anorm, double* norms, double* berr) {
   cudaStream_t st = h->stream;
   colmax_kernel<<<nrhs, 256, 0, st>>>(n, nrhs, R, lds, norms);
@@ -292,15 +301,9 @@ static int mixed_berr(egpu_context* h, int n, int nrhs, const double* R, const d
 // Gram-Schmidt applied twice, Givens rotations on the host.  Stops when every
 // column's preconditioned residual fell below inner_tol times its start, or
 // after kGmresRestart vectors.  R is consumed; D receives the correction.
-struct GmresWork {
-  double* V;      // kGmresRestart + 1 basis blocks of lds x nrhs
-  double* W;      // work block
-  double* coef;   // (kGmresRestart + 2) x nrhs device coefficients
-  double* dots;   // device scratch for dot products ((kGmresRestart + 1) x nrhs)
-};
-static int gmres_correction(egpu_context* h, int n, int nrhs, const double* As, long long lds, const double* Lf,
-                            const double* Winv, SweepFlags& fl, double* R, double* D, GmresWork& gw,
-                            double inner_tol, int* inner_iters) {
+int gmres_correction(egpu_context* h, int n, int nrhs, long long lds, const BlockOp& apply_a,
+                     const BlockSolve& precond, double* R, double* D, GmresWork& gw, double inner_tol,
+                     int* inner_iters) {
   cudaStream_t st = h->stream;
   const long long vs = lds * nrhs;  // stride between basis blocks
   const int m = kGmresRestart;
@@ -339,7 +342,7 @@ static int gmres_correction(egpu_context* h, int n, int nrhs, const double* As, 
     return EGPU_OK;
   };
   // z = M^-1 r, beta = ||z||, V_0 = z / beta
-  TRY(mixed_solve(h, n, nrhs, Lf, lds, Winv, R, fl));
+  TRY(precond(R));
   std::vector<double> beta, inv(nrhs), hv, nrm;
   TRY(self_norms(R, beta));
   for (int c = 0; c < nrhs; ++c) inv[c] = beta[c] > 0.0 ? 1.0 / beta[c] : 0.0;
@@ -353,12 +356,8 @@ static int gmres_correction(egpu_context* h, int n, int nrhs, const double* As, 
   for (int i = 0; i < m; ++i) {
     double* Vi = gw.V + i * vs;
     // W = M^-1 A V_i
-    EGPU_CUDA_TRY(cudaMemsetAsync(gw.W, 0, sizeof(double) * vs, st));
-    int rg = launch_dgemm_skinny(st, n, nrhs, n, 1.0, As, lds, Vi, lds, gw.W, lds, h->sm_count, h->dstatus);
-    if (rg == EGPU_ERR_UNSUPPORTED)
-      rg = launch_dgemm(st, false, true, n, nrhs, n, 1.0, As, lds, Vi, lds, 0.0, gw.W, lds, 0, false, h->dstatus);
-    TRY(rg);
-    TRY(mixed_solve(h, n, nrhs, Lf, lds, Winv, gw.W, fl));
+    TRY(apply_a(Vi, gw.W));
+    TRY(precond(gw.W));
     for (int pass = 0; pass < 2; ++pass) {  // classical Gram-Schmidt, twice
       TRY(dots(i + 1, gw.W, hv));
       TRY(axpy(i + 1, hv, gw.W));
@@ -412,21 +411,21 @@ static int gmres_correction(egpu_context* h, int n, int nrhs, const double* As, 
   return EGPU_OK;
 }
 
-// 1-norm condition estimate of the HPD A from its low-precision factor:
-// kappa_1 = ||A||_1 ||A^-1||_1 with ||A^-1||_1 estimated by Hager's method
-// (W. W. Hager, "Condition estimates", SIAM J. Sci. Stat. Comput. 5, 1984, as
+// 1-norm condition estimate of A from its low-precision factor: kappa_1 =
+// ||A||_1 ||A^-1||_1 with ||A^-1||_1 estimated by Hager's method (W. W.
+// Hager, "Condition estimates", SIAM J. Sci. Stat. Comput. 5, 1984, as
 // refined by N. J. Higham, ACM TOMS 14, 1988: the algorithm of LAPACK's
-// dlacon), with A^-1 applied as the factor's solve (A symmetric, so A^-T =
-// A^-1).  At most 5 iterations of two solves each, plus the closing test with
+// dlacon), with A^-1 and A^-T applied as the factor's solves.  At most 5 iterations of two solves each, plus the closing test with
 // the alternating vector; the small vector logic runs on the host.  V: two
 // work columns of ld lds on the device.
-static int cond1_estimate(egpu_context* h, int n, const double* Lf, long long lds, const double* Winv,
-                          SweepFlags& fl, double anorm, double* V, double* kappa) {
+// solve(V, trans): V := A^-1 V (trans 0) or A^-T V (trans 1), one column.
+int cond1_estimate(egpu_context* h, int n, const std::function<int(double*, int)>& solve, double anorm, double* V,
+                   double* kappa) {
   cudaStream_t st = h->stream;
   std::vector<double> x(n), y(n), z(n), xi(n), xi_old(n, 0.0);
-  auto apply = [&](std::vector<double>& v) -> int {  // v := A^-1 v
+  auto apply = [&](std::vector<double>& v, int trans) -> int {
     EGPU_CUDA_TRY(cudaMemcpyAsync(V, v.data(), sizeof(double) * n, cudaMemcpyHostToDevice, st));
-    TRY(mixed_solve(h, n, 1, Lf, lds, Winv, V, fl));
+    TRY(solve(V, trans));
     EGPU_CUDA_TRY(cudaMemcpyAsync(v.data(), V, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
     EGPU_CUDA_TRY(cudaStreamSynchronize(st));
     return EGPU_OK;
@@ -440,7 +439,7 @@ static int cond1_estimate(egpu_context* h, int n, const double* Lf, long long ld
   double est = 0.0;
   for (int k = 1; k <= 5; ++k) {
     y = x;
-    TRY(apply(y));
+    TRY(apply(y, 0));
     const double ny = norm1(y);
     if (k > 1 && ny <= est) break;  // no increase
     est = ny;
@@ -451,7 +450,7 @@ static int cond1_estimate(egpu_context* h, int n, const double* Lf, long long ld
     }
     if (same) break;  // the sign pattern repeats: converged
     z = xi;
-    TRY(apply(z));
+    TRY(apply(z, 1));
     int j = 0;
     double zx = 0.0;
     for (int i = 0; i < n; ++i) {
@@ -465,7 +464,7 @@ static int cond1_estimate(egpu_context* h, int n, const double* Lf, long long ld
   }
   // the alternating test vector guards against the method's known failures
   for (int i = 0; i < n; ++i) x[i] = (i % 2 ? -1.0 : 1.0) * (1.0 + (n > 1 ? (double)i / (n - 1) : 0.0));
-  TRY(apply(x));
+  TRY(apply(x, 0));
   est = std::max(est, 2.0 * norm1(x) / (3.0 * n));
   *kappa = anorm * est;
   return EGPU_OK;
@@ -486,6 +485,7 @@ int dposv_mixed_core_impl(egpu_context* h, int uplo, int n, int nrhs, const doub
   cudaStream_t st = h->stream;
   const MixedLayout L = mixed_layout(n, nrhs, nb);
   h->gmres_inner = 0;
+  h->mixed_mode = 0;
   TRY(ensure_ws(h, L.total + 4096));
   unsigned char* ws = static_cast<unsigned char*>(h->ws);
   double* As = reinterpret_cast<double*>(ws + L.as);
@@ -671,11 +671,16 @@ int dposv_mixed_core_impl(egpu_context* h, int uplo, int n, int nrhs, const doub
   int it = 0;
   double e = INFINITY, e_prev = INFINITY;
   h->gmres_inner = 0;
+  h->mixed_mode = 0;
   h->mixed_kappa = -1.0;
   bool to_gmres = false;
   double* V = reinterpret_cast<double*>(ws + L.gv);  // the GMRES basis is free until GMRES-IR runs
   auto estimate = [&]() -> int {
-    TRY(cond1_estimate(h, n, Lf, lds, Winv, fl, anorm, V, &h->mixed_kappa));
+    // A symmetric: A^-T = A^-1
+    const std::function<int(double*, int)> solve = [&](double* v, int) -> int {
+      return mixed_solve(h, n, 1, Lf, lds, Winv, v, fl);
+    };
+    TRY(cond1_estimate(h, n, solve, anorm, V, &h->mixed_kappa));
     to_gmres = h->mixed_kappa * kFactorU > kGmresAbove;
     return EGPU_OK;
   };
@@ -710,7 +715,15 @@ int dposv_mixed_core_impl(egpu_context* h, int uplo, int n, int nrhs, const doub
     int inner = 0;
     double e_best = e;
     while (it < max_iter) {
-      TRY(gmres_correction(h, n, nrhs, As, lds, Lf, Winv, fl, R, R, gw, 1e-10, &inner));
+      const BlockOp apply_a = [&](const double* Vi, double* Wo) -> int {
+        EGPU_CUDA_TRY(cudaMemsetAsync(Wo, 0, sizeof(double) * lds * nrhs, st));
+        int rg = launch_dgemm_skinny(st, n, nrhs, n, 1.0, As, lds, Vi, lds, Wo, lds, h->sm_count, h->dstatus);
+        if (rg == EGPU_ERR_UNSUPPORTED)
+          rg = launch_dgemm(st, false, true, n, nrhs, n, 1.0, As, lds, Vi, lds, 0.0, Wo, lds, 0, false, h->dstatus);
+        return rg;
+      };
+      const BlockSolve precond = [&](double* Wo) -> int { return mixed_solve(h, n, nrhs, Lf, lds, Winv, Wo, fl); };
+      TRY(gmres_correction(h, n, nrhs, lds, apply_a, precond, R, R, gw, 1e-10, &inner));
       copy_cols_kernel<<<cgrid, 256, 0, st>>>(n, nrhs, R, lds, Xw, lds, 1);
       count_launch();
       ++it;
@@ -725,6 +738,7 @@ int dposv_mixed_core_impl(egpu_context* h, int uplo, int n, int nrhs, const doub
       e_best = e;
     }
     h->gmres_inner = inner;
+    h->mixed_mode = 1;
   }
   copy_cols_kernel<<<cgrid, 256, 0, st>>>(n, nrhs, Xw, lds, X, ldx, 0);
   count_launch();
@@ -758,6 +772,8 @@ extern "C" int egpu_set_mixed_policy(egpu_handle h, int policy) {
   h->mixed_policy = policy;
   return EGPU_OK;
 }
+
+extern "C" int egpu_mixed_mode(egpu_handle h) { return h ? h->mixed_mode : -1; }
 
 extern "C" int egpu_mixed_condition_estimate(egpu_handle h, double* kappa1) {
   if (!h || !kappa1) return EGPU_ERR_ARG;

@@ -52,6 +52,16 @@ def spd_spectrum(n: int, kappa: float, seed: int, device: str | None = None):
     return np.asfortranarray(a.cpu().numpy())
 
 
+def general_spectrum(n: int, kappa: float, seed: int) -> np.ndarray:
+    """A nonsymmetric A = U diag(s) V^T (U, V orthogonal from the QR of two
+    Gaussian matrices, s log-spaced from 1 to 1/kappa): 2-norm condition kappa."""
+    r = rng(seed)
+    u, _ = np.linalg.qr(r.standard_normal((n, n)))
+    v, _ = np.linalg.qr(r.standard_normal((n, n)))
+    s = np.logspace(0.0, -np.log10(kappa), n)
+    return np.asfortranarray((u * s) @ v.T)
+
+
 def spd_spectrum_torch(n: int, kappa: float, seed: int, device: str):
     """Same matrix as spd_spectrum(..., device=device), left on the device as a
     column-major torch tensor."""

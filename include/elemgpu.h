@@ -243,7 +243,25 @@ EGPU_API int egpu_dposv_mixed(egpu_handle h, int uplo, int n, int nrhs, const do
  * corrections count in *iters. */
 EGPU_API int egpu_mixed_gmres_iterations(egpu_handle h);
 
-/* Refinement policy of egpu_dposv_mixed (no counterpart in the reference):
+/* Mixed-precision GaussianElimination (GaussianElimination.hpp:216-232 and
+ * lu::SolveAfter, LU/SolveAfter.hpp:101-146, compute the same x; no
+ * counterpart in the reference, which factors in the working precision only):
+ * LU with partial pivoting of an FP32 copy of A -- each 128-wide panel
+ * factored in FP64 by the pivoting panel kernel (lu::Panel, LU/Panel.hpp:19-89),
+ * the row-panel solve and trailing update on the tcgen05 tensor cores in
+ * TF32 x 3 split precision -- then iterative refinement with FP64 residuals
+ * against A and corrections through the factors (GMRES-IR preconditioned by
+ * them when plain refinement contracts slowly, or under policy 1 when the
+ * 1-norm condition estimate asks for it; the FP64 LU of a copy of A when the
+ * estimate says the FP32 factors cannot precondition, or GMRES-IR stagnates).  A and B are inputs only (an A
+ * that is not 16-byte aligned with even lda is copied once); X receives the solution; nrhs <= 64.  Returns EGPU_OK,
+ * EGPU_SINGULAR (an exact zero pivot of the low-precision factorization;
+ * egpu_get_status gives its column), EGPU_NO_CONVERGENCE or an error.
+ * Synchronous. */
+EGPU_API int egpu_dgesv_mixed(egpu_handle h, int n, int nrhs, const double* dA, int lda, const double* dB, int ldb,
+                              double* dX, int ldx, int max_iter, double tol, int* iters, double* berr);
+
+/* Refinement policy of egpu_dposv_mixed and egpu_dgesv_mixed (no counterpart in the reference):
  * 0 (default) adaptive -- plain iterative refinement, and when the first
  * correction contracts slowly a 1-norm condition estimate of A (Hager's method
  * with A^-1 applied through the low-precision factor) decides between
@@ -255,6 +273,10 @@ EGPU_API int egpu_set_mixed_policy(egpu_handle h, int policy);
 /* The last mixed solve's 1-norm condition estimate kappa_1(A) = ||A||_1
  * ||A^-1||_1 (-1 when that solve did not need one). */
 EGPU_API int egpu_mixed_condition_estimate(egpu_handle h, double* kappa1);
+/* How the last mixed solve finished: 0 plain refinement, 1 GMRES-IR, 2 the
+ * FP64 factorization (egpu_dgesv_mixed only: taken when the condition estimate
+ * puts kappa_1 * 2^-24 above 1e3, or when GMRES-IR stagnates); -1 no handle. */
+EGPU_API int egpu_mixed_mode(egpu_handle h);
 
 /* Host-memory form of egpu_dposv_mixed (A, B, X in host memory). */
 EGPU_API int egpu_host_dposv_mixed(egpu_handle h, int uplo, int n, int nrhs, const double* A, int lda,

@@ -204,3 +204,76 @@ def test_condition_estimate_skipped_when_refinement_contracts(handle):
     assert berr <= 1e-14
     assert handle.mixed_condition_estimate() == -1.0
     assert handle.mixed_gmres_iterations() == 0
+
+
+def _ge_oracle(A, B):
+    _, Xr, st = orc.gaussian_elimination(A, B, 128)
+    assert st == 0
+    return Xr
+
+
+@pytest.mark.parametrize("n,nrhs", [(1000, 4), (777, 1), (2048, 16), (129, 3)])
+def test_gaussian_elimination_mixed_well_conditioned(handle, n, nrhs):
+    A = inputs.uniform(n, n, 71)  # the reference's Uniform test matrix
+    B = inputs.normal(n, nrhs, 72)
+    dA = eg.colmajor_cuda(A)
+    dB = eg.colmajor_cuda(B)
+    X, it, be = handle.gaussian_elimination_mixed(dA, dB)
+    Xg = X.cpu().numpy()
+    assert be <= 1e-14, (it, be)
+    assert _berr(A, Xg, B) <= 1e-14
+    # A and B are inputs only
+    assert np.array_equal(dA.cpu().numpy(), A) and np.array_equal(dB.cpu().numpy(), B)
+    Xr = _ge_oracle(A, B)
+    kappa = np.linalg.cond(A, 1)
+    assert np.abs(Xg - Xr).max() <= kappa * 1e-13 * np.abs(Xr).max()
+
+
+@pytest.mark.parametrize("kind,kappa,mode", [("general", 1e4, 0), ("general", 3e7, 1), ("general", 1e8, 2),
+                                              ("spd", 1e8, 1)])
+@pytest.mark.parametrize("policy", [0, 1])
+def test_gaussian_elimination_mixed_ill_conditioned(handle, kind, kappa, mode, policy):
+    # nonsymmetric U diag(s) V^T and the serving stream's Q diag(s) Q^T: plain
+    # refinement, GMRES-IR, or (when the estimate says the FP32 factors cannot
+    # precondition) the FP64 factors; every route reaches backward error 1e-14
+    n, nrhs = 1024, 8
+    A = inputs.general_spectrum(n, kappa, 73) if kind == "general" else inputs.spd_spectrum(n, kappa, 73)
+    B = inputs.normal(n, nrhs, 74)
+    handle.set_mixed_policy(policy)
+    try:
+        X, it, be = handle.gaussian_elimination_mixed(eg.colmajor_cuda(A), eg.colmajor_cuda(B))
+        est = handle.mixed_condition_estimate()
+        got = handle.mixed_mode()
+    finally:
+        handle.set_mixed_policy(0)
+    Xg = X.cpu().numpy()
+    assert be <= 1e-14, (it, be, est)
+    assert _berr(A, Xg, B) <= 1e-14
+    assert got == mode, (got, est)
+    Xr = _ge_oracle(A, B)
+    assert np.abs(Xg - Xr).max() <= kappa * 1e-13 * np.abs(Xr).max()
+    if policy == 1 and mode < 2:
+        k1 = np.linalg.cond(A, 1)
+        assert k1 / 10 <= est <= k1 * 10, (est, k1)
+
+
+def test_gaussian_elimination_mixed_singular(handle):
+    n = 300
+    A = inputs.uniform(n, n, 75)
+    A[:, 200] = 0.0
+    with pytest.raises(eg.SingularMatrixError):
+        handle.gaussian_elimination_mixed(eg.colmajor_cuda(A), eg.colmajor_cuda(inputs.normal(n, 2, 76)))
+
+
+def test_gaussian_elimination_mixed_n8192(handle):
+    # the LU benchmark's size: backward error and the FP64 solve's x
+    n, k = 8192, 32
+    A = inputs.uniform(n, n, 77)
+    B = inputs.normal(n, k, 78)
+    dA, dB = eg.colmajor_cuda(A), eg.colmajor_cuda(B)
+    X, it, be = handle.gaussian_elimination_mixed(dA, dB)
+    assert be <= 1e-14, (it, be)
+    A64, X64 = dA.clone(), dB.clone()
+    handle.gaussian_elimination(A64, X64)  # FP64 LU: A64 := its factors, X64 := x
+    rel = (X - X64).abs().max().item() / X64.abs().max().item()
+    assert rel <= 1e-9, rel
