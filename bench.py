@@ -914,8 +914,11 @@ def kernel_case(args):
     mixed-precision HPD solve, 'tc' = the tcgen05 trailing update alone,
     'chol' = one plain FP64 Cholesky (warm-up call first); 'inverse',
     'hpdinverse', 'trtri', 'ldl', 'revchol', 'det' time those entry points
-    (best of three, flops: 2n^3, n^3, n^3/3, n^3/3, n^3/3, 2n^3/3).  --k sets
-    the inner dimension of 'update' and 'gemm' (default 128)."""
+    (best of three, flops: 2n^3, n^3, n^3/3, n^3/3, n^3/3, 2n^3/3); 'sweep32'
+    = the FP32 solve sweeps alone; 'batched' = one launch of each batched
+    kernel over n systems of the C4 shapes; 'mixed_lu' = one mixed-precision
+    GaussianElimination.  --k sets the inner dimension of 'update' and 'gemm'
+    (default 128)."""
     import torch
     import elemental_b200 as eg
     from elemental_b200 import inputs
@@ -1042,6 +1045,45 @@ def kernel_case(args):
                           "triangle_gbs": 2 * 2.0 * n * n / ms / 1e6,
                           "prepare_ms": s["other"]["busy_ms"] / max(1, s["other"]["launches"])}))
         return
+    elif args.case == "batched":
+        # one launch of each batched kernel over --n systems of the C4 shapes
+        # (n ~ U{32..512}, 8 RHS): HPD first, then GE; warm-up launch first
+        r = np.random.default_rng(SEED)
+        sizes = [int(x) for x in r.integers(32, 513, n)]
+        def fresh(kind):
+            As = [inputs.spd_spectrum_torch(m, 1e3, SEED + i, "cuda") if kind == 0 else
+                  eg.colmajor_cuda(torch.rand(m, m, dtype=torch.float64, device="cuda") * 2 - 1)
+                  for i, m in enumerate(sizes)]
+            Bs = [eg.colmajor_cuda(torch.randn(m, 8, dtype=torch.float64, device="cuda")) for m in sizes]
+            return As, Bs
+        for kind, solve in ((0, h.hpd_solve_batched), (1, h.gaussian_elimination_batched)):
+            solve(*fresh(kind))  # warm-up
+            As, Bs = fresh(kind)
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            info = solve(As, Bs)
+            e1.record()
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1)
+            fl = sum((m ** 3 / 3 if kind == 0 else 2 * m ** 3 / 3) + 2 * m * m * 8 for m in sizes)
+            print(json.dumps({"case": "batched", "kind": ["hpd", "ge"][kind], "count": n, "ms": ms,
+                              "tflops": fl / ms / 1e9, "failed": int(sum(1 for v in info if v))}))
+        return
+    elif args.case == "mixed_lu":
+        # one mixed-precision GaussianElimination at order n, 32 RHS, U[-1,1]
+        A = eg.colmajor_cuda(inputs.uniform(n, n, SEED))
+        B = eg.colmajor_cuda(inputs.normal(n, 32, SEED + 1))
+        h.gaussian_elimination_mixed(A, B)  # warm-up
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        X, it, be = h.gaussian_elimination_mixed(A, B)
+        e1.record()
+        torch.cuda.synchronize()
+        print(json.dumps({"case": "mixed_lu", "n": n, "ms": e0.elapsed_time(e1), "corrections": it, "berr": be,
+                          "mode": h.mixed_mode()}))
+        return
     elif args.case in ("inverse", "hpdinverse", "trtri", "ldl", "revchol", "det"):
         # the next rows (inverses, determinants, LDL, ReverseCholesky) at order
         # n: one warm-up call, then three timed calls on fresh copies of A
@@ -1104,7 +1146,8 @@ def main():
                     help="time only --workload (by default the mixed line also carries the other configurations)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline legs")
     ap.add_argument("--case", choices=["update", "gemm", "panel", "diag", "peaks", "mixed", "tc", "chol", "inverse",
-                                       "hpdinverse", "trtri", "ldl", "revchol", "det", "sweep32"],
+                                       "hpdinverse", "trtri", "ldl", "revchol", "det", "sweep32", "batched",
+                                       "mixed_lu"],
                     default=None,
                     help="run one launch of one kernel class (profiling)")
     ap.add_argument("--n", type=int, default=6144, help="size for --case")

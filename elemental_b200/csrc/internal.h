@@ -155,6 +155,10 @@ int launch_apply_composed(cudaStream_t st, int m, int ncols, double* A, long lon
 // Apply sequential swaps p[0..np) (absolute rows) to rows of A (m x n).
 int launch_laswp_seq(cudaStream_t st, int inverse, int m, int n, double* A, long long lda, const int* p, int np,
                      int* perm_scratch);
+// The two halves of it: perm := the sequential swaps composed (row r ends up
+// holding original row perm[r]); A := A[perm, :] through tmp (m x n doubles).
+int launch_compose_perm(cudaStream_t st, int inverse, int m, const int* p, int np, int* perm);
+int launch_permute_rows(cudaStream_t st, int m, int n, const int* perm, double* A, long long lda, double* tmp);
 
 // Unpivoted LU of a b x b diagonal block in place; W receives inv(unit L11),
 // W2 receives inv(U11).

@@ -335,23 +335,38 @@ int launch_apply_composed(cudaStream_t st, int m, int ncols, double* A, long lon
 }
 
 // Compose sequential swaps i <-> p[i] (forward, or reverse for the inverse)
-// into perm: after the swaps, row r holds original row perm[r].
-__global__ void compose_perm_kernel(int inverse, int m, const int* p, int np, int* perm) {
-  for (int r = threadIdx.x; r < m; r += blockDim.x) perm[r] = r;
+// into perm: after the swaps, row r holds original row perm[r].  The swaps
+// are a dependent chain (one thread); with `smem` the permutation and the
+// pivots are staged in shared memory first, so each step is a few shared
+// accesses instead of dependent global round trips.
+__global__ void compose_perm_kernel(int inverse, int m, const int* p, int np, int* perm, int smem) {
+  extern __shared__ int sperm[];
+  int* q = smem ? sperm : perm;
+  int* sp = sperm + m;
+  for (int r = threadIdx.x; r < m; r += blockDim.x) q[r] = r;
+  if (smem)
+    for (int i = threadIdx.x; i < np; i += blockDim.x) sp[i] = p[i];
   __syncthreads();
+  const int* pp = smem ? sp : p;
   if (threadIdx.x == 0) {
+    // a pivot outside [0, m) (caller data) is skipped, never followed
     if (!inverse) {
       for (int i = 0; i < np; ++i) {
-        const int k = p[i];
-        const int t = perm[i]; perm[i] = perm[k]; perm[k] = t;
+        const int k = pp[i];
+        if ((unsigned)k >= (unsigned)m || i >= m) continue;
+        const int t = q[i]; q[i] = q[k]; q[k] = t;
       }
     } else {
       for (int i = np - 1; i >= 0; --i) {
-        const int k = p[i];
-        const int t = perm[i]; perm[i] = perm[k]; perm[k] = t;
+        const int k = pp[i];
+        if ((unsigned)k >= (unsigned)m || i >= m) continue;
+        const int t = q[i]; q[i] = q[k]; q[k] = t;
       }
     }
   }
+  __syncthreads();
+  if (smem)
+    for (int r = threadIdx.x; r < m; r += blockDim.x) perm[r] = q[r];
 }
 
 // dst[r, c] = src[perm[r], c]
@@ -365,15 +380,25 @@ __global__ void gather_rows_kernel(int m, int n, const int* perm, const double* 
   }
 }
 
-// perm_scratch: int[m] followed by double[m * n] (8-byte aligned after m ints
-// rounded up to an even count).
-int launch_laswp_seq(cudaStream_t st, int inverse, int m, int n, double* A, long long lda, const int* p, int np,
-                     int* perm_scratch) {
-  if (m <= 0 || n <= 0 || np <= 0) return EGPU_OK;
-  int* perm = perm_scratch;
-  double* tmp = reinterpret_cast<double*>(perm_scratch + ((m + 1) & ~1));
-  compose_perm_kernel<<<1, 1024, 0, st>>>(inverse, m, p, np, perm);
+int launch_compose_perm(cudaStream_t st, int inverse, int m, const int* p, int np, int* perm) {
+  if (m <= 0) return EGPU_OK;
+  const size_t sbytes = sizeof(int) * ((size_t)m + np);
+  const bool smem = sbytes <= 200 * 1024;
+  static int attr_dev_mask = 0;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (smem && dev < 31 && !(attr_dev_mask & (1 << dev))) {
+    EGPU_CUDA_TRY(cudaFuncSetAttribute(compose_perm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    attr_dev_mask |= 1 << dev;
+  }
+  compose_perm_kernel<<<1, 1024, smem ? sbytes : 0, st>>>(inverse, m, p, np, perm, smem ? 1 : 0);
   count_launch();
+  EGPU_CUDA_TRY(cudaGetLastError());
+  return EGPU_OK;
+}
+
+int launch_permute_rows(cudaStream_t st, int m, int n, const int* perm, double* A, long long lda, double* tmp) {
+  if (m <= 0 || n <= 0) return EGPU_OK;
   const long long total = (long long)m * n;
   const int blocks = (int)std::min<long long>((total + 255) / 256, 148 * 16);
   gather_rows_kernel<<<blocks, 256, 0, st>>>(m, n, perm, A, lda, tmp, m);
@@ -384,6 +409,18 @@ int launch_laswp_seq(cudaStream_t st, int inverse, int m, int n, double* A, long
     return EGPU_ERR_CUDA;
   }
   return launch_copy(st, m, n, tmp, m, A, lda);
+}
+
+// perm_scratch: int[m] followed by double[m * n] (8-byte aligned after m ints
+// rounded up to an even count).
+int launch_laswp_seq(cudaStream_t st, int inverse, int m, int n, double* A, long long lda, const int* p, int np,
+                     int* perm_scratch) {
+  if (m <= 0 || n <= 0 || np <= 0) return EGPU_OK;
+  int* perm = perm_scratch;
+  double* tmp = reinterpret_cast<double*>(perm_scratch + ((m + 1) & ~1));
+  const int rc = launch_compose_perm(st, inverse, m, p, np, perm);
+  if (rc != EGPU_OK) return rc;
+  return launch_permute_rows(st, m, n, perm, A, lda, tmp);
 }
 
 }  // namespace egpu

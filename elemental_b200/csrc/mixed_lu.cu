@@ -113,34 +113,66 @@ __global__ void abs_sums_kernel(int n, const double* A, long long lda, double* r
   }
 }
 
+// UT := the transpose of Af's upper triangle (32 x 32 tiles through shared
+// memory; only tiles on or above Af's diagonal, so UT's lower triangle is U^T)
+__global__ void transpose_upper_kernel(int n, const float* Af, long long ldf, float* UT) {
+  __shared__ float tile[32][33];
+  const int bi = blockIdx.x, bj = blockIdx.y;  // tile row / column of Af
+  if (bj < bi) return;
+  const int tx = threadIdx.x, ty = threadIdx.y;  // 32 x 8
+  for (int q = ty; q < 32; q += 8) {
+    const int r = bi * 32 + tx, c = bj * 32 + q;
+    tile[q][tx] = (r < n && c < n) ? Af[r + (long long)c * ldf] : 0.f;
+  }
+  __syncthreads();
+  for (int q = ty; q < 32; q += 8) {
+    const int r = bj * 32 + tx, c = bi * 32 + q;  // UT(r, c) = Af(c, r)
+    if (r < n && c < n) UT[r + (long long)c * ldf] = tile[tx][q];
+  }
+}
+
+// The 128 x 128 diagonal blocks of the unit-lower L and of U^T, widened to
+// FP64 and packed (block q at q * 128 * 129, ld 128) for the batched inverse.
+__global__ void diag_blocks_kernel(int n, const float* Af, long long ldf, double* DL, double* DU) {
+  const int q = blockIdx.x, b = min(128, n - q * 128);
+  double* dl = DL + (long long)q * 128 * 129;
+  double* du = DU + (long long)q * 128 * 129;
+  const long long o = (long long)q * 128;
+  for (int e = threadIdx.x; e < b * b; e += blockDim.x) {
+    const int i = e % b, j = e / b;
+    dl[i + j * 128] = i >= j ? (double)Af[(o + i) + (o + j) * ldf] : 0.0;
+    du[i + j * 128] = i >= j ? (double)Af[(o + j) + (o + i) * ldf] : 0.0;
+  }
+}
+
 }  // namespace
 
 // Workspace of the mixed LU solve.
 struct MixedLuLayout {
   size_t as, af, lu, pan, piv, img, pre, w, scr, wh, wl, bh, bl, lh, ll, winvl, winvu, flags, perm, xw, r, norms, gv, gw, gc,
-      total;
+      ut, dl, du, winvut, swl, swu, permi, total;
   long long ldf, lds, ldk;
 };
 
-static MixedLuLayout mixed_lu_layout(int n, int nrhs, int nb, int sm_count, bool copy_a) {
+static MixedLuLayout mixed_lu_layout(int n, int nrhs, int nb, int fb, int sm_count, bool copy_a) {
   MixedLuLayout L;
   L.lds = ld_aligned(n);
   L.ldf = L.lds;
-  L.ldk = ((long long)nb + 31) / 32 * 32;
+  L.ldk = ((long long)fb + 31) / 32 * 32;
   size_t off = 0;
   auto take = [&](size_t bytes) { off = (off + 1023) & ~size_t(1023); size_t o = off; off += bytes; return o; };
   const int r = std::max(nrhs, 1);
   L.as = copy_a ? take(sizeof(double) * L.lds * n) : 0;  // an aligned copy of A for the FP64 products
   L.af = take(sizeof(float) * L.ldf * n);
   L.lu = take(sizeof(double) * L.lds * n);                    // the widened factors (solves)
-  L.pan = take(sizeof(double) * L.lds * nb);                   // one FP64 panel
+  L.pan = take(sizeof(double) * L.lds * fb);                   // one FP64 panel
   L.piv = take(sizeof(int) * (size_t)n);
-  L.img = take(sizeof(int) * (size_t)nb);
-  L.pre = take(sizeof(int) * (size_t)nb);
-  L.w = take(sizeof(double) * (size_t)nb * nb);
-  L.scr = take(lu_panel_scratch_bytes(n, nb, sm_count));
-  L.wh = take(sizeof(float) * (size_t)nb * L.ldk);
-  L.wl = take(sizeof(float) * (size_t)nb * L.ldk);
+  L.img = take(sizeof(int) * (size_t)fb);
+  L.pre = take(sizeof(int) * (size_t)fb);
+  L.w = take(sizeof(double) * (size_t)fb * fb);
+  L.scr = take(lu_panel_scratch_bytes(n, fb, sm_count));
+  L.wh = take(sizeof(float) * (size_t)fb * L.ldk);
+  L.wl = take(sizeof(float) * (size_t)fb * L.ldk);
   L.bh = take(sizeof(float) * (size_t)n * L.ldk);
   L.bl = take(sizeof(float) * (size_t)n * L.ldk);
   L.lh = take(sizeof(float) * (size_t)n * L.ldk);
@@ -148,7 +180,17 @@ static MixedLuLayout mixed_lu_layout(int n, int nrhs, int nb, int sm_count, bool
   L.winvl = take(winv_bytes(n, nb));
   L.winvu = take(winv_bytes(n, nb));
   L.flags = take(trsm_skinny_flag_bytes(n, nb));
+  if (nrhs <= 32) {  // the FP32 sweeps: U^T, the packed diagonal blocks, two sweep workspaces
+    const size_t nblk = (size_t)(n + nb - 1) / nb;
+    L.ut = take(sizeof(float) * L.ldf * n);
+    L.dl = take(sizeof(double) * nblk * 128 * 129);
+    L.du = take(sizeof(double) * nblk * 128 * 129);
+    L.winvut = take(winv_bytes(n, nb));
+    L.swl = take(sweep32_ws_bytes(n, nrhs));
+    L.swu = take(sweep32_ws_bytes(n, nrhs));
+  }
   L.perm = take(align_up(sizeof(int) * (size_t)((n + 1) & ~1), 256) + sizeof(double) * (size_t)n * r);
+  L.permi = take(sizeof(int) * (size_t)n);  // the inverse row permutation
   L.xw = take(sizeof(double) * L.lds * r);
   L.r = take(sizeof(double) * L.lds * r);
   L.norms = take(sizeof(double) * (2 * (size_t)n + 4 * (size_t)r));
@@ -224,10 +266,13 @@ static int dgesv_fp64_refined(egpu_context* h, int n, int nrhs, const double* A,
 
 int dgesv_mixed_core(egpu_context* h, int n, int nrhs, const double* A, long long lda, const double* B, long long ldb,
                      double* X, long long ldx, int max_iter, double tol, int* iters, double* berr) {
-  const int nb = 128;
+  const int nb = 128;  // the solves' diagonal blocks
+  // the factorization's panel width: the handle's block size (a multiple of
+  // 32 up to 128)
+  const int fb = std::max(32, std::min(128, h->nb / 32 * 32));
   cudaStream_t st = h->stream;
   const bool copy_a = !tma_compatible(A, lda);
-  const MixedLuLayout L = mixed_lu_layout(n, nrhs, nb, h->sm_count, copy_a);
+  const MixedLuLayout L = mixed_lu_layout(n, nrhs, nb, fb, h->sm_count, copy_a);
   TRY(ensure_ws(h, L.total + 4096));
   unsigned char* ws = static_cast<unsigned char*>(h->ws);
   if (copy_a) {  // the residual products read A through 16-byte loads
@@ -264,8 +309,8 @@ int dgesv_mixed_core(egpu_context* h, int n, int nrhs, const double* A, long lon
     EGPU_CUDA_TRY(cudaGetLastError());
   }
   // ---- factorization
-  for (int k = 0; k < n; k += nb) {
-    const int b = std::min(nb, n - k), m = n - k, n2 = n - k - b;
+  for (int k = 0; k < n; k += fb) {
+    const int b = std::min(fb, n - k), m = n - k, n2 = n - k - b;
     float* Ak = Af + k + (long long)k * ldf;
     {
       TraceMark tm(st, kTraceOther, 0.0, 12.0 * m * b);
@@ -273,7 +318,7 @@ int dgesv_mixed_core(egpu_context* h, int n, int nrhs, const double* A, long lon
       count_launch();
       EGPU_CUDA_TRY(cudaGetLastError());
     }
-    TRY(launch_lu_panel(st, m, b, P, lds, piv + k, k, image, preimage, W, nb, ws + L.scr, h->dstatus, h->sm_count));
+    TRY(launch_lu_panel(st, m, b, P, lds, piv + k, k, image, preimage, W, fb, ws + L.scr, h->dstatus, h->sm_count));
     {
       TraceMark tm(st, kTraceOther, 0.0, 12.0 * m * b);
       narrow_kernel<<<dim3((m + 255) / 256, b), 256, 0, st>>>(m, b, P, lds, Ak, ldf);
@@ -299,7 +344,7 @@ int dgesv_mixed_core(egpu_context* h, int n, int nrhs, const double* A, long lon
     float* A12 = Af + k + (long long)(k + b) * ldf;
     float* A22 = Af + (k + b) + (long long)(k + b) * ldf;
     // U12 = W A12: A = W (b x b, K-major rows), B = A12^T (n2 x b)
-    TRY(launch_split_tf32(st, b, b, W, nb, Wh, Wl, ldk));
+    TRY(launch_split_tf32(st, b, b, W, fb, Wh, Wl, ldk));
     {
       TraceMark tm(st, kTraceOther, 0.0, 12.0 * b * n2);
       split_tf32_t_kernel<<<n2, 128, 0, st>>>(b, n2, A12, ldf, Bh, Bl, ldk);
@@ -318,22 +363,57 @@ int dgesv_mixed_core(egpu_context* h, int n, int nrhs, const double* A, long lon
     TRY(launch_tc_gemm(st, n2, n2, b, -1.0f, Lh, Ll, Bh, Bl, ldk, 1.0f, A22, ldf, 0, 3, h->dstatus));
   }
   TRY(read_status_now(h, nullptr));  // an exact zero pivot: SingularMatrixException
-  // ---- the factors in FP64 for the solves, their diagonal-block inverses
-  {
-    widen_kernel<<<dim3((n + 255) / 256, std::min(n, 65535)), 256, 0, st>>>(n, n, Af, ldf, LU, lds);
+  // ---- the solves.  With nrhs <= 32 the refinement's corrections and the
+  // condition estimate sweep the FP32 factors directly (L from Af, U through
+  // its transpose UT; one-launch dataflow sweeps over explicit super-block
+  // inverses); GMRES-IR, which needs its preconditioner applied in FP64,
+  // sweeps an FP64 copy of the factors made when it is first needed.
+  const bool use32 = nrhs <= 32;
+  const int nblk = (n + nb - 1) / nb;
+  float* UT = use32 ? reinterpret_cast<float*>(ws + L.ut) : nullptr;
+  void* swl = use32 ? static_cast<void*>(ws + L.swl) : nullptr;
+  void* swu = use32 ? static_cast<void*>(ws + L.swu) : nullptr;
+  if (use32) {
+    double* DL = reinterpret_cast<double*>(ws + L.dl);
+    double* DU = reinterpret_cast<double*>(ws + L.du);
+    double* WinvUT = reinterpret_cast<double*>(ws + L.winvut);
+    const int nt = (n + 31) / 32;
+    transpose_upper_kernel<<<dim3(nt, nt), dim3(32, 8), 0, st>>>(n, Af, ldf, UT);
+    count_launch();
+    diag_blocks_kernel<<<nblk, 256, 0, st>>>(n, Af, ldf, DL, DU);
     count_launch();
     EGPU_CUDA_TRY(cudaGetLastError());
+    TRY(launch_trtri_blocks(st, EGPU_LOWER, 1, DL, 128, n, nb, WinvL, nb));
+    TRY(launch_trtri_blocks(st, EGPU_LOWER, 0, DU, 128, n, nb, WinvUT, nb));
+    TRY(sweep32_prepare(st, n, Af, ldf, WinvL, swl));
+    TRY(sweep32_prepare(st, n, UT, ldf, WinvUT, swu));
   }
-  TRY(launch_trtri_blocks(st, EGPU_LOWER, 1, LU, lds, n, nb, WinvL, nb));
-  TRY(launch_trtri_blocks(st, EGPU_UPPER, 0, LU, lds, n, nb, WinvU, nb));
   // V := A^-1 V (trans 0) or A^-T V (trans 1) through the factors
   // (lu::SolveAfter, LU/SolveAfter.hpp:101-146): pivots, then the unit-lower
   // and upper sweeps (or their transposes in the opposite order)
+  // the row permutation of the pivots and its inverse, composed once
+  int* permF = perm;
+  int* permI = reinterpret_cast<int*>(ws + L.permi);
+  double* ptmp = reinterpret_cast<double*>(perm + ((n + 1) & ~1));
+  TRY(launch_compose_perm(st, 0, n, piv, n, permF));
+  TRY(launch_compose_perm(st, 1, n, piv, n, permI));
+  bool have64 = false;
   int epoch = 0;
-  EGPU_CUDA_TRY(cudaMemsetAsync(flags, 0, trsm_skinny_flag_bytes(n, nb), st));
-  auto lu_solve = [&](double* V, int ncols, int trans) -> int {
+  auto materialize64 = [&]() -> int {  // FP64 factors and their block inverses
+    if (have64) return EGPU_OK;
+    widen_kernel<<<dim3((n + 255) / 256, std::min(n, 65535)), 256, 0, st>>>(n, n, Af, ldf, LU, lds);
+    count_launch();
+    EGPU_CUDA_TRY(cudaGetLastError());
+    if (!use32) TRY(launch_trtri_blocks(st, EGPU_LOWER, 1, LU, lds, n, nb, WinvL, nb));
+    TRY(launch_trtri_blocks(st, EGPU_UPPER, 0, LU, lds, n, nb, WinvU, nb));
+    EGPU_CUDA_TRY(cudaMemsetAsync(flags, 0, trsm_skinny_flag_bytes(n, nb), st));
+    have64 = true;
+    return EGPU_OK;
+  };
+  auto lu_solve64 = [&](double* V, int ncols, int trans) -> int {
+    TRY(materialize64());
     if (!trans) {
-      TRY(launch_laswp_seq(st, 0, n, ncols, V, lds, piv, n, perm));
+      TRY(launch_permute_rows(st, n, ncols, permF, V, lds, ptmp));
       TRY(launch_trsm_skinny(st, 0, 0, n, ncols, LU, lds, WinvL, nb, V, lds, flags, ++epoch, h->sm_count,
                              h->dstatus));
       return launch_trsm_skinny(st, 1, 0, n, ncols, LU, lds, WinvU, nb, V, lds, flags, ++epoch, h->sm_count,
@@ -343,7 +423,18 @@ int dgesv_mixed_core(egpu_context* h, int n, int nrhs, const double* A, long lon
                            h->dstatus));
     TRY(launch_trsm_skinny(st, 1, 1, n, ncols, LU, lds, WinvL, nb, V, lds, flags, ++epoch, h->sm_count,
                            h->dstatus));
-    return launch_laswp_seq(st, 1, n, ncols, V, lds, piv, n, perm);
+    return launch_permute_rows(st, n, ncols, permI, V, lds, ptmp);
+  };
+  auto lu_solve = [&](double* V, int ncols, int trans) -> int {
+    if (!use32) return lu_solve64(V, ncols, trans);
+    if (!trans) {  // P^T L U x = v: x = U^-1 L^-1 P v; U x = y is (U^T)^T x = y
+      TRY(launch_permute_rows(st, n, ncols, permF, V, lds, ptmp));
+      TRY(sweep32_solve(st, 0, n, ncols, Af, ldf, V, lds, swl, h->sm_count, h->dstatus));
+      return sweep32_solve(st, 1, n, ncols, UT, ldf, V, lds, swu, h->sm_count, h->dstatus);
+    }
+    TRY(sweep32_solve(st, 0, n, ncols, UT, ldf, V, lds, swu, h->sm_count, h->dstatus));
+    TRY(sweep32_solve(st, 1, n, ncols, Af, ldf, V, lds, swl, h->sm_count, h->dstatus));
+    return launch_permute_rows(st, n, ncols, permI, V, lds, ptmp);
   };
   auto residual = [&]() -> int {  // R = B - A Xw
     TRY(launch_copy_cols(st, n, nrhs, B, ldb, R, lds, 0));
@@ -410,7 +501,7 @@ int dgesv_mixed_core(egpu_context* h, int n, int nrhs, const double* A, long lon
         rg = launch_dgemm(st, false, true, n, nrhs, n, 1.0, A, lda, Vi, lds, 0.0, Wo, lds, 0, false, h->dstatus);
       return rg;
     };
-    const BlockSolve precond = [&](double* Wo) -> int { return lu_solve(Wo, nrhs, 0); };
+    const BlockSolve precond = [&](double* Wo) -> int { return lu_solve64(Wo, nrhs, 0); };
     int inner = 0;
     double e_best = e;
     while (it < max_iter) {
