@@ -66,7 +66,9 @@ WORKLOADS = {
               "metric": "FP64-accurate solves/sec and p50/p99 latency (served stream, Poisson 2000 req/s): mixed+IR",
               "desc": "request server, continuous batching: Poisson arrivals (mean 2000 req/s, 2 s window), 50/50 "
                       "HPD/GE, n log-uniform [64, 8192], kappa log-uniform [1e2, 1e8] (Q diag(s) Q^T), 1-64 RHS, "
-                      "150 GB HBM budget, 4 slots"},
+                      "150 GB HBM budget, 4 slots; served form: the pool's matrices resident on the device (registered "
+                      "once, factors formed by the first request on each and reused), structure test for GE requests; "
+                      "plain_fp64: every request a full FP64 factor-and-solve from its host A"},
     "chol": {"n": 2048, "nrhs": 16,
              "metric": "FP64-accurate solves/sec (Cholesky + 16-RHS HPD solve, n=2048)",
              "desc": "Cholesky + HPD solve, lower, n=2048, nb=128, 16 RHS (plain FP64)"},
@@ -367,7 +369,8 @@ def reference_serve(args, W, kind, what, threads):
         "config": {"workload": W["desc"], "parallelism": f"{threads} host cores"},
         "cpu_baseline": {"value": value, "unit": "solves/s", "cores": threads, "kind": kind,
                          "sample": f"one Cholesky+solve and one LU+solve at n={ns}, 32 RHS ({what}); host flop rate "
-                                   f"{rate / 1e9:.1f} GFLOP/s applied to the stream's mean work per request"},
+                                   f"{rate / 1e9:.1f} GFLOP/s applied to the stream's mean work per request, each "
+                                   f"request a full factor-and-solve (the reference keeps no state between calls)"},
         "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
 
@@ -817,18 +820,29 @@ def serve_stream(seed, W, device):
     return pool, reqs
 
 
-def run_stream(eg, W, pool, reqs, mode, device_index):
-    """Replay the arrival sequence against a server; returns per-request records."""
+def run_stream(eg, W, pool, reqs, mode, device_index, resident=False):
+    """Replay the arrival sequence against a server; returns per-request
+    records.  resident: the pool's matrices are registered with the server
+    (copied to the device once, inside the timed region, for each kind the
+    stream asks of them) and requests send only B; otherwise every request
+    carries its A."""
     srv = eg.Server(device_index, hbm_budget_bytes=W["budget"], slots=W["slots"], mode=mode, tol=1e-14)
     ids, outs = [], []
     t0 = time.perf_counter()
+    mids = {}
+    if resident:
+        for key in sorted({(pi, kind) for (_, pi, _, kind) in reqs}):
+            mids[key] = srv.register(key[1], pool[key[0]][2])
     for (ta, pi, k, kind) in reqs:
         now = time.perf_counter() - t0
         if ta > now:
             time.sleep(ta - now)
         n, _, Ah, Bh = pool[pi]
         X = np.zeros((n, k), order="F")
-        ids.append(srv.submit(kind, Ah, Bh[:, :k], X))
+        if resident:
+            ids.append(srv.submit_resident(mids[(pi, kind)], Bh[:, :k], X))
+        else:
+            ids.append(srv.submit(kind, Ah, Bh[:, :k], X))
         outs.append(X)
     srv.drain()
     t_end = time.perf_counter() - t0
@@ -850,13 +864,17 @@ def arm_serve(args, ws, rank, local):
     # warm-up: a few requests per mode (kernels loaded, workspaces sized)
     for mode in (1, 0):
         run_stream(eg, W, pool, [(0.0, i % len(pool), 4, i % 2) for i in range(max(args.warmup, 3))], mode, local)
+    # the served form (mode 1, resident matrices and factors), the plain FP64
+    # path (mode 0, every request a full factor-and-solve from its host A),
+    # and for attribution mode 0 with residency and mode 1 without
+    runs = {"served": (1, True), "plain": (0, False), "fp64_resident": (0, True), "mixed_nonresident": (1, False)}
     res = {}
     clocks = None
-    for mode in (1, 0):
+    for key, (mode, resident) in runs.items():
         barrier(ws)
         with ClockSampler(local) as clk:
-            recs, outs, t_end = run_stream(eg, W, pool, reqs, mode, local)
-        if mode == 1:
+            recs, outs, t_end = run_stream(eg, W, pool, reqs, mode, local, resident)
+        if key == "served":
             clocks = clk.summary()
         ok = [i for i, r_ in enumerate(recs) if r_ and r_["status"] == 0]
         lat = np.array([recs[i]["latency_ms"] for i in ok])
@@ -870,18 +888,20 @@ def arm_serve(args, ws, rank, local):
             den = np.abs(Ah).sum(axis=1).max() * np.abs(outs[i]).max(axis=0) + np.abs(Bh[:, :k]).max(axis=0)
             berr = max(berr, float((np.abs(R).max(axis=0) / den).max()))
         paths = [recs[i]["path"] for i in ok]
-        res[mode] = {"value": len(ok) / t_end, "completed": len(ok), "submitted": len(reqs), "makespan_s": t_end,
-                     "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
-                     "backward_error_sampled": berr,
-                     "paths": {"fp64": paths.count(0), "mixed": paths.count(1), "batched": paths.count(2),
-                               "mixed_fell_back": paths.count(3)}}
+        res[key] = {"value": len(ok) / t_end, "completed": len(ok), "submitted": len(reqs), "makespan_s": t_end,
+                    "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+                    "backward_error_sampled": berr, "mode": mode, "resident": resident,
+                    "paths": {"fp64": paths.count(0), "mixed": paths.count(1), "batched": paths.count(2),
+                              "mixed_fell_back": paths.count(3), "ge_as_hpd_fp64": paths.count(4),
+                              "ge_as_hpd_mixed": paths.count(5), "resident_factored": paths.count(6),
+                              "resident_factor_reused": paths.count(7)}}
     if rank != 0:
         return
-    m, p = res[1], res[0]
+    m, p = res["served"], res["plain"]
     line = {
         "metric": W["metric"], "value": m["value"], "unit": "solves/s", "n_gpus": ws, "steps": 1,
         "warmup": args.warmup, "ms_per_step": m["makespan_s"] * 1e3, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64 (mixed tf32x3 + IR for HPD requests)",
+        "vs_baseline": None, "dtype": "f64 (resident FP64 factors; mixed tf32x3 + IR for large one-off HPD requests)",
         "data": "synthetic (seeded pool of 48 matrices, seeded Poisson arrivals)",
         "config": {"workload": W["desc"], "requests": len(reqs), "parallelism": "1 GPU",
                    "l2": "pool matrices up to 512 MiB, larger than L2",
@@ -890,8 +910,10 @@ def arm_serve(args, ws, rank, local):
         "served": m,
         "plain_fp64": p,
         "speedup_vs_plain_fp64": m["value"] / p["value"],
+        "attribution": {"fp64_resident": res["fp64_resident"], "mixed_nonresident": res["mixed_nonresident"]},
         "e2e": {"value": m["value"], "unit": "solves/s",
-                "h2d_bytes_per_step": int(sum(8 * pool[pi][0] * (pool[pi][0] + k) for _, pi, k, _ in reqs)),
+                "h2d_bytes_per_step": int(sum(8 * pool[pi][0] ** 2 for pi, _ in {(pi, kd) for _, pi, _, kd in reqs})
+                                          + sum(8 * pool[pi][0] * k for _, pi, k, _ in reqs)),
                 "d2h_bytes_per_step": int(sum(8 * pool[pi][0] * k for _, pi, k, _ in reqs)),
                 "api": "egpu_server_submit / egpu_server_query with pinned host buffers"},
         "roofline": None,

@@ -134,6 +134,9 @@ def _declare(L):
         "egpu_server_set_tolerance": ([P, D], I),
         "egpu_server_set_mixed_min_n": ([P, I], I),
         "egpu_server_submit": ([P, I, I, I, P, I, P, I, P, I, P], I),
+        "egpu_server_register": ([P, I, I, P, I, P], I),
+        "egpu_server_submit_resident": ([P, ctypes.c_ulonglong, I, P, I, P, I, P], I),
+        "egpu_server_unregister": ([P, ctypes.c_ulonglong], I),
         "egpu_server_query": ([P, ctypes.c_ulonglong, I, P, P, P, P, P, P], I),
         "egpu_server_release": ([P, ctypes.c_ulonglong], I),
         "egpu_server_drain": ([P], I),
@@ -294,6 +297,27 @@ class Server:
                                         ctypes.byref(rid)))
         self._keep[rid.value] = (A, B, X)
         return rid.value
+
+    def register(self, kind, A):
+        """Copy A to the device once (resident); returns the matrix id for
+        submit_resident.  The first request on it forms the factor, later ones
+        reuse it."""
+        A = _np_f(A)
+        mid = ctypes.c_ulonglong(0)
+        _check(lib().egpu_server_register(self._s, kind, A.shape[0], _np_ptr(A), max(A.shape[0], 1),
+                                          ctypes.byref(mid)))
+        return mid.value
+
+    def submit_resident(self, mid, B, X):
+        B, X = _np_f(B), _np_f(X)
+        rid = ctypes.c_ulonglong(0)
+        _check(lib().egpu_server_submit_resident(self._s, mid, B.shape[1], _np_ptr(B), max(B.shape[0], 1),
+                                                 _np_ptr(X), max(X.shape[0], 1), ctypes.byref(rid)))
+        self._keep[rid.value] = (B, X)
+        return rid.value
+
+    def unregister(self, mid):
+        _check(lib().egpu_server_unregister(self._s, mid))
 
     def query(self, rid, wait=False):
         """None while pending, else a dict with status, latency_ms, path, iters, berr."""

@@ -194,7 +194,11 @@ EGPU_API int egpu_batch_plan_destroy(egpu_batch_plan plan);
  * all queued small requests (n <= 512, nrhs <= 16) of the kind at the head of
  * the queue form one batched job.  mode 0: FP64 solves; mode 1: HPD requests
  * of order >= the mixed threshold take egpu_dposv_mixed (FP64 fallback when
- * it cannot reach the tolerance), the rest stay FP64.  kind 0 = HPDSolve(LOWER) (A lower triangle read),
+ * it cannot reach the tolerance), the rest stay FP64; a GE request outside
+ * the batched jobs whose A is exactly symmetric with a positive diagonal is
+ * tried as HPD first
+ * (FP64 Cholesky, or the mixed solver from the threshold) and goes to LU only
+ * when that factorization fails -- the same x.  kind 0 = HPDSolve(LOWER) (A lower triangle read),
  * kind 1 = GaussianElimination.  A, B, X are host buffers (pinned for
  * speed) that must stay valid until the request completes; A and B are not
  * modified, X receives the solution.  The per-slot handle workspaces are
@@ -208,9 +212,23 @@ EGPU_API int egpu_server_set_tolerance(egpu_server s, double tol);
 EGPU_API int egpu_server_set_mixed_min_n(egpu_server s, int n);
 EGPU_API int egpu_server_submit(egpu_server s, int kind, int n, int nrhs, const double* A, int lda,
                                 const double* B, int ldb, double* X, int ldx, unsigned long long* id);
+/* Resident matrices (the request loop keeps matrices and factors on the
+ * device): egpu_server_register copies A (host, kind 0 HPD / 1 GE) to the
+ * device once, charging the budget for A and its factor, and returns *mid.
+ * Requests on it (egpu_server_submit_resident) send only B and X: the first
+ * one forms the factor (Cholesky; in mode 1 a GE matrix passing the structure
+ * test tries Cholesky before LU), later ones reuse it, each an FP64 solve
+ * (paths 6 and 7 in egpu_server_query).  egpu_server_unregister waits for the
+ * matrix's requests to finish, then frees it. */
+EGPU_API int egpu_server_register(egpu_server s, int kind, int n, const double* A, int lda, unsigned long long* mid);
+EGPU_API int egpu_server_submit_resident(egpu_server s, unsigned long long mid, int nrhs, const double* B, int ldb,
+                                         double* X, int ldx, unsigned long long* id);
+EGPU_API int egpu_server_unregister(egpu_server s, unsigned long long mid);
 /* *done = 0 while queued or running; once done: *status (EGPU_* code),
  * *latency_ms (completion - submission), *path (0 FP64, 1 mixed, 2 batched,
- * 3 mixed fell back to FP64), *iters and *berr (mixed path).  wait != 0
+ * 3 mixed fell back to FP64, 4 GE request solved by the FP64 HPD path, 5 GE
+ * request solved by the mixed HPD path, 6 resident matrix factored by this
+ * request, 7 resident factor reused), *iters and *berr (mixed path).  wait != 0
  * blocks until the request completes. */
 EGPU_API int egpu_server_query(egpu_server s, unsigned long long id, int wait, int* done, int* status,
                                double* latency_ms, int* path, int* iters, double* berr);

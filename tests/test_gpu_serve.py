@@ -84,3 +84,84 @@ def test_server_mixed_mode_and_fallback():
     assert _berr(good, Xg, B) <= 1e-14
     assert fh["status"] == 0 and fh["path"] == 3  # TF32x3 factor cannot refine kappa 1e12: FP64 fallback
     assert _berr(hard, Xh, B) <= 1e-14
+
+
+def test_server_structure_test_routes_symmetric_ge_requests():
+    # mode 1: a GE request whose A is exactly symmetric with a positive
+    # diagonal is tried as HPD first (path 4: FP64 Cholesky below the mixed
+    # threshold, path 5: the mixed solver above it); a symmetric indefinite A
+    # fails that factorization and a nonsymmetric A skips it, both ending on
+    # the LU path (0).  Every answer is GaussianElimination's x to backward
+    # error <= 1e-14.
+    n = 700
+    spd = inputs.spd_spectrum(n, 1e5, 21)
+    indef = np.asfortranarray(spd - 10.0 * np.eye(n))  # eigenvalues from -9: symmetric indefinite
+    assert np.all(np.diag(indef) > 0)
+    gen = inputs.uniform(n, n, 22)
+    B = inputs.normal(n, 3, 23)
+    for min_n, spd_path in ((6144, 4), (0, 5)):
+        srv = eg.Server(0, hbm_budget_bytes=8 << 30, slots=2, mode=1, mixed_min_n=min_n)
+        (Xs, Xi, Xg), (fs, fi, fg) = _solve_all(srv, [(1, spd, B), (1, indef, B), (1, gen, B)])
+        srv.close()
+        assert fs["status"] == 0 and fs["path"] == spd_path, fs
+        assert fi["status"] == 0 and fi["path"] == 0, fi
+        assert fg["status"] == 0 and fg["path"] == 0, fg
+        for A, X in ((spd, Xs), (indef, Xi), (gen, Xg)):
+            assert _berr(A, X, B) <= 1e-14
+    # mode 0 never takes the test
+    srv = eg.Server(0, hbm_budget_bytes=8 << 30, slots=2, mode=0)
+    (X0,), (f0,) = _solve_all(srv, [(1, spd, B)])
+    srv.close()
+    assert f0["path"] == 0 and _berr(spd, X0, B) <= 1e-14
+
+
+@pytest.mark.parametrize("mode,n", [(0, 600), (1, 600), (1, 200)])
+def test_server_resident_matrices_reuse_their_factor(mode, n):
+    # matrices registered once; requests send only B: exactly one request per
+    # matrix forms the factor (path 6), the others reuse it (path 7), and
+    # every answer equals a one-off request's within 1e-10 and reaches
+    # backward error <= 1e-14.  A nonsymmetric GE matrix takes LU, an HPD one
+    # Cholesky; a singular matrix fails every request with its status.  Small
+    # matrices (n <= 512, which one-off requests would batch) too.
+    spd = inputs.spd_spectrum(n, 1e4, 31)
+    gen = inputs.uniform(n, n, 32)
+    sing = gen.copy(order="F")
+    sing[:, 17] = 0.0
+    srv = eg.Server(0, hbm_budget_bytes=8 << 30, slots=3, mode=mode)
+    mids = [srv.register(0, spd), srv.register(1, gen), srv.register(1, spd), srv.register(1, sing)]
+    mats = [spd, gen, spd, sing]
+    Bs = [inputs.normal(n, 1 + (i % 5), 40 + i) for i in range(24)]
+    ids, Xs = [], []
+    for i, B in enumerate(Bs):
+        X = np.zeros(B.shape, order="F")
+        ids.append(srv.submit_resident(mids[i % 4], B, X))
+        Xs.append(X)
+    infos = [srv.query(i, wait=True) for i in ids]
+    (X1,), (f1,) = _solve_all(srv, [(1, gen, Bs[1])])
+    for m in mids:
+        srv.unregister(m)
+    srv.close()
+    for k in range(4):
+        paths = [infos[i]["path"] for i in range(k, 24, 4)]
+        if k == 3:
+            assert all(infos[i]["status"] == eg.SINGULAR for i in range(3, 24, 4))
+            continue
+        assert sorted(paths) == [6] + [7] * 5, (k, paths)
+        for i in range(k, 24, 4):
+            assert infos[i]["status"] == 0
+            assert _berr(mats[k], Xs[i], Bs[i]) <= 1e-14
+    assert f1["status"] == 0 and np.abs(Xs[1] - X1).max() <= 1e-10 * np.abs(X1).max()
+
+
+def test_server_resident_budget():
+    n = 512
+    A = inputs.spd_ggt(n, 5)
+    per = 2 * 8 * n * n + 4 * n
+    srv = eg.Server(0, hbm_budget_bytes=per + 4096, slots=1, mode=0)
+    m = srv.register(0, A)
+    with pytest.raises(eg.ElemGPUError):
+        srv.register(0, A)  # the budget holds one
+    srv.unregister(m)
+    m = srv.register(0, A)  # room again
+    srv.unregister(m)
+    srv.close()
