@@ -87,6 +87,185 @@ static cudaError_t launch_variant(cudaStream_t st, const CUtensorMap& ma, const 
   return cudaGetLastError();
 }
 
+
+// ---- small products ------------------------------------------------------
+// A product with only a few 128 x 64 tiles (a panel multiply or the next
+// block column's update of a small factorization) leaves most of the GPU
+// idle and is bound by the per-SM DMMA rate of the few CTAs it has.  This form spreads it over many more warps: each warp computes a
+// 32 x 32 tile of C (2 x 4 DMMA m16n8k8 tiles) straight from global memory
+// (L2), 16 k at a time with the next 16 in flight, and a CTA of WM x WN
+// warps covers a (32 WM) x (32 WN) tile.  All of a CTA's loads come before a
+// CTA barrier and its stores after it, so C may alias A when the CTA covers
+// every column of C (WN * 32 >= N), or B when it covers every row.
+struct SmallParams {
+  const double* A;
+  const double* B;
+  double* C;
+  long long lda, ldb, ldc;
+  int M, N, K, tri, wm, wn;
+  double alpha, beta;
+  const DevStatus* status;
+};
+
+template <bool AK, bool BK>
+__global__ void __launch_bounds__(128) dgemm_small_kernel(const SmallParams p) {
+  if (p.status != nullptr && p.status->code != 0) return;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int g = lane >> 2, t = lane & 3;
+  const int row0 = (blockIdx.x * p.wm + warp % p.wm) * 32;
+  const int col0 = (blockIdx.y * p.wn + warp / p.wm) * 32;
+  // a warp whose tile is wholly outside C or outside the triangle has no work
+  // but still meets the CTA barrier
+  const bool live = row0 < p.M && col0 < p.N && !(p.tri == 1 && row0 + 31 < col0) && !(p.tri == 2 && row0 > col0 + 31);
+  double acc[2][4][4];
+#pragma unroll
+  for (int i = 0; i < 2; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+      for (int r = 0; r < 4; ++r) acc[i][j][r] = 0.0;
+  if (live) {
+    // this lane's rows of op(A) and columns of op(B), clamped (a row or column
+    // past the edge is read at a valid address and multiplied by zero)
+    const double* ar[4];
+    const double* bc[4];
+    bool am[4], bm[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {  // rows row0 + g + 8 q
+      const int m = row0 + g + 8 * q;
+      am[q] = m < p.M;
+      ar[q] = p.A + (AK ? (long long)min(m, p.M - 1) * p.lda : (long long)min(m, p.M - 1));
+    }
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int n = col0 + 8 * j + g;
+      bm[j] = n < p.N;
+      bc[j] = p.B + (BK ? (long long)min(n, p.N - 1) * p.ldb : (long long)min(n, p.N - 1));
+    }
+    const long long as = AK ? 1 : p.lda, bs = BK ? 1 : p.ldb;  // k stride
+    double af[4][4], bf[4][4];  // [k offset t, t+4, t+8, t+12][row / column slot]
+    double an[4][4], bn[4][4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int k = t + 4 * u;
+      const bool kin = k < p.K;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) af[u][q] = (kin && am[q]) ? __ldg(ar[q] + k * as) : 0.0;
+#pragma unroll
+      for (int j = 0; j < 4; ++j) bf[u][j] = (kin && bm[j]) ? __ldg(bc[j] + k * bs) : 0.0;
+    }
+    for (int k0 = 0; k0 < p.K; k0 += 16) {
+      const bool more = k0 + 16 < p.K;
+      if (more) {
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const int k = k0 + 16 + t + 4 * u;
+          const bool kin = k < p.K;
+#pragma unroll
+          for (int q = 0; q < 4; ++q) an[u][q] = (kin && am[q]) ? __ldg(ar[q] + k * as) : 0.0;
+#pragma unroll
+          for (int j = 0; j < 4; ++j) bn[u][j] = (kin && bm[j]) ? __ldg(bc[j] + k * bs) : 0.0;
+        }
+      }
+      // two k8 steps: k = k0 + {t, t+4} and k0 + 8 + {t, t+4}
+#pragma unroll
+      for (int s2 = 0; s2 < 2; ++s2) {
+#pragma unroll
+        for (int i = 0; i < 2; ++i) {
+          // rows 16 i + g (slot 2 i) and 16 i + g + 8 (slot 2 i + 1)
+          const double a4[4] = {af[2 * s2][2 * i], af[2 * s2][2 * i + 1], af[2 * s2 + 1][2 * i],
+                                af[2 * s2 + 1][2 * i + 1]};
+#pragma unroll
+          for (int j = 0; j < 4; ++j) {
+            const double b2[2] = {bf[2 * s2][j], bf[2 * s2 + 1][j]};
+            dmma_16x8x8(acc[i][j], a4, b2);
+          }
+        }
+      }
+      if (more) {
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            af[u][q] = an[u][q];
+            bf[u][q] = bn[u][q];
+          }
+      }
+    }
+  }
+  // every load of the CTA is done before any store (C may alias A or B)
+  __syncthreads();
+  if (!live) return;
+#pragma unroll
+  for (int i = 0; i < 2; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        const int m = row0 + 16 * i + g + (r >= 2 ? 8 : 0);
+        const int n = col0 + 8 * j + 2 * t + (r & 1);
+        if (m >= p.M || n >= p.N) continue;
+        if ((p.tri == 1 && m < n) || (p.tri == 2 && m > n)) continue;
+        double* c = &p.C[m + (long long)n * p.ldc];
+        *c = p.beta == 0.0 ? p.alpha * acc[i][j][r] : fma(p.beta, *c, p.alpha * acc[i][j][r]);
+      }
+}
+
+// Byte ranges [lo, hi) of a column-major view (rows x cols, ld) in memory.
+static bool views_overlap(const double* a, long long rows_a, long long cols_a, long long lda, const double* b,
+                          long long rows_b, long long cols_b, long long ldb) {
+  const uintptr_t a0 = reinterpret_cast<uintptr_t>(a), a1 = a0 + 8 * ((cols_a - 1) * lda + rows_a);
+  const uintptr_t b0 = reinterpret_cast<uintptr_t>(b), b1 = b0 + 8 * ((cols_b - 1) * ldb + rows_b);
+  return a0 < b1 && b0 < a1;
+}
+
+// The small form when the 128 x 64 tiles would not fill the SMs; returns
+// EGPU_ERR_UNSUPPORTED when it does not apply (then the TMA engine runs).
+static int launch_dgemm_small(cudaStream_t st, bool a_kmajor, bool b_kmajor, int M, int N, int K, double alpha,
+                              const double* A, long long lda, const double* B, long long ldb, double beta, double* C,
+                              long long ldc, int tri, DevStatus* status) {
+  // only the smallest products (at most 40 of the engine's tiles, K <= 256):
+  // between that and a full wave the TMA engine measured as fast or faster
+  const long long big_tiles = (long long)((M + 127) / 128) * ((N + 63) / 64);
+  if (big_tiles > 40 || K > 256) return EGPU_ERR_UNSUPPORTED;
+  const bool alias_a = views_overlap(C, M, N, ldc, A, a_kmajor ? K : M, a_kmajor ? M : K, lda);
+  const bool alias_b = views_overlap(C, M, N, ldc, B, b_kmajor ? K : N, b_kmajor ? N : K, ldb);
+  int wm = 2, wn = 2;
+  if (alias_a && alias_b) return EGPU_ERR_UNSUPPORTED;
+  // in place only as the drivers use it: C is A (the same rows) or C is B
+  // (column n of C is column n of op(B)^T)
+  if (alias_a && !(C == A && ldc == lda && !a_kmajor)) return EGPU_ERR_UNSUPPORTED;
+  if (alias_b && !(C == B && ldc == ldb && b_kmajor)) return EGPU_ERR_UNSUPPORTED;
+  if (alias_a) {  // every column of C in one CTA
+    if (N > 128) return EGPU_ERR_UNSUPPORTED;
+    wn = (N + 31) / 32;
+    wm = std::max(1, 4 / wn);
+  } else if (alias_b) {  // every row of C in one CTA
+    if (M > 128) return EGPU_ERR_UNSUPPORTED;
+    wm = (M + 31) / 32;
+    wn = std::max(1, 4 / wm);
+  }
+  SmallParams p;
+  p.A = A; p.B = B; p.C = C; p.lda = lda; p.ldb = ldb; p.ldc = ldc;
+  p.M = M; p.N = N; p.K = K; p.tri = tri; p.wm = wm; p.wn = wn; p.alpha = alpha; p.beta = beta; p.status = status;
+  const dim3 grid((M + 32 * wm - 1) / (32 * wm), (N + 32 * wn - 1) / (32 * wn));
+  const double lo_n = std::min(M, N), rect = tri == 1 ? std::max(0, M - N) : std::max(0, N - M);
+  const double entries = tri == 0 ? (double)M * N : lo_n * (lo_n + 1) / 2 + rect * lo_n;
+  TraceMark tm(st, beta == 0.0 ? kTraceTrsm : kTraceUpdate, 2.0 * entries * K,
+               8.0 * ((double)M * K + (double)N * K + (beta == 0.0 ? 1.0 : 2.0) * entries));
+  if (a_kmajor && b_kmajor) dgemm_small_kernel<true, true><<<grid, 32 * wm * wn, 0, st>>>(p);
+  else if (a_kmajor) dgemm_small_kernel<true, false><<<grid, 32 * wm * wn, 0, st>>>(p);
+  else if (b_kmajor) dgemm_small_kernel<false, true><<<grid, 32 * wm * wn, 0, st>>>(p);
+  else dgemm_small_kernel<false, false><<<grid, 32 * wm * wn, 0, st>>>(p);
+  count_launch();
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    set_last_error(e, "dgemm_small launch", __FILE__, __LINE__);
+    return EGPU_ERR_CUDA;
+  }
+  return EGPU_OK;
+}
+
 // C = alpha * op(A) * op(B) + beta * C (tri: 0 full, 1 lower, 2 upper).
 //   a_kmajor = false: A stored M x K column-major (op = NORMAL)
 //   a_kmajor = true : A stored K x M column-major (op = TRANSPOSE)
@@ -103,6 +282,11 @@ int launch_dgemm(cudaStream_t st, bool a_kmajor, bool b_kmajor, int M, int N, in
   if (K <= 0) return launch_scale(st, M, N, beta, C, ldc, tri);
   if (!tma_compatible(A, lda) || !tma_compatible(B, ldb)) return EGPU_ERR_ALIGN;
   if (tri != 0 && wide) return EGPU_ERR_ARG;
+  {
+    const int rc = launch_dgemm_small(st, a_kmajor, b_kmajor, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, tri,
+                                      status);
+    if (rc != EGPU_ERR_UNSUPPORTED) return rc;
+  }
   const bool half = wide && !a_kmajor && (M + 127) / 128 < 2 * sm_count_of_current_device();
   const int BM = half ? 64 : 128, BN = wide ? 128 : 64;
   CUtensorMap ma, mb;
