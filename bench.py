@@ -411,6 +411,17 @@ def backward_error(A, X, B):
     return float((R.abs().amax(0) / den).max())
 
 
+# DRAM bytes (read + write) per algorithmic byte, from the committed ncu
+# captures of the same kernels on smaller cases (traffic grows with the bytes
+# the launch streams, so the ratio scales to the bench's launches)
+TRAFFIC_RATIO = {
+    "tc": (577.2 / 604.0, "profiles/tc_gemm_update_n12288.md: 330.6 + 246.6 MB of DRAM traffic for 604 MB of "
+                          "algorithmic bytes, scaled to this run's bytes per launch"),
+    "update": (429.1 / 352.0, "profiles/dgemm_update_k1024_n6144.md: 321.9 + 107.2 MB of DRAM traffic for 352 MB of "
+                              "algorithmic bytes, scaled to this run's bytes per launch"),
+}
+
+
 def roofline_of(trace, kind, peaks, busy_total_ms):
     """Roofline line for one traced kernel class.  Its time is the class's
     busy time on the device (the union of its launches' intervals across the
@@ -420,7 +431,10 @@ def roofline_of(trace, kind, peaks, busy_total_ms):
     if not t or not t.get("launches") or t["busy_ms"] <= 0:
         return None
     ms = t["busy_ms"]
-    common = {"launches": t["launches"], "time_ms": ms, "time_basis": "busy time of the kernel class (union of "
+    ratio, source = TRAFFIC_RATIO.get(kind, (None, None))
+    traffic = ratio * t["bytes"] / t["launches"] if ratio else None
+    common = {"traffic_source": source, "algorithmic_bytes_per_launch": t["bytes"] / t["launches"],
+              "launches": t["launches"], "time_ms": ms, "time_basis": "busy time of the kernel class (union of "
               "its launch intervals across streams, CUDA events on each launch's stream)",
               "share_of_busy_time": t["share_ms"] / busy_total_ms if busy_total_ms > 0 else None}
     if kind == "tc":  # FP32 C read-modify-write + split panels: HBM-bound at K = 128
@@ -429,10 +443,10 @@ def roofline_of(trace, kind, peaks, busy_total_ms):
         return {"bound": "hbm", "kernel": "tc_gemm_kernel (tcgen05 TF32x3 trailing update)", "achieved": achieved,
                 "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)" if peaks.get("hbm_gbs") else "fallback",
-                "tensor_tflops": t["flops"] / (ms / 1e3) / 1e12, "traffic": None, **common}
+                "tensor_tflops": t["flops"] / (ms / 1e3) / 1e12, "traffic": traffic, **common}
     achieved = t["flops"] / (ms / 1e3) / 1e12
     return {"bound": "tensor", "kernel": "dgemm_tma_kernel (FP64 DMMA trailing update)", "achieved": achieved,
-            "peak": FP64_PEAK_TFLOPS, "unit": "TFLOP/s", "frac": achieved / FP64_PEAK_TFLOPS, "traffic": None,
+            "peak": FP64_PEAK_TFLOPS, "unit": "TFLOP/s", "frac": achieved / FP64_PEAK_TFLOPS, "traffic": traffic,
             "peak_source": "measured FP64 DMMA peak (profiles/fp64_peak.md); MEASURED_PEAKS.json has no FP64 entry",
             **common}
 
@@ -783,7 +797,11 @@ def arm_batched(args, ws, rank, local):
         "roofline": {"bound": "tensor", "kernel": "chol_batched_kernel + lu_batched_kernel (FP64 DMMA)",
                      "achieved": achieved, "peak": FP64_PEAK_TFLOPS, "unit": "TFLOP/s",
                      "frac": achieved / FP64_PEAK_TFLOPS if achieved else None,
-                     "peak_source": "measured FP64 DMMA peak (profiles/fp64_peak.md)", "traffic": None},
+                     "peak_source": "measured FP64 DMMA peak (profiles/fp64_peak.md)",
+                     # profiles/lu_batched_kernel_512.md: 1.61 + 1.68 GB of DRAM traffic for 512 GE systems of
+                     # these shapes; the step's GE launch has W["count"] of them
+                     "traffic": 3.29e9 * W["count"] / 512,
+                     "traffic_source": "profiles/lu_batched_kernel_512.md (the GE launch; scaled by the system count)"},
         "kernels": {k: {"ms": v["ms"], "launches": v["launches"]} for k, v in ktrace.items() if v["launches"]},
         "gpu_launches": launches + 2 * args.steps,
         "gpu_launches_note": "2 persistent batched kernels per step, replayed from the CUDA graph",
