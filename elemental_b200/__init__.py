@@ -125,6 +125,9 @@ def _declare(L):
         "egpu_mixed_mode": ([H], I),
         "egpu_mixed_condition_estimate": ([H, P], I),
         "egpu_batch_plan_create": ([H, I, I, P, P, P, P, P, P, P], I),
+        "egpu_batch_plan_create_ex": ([H, I, I, I, P, P, P, P, P, P, P], I),
+        "egpu_batch_plan_iters": ([P, P, P], I),
+        "egpu_batch_plan_shape": ([P, P, P, P, P, P], I),
         "egpu_batch_plan_run": ([P, P], I),
         "egpu_batch_plan_info": ([P, P, P], I),
         "egpu_batch_plan_autotune": ([P, P, I, P, P], I),
@@ -353,9 +356,11 @@ class Server:
 class BatchPlan:
     """A device-resident batched solve (egpu_batch_plan_*): kind 0 = HPD solves,
     kind 1 = GaussianElimination.  The matrices stay where they are; run()
-    only enqueues work (capturable in a CUDA graph)."""
+    only enqueues work (capturable in a CUDA graph).  precision 0: FP64 (each
+    A receives its factor); precision 1: FP32 working copies + FP64 iterative
+    refinement to backward error <= 1e-14 (the A are left unchanged)."""
 
-    def __init__(self, handle, kind, As, Bs=None):
+    def __init__(self, handle, kind, As, Bs=None, precision=0):
         self.handle = handle
         cnt = len(As)
         n = (ctypes.c_int * cnt)(*[a.shape[0] for a in As])
@@ -370,7 +375,9 @@ class BatchPlan:
             ldb, ptrB = None, None
         self.count = cnt
         self._p = ctypes.c_void_p()
-        _check(lib().egpu_batch_plan_create(handle._h, kind, cnt, n, nr, ptrA, lda, ptrB, ldb, ctypes.byref(self._p)))
+        self.precision = precision
+        _check(lib().egpu_batch_plan_create_ex(handle._h, kind, precision, cnt, n, nr, ptrA, lda, ptrB, ldb,
+                                               ctypes.byref(self._p)))
 
     @staticmethod
     def _stream(stream):
@@ -394,6 +401,21 @@ class BatchPlan:
 
     def set_grid(self, grid):
         _check(lib().egpu_batch_plan_set_grid(self._p, grid))
+
+    def iters(self, stream=None):
+        """Refinement corrections per system of the last run (-1: the system
+        was re-solved in FP64 after its refinement stalled; 0 for FP64 plans)."""
+        out = (ctypes.c_int * max(self.count, 1))()
+        _check(lib().egpu_batch_plan_iters(self._p, self._stream(stream), out))
+        return list(out)[: self.count]
+
+    def shape(self):
+        """The launch shape per size class: [{"nmax", "panel", "threads", "grid"}]."""
+        nc = ctypes.c_int(0)
+        arr = [(ctypes.c_int * 3)() for _ in range(4)]
+        _check(lib().egpu_batch_plan_shape(self._p, ctypes.byref(nc), *arr))
+        return [{"nmax": arr[0][c], "panel": arr[1][c], "threads": arr[2][c], "grid": arr[3][c]}
+                for c in range(nc.value)]
 
     def close(self):
         if self._p:

@@ -1081,14 +1081,17 @@ struct egpu_batch_plan_s {
   egpu::BatchPlan* p;
 };
 
-int egpu_batch_plan_create(egpu_handle h, int kind, int count, const int* n, const int* nrhs, double* const* dA,
-                           const int* lda, double* const* dB, const int* ldb, egpu_batch_plan* out) {
+int egpu_batch_plan_create_ex(egpu_handle h, int kind, int precision, int count, const int* n, const int* nrhs,
+                              double* const* dA, const int* lda, double* const* dB, const int* ldb,
+                              egpu_batch_plan* out) {
   TRY(check_handle(h));
-  if (!out || (kind != 0 && kind != 1) || count < 0 || (count > 0 && (!n || !nrhs || !dA || !lda))) return EGPU_ERR_ARG;
+  if (!out || (kind != 0 && kind != 1) || (precision != 0 && precision != 1) || count < 0 ||
+      (count > 0 && (!n || !nrhs || !dA || !lda)))
+    return EGPU_ERR_ARG;
   *out = nullptr;
   Enter g(h);
   egpu::BatchPlan* p = nullptr;
-  TRY(egpu::batch_plan_create(h->device, h->sm_count, kind, count, n, nrhs, dA, lda, dB, ldb, &p));
+  TRY(egpu::batch_plan_create(h->device, h->sm_count, kind, precision, count, n, nrhs, dA, lda, dB, ldb, &p));
   auto* w = new (std::nothrow) egpu_batch_plan_s{h, p};
   if (!w) {
     egpu::batch_plan_destroy(p);
@@ -1096,6 +1099,22 @@ int egpu_batch_plan_create(egpu_handle h, int kind, int count, const int* n, con
   }
   *out = w;
   return EGPU_OK;
+}
+
+int egpu_batch_plan_create(egpu_handle h, int kind, int count, const int* n, const int* nrhs, double* const* dA,
+                           const int* lda, double* const* dB, const int* ldb, egpu_batch_plan* out) {
+  return egpu_batch_plan_create_ex(h, kind, 0, count, n, nrhs, dA, lda, dB, ldb, out);
+}
+
+int egpu_batch_plan_iters(egpu_batch_plan plan, void* stream, int* iters) {
+  if (!plan || !iters) return EGPU_ERR_ARG;
+  Enter g(plan->h);
+  return egpu::batch_plan_iters(plan->p, stream ? static_cast<cudaStream_t>(stream) : plan->h->stream, iters);
+}
+
+int egpu_batch_plan_shape(egpu_batch_plan plan, int* nclass, int* class_nmax, int* panel, int* threads, int* grid) {
+  if (!plan) return EGPU_ERR_ARG;
+  return egpu::batch_plan_shape(plan->p, nclass, class_nmax, panel, threads, grid);
 }
 
 int egpu_batch_plan_run(egpu_batch_plan plan, void* stream) {

@@ -168,10 +168,13 @@ int launch_getrf_diag_nopiv(cudaStream_t st, double* A, long long lda, int b, do
 // Batched (one persistent launch) HPDSolve, lower, n <= 512, nrhs <= 16.
 size_t egpu_batched_ws_bytes(int count, int sm_count);
 struct BatchPlan;
-int batch_plan_create(int device, int sm_count, int kind, int count, const int* n, const int* nrhs,
+// precision 0: FP64 (A receives the factor); 1: FP32 working copy + FP64 refinement (A unchanged)
+int batch_plan_create(int device, int sm_count, int kind, int precision, int count, const int* n, const int* nrhs,
                       double* const* A, const int* lda, double* const* B, const int* ldb, BatchPlan** out);
 int batch_plan_run(BatchPlan* p, cudaStream_t st);
 int batch_plan_info(BatchPlan* p, cudaStream_t st, int* info_host);
+int batch_plan_iters(BatchPlan* p, cudaStream_t st, int* iters_host);
+int batch_plan_shape(BatchPlan* p, int* nclass, int* class_nmax, int* panel, int* threads, int* grid);
 int batch_plan_autotune(BatchPlan* p, cudaStream_t st, int reps, double* best_ms, int* best_grid);
 void batch_plan_set_grid(BatchPlan* p, int grid);
 void batch_plan_destroy(BatchPlan* p);

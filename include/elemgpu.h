@@ -167,12 +167,18 @@ EGPU_API int egpu_dgesv(egpu_handle h, int n, int nrhs, double* dA, int lda, dou
 
 /* Batch plans: a batched HPD solve (kind 0, as egpu_dposv_batched) or
  * GaussianElimination (kind 1, as egpu_dgesv_batched) whose size-sorted
- * system list, queue and scratch stay on the device, so that a run is two
- * stream operations with no host synchronisation (a CUDA graph can capture
+ * system list, queue and scratch stay on the device, so that a run is a
+ * counter reset plus one persistent launch per size class, with no host
+ * synchronisation (a CUDA graph can capture
  * and replay it; the device pointers are fixed at creation: refill the
- * matrices in place between runs).  egpu_batch_plan_autotune times the
- * candidate persistent-grid sizes on the plan's own systems (the runs factor
- * them in place) and keeps the fastest; egpu_batch_plan_info copies the
+ * matrices in place between runs).  egpu_batch_plan_autotune chooses the
+ * launch shape: for the whole list and for each size class (n <= 128,
+ * <= 256, <= 512) it times the candidate panel widths (16, 32), CTA sizes
+ * (128, 256 threads: one or two CTAs per SM) and persistent grids on the
+ * plan's own systems -- restoring every input from a backup before each run
+ * and once more at the end -- and keeps the faster of the best single launch
+ * and the best launch per class (*best_grid: the first class's grid);
+ * egpu_batch_plan_info copies the
  * per-system info of the last run to the host and synchronises.  A plan
  * belongs to the handle that made it and must be destroyed before it.
  * No counterpart in the reference (it solves one system per call). */
@@ -185,6 +191,24 @@ EGPU_API int egpu_batch_plan_info(egpu_batch_plan plan, void* stream, int* info)
 EGPU_API int egpu_batch_plan_autotune(egpu_batch_plan plan, void* stream, int reps, double* best_ms,
                                       int* best_grid);
 EGPU_API int egpu_batch_plan_set_grid(egpu_batch_plan plan, int grid);
+/* As egpu_batch_plan_create with a precision: 0 = FP64 (as above); 1 = each
+ * system is converted once into an FP32 working copy (plan-owned), factored
+ * there (FP64 register arithmetic, values stored in FP32), and its solution
+ * refined in FP64 against A until the backward error max_j ||b_j - A x_j||_inf
+ * / (||A||_inf ||x_j||_inf + ||b_j||_inf) <= 1e-14; A is left unchanged and B
+ * receives X.  A system whose refinement stalls (or whose FP32 factorization
+ * breaks down) is re-solved in FP64 within the same launch. */
+EGPU_API int egpu_batch_plan_create_ex(egpu_handle h, int kind, int precision, int count, const int* n,
+                                       const int* nrhs, double* const* dA, const int* lda, double* const* dB,
+                                       const int* ldb, egpu_batch_plan* out);
+/* Refinement corrections of each system in the last run (precision 1; -1 =
+ * solved by the FP64 fallback; 0 for FP64 plans); synchronises. */
+EGPU_API int egpu_batch_plan_iters(egpu_batch_plan plan, void* stream, int* iters);
+/* The plan's launch shape: *nclass size classes (largest first), each with
+ * its largest order, panel width, CTA size (threads) and persistent grid
+ * (arrays of at least 3 entries; any pointer may be NULL). */
+EGPU_API int egpu_batch_plan_shape(egpu_batch_plan plan, int* nclass, int* class_nmax, int* panel, int* threads,
+                                   int* grid);
 EGPU_API int egpu_batch_plan_destroy(egpu_batch_plan plan);
 
 /* Request server (continuous batching on one GPU): no counterpart in the

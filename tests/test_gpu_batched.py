@@ -123,3 +123,95 @@ def test_batch_plan_graph_replay_matches_oracle(handle, kind):
         Xg = dB[i].cpu().numpy()
         assert np.max(np.abs(Xg - X)) <= 1e-8 * max(1.0, np.max(np.abs(X))), i
     plan.close()
+
+
+def _berr(A, X, B):
+    """max_j ||b_j - A x_j||_inf / (||A||_inf ||x_j||_inf + ||b_j||_inf)."""
+    R = B - A @ X
+    den = np.abs(A).sum(1).max() * np.abs(X).max(0) + np.abs(B).max(0)
+    return float((np.abs(R).max(0) / den).max())
+
+
+@pytest.mark.parametrize("kind", [0, 1])
+def test_refined_plan_uneven(handle, kind):
+    """FP32 working copies + FP64 refinement: every system reaches backward
+    error <= 1e-14, agrees with the oracle's FP64 solution, and leaves A
+    untouched (more than 8 right-hand sides take two chunks)."""
+    r = inputs.rng(900 + kind)
+    sizes = [1, 2, 31, 32, 33, 64, 127, 128, 129, 255, 256, 257, 300, 511, 512] + \
+        [int(x) for x in r.integers(1, 513, 17)]
+    As, Bs, dA, dB = [], [], [], []
+    for i, n in enumerate(sizes):
+        A = inputs.spd_ggt(n, 700 + i) if kind == 0 else inputs.uniform(n, n, 700 + i)
+        B = inputs.normal(n, 1 + (i * 5) % 16, 800 + i)
+        As.append(A); Bs.append(B)
+        dA.append(eg.colmajor_cuda(A)); dB.append(eg.colmajor_cuda(B))
+    plan = eg.BatchPlan(handle, kind, dA, dB, precision=1)
+    plan.run()
+    assert plan.info() == [0] * len(sizes)
+    its = plan.iters()
+    assert all(0 <= k <= 10 for k in its), its
+    for i, (A, B) in enumerate(zip(As, Bs)):
+        assert np.array_equal(dA[i].cpu().numpy(), A), i
+        Xg = dB[i].cpu().numpy()
+        assert _berr(A, Xg, B) <= 1e-14, (i, sizes[i])
+        if kind == 0:
+            _, X, st = orc.hpd_solve(A, B, orc.LOWER, nb=32)
+        else:
+            _, X, st = orc.gaussian_elimination(A, B, nb=32)
+        assert st == 0
+        assert np.max(np.abs(Xg - X)) <= 1e-8 * max(1.0, np.max(np.abs(X))), i
+    plan.close()
+
+
+def test_refined_plan_falls_back_to_fp64(handle):
+    """A system too ill-conditioned for the FP32 factor is re-solved in FP64
+    (iters -1) to the same backward error; a matrix that is not HPD reports
+    its column from the FP64 factorization; the others refine as usual."""
+    good = inputs.spd_ggt(200, 1)
+    ill = np.asfortranarray(inputs.spd_spectrum(160, 1e12, 2))
+    bad = good.copy(order="F")
+    bad[70, 70] = -3.0
+    mats = [good, ill, bad, inputs.spd_ggt(64, 3)]
+    Bs = [inputs.normal(m.shape[0], 3, 10 + i) for i, m in enumerate(mats)]
+    dA = [eg.colmajor_cuda(m) for m in mats]
+    dB = [eg.colmajor_cuda(b) for b in Bs]
+    plan = eg.BatchPlan(handle, 0, dA, dB, precision=1)
+    plan.run()
+    info, its = plan.info(), plan.iters()
+    assert info == [0, 0, 71, 0]
+    assert its[1] == -1 and its[2] == -1 and its[0] >= 0 and its[3] >= 0
+    for i in (0, 1, 3):
+        assert _berr(mats[i], dB[i].cpu().numpy(), Bs[i]) <= 1e-14, i
+    plan.close()
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_autotune_restores_inputs_and_reports_shapes(handle, precision):
+    """The tile-shape autotuner leaves every input as it found it, reports a
+    valid shape per size class, and the tuned plan still solves correctly."""
+    import torch
+    r = inputs.rng(31 + precision)
+    sizes = [int(x) for x in r.integers(32, 513, 40)] + [512, 100, 200]
+    As = [inputs.uniform(n, n, 60 + i) for i, n in enumerate(sizes)]
+    Bs = [inputs.normal(n, 1 + i % 8, 90 + i) for i, n in enumerate(sizes)]
+    dA = [eg.colmajor_cuda(a) for a in As]
+    dB = [eg.colmajor_cuda(b) for b in Bs]
+    plan = eg.BatchPlan(handle, 1, dA, dB, precision=precision)
+    ms, grid = plan.autotune(reps=1)
+    torch.cuda.synchronize()
+    assert ms > 0 and grid >= 1
+    for i in range(len(sizes)):
+        assert np.array_equal(dA[i].cpu().numpy(), As[i]), i
+        assert np.array_equal(dB[i].cpu().numpy(), Bs[i]), i
+    shape = plan.shape()
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    assert 1 <= len(shape) <= 3
+    for s in shape:
+        assert s["nmax"] in (128, 256, 512) and s["panel"] in (16, 32) and s["threads"] in (128, 256)
+        assert 1 <= s["grid"] <= 4 * sms
+    plan.run()
+    assert plan.info() == [0] * len(sizes)
+    for i, (A, B) in enumerate(zip(As, Bs)):
+        assert _berr(A, dB[i].cpu().numpy(), B) <= 1e-14, i
+    plan.close()
