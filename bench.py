@@ -653,6 +653,7 @@ def arm_batched(args, ws, rank, local):
         for k in (0, 1):
             tuned.append(plans[k].autotune(reps=1, stream=s0))
     torch.cuda.synchronize()
+    plans_shape = [p_.shape() for p_ in plans]
 
     def refill_and_run():
         cur = torch.cuda.current_stream()
@@ -748,6 +749,7 @@ def arm_batched(args, ws, rank, local):
     d2h = sum(int(outB[k].numel()) * 8 for k in (0, 1))
     for p_ in plans:
         p_.close()
+    refined = batched_refined(args, ws, dev, h, arenas, cnt, total, ms, r)
     if rank != 0:
         return
     flops = sum(n ** 3 / 3.0 for n in sizes[0]) + sum(2.0 * n ** 3 / 3.0 for n in sizes[1])
@@ -787,6 +789,8 @@ def arm_batched(args, ws, rank, local):
         "equiv_fp64_tflops": flops / (ms / args.steps / 1e3) / 1e12,
         "backward_error": berr,
         "autotuned_grid": {"hpd": tuned[0][1], "ge": tuned[1][1]},
+        "autotuned_shapes": {"hpd": plans_shape[0], "ge": plans_shape[1]},
+        "fp32_ir": refined,
         "shard": {"systems_per_rank": cnt, "load_balance": float(max(shard_load) / (sum(shard_load) / ws))}
         if ws > 1 else None,
         "plain_fp64": {"value": plain_value, "unit": "solves/s",
@@ -798,10 +802,10 @@ def arm_batched(args, ws, rank, local):
                      "achieved": achieved, "peak": FP64_PEAK_TFLOPS, "unit": "TFLOP/s",
                      "frac": achieved / FP64_PEAK_TFLOPS if achieved else None,
                      "peak_source": "measured FP64 DMMA peak (profiles/fp64_peak.md)",
-                     # profiles/lu_batched_kernel_512.md: 1.61 + 1.68 GB of DRAM traffic for 512 GE systems of
+                     # profiles/batched_kernel_512.md: 1.66 + 1.43 GB of DRAM traffic for 512 GE systems of
                      # these shapes; the step's GE launch has W["count"] of them
-                     "traffic": 3.29e9 * W["count"] / 512,
-                     "traffic_source": "profiles/lu_batched_kernel_512.md (the GE launch; scaled by the system count)"},
+                     "traffic": 3.09e9 * W["count"] / 512,
+                     "traffic_source": "profiles/batched_kernel_512.md (the GE launch; scaled by the system count)"},
         "kernels": {k: {"ms": v["ms"], "launches": v["launches"]} for k, v in ktrace.items() if v["launches"]},
         "gpu_launches": launches + 2 * args.steps,
         "gpu_launches_note": "2 persistent batched kernels per step, replayed from the CUDA graph",
@@ -809,6 +813,75 @@ def arm_batched(args, ws, rank, local):
         "cpu_baseline": cpu,
     }
     return line
+
+
+def batched_refined(args, ws, dev, h, arenas, cnt, total, fp64_ms, r):
+    """C4's FP32+IR variant on the same systems: refined batch plans (FP32
+    working copies, FP64 iterative refinement to backward error <= 1e-14,
+    an FP64 re-solve in the same launch for a system whose refinement
+    stalls), autotuned, the step (refill of the right-hand sides + both
+    launches) captured in a CUDA graph and timed like the FP64 plans.  The
+    refined plans leave A unchanged, so the step refills only B."""
+    import torch
+    import elemental_b200 as eg
+
+    s0, s1 = torch.cuda.Stream(device=dev), torch.cuda.Stream(device=dev)
+    for k in (0, 1):
+        arenas[k]["A"].copy_(arenas[k]["A0"])
+        arenas[k]["B"].copy_(arenas[k]["B0"])
+    torch.cuda.synchronize()
+    plans = [eg.BatchPlan(h, k, arenas[k]["vA"], arenas[k]["vB"], precision=1) for k in (0, 1)]
+    tuned = []
+    with torch.cuda.stream(s0):
+        for k in (0, 1):
+            tuned.append(plans[k].autotune(reps=1, stream=s0))
+    torch.cuda.synchronize()
+    shapes = [p_.shape() for p_ in plans]
+
+    def refill_and_run():
+        cur = torch.cuda.current_stream()
+        s1.wait_stream(cur)
+        for k, s in ((0, cur), (1, s1)):
+            with torch.cuda.stream(s):
+                arenas[k]["B"].copy_(arenas[k]["B0"])
+                plans[k].run(s)
+        cur.wait_stream(s1)
+
+    graph = torch.cuda.CUDAGraph()
+    s0.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(s0):
+        refill_and_run()
+    torch.cuda.synchronize()
+    with torch.cuda.graph(graph, stream=s0):
+        refill_and_run()
+    torch.cuda.synchronize()
+    ms, _, launches, clocks = timed(args, ws, dev, s0, h, graph.replay)
+    infos = [plans[k].info(s0) for k in (0, 1)]
+    iters = [plans[k].iters(s0) for k in (0, 1)]
+    torch.cuda.synchronize()
+    berr = 0.0
+    for k in (0, 1):
+        for i in r.choice(cnt[k], min(32, cnt[k]), replace=False):
+            b0 = torch.as_strided(arenas[k]["B0"], arenas[k]["vB"][i].shape, arenas[k]["vB"][i].stride(),
+                                  arenas[k]["vB"][i].storage_offset())
+            berr = max(berr, backward_error(arenas[k]["vA"][i], arenas[k]["vB"][i], b0))
+    for p_ in plans:
+        p_.close()
+    del graph
+    hist = {}
+    for its in iters:
+        for v in its:
+            hist[str(v)] = hist.get(str(v), 0) + 1
+    return {"value": total * args.steps / (ms / 1e3), "unit": "solves/s", "ms_per_step": ms / args.steps,
+            "speedup_vs_fp64_batched": fp64_ms / ms, "backward_error": berr,
+            "failed_systems": sum(1 for inf in infos for v in inf if v != 0),
+            "corrections_histogram": hist,
+            "corrections_note": "refinement corrections per system; -1 = re-solved in FP64 inside the launch "
+                                "after the refinement stalled",
+            "autotuned_grid": {"hpd": tuned[0][1], "ge": tuned[1][1]},
+            "autotuned_shapes": {"hpd": shapes[0], "ge": shapes[1]},
+            "step_includes": "device refill of every right-hand side (A is left unchanged), both refined launches",
+            "gpu_launches": launches + 2 * args.steps, "clocks": clocks}
 
 
 def serve_stream(seed, W, device):
@@ -949,8 +1022,8 @@ def arm_serve(args, ws, rank, local):
 def kernel_case(args):
     """One launch of a single kernel class at a chosen size, for profiler
     captures (ncu -k ...): 'update' = one lower Herk trailing update
-    (n x n, K = 128), 'gemm' = one Gemm trailing update, 'panel' = one LU panel
-    (n x 128), 'diag' = one diagonal-block Cholesky (128 x 128), 'mixed' = one
+    (n x n, K = 128), 'gemm' = one Gemm trailing update, 'lu' = one LU with
+    partial pivoting (warm-up call first), 'panel' = one LU panel (n x 128), 'diag' = one diagonal-block Cholesky (128 x 128), 'mixed' = one
     mixed-precision HPD solve, 'tc' = the tcgen05 trailing update alone,
     'chol' = one plain FP64 Cholesky (warm-up call first); 'inverse',
     'hpdinverse', 'trtri', 'ldl', 'revchol', 'det' time those entry points
@@ -985,6 +1058,22 @@ def kernel_case(args):
         torch.cuda.synchronize()
         ms = e0.elapsed_time(e1)
         print(json.dumps({"case": "chol", "n": n, "ms": ms, "tflops": n ** 3 / 3 / ms / 1e9}))
+        return
+    elif args.case == "lu":
+        # LU with partial pivoting of a U[-1,1] matrix of order n: warm-up, timed
+        A0 = eg.colmajor_cuda(torch.rand(n, n, dtype=torch.float64, device="cuda") * 2 - 1)
+        A = A0.clone()
+        p = torch.zeros(n, dtype=torch.int32, device="cuda")
+        h.lu(A, p)
+        A.copy_(A0)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        h.lu(A, p)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        print(json.dumps({"case": "lu", "n": n, "ms": ms, "tflops": 2 * n ** 3 / 3 / ms / 1e9}))
         return
     elif args.case == "panel":
         A = eg.colmajor_cuda(inputs.uniform(n, NB, 1))
@@ -1162,7 +1251,8 @@ def kernel_case(args):
 NESTED = {"chol": "C1", "lu": "C2", "mixed": "C3", "batched": "C4", "serve": "C5"}
 NESTED_KEYS = ("metric", "value", "unit", "ms_per_step", "steps", "backward_error", "latency_ms", "roofline", "e2e",
                "cpu_baseline", "plain_fp64", "speedup_vs_plain_fp64", "refinement", "kernels", "gpu_launches",
-               "clocks", "config", "impl", "steps_requested")
+               "clocks", "config", "impl", "steps_requested", "fp32_ir", "autotuned_grid", "autotuned_shapes",
+               "equiv_fp64_tflops")
 
 
 def run_workload(args, ws, rank, local, workload):
@@ -1185,7 +1275,7 @@ def main():
     ap.add_argument("--no-nested", action="store_true",
                     help="time only --workload (by default the mixed line also carries the other configurations)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline legs")
-    ap.add_argument("--case", choices=["update", "gemm", "panel", "diag", "peaks", "mixed", "tc", "chol", "inverse",
+    ap.add_argument("--case", choices=["update", "gemm", "lu", "panel", "diag", "peaks", "mixed", "tc", "chol", "inverse",
                                        "hpdinverse", "trtri", "ldl", "revchol", "det", "sweep32", "batched",
                                        "mixed_lu"],
                     default=None,
