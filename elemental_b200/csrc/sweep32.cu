@@ -9,19 +9,25 @@
 // dependency chain of a triangular solve is cut to n / S steps by explicit
 // inverses of the S x S diagonal super-blocks (S = 4 panels = 512):
 //   forward, super-block R:  y_R = W_R (z0_R + dz_R)          (phase A)
-//                            dz_Q -= L_QR y_R, Q > R          (phase B)
+//                            dz_Q -= L_QR y_R, Q > R + 1      (phase B)
+//                            dz_R+1 -= M_R (z0_R + dz_R)      (kind 2)
 //   backward, R downwards:   x_R = W_R^T (v_R + dv_R)          (phase A)
-//                            dv_Q -= L_RQ^T x_R, Q < R        (phase B)
+//                            dv_Q -= L_RQ^T x_R, Q < R - 1    (phase B)
+//                            dv_R-1 -= P_R^T (v_R + dv_R)     (kind 2)
+// with M_R = L_{R+1,R} W_R and P_R = W_R L_{R,R-1} formed once per factor:
+// the next super-block's deltas then need the same input as phase A of R, so
+// one step of the chain is one round of tile products instead of two.
 // Every piece of work is a tile item -- out(128 x 32) += T(128 x k) v(k x 32)
-// with T a 128-row tile of W_R or of L read through TMA -- and one
+// with T a 128-row tile of W_R, M_R, P_R or L read through TMA -- and one
 // cooperative launch works through a queue of items in an order that
-// respects their dependencies (phase A of R, then the phase-B items of R
-// that feed R + 1, then the rest of R's phase B, then phase A of R + 1, ...).
+// respects their dependencies (R's kind-2 items and phase A of R, then the
+// bulk phase-B items of the previous super-block, then R + 1's, ...).
 // CTAs take items from an atomic counter, start the item's TMA tile loads at
 // once, then wait (bounded) only for the counters of the items it depends on:
-// phase A of Q waits for all phase-B items that target Q, phase B of R for the
-// phase-A items of R.  No grid barrier separates the steps, so the serial
-// chain is the true dependency chain and the bulk of phase B overlaps it.
+// phase A and the kind-2 items of Q wait for all delta items that target Q,
+// phase B of R for the phase-A items of R.  Every item's dependencies lie
+// earlier in the queue, so the co-resident CTAs always make progress; no grid
+// barrier separates the steps, and the bulk of phase B overlaps the chain.
 // All results are accumulated with FP32 vector reductions into arrays zeroed
 // at the start.
 //
@@ -29,7 +35,7 @@
 // 128 diagonal-block inverses W_k (FP64, from the diagonal kernels) and the
 // off-diagonal blocks of L: X_kk = W_k, X_ij = -W_i sum_{k=j}^{i-1} L_ik X_kj
 // (block rows i = 1..3 of each super-block, one launch per i, all
-// super-blocks at once).
+// super-blocks at once), then M_R and P_R (one launch).
 #include <vector>
 
 #include "context.h"
@@ -45,6 +51,18 @@ constexpr int kTK = 32;          // k per TMA stage
 constexpr int kStages = 4;
 constexpr int kThreads = 256;
 constexpr int kRhs = 32;         // right-hand sides (nrhs <= 32 per launch)
+// Granularity of the items on the sweep's chain: the k split of the next
+// super-block's delta items and the k width of phase-A tiles (smaller: more,
+// shorter items per chain step)
+#ifndef EGPU_SWEEP_CRIT_SPLIT
+#define EGPU_SWEEP_CRIT_SPLIT 4
+#endif
+#ifndef EGPU_SWEEP_A_K
+#define EGPU_SWEEP_A_K 128
+#endif
+constexpr int kCritSplit = EGPU_SWEEP_CRIT_SPLIT;
+constexpr int kAK = EGPU_SWEEP_A_K;
+static_assert(kS % (kCritSplit * kTK) == 0 && kTM % kAK == 0 && kAK % kTK == 0, "chain item granularity");
 
 // shared-memory carve (floats), 1024-byte aligned pieces
 constexpr int kStageFloats = kTM * kTK;                     // 4096 floats = 16 KB
@@ -55,9 +73,11 @@ constexpr int kSmemBytes = kSmemFloats * 4 + 1024 + 128;  // + alignment slack +
 
 // An item: out[out_row .. +128) (+/-)= T[tile] * v[v_row + kbeg .. v_row + kend)
 struct Item {
-  short map;      // 0 L (rows contiguous), 1 L (columns), 2 W (rows contiguous), 3 W (columns)
+  short map;      // 0 L (rows contiguous), 1 L (columns), 2 W (rows contiguous), 3 W (columns),
+                  // 4 M (rows contiguous), 5 P (columns)
   short dir;      // 0 forward arrays, 1 backward arrays
-  short kind;     // 0 phase A (out: y/x of super-block, +), 1 phase B (out: deltas, -)
+  short kind;     // 0 phase A (out: y/x of super-block, +), 1 phase B (out: deltas, -),
+                  // 2 the next super-block's deltas from phase A's input (M / P tile, -)
   short nk;       // TMA stages
   int tm;         // tile coordinate along M (row of T, or column of T for maps 1/3)
   int tk;         // coordinate of k = kbeg along K in the tensor
@@ -118,6 +138,8 @@ __global__ void __launch_bounds__(kThreads, 1) sweep32_kernel(const __grid_const
                                                               const __grid_constant__ CUtensorMap mL1,
                                                               const __grid_constant__ CUtensorMap mW0,
                                                               const __grid_constant__ CUtensorMap mW1,
+                                                              const __grid_constant__ CUtensorMap mM0,
+                                                              const __grid_constant__ CUtensorMap mP1,
                                                               SweepDF p) {
   extern __shared__ float smem_raw[];
   float* sm = align1024(smem_raw);
@@ -155,8 +177,13 @@ __global__ void __launch_bounds__(kThreads, 1) sweep32_kernel(const __grid_const
     __syncthreads();
     if (idx >= p.items) break;
     const Item it = p.table[idx];
-    const bool mcontig = it.map == 0 || it.map == 2;
-    const CUtensorMap* mp = it.map == 0 ? &mL0 : it.map == 1 ? &mL1 : it.map == 2 ? &mW0 : &mW1;
+    const bool mcontig = it.map == 0 || it.map == 2 || it.map == 4;
+    const CUtensorMap* mp = it.map == 0   ? &mL0
+                            : it.map == 1 ? &mL1
+                            : it.map == 2 ? &mW0
+                            : it.map == 3 ? &mW1
+                            : it.map == 4 ? &mM0
+                                          : &mP1;
     // the tile does not depend on anything: start its loads now
     if (tid == 0) {
       for (int s = 0; s < min(kStages, (int)it.nk); ++s) issue(mp, mcontig, stages, full, s, it.tm, it.tk + s * kTK);
@@ -170,31 +197,41 @@ __global__ void __launch_bounds__(kThreads, 1) sweep32_kernel(const __grid_const
     }
     __syncthreads();
     ok = *s_ok != 0;
-    // v rows [vrow, vrow + 32 nk) -> smem.  Phase A: forward z0 + dz;
-    // backward (y, or z0 when only the backward sweep runs) + dv.  Phase B:
-    // the super-block's results y / x.
+    // v rows [vrow, vrow + 32 nk) -> smem.  Phase A (and kind 2): forward
+    // z0 + dz; backward (y, or z0 when only the backward sweep runs) + dv.
+    // Phase B: the super-block's results y / x.  Four rows' loads are in
+    // flight before any is stored.
     {
       const float* s0;
       const float* s1 = nullptr;
-      if (it.kind == 0) {
+      if (it.kind != 1) {
         s0 = it.dir == 0 ? p.Z0 : (p.out_backward == 2 ? p.Yf : p.Z0);
         s1 = it.dir == 0 ? p.Df : p.Db;
       } else {
         s0 = it.dir == 0 ? p.Yf : p.Yb;
       }
-      const int rows = it.nk * kTK;
-      for (int e = tid; e < rows * (kRhs / 4); e += kThreads) {
-        const int r = e / (kRhs / 4), q = e % (kRhs / 4);
-        const int gr = it.vrow + r;
-        float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (gr < p.n) {
-          v = __ldcg(reinterpret_cast<const float4*>(s0 + (size_t)gr * kRhs) + q);
-          if (s1 != nullptr) {
-            const float4 d = __ldcg(reinterpret_cast<const float4*>(s1 + (size_t)gr * kRhs) + q);
-            v.x += d.x; v.y += d.y; v.z += d.z; v.w += d.w;
+      const int total = it.nk * kTK * (kRhs / 4);
+      for (int e0 = tid; e0 < total; e0 += 4 * kThreads) {
+        float4 v[4], d[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const int e = e0 + u * kThreads;
+          const int gr = it.vrow + e / (kRhs / 4), q = e % (kRhs / 4);
+          v[u] = make_float4(0.f, 0.f, 0.f, 0.f);
+          d[u] = v[u];
+          if (e < total && gr < p.n) {
+            v[u] = __ldcg(reinterpret_cast<const float4*>(s0 + (size_t)gr * kRhs) + q);
+            if (s1 != nullptr) d[u] = __ldcg(reinterpret_cast<const float4*>(s1 + (size_t)gr * kRhs) + q);
           }
         }
-        reinterpret_cast<float4*>(vs + r * kRhs)[q] = v;
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const int e = e0 + u * kThreads;
+          if (e < total) {
+            const float4 w4 = make_float4(v[u].x + d[u].x, v[u].y + d[u].y, v[u].z + d[u].z, v[u].w + d[u].w);
+            reinterpret_cast<float4*>(vs + (e / (kRhs / 4)) * kRhs)[e % (kRhs / 4)] = w4;
+          }
+        }
       }
     }
     __syncthreads();
@@ -255,7 +292,8 @@ __global__ void __launch_bounds__(kThreads, 1) sweep32_kernel(const __grid_const
       __syncthreads();  // every thread is done with stage s
       if (tid == 0 && ks + kStages < it.nk) issue(mp, mcontig, stages, full, s, it.tm, it.tk + (ks + kStages) * kTK);
     }
-    // out rows: phase A adds into the results, phase B subtracts into the deltas
+    // out rows: phase A adds into the results, phase B and kind 2 subtract
+    // into the deltas
     {
       float* out = it.kind == 0 ? (it.dir == 0 ? p.Yf : p.Yb) : (it.dir == 0 ? p.Df : p.Db);
       const float sg = it.kind == 0 ? 1.f : -1.f;
@@ -300,10 +338,12 @@ struct Prod {
 
 constexpr int kBsLd = 129;  // padded: consecutive k of one column land in distinct banks
 
-// A rows from a_rows on read as zero (they may lie past the matrix); the
-// output's rows [0, out_rows) x columns [0, out_cols) are stored.
+// A rows from a_rows on, and rows k0 + k >= k_rows[t] of every B_t, read as
+// zero (they may lie past the matrix); the output's rows [0, out_rows) x
+// columns [0, out_cols) are stored.
 __device__ void tile128_products(const Prod* prods, int terms, float alpha, float* C, long long ldc,
-                                 float* As, float* Bs, int a_rows, int out_rows, int out_cols) {
+                                 float* As, float* Bs, int a_rows, int out_rows, int out_cols,
+                                 const int* k_rows = nullptr) {
   const int tid = threadIdx.x;
   const int tr = (tid & 15) * 8, tc = (tid >> 4) * 8;
   float acc[8][8];
@@ -318,9 +358,10 @@ __device__ void tile128_products(const Prod* prods, int terms, float alpha, floa
         const int k = e >> 7, r = e & 127;
         As[k * 128 + r] = r < a_rows ? prods[t].A[r + (long long)(k0 + k) * prods[t].lda] : 0.f;
       }
+      const int kr = k_rows ? k_rows[t] : kPB;
       for (int e = tid; e < 32 * 128; e += kThreads) {  // consecutive threads: consecutive k
         const int k = e & 31, c = e >> 5;
-        Bs[k * kBsLd + c] = prods[t].B[(k0 + k) + (long long)c * prods[t].ldb];
+        Bs[k * kBsLd + c] = (k0 + k) < kr ? prods[t].B[(k0 + k) + (long long)c * prods[t].ldb] : 0.f;
       }
       __syncthreads();
 #pragma unroll 4
@@ -404,6 +445,53 @@ __global__ void __launch_bounds__(kThreads) superinv_row_kernel(int n, int nsupe
   tile128_products(&w, 1, -1.f, X + bi * kPB + (size_t)(j * kPB) * kS, kS, As, Bs, kPB, rows_valid, kPB);
 }
 
+// The products that put one super-block step of each sweep on one phase:
+//   forward  (z = 0):  M_R = L_{R+1,R} W_R   for R = 0 .. nsuper - 2, in Mc
+//   backward (z = 1):  P_R = W_R L_{R,R-1}   for R = 1 .. nsuper - 1, in Pc
+// (Mc / Pc: kS rows, block R at columns R kS .. R kS + kS - 1, ld kS, as Wc.)
+// One CTA per 128 x 128 output tile (blockIdx.x = 4 mt + nt); W_R is lower
+// triangular, so only the k blocks where it is nonzero are multiplied.  Rows
+// and k indices past the matrix read as zero and every tile is written whole.
+__global__ void __launch_bounds__(kThreads) superprod_kernel(int n, int nsuper, const float* L, long long ldl,
+                                                             const float* Wc, float* Mc, float* Pc) {
+  extern __shared__ float sh[];
+  float* As = sh;
+  float* Bs = sh + 32 * 128;
+  const int mt = blockIdx.x >> 2, nt = blockIdx.x & 3;
+  const int z = blockIdx.z;
+  const int R = z == 0 ? (int)blockIdx.y : (int)blockIdx.y + 1;
+  const float* W = Wc + (size_t)R * kS * kS;
+  Prod prods[4];
+  int kr[4];
+  int terms = 0, a_rows = kPB;
+  if (z == 0) {  // M_R(mt, nt) = sum_t L_{R+1,R}(mt, t) W_R(t, nt), t >= nt
+    const long long r0 = (long long)(R + 1) * kS + mt * kPB;
+    a_rows = (int)max(0LL, min((long long)kPB, (long long)n - r0));
+    for (int t = nt; t < 4; ++t) {
+      prods[terms].A = L + r0 + (long long)(R * kS + t * kPB) * ldl;
+      prods[terms].lda = ldl;
+      prods[terms].B = W + t * kPB + (size_t)(nt * kPB) * kS;
+      prods[terms].ldb = kS;
+      kr[terms] = kPB;
+      ++terms;
+    }
+    if (a_rows == 0) terms = 0;  // the tile lies past the matrix: zeros
+  } else {  // P_R(mt, nt) = sum_t W_R(mt, t) L_{R,R-1}(t, nt), t <= mt, rows of R inside the matrix
+    for (int t = 0; t <= mt; ++t) {
+      const long long k0 = (long long)R * kS + t * kPB;
+      if (k0 >= n) break;
+      prods[terms].A = W + mt * kPB + (size_t)(t * kPB) * kS;
+      prods[terms].lda = kS;
+      prods[terms].B = L + k0 + (long long)((R - 1) * kS + nt * kPB) * ldl;
+      prods[terms].ldb = ldl;
+      kr[terms] = (int)min((long long)kPB, (long long)n - k0);
+      ++terms;
+    }
+  }
+  float* out = (z == 0 ? Mc : Pc) + (size_t)R * kS * kS + mt * kPB + (size_t)(nt * kPB) * kS;
+  tile128_products(prods, terms, 1.f, out, kS, As, Bs, a_rows, kPB, kPB, kr);
+}
+
 }  // namespace
 
 // ---- host: the item queue --------------------------------------------
@@ -422,9 +510,11 @@ struct CounterIx {
 static void build_items(int n, int G, int dir, bool after_forward, std::vector<Item>& out, const CounterIx& cx) {
   const int nsuper = (n + kS - 1) / kS;
   auto sb_of = [&](int R) { return std::min(kS, n - R * kS); };
-  std::vector<int> cd_need(nsuper, 0);  // phase-B items that will target each super-block
-  // phase-B items of super-block R: critical (the next super-block of the
-  // sweep, k split 4 ways) or bulk (the others)
+  std::vector<int> cd_need(nsuper, 0);  // delta items (kinds 1 and 2) that will target each super-block
+  // Delta items of super-block R: critical -- the next super-block of the
+  // sweep, from the M_R / P_R products and phase A's input (kind 2, k split
+  // kCritSplit ways), so they run beside phase A of R -- or bulk (phase B,
+  // the others)
   auto b_items = [&](int R, bool critical, std::vector<Item>& v) {
     const int r0 = R * kS, sb = sb_of(R);
     // targets: forward rows of later super-blocks; backward columns of earlier ones
@@ -439,25 +529,39 @@ static void build_items(int n, int G, int dir, bool after_forward, std::vector<I
     while (ksplit_bulk < 4 && bulk_tiles * ksplit_bulk * 2 <= G) ksplit_bulk *= 2;
     for (size_t t = critical ? 0 : 1; t < (critical ? std::min<size_t>(1, targets.size()) : targets.size()); ++t) {
       const int Q = targets[t], q0 = Q * kS, sq = sb_of(Q);
-      const int ksplit = t == 0 ? 4 : ksplit_bulk;  // the next super-block's items are on the chain: finest
+      const int ksplit = t == 0 ? kCritSplit : ksplit_bulk;  // the next super-block's items are on the chain
       const int kch = kS / ksplit;
       for (int m = 0; m < sq; m += kTM)
         for (int kp = 0; kp < ksplit; ++kp) {
           const int kb = kp * kch, ke = std::min(sb, kb + kch);
           if (ke <= kb) continue;
           Item it{};
-          it.map = dir == 0 ? 0 : 1;
           it.dir = dir;
-          it.kind = 1;
           it.nk = (ke - kb + kTK - 1) / kTK;
-          it.tm = q0 + m;      // forward: rows of L; backward: columns of L
-          it.tk = r0 + kb;     // forward: columns of L; backward: rows of L
           it.vrow = r0 + kb;
           it.orow = q0 + m;
           it.orows = std::min(kTM, sq - m);
-          it.dep0 = cx.cy(dir, R);
           it.need0 = 0;  // filled below
           it.dep1 = -1;
+          if (critical) {
+            // forward: rows m of M_R (block R at Mc columns R kS ..); backward:
+            // columns R kS + m of Pc, k along P_R's rows
+            it.map = dir == 0 ? 4 : 5;
+            it.kind = 2;
+            it.tm = dir == 0 ? m : R * kS + m;
+            it.tk = dir == 0 ? R * kS + kb : kb;
+            it.dep0 = cx.cd(dir, R);
+            if (dir == 1 && after_forward) {  // its input y_R: the forward phase A of R
+              it.dep1 = cx.cy(0, R);
+              it.need1 = 0;  // filled by the caller
+            }
+          } else {
+            it.map = dir == 0 ? 0 : 1;
+            it.kind = 1;
+            it.tm = q0 + m;      // forward: rows of L; backward: columns of L
+            it.tk = r0 + kb;     // forward: columns of L; backward: rows of L
+            it.dep0 = cx.cy(dir, R);
+          }
           it.done = cx.cd(dir, Q);
           ++cd_need[Q];
           v.push_back(it);
@@ -467,14 +571,15 @@ static void build_items(int n, int G, int dir, bool after_forward, std::vector<I
   auto a_items = [&](int R, std::vector<Item>& v) {
     const int r0 = R * kS, sb = sb_of(R);
     for (int mt = 0; mt < sb; mt += kTM)
-      for (int kt = 0; kt < sb; kt += kTM) {
-        // W_R lower: forward tile (mt, kt) nonzero for kt <= mt; W_R^T upper: kt >= mt
-        if (dir == 0 ? kt > mt : kt < mt) continue;
+      for (int kt = 0; kt < sb; kt += kAK) {
+        // W_R lower: the forward tile (rows mt.., k kt..) is nonzero when
+        // kt < mt + kTM; W_R^T upper: when kt + kAK > mt
+        if (dir == 0 ? kt >= mt + kTM : kt + kAK <= mt) continue;
         Item it{};
         it.map = dir == 0 ? 2 : 3;
         it.dir = dir;
         it.kind = 0;
-        it.nk = (std::min(kTM, sb - kt) + kTK - 1) / kTK;
+        it.nk = (std::min(kAK, sb - kt) + kTK - 1) / kTK;
         // W_R block in the (kS x kS nsuper) tensor: rows i, columns R kS + j
         it.tm = dir == 0 ? mt : R * kS + mt;
         it.tk = dir == 0 ? R * kS + kt : kt;
@@ -493,24 +598,26 @@ static void build_items(int n, int G, int dir, bool after_forward, std::vector<I
       }
   };
   const size_t first = out.size();
-  // dependency order with the chain first: A(R), then the bulk of the
-  // previous super-block's phase B, then R's items for the next super-block
-  // (phase A of R + 1 needs those and the earlier bulk, all queued before it)
+  // dependency order with the chain first: R's items for the next
+  // super-block and phase A of R (both wait for the deltas of R only), then
+  // the bulk of the previous super-block's phase B (phase A of R + 1 needs
+  // those and R's critical items, all queued before it)
   for (int s = 0; s <= nsuper; ++s) {
     const int R = dir == 0 ? s : nsuper - 1 - s;
     const int Rp = dir == 0 ? s - 1 : nsuper - s;  // the previous super-block of the sweep
+    if (s < nsuper) b_items(R, true, out);
     if (s < nsuper) a_items(R, out);
     if (s >= 1) b_items(Rp, false, out);
-    if (s < nsuper) b_items(R, true, out);
   }
-  // needs: phase A of R waits for every phase-B item targeting R, phase B of
-  // R for all phase-A items of R
+  // needs: phase A of R and R's critical items wait for every delta item
+  // targeting R; phase B of R for all phase-A items of R
   std::vector<int> a_count(nsuper, 0);
   for (size_t i = first; i < out.size(); ++i)
     if (out[i].kind == 0) ++a_count[(out[i].orow) / kS];
   for (size_t i = first; i < out.size(); ++i) {
     Item& it = out[i];
     if (it.kind == 0) it.need0 = cd_need[it.orow / kS];
+    else if (it.kind == 2) it.need0 = cd_need[it.vrow / kS];
     else it.need0 = a_count[it.vrow / kS];
   }
 }
@@ -520,17 +627,19 @@ size_t sweep32_ws_bytes(int n, int nrhs) {
   const int nsuper = (n + kS - 1) / kS;
   size_t b = 0;
   b += (size_t)nsuper * kS * kS * sizeof(float) + 1024;      // Wc
+  b += 2 * ((size_t)nsuper * kS * kS * sizeof(float) + 1024);  // Mc, Pc
   b += (size_t)nsuper * 4 * kPB * kPB * sizeof(float);       // temporaries of the inverse
   b += 5 * ((size_t)n * kRhs * sizeof(float) + 1024);        // Z0, Df, Yf, Db, Yb
   b += (size_t)(2 + 4 * nsuper) * sizeof(int) + 1024;        // counters
   b += 1024;                                                  // barrier
-  b += (size_t)2 * (nsuper * 10 + nsuper * nsuper * 16 + 64) * sizeof(Item) + 1024;  // item table (bound)
+  b += (size_t)2 * (nsuper * (4 * (kS / kAK) + 4 * kCritSplit) + nsuper * nsuper * 16 + 64) * sizeof(Item) +
+       1024;  // item table (bound)
   return b + 16 * 1024;  // every piece is 1024-aligned
 }
 
 namespace {
 struct SweepWs {
-  float *Wc, *tmp, *Z0, *Df, *Yf, *Db, *Yb;
+  float *Wc, *Mc, *Pc, *tmp, *Z0, *Df, *Yf, *Db, *Yb;
   int* counters;
   unsigned* bar;
   Item* table;
@@ -541,6 +650,8 @@ SweepWs carve(void* ws, int n) {
   uintptr_t b = reinterpret_cast<uintptr_t>(ws);
   auto take = [&](size_t bytes) { b = align_up(b, 1024); uintptr_t o = b; b += bytes; return o; };
   w.Wc = reinterpret_cast<float*>(take((size_t)nsuper * kS * kS * sizeof(float)));
+  w.Mc = reinterpret_cast<float*>(take((size_t)nsuper * kS * kS * sizeof(float)));
+  w.Pc = reinterpret_cast<float*>(take((size_t)nsuper * kS * kS * sizeof(float)));
   w.tmp = reinterpret_cast<float*>(take((size_t)nsuper * 4 * kPB * kPB * sizeof(float)));
   w.Z0 = reinterpret_cast<float*>(take((size_t)n * kRhs * sizeof(float)));
   w.Df = reinterpret_cast<float*>(take((size_t)n * kRhs * sizeof(float)));
@@ -575,6 +686,12 @@ int sweep32_prepare(cudaStream_t st, int n, const float* L, long long ldl, const
     count_launch();
     EGPU_CUDA_TRY(cudaGetLastError());
   }
+  if (nsuper > 1) {  // the one-phase chain products M_R and P_R (shb < 48 KB: no attribute needed)
+    TraceMark tp(st, kTraceOther, 2.0 * (nsuper - 1) * 2.0 * kS * kS * kS * 0.625, 24.0 * (nsuper - 1) * kS * kS);
+    superprod_kernel<<<dim3(16, nsuper - 1, 2), kThreads, shb, st>>>(n, nsuper, L, ldl, w.Wc, w.Mc, w.Pc);
+    count_launch();
+    EGPU_CUDA_TRY(cudaGetLastError());
+  }
   return EGPU_OK;
 }
 
@@ -598,16 +715,18 @@ int sweep32_solve(cudaStream_t st, int trans, int n, int nrhs, const float* L, l
       std::vector<int> ay(nsuper, 0);
       for (size_t i = 0; i < b0; ++i)
         if (items[i].kind == 0) ++ay[items[i].orow / kS];
-      for (size_t i = b0; i < items.size(); ++i)
-        if (items[i].dep1 >= 0) items[i].need1 = ay[items[i].orow / kS];
+      for (size_t i = b0; i < items.size(); ++i)  // the super-block whose y the item reads
+        if (items[i].dep1 >= 0) items[i].need1 = ay[(items[i].kind == 2 ? items[i].vrow : items[i].orow) / kS];
     }
   }
-  CUtensorMap m[4];
+  CUtensorMap m[6];
   // L: {n rows, n columns}; W: {kS rows, kS * nsuper columns}
   if (!make_tma_2d(&m[0], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, L, n, n, ldl * 4, 32, kTK, false) ||
       !make_tma_2d(&m[1], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, L, n, n, ldl * 4, kTK, kTM, true) ||
       !make_tma_2d(&m[2], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, w.Wc, kS, (uint64_t)kS * nsuper, kS * 4, 32, kTK, false) ||
-      !make_tma_2d(&m[3], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, w.Wc, kS, (uint64_t)kS * nsuper, kS * 4, kTK, kTM, true))
+      !make_tma_2d(&m[3], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, w.Wc, kS, (uint64_t)kS * nsuper, kS * 4, kTK, kTM, true) ||
+      !make_tma_2d(&m[4], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, w.Mc, kS, (uint64_t)kS * nsuper, kS * 4, 32, kTK, false) ||
+      !make_tma_2d(&m[5], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, w.Pc, kS, (uint64_t)kS * nsuper, kS * 4, kTK, kTM, true))
     return EGPU_ERR_TMA;
   static int attr_dev_mask = 0;
   int dev = 0;
@@ -637,7 +756,7 @@ int sweep32_solve(cudaStream_t st, int trans, int n, int nrhs, const float* L, l
   attr[0].val.cooperative = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  EGPU_CUDA_TRY(cudaLaunchKernelEx(&cfg, sweep32_kernel, m[0], m[1], m[2], m[3], p));
+  EGPU_CUDA_TRY(cudaLaunchKernelEx(&cfg, sweep32_kernel, m[0], m[1], m[2], m[3], m[4], m[5], p));
   count_launch();
   // (a copy from pageable host memory returns once the data is staged, so the
   // table's host vector may go)

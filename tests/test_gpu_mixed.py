@@ -36,18 +36,24 @@ def test_tc_gemm_split_full(handle, M, N, K, terms):
     assert err <= _bound(A, B, K, bits) + 2.0 ** -22 * np.abs(ref).max(), err
 
 
-def test_tc_gemm_split_lower_leaves_upper(handle):
-    n, K = 384, 128
+@pytest.mark.parametrize("n", [384, 1000])
+@pytest.mark.parametrize("beta", [0.0, 1.0])
+def test_tc_gemm_split_lower_leaves_upper(handle, n, beta):
+    # lower-triangle update (the mixed factorization's trailing update); with
+    # beta != 0 and ldc a multiple of 4 the C tiles are staged through shared
+    # memory by TMA, with a partial last tile row at n = 1000
+    K = 128
     A = inputs.normal(n, K, 21)
     C0 = np.full((n, n), 7.0, dtype=np.float32)
+    C0[np.tril_indices(n)] = inputs.normal(n, n, 22)[np.tril_indices(n)]
     dC = eg.colmajor_cuda(C0.astype(np.float64)).float().t().contiguous().t()
     dA = eg.colmajor_cuda(A)
-    handle.tc_gemm_split(dA, dA, dC, alpha=1.0, beta=0.0, lower=True, terms=3)
+    handle.tc_gemm_split(dA, dA, dC, alpha=-1.0, beta=beta, lower=True, terms=3)
     torch.cuda.synchronize()
     out = dC.cpu().numpy().astype(np.float64)
     low = np.tril(np.ones((n, n), bool))
-    ref = A @ A.T
-    assert np.abs(out[low] - ref[low]).max() <= _bound(A, A, K, 20)
+    ref = beta * C0.astype(np.float64) - A @ A.T
+    assert np.abs(out[low] - ref[low]).max() <= _bound(A, A, K, 20) + 2.0 ** -22 * np.abs(ref).max()
     assert np.all(out[~low] == 7.0)
 
 
