@@ -18,18 +18,10 @@
 //                  four per 32-wide k tile and term, into one of two TMEM
 //                  accumulators (256 columns) so that a tile's epilogue
 //                  overlaps the next tile's MMAs;
-//   warps 0-7    : epilogue, tcgen05.ld.32x32b of their 32 TMEM lanes (warp
-//                  e: lanes 32 (e % 4)..) and a coalesced store, one output
-//                  row per thread.  With beta != 0 and a TMA-addressable C,
-//                  C is staged through a 128 x 64 shared-memory buffer by
-//                  TMA, one half tile at a time: all eight warps work on one
-//                  half (warp e: columns 32 (e / 4)..), and the next half's
-//                  load (this tile's second, or the next tile's first) is
-//                  issued as soon as every epilogue thread has read the
-//                  current one, so the C reads overlap the arithmetic and
-//                  the stores.  Otherwise (beta == 0, or C not 16-byte
-//                  aligned with ldc % 4 == 0) each thread reads its 64 C
-//                  entries into registers before the accumulator is ready.
+//   warps 0-7    : epilogue, C rows read into registers before the
+//                  accumulator is ready, then tcgen05.ld.32x32b of their 32
+//                  TMEM lanes (warp e: lanes 32 (e % 4).., columns 64 (e / 4)..)
+//                  and a coalesced store, one output row per thread.
 #include <cudaTypedefs.h>
 
 #include "internal.h"
@@ -43,28 +35,14 @@ constexpr int kTcThreads = 320;  // 8 epilogue warps, producer, MMA issuer
 constexpr int kTcEpiWarps = 8;
 constexpr int kTcProdWarp = 8, kTcMmaWarp = 9;
 constexpr int kTcTileBytes = kTcBM * kTcBK * 4;  // 16 KiB per operand tile
-constexpr int kTcCHalfBytes = kTcBM * 64 * 4;     // 32 KiB: half a C tile (128 rows x 64 columns)
 
 template <int NT>
 struct TcShape {
   static constexpr int kOps = NT == 1 ? 2 : 4;  // A_hi, B_hi (+ A_lo, B_lo)
   static constexpr int kStages = NT == 1 ? 6 : 3;
   static constexpr int kStageBytes = kOps * kTcTileBytes;
-  static constexpr int kSmemBytes = kStages * kStageBytes + kTcCHalfBytes + 1024 /*align*/ + 256 /*barriers*/;
+  static constexpr int kSmemBytes = kStages * kStageBytes + 1024 /*align*/ + 256 /*barriers*/;
 };
-static_assert(TcShape<3>::kSmemBytes <= 227 * 1024 && TcShape<1>::kSmemBytes <= 227 * 1024, "shared memory");
-
-// Barrier 1 across the 256 epilogue threads (warps 0-7) with an OR
-// reduction: every thread gets the OR of the flags.
-__device__ __forceinline__ bool epi_bar_or(bool v) {
-  uint32_t r;
-  asm volatile(
-      "{\n .reg .pred p, q;\n setp.ne.u32 p, %1, 0;\n bar.red.or.pred q, 1, 256, p;\n selp.u32 %0, 1, 0, q;\n}\n"
-      : "=r"(r)
-      : "r"((uint32_t)v)
-      : "memory");
-  return r != 0;
-}
 
 struct TcParams {
   float* C;
@@ -143,24 +121,21 @@ __device__ __forceinline__ void tc_tile_of(const TcParams& p, int bid, int& tm, 
 
 }  // namespace
 
-template <int NT, bool CPF>
+template <int NT>
 __global__ void __maxnreg__(200) tc_gemm_kernel(const __grid_constant__ CUtensorMap mah,
                                                                  const __grid_constant__ CUtensorMap mbh,
                                                                  const __grid_constant__ CUtensorMap mal,
                                                                  const __grid_constant__ CUtensorMap mbl,
-                                                                 const __grid_constant__ CUtensorMap mc,
                                                                  TcParams p, int ntiles, int per_cta) {
   using S = TcShape<NT>;
   extern __shared__ unsigned char tc_smem_raw[];
   unsigned char* smem = reinterpret_cast<unsigned char*>(
       (reinterpret_cast<uintptr_t>(tc_smem_raw) + 1023) & ~uintptr_t(1023));  // swizzle atoms: 1 KiB aligned
-  float* cbuf = reinterpret_cast<float*>(smem + S::kStages * S::kStageBytes);  // C half tile (CPF)
-  uint64_t* full = reinterpret_cast<uint64_t*>(smem + S::kStages * S::kStageBytes + kTcCHalfBytes);
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + S::kStages * S::kStageBytes);
   uint64_t* empty = full + S::kStages;
   uint64_t* tfull = empty + S::kStages;  // [2] accumulator ready
   uint64_t* tempty = tfull + 2;          // [2] accumulator drained (8 epilogue warps arrive)
-  uint64_t* cfull = tempty + 2;          // C half tile landed in cbuf
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(cfull + 1);
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(tempty + 2);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -174,7 +149,6 @@ __global__ void __maxnreg__(200) tc_gemm_kernel(const __grid_constant__ CUtensor
   if (tid == 0) {
     for (int s = 0; s < S::kStages; ++s) { mbar_init(&full[s], 1); mbar_init(&empty[s], 1); }
     for (int a = 0; a < 2; ++a) { mbar_init(&tfull[a], 1); mbar_init(&tempty[a], kTcEpiWarps); }
-    mbar_init(cfull, 1);
     *abort_flag = 0;
     fence_mbar_init();
   }
@@ -246,79 +220,6 @@ __global__ void __maxnreg__(200) tc_gemm_kernel(const __grid_constant__ CUtensor
         tc_commit(&tfull[a]);  // accumulator a complete
       }
     }
-  } else if constexpr (CPF) {
-    // ---- epilogue, C through shared memory (beta != 0): per tile, two
-    // 64-column halves; warp e reads TMEM lanes 32 (e % 4) .. and columns
-    // 32 (e / 4) .. of the half; each thread owns one output row.  Thread 0
-    // issues the TMA load of the next half once every epilogue thread has
-    // read the current one (barrier 1, which also makes a failed wait
-    // anywhere stop all eight warps together).
-    const int q = warp & 3, sub = warp >> 2;
-    auto issue_c = [&](int t, int h) {
-      int tm, tn;
-      tc_tile_of(p, t, tm, tn);
-      mbar_expect_tx(cfull, kTcCHalfBytes);
-      tma_load_2d(cbuf, &mc, cfull, tm * kTcBM, tn * kTcBN + h * 64);
-    };
-    if (tid == 0 && t_first < t_end) issue_c(t_first, 0);
-    uint32_t cpar = 0;
-    int i = 0;
-    bool run = true;
-    for (int t = t_first; t < t_end && run; ++t, ++i) {
-      int tm, tn;
-      tc_tile_of(p, t, tm, tn);
-      const int r = tm * kTcBM + q * 32 + lane;
-      const int a = i & 1;
-      for (int h = 0; h < 2; ++h) {
-        const int n0 = tn * kTcBN + h * 64 + sub * 32;
-        // columns n0 + j, j < jmax, of row r are written (bounds, lower triangle)
-        int jmax = r < p.M ? min(32, p.N - n0) : 0;
-        if (p.tri) jmax = min(jmax, r - n0 + 1);
-        bool good = mbar_wait_bounded(cfull, cpar);
-        cpar ^= 1u;
-        float cv[32];
-#pragma unroll
-        for (int j = 0; j < 32; ++j) cv[j] = cbuf[(sub * 32 + j) * kTcBM + q * 32 + lane];
-        fence_proxy_async_smem();  // these reads before the next TMA write into cbuf
-        if (h == 0 && good) good = mbar_wait_bounded(&tfull[a], (uint32_t)(i >> 1) & 1u);
-        if (epi_bar_or(!good || *abort_flag)) {
-          if (tid == 0) { *abort_flag = 1; set_status(p.status, kTimeout, 105); }
-          run = false;
-          break;
-        }
-        if (tid == 0) {
-          if (h == 0) issue_c(t, 1);
-          else if (t + 1 < t_end) issue_c(t + 1, 0);
-        }
-        tc_fence_after();
-        float v[32];
-        tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(a * kTcBN + h * 64 + sub * 32), v);
-        float* cp = p.C + (long long)n0 * p.ldc + (r < p.M ? r : 0);
-#pragma unroll
-        for (int j = 0; j < 32; ++j, cp += p.ldc) {
-          v[j] = j < jmax ? fmaf(p.alpha, v[j], p.beta * cv[j]) : 0.0f;
-          if (j < jmax) *cp = v[j];
-        }
-        if (p.sh != nullptr && r >= p.srow0 && r < p.M && n0 < p.swidth) {  // the result's TF32 split
-          float* sh = p.sh + (long long)(r - p.srow0) * p.sldk + n0;
-          float* sl = p.sl + (long long)(r - p.srow0) * p.sldk + n0;
-#pragma unroll
-          for (int j4 = 0; j4 < 32; j4 += 4) {
-            float4 h4, l4;
-            h4.x = tf32_rna(v[j4]);     l4.x = tf32_rna(v[j4] - h4.x);
-            h4.y = tf32_rna(v[j4 + 1]); l4.y = tf32_rna(v[j4 + 1] - h4.y);
-            h4.z = tf32_rna(v[j4 + 2]); l4.z = tf32_rna(v[j4 + 2] - h4.z);
-            h4.w = tf32_rna(v[j4 + 3]); l4.w = tf32_rna(v[j4 + 3] - h4.w);
-            *reinterpret_cast<float4*>(sh + j4) = h4;
-            *reinterpret_cast<float4*>(sl + j4) = l4;
-          }
-        }
-      }
-      if (!run) break;
-      tc_fence_before();
-      __syncwarp();
-      if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&tempty[a])) : "memory");
-    }
   } else {
     // ---- epilogue: warp e reads TMEM lanes 32 (e % 4) .. (its quarter) and
     // columns 64 (e / 4) .. of each tile; each thread owns one output row.
@@ -388,11 +289,11 @@ __global__ void __maxnreg__(200) tc_gemm_kernel(const __grid_constant__ CUtensor
   }
 }
 
-template <int NT, bool CPF>
+template <int NT>
 static cudaError_t tc_launch_variant(cudaStream_t st, const CUtensorMap& mah, const CUtensorMap& mbh,
-                                     const CUtensorMap& mal, const CUtensorMap& mbl, const CUtensorMap& mc,
-                                     const TcParams& p, long long nblocks) {
-  auto kern = tc_gemm_kernel<NT, CPF>;
+                                     const CUtensorMap& mal, const CUtensorMap& mbl, const TcParams& p,
+                                     long long nblocks) {
+  auto kern = tc_gemm_kernel<NT>;
   static unsigned attr_mask = 0;
   int dev = 0;
   cudaGetDevice(&dev);
@@ -405,7 +306,7 @@ static cudaError_t tc_launch_variant(cudaStream_t st, const CUtensorMap& mah, co
   cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, dev);
   const int per_cta = (int)std::max<long long>(1, std::min<long long>(8, nblocks / (4LL * dev_sms)));
   const unsigned grid = (unsigned)((nblocks + per_cta - 1) / per_cta);
-  kern<<<grid, kTcThreads, TcShape<NT>::kSmemBytes, st>>>(mah, mbh, mal, mbl, mc, p, (int)nblocks, per_cta);
+  kern<<<grid, kTcThreads, TcShape<NT>::kSmemBytes, st>>>(mah, mbh, mal, mbl, p, (int)nblocks, per_cta);
   count_launch();
   return cudaGetLastError();
 }
@@ -450,19 +351,8 @@ int launch_tc_gemm(cudaStream_t st, int M, int N, int K, float alpha, const floa
   const double bytes = 4.0 * terms * ((double)M * K + (double)N * K) / (terms == 3 ? 1.5 : 1.0) +
                        4.0 * (beta == 0.0f ? 1.0 : 2.0) * M * N * (tri ? 0.5 : 1.0);
   TraceMark tm(st, kTraceTc, flops, bytes);
-  // C staged through shared memory by TMA when it is read (beta != 0) and
-  // TMA-addressable (16-byte aligned base, ldc a multiple of 4)
-  CUtensorMap mc = mah;
-  const bool cpf = beta != 0.0f && reinterpret_cast<uintptr_t>(C) % 16 == 0 && ldc % 4 == 0 &&
-                   make_tma_2d(&mc, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, C, M, N, (uint64_t)ldc * sizeof(float), kTcBM,
-                               64, false);
-  cudaError_t e;
-  if (terms == 1)
-    e = cpf ? tc_launch_variant<1, true>(st, mah, mbh, mal, mbl, mc, p, nblocks)
-            : tc_launch_variant<1, false>(st, mah, mbh, mal, mbl, mc, p, nblocks);
-  else
-    e = cpf ? tc_launch_variant<3, true>(st, mah, mbh, mal, mbl, mc, p, nblocks)
-            : tc_launch_variant<3, false>(st, mah, mbh, mal, mbl, mc, p, nblocks);
+  cudaError_t e = terms == 1 ? tc_launch_variant<1>(st, mah, mbh, mal, mbl, p, nblocks)
+                             : tc_launch_variant<3>(st, mah, mbh, mal, mbl, p, nblocks);
   if (e != cudaSuccess) {
     set_last_error(e, "tc_gemm launch", __FILE__, __LINE__);
     return EGPU_ERR_CUDA;
