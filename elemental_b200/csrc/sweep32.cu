@@ -288,9 +288,11 @@ __global__ void __launch_bounds__(kThreads, 1) sweep32_kernel(const __grid_const
           }
         }
       }
-      fence_proxy_async_smem();
-      __syncthreads();  // every thread is done with stage s
-      if (tid == 0 && ks + kStages < it.nk) issue(mp, mcontig, stages, full, s, it.tm, it.tk + (ks + kStages) * kTK);
+      if (ks + kStages < it.nk) {  // stage s is refilled (item-uniform): every thread done with it first
+        fence_proxy_async_smem();
+        __syncthreads();
+        if (tid == 0) issue(mp, mcontig, stages, full, s, it.tm, it.tk + (ks + kStages) * kTK);
+      }
     }
     // out rows: phase A adds into the results, phase B and kind 2 subtract
     // into the deltas
@@ -309,6 +311,7 @@ __global__ void __launch_bounds__(kThreads, 1) sweep32_kernel(const __grid_const
       }
     }
     __threadfence();
+    fence_proxy_async_smem();  // this item's stage reads before the next item's TMA writes
     __syncthreads();
     if (tid == 0) atomicAdd(p.counters + it.done, 1);
   }
