@@ -286,27 +286,6 @@ __device__ inline void warp_trinv16_cols(const double* S, int lds, int o, double
     for (int k = 0; k < 16; ++k) X[k + lane * ldx] = x[k];
 }
 
-// Columns of X = inv(L) for the 16 x 16 lower block L at S[o.., o..], given
-// rinv = 1 / L[lane][lane] in lane `lane` (< 16), formed right-looking: lane
-// c keeps the partial sums s_i = sum_{m<i} L[i][m] x[m] of its column, and at
-// step m sets x[m] = (delta_mc - s_m) rinv_m and adds L[i][m] x[m] to every
-// later s_i.  The dependent chain per step is one multiply and one FMA (the
-// left-looking form chains the whole sum of each row).
-__device__ inline void warp_trinv16_cols_right(const double* S, int lds, int o, double rinv, double* X, int ldx) {
-  const int lane = threadIdx.x & 31;
-  double acc[16];
-#pragma unroll
-  for (int i = 0; i < 16; ++i) acc[i] = 0.0;
-#pragma unroll
-  for (int m = 0; m < 16; ++m) {
-    const double rm = __shfl_sync(0xffffffffu, rinv, m);
-    const double xm = (m < lane) ? 0.0 : (m == lane ? rm : -acc[m] * rm);
-    if (lane < 16) X[m + lane * ldx] = xm;  // off the chain
-#pragma unroll
-    for (int i = m + 1; i < 16; ++i) acc[i] = fma(S[(o + i) + (o + m) * lds], xm, acc[i]);
-  }
-}
-
 // Cholesky of one 16 x 16 lower block at S[o.., o..] by one warp, rows in
 // registers (lane i < 16 holds row i), pivots broadcast by shuffles; the
 // factor goes back into S and its inverse into X (16 x 16, ld ldx).
@@ -345,7 +324,7 @@ __device__ inline int warp_chol16(double* S, int lds, int o, double* X, int ldx)
   for (int k = 0; k < 16; ++k)
     if (act && k <= lane) S[(o + lane) + (o + k) * lds] = d[k];
   __syncwarp();
-  warp_trinv16_cols_right(S, lds, o, myr, X, ldx);
+  warp_trinv16_cols(S, lds, o, myr, X, ldx);
   return 0;
 }
 
