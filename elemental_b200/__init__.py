@@ -118,6 +118,7 @@ def _declare(L):
         "egpu_dposv_batched": ([H, I, P, P, P, P, P, P, P], I),
         "egpu_dposv_mixed": ([H, I, I, I, P, I, P, I, P, I, I, D, P, P], I),
         "egpu_tc_gemm_split": ([H, I, I, I, D, P, I, P, I, D, P, I, I, I], I),
+        "egpu_sweep32_queue": ([I, I, I, P, I], I),
         "egpu_host_dposv_mixed": ([H, I, I, I, P, I, P, I, P, I, I, D, P, P], I),
         "egpu_mixed_gmres_iterations": ([H], I),
         "egpu_set_mixed_policy": ([H, I], I),
@@ -246,6 +247,20 @@ def _device_vec(t, count: int, dtype: str, device: int):
     if not t.is_contiguous() or t.numel() < count:
         raise ValueError(f"expected a contiguous vector of at least {count} elements, got shape {tuple(t.shape)}")
     return ctypes.c_void_p(t.data_ptr())
+
+
+def sweep32_queue(n: int, trans: int, sm_count: int = 148):
+    """The tile-item queue the FP32 sweep launches for order n
+    (egpu_sweep32_queue; host only): an int32 array of shape (items, 14) with
+    columns map, dir, kind, nk, tm, tk, vrow, orow, orows, dep0, need0, dep1,
+    need1, done."""
+    import numpy as np
+    cnt = lib().egpu_sweep32_queue(n, trans, sm_count, None, 0)
+    _check(min(cnt, 0))
+    out = np.zeros((max(cnt, 1), 14), dtype=np.int32)
+    got = lib().egpu_sweep32_queue(n, trans, sm_count, out.ctypes.data_as(ctypes.c_void_p), cnt)
+    _check(min(got, 0))
+    return out[:cnt]
 
 
 def partition_systems(n, kind, parts: int):

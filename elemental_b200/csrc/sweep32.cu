@@ -625,6 +625,26 @@ static void build_items(int n, int G, int dir, bool after_forward, std::vector<I
   }
 }
 
+// The whole queue of one launch: forward (trans 0), backward (1) or both
+// (2), the backward phase A and kind-2 items of R then also waiting for the
+// forward phase A of R (whose y they read).
+static void build_queue(int n, int trans, int sm_count, std::vector<Item>& items) {
+  const int nsuper = (n + kS - 1) / kS;
+  const CounterIx cx{nsuper};
+  if (trans == 0 || trans == 2) build_items(n, sm_count, 0, false, items, cx);
+  if (trans == 1 || trans == 2) {
+    const size_t b0 = items.size();
+    build_items(n, sm_count, 1, trans == 2, items, cx);
+    if (trans == 2) {
+      std::vector<int> ay(nsuper, 0);
+      for (size_t i = 0; i < b0; ++i)
+        if (items[i].kind == 0) ++ay[items[i].orow / kS];
+      for (size_t i = b0; i < items.size(); ++i)  // the super-block whose y the item reads
+        if (items[i].dep1 >= 0) items[i].need1 = ay[(items[i].kind == 2 ? items[i].vrow : items[i].orow) / kS];
+    }
+  }
+}
+
 size_t sweep32_ws_bytes(int n, int nrhs) {
   (void)nrhs;
   const int nsuper = (n + kS - 1) / kS;
@@ -710,18 +730,7 @@ int sweep32_solve(cudaStream_t st, int trans, int n, int nrhs, const float* L, l
   const SweepWs w = carve(ws, n);
   const CounterIx cx{nsuper};
   std::vector<Item> items;
-  if (trans == 0 || trans == 2) build_items(n, sm_count, 0, false, items, cx);
-  if (trans == 1 || trans == 2) {
-    const size_t b0 = items.size();
-    build_items(n, sm_count, 1, trans == 2, items, cx);
-    if (trans == 2) {  // backward phase A of R also waits for the forward phase A of R
-      std::vector<int> ay(nsuper, 0);
-      for (size_t i = 0; i < b0; ++i)
-        if (items[i].kind == 0) ++ay[items[i].orow / kS];
-      for (size_t i = b0; i < items.size(); ++i)  // the super-block whose y the item reads
-        if (items[i].dep1 >= 0) items[i].need1 = ay[(items[i].kind == 2 ? items[i].vrow : items[i].orow) / kS];
-    }
-  }
+  build_queue(n, trans, sm_count, items);
   CUtensorMap m[6];
   // L: {n rows, n columns}; W: {kS rows, kS * nsuper columns}
   if (!make_tma_2d(&m[0], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, L, n, n, ldl * 4, 32, kTK, false) ||
@@ -784,6 +793,23 @@ __global__ void widen_diag_blocks_kernel(int n, const float* L, long long ldl, d
 }  // namespace egpu
 
 using namespace egpu;
+
+// Host-only view of the queue (no device work): 14 ints per item.
+extern "C" int egpu_sweep32_queue(int n, int trans, int sm_count, int* out, int max_items) {
+  if (n < 1 || trans < 0 || trans > 2 || sm_count < 1 || max_items < 0) return EGPU_ERR_ARG;
+  std::vector<Item> items;
+  build_queue(n, trans, sm_count, items);
+  const int cnt = (int)items.size();
+  if (out != nullptr) {
+    for (int i = 0; i < std::min(cnt, max_items); ++i) {
+      const Item& it = items[i];
+      const int v[14] = {it.map, it.dir, it.kind, it.nk, it.tm, it.tk, it.vrow, it.orow, it.orows,
+                         it.dep0, it.need0, it.dep1, it.need1, it.done};
+      for (int k = 0; k < 14; ++k) out[(size_t)i * 14 + k] = v[k];
+    }
+  }
+  return cnt;
+}
 
 extern "C" int egpu_sweep32_solve(egpu_handle h, int trans, int n, int nrhs, const float* dL, int ldl, double* dX,
                                   int ldx) {

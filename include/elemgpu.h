@@ -341,6 +341,20 @@ EGPU_API int egpu_tc_gemm_split(egpu_handle h, int M, int N, int K, double alpha
 EGPU_API int egpu_sweep32_solve(egpu_handle h, int trans, int n, int nrhs, const float* dL, int ldl, double* dX,
                                 int ldx);
 
+/* The work queue egpu_sweep32_solve launches for order n (host only, no
+ * device needed; for tests and profiling, no counterpart in the reference):
+ * returns the number of tile items and, when out != NULL, writes up to
+ * max_items of them, 14 ints each in queue order -- tile map (0 L rows, 1 L
+ * columns, 2 / 3 super-block inverse rows / columns, 4 L_{R+1,R} W_R rows,
+ * 5 W_R L_{R,R-1} columns), direction, kind (0 super-block product, 1 bulk
+ * delta, 2 next-block delta from the same input as kind 0), k chunks of 32,
+ * tile coordinates (M, K), first input row, first output row, output rows,
+ * then the dependency counter / count pairs (second counter -1: none) and the
+ * counter the item increments.  Counters: 0 queue, 1 abort, then per
+ * direction d and super-block R: 2 + 2 (d nsuper + R) (its kind-0 items
+ * done) and 3 + 2 (d nsuper + R) (the delta items targeting R done). */
+EGPU_API int egpu_sweep32_queue(int n, int trans, int sm_count, int* out, int max_items);
+
 /* Batched HPDSolve(LOWER, NORMAL, A_i, B_i) (HPDSolve.hpp:18-28) for `count`
  * independent systems of uneven orders n[i] <= 512 with nrhs[i] <= 16, in one
  * persistent launch (one CTA per system at a time, largest first).  n, nrhs,
